@@ -1,0 +1,400 @@
+/*
+ * fdtd_oracle.c -- TEST INFRASTRUCTURE.  CPU restatement (FP64, plain loops)
+ * of rfsyn's FDTD time loop, used only by tests/, smoke() and the CPU leg of
+ * bench.py as the checker.  Never linked into the product.
+ *
+ * Parity pin: tests compare every function here against rfsyn itself built
+ * from its sources (oracle/_ref, recipe in oracle/Makefile) and against the
+ * committed golden fixtures in tests/golden/.
+ *
+ * Followed, line by line in arithmetic order:
+ *   grid / dt / index wrap ....... engine/fdtd/grid.c:7-46, grid.h:21-30
+ *   CPML profiles ................ engine/fdtd/cpml.c:21-150
+ *   cpml_term .................... engine/fdtd/cpml.h:46-51
+ *   H update (CPML, vacuum) ...... engine/fdtd/cpml.c:176-219, grid.c:62-90
+ *   E update with materials ...... engine/fdtd/materials.c:911-1060
+ *   material coefficients ........ engine/fdtd/materials.c:92-125
+ *   box / override semantics ..... engine/fdtd/materials.c:476-636
+ *   2x2 tensor edge .............. engine/fdtd/materials.c:836-903
+ *   sources ...................... engine/fdtd/source.c:8-57
+ *   probes, DFT .................. engine/fdtd/probe.c:40-92
+ * The data structures are the plainest possible (dense per-component override
+ * and tensor planes, full-grid psi) so the restatement is easy to audit.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "scene.h"
+
+#define O_C0 299792458.0
+#define O_EPS0 8.8541878128e-12
+#define O_MU0 1.25663706212e-6
+#define O_PI 3.14159265358979323846
+
+typedef struct {
+    size_t n[3];          /* nx, ny, nz */
+    unsigned per;
+    double dx, dt;
+    size_t total;
+    double *E[3], *H[3];
+    /* CPML: per axis, integer (m) and half (h) profiles */
+    int cpml;
+    double *km[3], *bm[3], *am[3], *kh[3], *bh[3], *ah[3];
+    double *psiH[3][2], *psiE[3][2];
+    /* materials */
+    uint8_t *id;
+    double tca[256], tcb[256], teps[256], tsig[256];
+    size_t ntab;
+    uint8_t *has_ovr[3];
+    double *oca[3], *ocb[3];
+    uint8_t *has_t[2];
+    double *tm11[2], *tm12[2], *tm22[2], *tscale[2];
+} orc_t;
+
+static int periodic(const orc_t *o, int a) { return (o->per >> a) & 1u; }
+
+/* grid.h:25-30 */
+static size_t at(const orc_t *o, size_t i, size_t j, size_t k) {
+    if (periodic(o, 0)) i %= o->n[0];
+    if (periodic(o, 1)) j %= o->n[1];
+    if (periodic(o, 2)) k %= o->n[2];
+    return (i * (o->n[1] + 1) + j) * (o->n[2] + 1) + k;
+}
+
+static size_t back(size_t q, size_t n) { return q == 0 ? n - 1 : q - 1; }
+
+/* cpml.c:21-89, one axis */
+static void profiles(orc_t *o, int a, const scn_scene_t *s, double sigma_max) {
+    size_t n = o->n[a];
+    o->km[a] = malloc((n + 1) * 8); o->bm[a] = malloc((n + 1) * 8); o->am[a] = malloc((n + 1) * 8);
+    o->kh[a] = malloc(n * 8); o->bh[a] = malloc(n * 8); o->ah[a] = malloc(n * 8);
+    double d = (double)s->npml * o->dx, len = (double)n * o->dx;
+    for (size_t q = 0; q < 2 * n + 1; q++) {
+        /* even q: integer position q/2; odd q: half position */
+        int half = q & 1;
+        size_t idx = q / 2;
+        double x = half ? ((double)idx + 0.5) * o->dx : (double)idx * o->dx;
+        double rho = -1.0;
+        if (x < d) rho = d - x;
+        else if (x > len - d) rho = x - (len - d);
+        double kinv = 1.0, b = 1.0, av = 0.0;
+        if (rho >= 0.0 && !periodic(o, a)) {
+            double r = rho / d;
+            if (r > 1.0) r = 1.0;
+            double sg = sigma_max * pow(r, s->m);
+            double kp = 1.0 + (s->kappa_max - 1.0) * pow(r, s->m);
+            double al = s->alpha_max * pow(1.0 - r, s->ma);
+            b = exp(-(sg / kp + al) * o->dt / O_EPS0);
+            av = (sg > 0.0) ? sg * (b - 1.0) / (o->dx * kp * (sg + kp * al)) : 0.0;
+            kinv = 1.0 / kp;
+        }
+        if (half) { o->kh[a][idx] = kinv; o->bh[a][idx] = b; o->ah[a][idx] = av; }
+        else { o->km[a][idx] = kinv; o->bm[a][idx] = b; o->am[a][idx] = av; }
+    }
+}
+
+static void orc_free(orc_t *o) {
+    for (int c = 0; c < 3; c++) {
+        free(o->E[c]); free(o->H[c]);
+        free(o->km[c]); free(o->bm[c]); free(o->am[c]); free(o->kh[c]); free(o->bh[c]); free(o->ah[c]);
+        for (int t = 0; t < 2; t++) { free(o->psiH[c][t]); free(o->psiE[c][t]); }
+        free(o->has_ovr[c]); free(o->oca[c]); free(o->ocb[c]);
+    }
+    for (int c = 0; c < 2; c++) { free(o->has_t[c]); free(o->tm11[c]); free(o->tm12[c]); free(o->tm22[c]); free(o->tscale[c]); }
+    free(o->id);
+}
+
+/* materials.c:92-125 */
+static int coeff(const orc_t *o, double eps_r, double sigma, double *ca, double *cb) {
+    if (!isfinite(eps_r) || eps_r < 1.0 || !isfinite(sigma) || sigma < 0.0) return -1;
+    double eps = eps_r * O_EPS0;
+    double loss = (sigma * o->dt) / (2.0 * eps);
+    double b = o->dt / (eps * o->dx);
+    *ca = (1.0 - loss) / (1.0 + loss);
+    *cb = b / (1.0 + loss);
+    return 0;
+}
+
+static int table_id(orc_t *o, double eps_r, double sigma) {
+    for (size_t q = 0; q < o->ntab; q++)
+        if (o->teps[q] == eps_r && o->tsig[q] == sigma) return (int)q;
+    if (o->ntab >= 256) return -1;
+    if (coeff(o, eps_r, sigma, &o->tca[o->ntab], &o->tcb[o->ntab]) != 0) return -1;
+    o->teps[o->ntab] = eps_r;
+    o->tsig[o->ntab] = sigma;
+    return (int)o->ntab++;
+}
+
+static int orc_init(orc_t *o, const scn_scene_t *s) {
+    memset(o, 0, sizeof(*o));
+    o->n[0] = s->nx; o->n[1] = s->ny; o->n[2] = s->nz;
+    o->per = s->periodic;
+    o->dx = s->dx;
+    o->dt = s->courant * (s->dx / (O_C0 * sqrt(3.0)));
+    o->total = (s->nx + 1) * (s->ny + 1) * (s->nz + 1);
+    for (int c = 0; c < 3; c++) {
+        o->E[c] = calloc(o->total, 8);
+        o->H[c] = calloc(o->total, 8);
+        o->has_ovr[c] = calloc(o->total, 1);
+        o->oca[c] = calloc(o->total, 8);
+        o->ocb[c] = calloc(o->total, 8);
+        if (!o->E[c] || !o->H[c] || !o->has_ovr[c] || !o->oca[c] || !o->ocb[c]) return -1;
+    }
+    for (int c = 0; c < 2; c++) {
+        o->has_t[c] = calloc(o->total, 1);
+        o->tm11[c] = calloc(o->total, 8); o->tm12[c] = calloc(o->total, 8);
+        o->tm22[c] = calloc(o->total, 8); o->tscale[c] = calloc(o->total, 8);
+        if (!o->has_t[c] || !o->tm11[c] || !o->tm12[c] || !o->tm22[c] || !o->tscale[c]) return -1;
+    }
+    o->id = calloc(o->total, 1);
+    if (!o->id) return -1;
+    table_id(o, 1.0, 0.0);
+    if (s->npml) {
+        o->cpml = 1;
+        double eta0 = sqrt(O_MU0 / O_EPS0);
+        double sigma_max = -(s->m + 1.0) * log(s->r0) / (2.0 * eta0 * (double)s->npml * o->dx);
+        for (int a = 0; a < 3; a++) profiles(o, a, s, sigma_max);
+        for (int c = 0; c < 3; c++)
+            for (int t = 0; t < 2; t++) {
+                o->psiH[c][t] = calloc(o->total, 8);
+                o->psiE[c][t] = calloc(o->total, 8);
+                if (!o->psiH[c][t] || !o->psiE[c][t]) return -1;
+            }
+    }
+    /* scene: boxes clear overrides inside them (materials.c:476-528) */
+    for (size_t q = 0; q < s->n_boxes; q++) {
+        const scn_box_t *b = &s->boxes[q];
+        int id = table_id(o, b->eps_r, b->sigma);
+        if (id < 0) return -1;
+        size_t i1 = b->i1, j1 = b->j1, k1 = b->k1;
+        if (periodic(o, 0) && i1 > o->n[0]) i1 = o->n[0];
+        if (periodic(o, 1) && j1 > o->n[1]) j1 = o->n[1];
+        if (periodic(o, 2) && k1 > o->n[2]) k1 = o->n[2];
+        for (size_t i = b->i0; i < i1; i++)
+            for (size_t j = b->j0; j < j1; j++)
+                for (size_t k = b->k0; k < k1; k++) {
+                    /* keys of the box use unwrapped coordinates */
+                    size_t raw = (i * (o->n[1] + 1) + j) * (o->n[2] + 1) + k;
+                    size_t w = at(o, i, j, k);
+                    o->id[w] = (uint8_t)id;
+                    for (int c = 0; c < 3; c++) o->has_ovr[c][raw] = 0;
+                    for (int c = 0; c < 2; c++) o->has_t[c][raw] = 0;
+                }
+    }
+    for (size_t q = 0; q < s->n_comps; q++) {
+        const scn_comp_t *c = &s->comps[q];
+        size_t w = at(o, c->i, c->j, c->k);
+        if (coeff(o, c->eps_r, c->sigma, &o->oca[c->comp][w], &o->ocb[c->comp][w]) != 0) return -1;
+        o->has_ovr[c->comp][w] = 1;
+    }
+    for (size_t q = 0; q < s->n_tensors; q++) {
+        const scn_tensor_t *t = &s->tensors[q];
+        size_t w = at(o, t->i, t->j, t->k);
+        o->has_t[t->comp][w] = 1;
+        o->tm11[t->comp][w] = t->m11;
+        o->tm12[t->comp][w] = t->m12;
+        o->tm22[t->comp][w] = t->m22;
+        o->tscale[t->comp][w] = o->dt / (O_EPS0 * o->dx);
+    }
+    return 0;
+}
+
+/* cpml.h:46-51 */
+static double stretch(double diff, double kinv, double b, double a, double dx, double *psi) {
+    *psi = b * (*psi) + a * diff;
+    return diff * kinv + dx * (*psi);
+}
+
+/* H update (cpml.c:176-219).  Component c: H_c -= cb (dA - dB) with
+ * A = d E_{c+2} / d x_{c+1} and B = d E_{c+1} / d x_{c+2} (forward). */
+static void update_h(orc_t *o) {
+    const double cb = o->dt / (O_MU0 * o->dx);
+    for (int c = 0; c < 3; c++) {
+        const int fa = (c + 2) % 3, axa = (c + 1) % 3;
+        const int fb = (c + 1) % 3, axb = (c + 2) % 3;
+        size_t lim[3] = {o->n[0], o->n[1], o->n[2]};
+        if (!periodic(o, c)) lim[c]++;
+        for (size_t i = 0; i < lim[0]; i++)
+            for (size_t j = 0; j < lim[1]; j++)
+                for (size_t k = 0; k < lim[2]; k++) {
+                    size_t p[3] = {i, j, k};
+                    size_t here = at(o, i, j, k);
+                    size_t qa[3] = {i, j, k}, qb[3] = {i, j, k};
+                    qa[axa]++;
+                    qb[axb]++;
+                    double dA = o->E[fa][at(o, qa[0], qa[1], qa[2])] - o->E[fa][here];
+                    double dB = o->E[fb][at(o, qb[0], qb[1], qb[2])] - o->E[fb][here];
+                    double tA = dA, tB = dB;
+                    if (o->cpml) {
+                        tA = stretch(dA, o->kh[axa][p[axa]], o->bh[axa][p[axa]], o->ah[axa][p[axa]], o->dx,
+                                     &o->psiH[c][0][here]);
+                        tB = stretch(dB, o->kh[axb][p[axb]], o->bh[axb][p[axb]], o->ah[axb][p[axb]], o->dx,
+                                     &o->psiH[c][1][here]);
+                    }
+                    o->H[c][here] -= cb * (tA - tB);
+                }
+    }
+}
+
+/* materials.c:836-845 */
+static double pair_w(double x11, double x12, double x22, double y11, double y12, double y22) {
+    double rx = (x12 / sqrt(x11)) / sqrt(x22);
+    double ry = (y12 / sqrt(y11)) / sqrt(y22);
+    double rho = 0.5 * rx + 0.5 * ry;
+    return (0.25 * rho * sqrt(x11)) * sqrt(y11);
+}
+
+/* materials.c:847-903 */
+static void tensor_edge(orc_t *o, int c, size_t i, size_t j, size_t k) {
+    size_t w = at(o, i, j, k);
+    const double m11 = o->tm11[c][w], m12 = o->tm12[c][w], m22 = o->tm22[c][w];
+    double *Hz = o->H[2];
+    double value;
+    if (c == 0) {
+        size_t ip = (i + 1 == o->n[0]) ? 0 : i + 1, jm = back(j, o->n[1]);
+        size_t ni[4] = {i, ip, i, ip}, nj[4] = {j, j, jm, jm};
+        value = m11 * (Hz[at(o, i, j, k)] - Hz[at(o, i, jm, k)]);
+        for (int q = 0; q < 4; q++) {
+            size_t ow = at(o, ni[q], nj[q], k);
+            if (!o->has_t[1][ow]) continue;
+            size_t um = back(ni[q], o->n[0]);
+            double curl = -(Hz[at(o, ni[q], nj[q], k)] - Hz[at(o, um, nj[q], k)]);
+            value += pair_w(m11, m12, m22, o->tm11[1][ow], o->tm12[1][ow], o->tm22[1][ow]) * curl;
+        }
+        o->E[0][w] += o->tscale[0][w] * value;
+    } else {
+        size_t im = back(i, o->n[0]), jp = (j + 1 == o->n[1]) ? 0 : j + 1;
+        size_t ni[4] = {i, im, i, im}, nj[4] = {j, j, jp, jp};
+        value = -m11 * (Hz[at(o, i, j, k)] - Hz[at(o, im, j, k)]);
+        for (int q = 0; q < 4; q++) {
+            size_t ow = at(o, ni[q], nj[q], k);
+            if (!o->has_t[0][ow]) continue;
+            size_t vm = back(nj[q], o->n[1]);
+            double curl = Hz[at(o, ni[q], nj[q], k)] - Hz[at(o, ni[q], vm, k)];
+            value += pair_w(o->tm11[0][ow], o->tm12[0][ow], o->tm22[0][ow], m11, m12, m22) * curl;
+        }
+        o->E[1][w] += o->tscale[1][w] * value;
+    }
+}
+
+/* E update (materials.c:911-1060).  Component c: E_c = Ca E_c + Cb (dA - dB)
+ * with A = d H_{c+2} / d x_{c+1}, B = d H_{c+1} / d x_{c+2} (backward);
+ * index 0 of an axis other than c is swept only when that axis is periodic. */
+static void update_e(orc_t *o) {
+    for (int c = 0; c < 3; c++) {
+        const int fa = (c + 2) % 3, axa = (c + 1) % 3;
+        const int fb = (c + 1) % 3, axb = (c + 2) % 3;
+        size_t lo[3];
+        for (int a = 0; a < 3; a++) lo[a] = (a == c || periodic(o, a)) ? 0 : 1;
+        for (size_t i = lo[0]; i < o->n[0]; i++)
+            for (size_t j = lo[1]; j < o->n[1]; j++)
+                for (size_t k = lo[2]; k < o->n[2]; k++) {
+                    size_t here = at(o, i, j, k);
+                    if (c < 2 && o->has_t[c][here]) {
+                        tensor_edge(o, c, i, j, k);
+                        continue;
+                    }
+                    size_t p[3] = {i, j, k};
+                    size_t qa[3] = {i, j, k}, qb[3] = {i, j, k};
+                    qa[axa] = back(qa[axa], o->n[axa]);
+                    qb[axb] = back(qb[axb], o->n[axb]);
+                    double ca, cb;
+                    if (o->has_ovr[c][here]) { ca = o->oca[c][here]; cb = o->ocb[c][here]; }
+                    else { ca = o->tca[o->id[here]]; cb = o->tcb[o->id[here]]; }
+                    double tA = o->H[fa][here] - o->H[fa][at(o, qa[0], qa[1], qa[2])];
+                    double tB = o->H[fb][here] - o->H[fb][at(o, qb[0], qb[1], qb[2])];
+                    if (o->cpml) {
+                        tA = stretch(tA, o->km[axa][p[axa]], o->bm[axa][p[axa]], o->am[axa][p[axa]], o->dx,
+                                     &o->psiE[c][0][here]);
+                        tB = stretch(tB, o->km[axb][p[axb]], o->bm[axb][p[axb]], o->am[axb][p[axb]], o->dx,
+                                     &o->psiE[c][1][here]);
+                    }
+                    o->E[c][here] = ca * o->E[c][here] + cb * (tA - tB);
+                }
+    }
+}
+
+/* source.c:8-26 */
+static double wave(const scn_source_t *s, double t) {
+    if (s->waveform == 0) {
+        double u = (t - s->p0) / s->p1;
+        return -2.0 * u * exp(-u * u);
+    }
+    if (s->waveform == 1) {
+        double a = O_PI * s->p0 * (t - s->p1);
+        double a2 = a * a;
+        return (1.0 - 2.0 * a2) * exp(-a2);
+    }
+    double u = (t - s->p1) / s->p2;
+    double env = exp(-u * u);
+    return env * sin(2.0 * O_PI * s->p0 * (t - s->p1));
+}
+
+static double *field(orc_t *o, int comp) { return comp < 3 ? o->E[comp] : o->H[comp - 3]; }
+
+static void step(orc_t *o, const scn_scene_t *s, size_t n) {
+    update_h(o);
+    double t = ((double)n + s->src_t_offset) * o->dt;
+    for (size_t q = 0; q < s->n_sources; q++) {
+        const scn_source_t *src = &s->sources[q];
+        if (src->i > o->n[0] || src->j > o->n[1] || src->k > o->n[2] || src->comp > 2) continue;
+        double v = src->amplitude * wave(src, t);
+        double *f = o->E[src->comp];
+        size_t w = at(o, src->i, src->j, src->k);
+        if (src->mode == 0) f[w] += v;
+        else f[w] = v;
+    }
+    update_e(o);
+}
+
+/* Runs the scene; probe_td n_probes*n_steps, dft_re/im n_probes*n_freqs. */
+int orc_run(const scn_scene_t *s, double *probe_td, double *dft_re, double *dft_im) {
+    orc_t o;
+    int rc = -1;
+    if (orc_init(&o, s) != 0) goto out;
+    if (dft_re && dft_im && s->n_freqs) {
+        memset(dft_re, 0, s->n_probes * s->n_freqs * 8);
+        memset(dft_im, 0, s->n_probes * s->n_freqs * 8);
+    }
+    for (size_t n = 0; n < s->n_steps; n++) {
+        step(&o, s, n);
+        double td = ((double)n + s->dft_t_offset) * o.dt;
+        for (size_t q = 0; q < s->n_probes; q++) {
+            const scn_probe_t *p = &s->probes[q];
+            double v = field(&o, p->comp)[at(&o, p->i, p->j, p->k)];
+            if (probe_td) probe_td[q * s->n_steps + n] = v;
+            if (dft_re && dft_im)
+                for (size_t f = 0; f < s->n_freqs; f++) {
+                    double w = 2.0 * O_PI * s->freqs[f];
+                    dft_re[q * s->n_freqs + f] += v * cos(w * td) * o.dt;
+                    dft_im[q * s->n_freqs + f] -= v * sin(w * td) * o.dt;
+                }
+        }
+    }
+    rc = 0;
+out:
+    orc_free(&o);
+    return rc;
+}
+
+int orc_run_fields(const scn_scene_t *s, const double *initial, double *fields_out) {
+    orc_t o;
+    int rc = -1;
+    if (orc_init(&o, s) != 0) goto out;
+    if (initial)
+        for (int c = 0; c < 6; c++) memcpy(field(&o, c), initial + c * o.total, o.total * 8);
+    for (size_t n = 0; n < s->n_steps; n++) {
+        update_h(&o);
+        update_e(&o);
+    }
+    for (int c = 0; c < 6; c++) memcpy(fields_out + c * o.total, field(&o, c), o.total * 8);
+    rc = 0;
+out:
+    orc_free(&o);
+    return rc;
+}
+
+/* dt of a scene (grid.c:27-28) */
+double orc_dt(double dx, double courant) { return courant * (dx / (O_C0 * sqrt(3.0))); }

@@ -1,0 +1,48 @@
+/*
+ * scene.h -- TEST INFRASTRUCTURE (oracle).  A flat, self-contained scene
+ * description shared by
+ *   - fdtd_oracle.c   : the CPU restatement of rfsyn's FDTD loop (FP64),
+ *   - scene_driver.c  : a driver that replays the scene through rfsyn's public
+ *                       C API, linked either against rfsyn itself (compiled
+ *                       from its sources into oracle/_ref) or against
+ *                       librfsyn_fdtd_b200.so (step-wise GPU path),
+ * so one case runs identically on every implementation.  Never linked into
+ * the product.
+ *
+ * Loop of one run (rfsyn engine/fdtd/simulate.c:48-54 generalised):
+ *   for n in 0..n_steps-1:
+ *     H update (CPML when npml > 0)
+ *     every source applied at t = (n + src_t_offset) dt
+ *     E update with materials (CPML when npml > 0)
+ *     probes record; DFT accumulates at t = (n + dft_t_offset) dt
+ */
+#ifndef RFSYN_ORACLE_SCENE_H
+#define RFSYN_ORACLE_SCENE_H
+
+#include <stddef.h>
+
+typedef struct { size_t i0, i1, j0, j1, k0, k1; double eps_r, sigma; } scn_box_t;
+typedef struct { int comp; size_t i, j, k; double eps_r, sigma; } scn_comp_t;
+typedef struct { int comp; size_t i, j, k; double m11, m12, m22; } scn_tensor_t;
+/* waveform: 0 Gaussian derivative (p0 t0, p1 tau), 1 Ricker (p0 f0, p1 t0),
+ *           2 modulated Gaussian (p0 f, p1 t0, p2 tau).  mode 0 soft, 1 hard. */
+typedef struct { size_t i, j, k; int comp, mode; double amplitude; int waveform; double p0, p1, p2; } scn_source_t;
+typedef struct { size_t i, j, k; int comp; } scn_probe_t;
+
+typedef struct {
+    size_t nx, ny, nz;
+    double dx, courant;
+    size_t n_steps;
+    unsigned periodic;
+    size_t npml;                        /* 0: no CPML */
+    double m, ma, kappa_max, alpha_max, r0;
+    size_t n_boxes;   const scn_box_t *boxes;       /* applied first, in order */
+    size_t n_comps;   const scn_comp_t *comps;      /* then scalar overrides */
+    size_t n_tensors; const scn_tensor_t *tensors;  /* then tensor edges */
+    size_t n_sources; const scn_source_t *sources;
+    size_t n_probes;  const scn_probe_t *probes;
+    size_t n_freqs;   const double *freqs;
+    double src_t_offset, dft_t_offset;
+} scn_scene_t;
+
+#endif

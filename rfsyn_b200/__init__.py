@@ -1,0 +1,270 @@
+"""Python host mirror of the rfsyn-b200 C ABI (ctypes).
+
+The product is the C-ABI library ``rfsyn_b200/lib/librfsyn_fdtd_b200.so``
+(reference-compatible entry points in ``include/rfsyn_fdtd.h``, extensions in
+``include/rfsyn_fdtd_b200.h``).  This module only binds it: every call goes
+to the CUDA engine behind the library; there is no Python or CPU compute path.
+Importing fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "librfsyn_fdtd_b200.so"
+
+FIELD_EX, FIELD_EY, FIELD_EZ, FIELD_HX, FIELD_HY, FIELD_HZ = range(6)
+SRC_SOFT, SRC_HARD = 0, 1
+FP64, FP32 = 0, 1
+SPLIT, FUSED = 0, 1
+WAVE_GAUSSIAN_DERIV, WAVE_RICKER, WAVE_MOD_GAUSSIAN, WAVE_SAMPLES = range(4)
+
+C0 = 299792458.0
+EPS0 = 8.8541878128e-12
+MU0 = 1.25663706212e-6
+
+
+class FdtdSimConfig(C.Structure):
+    """fdtd_sim_config_t (engine/fdtd/simulate.h:9-23)."""
+
+    _fields_ = [
+        ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
+        ("dx", C.c_double), ("courant_safety", C.c_double), ("n_steps", C.c_size_t),
+        ("npml", C.c_size_t),
+        ("src_i", C.c_size_t), ("src_j", C.c_size_t), ("src_k", C.c_size_t),
+        ("src_component", C.c_int), ("t0_over_dt", C.c_double), ("tau_over_dt", C.c_double),
+        ("probe_i", C.c_size_t), ("probe_j", C.c_size_t), ("probe_k", C.c_size_t),
+        ("probe_component", C.c_int),
+    ]
+
+
+class CpmlParams(C.Structure):
+    """cpml_params_t (engine/fdtd/cpml.h:29-36)."""
+
+    _fields_ = [("npml", C.c_size_t), ("m", C.c_double), ("ma", C.c_double),
+                ("kappa_max", C.c_double), ("alpha_max", C.c_double), ("r0", C.c_double)]
+
+
+class B200Source(C.Structure):
+    _fields_ = [("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t), ("component", C.c_int),
+                ("mode", C.c_int), ("amplitude", C.c_double), ("waveform", C.c_int),
+                ("p0", C.c_double), ("p1", C.c_double), ("p2", C.c_double),
+                ("samples", C.POINTER(C.c_double))]
+
+
+class B200Probe(C.Structure):
+    _fields_ = [("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t), ("component", C.c_int)]
+
+
+class B200Config(C.Structure):
+    _fields_ = [
+        ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
+        ("dx", C.c_double), ("courant_safety", C.c_double), ("n_steps", C.c_size_t),
+        ("periodic_axes", C.c_uint), ("cpml", CpmlParams), ("precision", C.c_int), ("schedule", C.c_int),
+        ("n_sources", C.c_size_t), ("sources", C.POINTER(B200Source)), ("source_time_offset_steps", C.c_double),
+        ("n_probes", C.c_size_t), ("probes", C.POINTER(B200Probe)),
+        ("n_freqs", C.c_size_t), ("freqs_hz", C.POINTER(C.c_double)), ("dft_time_offset_steps", C.c_double),
+    ]
+
+
+class B200Result(C.Structure):
+    _fields_ = [("probe_td", C.POINTER(C.c_double)), ("dft_re", C.POINTER(C.c_double)),
+                ("dft_im", C.POINTER(C.c_double)), ("sample_rate_hz", C.c_double), ("device_ms", C.c_double)]
+
+
+SETUP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the built library (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is not built; run `python -m rfsyn_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, D, S, I, V = C.c_void_p, C.c_double, C.c_size_t, C.c_int, None
+    sig = {
+        "fdtd_simulate_echo": (I, [C.POINTER(FdtdSimConfig), C.POINTER(D), C.POINTER(D)]),
+        "fdtd_simulate_echo_with_setup": (I, [C.POINTER(FdtdSimConfig), C.POINTER(D), C.POINTER(D), P, P]),
+        "fdtd_b200_run": (I, [C.POINTER(B200Config), P, P, C.POINTER(B200Result)]),
+        "fdtd_b200_sim_create": (P, [C.POINTER(B200Config), P, P, P]),
+        "fdtd_b200_sim_destroy": (V, [P]),
+        "fdtd_b200_sim_reset": (I, [P]),
+        "fdtd_b200_sim_advance": (I, [P, S]),
+        "fdtd_b200_sim_synchronize": (I, [P]),
+        "fdtd_b200_sim_steps_done": (S, [P]),
+        "fdtd_b200_sim_stream": (P, [P]),
+        "fdtd_b200_sim_read_probes": (I, [P, C.POINTER(D)]),
+        "fdtd_b200_sim_dft": (I, [P, C.POINTER(D), C.POINTER(D)]),
+        "fdtd_b200_sim_read_field": (I, [P, I, C.POINTER(D)]),
+        "fdtd_b200_sim_launches_per_step": (I, [P]),
+        "fdtd_b200_last_error": (C.c_char_p, []),
+        "fdtd_b200_launch_count": (C.c_ulonglong, []),
+        "fdtd_b200_set_default_precision": (I, [I]),
+        "fdtd_b200_set_default_schedule": (I, [I]),
+        "fdtd_b200_version": (C.c_char_p, []),
+        "cpml_default_params": (CpmlParams, [S]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().fdtd_b200_last_error().decode()
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def simulate_echo(cfg: FdtdSimConfig, setup=None, context=None) -> tuple[int, np.ndarray, float]:
+    """rfsyn's fdtd_simulate_echo[_with_setup] through the C ABI."""
+    lib = load()
+    out = np.zeros(max(cfg.n_steps, 1), dtype=np.float64)
+    fs = C.c_double(0.0)
+    if setup is None:
+        rc = lib.fdtd_simulate_echo(C.byref(cfg), _dptr(out), C.byref(fs))
+    else:
+        rc = lib.fdtd_simulate_echo_with_setup(C.byref(cfg), _dptr(out), C.byref(fs), setup, context)
+    return rc, out[: cfg.n_steps], fs.value
+
+
+class RunConfig:
+    """Builds an fdtd_b200_config_t and keeps the arrays it points to alive."""
+
+    def __init__(self, nx, ny, nz, dx, n_steps, npml, *, courant=0.99, periodic=0, precision=FP64,
+                 schedule=FUSED, cpml: CpmlParams | None = None, sources=(), probes=(), freqs=(),
+                 source_time_offset=0.0, dft_time_offset=1.0):
+        self.c = B200Config()
+        c = self.c
+        c.nx, c.ny, c.nz, c.dx, c.n_steps = nx, ny, nz, dx, n_steps
+        c.courant_safety = courant
+        c.periodic_axes = periodic
+        c.cpml = cpml if cpml is not None else load().cpml_default_params(npml)
+        if npml == 0:
+            c.cpml.npml = 0
+        c.precision, c.schedule = precision, schedule
+        self._src = (B200Source * max(len(sources), 1))()
+        self._samples = []
+        for q, s in enumerate(sources):
+            src = self._src[q]
+            src.i, src.j, src.k = s["i"], s["j"], s["k"]
+            src.component = s.get("component", FIELD_EZ)
+            src.mode = s.get("mode", SRC_SOFT)
+            src.amplitude = s.get("amplitude", 1.0)
+            src.waveform = s.get("waveform", WAVE_GAUSSIAN_DERIV)
+            src.p0, src.p1, src.p2 = s.get("p0", 0.0), s.get("p1", 1.0), s.get("p2", 1.0)
+            if "samples" in s:
+                arr = np.ascontiguousarray(s["samples"], dtype=np.float64)
+                self._samples.append(arr)
+                src.samples = _dptr(arr)
+        c.n_sources = len(sources)
+        c.sources = self._src
+        c.source_time_offset_steps = source_time_offset
+        self._probes = (B200Probe * max(len(probes), 1))()
+        for q, p in enumerate(probes):
+            self._probes[q].i, self._probes[q].j, self._probes[q].k = p["i"], p["j"], p["k"]
+            self._probes[q].component = p.get("component", FIELD_EZ)
+        c.n_probes = len(probes)
+        c.probes = self._probes
+        self._freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+        c.n_freqs = len(self._freqs)
+        c.freqs_hz = _dptr(self._freqs) if len(self._freqs) else None
+        c.dft_time_offset_steps = dft_time_offset
+
+
+def run(rc: RunConfig, setup=None, context=None) -> dict:
+    """fdtd_b200_run: one full run; returns probe series, DFT and GPU time."""
+    lib = load()
+    c = rc.c
+    td = np.zeros((max(c.n_probes, 1), c.n_steps))
+    re = np.zeros((max(c.n_probes, 1), max(c.n_freqs, 1)))
+    im = np.zeros_like(re)
+    res = B200Result()
+    res.probe_td = _dptr(td)
+    res.dft_re = _dptr(re)
+    res.dft_im = _dptr(im)
+    status = lib.fdtd_b200_run(C.byref(c), setup, context, C.byref(res))
+    if status != 0:
+        raise RuntimeError(f"fdtd_b200_run failed: {last_error()}")
+    return {"td": td[: c.n_probes], "dft": (re + 1j * im)[: c.n_probes, : c.n_freqs],
+            "fs": res.sample_rate_hz, "device_ms": res.device_ms}
+
+
+class Sim:
+    """A resident session (fdtd_b200_sim_*)."""
+
+    def __init__(self, rc: RunConfig, setup=None, context=None, stream: int | None = None):
+        self.lib = load()
+        self.rc = rc
+        self.h = self.lib.fdtd_b200_sim_create(C.byref(rc.c), setup, context, stream)
+        if not self.h:
+            raise RuntimeError(f"fdtd_b200_sim_create failed: {last_error()}")
+
+    def reset(self):
+        if self.lib.fdtd_b200_sim_reset(self.h) != 0:
+            raise RuntimeError(last_error())
+
+    def advance(self, n: int):
+        if self.lib.fdtd_b200_sim_advance(self.h, n) != 0:
+            raise RuntimeError(last_error())
+
+    def synchronize(self):
+        if self.lib.fdtd_b200_sim_synchronize(self.h) != 0:
+            raise RuntimeError(last_error())
+
+    @property
+    def stream(self) -> int:
+        return self.lib.fdtd_b200_sim_stream(self.h) or 0
+
+    @property
+    def launches_per_step(self) -> int:
+        return self.lib.fdtd_b200_sim_launches_per_step(self.h)
+
+    def probes(self) -> np.ndarray:
+        c = self.rc.c
+        out = np.zeros((max(c.n_probes, 1), c.n_steps))
+        if self.lib.fdtd_b200_sim_read_probes(self.h, _dptr(out)) != 0:
+            raise RuntimeError(last_error())
+        return out[: c.n_probes]
+
+    def dft(self) -> np.ndarray:
+        c = self.rc.c
+        re = np.zeros((max(c.n_probes, 1), max(c.n_freqs, 1)))
+        im = np.zeros_like(re)
+        if self.lib.fdtd_b200_sim_dft(self.h, _dptr(re), _dptr(im)) != 0:
+            raise RuntimeError(last_error())
+        return (re + 1j * im)[: c.n_probes, : c.n_freqs]
+
+    def field(self, component: int) -> np.ndarray:
+        c = self.rc.c
+        out = np.zeros((c.nx + 1, c.ny + 1, c.nz + 1))
+        if self.lib.fdtd_b200_sim_read_field(self.h, component, _dptr(out)) != 0:
+            raise RuntimeError(last_error())
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.fdtd_b200_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dt_of(dx: float, courant: float = 0.99) -> float:
+    return courant * (dx / (C0 * np.sqrt(3.0)))

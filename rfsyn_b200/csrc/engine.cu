@@ -1,0 +1,809 @@
+// engine.cu -- device memory, uploads, CUDA-graph time loop and the step-wise
+// update entry points behind rfsyn's fdtd_update_* functions.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <atomic>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.cuh"
+#include "fused.cuh"
+
+using namespace rfb;
+
+// ---------------------------------------------------------------------------
+// errors and launch accounting
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512];
+static std::atomic<unsigned long long> g_launches{0};
+
+extern "C" void rfb_set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+extern "C" const char *rfb_last_error(void) { return g_err; }
+extern "C" unsigned long long rfb_launch_count(void) { return g_launches.load(); }
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            rfb_set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            goto fail;                                                                  \
+        }                                                                               \
+    } while (0)
+
+#define MU0_ 1.25663706212e-6
+
+static long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+// Row pitch (elements) of the device layout: rows start on 128-byte lines.
+static long long pitch_for(int nz, size_t esz) { return round_up(nz + 1, (long long)(128 / esz)); }
+
+// ---------------------------------------------------------------------------
+// CPML on the device: profiles in the run precision, psi over slabs only.
+// ---------------------------------------------------------------------------
+struct SlabExt {
+    int lo, hi, ns;
+};
+
+// Leading / trailing non-identity runs of a profile (kappa_inv, b, a) =
+// (1, 1, 0) marks the unstretched interior (rfsyn cpml.c:50-52).
+static SlabExt slab_extent(const double *kinv, const double *b, const double *a, int len) {
+    auto ident = [&](int q) { return kinv[q] == 1.0 && b[q] == 1.0 && a[q] == 0.0; };
+    int lead = 0;
+    while (lead < len && !ident(lead)) lead++;
+    int trail = 0;
+    while (trail < len - lead && !ident(len - 1 - trail)) trail++;
+    bool interior_ok = true;
+    for (int q = lead; q < len - trail; q++)
+        if (!ident(q)) interior_ok = false;
+    SlabExt s;
+    if (!interior_ok) {
+        s.lo = len; s.hi = len;
+    } else {
+        s.lo = lead; s.hi = len - trail;
+    }
+    s.ns = s.lo + (len - s.hi);
+    return s;
+}
+
+struct DevCpml {
+    int on = 0;
+    int prec = RFB_FP64;
+    void *prof[3][6] = {};  // kinv_m b_m a_m kinv_h b_h a_h
+    SlabExt em[3], eh[3];
+    void *psi_e[6] = {};
+    void *psi_h[2][6] = {};
+    size_t psi_e_bytes[6] = {}, psi_h_bytes[6] = {};
+};
+
+static void *dev_upload_conv(const double *src, size_t n, int prec) {
+    void *d = nullptr;
+    size_t esz = prec == RFB_FP64 ? 8 : 4;
+    if (cudaMalloc(&d, n * esz) != cudaSuccess) return nullptr;
+    if (prec == RFB_FP64) {
+        if (cudaMemcpy(d, src, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    } else {
+        std::vector<float> tmp(n);
+        for (size_t q = 0; q < n; q++) tmp[q] = (float)src[q];
+        if (cudaMemcpy(d, tmp.data(), n * 4, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    }
+    return d;
+}
+
+static void devcpml_free(DevCpml &c) {
+    for (int a = 0; a < 3; a++)
+        for (int q = 0; q < 6; q++) cudaFree(c.prof[a][q]), c.prof[a][q] = nullptr;
+    for (int p = 0; p < 6; p++) {
+        cudaFree(c.psi_e[p]); c.psi_e[p] = nullptr;
+        cudaFree(c.psi_h[0][p]); c.psi_h[0][p] = nullptr;
+        cudaFree(c.psi_h[1][p]); c.psi_h[1][p] = nullptr;
+    }
+    c.on = 0;
+}
+
+// nbuf_h: 1 for in-place schedules, 2 for ping-pong H psi.
+static int devcpml_init(DevCpml &c, const rfb_geom_t *g, const rfb_cpml_desc_t *d, int prec, long long pitch,
+                        int nbuf_h) {
+    c.prec = prec;
+    c.on = 1;
+    const int n[3] = {g->nx, g->ny, g->nz};
+    const size_t esz = prec == RFB_FP64 ? 8 : 4;
+    for (int a = 0; a < 3; a++) {
+        const double *src[6] = {d->kinv_m[a], d->b_m[a], d->a_m[a], d->kinv_h[a], d->b_h[a], d->a_h[a]};
+        for (int q = 0; q < 6; q++) {
+            size_t len = q < 3 ? (size_t)n[a] + 1 : (size_t)n[a];
+            c.prof[a][q] = dev_upload_conv(src[q], len, prec);
+            if (!c.prof[a][q]) { rfb_set_error("cpml profile upload failed"); return -1; }
+        }
+        c.em[a] = slab_extent(d->kinv_m[a], d->b_m[a], d->a_m[a], n[a] + 1);
+        c.eh[a] = slab_extent(d->kinv_h[a], d->b_h[a], d->a_h[a], n[a]);
+    }
+    // extents of a psi array with slab axis ax and ns slab cells
+    auto bytes = [&](int ax, int ns) -> size_t {
+        size_t e;
+        if (ax == 0) e = (size_t)ns * (g->ny + 1) * pitch;
+        else if (ax == 1) e = (size_t)(g->nx + 1) * ns * pitch;
+        else e = (size_t)(g->nx + 1) * (g->ny + 1) * ns;
+        return e * esz;
+    };
+    for (int p = 0; p < 6; p++) {
+        int ax = psi_axis_e(p);
+        size_t be = bytes(ax, c.em[ax].ns);
+        c.psi_e_bytes[p] = be;
+        if (be) {
+            if (cudaMalloc(&c.psi_e[p], be) != cudaSuccess) { rfb_set_error("psi alloc failed"); return -1; }
+            cudaMemset(c.psi_e[p], 0, be);
+        }
+        int ah = psi_axis_h(p);
+        size_t bh = bytes(ah, c.eh[ah].ns);
+        c.psi_h_bytes[p] = bh;
+        if (bh) {
+            for (int b = 0; b < nbuf_h; b++) {
+                if (cudaMalloc(&c.psi_h[b][p], bh) != cudaSuccess) { rfb_set_error("psi alloc failed"); return -1; }
+                cudaMemset(c.psi_h[b][p], 0, bh);
+            }
+            if (nbuf_h == 1) c.psi_h[1][p] = nullptr;
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+static void fill_cpml_args(Args<T> &a, const DevCpml &c, int hin, int hout) {
+    a.cpml_on = c.on;
+    if (!c.on) return;
+    for (int ax = 0; ax < 3; ax++) {
+        a.kinv_m[ax] = (const T *)c.prof[ax][0];
+        a.b_m[ax] = (const T *)c.prof[ax][1];
+        a.a_m[ax] = (const T *)c.prof[ax][2];
+        a.kinv_h[ax] = (const T *)c.prof[ax][3];
+        a.b_h[ax] = (const T *)c.prof[ax][4];
+        a.a_h[ax] = (const T *)c.prof[ax][5];
+        a.lo_m[ax] = c.em[ax].lo; a.hi_m[ax] = c.em[ax].hi; a.ns_m[ax] = c.em[ax].ns;
+        a.lo_h[ax] = c.eh[ax].lo; a.hi_h[ax] = c.eh[ax].hi; a.ns_h[ax] = c.eh[ax].ns;
+    }
+    for (int p = 0; p < 6; p++) {
+        a.psi_e[p] = (T *)c.psi_e[p];
+        a.psi_hi[p] = (T *)c.psi_h[hin][p];
+        a.psi_ho[p] = (T *)(c.psi_h[hout][p] ? c.psi_h[hout][p] : c.psi_h[hin][p]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scene on the device: code volume, coefficient table, interface list.
+// ---------------------------------------------------------------------------
+struct DevScene {
+    int prec = RFB_FP64;
+    uint8_t *codes = nullptr;
+    void *tca = nullptr, *tcb = nullptr;
+    int n_cells = 0;
+    int *lc_ijk = nullptr;
+    uint8_t *l_kind = nullptr;
+    void *l_ca = nullptr, *l_cb = nullptr;
+    int *l_tix = nullptr, *l_src = nullptr;
+    void *t_m11 = nullptr, *t_scale = nullptr, *t_w = nullptr;
+    int *t_main = nullptr, *t_nq = nullptr, *t_uv = nullptr, *t_sign = nullptr;
+    int n_skip = 0;
+    long long skip[MAX_SKIP] = {};
+};
+
+static void devscene_free(DevScene &s) {
+    cudaFree(s.codes); cudaFree(s.tca); cudaFree(s.tcb);
+    cudaFree(s.lc_ijk); cudaFree(s.l_kind); cudaFree(s.l_ca); cudaFree(s.l_cb);
+    cudaFree(s.l_tix); cudaFree(s.l_src);
+    cudaFree(s.t_m11); cudaFree(s.t_scale); cudaFree(s.t_w);
+    cudaFree(s.t_main); cudaFree(s.t_nq); cudaFree(s.t_uv); cudaFree(s.t_sign);
+    s = DevScene();
+}
+
+template <typename X>
+static X *dev_copy(const X *src, size_t n) {
+    if (!n || !src) return nullptr;
+    X *d = nullptr;
+    if (cudaMalloc(&d, n * sizeof(X)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, src, n * sizeof(X), cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    return d;
+}
+
+static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image_t *img, int prec,
+                         long long pitch) {
+    s.prec = prec;
+    double tca[256], tcb[256];
+    for (int q = 0; q < 256; q++) { tca[q] = 1.0; tcb[q] = 0.0; }
+    int tc = img ? img->table_count : 0;
+    for (int q = 0; q < tc; q++) { tca[q] = img->table_ca[q]; tcb[q] = img->table_cb[q]; }
+    s.tca = dev_upload_conv(tca, 256, prec);
+    s.tcb = dev_upload_conv(tcb, 256, prec);
+    if (!s.tca || !s.tcb) { rfb_set_error("table upload failed"); return -1; }
+    const size_t plane_b = (size_t)(g->ny + 1) * pitch;
+    const size_t total_b = plane_b * (g->nx + 1);
+    s.n_cells = img ? (int)img->n_cells : 0;
+    if (img && img->codes) {
+        if (cudaMalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
+        if (cudaMemcpy2D(s.codes, pitch, img->codes, g->nz + 1, g->nz + 1, (size_t)(g->nx + 1) * (g->ny + 1),
+                         cudaMemcpyHostToDevice) != cudaSuccess) {
+            rfb_set_error("code volume upload failed");
+            return -1;
+        }
+    }
+    if (s.n_cells) {
+        const size_t ne = 3 * (size_t)s.n_cells;
+        s.lc_ijk = dev_copy(img->cell_ijk, 3 * (size_t)s.n_cells);
+        s.l_kind = dev_copy(img->kind, ne);
+        s.l_ca = dev_upload_conv(img->ca, ne, prec);
+        s.l_cb = dev_upload_conv(img->cb, ne, prec);
+        s.l_tix = dev_copy(img->tix, ne);
+        s.l_src = dev_copy(img->src, ne);
+        if (!s.lc_ijk || !s.l_kind || !s.l_ca || !s.l_cb || !s.l_tix || !s.l_src) {
+            rfb_set_error("interface list upload failed");
+            return -1;
+        }
+        if (img->n_tensors) {
+            size_t nt = img->n_tensors;
+            s.t_m11 = dev_upload_conv(img->t_m11, nt, prec);
+            s.t_scale = dev_upload_conv(img->t_scale, nt, prec);
+            s.t_w = dev_upload_conv(img->t_w, 4 * nt, prec);
+            s.t_main = dev_copy(img->t_main, 4 * nt);
+            s.t_nq = dev_copy(img->t_nq, nt);
+            s.t_uv = dev_copy(img->t_uv, 16 * nt);
+            s.t_sign = dev_copy(img->t_sign, nt);
+            if (!s.t_m11 || !s.t_scale || !s.t_w || !s.t_main || !s.t_nq || !s.t_uv || !s.t_sign) {
+                rfb_set_error("tensor list upload failed");
+                return -1;
+            }
+        }
+        if (!s.codes) {
+            if (s.n_cells <= MAX_SKIP) {
+                s.n_skip = s.n_cells;
+                for (int q = 0; q < s.n_cells; q++)
+                    s.skip[q] = ((long long)img->cell_ijk[3 * q] * (g->ny + 1) + img->cell_ijk[3 * q + 1]) * pitch +
+                                img->cell_ijk[3 * q + 2];
+            } else {
+                if (cudaMalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
+                cudaMemset(s.codes, 0, total_b);
+                k_mark_list<<<(s.n_cells + 255) / 256, 256>>>(s.codes, s.lc_ijk, s.n_cells, g->ny, pitch);
+                g_launches++;
+                if (cudaDeviceSynchronize() != cudaSuccess) { rfb_set_error("mark list failed"); return -1; }
+            }
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+static void fill_scene_args(Args<T> &a, const DevScene &s) {
+    a.codes = s.codes;
+    a.tca = (const T *)s.tca;
+    a.tcb = (const T *)s.tcb;
+    a.n_skip = s.n_skip;
+    for (int q = 0; q < MAX_SKIP; q++) a.skip[q] = s.skip[q];
+    a.n_cells = s.n_cells;
+    a.lc_ijk = s.lc_ijk;
+    a.l_kind = s.l_kind;
+    a.l_ca = (const T *)s.l_ca;
+    a.l_cb = (const T *)s.l_cb;
+    a.l_tix = s.l_tix;
+    a.l_src = s.l_src;
+    a.t_m11 = (const T *)s.t_m11;
+    a.t_scale = (const T *)s.t_scale;
+    a.t_w = (const T *)s.t_w;
+    a.t_main = s.t_main;
+    a.t_nq = s.t_nq;
+    a.t_uv = s.t_uv;
+    a.t_sign = s.t_sign;
+}
+
+template <typename T>
+static void fill_geom_args(Args<T> &a, const rfb_geom_t *g, long long pitch) {
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    a.per = g->periodic;
+    a.pitch = pitch;
+    a.plane = (long long)(g->ny + 1) * pitch;
+    a.cbh = (T)(g->dt / (MU0_ * g->dx));
+    a.dx = (T)g->dx;
+}
+
+// ---------------------------------------------------------------------------
+// Engine (device time loop)
+// ---------------------------------------------------------------------------
+struct rfb_engine {
+    rfb_geom_t g;
+    int prec, sched;
+    long long pitch;
+    size_t esz, total;
+    void *fld[2][6] = {};
+    int nbuf = 1;
+    DevCpml cpml;
+    DevScene scene;
+    int n_src = 0;
+    void *src_val = nullptr;
+    int *src_hard = nullptr;
+    int n_probes = 0;
+    long long *probe_cell = nullptr;
+    int *probe_comp = nullptr;
+    void *ts = nullptr;
+    int *d_step = nullptr;
+    size_t n_steps = 0, steps_done = 0;
+    double *d_omega = nullptr, *d_re = nullptr, *d_im = nullptr;
+    size_t dft_cap = 0;
+    cudaStream_t stream = nullptr;
+    int own_stream = 0;
+    int parity = 0;
+    static constexpr int CHUNK = 16;
+    cudaGraphExec_t g1[2] = {nullptr, nullptr}, gk[2] = {nullptr, nullptr};
+    int launches_per_step = 0;
+    FusedPlan plan;
+};
+
+template <typename T>
+static Args<T> engine_args(const rfb_engine *e, int par) {
+    Args<T> a;
+    memset(&a, 0, sizeof a);
+    fill_geom_args(a, &e->g, e->pitch);
+    const int in = e->nbuf == 2 ? par : 0, out = e->nbuf == 2 ? 1 - par : 0;
+    for (int c = 0; c < 3; c++) {
+        a.E[c] = (T *)e->fld[in][c];
+        a.H[c] = (T *)e->fld[in][3 + c];
+        a.Eo[c] = (T *)e->fld[out][c];
+        a.Ho[c] = (T *)e->fld[out][3 + c];
+    }
+    fill_cpml_args(a, e->cpml, in, e->cpml.psi_h[1][0] || e->nbuf == 2 ? out : in);
+    fill_scene_args(a, e->scene);
+    a.src_val = (const T *)e->src_val;
+    a.src_hard = e->src_hard;
+    a.n_steps = (long long)e->n_steps;
+    a.d_step = e->d_step;
+    return a;
+}
+
+template <typename T>
+static void enqueue_step(rfb_engine *e, int par) {
+    Args<T> a = engine_args<T>(e, par);
+    const rfb_geom_t &g = e->g;
+    if (e->sched == RFB_SCHED_FUSED) {
+        launch_fused<T>(a, e->plan, e->stream);
+    } else {
+        dim3 blk(32, 8);
+        dim3 grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
+        k_h_split<T><<<grd, blk, 0, e->stream>>>(a);
+        k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
+    }
+    if (a.n_cells) k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
+    ProbeArgs<T> p;
+    p.n = e->n_probes;
+    p.cell = e->probe_cell;
+    p.comp = e->probe_comp;
+    const int out = e->nbuf == 2 ? 1 - par : 0;
+    for (int c = 0; c < 6; c++) p.F[c] = (const T *)e->fld[out][c];
+    p.ts = (T *)e->ts;
+    p.n_steps = (long long)e->n_steps;
+    p.d_step = e->d_step;
+    k_probe_gather<T><<<1, 128, 0, e->stream>>>(p);
+}
+
+static int count_step_launches(const rfb_engine *e) {
+    int n = (e->sched == RFB_SCHED_FUSED) ? 1 : 2;
+    if (e->scene.n_cells) n++;
+    return n + 1;
+}
+
+static int build_graph(rfb_engine *e, int par, int steps, cudaGraphExec_t *out) {
+    cudaGraph_t graph = nullptr;
+    int p = par;
+    CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < steps; s++) {
+        if (e->prec == RFB_FP64) enqueue_step<double>(e, p);
+        else enqueue_step<float>(e, p);
+        if (e->nbuf == 2) p ^= 1;
+    }
+    CK(cudaStreamEndCapture(e->stream, &graph));
+    CK(cudaGraphInstantiate(out, graph, 0));
+    cudaGraphDestroy(graph);
+    return 0;
+fail:
+    if (graph) cudaGraphDestroy(graph);
+    return -1;
+}
+
+extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
+    if (!e) return;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (int q = 0; q < 2; q++) {
+        if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
+        if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
+    }
+    for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 6; c++) cudaFree(e->fld[b][c]);
+    devcpml_free(e->cpml);
+    devscene_free(e->scene);
+    cudaFree(e->src_val); cudaFree(e->src_hard);
+    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step);
+    cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision, int schedule,
+                                           const rfb_cpml_desc_t *cpml, const rfb_scene_image_t *scene,
+                                           size_t n_sources, const rfb_source_desc_t *sources, size_t n_probes,
+                                           const rfb_probe_desc_t *probes, size_t n_steps, void *stream) {
+    rfb_engine *e = new rfb_engine();
+    e->g = *geom;
+    e->prec = precision;
+    e->sched = schedule;
+    e->esz = precision == RFB_FP64 ? 8 : 4;
+    e->pitch = pitch_for(geom->nz, e->esz);
+    e->total = (size_t)(geom->nx + 1) * (geom->ny + 1) * e->pitch;
+    e->nbuf = schedule == RFB_SCHED_FUSED ? 2 : 1;
+    e->n_steps = n_steps;
+    if (schedule == RFB_SCHED_FUSED) {
+        int active = 0;
+        for (size_t s = 0; s < n_sources; s++) {
+            if ((sources[s].i == geom->nx && !(geom->periodic & 1u)) ||
+                (sources[s].j == geom->ny && !(geom->periodic & 2u)) ||
+                (sources[s].k == geom->nz && !(geom->periodic & 4u)))
+                active = 1;
+        }
+        if (fused_plan_default(&e->plan, geom, active) != 0) {
+            rfb_set_error("grid too large for the fused schedule");
+            delete e;
+            return nullptr;
+        }
+    }
+    if (stream) {
+        e->stream = (cudaStream_t)stream;
+    } else {
+        CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        e->own_stream = 1;
+    }
+    for (int b = 0; b < e->nbuf; b++)
+        for (int c = 0; c < 6; c++) {
+            CK(cudaMalloc(&e->fld[b][c], e->total * e->esz));
+            CK(cudaMemset(e->fld[b][c], 0, e->total * e->esz));
+        }
+    if (cpml && devcpml_init(e->cpml, geom, cpml, precision, e->pitch, e->nbuf) != 0) goto fail_noset;
+    if (devscene_init(e->scene, geom, scene, precision, e->pitch) != 0) goto fail_noset;
+    e->n_src = (int)n_sources;
+    if (n_sources) {
+        std::vector<double> vals(n_sources * n_steps);
+        std::vector<int> hard(n_sources);
+        for (size_t s = 0; s < n_sources; s++) {
+            memcpy(&vals[s * n_steps], sources[s].values, n_steps * sizeof(double));
+            hard[s] = sources[s].hard;
+        }
+        e->src_val = dev_upload_conv(vals.data(), vals.size(), precision);
+        e->src_hard = dev_copy(hard.data(), n_sources);
+        if (!e->src_val || !e->src_hard) { rfb_set_error("source upload failed"); goto fail_noset; }
+    }
+    e->n_probes = (int)n_probes;
+    if (n_probes) {
+        std::vector<long long> cell(n_probes);
+        std::vector<int> comp(n_probes);
+        for (size_t q = 0; q < n_probes; q++) {
+            cell[q] = ((long long)probes[q].i * (geom->ny + 1) + probes[q].j) * e->pitch + probes[q].k;
+            comp[q] = probes[q].component;
+        }
+        e->probe_cell = dev_copy(cell.data(), n_probes);
+        e->probe_comp = dev_copy(comp.data(), n_probes);
+        CK(cudaMalloc(&e->ts, n_probes * n_steps * e->esz));
+        CK(cudaMemset(e->ts, 0, n_probes * n_steps * e->esz));
+        if (!e->probe_cell || !e->probe_comp) { rfb_set_error("probe upload failed"); goto fail_noset; }
+    }
+    CK(cudaMalloc(&e->d_step, sizeof(int)));
+    CK(cudaMemset(e->d_step, 0, sizeof(int)));
+    CK(cudaDeviceSynchronize());
+    e->launches_per_step = count_step_launches(e);
+    return e;
+fail:
+fail_noset:
+    rfb_engine_destroy(e);
+    return nullptr;
+}
+
+extern "C" int rfb_engine_reset(rfb_engine_t *e) {
+    for (int b = 0; b < e->nbuf; b++)
+        for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(e->fld[b][c], 0, e->total * e->esz, e->stream));
+    for (int p = 0; p < 6; p++) {
+        if (e->cpml.psi_e[p]) CK(cudaMemsetAsync(e->cpml.psi_e[p], 0, e->cpml.psi_e_bytes[p], e->stream));
+        for (int b = 0; b < 2; b++)
+            if (e->cpml.psi_h[b][p]) CK(cudaMemsetAsync(e->cpml.psi_h[b][p], 0, e->cpml.psi_h_bytes[p], e->stream));
+    }
+    CK(cudaMemsetAsync(e->d_step, 0, sizeof(int), e->stream));
+    e->steps_done = 0;
+    e->parity = 0;
+    return 0;
+fail:
+    return -1;
+}
+
+extern "C" int rfb_engine_advance(rfb_engine_t *e, size_t n) {
+    if (e->steps_done + n > e->n_steps) {
+        rfb_set_error("advance past the configured step count (%zu + %zu > %zu)", e->steps_done, n, e->n_steps);
+        return -1;
+    }
+    const int per_parity = e->nbuf == 2 ? 2 : 1;
+    while (n > 0) {
+        const int par = per_parity == 2 ? e->parity : 0;
+        if (n >= (size_t)rfb_engine::CHUNK) {
+            if (!e->gk[par] && build_graph(e, par, rfb_engine::CHUNK, &e->gk[par]) != 0) return -1;
+            CK(cudaGraphLaunch(e->gk[par], e->stream));
+            g_launches += (unsigned long long)rfb_engine::CHUNK * e->launches_per_step;
+            n -= rfb_engine::CHUNK;
+            e->steps_done += rfb_engine::CHUNK;
+            // CHUNK is even: parity unchanged
+        } else {
+            if (!e->g1[par] && build_graph(e, par, 1, &e->g1[par]) != 0) return -1;
+            CK(cudaGraphLaunch(e->g1[par], e->stream));
+            g_launches += e->launches_per_step;
+            n -= 1;
+            e->steps_done += 1;
+            if (per_parity == 2) e->parity ^= 1;
+        }
+    }
+    return 0;
+fail:
+    return -1;
+}
+
+extern "C" int rfb_engine_advance_timed(rfb_engine_t *e, size_t n, double *ms) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    float t = 0.f;
+    int rc = -1;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, e->stream));
+    if (rfb_engine_advance(e, n) != 0) goto out;
+    CK(cudaEventRecord(b, e->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&t, a, b));
+    if (ms) *ms = t;
+    rc = 0;
+    goto out;
+fail:
+out:
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    return rc;
+}
+
+extern "C" int rfb_engine_sync(rfb_engine_t *e) {
+    CK(cudaStreamSynchronize(e->stream));
+    return 0;
+fail:
+    return -1;
+}
+
+extern "C" void *rfb_engine_stream(rfb_engine_t *e) { return (void *)e->stream; }
+extern "C" size_t rfb_engine_steps_done(rfb_engine_t *e) { return e->steps_done; }
+extern "C" int rfb_engine_launches_per_step(rfb_engine_t *e) { return e->launches_per_step; }
+
+extern "C" int rfb_engine_read_probes(rfb_engine_t *e, double *out) {
+    size_t n = (size_t)e->n_probes * e->n_steps;
+    if (!n) return 0;
+    CK(cudaStreamSynchronize(e->stream));
+    if (e->prec == RFB_FP64) {
+        CK(cudaMemcpy(out, e->ts, n * 8, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(n);
+        CK(cudaMemcpy(tmp.data(), e->ts, n * 4, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < n; q++) out[q] = tmp[q];
+    }
+    return 0;
+fail:
+    return -1;
+}
+
+extern "C" int rfb_engine_probe_dft(rfb_engine_t *e, size_t n_freqs, const double *freqs_hz, double t_offset_steps,
+                                    double *out_re, double *out_im) {
+    if (!e->n_probes || !n_freqs) return 0;
+    std::vector<double> om(n_freqs);
+    const size_t nout = (size_t)e->n_probes * n_freqs;
+    for (size_t f = 0; f < n_freqs; f++) om[f] = 2.0 * 3.14159265358979323846 * freqs_hz[f];
+    if (e->dft_cap < n_freqs || !e->d_re) {
+        cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
+        e->d_omega = e->d_re = e->d_im = nullptr;
+        CK(cudaMalloc(&e->d_omega, n_freqs * 8));
+        CK(cudaMalloc(&e->d_re, nout * 8));
+        CK(cudaMalloc(&e->d_im, nout * 8));
+        e->dft_cap = n_freqs;
+    }
+    CK(cudaMemcpyAsync(e->d_omega, om.data(), n_freqs * 8, cudaMemcpyHostToDevice, e->stream));
+    {
+        dim3 grd((unsigned)((n_freqs + 127) / 128), e->n_probes);
+        if (e->prec == RFB_FP64)
+            k_probe_dft<double><<<grd, 128, 0, e->stream>>>((const double *)e->ts, (long long)e->n_steps, e->n_probes,
+                                                            (int)e->steps_done, (int)n_freqs, e->d_omega, e->g.dt,
+                                                            t_offset_steps, e->d_re, e->d_im);
+        else
+            k_probe_dft<float><<<grd, 128, 0, e->stream>>>((const float *)e->ts, (long long)e->n_steps, e->n_probes,
+                                                           (int)e->steps_done, (int)n_freqs, e->d_omega, e->g.dt,
+                                                           t_offset_steps, e->d_re, e->d_im);
+        g_launches++;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out_re, e->d_re, nout * 8, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(out_im, e->d_im, nout * 8, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    return 0;
+fail:
+    return -1;
+}
+
+extern "C" int rfb_engine_read_field(rfb_engine_t *e, int component, double *host) {
+    const rfb_geom_t &g = e->g;
+    const int buf = e->nbuf == 2 ? e->parity : 0;
+    const size_t rows = (size_t)(g.nx + 1) * (g.ny + 1);
+    CK(cudaStreamSynchronize(e->stream));
+    if (e->prec == RFB_FP64) {
+        CK(cudaMemcpy2D(host, (g.nz + 1) * 8, e->fld[buf][component], e->pitch * 8, (g.nz + 1) * 8, rows,
+                        cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(rows * (g.nz + 1));
+        CK(cudaMemcpy2D(tmp.data(), (g.nz + 1) * 4, e->fld[buf][component], e->pitch * 4, (g.nz + 1) * 4, rows,
+                        cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < tmp.size(); q++) host[q] = tmp[q];
+    }
+    return 0;
+fail:
+    return -1;
+}
+
+// ---------------------------------------------------------------------------
+// Step-wise API: FP64 device mirror of a host grid.
+// ---------------------------------------------------------------------------
+struct rfb_fields {
+    rfb_geom_t g;
+    long long pitch;
+    size_t total;
+    double *f[6] = {};
+    cudaStream_t stream = nullptr;
+};
+struct rfb_cpml_dev {
+    DevCpml c;
+    int nx, ny, nz;
+};
+struct rfb_scene_dev {
+    DevScene s;
+};
+
+extern "C" rfb_fields_t *rfb_fields_create(const rfb_geom_t *geom) {
+    rfb_fields *f = new rfb_fields();
+    f->g = *geom;
+    f->pitch = pitch_for(geom->nz, 8);
+    f->total = (size_t)(geom->nx + 1) * (geom->ny + 1) * f->pitch;
+    CK(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+    for (int c = 0; c < 6; c++) CK(cudaMalloc(&f->f[c], f->total * 8));
+    return f;
+fail:
+    rfb_fields_destroy(f);
+    return nullptr;
+}
+
+extern "C" void rfb_fields_destroy(rfb_fields_t *f) {
+    if (!f) return;
+    for (int c = 0; c < 6; c++) cudaFree(f->f[c]);
+    if (f->stream) cudaStreamDestroy(f->stream);
+    delete f;
+}
+
+extern "C" rfb_cpml_dev_t *rfb_cpml_dev_create(const rfb_geom_t *geom, const rfb_cpml_desc_t *desc) {
+    rfb_cpml_dev *c = new rfb_cpml_dev();
+    c->nx = geom->nx; c->ny = geom->ny; c->nz = geom->nz;
+    if (devcpml_init(c->c, geom, desc, RFB_FP64, pitch_for(geom->nz, 8), 1) != 0) {
+        devcpml_free(c->c);
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+extern "C" void rfb_cpml_dev_destroy(rfb_cpml_dev_t *c) {
+    if (!c) return;
+    devcpml_free(c->c);
+    delete c;
+}
+extern "C" rfb_scene_dev_t *rfb_scene_dev_create(const rfb_geom_t *geom, const rfb_scene_image_t *img) {
+    rfb_scene_dev *s = new rfb_scene_dev();
+    if (devscene_init(s->s, geom, img, RFB_FP64, pitch_for(geom->nz, 8)) != 0) {
+        devscene_free(s->s);
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+extern "C" void rfb_scene_dev_destroy(rfb_scene_dev_t *s) {
+    if (!s) return;
+    devscene_free(s->s);
+    delete s;
+}
+
+static int fields_xfer(rfb_fields *f, double *const host[6], int first, int count, bool up) {
+    const rfb_geom_t &g = f->g;
+    const size_t rows = (size_t)(g.nx + 1) * (g.ny + 1);
+    for (int c = first; c < first + count; c++) {
+        if (up)
+            CK(cudaMemcpy2DAsync(f->f[c], f->pitch * 8, host[c], (g.nz + 1) * 8, (g.nz + 1) * 8, rows,
+                                 cudaMemcpyHostToDevice, f->stream));
+        else
+            CK(cudaMemcpy2DAsync(host[c], (g.nz + 1) * 8, f->f[c], f->pitch * 8, (g.nz + 1) * 8, rows,
+                                 cudaMemcpyDeviceToHost, f->stream));
+    }
+    return 0;
+fail:
+    return -1;
+}
+
+static Args<double> step_args(rfb_fields *f, const rfb_geom_t *geom) {
+    Args<double> a;
+    memset(&a, 0, sizeof a);
+    fill_geom_args(a, geom, f->pitch);
+    for (int c = 0; c < 3; c++) {
+        a.E[c] = a.Eo[c] = f->f[c];
+        a.H[c] = a.Ho[c] = f->f[3 + c];
+    }
+    return a;
+}
+
+extern "C" int rfb_step_update_h(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *cpml,
+                                 double *const host[6]) {
+    f->g = *geom;
+    Args<double> a = step_args(f, geom);
+    if (cpml) fill_cpml_args(a, cpml->c, 0, 0);
+    dim3 blk(32, 8), grd((geom->nz + 1 + 31) / 32, (geom->ny + 1 + 7) / 8, geom->nx + 1);
+    if (fields_xfer(f, host, 0, 6, true)) return -1;
+    k_h_split<double><<<grd, blk, 0, f->stream>>>(a);
+    g_launches++;
+    CK(cudaGetLastError());
+    if (fields_xfer(f, host, 3, 3, false)) return -1;
+    CK(cudaStreamSynchronize(f->stream));
+    return 0;
+fail:
+    return -1;
+}
+
+extern "C" int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *cpml,
+                                 rfb_scene_dev_t *scene, double vacuum_cb, double *const host[6]) {
+    f->g = *geom;
+    Args<double> a = step_args(f, geom);
+    if (cpml) fill_cpml_args(a, cpml->c, 0, 0);
+    DevScene vac;
+    double *vca = nullptr, *vcb = nullptr;
+    if (scene) {
+        fill_scene_args(a, scene->s);
+    } else {
+        // vacuum table: Ca = 1, Cb = dt/(eps0 dx) (grid.c:92-118)
+        double one = 1.0;
+        vca = dev_copy(&one, 1);
+        vcb = dev_copy(&vacuum_cb, 1);
+        if (!vca || !vcb) { rfb_set_error("vacuum table upload failed"); cudaFree(vca); cudaFree(vcb); return -1; }
+        a.tca = vca;
+        a.tcb = vcb;
+    }
+    dim3 blk(32, 8), grd((geom->nz + 1 + 31) / 32, (geom->ny + 1 + 7) / 8, geom->nx + 1);
+    int rc = -1;
+    if (fields_xfer(f, host, 0, 6, true)) goto out;
+    k_e_split<double><<<grd, blk, 0, f->stream>>>(a);
+    g_launches++;
+    if (a.n_cells) {
+        // the step-wise list carries no sources: d_step is unused
+        k_e_list<double><<<(3 * a.n_cells + 255) / 256, 256, 0, f->stream>>>(a);
+        g_launches++;
+    }
+    if (cudaGetLastError() != cudaSuccess) { rfb_set_error("E update launch failed"); goto out; }
+    if (fields_xfer(f, host, 0, 3, false)) goto out;
+    if (cudaStreamSynchronize(f->stream) != cudaSuccess) { rfb_set_error("E update failed"); goto out; }
+    rc = 0;
+out:
+    cudaStreamSynchronize(f->stream);
+    cudaFree(vca);
+    cudaFree(vcb);
+    (void)vac;
+    return rc;
+}

@@ -1,0 +1,173 @@
+/*
+ * engine.h -- internal C interface between the host library (C) and the
+ * CUDA engine (engine.cu).  Not part of the public ABI.
+ *
+ * Device layout shared by every kernel: a field component of a grid with
+ * sizes nx, ny, nz is one array of (nx+1)*(ny+1)*pitch elements, index
+ * (i*(ny+1) + j)*pitch + k, i.e. rfsyn's padded (i, j, k)-order with k
+ * fastest (engine/fdtd/grid.h:25-30) and the k row padded to `pitch`
+ * elements so every row starts on a 128-byte boundary.
+ */
+#ifndef RFSYN_B200_ENGINE_H
+#define RFSYN_B200_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { RFB_FP64 = 0, RFB_FP32 = 1 };
+
+/* Loop schedule of the device time loop. */
+enum {
+    RFB_SCHED_SPLIT = 0,  /* H kernel, then E kernel, in place              */
+    RFB_SCHED_FUSED = 1   /* one H+E march per step, ping-pong buffers      */
+};
+
+/* Host geometry of one grid. */
+typedef struct {
+    int nx, ny, nz;
+    unsigned periodic;      /* x=1, y=2, z=4 */
+    double dx, dt;
+} rfb_geom_t;
+
+/* CPML profiles on the host, rfsyn's per-axis arrays (engine/fdtd/cpml.c:21-89):
+ * index 0..2 = x, y, z; *_m have n+1 entries (integer positions), *_h have n
+ * (half-integer positions). */
+typedef struct {
+    const double *kinv_m[3], *b_m[3], *a_m[3];
+    const double *kinv_h[3], *b_h[3], *a_h[3];
+} rfb_cpml_desc_t;
+
+/* Per-(cell, component) entry kinds of the interface list. */
+enum {
+    RFB_LK_COPY   = 0,  /* component not updated (PEC or padded): keep value */
+    RFB_LK_SCALAR = 1,  /* E = Ca E + Cb (dA - dB) with CPML where present    */
+    RFB_LK_TENSOR = 2,  /* rfsyn 2x2 tensor edge (materials.c:847-903)        */
+    RFB_LK_ADE    = 3   /* dispersive (Debye / Lorentz) cell                  */
+};
+
+/* Scene image produced by the host materials description and consumed by the
+ * engine.  Everything is double on the host; the engine converts to the run
+ * precision on upload. */
+typedef struct {
+    /* Code volume, rfsyn's padded layout (pitch nz+1).  NULL means every cell
+     * uses table entry 0 and no cell is diverted to the list. */
+    const uint8_t *codes;
+    int table_count;
+    double table_ca[256], table_cb[256];
+
+    /* Interface list: n_entries = 3 * n_cells, entry e = 3*cell + component. */
+    size_t n_cells;
+    const int32_t *cell_ijk;    /* 3 per cell: i, j, k (canonical)            */
+    const uint8_t *kind;        /* per entry                                  */
+    const double *ca, *cb;      /* per entry (scalar kind)                    */
+    const int32_t *tix;         /* per entry: tensor record or -1             */
+    const int32_t *src;         /* per entry: source slot or -1               */
+    const int32_t *aix;         /* per entry: ADE record or -1                */
+
+    /* Tensor records (2x2 edges).  Each record: main coefficient (m11 for Ex,
+     * -m11 for Ey), the difference Hz(main0) - Hz(main1), scale and up to four
+     * couplings value += w * sign * (Hz(a) - Hz(b)). */
+    size_t n_tensors;
+    const double *t_m11, *t_scale;
+    const int32_t *t_main;      /* 4 per record: u0, v0, u1, v1               */
+    const int32_t *t_nq;        /* couplings used                              */
+    const double *t_w;          /* 4 per record                               */
+    const int32_t *t_uv;        /* 16 per record: ua, va, ub, vb per coupling  */
+    const int32_t *t_sign;      /* per record: +1 or -1 applied to couplings   */
+
+    /* ADE records (dispersive cells), see rfb_ade_desc in the engine. */
+    size_t n_ade;
+    const double *ade_c;        /* RFB_ADE_NC coefficients per record          */
+    int ade_npoles;             /* poles per record (all records share it)     */
+} rfb_scene_image_t;
+
+#define RFB_ADE_NC 16
+
+/* One point source: the per-step values s_n = amplitude * waveform(t_n) are
+ * evaluated on the host (rfsyn's source.c:40-57 semantics) and uploaded. */
+typedef struct {
+    int i, j, k, component;
+    int hard;               /* 0 = SOFT (add), 1 = HARD (assign) */
+    const double *values;   /* n_steps values */
+} rfb_source_desc_t;
+
+typedef struct {
+    int i, j, k, component; /* component 0..5 = Ex..Hz */
+} rfb_probe_desc_t;
+
+typedef struct rfb_engine rfb_engine_t;
+
+/* Creation of a device engine for one simulation.  `stream` may be NULL
+ * (the engine creates its own) or a cudaStream_t owned by the caller. */
+rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision, int schedule,
+                                const rfb_cpml_desc_t *cpml,      /* NULL: no CPML  */
+                                const rfb_scene_image_t *scene,   /* NULL: vacuum   */
+                                size_t n_sources, const rfb_source_desc_t *sources,
+                                size_t n_probes, const rfb_probe_desc_t *probes,
+                                size_t n_steps, void *stream);
+void rfb_engine_destroy(rfb_engine_t *e);
+
+/* Zero fields, psi and ADE state and rewind the step counter (async). */
+int rfb_engine_reset(rfb_engine_t *e);
+/* Enqueue n steps on the engine stream (CUDA graph replay). */
+int rfb_engine_advance(rfb_engine_t *e, size_t n);
+/* Blocking copy of the probe time series (n_probes * n_steps doubles, probe
+ * major).  Only the first `steps_done` samples of each probe are valid. */
+int rfb_engine_read_probes(rfb_engine_t *e, double *out);
+/* Running DFT of every probe series over bins freqs (Kahan-compensated FP32
+ * accumulation in FP32 runs, FP64 otherwise; FP64 phase recurrence); sample n
+ * is taken at t = (n + t_offset_steps) * dt and weighted by dt. */
+int rfb_engine_probe_dft(rfb_engine_t *e, size_t n_freqs, const double *freqs_hz,
+                         double t_offset_steps, double *out_re, double *out_im);
+int rfb_engine_sync(rfb_engine_t *e);
+/* advance + synchronise, returning the GPU time of the n steps (CUDA events
+ * recorded on the engine stream). */
+int rfb_engine_advance_timed(rfb_engine_t *e, size_t n, double *ms);
+void *rfb_engine_stream(rfb_engine_t *e);
+size_t rfb_engine_steps_done(rfb_engine_t *e);
+/* Kernel launches per time step (for launch accounting). */
+int rfb_engine_launches_per_step(rfb_engine_t *e);
+/* Download one field component (0..5) into a host array in rfsyn layout. */
+int rfb_engine_read_field(rfb_engine_t *e, int component, double *host);
+
+/* ---- step-wise API support (rfsyn's fdtd_update_* on host arrays) -------- */
+typedef struct rfb_fields rfb_fields_t;      /* FP64 device mirror of a grid  */
+typedef struct rfb_cpml_dev rfb_cpml_dev_t;  /* device profiles + slab psi    */
+typedef struct rfb_scene_dev rfb_scene_dev_t;/* device codes + list           */
+
+rfb_fields_t *rfb_fields_create(const rfb_geom_t *geom);
+void rfb_fields_destroy(rfb_fields_t *f);
+rfb_cpml_dev_t *rfb_cpml_dev_create(const rfb_geom_t *geom, const rfb_cpml_desc_t *desc);
+void rfb_cpml_dev_destroy(rfb_cpml_dev_t *c);
+rfb_scene_dev_t *rfb_scene_dev_create(const rfb_geom_t *geom, const rfb_scene_image_t *img);
+void rfb_scene_dev_destroy(rfb_scene_dev_t *s);
+
+/* host arrays: ex, ey, ez, hx, hy, hz in rfsyn layout (double). */
+int rfb_step_update_h(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *cpml,
+                      double *const host[6]);
+/* vacuum_cb: Cb of the vacuum table used when scene is NULL. */
+int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *cpml,
+                      rfb_scene_dev_t *scene, double vacuum_cb, double *const host[6]);
+
+/* FP64 energy audit on the device: returns sum over cells of
+ * 0.5*(eps E^2 + mu0 H^2) * dx^3 with eps recovered from Cb
+ * (validate_long_term_stability.c:166-209). */
+int rfb_step_energy(rfb_fields_t *f, const rfb_geom_t *geom, rfb_scene_dev_t *scene,
+                    double vacuum_cb, double *const host[6], double *out_energy);
+
+/* Last error message of the calling thread ("" if none). */
+const char *rfb_last_error(void);
+void rfb_set_error(const char *fmt, ...);
+
+/* Number of kernels this process has launched through the engine. */
+unsigned long long rfb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,671 @@
+/* materials.c -- host-side scene description (rfsyn materials API,
+ * engine/fdtd/materials.c:27-799 semantics) and its compilation into the
+ * device image: a per-cell code volume plus a compact interface list that
+ * carries every per-component override and tensor edge.
+ *
+ * Storage here is B200-first rather than rfsyn's: overrides live in
+ * open-addressing hash maps keyed by padded_index*3 + component (O(1) set /
+ * clear / lookup instead of sorted arrays with memmove), and are sorted only
+ * once, when the device image is built. */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "host.h"
+
+#define MATERIAL_LIMIT 256
+
+typedef struct {
+    double eps_r, sigma;
+    material_coeff_t coeff;
+} mat_entry_t;
+
+/* ---- open-addressing map: uint64 key -> fixed-size value ------------------ */
+typedef struct {
+    uint64_t *keys;    /* UINT64_MAX = empty */
+    double *vals;      /* vw doubles per slot */
+    size_t cap, count, vw;
+} omap_t;
+
+#define OMAP_EMPTY UINT64_MAX
+
+static uint64_t mix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+
+static int omap_init(omap_t *m, size_t vw) {
+    m->vw = vw;
+    m->cap = 0;
+    m->count = 0;
+    m->keys = NULL;
+    m->vals = NULL;
+    return 0;
+}
+
+static void omap_free(omap_t *m) {
+    free(m->keys);
+    free(m->vals);
+    m->keys = NULL;
+    m->vals = NULL;
+    m->cap = m->count = 0;
+}
+
+static long omap_find(const omap_t *m, uint64_t key) {
+    if (!m->cap) return -1;
+    size_t mask = m->cap - 1, h = mix64(key) & mask;
+    for (;;) {
+        if (m->keys[h] == OMAP_EMPTY) return -1;
+        if (m->keys[h] == key) return (long)h;
+        h = (h + 1) & mask;
+    }
+}
+
+static int omap_grow(omap_t *m, size_t want_cap) {
+    uint64_t *ok = m->keys;
+    double *ov = m->vals;
+    size_t ocap = m->cap;
+    uint64_t *nk = malloc(want_cap * sizeof(uint64_t));
+    double *nv = malloc(want_cap * m->vw * sizeof(double));
+    if (!nk || !nv) {
+        free(nk);
+        free(nv);
+        return -1;
+    }
+    for (size_t q = 0; q < want_cap; q++) nk[q] = OMAP_EMPTY;
+    size_t mask = want_cap - 1;
+    for (size_t q = 0; q < ocap; q++) {
+        if (ok[q] == OMAP_EMPTY) continue;
+        size_t h = mix64(ok[q]) & mask;
+        while (nk[h] != OMAP_EMPTY) h = (h + 1) & mask;
+        nk[h] = ok[q];
+        memcpy(nv + h * m->vw, ov + q * m->vw, m->vw * sizeof(double));
+    }
+    free(ok);
+    free(ov);
+    m->keys = nk;
+    m->vals = nv;
+    m->cap = want_cap;
+    return 0;
+}
+
+static int omap_put(omap_t *m, uint64_t key, const double *val) {
+    long at = omap_find(m, key);
+    if (at >= 0) {
+        memcpy(m->vals + (size_t)at * m->vw, val, m->vw * sizeof(double));
+        return 0;
+    }
+    if ((m->count + 1) * 2 > m->cap) {
+        if (omap_grow(m, m->cap ? m->cap * 2 : 64) != 0) return -1;
+    }
+    size_t mask = m->cap - 1, h = mix64(key) & mask;
+    while (m->keys[h] != OMAP_EMPTY) h = (h + 1) & mask;
+    m->keys[h] = key;
+    memcpy(m->vals + h * m->vw, val, m->vw * sizeof(double));
+    m->count++;
+    return 0;
+}
+
+/* Backward-shift deletion keeps probe chains intact without tombstones. */
+static void omap_del_slot(omap_t *m, size_t h) {
+    size_t mask = m->cap - 1;
+    size_t hole = h;
+    size_t q = (h + 1) & mask;
+    while (m->keys[q] != OMAP_EMPTY) {
+        size_t home = mix64(m->keys[q]) & mask;
+        /* can the entry at q move into the hole? (home not in (hole, q]) */
+        int movable = (q > hole) ? (home <= hole || home > q) : (home <= hole && home > q);
+        if (movable) {
+            m->keys[hole] = m->keys[q];
+            memcpy(m->vals + hole * m->vw, m->vals + q * m->vw, m->vw * sizeof(double));
+            hole = q;
+        }
+        q = (q + 1) & mask;
+    }
+    m->keys[hole] = OMAP_EMPTY;
+    m->count--;
+}
+
+static void omap_del(omap_t *m, uint64_t key) {
+    long at = omap_find(m, key);
+    if (at >= 0) omap_del_slot(m, (size_t)at);
+}
+
+/* ---- the description --------------------------------------------------------- */
+struct materials {
+    size_t nx, ny, nz, total;
+    double dx, dt;
+    uint8_t *ids;
+    mat_entry_t table[MATERIAL_LIMIT];
+    size_t table_count;
+    omap_t scalar;  /* key -> (Ca, Cb) */
+    omap_t tensor;  /* key -> (m11, m12, m22, scale) */
+    unsigned long version;
+    /* device copy for the step-wise API */
+    rfb_scene_dev_t *dev;
+    unsigned long dev_version;
+    unsigned dev_periodic;
+};
+
+int materials_matches(const materials_t *mat, const fdtd_grid_t *g) {
+    return mat && g && mat->nx == g->nx && mat->ny == g->ny && mat->nz == g->nz && mat->dx == g->dx &&
+           mat->dt == g->dt;
+}
+
+static int component_number(field_component_t c) {
+    switch (c) {
+    case FIELD_EX: return 0;
+    case FIELD_EY: return 1;
+    case FIELD_EZ: return 2;
+    default: return -1;
+    }
+}
+
+/* Valid padded coordinates of an E component; periodic axes omit the
+ * duplicate endpoint (materials.c:70-90). */
+static int component_valid(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k) {
+    if (!g || c < 0 || c > 2) return 0;
+    size_t ni = g->nx, nj = g->ny, nk = g->nz;
+    if (c != 0 && !(g->periodic_axes & 1u)) ni++;
+    if (c != 1 && !(g->periodic_axes & 2u)) nj++;
+    if (c != 2 && !(g->periodic_axes & 4u)) nk++;
+    return i < ni && j < nj && k < nk;
+}
+
+/* Lossy update coefficients (materials.c:92-125): loss = sigma dt / (2 eps),
+ * Ca = (1 - loss)/(1 + loss), Cb = dt/(eps dx)/(1 + loss). */
+static int make_coeff(const materials_t *mat, double eps_r, double sigma, material_coeff_t *out) {
+    if (!mat || !out || !isfinite(eps_r) || eps_r < 1.0 || !isfinite(sigma) || sigma < 0.0) return -1;
+    double eps = eps_r * EPS0;
+    double loss = (sigma * mat->dt) / (2.0 * eps);
+    double cb = mat->dt / (eps * mat->dx);
+    if (!isfinite(eps) || eps <= 0.0 || !isfinite(loss) || !isfinite(cb) || cb <= 0.0) return -1;
+    material_coeff_t coeff = {.Ca = (1.0 - loss) / (1.0 + loss), .Cb = cb / (1.0 + loss)};
+    if (!isfinite(coeff.Ca) || !isfinite(coeff.Cb) || coeff.Cb <= 0.0) return -1;
+    *out = coeff;
+    return 0;
+}
+
+materials_t *materials_create(const fdtd_grid_t *g) {
+    if (!g || g->nx == 0 || g->ny == 0 || g->nz == 0) return NULL;
+    if (!isfinite(g->dx) || g->dx <= 0.0 || !isfinite(g->dt) || g->dt <= 0.0) return NULL;
+    if (g->nx == SIZE_MAX || g->ny == SIZE_MAX || g->nz == SIZE_MAX) return NULL;
+    size_t nx1 = g->nx + 1, ny1 = g->ny + 1, nz1 = g->nz + 1;
+    if (nx1 > SIZE_MAX / ny1) return NULL;
+    size_t total = nx1 * ny1;
+    if (total > SIZE_MAX / nz1) return NULL;
+    total *= nz1;
+    if (total > SIZE_MAX / 3) return NULL;
+    materials_t *mat = calloc(1, sizeof(*mat));
+    if (!mat) return NULL;
+    mat->nx = g->nx;
+    mat->ny = g->ny;
+    mat->nz = g->nz;
+    mat->total = total;
+    mat->dx = g->dx;
+    mat->dt = g->dt;
+    omap_init(&mat->scalar, 2);
+    omap_init(&mat->tensor, 4);
+    mat->ids = calloc(total, 1);
+    if (!mat->ids) {
+        materials_destroy(mat);
+        return NULL;
+    }
+    material_id_t vacuum;
+    if (materials_register(mat, 1.0, 0.0, &vacuum) != 0) {
+        materials_destroy(mat);
+        return NULL;
+    }
+    return mat;
+}
+
+void materials_destroy(materials_t *mat) {
+    if (!mat) return;
+    free(mat->ids);
+    omap_free(&mat->scalar);
+    omap_free(&mat->tensor);
+    rfb_scene_dev_destroy(mat->dev);
+    free(mat);
+}
+
+int materials_register(materials_t *mat, double eps_r, double sigma, material_id_t *id_out) {
+    material_coeff_t coeff;
+    if (!mat || !id_out || make_coeff(mat, eps_r, sigma, &coeff) != 0) return -1;
+    for (size_t n = 0; n < mat->table_count; n++) {
+        if (mat->table[n].eps_r == eps_r && mat->table[n].sigma == sigma) {
+            *id_out = (material_id_t)n;
+            return 0;
+        }
+    }
+    if (mat->table_count >= MATERIAL_LIMIT) return -1;
+    size_t n = mat->table_count++;
+    mat->table[n].eps_r = eps_r;
+    mat->table[n].sigma = sigma;
+    mat->table[n].coeff = coeff;
+    mat->version++;
+    *id_out = (material_id_t)n;
+    return 0;
+}
+
+/* Padded ends accepted; periodic starts must be canonical (materials.c:425-454). */
+static int box_valid(const materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0, size_t j1,
+                     size_t k0, size_t k1) {
+    if (!materials_matches(mat, g)) return 0;
+    if (i0 >= i1 || j0 >= j1 || k0 >= k1) return 0;
+    if (i1 > g->nx + 1 || j1 > g->ny + 1 || k1 > g->nz + 1) return 0;
+    if ((g->periodic_axes & 1u) && i0 >= g->nx) return 0;
+    if ((g->periodic_axes & 2u) && j0 >= g->ny) return 0;
+    if ((g->periodic_axes & 4u) && k0 >= g->nz) return 0;
+    return 1;
+}
+
+static int key_in_box(const materials_t *mat, uint64_t key, size_t i0, size_t i1, size_t j0, size_t j1, size_t k0,
+                      size_t k1) {
+    size_t idx = (size_t)(key / 3);
+    size_t k = idx % (mat->nz + 1);
+    size_t row = idx / (mat->nz + 1);
+    size_t j = row % (mat->ny + 1);
+    size_t i = row / (mat->ny + 1);
+    return i >= i0 && i < i1 && j >= j0 && j < j1 && k >= k0 && k < k1;
+}
+
+static void clear_box_overrides(materials_t *mat, omap_t *m, size_t i0, size_t i1, size_t j0, size_t j1, size_t k0,
+                                size_t k1) {
+    if (!m->count) return;
+    /* collect then delete, so deletion shifts cannot skip entries */
+    uint64_t *victims = malloc(m->count * sizeof(uint64_t));
+    size_t nv = 0;
+    if (!victims) return;
+    for (size_t q = 0; q < m->cap; q++)
+        if (m->keys[q] != OMAP_EMPTY && key_in_box(mat, m->keys[q], i0, i1, j0, j1, k0, k1))
+            victims[nv++] = m->keys[q];
+    for (size_t q = 0; q < nv; q++) omap_del(m, victims[q]);
+    free(victims);
+}
+
+int materials_assign_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0, size_t j1,
+                         size_t k0, size_t k1, material_id_t id) {
+    if (!box_valid(mat, g, i0, i1, j0, j1, k0, k1) || (size_t)id >= mat->table_count) return -1;
+    if ((g->periodic_axes & 1u) && i1 > g->nx) i1 = g->nx;
+    if ((g->periodic_axes & 2u) && j1 > g->ny) j1 = g->ny;
+    if ((g->periodic_axes & 4u) && k1 > g->nz) k1 = g->nz;
+    for (size_t i = i0; i < i1; i++)
+        for (size_t j = j0; j < j1; j++) {
+            uint8_t *row = mat->ids + fdtd_index(g, i, j, 0);
+            if (!(g->periodic_axes & 4u)) {
+                memset(row + k0, id, k1 - k0);
+            } else {
+                for (size_t k = k0; k < k1; k++) mat->ids[fdtd_index(g, i, j, k)] = id;
+            }
+        }
+    clear_box_overrides(mat, &mat->scalar, i0, i1, j0, j1, k0, k1);
+    clear_box_overrides(mat, &mat->tensor, i0, i1, j0, j1, k0, k1);
+    mat->version++;
+    return 0;
+}
+
+int materials_set_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0, size_t j1, size_t k0,
+                      size_t k1, double eps_r, double sigma) {
+    if (!box_valid(mat, g, i0, i1, j0, j1, k0, k1)) return -1;
+    material_id_t id;
+    if (materials_register(mat, eps_r, sigma, &id) != 0) return -1;
+    return materials_assign_box(mat, g, i0, i1, j0, j1, k0, k1, id);
+}
+
+int materials_set_component(materials_t *mat, const fdtd_grid_t *g, field_component_t component, size_t i, size_t j,
+                            size_t k, double eps_r, double sigma) {
+    int c = component_number(component);
+    material_coeff_t coeff;
+    if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k) || make_coeff(mat, eps_r, sigma, &coeff) != 0)
+        return -1;
+    uint64_t key = (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c;
+    double v[2] = {coeff.Ca, coeff.Cb};
+    if (omap_put(&mat->scalar, key, v) != 0) return -1;
+    mat->version++;
+    return 0;
+}
+
+int materials_clear_component(materials_t *mat, const fdtd_grid_t *g, field_component_t component, size_t i, size_t j,
+                              size_t k) {
+    int c = component_number(component);
+    if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    omap_del(&mat->scalar, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
+    mat->version++;
+    return 0;
+}
+
+static material_coeff_t lookup(const materials_t *mat, size_t idx, int c) {
+    long at = omap_find(&mat->scalar, (uint64_t)idx * 3 + (uint64_t)c);
+    if (at >= 0) {
+        material_coeff_t r = {mat->scalar.vals[2 * at], mat->scalar.vals[2 * at + 1]};
+        return r;
+    }
+    return mat->table[mat->ids[idx]].coeff;
+}
+
+int materials_get_coefficients(const materials_t *mat, const fdtd_grid_t *g, field_component_t component, size_t i,
+                               size_t j, size_t k, material_coeff_t *out) {
+    int c = component_number(component);
+    if (!out || !materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    *out = lookup(mat, fdtd_index(g, i, j, k), c);
+    return 0;
+}
+
+/* x/y interior margins for the 4-neighbour tensor stencil (materials.c:273-294). */
+static int tensor_margin_ok(const fdtd_grid_t *g, size_t i, size_t j) {
+    if (!(g->periodic_axes & 1u) && (g->nx < 3 || i == 0 || i >= g->nx - 1)) return 0;
+    if (!(g->periodic_axes & 2u) && (g->ny < 3 || j == 0 || j >= g->ny - 1)) return 0;
+    return 1;
+}
+
+/* Positive definiteness of [[a b][b c]] without forming ac - b^2
+ * (materials.c:296-308). */
+static int tensor_spd(double a, double b, double c) {
+    if (!isfinite(a) || !isfinite(b) || !isfinite(c) || a <= 0.0 || c <= 0.0) return 0;
+    return fabs(b) / sqrt(a) < sqrt(c);
+}
+
+int materials_set_component_tensor(materials_t *mat, const fdtd_grid_t *g, field_component_t component, size_t i,
+                                   size_t j, size_t k, double m11, double m12, double m22) {
+    int c = component_number(component);
+    if (c != 0 && c != 1) return -1;
+    if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k) || !tensor_margin_ok(g, i, j) ||
+        !tensor_spd(m11, m12, m22))
+        return -1;
+    double scale = mat->dt / (EPS0 * mat->dx);
+    if (!isfinite(scale) || scale <= 0.0) return -1;
+    double v[4] = {m11, m12, m22, scale};
+    if (omap_put(&mat->tensor, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, v) != 0) return -1;
+    mat->version++;
+    return 0;
+}
+
+int materials_clear_component_tensor(materials_t *mat, const fdtd_grid_t *g, field_component_t component, size_t i,
+                                     size_t j, size_t k) {
+    int c = component_number(component);
+    if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    omap_del(&mat->tensor, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
+    mat->version++;
+    return 0;
+}
+
+static const double *tensor_at(const materials_t *mat, size_t idx, int c) {
+    long at = omap_find(&mat->tensor, (uint64_t)idx * 3 + (uint64_t)c);
+    return at >= 0 ? mat->tensor.vals + 4 * (size_t)at : NULL;
+}
+
+int materials_get_tensor(const materials_t *mat, const fdtd_grid_t *g, field_component_t component, size_t i, size_t j,
+                         size_t k, material_tensor_t *out) {
+    int c = component_number(component);
+    if (!out || !materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    const double *t = tensor_at(mat, fdtd_index(g, i, j, k), c);
+    if (!t) return 1;
+    out->m11 = t[0];
+    out->m12 = t[1];
+    out->m22 = t[2];
+    out->scale = t[3];
+    return 0;
+}
+
+/* Symmetric Ex/Ey coupling weight of two tensor edges (materials.c:836-845):
+ * 0.25 * rho * sqrt(m11_x) * sqrt(m11_y) with rho the mean normalised
+ * off-diagonal correlation; evaluated in the same order for bit parity. */
+static double pair_weight(const double *ex, const double *ey) {
+    double rx = (ex[1] / sqrt(ex[0])) / sqrt(ex[2]);
+    double ry = (ey[1] / sqrt(ey[0])) / sqrt(ey[2]);
+    double rho = 0.5 * rx + 0.5 * ry;
+    return (0.25 * rho * sqrt(ex[0])) * sqrt(ey[0]);
+}
+
+static size_t prev_q(size_t q, size_t n) { return q == 0 ? n - 1 : q - 1; }
+static size_t next_q(size_t q, size_t n) { return q + 1 == n ? 0 : q + 1; }
+
+/* Component c of canonical cell (i,j,k) is swept by rfsyn's E loops
+ * (materials.c:915-1059). */
+static int e_swept(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k) {
+    size_t i0 = (g->periodic_axes & 1u) ? 0 : 1, j0 = (g->periodic_axes & 2u) ? 0 : 1,
+           k0 = (g->periodic_axes & 4u) ? 0 : 1;
+    if (i >= g->nx || j >= g->ny || k >= g->nz) return 0;
+    if (c != 0 && i < i0) return 0;
+    if (c != 1 && j < j0) return 0;
+    if (c != 2 && k < k0) return 0;
+    return 1;
+}
+
+static int cmp_u64(const void *a, const void *b) {
+    uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+void rfb_scene_build_free(rfb_scene_build_t *b) {
+    if (!b) return;
+    free(b->codes); free(b->cell_ijk); free(b->kind); free(b->ca); free(b->cb);
+    free(b->tix); free(b->src); free(b->aix);
+    free(b->t_m11); free(b->t_scale); free(b->t_w); free(b->t_main); free(b->t_nq); free(b->t_uv); free(b->t_sign);
+    memset(b, 0, sizeof(*b));
+}
+
+int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n_extra, const rfb_extra_cell_t *extra,
+                          rfb_scene_build_t *out) {
+    memset(out, 0, sizeof(*out));
+    if (!materials_matches(mat, g)) {
+        rfb_set_error("materials do not match the grid");
+        return -1;
+    }
+    const size_t nz1 = g->nz + 1;
+    /* 1. cells on the interface list (padded linear index) */
+    size_t cap = mat->scalar.count + mat->tensor.count + n_extra;
+    int id255 = 0;
+    if (mat->table_count == MATERIAL_LIMIT) {
+        /* code 255 marks list cells: cells of material 255 go to the list too */
+        for (size_t q = 0; q < mat->total; q++)
+            if (mat->ids[q] == 255) { id255 = 1; cap++; }
+    }
+    uint64_t *cells = malloc((cap ? cap : 1) * sizeof(uint64_t));
+    if (!cells) goto oom;
+    size_t nc = 0;
+    for (size_t q = 0; q < mat->scalar.cap; q++)
+        if (mat->scalar.keys[q] != OMAP_EMPTY) cells[nc++] = mat->scalar.keys[q] / 3;
+    for (size_t q = 0; q < mat->tensor.cap; q++)
+        if (mat->tensor.keys[q] != OMAP_EMPTY) cells[nc++] = mat->tensor.keys[q] / 3;
+    for (size_t q = 0; q < n_extra; q++)
+        cells[nc++] = ((uint64_t)extra[q].i * (g->ny + 1) + (uint64_t)extra[q].j) * nz1 + (uint64_t)extra[q].k;
+    if (id255)
+        for (size_t q = 0; q < mat->total; q++)
+            if (mat->ids[q] == 255) cells[nc++] = q;
+    qsort(cells, nc, sizeof(uint64_t), cmp_u64);
+    size_t nu = 0;
+    for (size_t q = 0; q < nc; q++)
+        if (nu == 0 || cells[nu - 1] != cells[q]) cells[nu++] = cells[q];
+    nc = nu;
+
+    /* 2. code volume: needed when any cell uses a non-vacuum material or the
+     *    list is long; otherwise the engine works code-less */
+    int uniform = 1;
+    for (size_t q = 0; q < mat->total && uniform; q++)
+        if (mat->ids[q] != 0) uniform = 0;
+    if (!uniform) {
+        out->codes = malloc(mat->total);
+        if (!out->codes) goto oom;
+        memcpy(out->codes, mat->ids, mat->total);
+        for (size_t q = 0; q < nc; q++) out->codes[cells[q]] = 255;
+    }
+    rfb_scene_image_t *img = &out->img;
+    img->codes = out->codes;
+    img->table_count = (int)mat->table_count;
+    for (size_t q = 0; q < mat->table_count; q++) {
+        img->table_ca[q] = mat->table[q].coeff.Ca;
+        img->table_cb[q] = mat->table[q].coeff.Cb;
+    }
+    /* 3. list entries */
+    const size_t ne = 3 * nc;
+    out->cell_ijk = malloc((3 * nc + 1) * sizeof(int32_t));
+    out->kind = malloc(ne + 1);
+    out->ca = malloc((ne + 1) * sizeof(double));
+    out->cb = malloc((ne + 1) * sizeof(double));
+    out->tix = malloc((ne + 1) * sizeof(int32_t));
+    out->src = malloc((ne + 1) * sizeof(int32_t));
+    out->aix = malloc((ne + 1) * sizeof(int32_t));
+    size_t tcap = mat->tensor.count + 1;
+    out->t_m11 = malloc(tcap * sizeof(double));
+    out->t_scale = malloc(tcap * sizeof(double));
+    out->t_w = calloc(4 * tcap, sizeof(double));
+    out->t_main = calloc(4 * tcap, sizeof(int32_t));
+    out->t_nq = calloc(tcap, sizeof(int32_t));
+    out->t_uv = calloc(16 * tcap, sizeof(int32_t));
+    out->t_sign = calloc(tcap, sizeof(int32_t));
+    if (!out->cell_ijk || !out->kind || !out->ca || !out->cb || !out->tix || !out->src || !out->aix || !out->t_m11 ||
+        !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign)
+        goto oom;
+    size_t nt = 0;
+    for (size_t q = 0; q < nc; q++) {
+        size_t idx = (size_t)cells[q];
+        size_t k = idx % nz1, row = idx / nz1, j = row % (g->ny + 1), i = row / (g->ny + 1);
+        out->cell_ijk[3 * q] = (int32_t)i;
+        out->cell_ijk[3 * q + 1] = (int32_t)j;
+        out->cell_ijk[3 * q + 2] = (int32_t)k;
+        for (int c = 0; c < 3; c++) {
+            size_t e = 3 * q + (size_t)c;
+            out->tix[e] = -1;
+            out->src[e] = -1;
+            out->aix[e] = -1;
+            material_coeff_t co = lookup(mat, idx, c);
+            out->ca[e] = co.Ca;
+            out->cb[e] = co.Cb;
+            if (!e_swept(g, c, i, j, k)) {
+                out->kind[e] = RFB_LK_COPY;
+                continue;
+            }
+            const double *t = (c < 2) ? tensor_at(mat, idx, c) : NULL;
+            if (!t) {
+                out->kind[e] = RFB_LK_SCALAR;
+                continue;
+            }
+            /* tensor edge record (materials.c:847-903) */
+            out->kind[e] = RFB_LK_TENSOR;
+            out->tix[e] = (int32_t)nt;
+            out->t_scale[nt] = t[3];
+            int32_t *mn = out->t_main + 4 * nt;
+            int nq = 0;
+            if (c == 0) {
+                size_t ip = next_q(i, g->nx), jm = prev_q(j, g->ny);
+                out->t_m11[nt] = t[0];
+                mn[0] = (int32_t)i; mn[1] = (int32_t)j; mn[2] = (int32_t)i; mn[3] = (int32_t)jm;
+                size_t ni[4] = {i, ip, i, ip}, nj[4] = {j, j, jm, jm};
+                out->t_sign[nt] = -1;
+                for (int s = 0; s < 4; s++) {
+                    const double *o = tensor_at(mat, fdtd_index(g, ni[s], nj[s], k), 1);
+                    if (!o) continue;
+                    size_t um = prev_q(ni[s], g->nx);
+                    out->t_w[4 * nt + nq] = pair_weight(t, o);
+                    int32_t *uv = out->t_uv + 16 * nt + 4 * nq;
+                    uv[0] = (int32_t)ni[s]; uv[1] = (int32_t)nj[s]; uv[2] = (int32_t)um; uv[3] = (int32_t)nj[s];
+                    nq++;
+                }
+            } else {
+                size_t im = prev_q(i, g->nx), jp = next_q(j, g->ny);
+                out->t_m11[nt] = -t[0];
+                mn[0] = (int32_t)i; mn[1] = (int32_t)j; mn[2] = (int32_t)im; mn[3] = (int32_t)j;
+                size_t ni[4] = {i, im, i, im}, nj[4] = {j, j, jp, jp};
+                out->t_sign[nt] = 1;
+                for (int s = 0; s < 4; s++) {
+                    const double *o = tensor_at(mat, fdtd_index(g, ni[s], nj[s], k), 0);
+                    if (!o) continue;
+                    size_t vm = prev_q(nj[s], g->ny);
+                    out->t_w[4 * nt + nq] = pair_weight(o, t);
+                    int32_t *uv = out->t_uv + 16 * nt + 4 * nq;
+                    uv[0] = (int32_t)ni[s]; uv[1] = (int32_t)nj[s]; uv[2] = (int32_t)ni[s]; uv[3] = (int32_t)vm;
+                    nq++;
+                }
+            }
+            out->t_nq[nt] = nq;
+            nt++;
+        }
+    }
+    /* sources attached to extra cells */
+    for (size_t q = 0; q < n_extra; q++) {
+        if (extra[q].component < 0 || extra[q].slot < 0) continue;
+        uint64_t key = ((uint64_t)extra[q].i * (g->ny + 1) + (uint64_t)extra[q].j) * nz1 + (uint64_t)extra[q].k;
+        uint64_t *hit = bsearch(&key, cells, nc, sizeof(uint64_t), cmp_u64);
+        if (!hit) continue;
+        size_t e = 3 * (size_t)(hit - cells) + (size_t)extra[q].component;
+        if (out->src[e] >= 0) {
+            rfb_set_error("two sources on the same field sample");
+            free(cells);
+            rfb_scene_build_free(out);
+            return -1;
+        }
+        out->src[e] = extra[q].slot;
+    }
+    free(cells);
+    img->n_cells = nc;
+    img->cell_ijk = out->cell_ijk;
+    img->kind = out->kind;
+    img->ca = out->ca;
+    img->cb = out->cb;
+    img->tix = out->tix;
+    img->src = out->src;
+    img->aix = out->aix;
+    img->n_tensors = nt;
+    img->t_m11 = out->t_m11;
+    img->t_scale = out->t_scale;
+    img->t_main = out->t_main;
+    img->t_nq = out->t_nq;
+    img->t_w = out->t_w;
+    img->t_uv = out->t_uv;
+    img->t_sign = out->t_sign;
+    return 0;
+oom:
+    free(cells);
+    rfb_scene_build_free(out);
+    rfb_set_error("out of host memory building the scene image");
+    return -1;
+}
+
+rfb_scene_dev_t *materials_device(const materials_t *cmat, const fdtd_grid_t *g) {
+    materials_t *mat = (materials_t *)cmat;
+    if (mat->dev && mat->dev_version == mat->version && mat->dev_periodic == g->periodic_axes) return mat->dev;
+    rfb_scene_dev_destroy(mat->dev);
+    mat->dev = NULL;
+    rfb_scene_build_t b;
+    if (materials_build_image(mat, g, 0, NULL, &b) != 0) return NULL;
+    rfb_geom_t geom;
+    rfb_geom_from_grid(g, &geom);
+    mat->dev = rfb_scene_dev_create(&geom, &b.img);
+    rfb_scene_build_free(&b);
+    mat->dev_version = mat->version;
+    mat->dev_periodic = g->periodic_axes;
+    return mat->dev;
+}
+
+rfb_fields_t *rfb_grid_device(fdtd_grid_t *g, rfb_geom_t *geom, double *h[6]);
+rfb_cpml_dev_t *rfb_cpml_device(cpml_t *p, const fdtd_grid_t *g);
+
+void fdtd_update_e_materials(fdtd_grid_t *g, const materials_t *mat) {
+    if (!materials_matches(mat, g)) return;
+    rfb_scene_dev_t *s = materials_device(mat, g);
+    if (!s) return;
+    rfb_geom_t geom;
+    double *h[6];
+    rfb_fields_t *f = rfb_grid_device(g, &geom, h);
+    if (!f) return;
+    rfb_step_update_e(f, &geom, NULL, s, g->dt / (EPS0 * g->dx), h);
+}
+
+void fdtd_update_e_cpml_materials(fdtd_grid_t *g, cpml_t *pml, const materials_t *mat) {
+    if (!materials_matches(mat, g) || !pml || pml->dx != g->dx) return;
+    rfb_cpml_dev_t *c = rfb_cpml_device(pml, g);
+    if (!c) return;
+    rfb_scene_dev_t *s = materials_device(mat, g);
+    if (!s) return;
+    rfb_geom_t geom;
+    double *h[6];
+    rfb_fields_t *f = rfb_grid_device(g, &geom, h);
+    if (!f) return;
+    rfb_step_update_e(f, &geom, c, s, g->dt / (EPS0 * g->dx), h);
+}

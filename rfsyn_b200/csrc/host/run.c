@@ -1,0 +1,394 @@
+/* run.c -- the device time loop behind rfsyn's fdtd_simulate_echo*,
+ * fdtd_stage_create and the extension API (fdtd_b200_*).
+ *
+ * rfsyn's loop (engine/fdtd/simulate.c:48-54) is, per step n:
+ *   H update with CPML; source at t = n dt; E update with CPML + materials;
+ *   probe record.
+ * Here the whole loop runs on the GPU: the engine replays a CUDA graph of
+ * the step kernels, sources are injected by the interface-list kernel and
+ * probes are gathered on the device; only the time series comes back. */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "host.h"
+
+static int g_prec = -1, g_sched = -1;
+
+int rfb_default_precision(void) {
+    if (g_prec < 0) {
+        const char *v = getenv("RFSYN_FDTD_PRECISION");
+        g_prec = (v && (!strcmp(v, "fp32") || !strcmp(v, "FP32"))) ? RFB_FP32 : RFB_FP64;
+    }
+    return g_prec;
+}
+
+int rfb_default_schedule(void) {
+    if (g_sched < 0) {
+        const char *v = getenv("RFSYN_FDTD_SCHEDULE");
+        g_sched = (v && !strcmp(v, "split")) ? RFB_SCHED_SPLIT : RFB_SCHED_FUSED;
+    }
+    return g_sched;
+}
+
+int fdtd_b200_set_default_precision(int precision) {
+    if (precision != FDTD_B200_FP64 && precision != FDTD_B200_FP32) return -1;
+    g_prec = precision;
+    return 0;
+}
+
+int fdtd_b200_set_default_schedule(int schedule) {
+    if (schedule != FDTD_B200_SCHED_SPLIT && schedule != FDTD_B200_SCHED_FUSED) return -1;
+    g_sched = schedule;
+    return 0;
+}
+
+const char *fdtd_b200_last_error(void) { return rfb_last_error(); }
+unsigned long long fdtd_b200_launch_count(void) { return rfb_launch_count(); }
+const char *fdtd_b200_version(void) { return "rfsyn-b200 0.1 (sm_100a)"; }
+
+void fdtd_b200_config_init(fdtd_b200_config_t *cfg, size_t nx, size_t ny, size_t nz, double dx, size_t n_steps,
+                           size_t npml) {
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->nx = nx;
+    cfg->ny = ny;
+    cfg->nz = nz;
+    cfg->dx = dx;
+    cfg->courant_safety = 0.99;
+    cfg->n_steps = n_steps;
+    cfg->cpml = cpml_default_params(npml);
+    cfg->precision = FDTD_B200_FP64;
+    cfg->schedule = FDTD_B200_SCHED_FUSED;
+    cfg->source_time_offset_steps = 0.0;
+    cfg->dft_time_offset_steps = 1.0;
+}
+
+struct fdtd_b200_sim {
+    rfb_engine_t *eng;
+    size_t n_steps, n_probes, n_freqs;
+    double dt;
+    double *freqs;
+    double dft_offset;
+    size_t nx, ny, nz;
+};
+
+static double wave_value(const fdtd_b200_source_t *s, double t, size_t n) {
+    switch (s->waveform) {
+    case FDTD_B200_WAVE_GAUSSIAN_DERIV: {
+        source_gaussian_deriv_params_t p = {s->p0, s->p1};
+        return s->amplitude * source_waveform_gaussian_derivative(t, &p);
+    }
+    case FDTD_B200_WAVE_RICKER: {
+        source_ricker_params_t p = {s->p0, s->p1};
+        return s->amplitude * source_waveform_ricker(t, &p);
+    }
+    case FDTD_B200_WAVE_MOD_GAUSSIAN: {
+        source_modulated_gaussian_params_t p = {s->p0, s->p1, s->p2};
+        return s->amplitude * source_waveform_modulated_gaussian(t, &p);
+    }
+    default:
+        return s->samples[n];
+    }
+}
+
+static size_t canon(size_t q, size_t n, int periodic) { return periodic ? q % n : q; }
+
+fdtd_b200_sim_t *fdtd_b200_sim_create(const fdtd_b200_config_t *cfg, fdtd_material_setup_fn setup, void *context,
+                                      void *cuda_stream) {
+    fdtd_grid_t g;
+    cpml_t *pml = NULL;
+    materials_t *mat = NULL;
+    rfb_scene_build_t scene;
+    int have_scene = 0;
+    double *vals = NULL;
+    rfb_source_desc_t *sd = NULL;
+    rfb_extra_cell_t *extra = NULL;
+    rfb_probe_desc_t *pd = NULL;
+    fdtd_b200_sim_t *sim = NULL;
+
+    if (!cfg) { rfb_set_error("NULL config"); return NULL; }
+    if (cfg->n_steps == 0) { rfb_set_error("n_steps must be positive"); return NULL; }
+    if (cfg->precision != FDTD_B200_FP64 && cfg->precision != FDTD_B200_FP32) {
+        rfb_set_error("unknown precision %d", cfg->precision);
+        return NULL;
+    }
+    if (rfb_grid_geometry(&g, cfg->nx, cfg->ny, cfg->nz, cfg->dx, cfg->courant_safety) != 0) {
+        rfb_set_error("invalid grid geometry");
+        return NULL;
+    }
+    if (cfg->nx > 60000 || cfg->ny > 60000 || cfg->nz > 60000) {
+        rfb_set_error("grid axis longer than 60000 cells");
+        return NULL;
+    }
+    if (fdtd_grid_set_periodic(&g, cfg->periodic_axes) != 0) {
+        rfb_set_error("invalid periodic axes");
+        return NULL;
+    }
+    const int px = g.periodic_axes & 1u, py = g.periodic_axes & 2u, pz = g.periodic_axes & 4u;
+    if (cfg->cpml.npml > 0) {
+        pml = cpml_create(&g, cfg->cpml);
+        if (!pml) { rfb_set_error("invalid CPML parameters for this grid"); return NULL; }
+    }
+    mat = materials_create(&g);
+    if (!mat) { rfb_set_error("materials_create failed"); goto fail; }
+    if (setup && setup(&g, mat, context) != 0) { rfb_set_error("scene setup callback failed"); goto fail; }
+
+    const size_t ns = cfg->n_sources, np = cfg->n_probes, nt = cfg->n_steps;
+    if (ns) {
+        vals = malloc(ns * nt * sizeof(double));
+        sd = calloc(ns, sizeof(*sd));
+        extra = calloc(ns, sizeof(*extra));
+        if (!vals || !sd || !extra) { rfb_set_error("out of host memory"); goto fail; }
+    }
+    for (size_t s = 0; s < ns; s++) {
+        const fdtd_b200_source_t *src = &cfg->sources[s];
+        if (src->i > g.nx || src->j > g.ny || src->k > g.nz) { rfb_set_error("source %zu outside the grid", s); goto fail; }
+        if (src->component > FIELD_EZ) { rfb_set_error("source %zu drives a non-E component", s); goto fail; }
+        if (src->waveform == FDTD_B200_WAVE_SAMPLES && !src->samples) { rfb_set_error("source %zu has no samples", s); goto fail; }
+        if (src->waveform < 0 || src->waveform > FDTD_B200_WAVE_SAMPLES) { rfb_set_error("source %zu: unknown waveform", s); goto fail; }
+        for (size_t n = 0; n < nt; n++) {
+            double t = ((double)n + cfg->source_time_offset_steps) * g.dt;
+            vals[s * nt + n] = wave_value(src, t, n);
+        }
+        sd[s].i = (int)canon(src->i, g.nx, px);
+        sd[s].j = (int)canon(src->j, g.ny, py);
+        sd[s].k = (int)canon(src->k, g.nz, pz);
+        sd[s].component = (int)src->component;
+        sd[s].hard = src->mode == SRC_HARD;
+        sd[s].values = vals + s * nt;
+        extra[s].i = sd[s].i;
+        extra[s].j = sd[s].j;
+        extra[s].k = sd[s].k;
+        extra[s].component = sd[s].component;
+        extra[s].slot = (int)s;
+    }
+    if (np) {
+        pd = calloc(np, sizeof(*pd));
+        if (!pd) { rfb_set_error("out of host memory"); goto fail; }
+    }
+    for (size_t q = 0; q < np; q++) {
+        const fdtd_b200_probe_t *p = &cfg->probes[q];
+        if (p->i > g.nx || p->j > g.ny || p->k > g.nz) { rfb_set_error("probe %zu outside the grid", q); goto fail; }
+        if (p->component > FIELD_HZ) { rfb_set_error("probe %zu: unknown component", q); goto fail; }
+        pd[q].i = (int)canon(p->i, g.nx, px);
+        pd[q].j = (int)canon(p->j, g.ny, py);
+        pd[q].k = (int)canon(p->k, g.nz, pz);
+        pd[q].component = (int)p->component;
+    }
+    if (materials_build_image(mat, &g, ns, extra, &scene) != 0) goto fail;
+    have_scene = 1;
+
+    sim = calloc(1, sizeof(*sim));
+    if (!sim) { rfb_set_error("out of host memory"); goto fail; }
+    sim->n_steps = nt;
+    sim->n_probes = np;
+    sim->dt = g.dt;
+    sim->nx = g.nx; sim->ny = g.ny; sim->nz = g.nz;
+    sim->dft_offset = cfg->dft_time_offset_steps;
+    sim->n_freqs = cfg->n_freqs;
+    if (cfg->n_freqs) {
+        if (!cfg->freqs_hz) { rfb_set_error("n_freqs without freqs_hz"); goto fail; }
+        sim->freqs = malloc(cfg->n_freqs * sizeof(double));
+        if (!sim->freqs) { rfb_set_error("out of host memory"); goto fail; }
+        memcpy(sim->freqs, cfg->freqs_hz, cfg->n_freqs * sizeof(double));
+    }
+    rfb_geom_t geom;
+    rfb_geom_from_grid(&g, &geom);
+    rfb_cpml_desc_t cd;
+    if (pml) rfb_cpml_desc_from(pml, &cd);
+    sim->eng = rfb_engine_create(&geom, cfg->precision, cfg->schedule, pml ? &cd : NULL, &scene.img, ns, sd, np, pd, nt,
+                                 cuda_stream);
+    if (!sim->eng) goto fail;
+    rfb_scene_build_free(&scene);
+    free(vals); free(sd); free(extra); free(pd);
+    materials_destroy(mat);
+    cpml_destroy(pml);
+    return sim;
+fail:
+    if (sim) {
+        free(sim->freqs);
+        free(sim);
+    }
+    if (have_scene) rfb_scene_build_free(&scene);
+    free(vals); free(sd); free(extra); free(pd);
+    materials_destroy(mat);
+    cpml_destroy(pml);
+    return NULL;
+}
+
+void fdtd_b200_sim_destroy(fdtd_b200_sim_t *sim) {
+    if (!sim) return;
+    rfb_engine_destroy(sim->eng);
+    free(sim->freqs);
+    free(sim);
+}
+
+int fdtd_b200_sim_reset(fdtd_b200_sim_t *sim) { return sim ? rfb_engine_reset(sim->eng) : -1; }
+int fdtd_b200_sim_advance(fdtd_b200_sim_t *sim, size_t n) { return sim ? rfb_engine_advance(sim->eng, n) : -1; }
+int fdtd_b200_sim_synchronize(fdtd_b200_sim_t *sim) { return sim ? rfb_engine_sync(sim->eng) : -1; }
+size_t fdtd_b200_sim_steps_done(const fdtd_b200_sim_t *sim) { return sim ? rfb_engine_steps_done(sim->eng) : 0; }
+void *fdtd_b200_sim_stream(const fdtd_b200_sim_t *sim) { return sim ? rfb_engine_stream(sim->eng) : NULL; }
+int fdtd_b200_sim_launches_per_step(const fdtd_b200_sim_t *sim) {
+    return sim ? rfb_engine_launches_per_step(sim->eng) : 0;
+}
+
+int fdtd_b200_sim_read_probes(fdtd_b200_sim_t *sim, double *probe_td) {
+    if (!sim || !probe_td) return -1;
+    return rfb_engine_read_probes(sim->eng, probe_td);
+}
+
+int fdtd_b200_sim_dft(fdtd_b200_sim_t *sim, double *re, double *im) {
+    if (!sim || !re || !im) return -1;
+    return rfb_engine_probe_dft(sim->eng, sim->n_freqs, sim->freqs, sim->dft_offset, re, im);
+}
+
+int fdtd_b200_sim_read_field(fdtd_b200_sim_t *sim, field_component_t c, double *host) {
+    if (!sim || !host || c > FIELD_HZ) return -1;
+    return rfb_engine_read_field(sim->eng, (int)c, host);
+}
+
+int fdtd_b200_run(const fdtd_b200_config_t *cfg, fdtd_material_setup_fn setup, void *context,
+                  fdtd_b200_result_t *result) {
+    if (!result) { rfb_set_error("NULL result"); return -1; }
+    fdtd_b200_sim_t *sim = fdtd_b200_sim_create(cfg, setup, context, NULL);
+    if (!sim) return -1;
+    int rc = -1;
+    double ms = 0.0;
+    if (rfb_engine_advance_timed(sim->eng, cfg->n_steps, &ms) != 0) goto out;
+    if (result->probe_td && rfb_engine_read_probes(sim->eng, result->probe_td) != 0) goto out;
+    if (result->dft_re && result->dft_im && sim->n_freqs &&
+        rfb_engine_probe_dft(sim->eng, sim->n_freqs, sim->freqs, sim->dft_offset, result->dft_re, result->dft_im) != 0)
+        goto out;
+    result->sample_rate_hz = 1.0 / sim->dt;
+    result->device_ms = ms;
+    rc = 0;
+out:
+    fdtd_b200_sim_destroy(sim);
+    return rc;
+}
+
+/* ---- rfsyn's entry points --------------------------------------------------- */
+
+int fdtd_simulate_echo_with_setup(const fdtd_sim_config_t *cfg, double *out_td, double *sample_rate_out,
+                                  fdtd_material_setup_fn setup, void *context) {
+    if (!cfg || !out_td) return -1;
+    if (cfg->n_steps == 0) return -1;
+    fdtd_grid_t g;
+    if (rfb_grid_geometry(&g, cfg->nx, cfg->ny, cfg->nz, cfg->dx, cfg->courant_safety) != 0) return -1;
+    if (cfg->src_i > g.nx || cfg->src_j > g.ny || cfg->src_k > g.nz || cfg->probe_i > g.nx ||
+        cfg->probe_j > g.ny || cfg->probe_k > g.nz)
+        return -1;
+    fdtd_b200_config_t b;
+    fdtd_b200_config_init(&b, cfg->nx, cfg->ny, cfg->nz, cfg->dx, cfg->n_steps, cfg->npml);
+    b.courant_safety = cfg->courant_safety;
+    b.cpml = cpml_default_params(cfg->npml);
+    b.precision = rfb_default_precision();
+    b.schedule = rfb_default_schedule();
+    /* simulate.c:37-38: soft Gaussian-derivative source, amplitude 1, t = n dt;
+     * a non-E source component is ignored, as rfsyn's source_apply does */
+    fdtd_b200_source_t src;
+    memset(&src, 0, sizeof src);
+    src.i = cfg->src_i; src.j = cfg->src_j; src.k = cfg->src_k;
+    src.component = cfg->src_component;
+    src.mode = SRC_SOFT;
+    src.amplitude = 1.0;
+    src.waveform = FDTD_B200_WAVE_GAUSSIAN_DERIV;
+    src.p0 = cfg->t0_over_dt * g.dt;
+    src.p1 = cfg->tau_over_dt * g.dt;
+    b.n_sources = (cfg->src_component <= FIELD_EZ) ? 1 : 0;
+    b.sources = &src;
+    b.source_time_offset_steps = 0.0;
+    fdtd_b200_probe_t probe = {cfg->probe_i, cfg->probe_j, cfg->probe_k, cfg->probe_component};
+    int valid_probe = cfg->probe_component <= FIELD_HZ;
+    b.n_probes = valid_probe ? 1 : 0;
+    b.probes = &probe;
+    fdtd_b200_result_t r;
+    memset(&r, 0, sizeof r);
+    r.probe_td = valid_probe ? out_td : NULL;
+    if (!valid_probe) memset(out_td, 0, cfg->n_steps * sizeof(double));
+    if (fdtd_b200_run(&b, setup, context, &r) != 0) return -1;
+    if (sample_rate_out) *sample_rate_out = 1.0 / g.dt;
+    return 0;
+}
+
+int fdtd_simulate_echo(const fdtd_sim_config_t *cfg, double *out_td, double *sample_rate_out) {
+    return fdtd_simulate_echo_with_setup(cfg, out_td, sample_rate_out, NULL, NULL);
+}
+
+/* ---- the stage (cli/fdtd_stage.c:10-41) and its signal type ------------------ */
+
+typedef struct {
+    fdtd_sim_config_t cfg;
+} stage_ctx_t;
+
+static int stage_apply(void *ctx_v, signal_t *sig) {
+    stage_ctx_t *ctx = (stage_ctx_t *)ctx_v;
+    if (!ctx || !sig) return -1;
+    if (signal_resize(sig, ctx->cfg.n_steps) != 0) return -1;
+    double *buf = malloc(ctx->cfg.n_steps * sizeof(double));
+    if (!buf) return -1;
+    double fs = 0.0;
+    if (fdtd_simulate_echo(&ctx->cfg, buf, &fs) != 0) {
+        free(buf);
+        return -1;
+    }
+    for (size_t n = 0; n < sig->n_samples; n++) sig->samples[n] = (float)buf[n];
+    free(buf);
+    sig->sample_rate_hz = fs;
+    return 0;
+}
+
+static void stage_destroy(void *ctx) { free(ctx); }
+
+transform_t fdtd_stage_create(const fdtd_sim_config_t *cfg) {
+    transform_t none = {NULL, NULL, NULL};
+    if (!cfg) return none;
+    stage_ctx_t *ctx = malloc(sizeof(*ctx));
+    if (!ctx) return none;
+    ctx->cfg = *cfg;
+    transform_t t = {stage_apply, stage_destroy, ctx};
+    return t;
+}
+
+signal_t *signal_create(size_t n_samples, double sample_rate_hz, double center_freq_hz) {
+    if (n_samples > SIZE_MAX / sizeof(rfsyn_float_complex)) return NULL;
+    signal_t *sig = calloc(1, sizeof(*sig));
+    if (!sig) return NULL;
+    sig->samples = calloc(n_samples, sizeof(rfsyn_float_complex));
+    if (!sig->samples && n_samples > 0) {
+        free(sig);
+        return NULL;
+    }
+    sig->n_samples = n_samples;
+    sig->sample_rate_hz = sample_rate_hz;
+    sig->center_freq_hz = center_freq_hz;
+    return sig;
+}
+
+void signal_destroy(signal_t *sig) {
+    if (!sig) return;
+    free(sig->samples);
+    if (sig->metadata && sig->meta_free) sig->meta_free(sig->metadata);
+    free(sig);
+}
+
+int signal_resize(signal_t *sig, size_t n) {
+    if (!sig) return -1;
+    if (n > SIZE_MAX / sizeof(rfsyn_float_complex)) return -1;
+    rfsyn_float_complex *grown = realloc(sig->samples, n * sizeof(rfsyn_float_complex));
+    if (!grown && n > 0) return -1;
+    if (n > sig->n_samples) memset(grown + sig->n_samples, 0, (n - sig->n_samples) * sizeof(rfsyn_float_complex));
+    sig->samples = grown;
+    sig->n_samples = n;
+    return 0;
+}
+
+signal_t *signal_copy(const signal_t *sig) {
+    if (!sig) return NULL;
+    signal_t *c = signal_create(sig->n_samples, sig->sample_rate_hz, sig->center_freq_hz);
+    if (!c) return NULL;
+    memcpy(c->samples, sig->samples, sig->n_samples * sizeof(rfsyn_float_complex));
+    c->metadata = sig->metadata;
+    return c;
+}

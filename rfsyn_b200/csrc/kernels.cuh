@@ -1,0 +1,337 @@
+// kernels.cuh -- sm_100a kernels of the FDTD time loop.
+//
+// One templated source serves FP64 (bit-for-bit with rfsyn's CPU loops: the
+// same operation order, every multiply and add rounded separately through
+// __dmul_rn/__dadd_rn so nothing is contracted into an FMA) and FP32 (plain
+// operators, the compiler may contract).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rfb {
+
+__device__ __forceinline__ double xm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xa(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float xm(float a, float b) { return a * b; }
+__device__ __forceinline__ float xa(float a, float b) { return a + b; }
+__device__ __forceinline__ float xs(float a, float b) { return a - b; }
+
+constexpr int LIST_CODE = 255;
+constexpr int MAX_SKIP = 4;
+
+// psi arrays (slab storage).  H: hx_y hx_z hy_z hy_x hz_x hz_y,
+// E: ex_y ex_z ey_z ey_x ez_x ez_y.  Axis of the slab of each array:
+__host__ __device__ constexpr int psi_axis_h(int p) { return p == 0 ? 1 : p == 1 ? 2 : p == 2 ? 2 : p == 3 ? 0 : p == 4 ? 0 : 1; }
+__host__ __device__ constexpr int psi_axis_e(int p) { return psi_axis_h(p); }
+
+template <typename T>
+struct Args {
+    int nx, ny, nz;
+    unsigned per;
+    long long pitch, plane;  // plane = (ny+1)*pitch
+    T *E[3], *H[3];          // inputs (split: updated in place)
+    T *Eo[3], *Ho[3];        // outputs (split: same as inputs)
+    T cbh, dx;
+    // CPML
+    int cpml_on;
+    const T *kinv_m[3], *b_m[3], *a_m[3];
+    const T *kinv_h[3], *b_h[3], *a_h[3];
+    int lo_m[3], hi_m[3], ns_m[3];
+    int lo_h[3], hi_h[3], ns_h[3];
+    T *psi_e[6];
+    T *psi_hi[6], *psi_ho[6];
+    // scene
+    const uint8_t *codes;    // NULL: table entry 0 everywhere except skip cells
+    const T *tca, *tcb;      // 256 entries
+    int n_skip;
+    long long skip[MAX_SKIP];
+    // interface list
+    int n_cells;
+    const int *lc_ijk;
+    const uint8_t *l_kind;
+    const T *l_ca, *l_cb;
+    const int *l_tix, *l_src;
+    const T *t_m11, *t_scale, *t_w;
+    const int *t_main, *t_nq, *t_uv, *t_sign;
+    // sources
+    const T *src_val;
+    const int *src_hard;
+    long long n_steps;
+    const int *d_step;
+};
+
+template <typename T>
+__device__ __forceinline__ long long cidx(const Args<T> &a, int i, int j, int k) {
+    return ((long long)i * (a.ny + 1) + j) * a.pitch + k;
+}
+
+__device__ __forceinline__ int slab_of(int q, int lo, int hi) {
+    return q < lo ? q : (q >= hi ? lo + (q - hi) : -1);
+}
+
+// Index of slab cell s of a psi array whose slab axis is `axis`.
+template <typename T>
+__device__ __forceinline__ long long psi_idx(const Args<T> &a, int axis, int ns, int s, int i, int j, int k) {
+    if (axis == 0) return ((long long)s * (a.ny + 1) + j) * a.pitch + k;
+    if (axis == 1) return ((long long)i * ns + s) * a.pitch + k;
+    return ((long long)i * (a.ny + 1) + j) * ns + s;
+}
+
+// rfsyn's cpml_term (engine/fdtd/cpml.h:46-51): psi = b psi + a diff;
+// returns diff kappa_inv + dx psi.
+template <typename T>
+__device__ __forceinline__ T cpml_step(T diff, T kinv, T b, T ac, T dx, T psi_old, T *psi_new) {
+    T p = xa(xm(b, psi_old), xm(ac, diff));
+    *psi_new = p;
+    return xa(xm(diff, kinv), xm(dx, p));
+}
+
+// Stretched difference for an H component along `axis` at position q, using
+// psi array p (ping-pong in/out).
+template <typename T>
+__device__ __forceinline__ T h_term(const Args<T> &a, int p, int axis, int q, T diff, int i, int j, int k) {
+    if (!a.cpml_on) return diff;
+    int s = slab_of(q, a.lo_h[axis], a.hi_h[axis]);
+    if (s < 0) return diff;
+    long long pi = psi_idx(a, axis, a.ns_h[axis], s, i, j, k);
+    T pn;
+    T r = cpml_step(diff, a.kinv_h[axis][q], a.b_h[axis][q], a.a_h[axis][q], a.dx, a.psi_hi[p][pi], &pn);
+    a.psi_ho[p][pi] = pn;
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T e_term(const Args<T> &a, int p, int axis, int q, T diff, int i, int j, int k) {
+    if (!a.cpml_on) return diff;
+    int s = slab_of(q, a.lo_m[axis], a.hi_m[axis]);
+    if (s < 0) return diff;
+    long long pi = psi_idx(a, axis, a.ns_m[axis], s, i, j, k);
+    T pn;
+    T r = cpml_step(diff, a.kinv_m[axis][q], a.b_m[axis][q], a.a_m[axis][q], a.dx, a.psi_e[p][pi], &pn);
+    a.psi_e[p][pi] = pn;
+    return r;
+}
+
+// ---- H update (rfsyn cpml.c:176-219; vacuum grid.c:62-90) ----------------
+// One thread per padded cell, all three components; reads E and H from the
+// input buffers and writes H to the output buffers.
+template <typename T>
+__device__ __forceinline__ void h_cell(const Args<T> &a, int i, int j, int k) {
+    const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
+    const long long c = cidx(a, i, j, k);
+    const int jp = (py && j + 1 == a.ny) ? 0 : j + 1;
+    const int kp = (pz && k + 1 == a.nz) ? 0 : k + 1;
+    const int ip = (px && i + 1 == a.nx) ? 0 : i + 1;
+    if (i < a.nx + (px ? 0 : 1) && j < a.ny && k < a.nz) {
+        T dA = xs(a.E[2][cidx(a, i, jp, k)], a.E[2][c]);
+        T dB = xs(a.E[1][cidx(a, i, j, kp)], a.E[1][c]);
+        T tA = h_term(a, 0, 1, j, dA, i, j, k);
+        T tB = h_term(a, 1, 2, k, dB, i, j, k);
+        a.Ho[0][c] = xs(a.H[0][c], xm(a.cbh, xs(tA, tB)));
+    }
+    if (i < a.nx && j < a.ny + (py ? 0 : 1) && k < a.nz) {
+        T dA = xs(a.E[0][cidx(a, i, j, kp)], a.E[0][c]);
+        T dB = xs(a.E[2][cidx(a, ip, j, k)], a.E[2][c]);
+        T tA = h_term(a, 2, 2, k, dA, i, j, k);
+        T tB = h_term(a, 3, 0, i, dB, i, j, k);
+        a.Ho[1][c] = xs(a.H[1][c], xm(a.cbh, xs(tA, tB)));
+    }
+    if (i < a.nx && j < a.ny && k < a.nz + (pz ? 0 : 1)) {
+        T dA = xs(a.E[1][cidx(a, ip, j, k)], a.E[1][c]);
+        T dB = xs(a.E[0][cidx(a, i, jp, k)], a.E[0][c]);
+        T tA = h_term(a, 4, 0, i, dA, i, j, k);
+        T tB = h_term(a, 5, 1, j, dB, i, j, k);
+        a.Ho[2][c] = xs(a.H[2][c], xm(a.cbh, xs(tA, tB)));
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_split(Args<T> a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k > a.nz || j > a.ny || i > a.nx) return;
+    h_cell(a, i, j, k);
+}
+
+// Scalar E update of component comp at (i,j,k): rfsyn materials.c:920-1059.
+// `v` is the current E value (source already applied).
+template <typename T>
+__device__ __forceinline__ T e_scalar(const Args<T> &a, int comp, int i, int j, int k, T v, T ca, T cb) {
+    const long long c = cidx(a, i, j, k);
+    const int im = i == 0 ? a.nx - 1 : i - 1;
+    const int jm = j == 0 ? a.ny - 1 : j - 1;
+    const int km = k == 0 ? a.nz - 1 : k - 1;
+    T tA, tB;
+    if (comp == 0) {
+        tA = e_term(a, 0, 1, j, xs(a.Ho[2][c], a.Ho[2][cidx(a, i, jm, k)]), i, j, k);
+        tB = e_term(a, 1, 2, k, xs(a.Ho[1][c], a.Ho[1][cidx(a, i, j, km)]), i, j, k);
+    } else if (comp == 1) {
+        tA = e_term(a, 2, 2, k, xs(a.Ho[0][c], a.Ho[0][cidx(a, i, j, km)]), i, j, k);
+        tB = e_term(a, 3, 0, i, xs(a.Ho[2][c], a.Ho[2][cidx(a, im, j, k)]), i, j, k);
+    } else {
+        tA = e_term(a, 4, 0, i, xs(a.Ho[1][c], a.Ho[1][cidx(a, im, j, k)]), i, j, k);
+        tB = e_term(a, 5, 1, j, xs(a.Ho[0][c], a.Ho[0][cidx(a, i, jm, k)]), i, j, k);
+    }
+    return xa(xm(ca, v), xm(cb, xs(tA, tB)));
+}
+
+template <typename T>
+__device__ __forceinline__ bool e_updated(const Args<T> &a, int comp, int i, int j, int k) {
+    const int i0 = (a.per & 1u) ? 0 : 1, j0 = (a.per & 2u) ? 0 : 1, k0 = (a.per & 4u) ? 0 : 1;
+    if (i >= a.nx || j >= a.ny || k >= a.nz) return false;
+    if (comp != 0 && i < i0) return false;
+    if (comp != 1 && j < j0) return false;
+    if (comp != 2 && k < k0) return false;
+    return true;
+}
+
+// ---- bulk E update (cells not on the interface list) ---------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_e_split(Args<T> a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= a.nz || j >= a.ny || i >= a.nx) return;
+    const long long c = cidx(a, i, j, k);
+    int code = 0;
+    if (a.codes) {
+        code = a.codes[c];
+        if (code == LIST_CODE) return;
+    } else {
+        for (int s = 0; s < a.n_skip; s++)
+            if (a.skip[s] == c) return;
+    }
+    const T ca = a.tca[code], cb = a.tcb[code];
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++) {
+        if (e_updated(a, comp, i, j, k))
+            a.Eo[comp][c] = e_scalar(a, comp, i, j, k, a.E[comp][c], ca, cb);
+    }
+}
+
+// ---- interface list: overrides, tensor edges, sources --------------------
+// One thread per (cell, component) entry.  Reads E from the input buffers,
+// H from the output buffers (already advanced), writes E output.
+template <typename T>
+__global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * a.n_cells) return;
+    const int cell = e / 3, comp = e - 3 * cell;
+    const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
+    const long long c = cidx(a, i, j, k);
+    T v = a.E[comp][c];
+    const int s = a.l_src[e];
+    if (s >= 0) {
+        const int n = *a.d_step;
+        const T sv = (n < a.n_steps) ? a.src_val[(long long)s * a.n_steps + n] : T(0);
+        v = a.src_hard[s] ? sv : xa(v, sv);
+    }
+    const int kind = a.l_kind[e];
+    if (kind == 1) {
+        v = e_scalar(a, comp, i, j, k, v, a.l_ca[e], a.l_cb[e]);
+    } else if (kind == 2) {
+        // rfsyn materials.c:847-903: value = m11 dHz + sum_q w_q curl_q,
+        // E += scale * value.
+        const int t = a.l_tix[e];
+        const int *mn = a.t_main + 4 * t;
+        T value = xm(a.t_m11[t], xs(a.Ho[2][cidx(a, mn[0], mn[1], k)], a.Ho[2][cidx(a, mn[2], mn[3], k)]));
+        const int nq = a.t_nq[t];
+        const bool neg = a.t_sign[t] < 0;
+        for (int q = 0; q < nq; q++) {
+            const int *uv = a.t_uv + 16 * t + 4 * q;
+            T d = xs(a.Ho[2][cidx(a, uv[0], uv[1], k)], a.Ho[2][cidx(a, uv[2], uv[3], k)]);
+            if (neg) d = -d;
+            value = xa(value, xm(a.t_w[4 * t + q], d));
+        }
+        v = xa(v, xm(a.t_scale[t], value));
+    }
+    a.Eo[comp][c] = v;
+}
+
+// ---- probes ---------------------------------------------------------------
+template <typename T>
+struct ProbeArgs {
+    int n;
+    const long long *cell;
+    const int *comp;
+    const T *F[6];
+    T *ts;
+    long long n_steps;
+    int *d_step;
+};
+
+// Records sample n of every probe after the step, then advances the device
+// step counter (single block).
+template <typename T>
+__global__ void k_probe_gather(ProbeArgs<T> p) {
+    __shared__ int n;
+    if (threadIdx.x == 0) n = *p.d_step;
+    __syncthreads();
+    if (n < p.n_steps)
+        for (int q = threadIdx.x; q < p.n; q += blockDim.x)
+            p.ts[(long long)q * p.n_steps + n] = p.F[p.comp[q]][p.cell[q]];
+    __syncthreads();
+    if (threadIdx.x == 0) *p.d_step = n + 1;
+}
+
+// ---- running DFT of the probe series -------------------------------------
+// Thread per (probe, bin).  FP64 runs: acc += v cos(w t) dt in FP64 with
+// direct sincos (rfsyn probe.c:78-92).  FP32 runs: Kahan-compensated FP32
+// accumulation, phasor advanced by an FP64 recurrence re-anchored every 64
+// samples.
+template <typename T>
+__global__ void k_probe_dft(const T *ts, long long n_steps, int n_probes, int steps_done, int n_freqs,
+                            const double *omega, double dt, double t_off, double *out_re, double *out_im) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (f >= n_freqs || p >= n_probes) return;
+    const T *s = ts + (long long)p * n_steps;
+    const double w = omega[f];
+    if (sizeof(T) == 8) {
+        double re = 0.0, im = 0.0;
+        for (int n = 0; n < steps_done; n++) {
+            double t = ((double)n + t_off) * dt;
+            double sn, cn;
+            sincos(w * t, &sn, &cn);
+            double v = (double)s[n];
+            re = __dadd_rn(re, __dmul_rn(__dmul_rn(v, cn), dt));
+            im = __dsub_rn(im, __dmul_rn(__dmul_rn(v, sn), dt));
+        }
+        out_re[(long long)p * n_freqs + f] = re;
+        out_im[(long long)p * n_freqs + f] = im;
+    } else {
+        float re = 0.f, im = 0.f, cre = 0.f, cim = 0.f;  // Kahan compensation
+        double cw, sw;
+        sincos(w * dt, &sw, &cw);
+        double cn = 1.0, sn = 0.0;
+        const float fdt = (float)dt;
+        for (int n = 0; n < steps_done; n++) {
+            if ((n & 63) == 0) sincos(w * (((double)n + t_off) * dt), &sn, &cn);
+            const float v = (float)s[n] * fdt;
+            float yr = v * (float)cn - cre;
+            float tr = re + yr;
+            cre = (tr - re) - yr;
+            re = tr;
+            float yi = -v * (float)sn - cim;
+            float ti = im + yi;
+            cim = (ti - im) - yi;
+            im = ti;
+            const double c2 = cn * cw - sn * sw;
+            sn = sn * cw + cn * sw;
+            cn = c2;
+        }
+        out_re[(long long)p * n_freqs + f] = (double)re;
+        out_im[(long long)p * n_freqs + f] = (double)im;
+    }
+}
+
+// Marks list cells in a code volume (code-less scenes with many list cells).
+__global__ void k_mark_list(uint8_t *codes, const int *ijk, int n, int ny, long long pitch) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    codes[((long long)ijk[3 * q] * (ny + 1) + ijk[3 * q + 1]) * pitch + ijk[3 * q + 2]] = LIST_CODE;
+}
+
+}  // namespace rfb
