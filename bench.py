@@ -1,0 +1,351 @@
+"""Benchmark of the FDTD stage time loop (one JSON line on rank 0).
+
+Workload: the 256^3 FP32 scene with 24 subpixel-smoothed dielectric spheres,
+3 Debye spheres, 12-cell CPML, 16 probes x 256 DFT bins and 4000 steps
+(rfsyn_b200.scenes.c2).  A bench "step" is one full simulation of that scene
+(reset + 4000 time steps + probe DFT on the device).  Metric:
+Mcell-updates/s = nx*ny*nz*n_steps*K / seconds, whole job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times rfsyn's own CPU loop (compiled from its sources into
+oracle/_ref, or the CPU oracle port when that build is absent) on all host
+cores, on a bounded sample of the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "fused_sweep_c2.md"
+METRIC = "Mcell-updates/s"
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """dram bytes (read + write) per sweep launch from the committed ncu
+    summary (line 'traffic_bytes_per_launch: N'), or None."""
+    try:
+        for line in TRAFFIC.read_text().splitlines():
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                     f[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        except Exception:
+            pass
+        finally:
+            if self.path:
+                try:
+                    os.unlink(self.path)
+                except OSError:
+                    pass
+        load = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes_per_sweep(info, esz: int) -> float:
+    """Compulsory bytes of one H+E sweep launch: every field component read
+    and written once (12 accesses per cell), the material code (1 B), and
+    4 psi read + write per (cell, CPML slab axis); E of interface-list cells
+    is written by the list kernel, not by the sweep."""
+    b = info.cells * (12 * esz + 1) - info.list_cells * 3 * esz
+    b += info.slab_cell_axes * 8 * esz
+    return float(b)
+
+
+# ---------------------------------------------------------------------------
+# CPU reference arm
+# ---------------------------------------------------------------------------
+def cpu_reference(workload, steps: int, threads: int) -> dict:
+    """rfsyn's own CPU loop (oracle/_ref) on `threads` independent copies of
+    the scene, `steps` time steps each; throughput over the slowest copy."""
+    import ctypes as C
+
+    import oracle
+    from tests.cases import workload_to_scene
+
+    kind = "reference" if oracle.ref_available() else "port"
+    scene = workload_to_scene(workload)
+    scene.n_steps = steps
+    scene.probes, scene.freqs = [], []
+    cs = scene.to_c()
+    if kind == "reference":
+        lib = C.CDLL(str(oracle.REF_LIB))
+        fn = lib.scn_time
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        results = [None] * threads
+
+        def work(q):
+            a, b = C.c_double(0), C.c_double(0)
+            rc = fn(C.byref(cs), steps, C.byref(a), C.byref(b))
+            results[q] = (rc, a.value, b.value)
+
+        ts = [threading.Thread(target=work, args=(q,)) for q in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if any(r is None or r[0] != 0 for r in results):
+            raise RuntimeError("reference CPU run failed")
+        loop = max(r[2] for r in results)
+    else:
+        threads = 1
+        t0 = time.perf_counter()
+        oracle.run_oracle(scene)
+        loop = time.perf_counter() - t0
+    value = threads * workload.cells * steps / loop / 1e6
+    return {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": f"{threads} independent copies of the {workload.nx}^3 scene x {steps} of its "
+                      f"{workload.n_steps} steps (FP64; Debye spheres at their static permittivity)",
+            "loop_s": loop}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from rfsyn_b200 import scenes
+
+    w = scenes.c2()
+    threads = max(1, min(os.cpu_count() or 1, 16))
+    res = []
+    for s in range(args.warmup + args.steps):
+        r = cpu_reference(w, args.ref_sample_steps, threads)
+        if s >= args.warmup:
+            res.append(r)
+    value = statistics.median(r["value"] for r in res)
+    cb = dict(res[-1])
+    cb["value"] = value
+    cb.pop("loop_s", None)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG32 scene)",
+        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "n_steps_sampled": args.ref_sample_steps,
+                   "n_steps_full": w.n_steps},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import rfsyn_b200 as rb
+    from rfsyn_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    # each rank simulates its own independent scene (weak scaling, no collective on the data path)
+    w = scenes.c2(seed=2 + rank)
+    rc = scenes.run_config(w)
+    setup = scenes.sphere_setup(w)
+    sim = rb.Sim(rc, setup.ptr if setup else None, None)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    info = sim.info()
+    esz = 4 if w.precision == rb.FP32 else 8
+
+    def one_step():
+        sim.reset()
+        sim.advance(w.n_steps)
+
+    for _ in range(args.warmup):
+        one_step()
+    sim.synchronize()
+    lib = rb.load()
+    launches0 = lib.fdtd_b200_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            one_step()
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    launches = lib.fdtd_b200_launch_count() - launches0
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        if world > 1:
+            dist.barrier()
+    clocks = clk.summary()
+    cells_total = world * w.cells * w.n_steps * args.steps
+    value = cells_total / (ms / 1e3) / 1e6
+
+    # results of the last timed step: probes and spectra (correctness guard)
+    dft = sim.dft()
+    import numpy as np
+
+    finite = bool(np.all(np.isfinite(dft)))
+
+    # live per-kernel timing of the dominant sweep kernel (same scene)
+    sim.reset()
+    sweep_ms, other_ms = sim.time_kernels(200)
+    sweep_launch_ms = sweep_ms / 200
+    alg = algorithmic_bytes_per_sweep(info, esz)
+    peak, peak_kind = hbm_peak()
+    achieved = alg / (sweep_launch_ms / 1e3) / 1e9
+    traffic = ncu_traffic_per_launch()
+    sim.close()
+
+    # end to end through the C ABI with host buffers: setup on the host,
+    # scene upload, the full loop, DFT, download of series and spectra
+    e2e_ms = []
+    h2d = d2h = 0
+    for _ in range(max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = rb.run(rc, setup.ptr if setup else None, None)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        d2h = r["td"].nbytes + r["dft"].nbytes
+    h2d = info.h2d_bytes
+    e2e_ms = max(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * w.cells * w.n_steps / (e2e_ms / 1e3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_reference(w, args.ref_sample_steps, max(1, min(os.cpu_count() or 1, 16)))
+            cb.pop("loop_s", None)
+            cpu = cb
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "unavailable", "sample": str(exc)}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32 scene: 24 smoothed + 3 Debye spheres)",
+        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "n_steps": w.n_steps, "npml": w.npml,
+                   "probes": len(w.probes), "dft_bins": len(w.freqs), "spheres": len(w.spheres),
+                   "list_cells": info.list_cells, "dispersive_samples": info.dispersive,
+                   "schedule": "fused" if info.schedule == rb.FUSED else "split", "tile_j": info.tile_j,
+                   "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
+                   "l2": "inputs larger than L2 (fields 6 x 2 x 76 MB per scene)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": "k_fused (H+E sweep)",
+                     "algorithmic_bytes_per_launch": alg, "launch_ms": sweep_launch_ms,
+                     "other_kernels_ms_per_step": other_ms / 200},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "finite": finite,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--ref-sample-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -99,6 +99,9 @@ int fdtd_b200_sim_reset(fdtd_b200_sim_t *sim);
 /* Enqueue n more steps (asynchronous; CUDA-graph replay). */
 int fdtd_b200_sim_advance(fdtd_b200_sim_t *sim, size_t n_steps);
 int fdtd_b200_sim_synchronize(fdtd_b200_sim_t *sim);
+/* advance + synchronise; *ms = GPU time of the n steps, from CUDA events
+ * recorded on the session stream around them. */
+int fdtd_b200_sim_advance_timed(fdtd_b200_sim_t *sim, size_t n_steps, double *ms);
 size_t fdtd_b200_sim_steps_done(const fdtd_b200_sim_t *sim);
 void *fdtd_b200_sim_stream(const fdtd_b200_sim_t *sim);
 /* n_probes * n_steps doubles, probe-major (blocking). */
@@ -109,6 +112,76 @@ int fdtd_b200_sim_dft(fdtd_b200_sim_t *sim, double *dft_re, double *dft_im);
 int fdtd_b200_sim_read_field(fdtd_b200_sim_t *sim, field_component_t component, double *host);
 /* Kernels launched per time step by this session. */
 int fdtd_b200_sim_launches_per_step(const fdtd_b200_sim_t *sim);
+
+/* Shape of a session's device work, for roofline accounting. */
+typedef struct {
+    size_t cells;            /* nx * ny * nz */
+    size_t list_cells;       /* cells on the interface list (overrides, tensors, dispersive, sources) */
+    size_t dispersive;       /* dispersive (ADE) samples */
+    size_t slab_cell_axes;   /* sum over cells of the CPML slab axes containing them */
+    size_t h2d_bytes;        /* scene bytes uploaded at creation */
+    int precision, schedule;
+    int tile_j, seg_len;     /* fused sweep plan */
+} fdtd_b200_sim_info_t;
+
+int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info);
+
+/* Runs n more steps launching each kernel separately (no graph) with CUDA
+ * events around every launch; *sweep_ms = summed GPU time of the H/E sweep
+ * kernel(s), *other_ms = the interface-list and probe kernels. */
+int fdtd_b200_sim_time_kernels(fdtd_b200_sim_t *sim, size_t n_steps, double *sweep_ms, double *other_ms);
+
+/* ---- dispersive media (auxiliary differential equations) ----------------------
+ * rfsyn models only static eps_r and sigma (engine/fdtd/materials.c:92-125);
+ * these entry points add per-component dispersive samples integrated with
+ * polarisation-current ADEs (Taflove & Hagness, Computational
+ * Electrodynamics, 3rd ed., ch. 9):
+ *   eps(w) = eps_inf + sum_p chi_p(w),   sigma static conductivity,
+ *   Debye   chi_p = delta_eps_p / (1 + j w tau_p),
+ *   Lorentz chi_p = delta_eps_p w_p^2 / (w_p^2 + 2 j w gamma_p - w^2).
+ * A dispersive sample takes precedence over a scalar override of the same
+ * component; a 2x2 tensor edge takes precedence over both; box assignment
+ * clears dispersive samples inside the box, as it clears overrides. */
+#define FDTD_B200_MAX_POLES 2
+typedef enum { FDTD_B200_POLE_DEBYE = 0, FDTD_B200_POLE_LORENTZ = 1 } fdtd_b200_pole_kind_t;
+
+typedef struct {
+    double eps_inf;                          /* >= 1 */
+    double sigma;                            /* >= 0, S/m */
+    int n_poles;                             /* 1 .. FDTD_B200_MAX_POLES */
+    int kind[FDTD_B200_MAX_POLES];           /* fdtd_b200_pole_kind_t */
+    double delta_eps[FDTD_B200_MAX_POLES];   /* > 0 */
+    double tau[FDTD_B200_MAX_POLES];         /* Debye relaxation time (s) */
+    double omega_p[FDTD_B200_MAX_POLES];     /* Lorentz resonance (rad/s) */
+    double gamma[FDTD_B200_MAX_POLES];       /* Lorentz damping (1/s) */
+} fdtd_b200_dispersive_t;
+
+int fdtd_b200_materials_set_component_dispersive(materials_t *mat, const fdtd_grid_t *g,
+                                                 field_component_t component, size_t i, size_t j, size_t k,
+                                                 const fdtd_b200_dispersive_t *model);
+int fdtd_b200_materials_clear_component_dispersive(materials_t *mat, const fdtd_grid_t *g,
+                                                   field_component_t component, size_t i, size_t j, size_t k);
+
+/* ---- spheres with subpixel smoothing -------------------------------------------
+ * Rasterises spheres (centre and radius in cell units: the E_x sample of cell
+ * (i,j,k) sits at (i+1/2, j, k), E_y at (i, j+1/2, k), E_z at (i, j, k+1/2))
+ * in list order, later spheres over earlier ones.  The fill fraction f of the
+ * unit cube around every E sample near a surface is computed on the GPU in
+ * FP64 (supersampled, 8^3 points).  A cell whose three samples are inside
+ * takes the sphere's material id; samples cut by the surface get a scalar
+ * override with the diagonal of the smoothed inverse permittivity
+ *   1/eps_c = n_c^2 <1/eps> + (1 - n_c^2) / <eps>,  <.> weighted by f,
+ * n the outward surface normal, sigma mixed by f (smoothing = 1), or the
+ * inside material when f >= 1/2 (smoothing = 0).  Dispersive spheres
+ * (model != NULL) are always staircased onto dispersive samples. */
+typedef struct {
+    double cx, cy, cz, radius;
+    double eps_r, sigma;
+    const fdtd_b200_dispersive_t *model;     /* NULL: plain dielectric */
+} fdtd_b200_sphere_t;
+
+int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_sphere_t *spheres,
+                                    size_t n_spheres, int smoothing);
 
 /* ---- process-wide settings and diagnostics ---------------------------------- */
 /* Precision / schedule used by rfsyn's own entry points (fdtd_simulate_echo,

@@ -52,6 +52,32 @@ class ScnProbe(C.Structure):
     _fields_ = [("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t), ("comp", C.c_int)]
 
 
+class ScnDisp(C.Structure):
+    _fields_ = [("comp", C.c_int), ("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t),
+                ("eps_inf", C.c_double), ("sigma", C.c_double), ("npoles", C.c_int), ("kind", C.c_int * 2),
+                ("delta_eps", C.c_double * 2), ("tau", C.c_double * 2), ("omega_p", C.c_double * 2),
+                ("gamma", C.c_double * 2)]
+
+
+class ScnSphere(C.Structure):
+    _fields_ = [("cx", C.c_double), ("cy", C.c_double), ("cz", C.c_double), ("radius", C.c_double),
+                ("eps_r", C.c_double), ("sigma", C.c_double), ("disp", C.c_int)]
+
+
+MODEL_ONLY = (1 << 64) - 1  # i of a dispersive entry used only as a sphere material
+
+
+def disp_entry(comp, i, j, k, eps_inf, sigma, poles):
+    """poles: list of ("debye", delta_eps, tau) / ("lorentz", delta_eps, omega_p, gamma)."""
+    kind, de, tau, wp, gm = [0, 0], [0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [0.0, 0.0]
+    for q, p in enumerate(poles):
+        if p[0] == "debye":
+            kind[q], de[q], tau[q] = 0, p[1], p[2]
+        else:
+            kind[q], de[q], wp[q], gm[q] = 1, p[1], p[2], p[3]
+    return (comp, i, j, k, eps_inf, sigma, len(poles), tuple(kind), tuple(de), tuple(tau), tuple(wp), tuple(gm))
+
+
 class ScnScene(C.Structure):
     _fields_ = [
         ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t), ("dx", C.c_double), ("courant", C.c_double),
@@ -61,6 +87,9 @@ class ScnScene(C.Structure):
         ("n_boxes", C.c_size_t), ("boxes", C.POINTER(ScnBox)),
         ("n_comps", C.c_size_t), ("comps", C.POINTER(ScnComp)),
         ("n_tensors", C.c_size_t), ("tensors", C.POINTER(ScnTensor)),
+        ("n_disp", C.c_size_t), ("disp", C.POINTER(ScnDisp)),
+        ("n_spheres", C.c_size_t), ("spheres", C.POINTER(ScnSphere)),
+        ("smoothing", C.c_int),
         ("n_sources", C.c_size_t), ("sources", C.POINTER(ScnSource)),
         ("n_probes", C.c_size_t), ("probes", C.POINTER(ScnProbe)),
         ("n_freqs", C.c_size_t), ("freqs", C.POINTER(C.c_double)),
@@ -88,6 +117,9 @@ class Scene:
     boxes: list = field(default_factory=list)      # (i0,i1,j0,j1,k0,k1,eps,sigma)
     comps: list = field(default_factory=list)      # (comp,i,j,k,eps,sigma)
     tensors: list = field(default_factory=list)    # (comp,i,j,k,m11,m12,m22)
+    disp: list = field(default_factory=list)       # disp_entry(...) tuples
+    spheres: list = field(default_factory=list)    # (cx,cy,cz,r,eps,sigma,disp_index or -1)
+    smoothing: int = 1
     sources: list = field(default_factory=list)    # (i,j,k,comp,mode,amp,waveform,p0,p1,p2)
     probes: list = field(default_factory=list)     # (i,j,k,comp)
     freqs: list = field(default_factory=list)
@@ -102,7 +134,7 @@ class Scene:
         """Returns the C struct; the arrays stay alive as attributes of it."""
         s = ScnScene()
         for name in ("nx", "ny", "nz", "dx", "courant", "n_steps", "periodic", "npml", "m", "ma", "kappa_max",
-                     "alpha_max", "r0", "src_t_offset", "dft_t_offset"):
+                     "alpha_max", "r0", "src_t_offset", "dft_t_offset", "smoothing"):
             setattr(s, name, getattr(self, name))
         keep = []
 
@@ -114,6 +146,13 @@ class Scene:
         s.n_boxes, s.boxes = arr(ScnBox, self.boxes)
         s.n_comps, s.comps = arr(ScnComp, self.comps)
         s.n_tensors, s.tensors = arr(ScnTensor, self.tensors)
+        drows = []
+        for d in self.disp:
+            comp, i, j, k, ei, sg, npl, kind, de, tau, wp, gm = d
+            drows.append((comp, i, j, k, ei, sg, npl, (C.c_int * 2)(*kind), (C.c_double * 2)(*de),
+                          (C.c_double * 2)(*tau), (C.c_double * 2)(*wp), (C.c_double * 2)(*gm)))
+        s.n_disp, s.disp = arr(ScnDisp, drows)
+        s.n_spheres, s.spheres = arr(ScnSphere, self.spheres)
         s.n_sources, s.sources = arr(ScnSource, self.sources)
         s.n_probes, s.probes = arr(ScnProbe, self.probes)
         f = (C.c_double * max(len(self.freqs), 1))(*self.freqs)

@@ -18,6 +18,12 @@
  *   2x2 tensor edge .............. engine/fdtd/materials.c:836-903
  *   sources ...................... engine/fdtd/source.c:8-57
  *   probes, DFT .................. engine/fdtd/probe.c:40-92
+ * Beyond rfsyn (no reference counterpart; pinned by physics checks in tests):
+ *   dispersive ADE samples ....... Taflove & Hagness, Computational
+ *                                  Electrodynamics 3rd ed. sec. 9.4 (Debye
+ *                                  and Lorentz polarisation currents)
+ *   sphere fill fractions and the diagonal of the smoothed inverse
+ *   permittivity (Farjadpour et al., Opt. Lett. 31, 2972 (2006))
  * The data structures are the plainest possible (dense per-component override
  * and tensor planes, full-grid psi) so the restatement is easy to audit.
  */
@@ -27,6 +33,7 @@
 #include <string.h>
 
 #include "scene.h"
+#include "sphere_raster.h"
 
 #define O_C0 299792458.0
 #define O_EPS0 8.8541878128e-12
@@ -51,6 +58,11 @@ typedef struct {
     double *oca[3], *ocb[3];
     uint8_t *has_t[2];
     double *tm11[2], *tm12[2], *tm22[2], *tscale[2];
+    /* dispersive samples: per-component index into the ADE arrays (-1) */
+    int *dix[3];
+    size_t nd, dcap;
+    double *drec;   /* 16 per sample */
+    double *dst;    /* 5 per sample: J0 J1 J0- J1- E- */
 } orc_t;
 
 static int periodic(const orc_t *o, int a) { return (o->per >> a) & 1u; }
@@ -103,8 +115,111 @@ static void orc_free(orc_t *o) {
         free(o->has_ovr[c]); free(o->oca[c]); free(o->ocb[c]);
     }
     for (int c = 0; c < 2; c++) { free(o->has_t[c]); free(o->tm11[c]); free(o->tm12[c]); free(o->tm22[c]); free(o->tscale[c]); }
+    for (int c = 0; c < 3; c++) free(o->dix[c]);
+    free(o->drec);
+    free(o->dst);
     free(o->id);
 }
+
+/* ADE coefficients of a dispersive sample (see the product's record layout):
+ * E+ = ca E + cb (dA - dB) + ce E- - sum_p (cj J + cjm J-),
+ * J+ = aJ J + aJm J- + aE (E+ - E_ref).  Debye: k = (1 - dt/2tau)/(1 + dt/2tau),
+ * beta = eps0 de dt/tau / (1 + dt/2tau); Lorentz: a = (2 - wp^2 dt^2)/(1+g dt),
+ * xi = (g dt - 1)/(1 + g dt), gl = eps0 de wp^2 dt^2/(1 + g dt); Ampere at
+ * n+1/2 gives A = eps0 eps_inf + sigma dt/2 + sum beta/2 + sum gl/4. */
+static void ade_coeffs(const scn_disp_t *d, double dt, double dx, double *r) {
+    double e0ei = O_EPS0 * d->eps_inf, hb = 0.0, qg = 0.0;
+    double kJ[2] = {0, 0}, kJm[2] = {0, 0}, kE[2] = {0, 0};
+    for (int p = 0; p < d->npoles; p++) {
+        if (d->kind[p] == 0) {
+            double den = 1.0 + dt / (2.0 * d->tau[p]);
+            double beta = (O_EPS0 * d->delta_eps[p] * dt / d->tau[p]) / den;
+            kJ[p] = (1.0 - dt / (2.0 * d->tau[p])) / den;
+            kE[p] = beta / dt;
+            hb += 0.5 * beta;
+        } else {
+            double den = 1.0 + d->gamma[p] * dt;
+            double gl = O_EPS0 * d->delta_eps[p] * d->omega_p[p] * d->omega_p[p] * dt * dt / den;
+            kJ[p] = (2.0 - d->omega_p[p] * d->omega_p[p] * dt * dt) / den;
+            kJm[p] = (d->gamma[p] * dt - 1.0) / den;
+            kE[p] = gl / (2.0 * dt);
+            qg += 0.25 * gl;
+        }
+    }
+    double A = e0ei + 0.5 * d->sigma * dt + hb + qg;
+    memset(r, 0, 16 * sizeof(double));
+    r[0] = (e0ei - 0.5 * d->sigma * dt + hb) / A;
+    r[1] = dt / (A * dx);
+    r[2] = qg / A;
+    r[3] = (double)d->npoles;
+    for (int p = 0; p < d->npoles; p++) {
+        double *w = r + 4 + 6 * p;
+        w[0] = (double)d->kind[p];
+        w[1] = 0.5 * dt * (1.0 + kJ[p]) / A;
+        w[2] = 0.5 * dt * kJm[p] / A;
+        w[3] = kJ[p];
+        w[4] = kJm[p];
+        w[5] = kE[p];
+    }
+}
+
+static int set_disp(orc_t *o, int c, size_t w, const scn_disp_t *d) {
+    if (o->dix[c][w] < 0) {
+        if (o->nd == o->dcap) {
+            o->dcap = o->dcap ? 2 * o->dcap : 64;
+            double *nr = realloc(o->drec, o->dcap * 16 * sizeof(double));
+            if (nr) o->drec = nr;
+            double *ns = realloc(o->dst, o->dcap * 5 * sizeof(double));
+            if (ns) o->dst = ns;
+            if (!nr || !ns) return -1;
+        }
+        o->dix[c][w] = (int)o->nd++;
+    }
+    size_t q = (size_t)o->dix[c][w];
+    ade_coeffs(d, o->dt, o->dx, o->drec + 16 * q);
+    memset(o->dst + 5 * q, 0, 5 * sizeof(double));
+    return 0;
+}
+
+static int coeff(const orc_t *o, double eps_r, double sigma, double *ca, double *cb);
+static int table_id(orc_t *o, double eps_r, double sigma);
+
+/* oracle-side callbacks of the shared sphere rasteriser */
+static void sr_bg(void *ctx, size_t w, double *eps, double *sig) {
+    orc_t *o = (orc_t *)ctx;
+    *eps = o->teps[o->id[w]];
+    *sig = o->tsig[o->id[w]];
+}
+static void clear_samples(orc_t *o, size_t w) {
+    for (int c = 0; c < 3; c++) o->has_ovr[c][w] = 0, o->dix[c][w] = -1;
+    for (int c = 0; c < 2; c++) o->has_t[c][w] = 0;
+}
+static int sr_fill(void *ctx, size_t w, const scn_sphere_t *sp) {
+    orc_t *o = (orc_t *)ctx;
+    int id = table_id(o, sp->eps_r, sp->sigma);
+    if (id < 0) return -1;
+    clear_samples(o, w);
+    o->id[w] = (uint8_t)id;
+    return 0;
+}
+static int sr_fill_disp(void *ctx, size_t w, const scn_disp_t *d) {
+    orc_t *o = (orc_t *)ctx;
+    clear_samples(o, w);
+    for (int c = 0; c < 3; c++)
+        if (set_disp(o, c, w, d) != 0) return -1;
+    return 0;
+}
+static int sr_sample(void *ctx, size_t w, int c, double eps, double sig) {
+    orc_t *o = (orc_t *)ctx;
+    if (coeff(o, eps, sig, &o->oca[c][w], &o->ocb[c][w]) != 0) return -1;
+    o->has_ovr[c][w] = 1;
+    o->dix[c][w] = -1;
+    return 0;
+}
+static int sr_sample_disp(void *ctx, size_t w, int c, const scn_disp_t *d) {
+    return set_disp((orc_t *)ctx, c, w, d);
+}
+static size_t sr_canon(const void *geo, size_t i, size_t j, size_t k) { return at((const orc_t *)geo, i, j, k); }
 
 /* materials.c:92-125 */
 static int coeff(const orc_t *o, double eps_r, double sigma, double *ca, double *cb) {
@@ -150,6 +265,11 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
     }
     o->id = calloc(o->total, 1);
     if (!o->id) return -1;
+    for (int c = 0; c < 3; c++) {
+        o->dix[c] = malloc(o->total * sizeof(int));
+        if (!o->dix[c]) return -1;
+        for (size_t q = 0; q < o->total; q++) o->dix[c][q] = -1;
+    }
     table_id(o, 1.0, 0.0);
     if (s->npml) {
         o->cpml = 1;
@@ -179,7 +299,7 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
                     size_t raw = (i * (o->n[1] + 1) + j) * (o->n[2] + 1) + k;
                     size_t w = at(o, i, j, k);
                     o->id[w] = (uint8_t)id;
-                    for (int c = 0; c < 3; c++) o->has_ovr[c][raw] = 0;
+                    for (int c = 0; c < 3; c++) o->has_ovr[c][raw] = 0, o->dix[c][raw] = -1;
                     for (int c = 0; c < 2; c++) o->has_t[c][raw] = 0;
                 }
     }
@@ -197,6 +317,18 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
         o->tm12[t->comp][w] = t->m12;
         o->tm22[t->comp][w] = t->m22;
         o->tscale[t->comp][w] = o->dt / (O_EPS0 * o->dx);
+    }
+    for (size_t q = 0; q < s->n_disp; q++) {
+        const scn_disp_t *d = &s->disp[q];
+        if (d->i > o->n[0]) continue;  /* model-only entry (sphere material) */
+        if (set_disp(o, d->comp, at(o, d->i, d->j, d->k), d) != 0) return -1;
+    }
+    /* spheres in list order (oracle/sphere_raster.h) */
+    if (s->n_spheres) {
+        for (size_t q = 0; q < s->n_spheres; q++)
+            if (s->spheres[q].disp < 0 && table_id(o, s->spheres[q].eps_r, s->spheres[q].sigma) < 0) return -1;
+        sr_target_t tg = {o, sr_bg, sr_fill, sr_fill_disp, sr_sample, sr_sample_disp};
+        if (sr_rasterise(s, o->n, o->per, sr_canon, o, &tg) != 0) return -1;
     }
     return 0;
 }
@@ -310,6 +442,26 @@ static void update_e(orc_t *o) {
                                      &o->psiE[c][0][here]);
                         tB = stretch(tB, o->km[axb][p[axb]], o->bm[axb][p[axb]], o->am[axb][p[axb]], o->dx,
                                      &o->psiE[c][1][here]);
+                    }
+                    if (o->dix[c][here] >= 0) {
+                        /* polarisation-current ADE (Debye / Lorentz poles) */
+                        const double *r = o->drec + 16 * (size_t)o->dix[c][here];
+                        double *st = o->dst + 5 * (size_t)o->dix[c][here];
+                        double v = o->E[c][here], em = st[4];
+                        double en = r[0] * v + r[1] * (tA - tB);
+                        en = en + r[2] * em;
+                        int np = (int)r[3];
+                        for (int q = 0; q < np; q++) en = en - (r[5 + 6 * q] * st[q] + r[6 + 6 * q] * st[2 + q]);
+                        for (int q = 0; q < np; q++) {
+                            const double *w = r + 4 + 6 * q;
+                            double eref = w[0] != 0.0 ? em : v;
+                            double jn = (w[3] * st[q] + w[4] * st[2 + q]) + w[5] * (en - eref);
+                            st[2 + q] = st[q];
+                            st[q] = jn;
+                        }
+                        st[4] = v;
+                        o->E[c][here] = en;
+                        continue;
                     }
                     o->E[c][here] = ca * o->E[c][here] + cb * (tA - tB);
                 }

@@ -28,6 +28,21 @@ typedef struct { int comp; size_t i, j, k; double m11, m12, m22; } scn_tensor_t;
  *           2 modulated Gaussian (p0 f, p1 t0, p2 tau).  mode 0 soft, 1 hard. */
 typedef struct { size_t i, j, k; int comp, mode; double amplitude; int waveform; double p0, p1, p2; } scn_source_t;
 typedef struct { size_t i, j, k; int comp; } scn_probe_t;
+/* dispersive sample (no rfsyn counterpart): kind 0 Debye (tau), 1 Lorentz
+ * (omega_p, gamma) per pole */
+typedef struct {
+    int comp; size_t i, j, k;
+    double eps_inf, sigma;
+    int npoles;
+    int kind[2];
+    double delta_eps[2], tau[2], omega_p[2], gamma[2];
+} scn_disp_t;
+/* sphere in cell units (no rfsyn counterpart); disp >= 0 selects a
+ * dispersive model from the disp list (its position fields are ignored) */
+typedef struct {
+    double cx, cy, cz, radius, eps_r, sigma;
+    int disp;
+} scn_sphere_t;
 
 typedef struct {
     size_t nx, ny, nz;
@@ -39,6 +54,9 @@ typedef struct {
     size_t n_boxes;   const scn_box_t *boxes;       /* applied first, in order */
     size_t n_comps;   const scn_comp_t *comps;      /* then scalar overrides */
     size_t n_tensors; const scn_tensor_t *tensors;  /* then tensor edges */
+    size_t n_disp;    const scn_disp_t *disp;       /* then dispersive samples */
+    size_t n_spheres; const scn_sphere_t *spheres;  /* then spheres, in order */
+    int smoothing;                                  /* sphere smoothing on/off */
     size_t n_sources; const scn_source_t *sources;
     size_t n_probes;  const scn_probe_t *probes;
     size_t n_freqs;   const double *freqs;

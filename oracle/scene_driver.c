@@ -10,11 +10,139 @@
  */
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "rfsyn_fdtd.h"
 #include "scene.h"
+#include "sphere_raster.h"
+#ifdef SCN_WITH_B200_EXT
+#include "rfsyn_fdtd_b200.h"
+#endif
 
 static field_component_t comp_of(int c) { return (field_component_t)c; }
+
+#ifndef SCN_WITH_B200_EXT
+static double static_eps(const scn_disp_t *d) {
+    double e = d->eps_inf;
+    for (int p = 0; p < d->npoles; p++) e += d->delta_eps[p];
+    return e;
+}
+
+/* Spheres for rfsyn: rasterised into a shadow state with the shared
+ * rasteriser, then handed to rfsyn's own API as column boxes of equal id
+ * followed by per-component overrides in increasing key order (rfsyn keeps
+ * overrides sorted, so in-order insertion appends). */
+typedef struct {
+    const fdtd_grid_t *g;
+    materials_t *m;
+    uint8_t *ids;
+    double teps[256], tsig[256];
+    int ntab;
+    int32_t *ovr;   /* per (cell, comp): index into oe/os or -1 */
+    double *oe, *os;
+    size_t no, cap;
+} shadow_t;
+
+static int sh_id(shadow_t *h, double eps, double sig) {
+    material_id_t id;
+    if (materials_register(h->m, eps, sig, &id) != 0) return -1;
+    h->teps[id] = eps;
+    h->tsig[id] = sig;
+    if ((int)id >= h->ntab) h->ntab = (int)id + 1;
+    return (int)id;
+}
+static void sh_bg(void *ctx, size_t w, double *eps, double *sig) {
+    shadow_t *h = (shadow_t *)ctx;
+    *eps = h->teps[h->ids[w]];
+    *sig = h->tsig[h->ids[w]];
+}
+static int sh_set(shadow_t *h, size_t w, int c, double eps, double sig) {
+    if (h->ovr[3 * w + (size_t)c] < 0) {
+        if (h->no == h->cap) {
+            h->cap = h->cap ? 2 * h->cap : 1024;
+            double *ne = realloc(h->oe, h->cap * sizeof(double));
+            if (ne) h->oe = ne;
+            double *ns = realloc(h->os, h->cap * sizeof(double));
+            if (ns) h->os = ns;
+            if (!ne || !ns) return -1;
+        }
+        h->ovr[3 * w + (size_t)c] = (int32_t)h->no++;
+    }
+    h->oe[h->ovr[3 * w + (size_t)c]] = eps;
+    h->os[h->ovr[3 * w + (size_t)c]] = sig;
+    return 0;
+}
+static int sh_fill(void *ctx, size_t w, const scn_sphere_t *sp) {
+    shadow_t *h = (shadow_t *)ctx;
+    int id = sh_id(h, sp->eps_r, sp->sigma);
+    if (id < 0) return -1;
+    h->ids[w] = (uint8_t)id;
+    for (int c = 0; c < 3; c++) h->ovr[3 * w + (size_t)c] = -1;
+    return 0;
+}
+static int sh_fill_disp(void *ctx, size_t w, const scn_disp_t *d) {
+    shadow_t *h = (shadow_t *)ctx;
+    int id = sh_id(h, static_eps(d), d->sigma);
+    if (id < 0) return -1;
+    h->ids[w] = (uint8_t)id;
+    for (int c = 0; c < 3; c++) h->ovr[3 * w + (size_t)c] = -1;
+    return 0;
+}
+static int sh_sample(void *ctx, size_t w, int c, double eps, double sig) { return sh_set((shadow_t *)ctx, w, c, eps, sig); }
+static int sh_sample_disp(void *ctx, size_t w, int c, const scn_disp_t *d) {
+    return sh_set((shadow_t *)ctx, w, c, static_eps(d), d->sigma);
+}
+static size_t sh_canon(const void *geo, size_t i, size_t j, size_t k) { return fdtd_index((const fdtd_grid_t *)geo, i, j, k); }
+
+static int ref_spheres(const fdtd_grid_t *g, materials_t *m, const scn_scene_t *s) {
+    int rc = -1;
+    size_t total = (g->nx + 1) * (g->ny + 1) * (g->nz + 1);
+    shadow_t h;
+    memset(&h, 0, sizeof h);
+    h.g = g;
+    h.m = m;
+    h.ids = calloc(total, 1);
+    h.ovr = malloc(3 * total * sizeof(int32_t));
+    if (!h.ids || !h.ovr) goto out;
+    for (size_t q = 0; q < 3 * total; q++) h.ovr[q] = -1;
+    if (sh_id(&h, 1.0, 0.0) != 0) goto out;
+    /* the spheres are applied after the scene's boxes, which this shadow does
+     * not track: scenes given to rfsyn with spheres carry no boxes */
+    if (s->n_boxes) goto out;
+    {
+        const size_t n[3] = {g->nx, g->ny, g->nz};
+        sr_target_t tg = {&h, sh_bg, sh_fill, sh_fill_disp, sh_sample, sh_sample_disp};
+        if (sr_rasterise(s, n, g->periodic_axes, sh_canon, g, &tg) != 0) goto out;
+    }
+    /* ids: runs of equal non-vacuum id along k become boxes */
+    for (size_t i = 0; i <= g->nx; i++)
+        for (size_t j = 0; j <= g->ny; j++) {
+            size_t base = (i * (g->ny + 1) + j) * (g->nz + 1);
+            size_t k = 0;
+            while (k <= g->nz) {
+                uint8_t id = h.ids[base + k];
+                size_t k1 = k + 1;
+                while (k1 <= g->nz && h.ids[base + k1] == id) k1++;
+                if (id != 0 && materials_assign_box(m, g, i, i + 1, j, j + 1, k, k1, id) != 0) goto out;
+                k = k1;
+            }
+        }
+    for (size_t q = 0; q < 3 * total; q++) {
+        if (h.ovr[q] < 0) continue;
+        size_t w = q / 3, c = q % 3, kk = w % (g->nz + 1), row = w / (g->nz + 1);
+        if (materials_set_component(m, g, comp_of((int)c), row / (g->ny + 1), row % (g->ny + 1), kk, h.oe[h.ovr[q]],
+                                    h.os[h.ovr[q]]) != 0)
+            goto out;
+    }
+    rc = 0;
+out:
+    free(h.ids);
+    free(h.ovr);
+    free(h.oe);
+    free(h.os);
+    return rc;
+}
+#endif
 
 /* Applies boxes, then scalar overrides, then tensor edges (in list order). */
 int scn_setup(const fdtd_grid_t *g, materials_t *m, void *ctx) {
@@ -32,6 +160,57 @@ int scn_setup(const fdtd_grid_t *g, materials_t *m, void *ctx) {
         if (materials_set_component_tensor(m, g, comp_of(t->comp), t->i, t->j, t->k, t->m11, t->m12, t->m22) != 0)
             return -1;
     }
+#ifdef SCN_WITH_B200_EXT
+    for (size_t q = 0; q < s->n_disp; q++) {
+        const scn_disp_t *d = &s->disp[q];
+        fdtd_b200_dispersive_t md;
+        memset(&md, 0, sizeof md);
+        md.eps_inf = d->eps_inf;
+        md.sigma = d->sigma;
+        md.n_poles = d->npoles;
+        for (int p = 0; p < 2; p++) {
+            md.kind[p] = d->kind[p];
+            md.delta_eps[p] = d->delta_eps[p];
+            md.tau[p] = d->tau[p];
+            md.omega_p[p] = d->omega_p[p];
+            md.gamma[p] = d->gamma[p];
+        }
+        if (d->i <= g->nx && fdtd_b200_materials_set_component_dispersive(m, g, comp_of(d->comp), d->i, d->j, d->k, &md) != 0)
+            return -1;
+    }
+    if (s->n_spheres) {
+        fdtd_b200_sphere_t *sp = calloc(s->n_spheres, sizeof(*sp));
+        fdtd_b200_dispersive_t *md = calloc(s->n_spheres, sizeof(*md));
+        if (!sp || !md) { free(sp); free(md); return -1; }
+        for (size_t q = 0; q < s->n_spheres; q++) {
+            const scn_sphere_t *b = &s->spheres[q];
+            sp[q].cx = b->cx; sp[q].cy = b->cy; sp[q].cz = b->cz; sp[q].radius = b->radius;
+            sp[q].eps_r = b->eps_r; sp[q].sigma = b->sigma;
+            if (b->disp >= 0) {
+                const scn_disp_t *d = &s->disp[b->disp];
+                md[q].eps_inf = d->eps_inf; md[q].sigma = d->sigma; md[q].n_poles = d->npoles;
+                for (int p = 0; p < 2; p++) {
+                    md[q].kind[p] = d->kind[p]; md[q].delta_eps[p] = d->delta_eps[p]; md[q].tau[p] = d->tau[p];
+                    md[q].omega_p[p] = d->omega_p[p]; md[q].gamma[p] = d->gamma[p];
+                }
+                sp[q].model = &md[q];
+            }
+        }
+        int rc = fdtd_b200_materials_add_spheres(m, g, sp, s->n_spheres, s->smoothing);
+        free(sp);
+        free(md);
+        if (rc != 0) return -1;
+    }
+#else
+    /* rfsyn has no dispersive media: dispersive samples enter rfsyn at their
+     * static permittivity eps_inf + sum delta_eps */
+    for (size_t q = 0; q < s->n_disp; q++) {
+        const scn_disp_t *d = &s->disp[q];
+        if (d->i > g->nx) continue;
+        if (materials_set_component(m, g, comp_of(d->comp), d->i, d->j, d->k, static_eps(d), d->sigma) != 0) return -1;
+    }
+    if (s->n_spheres && ref_spheres(g, m, s) != 0) return -1;
+#endif
     return 0;
 }
 
@@ -144,6 +323,63 @@ int scn_run_fields(const scn_scene_t *s, const double *initial, double *fields_o
         else fdtd_update_e_materials(g, m);
     }
     for (int c = 0; c < 6; c++) memcpy(fields_out + c * total, f[c], total * sizeof(double));
+    rc = 0;
+out:
+    materials_destroy(m);
+    cpml_destroy(p);
+    fdtd_grid_destroy(g);
+    return rc;
+}
+
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* Builds the scene, then times `steps` steps of the loop (H, sources, E)
+ * without probes: *setup_s and *loop_s are wall-clock seconds. */
+int scn_time(const scn_scene_t *s, size_t steps, double *setup_s, double *loop_s) {
+    int rc = -1;
+    double t0 = now_s();
+    fdtd_grid_t *g = fdtd_grid_create(s->nx, s->ny, s->nz, s->dx, s->courant);
+    cpml_t *p = NULL;
+    materials_t *m = NULL;
+    source_t src;
+    source_modulated_gaussian_params_t mg;
+    source_gaussian_deriv_params_t gd;
+    if (!g) return -1;
+    if (fdtd_grid_set_periodic(g, s->periodic) != 0) goto out;
+    if (s->npml) {
+        cpml_params_t cp = {s->npml, s->m, s->ma, s->kappa_max, s->alpha_max, s->r0};
+        p = cpml_create(g, cp);
+        if (!p) goto out;
+    }
+    m = materials_create(g);
+    if (!m || scn_setup(g, m, (void *)s) != 0) goto out;
+    if (s->n_sources) {
+        const scn_source_t *d = &s->sources[0];
+        if (d->waveform == 2) {
+            mg.freq_hz = d->p0; mg.t0 = d->p1; mg.tau = d->p2;
+            src = source_make_point(d->i, d->j, d->k, comp_of(d->comp), SRC_SOFT, d->amplitude,
+                                    source_waveform_modulated_gaussian, &mg);
+        } else {
+            gd.t0 = d->p0; gd.tau = d->p1;
+            src = source_make_point(d->i, d->j, d->k, comp_of(d->comp), SRC_SOFT, d->amplitude,
+                                    source_waveform_gaussian_derivative, &gd);
+        }
+    }
+    double t1 = now_s();
+    for (size_t n = 0; n < steps; n++) {
+        if (p) fdtd_update_h_cpml(g, p);
+        else fdtd_update_h(g);
+        if (s->n_sources) source_apply(&src, g, (double)n * g->dt);
+        if (p) fdtd_update_e_cpml_materials(g, p, m);
+        else fdtd_update_e_materials(g, m);
+    }
+    double t2 = now_s();
+    if (setup_s) *setup_s = t1 - t0;
+    if (loop_s) *loop_s = t2 - t1;
     rc = 0;
 out:
     materials_destroy(m);

@@ -76,7 +76,63 @@ class B200Result(C.Structure):
                 ("dft_im", C.POINTER(C.c_double)), ("sample_rate_hz", C.c_double), ("device_ms", C.c_double)]
 
 
+class Dispersive(C.Structure):
+    """fdtd_b200_dispersive_t."""
+
+    _fields_ = [("eps_inf", C.c_double), ("sigma", C.c_double), ("n_poles", C.c_int), ("kind", C.c_int * 2),
+                ("delta_eps", C.c_double * 2), ("tau", C.c_double * 2), ("omega_p", C.c_double * 2),
+                ("gamma", C.c_double * 2)]
+
+
+class Sphere(C.Structure):
+    """fdtd_b200_sphere_t."""
+
+    _fields_ = [("cx", C.c_double), ("cy", C.c_double), ("cz", C.c_double), ("radius", C.c_double),
+                ("eps_r", C.c_double), ("sigma", C.c_double), ("model", C.POINTER(Dispersive))]
+
+
+class SimInfo(C.Structure):
+    _fields_ = [("cells", C.c_size_t), ("list_cells", C.c_size_t), ("dispersive", C.c_size_t),
+                ("slab_cell_axes", C.c_size_t), ("h2d_bytes", C.c_size_t), ("precision", C.c_int),
+                ("schedule", C.c_int), ("tile_j", C.c_int), ("seg_len", C.c_int)]
+
+
 SETUP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+
+
+def dispersive(eps_inf: float, sigma: float, poles) -> Dispersive:
+    """poles: ("debye", delta_eps, tau) / ("lorentz", delta_eps, omega_p, gamma)."""
+    d = Dispersive()
+    d.eps_inf, d.sigma, d.n_poles = eps_inf, sigma, len(poles)
+    for q, p in enumerate(poles):
+        if p[0] == "debye":
+            d.kind[q], d.delta_eps[q], d.tau[q] = 0, p[1], p[2]
+        else:
+            d.kind[q], d.delta_eps[q], d.omega_p[q], d.gamma[q] = 1, p[1], p[2], p[3]
+    return d
+
+
+class SphereSetup:
+    """An fdtd_material_setup_fn that rasterises spheres through
+    fdtd_b200_materials_add_spheres (keeps the ctypes objects alive)."""
+
+    def __init__(self, spheres, smoothing: int = 1):
+        lib = load()
+        self._models = []
+        self._arr = (Sphere * max(len(spheres), 1))()
+        for q, (cx, cy, cz, r, eps, sig, model) in enumerate(spheres):
+            sp = self._arr[q]
+            sp.cx, sp.cy, sp.cz, sp.radius, sp.eps_r, sp.sigma = cx, cy, cz, r, eps, sig
+            if model is not None:
+                self._models.append(model)
+                sp.model = C.pointer(model)
+        n = len(spheres)
+
+        def cb(grid, mat, ctx):
+            return lib.fdtd_b200_materials_add_spheres(mat, grid, self._arr, n, smoothing)
+
+        self.fn = SETUP_FN(cb)
+        self.ptr = C.cast(self.fn, C.c_void_p)
 
 _lib = None
 
@@ -99,6 +155,7 @@ def load() -> C.CDLL:
         "fdtd_b200_sim_reset": (I, [P]),
         "fdtd_b200_sim_advance": (I, [P, S]),
         "fdtd_b200_sim_synchronize": (I, [P]),
+        "fdtd_b200_sim_advance_timed": (I, [P, S, C.POINTER(D)]),
         "fdtd_b200_sim_steps_done": (S, [P]),
         "fdtd_b200_sim_stream": (P, [P]),
         "fdtd_b200_sim_read_probes": (I, [P, C.POINTER(D)]),
@@ -111,6 +168,9 @@ def load() -> C.CDLL:
         "fdtd_b200_set_default_schedule": (I, [I]),
         "fdtd_b200_version": (C.c_char_p, []),
         "cpml_default_params": (CpmlParams, [S]),
+        "fdtd_b200_materials_add_spheres": (I, [P, P, C.POINTER(Sphere), S, I]),
+        "fdtd_b200_sim_info": (I, [P, C.POINTER(SimInfo)]),
+        "fdtd_b200_sim_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -220,6 +280,13 @@ class Sim:
         if self.lib.fdtd_b200_sim_advance(self.h, n) != 0:
             raise RuntimeError(last_error())
 
+    def advance_timed(self, n: int) -> float:
+        """Advances n steps and returns their GPU time in ms (CUDA events)."""
+        ms = C.c_double(0.0)
+        if self.lib.fdtd_b200_sim_advance_timed(self.h, n, C.byref(ms)) != 0:
+            raise RuntimeError(last_error())
+        return ms.value
+
     def synchronize(self):
         if self.lib.fdtd_b200_sim_synchronize(self.h) != 0:
             raise RuntimeError(last_error())
@@ -231,6 +298,19 @@ class Sim:
     @property
     def launches_per_step(self) -> int:
         return self.lib.fdtd_b200_sim_launches_per_step(self.h)
+
+    def info(self) -> SimInfo:
+        si = SimInfo()
+        if self.lib.fdtd_b200_sim_info(self.h, C.byref(si)) != 0:
+            raise RuntimeError(last_error())
+        return si
+
+    def time_kernels(self, n: int) -> tuple[float, float]:
+        """Runs n steps kernel by kernel; returns (sweep_ms, other_ms)."""
+        a, b = C.c_double(0), C.c_double(0)
+        if self.lib.fdtd_b200_sim_time_kernels(self.h, n, C.byref(a), C.byref(b)) != 0:
+            raise RuntimeError(last_error())
+        return a.value, b.value
 
     def probes(self) -> np.ndarray:
         c = self.rc.c

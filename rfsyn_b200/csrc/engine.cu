@@ -43,8 +43,13 @@ extern "C" unsigned long long rfb_launch_count(void) { return g_launches.load();
 
 static long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
-// Row pitch (elements) of the device layout: rows start on 128-byte lines.
-static long long pitch_for(int nz, size_t esz) { return round_up(nz + 1, (long long)(128 / esz)); }
+// Row pitch (elements) of the device layout: a multiple of 32 elements, so
+// every row starts on a 128-byte line and a 32-wide k tile never runs past
+// the end of its row (also for the one-byte code volume).
+static long long pitch_for(int nz, size_t esz) {
+    (void)esz;
+    return round_up(nz + 1, 32);
+}
 
 // ---------------------------------------------------------------------------
 // CPML on the device: profiles in the run precision, psi over slabs only.
@@ -188,7 +193,9 @@ struct DevScene {
     int *lc_ijk = nullptr;
     uint8_t *l_kind = nullptr;
     void *l_ca = nullptr, *l_cb = nullptr;
-    int *l_tix = nullptr, *l_src = nullptr;
+    int *l_tix = nullptr, *l_src = nullptr, *l_aix = nullptr;
+    void *ade_c = nullptr, *ade_s = nullptr;
+    size_t ade_s_bytes = 0;
     void *t_m11 = nullptr, *t_scale = nullptr, *t_w = nullptr;
     int *t_main = nullptr, *t_nq = nullptr, *t_uv = nullptr, *t_sign = nullptr;
     int n_skip = 0;
@@ -198,7 +205,7 @@ struct DevScene {
 static void devscene_free(DevScene &s) {
     cudaFree(s.codes); cudaFree(s.tca); cudaFree(s.tcb);
     cudaFree(s.lc_ijk); cudaFree(s.l_kind); cudaFree(s.l_ca); cudaFree(s.l_cb);
-    cudaFree(s.l_tix); cudaFree(s.l_src);
+    cudaFree(s.l_tix); cudaFree(s.l_src); cudaFree(s.l_aix); cudaFree(s.ade_c); cudaFree(s.ade_s);
     cudaFree(s.t_m11); cudaFree(s.t_scale); cudaFree(s.t_w);
     cudaFree(s.t_main); cudaFree(s.t_nq); cudaFree(s.t_uv); cudaFree(s.t_sign);
     s = DevScene();
@@ -242,7 +249,8 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
         s.l_cb = dev_upload_conv(img->cb, ne, prec);
         s.l_tix = dev_copy(img->tix, ne);
         s.l_src = dev_copy(img->src, ne);
-        if (!s.lc_ijk || !s.l_kind || !s.l_ca || !s.l_cb || !s.l_tix || !s.l_src) {
+        s.l_aix = dev_copy(img->aix, ne);
+        if (!s.lc_ijk || !s.l_kind || !s.l_ca || !s.l_cb || !s.l_tix || !s.l_src || !s.l_aix) {
             rfb_set_error("interface list upload failed");
             return -1;
         }
@@ -259,6 +267,15 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
                 rfb_set_error("tensor list upload failed");
                 return -1;
             }
+        }
+        if (img->n_ade) {
+            s.ade_c = dev_upload_conv(img->ade_c, img->n_ade * RFB_ADE_NC, prec);
+            s.ade_s_bytes = ne * 5 * (prec == RFB_FP64 ? 8 : 4);
+            if (!s.ade_c || cudaMalloc(&s.ade_s, s.ade_s_bytes) != cudaSuccess) {
+                rfb_set_error("dispersive state allocation failed");
+                return -1;
+            }
+            cudaMemset(s.ade_s, 0, s.ade_s_bytes);
         }
         if (!s.codes) {
             if (s.n_cells <= MAX_SKIP) {
@@ -292,6 +309,9 @@ static void fill_scene_args(Args<T> &a, const DevScene &s) {
     a.l_cb = (const T *)s.l_cb;
     a.l_tix = s.l_tix;
     a.l_src = s.l_src;
+    a.l_aix = s.l_aix;
+    a.ade_c = (const T *)s.ade_c;
+    a.ade_s = (T *)s.ade_s;
     a.t_m11 = (const T *)s.t_m11;
     a.t_scale = (const T *)s.t_scale;
     a.t_w = (const T *)s.t_w;
@@ -341,6 +361,7 @@ struct rfb_engine {
     cudaGraphExec_t g1[2] = {nullptr, nullptr}, gk[2] = {nullptr, nullptr};
     int launches_per_step = 0;
     FusedPlan plan;
+    size_t h2d_bytes = 0, n_ade = 0;
 };
 
 template <typename T>
@@ -452,7 +473,17 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
                 (sources[s].k == geom->nz && !(geom->periodic & 4u)))
                 active = 1;
         }
-        if (fused_plan_default(&e->plan, geom, active) != 0) {
+        if (fused_prepare() != 0) {
+            rfb_set_error("cannot configure the fused kernel's shared memory");
+            delete e;
+            return nullptr;
+        }
+        int rc = fused_plan_default(&e->plan, geom, active);
+        const char *ov = getenv("RFSYN_FDTD_PLAN");  // "tj,seg_len": manual tile plan
+        int tj = 0, seg = 0;
+        if (rc == 0 && ov && sscanf(ov, "%d,%d", &tj, &seg) == 2 && (tj == 8 || tj == 16))
+            rc = fused_plan_dims(&e->plan, geom, active, tj, seg);
+        if (rc != 0) {
             rfb_set_error("grid too large for the fused schedule");
             delete e;
             return nullptr;
@@ -501,6 +532,17 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
     CK(cudaMemset(e->d_step, 0, sizeof(int)));
     CK(cudaDeviceSynchronize());
     e->launches_per_step = count_step_launches(e);
+    if (scene) {
+        const size_t ne = 3 * scene->n_cells;
+        e->h2d_bytes += (scene->codes ? (size_t)(geom->nx + 1) * (geom->ny + 1) * (geom->nz + 1) : 0) +
+                        2 * 256 * e->esz + 3 * scene->n_cells * 4 + ne * (1 + 2 * e->esz + 3 * 4) +
+                        scene->n_tensors * (6 * e->esz + 25 * 4) + scene->n_ade * RFB_ADE_NC * e->esz;
+        for (size_t q = 0; q < ne; q++)
+            if (scene->kind[q] == RFB_LK_ADE) e->n_ade++;
+    }
+    e->h2d_bytes += n_sources * n_steps * e->esz + n_probes * 12;
+    if (cpml)
+        e->h2d_bytes += 6 * e->esz * ((size_t)geom->nx + geom->ny + geom->nz + 3);
     return e;
 fail:
 fail_noset:
@@ -516,6 +558,7 @@ extern "C" int rfb_engine_reset(rfb_engine_t *e) {
         for (int b = 0; b < 2; b++)
             if (e->cpml.psi_h[b][p]) CK(cudaMemsetAsync(e->cpml.psi_h[b][p], 0, e->cpml.psi_h_bytes[p], e->stream));
     }
+    if (e->scene.ade_s) CK(cudaMemsetAsync(e->scene.ade_s, 0, e->scene.ade_s_bytes, e->stream));
     CK(cudaMemsetAsync(e->d_step, 0, sizeof(int), e->stream));
     e->steps_done = 0;
     e->parity = 0;
@@ -572,6 +615,91 @@ out:
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
     return rc;
+}
+
+extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
+    out->list_cells = (size_t)e->scene.n_cells;
+    out->dispersive = e->n_ade;
+    out->h2d_bytes = e->h2d_bytes;
+    out->tile_j = e->plan.tj;
+    out->seg_len = e->plan.d.seg_len;
+    size_t sca = 0;
+    if (e->cpml.on) {
+        // cells of the swept volume inside the slab of each axis (H profiles)
+        const int n[3] = {e->g.nx, e->g.ny, e->g.nz};
+        for (int a = 0; a < 3; a++) {
+            const size_t others = (size_t)e->g.nx * e->g.ny * e->g.nz / (size_t)n[a];
+            sca += (size_t)e->cpml.eh[a].ns * others;
+        }
+    }
+    out->slab_cell_axes = sca;
+    return 0;
+}
+
+// Launches the step kernels one by one with events around each, outside any
+// graph, to attribute GPU time to the sweep and to the list / probe kernels.
+template <typename T>
+static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *other_ms) {
+    cudaEvent_t ev[4] = {};
+    double sw = 0.0, ot = 0.0;
+    int rc = -1;
+    for (int q = 0; q < 4; q++) CK(cudaEventCreate(&ev[q]));
+    for (size_t s = 0; s < n; s++) {
+        const int par = e->nbuf == 2 ? e->parity : 0;
+        Args<T> a = engine_args<T>(e, par);
+        const rfb_geom_t &g = e->g;
+        CK(cudaEventRecord(ev[0], e->stream));
+        if (e->sched == RFB_SCHED_FUSED) {
+            launch_fused<T>(a, e->plan, e->stream);
+            g_launches++;
+        } else {
+            dim3 blk(32, 8), grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
+            k_h_split<T><<<grd, blk, 0, e->stream>>>(a);
+            k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
+            g_launches += 2;
+        }
+        CK(cudaEventRecord(ev[1], e->stream));
+        if (a.n_cells) {
+            k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
+            g_launches++;
+        }
+        ProbeArgs<T> p;
+        p.n = e->n_probes;
+        p.cell = e->probe_cell;
+        p.comp = e->probe_comp;
+        const int out = e->nbuf == 2 ? 1 - par : 0;
+        for (int c = 0; c < 6; c++) p.F[c] = (const T *)e->fld[out][c];
+        p.ts = (T *)e->ts;
+        p.n_steps = (long long)e->n_steps;
+        p.d_step = e->d_step;
+        k_probe_gather<T><<<1, 128, 0, e->stream>>>(p);
+        g_launches++;
+        CK(cudaEventRecord(ev[2], e->stream));
+        CK(cudaEventSynchronize(ev[2]));
+        float t1 = 0.f, t2 = 0.f;
+        CK(cudaEventElapsedTime(&t1, ev[0], ev[1]));
+        CK(cudaEventElapsedTime(&t2, ev[1], ev[2]));
+        sw += t1;
+        ot += t2;
+        e->steps_done++;
+        if (e->nbuf == 2) e->parity ^= 1;
+    }
+    *sweep_ms = sw;
+    *other_ms = ot;
+    rc = 0;
+fail:
+    for (int q = 0; q < 4; q++)
+        if (ev[q]) cudaEventDestroy(ev[q]);
+    return rc;
+}
+
+extern "C" int rfb_engine_time_kernels(rfb_engine_t *e, size_t n, double *sweep_ms, double *other_ms) {
+    if (e->steps_done + n > e->n_steps) {
+        rfb_set_error("time_kernels past the configured step count");
+        return -1;
+    }
+    return e->prec == RFB_FP64 ? time_kernels_t<double>(e, n, sweep_ms, other_ms)
+                               : time_kernels_t<float>(e, n, sweep_ms, other_ms);
 }
 
 extern "C" int rfb_engine_sync(rfb_engine_t *e) {
@@ -654,6 +782,81 @@ extern "C" int rfb_engine_read_field(rfb_engine_t *e, int component, double *hos
     return 0;
 fail:
     return -1;
+}
+
+// ---------------------------------------------------------------------------
+// Sphere fill fractions (FP64 subpixel construction on the GPU)
+// ---------------------------------------------------------------------------
+// Unit cube around the sample: exact 0 / 1 when the half diagonal sqrt(3)/2
+// clears the surface, else the share of an 8^3 lattice of points at offsets
+// (a + 1/2)/8 - 1/2 whose squared distance is <= r^2.
+__global__ void k_sphere_fractions(double cx, double cy, double cz, double r, int i0, int j0, int k0, int ni, int nj,
+                                   int nk, double *f, double *n2) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ncell = (long long)ni * nj * nk;
+    if (t >= 3 * ncell) return;
+    const long long cell = t / 3;
+    const int comp = (int)(t - 3 * cell);
+    const int k = k0 + (int)(cell % nk);
+    const int j = j0 + (int)((cell / nk) % nj);
+    const int i = i0 + (int)(cell / ((long long)nk * nj));
+    const double x = __dadd_rn((double)i, comp == 0 ? 0.5 : 0.0);
+    const double y = __dadd_rn((double)j, comp == 1 ? 0.5 : 0.0);
+    const double z = __dadd_rn((double)k, comp == 2 ? 0.5 : 0.0);
+    const double dx = __dsub_rn(x, cx), dy = __dsub_rn(y, cy), dz = __dsub_rn(z, cz);
+    const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    const double cc = comp == 0 ? dx : comp == 1 ? dy : dz;
+    double nn = 0.0;
+    if (d > 0.0) {
+        const double u = __ddiv_rn(cc, d);
+        nn = __dmul_rn(u, u);
+    }
+    const double h = 0.8660254037844386;
+    double frac;
+    if (__dadd_rn(d, h) <= r) {
+        frac = 1.0;
+    } else if (__dsub_rn(d, h) >= r) {
+        frac = 0.0;
+    } else {
+        const double r2 = __dmul_rn(r, r);
+        int count = 0;
+        for (int a = 0; a < 8; a++) {
+            const double px = __dsub_rn(__dadd_rn(x, __dsub_rn(__ddiv_rn(__dadd_rn((double)a, 0.5), 8.0), 0.5)), cx);
+            for (int b = 0; b < 8; b++) {
+                const double py = __dsub_rn(__dadd_rn(y, __dsub_rn(__ddiv_rn(__dadd_rn((double)b, 0.5), 8.0), 0.5)), cy);
+                for (int e = 0; e < 8; e++) {
+                    const double pz =
+                        __dsub_rn(__dadd_rn(z, __dsub_rn(__ddiv_rn(__dadd_rn((double)e, 0.5), 8.0), 0.5)), cz);
+                    const double q = __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz));
+                    count += q <= r2;
+                }
+            }
+        }
+        frac = __ddiv_rn((double)count, 512.0);
+    }
+    f[t] = frac;
+    n2[t] = nn;
+}
+
+extern "C" int rfb_sphere_fractions(const double centre[3], double radius, int i0, int j0, int k0, int ni, int nj,
+                                    int nk, double *f, double *n2) {
+    const size_t n = 3 * (size_t)ni * nj * nk;
+    double *df = nullptr, *dn = nullptr;
+    int rc = -1;
+    if (!n) return 0;
+    CK(cudaMalloc(&df, n * 8));
+    CK(cudaMalloc(&dn, n * 8));
+    k_sphere_fractions<<<(unsigned)((n + 255) / 256), 256>>>(centre[0], centre[1], centre[2], radius, i0, j0, k0, ni,
+                                                             nj, nk, df, dn);
+    g_launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(f, df, n * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(n2, dn, n * 8, cudaMemcpyDeviceToHost));
+    rc = 0;
+fail:
+    cudaFree(df);
+    cudaFree(dn);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

@@ -131,6 +131,12 @@ void *rfb_engine_stream(rfb_engine_t *e);
 size_t rfb_engine_steps_done(rfb_engine_t *e);
 /* Kernel launches per time step (for launch accounting). */
 int rfb_engine_launches_per_step(rfb_engine_t *e);
+typedef struct {
+    size_t list_cells, dispersive, slab_cell_axes, h2d_bytes;
+    int tile_j, seg_len;
+} rfb_engine_info_t;
+int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out);
+int rfb_engine_time_kernels(rfb_engine_t *e, size_t n, double *sweep_ms, double *other_ms);
 /* Download one field component (0..5) into a host array in rfsyn layout. */
 int rfb_engine_read_field(rfb_engine_t *e, int component, double *host);
 
@@ -158,6 +164,14 @@ int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *c
  * (validate_long_term_stability.c:166-209). */
 int rfb_step_energy(rfb_fields_t *f, const rfb_geom_t *geom, rfb_scene_dev_t *scene,
                     double vacuum_cb, double *const host[6], double *out_energy);
+
+/* Fill fractions of a sphere (centre / radius in cell units) for the three E
+ * samples of every cell of the box [i0, i0+ni) x [j0, j0+nj) x [k0, k0+nk):
+ * f[3*cell + c] and the squared normal component n2[3*cell + c] along the
+ * sample's own axis; cell = ((i-i0)*nj + (j-j0))*nk + (k-k0).  FP64 on the
+ * GPU, every operation rounded separately (bit-identical to the oracle). */
+int rfb_sphere_fractions(const double centre[3], double radius, int i0, int j0, int k0, int ni, int nj, int nk,
+                         double *f, double *n2);
 
 /* Last error message of the calling thread ("" if none). */
 const char *rfb_last_error(void);

@@ -48,7 +48,10 @@ typedef struct {
     int32_t *tix, *src, *aix;
     double *t_m11, *t_scale, *t_w;
     int32_t *t_main, *t_nq, *t_uv, *t_sign;
+    double *ade_c;
 } rfb_scene_build_t;
+
+void rfb_ade_record(const double *model, double dt, double dx, double *out);
 
 typedef struct {
     int i, j, k;

@@ -15,6 +15,9 @@
 #include "host.h"
 
 #define MATERIAL_LIMIT 256
+/* dispersive model packed as doubles: eps_inf, sigma, n_poles, then per pole
+ * kind, delta_eps, tau, omega_p, gamma */
+#define DISP_W 13
 
 typedef struct {
     double eps_r, sigma;
@@ -145,6 +148,7 @@ struct materials {
     size_t table_count;
     omap_t scalar;  /* key -> (Ca, Cb) */
     omap_t tensor;  /* key -> (m11, m12, m22, scale) */
+    omap_t disp;    /* key -> dispersive model (DISP_W doubles) */
     unsigned long version;
     /* device copy for the step-wise API */
     rfb_scene_dev_t *dev;
@@ -211,6 +215,7 @@ materials_t *materials_create(const fdtd_grid_t *g) {
     mat->dt = g->dt;
     omap_init(&mat->scalar, 2);
     omap_init(&mat->tensor, 4);
+    omap_init(&mat->disp, DISP_W);
     mat->ids = calloc(total, 1);
     if (!mat->ids) {
         materials_destroy(mat);
@@ -229,6 +234,7 @@ void materials_destroy(materials_t *mat) {
     free(mat->ids);
     omap_free(&mat->scalar);
     omap_free(&mat->tensor);
+    omap_free(&mat->disp);
     rfb_scene_dev_destroy(mat->dev);
     free(mat);
 }
@@ -305,6 +311,7 @@ int materials_assign_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size
         }
     clear_box_overrides(mat, &mat->scalar, i0, i1, j0, j1, k0, k1);
     clear_box_overrides(mat, &mat->tensor, i0, i1, j0, j1, k0, k1);
+    clear_box_overrides(mat, &mat->disp, i0, i1, j0, j1, k0, k1);
     mat->version++;
     return 0;
 }
@@ -412,6 +419,206 @@ int materials_get_tensor(const materials_t *mat, const fdtd_grid_t *g, field_com
     return 0;
 }
 
+/* ---- dispersive samples ------------------------------------------------------ */
+static int pack_model(const fdtd_b200_dispersive_t *m, double *v) {
+    if (!m || !isfinite(m->eps_inf) || m->eps_inf < 1.0 || !isfinite(m->sigma) || m->sigma < 0.0 || m->n_poles < 1 ||
+        m->n_poles > FDTD_B200_MAX_POLES)
+        return -1;
+    memset(v, 0, DISP_W * sizeof(double));
+    v[0] = m->eps_inf;
+    v[1] = m->sigma;
+    v[2] = (double)m->n_poles;
+    for (int p = 0; p < m->n_poles; p++) {
+        double *w = v + 3 + 5 * p;
+        if (!isfinite(m->delta_eps[p]) || m->delta_eps[p] <= 0.0) return -1;
+        if (m->kind[p] == FDTD_B200_POLE_DEBYE) {
+            if (!isfinite(m->tau[p]) || m->tau[p] <= 0.0) return -1;
+        } else if (m->kind[p] == FDTD_B200_POLE_LORENTZ) {
+            if (!isfinite(m->omega_p[p]) || m->omega_p[p] <= 0.0 || !isfinite(m->gamma[p]) || m->gamma[p] < 0.0)
+                return -1;
+        } else {
+            return -1;
+        }
+        w[0] = (double)m->kind[p];
+        w[1] = m->delta_eps[p];
+        w[2] = m->tau[p];
+        w[3] = m->omega_p[p];
+        w[4] = m->gamma[p];
+    }
+    return 0;
+}
+
+int fdtd_b200_materials_set_component_dispersive(materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                                 size_t i, size_t j, size_t k, const fdtd_b200_dispersive_t *model) {
+    int c = component_number(component);
+    double v[DISP_W];
+    if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k) || pack_model(model, v) != 0) return -1;
+    if (omap_put(&mat->disp, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, v) != 0) return -1;
+    mat->version++;
+    return 0;
+}
+
+int fdtd_b200_materials_clear_component_dispersive(materials_t *mat, const fdtd_grid_t *g,
+                                                   field_component_t component, size_t i, size_t j, size_t k) {
+    int c = component_number(component);
+    if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    omap_del(&mat->disp, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
+    mat->version++;
+    return 0;
+}
+
+/* ADE update record of a dispersive sample (RFB_ADE_NC doubles):
+ *   [0] ca  [1] cb  [2] ce  [3] n_poles, then per pole
+ *   kind, cj, cjm, aJ, aJm, aE
+ * for  E+ = ca E + cb (dA - dB) + ce E- - sum_p (cj J_p + cjm J_p-)
+ *      J_p+ = aJ J_p + aJm J_p- + aE (E+ - E_ref),  E_ref = E (Debye) or E- (Lorentz)
+ * where - / + denote the previous / next time level.  Derivation: Ampere's
+ * law at n+1/2 with the centred Debye update J+ = k J + beta (E+ - E)/dt and
+ * the centred Lorentz update J+ = a J + xi J- + g (E+ - E-)/(2 dt) (Taflove &
+ * Hagness 3rd ed. sec. 9.4). */
+void rfb_ade_record(const double *m, double dt, double dx, double *out) {
+    const double e0ei = EPS0 * m[0], sigma = m[1];
+    const int np = (int)m[2];
+    double kJ[FDTD_B200_MAX_POLES], kJm[FDTD_B200_MAX_POLES], kE[FDTD_B200_MAX_POLES];
+    double half_beta = 0.0, quarter_g = 0.0;
+    for (int p = 0; p < np; p++) {
+        const double *w = m + 3 + 5 * p;
+        if ((int)w[0] == FDTD_B200_POLE_DEBYE) {
+            double den = 1.0 + dt / (2.0 * w[2]);
+            double beta = (EPS0 * w[1] * dt / w[2]) / den;
+            kJ[p] = (1.0 - dt / (2.0 * w[2])) / den;
+            kJm[p] = 0.0;
+            kE[p] = beta / dt;
+            half_beta += 0.5 * beta;
+        } else {
+            double den = 1.0 + w[4] * dt;
+            double g = EPS0 * w[1] * w[3] * w[3] * dt * dt / den;
+            kJ[p] = (2.0 - w[3] * w[3] * dt * dt) / den;
+            kJm[p] = (w[4] * dt - 1.0) / den;
+            kE[p] = g / (2.0 * dt);
+            quarter_g += 0.25 * g;
+        }
+    }
+    const double A = e0ei + 0.5 * sigma * dt + half_beta + quarter_g;
+    memset(out, 0, RFB_ADE_NC * sizeof(double));
+    out[0] = (e0ei - 0.5 * sigma * dt + half_beta) / A;
+    out[1] = dt / (A * dx);
+    out[2] = quarter_g / A;
+    out[3] = (double)np;
+    for (int p = 0; p < np; p++) {
+        double *r = out + 4 + 6 * p;
+        r[0] = m[3 + 5 * p];
+        r[1] = 0.5 * dt * (1.0 + kJ[p]) / A;
+        r[2] = 0.5 * dt * kJm[p] / A;
+        r[3] = kJ[p];
+        r[4] = kJm[p];
+        r[5] = kE[p];
+    }
+}
+
+/* ---- spheres ------------------------------------------------------------------ */
+static int sample_valid(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k) {
+    return component_valid(g, c, i, j, k);
+}
+
+int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_sphere_t *spheres,
+                                    size_t n_spheres, int smoothing) {
+    if (!materials_matches(mat, g) || (!spheres && n_spheres)) return -1;
+    const size_t n[3] = {g->nx, g->ny, g->nz};
+    for (size_t q = 0; q < n_spheres; q++) {
+        const fdtd_b200_sphere_t *sp = &spheres[q];
+        if (!isfinite(sp->cx) || !isfinite(sp->cy) || !isfinite(sp->cz) || !isfinite(sp->radius) || sp->radius <= 0.0)
+            return -1;
+        double dmodel[DISP_W];
+        material_id_t sid = 0;
+        if (sp->model) {
+            if (pack_model(sp->model, dmodel) != 0) return -1;
+        } else if (materials_register(mat, sp->eps_r, sp->sigma, &sid) != 0) {
+            return -1;
+        }
+        const double cen[3] = {sp->cx, sp->cy, sp->cz};
+        long lo[3], hi[3];
+        for (int a = 0; a < 3; a++) {
+            lo[a] = (long)floor(cen[a] - sp->radius) - 2;
+            hi[a] = (long)ceil(cen[a] + sp->radius) + 2;
+            if (lo[a] < 0) lo[a] = 0;
+            if (hi[a] > (long)n[a]) hi[a] = (long)n[a];
+        }
+        if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
+        const int ni = (int)(hi[0] - lo[0] + 1), nj = (int)(hi[1] - lo[1] + 1), nk = (int)(hi[2] - lo[2] + 1);
+        const size_t ncell = (size_t)ni * nj * nk;
+        double *f = malloc(3 * ncell * sizeof(double)), *n2 = malloc(3 * ncell * sizeof(double));
+        if (!f || !n2 || rfb_sphere_fractions(cen, sp->radius, (int)lo[0], (int)lo[1], (int)lo[2], ni, nj, nk, f, n2)) {
+            free(f);
+            free(n2);
+            return -1;
+        }
+        for (int di = 0; di < ni; di++)
+            for (int dj = 0; dj < nj; dj++)
+                for (int dk = 0; dk < nk; dk++) {
+                    const size_t i = (size_t)(lo[0] + di), j = (size_t)(lo[1] + dj), k = (size_t)(lo[2] + dk);
+                    const size_t cell = ((size_t)di * nj + (size_t)dj) * nk + (size_t)dk;
+                    const double *fc = f + 3 * cell, *nc = n2 + 3 * cell;
+                    int valid[3];
+                    for (int c = 0; c < 3; c++) valid[c] = sample_valid(g, c, i, j, k);
+                    const size_t w = fdtd_index(g, i, j, k);
+                    if (fc[0] == 1.0 && fc[1] == 1.0 && fc[2] == 1.0 && valid[0] && valid[1] && valid[2]) {
+                        for (int c = 0; c < 3; c++) {
+                            omap_del(&mat->scalar, (uint64_t)w * 3 + (uint64_t)c);
+                            omap_del(&mat->disp, (uint64_t)w * 3 + (uint64_t)c);
+                        }
+                        for (int c = 0; c < 2; c++) omap_del(&mat->tensor, (uint64_t)w * 3 + (uint64_t)c);
+                        if (sp->model) {
+                            for (int c = 0; c < 3; c++)
+                                if (omap_put(&mat->disp, (uint64_t)w * 3 + (uint64_t)c, dmodel) != 0) goto oom;
+                        } else {
+                            mat->ids[w] = sid;
+                        }
+                        continue;
+                    }
+                    for (int c = 0; c < 3; c++) {
+                        if (!valid[c] || fc[c] <= 0.0) continue;
+                        const uint64_t key = (uint64_t)w * 3 + (uint64_t)c;
+                        if (sp->model) {
+                            if (fc[c] >= 0.5 && omap_put(&mat->disp, key, dmodel) != 0) goto oom;
+                            continue;
+                        }
+                        double eps_c, sig_c;
+                        if (!smoothing || fc[c] == 1.0) {
+                            if (fc[c] < 0.5) continue;
+                            eps_c = sp->eps_r;
+                            sig_c = sp->sigma;
+                        } else {
+                            /* diagonal of the smoothed inverse permittivity */
+                            const double eb = mat->table[mat->ids[w]].eps_r, sb = mat->table[mat->ids[w]].sigma;
+                            const double mean = fc[c] * sp->eps_r + (1.0 - fc[c]) * eb;
+                            const double minv = fc[c] / sp->eps_r + (1.0 - fc[c]) / eb;
+                            const double inv = nc[c] * minv + (1.0 - nc[c]) / mean;
+                            eps_c = 1.0 / inv;
+                            sig_c = fc[c] * sp->sigma + (1.0 - fc[c]) * sb;
+                        }
+                        material_coeff_t co;
+                        if (make_coeff(mat, eps_c, sig_c, &co) != 0) goto fail;
+                        double v[2] = {co.Ca, co.Cb};
+                        if (omap_put(&mat->scalar, key, v) != 0) goto oom;
+                        omap_del(&mat->disp, key);
+                    }
+                }
+        free(f);
+        free(n2);
+        mat->version++;
+        continue;
+    oom:
+        rfb_set_error("out of host memory rasterising spheres");
+    fail:
+        free(f);
+        free(n2);
+        mat->version++;
+        return -1;
+    }
+    return 0;
+}
+
 /* Symmetric Ex/Ey coupling weight of two tensor edges (materials.c:836-845):
  * 0.25 * rho * sqrt(m11_x) * sqrt(m11_y) with rho the mean normalised
  * off-diagonal correlation; evaluated in the same order for bit parity. */
@@ -447,6 +654,7 @@ void rfb_scene_build_free(rfb_scene_build_t *b) {
     free(b->codes); free(b->cell_ijk); free(b->kind); free(b->ca); free(b->cb);
     free(b->tix); free(b->src); free(b->aix);
     free(b->t_m11); free(b->t_scale); free(b->t_w); free(b->t_main); free(b->t_nq); free(b->t_uv); free(b->t_sign);
+    free(b->ade_c);
     memset(b, 0, sizeof(*b));
 }
 
@@ -459,7 +667,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     }
     const size_t nz1 = g->nz + 1;
     /* 1. cells on the interface list (padded linear index) */
-    size_t cap = mat->scalar.count + mat->tensor.count + n_extra;
+    size_t cap = mat->scalar.count + mat->tensor.count + mat->disp.count + n_extra;
     int id255 = 0;
     if (mat->table_count == MATERIAL_LIMIT) {
         /* code 255 marks list cells: cells of material 255 go to the list too */
@@ -473,6 +681,8 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         if (mat->scalar.keys[q] != OMAP_EMPTY) cells[nc++] = mat->scalar.keys[q] / 3;
     for (size_t q = 0; q < mat->tensor.cap; q++)
         if (mat->tensor.keys[q] != OMAP_EMPTY) cells[nc++] = mat->tensor.keys[q] / 3;
+    for (size_t q = 0; q < mat->disp.cap; q++)
+        if (mat->disp.keys[q] != OMAP_EMPTY) cells[nc++] = mat->disp.keys[q] / 3;
     for (size_t q = 0; q < n_extra; q++)
         cells[nc++] = ((uint64_t)extra[q].i * (g->ny + 1) + (uint64_t)extra[q].j) * nz1 + (uint64_t)extra[q].k;
     if (id255)
@@ -523,6 +733,15 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign)
         goto oom;
     size_t nt = 0;
+    /* ADE records, deduplicated by model */
+    size_t n_models = 0, model_cap = 16;
+    double *models = malloc(model_cap * DISP_W * sizeof(double));
+    double *records = malloc(model_cap * RFB_ADE_NC * sizeof(double));
+    out->ade_c = records; /* owned by the image from here on */
+    if (!models || !records) {
+        free(models);
+        goto oom;
+    }
     for (size_t q = 0; q < nc; q++) {
         size_t idx = (size_t)cells[q];
         size_t k = idx % nz1, row = idx / nz1, j = row % (g->ny + 1), i = row / (g->ny + 1);
@@ -543,7 +762,32 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
             }
             const double *t = (c < 2) ? tensor_at(mat, idx, c) : NULL;
             if (!t) {
-                out->kind[e] = RFB_LK_SCALAR;
+                long long dm = omap_find(&mat->disp, (uint64_t)idx * 3 + (uint64_t)c);
+                if (dm < 0) {
+                    out->kind[e] = RFB_LK_SCALAR;
+                    continue;
+                }
+                const double *mv = mat->disp.vals + (size_t)dm * DISP_W;
+                size_t r = 0;
+                while (r < n_models && memcmp(models + r * DISP_W, mv, DISP_W * sizeof(double)) != 0) r++;
+                if (r == n_models) {
+                    if (n_models == model_cap) {
+                        model_cap *= 2;
+                        double *nm = realloc(models, model_cap * DISP_W * sizeof(double));
+                        if (nm) models = nm;
+                        double *nr = realloc(records, model_cap * RFB_ADE_NC * sizeof(double));
+                        if (nr) records = out->ade_c = nr;
+                        if (!nm || !nr) {
+                            free(models);
+                            goto oom;
+                        }
+                    }
+                    memcpy(models + r * DISP_W, mv, DISP_W * sizeof(double));
+                    rfb_ade_record(mv, mat->dt, mat->dx, records + r * RFB_ADE_NC);
+                    n_models++;
+                }
+                out->kind[e] = RFB_LK_ADE;
+                out->aix[e] = (int32_t)r;
                 continue;
             }
             /* tensor edge record (materials.c:847-903) */
@@ -596,6 +840,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         size_t e = 3 * (size_t)(hit - cells) + (size_t)extra[q].component;
         if (out->src[e] >= 0) {
             rfb_set_error("two sources on the same field sample");
+            free(models);
             free(cells);
             rfb_scene_build_free(out);
             return -1;
@@ -603,6 +848,9 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         out->src[e] = extra[q].slot;
     }
     free(cells);
+    free(models);
+    img->n_ade = n_models;
+    img->ade_c = records;
     img->n_cells = nc;
     img->cell_ijk = out->cell_ijk;
     img->kind = out->kind;

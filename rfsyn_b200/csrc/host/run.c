@@ -71,6 +71,7 @@ struct fdtd_b200_sim {
     double *freqs;
     double dft_offset;
     size_t nx, ny, nz;
+    int precision, schedule;
 };
 
 static double wave_value(const fdtd_b200_source_t *s, double t, size_t n) {
@@ -186,6 +187,8 @@ fdtd_b200_sim_t *fdtd_b200_sim_create(const fdtd_b200_config_t *cfg, fdtd_materi
     sim->dt = g.dt;
     sim->nx = g.nx; sim->ny = g.ny; sim->nz = g.nz;
     sim->dft_offset = cfg->dft_time_offset_steps;
+    sim->precision = cfg->precision;
+    sim->schedule = cfg->schedule;
     sim->n_freqs = cfg->n_freqs;
     if (cfg->n_freqs) {
         if (!cfg->freqs_hz) { rfb_set_error("n_freqs without freqs_hz"); goto fail; }
@@ -226,11 +229,35 @@ void fdtd_b200_sim_destroy(fdtd_b200_sim_t *sim) {
 
 int fdtd_b200_sim_reset(fdtd_b200_sim_t *sim) { return sim ? rfb_engine_reset(sim->eng) : -1; }
 int fdtd_b200_sim_advance(fdtd_b200_sim_t *sim, size_t n) { return sim ? rfb_engine_advance(sim->eng, n) : -1; }
+int fdtd_b200_sim_advance_timed(fdtd_b200_sim_t *sim, size_t n, double *ms) {
+    return sim ? rfb_engine_advance_timed(sim->eng, n, ms) : -1;
+}
 int fdtd_b200_sim_synchronize(fdtd_b200_sim_t *sim) { return sim ? rfb_engine_sync(sim->eng) : -1; }
 size_t fdtd_b200_sim_steps_done(const fdtd_b200_sim_t *sim) { return sim ? rfb_engine_steps_done(sim->eng) : 0; }
 void *fdtd_b200_sim_stream(const fdtd_b200_sim_t *sim) { return sim ? rfb_engine_stream(sim->eng) : NULL; }
 int fdtd_b200_sim_launches_per_step(const fdtd_b200_sim_t *sim) {
     return sim ? rfb_engine_launches_per_step(sim->eng) : 0;
+}
+
+int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info) {
+    if (!sim || !info) return -1;
+    rfb_engine_info_t ei;
+    if (rfb_engine_info(sim->eng, &ei) != 0) return -1;
+    info->cells = sim->nx * sim->ny * sim->nz;
+    info->list_cells = ei.list_cells;
+    info->dispersive = ei.dispersive;
+    info->slab_cell_axes = ei.slab_cell_axes;
+    info->h2d_bytes = ei.h2d_bytes;
+    info->precision = sim->precision;
+    info->schedule = sim->schedule;
+    info->tile_j = ei.tile_j;
+    info->seg_len = ei.seg_len;
+    return 0;
+}
+
+int fdtd_b200_sim_time_kernels(fdtd_b200_sim_t *sim, size_t n, double *sweep_ms, double *other_ms) {
+    if (!sim || !sweep_ms || !other_ms) return -1;
+    return rfb_engine_time_kernels(sim->eng, n, sweep_ms, other_ms);
 }
 
 int fdtd_b200_sim_read_probes(fdtd_b200_sim_t *sim, double *probe_td) {

@@ -51,7 +51,9 @@ struct Args {
     const int *lc_ijk;
     const uint8_t *l_kind;
     const T *l_ca, *l_cb;
-    const int *l_tix, *l_src;
+    const int *l_tix, *l_src, *l_aix;
+    const T *ade_c;          // RFB_ADE_NC coefficients per dispersive model
+    T *ade_s;                // 5 state values per list entry: J0 J1 J0- J1- E-
     const T *t_m11, *t_scale, *t_w;
     const int *t_main, *t_nq, *t_uv, *t_sign;
     // sources
@@ -211,6 +213,49 @@ __global__ void __launch_bounds__(256) k_e_split(Args<T> a) {
     }
 }
 
+// Dispersive E update (record layout of rfb_ade_record):
+//   E+ = ca E + cb (dA - dB) + ce E- - sum_p (cj J_p + cjm J_p-)
+//   J_p+ = aJ J_p + aJm J_p- + aE (E+ - E_ref), E_ref = E (Debye), E- (Lorentz)
+template <typename T>
+__device__ __forceinline__ T e_ade(const Args<T> &a, int e, int comp, int i, int j, int k, T v) {
+    const T *r = a.ade_c + 16 * a.l_aix[e];
+    T *st = a.ade_s + 5 * (long long)e;
+    // curl with CPML where present: reuse the scalar update with (1, 1)
+    // coefficients would change rounding, so form the stretched difference here
+    const long long c = cidx(a, i, j, k);
+    const int im = i == 0 ? a.nx - 1 : i - 1;
+    const int jm = j == 0 ? a.ny - 1 : j - 1;
+    const int km = k == 0 ? a.nz - 1 : k - 1;
+    T tA, tB;
+    if (comp == 0) {
+        tA = e_term(a, 0, 1, j, xs(a.Ho[2][c], a.Ho[2][cidx(a, i, jm, k)]), i, j, k);
+        tB = e_term(a, 1, 2, k, xs(a.Ho[1][c], a.Ho[1][cidx(a, i, j, km)]), i, j, k);
+    } else if (comp == 1) {
+        tA = e_term(a, 2, 2, k, xs(a.Ho[0][c], a.Ho[0][cidx(a, i, j, km)]), i, j, k);
+        tB = e_term(a, 3, 0, i, xs(a.Ho[2][c], a.Ho[2][cidx(a, im, j, k)]), i, j, k);
+    } else {
+        tA = e_term(a, 4, 0, i, xs(a.Ho[1][c], a.Ho[1][cidx(a, im, j, k)]), i, j, k);
+        tB = e_term(a, 5, 1, j, xs(a.Ho[0][c], a.Ho[0][cidx(a, i, jm, k)]), i, j, k);
+    }
+    const T em = st[4];
+    T en = xa(xm(r[0], v), xm(r[1], xs(tA, tB)));
+    en = xa(en, xm(r[2], em));
+    const int np = (int)r[3];
+    for (int p = 0; p < np; p++) {
+        const T *w = r + 4 + 6 * p;
+        en = xs(en, xa(xm(w[1], st[p]), xm(w[2], st[2 + p])));
+    }
+    for (int p = 0; p < np; p++) {
+        const T *w = r + 4 + 6 * p;
+        const T eref = (w[0] != T(0)) ? em : v;
+        const T jn = xa(xa(xm(w[3], st[p]), xm(w[4], st[2 + p])), xm(w[5], xs(en, eref)));
+        st[2 + p] = st[p];
+        st[p] = jn;
+    }
+    st[4] = v;
+    return en;
+}
+
 // ---- interface list: overrides, tensor edges, sources --------------------
 // One thread per (cell, component) entry.  Reads E from the input buffers,
 // H from the output buffers (already advanced), writes E output.
@@ -246,6 +291,9 @@ __global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
             value = xa(value, xm(a.t_w[4 * t + q], d));
         }
         v = xa(v, xm(a.t_scale[t], value));
+    } else if (kind == 3) {
+        // dispersive sample: polarisation-current ADE (Debye / Lorentz poles)
+        v = e_ade(a, e, comp, i, j, k, v);
     }
     a.Eo[comp][c] = v;
 }

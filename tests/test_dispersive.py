@@ -1,0 +1,111 @@
+"""Dispersive (ADE) samples and smoothed spheres: features with no rfsyn
+counterpart.  The CPU oracle restates them (oracle/fdtd_oracle.c) and is
+pinned by physics: the static limit (delta_eps -> 0 reproduces a plain
+eps_inf medium), and the sphere fill fractions' volume partition.  The GPU
+paths are held bit-for-bit to the oracle in FP64."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import rfsyn_b200 as rb
+from oracle import MODEL_ONLY, Scene, disp_entry
+from tests.cases import run_device
+
+DT = Scene(nx=1, ny=1, nz=1).dt
+BASE = dict(nx=16, ny=14, nz=12, n_steps=80, npml=3, sources=[(8, 7, 6, 2, 0, 1.0, 0, 20 * DT, 5 * DT, 0)],
+            probes=[(11, 7, 6, 2), (8, 9, 6, 0), (6, 5, 4, 1)], freqs=[20e9, 45e9])
+
+DEBYE = ("debye", 20.0, 3e-11)
+LORENTZ = ("lorentz", 3.0, 2 * math.pi * 12e9, 2 * math.pi * 0.5e9)
+
+SCENES = {
+    "debye_box": Scene(**BASE, disp=[disp_entry(c, i, j, k, 2.5, 0.0, [DEBYE])
+                                     for c in range(3) for i in range(4, 12) for j in range(3, 11) for k in range(3, 9)]),
+    "lorentz_debye_slab_lossy": Scene(**BASE, disp=[disp_entry(c, i, j, k, 2.0, 0.01, [LORENTZ, ("debye", 5.0, 1e-10)])
+                                                    for c in range(3) for i in range(2, 15) for j in range(1, 13)
+                                                    for k in range(6, 8)]),
+    "spheres_smoothed": Scene(**BASE, disp=[disp_entry(0, MODEL_ONLY, 0, 0, 2.5, 0.0, [DEBYE]),
+                                            disp_entry(0, MODEL_ONLY, 0, 0, 2.0, 0.01, [LORENTZ])],
+                              spheres=[(8.3, 7.1, 6.2, 3.7, 6.0, 0.01, -1), (5.0, 5.0, 5.0, 2.2, 1.0, 0.0, 0),
+                                       (10.5, 9.0, 7.0, 2.5, 1.0, 0.0, 1), (7.0, 4.0, 8.0, 2.9, 3.5, 0.0, -1)]),
+    "spheres_staircase": Scene(**BASE, smoothing=0, spheres=[(8.3, 7.1, 6.2, 3.7, 6.0, 0.01, -1),
+                                                             (7.6, 6.0, 5.5, 2.4, 11.0, 0.0, -1)]),
+}
+
+
+def test_oracle_debye_static_limit():
+    # Debye with delta_eps -> 0 is a plain eps_inf medium
+    a = oracle.run_oracle(Scene(**BASE, boxes=[(4, 12, 3, 11, 3, 9, 3.0, 0.0)]))
+    b = oracle.run_oracle(Scene(**BASE, disp=[disp_entry(c, i, j, k, 3.0, 0.0, [("debye", 1e-9, 1e-11)])
+                                              for c in range(3) for i in range(4, 12) for j in range(3, 11)
+                                              for k in range(3, 9)]))
+    assert np.abs(a["td"] - b["td"]).max() <= 1e-8 * np.abs(a["td"]).max()
+
+
+def test_oracle_lorentz_static_limit():
+    a = oracle.run_oracle(Scene(**BASE, boxes=[(4, 12, 3, 11, 3, 9, 2.0, 0.0)]))
+    b = oracle.run_oracle(Scene(**BASE, disp=[disp_entry(c, i, j, k, 2.0, 0.0, [("lorentz", 1e-9, 2e11, 1e9)])
+                                              for c in range(3) for i in range(4, 12) for j in range(3, 11)
+                                              for k in range(3, 9)]))
+    assert np.abs(a["td"] - b["td"]).max() <= 1e-8 * np.abs(a["td"]).max()
+
+
+def test_oracle_debye_raises_low_frequency_delay():
+    # a Debye medium is slower at low frequency (eps_s = eps_inf + delta_eps)
+    # than its eps_inf limit: the pulse through it arrives later
+    s_inf = Scene(**{**BASE, "n_steps": 140}, boxes=[(4, 13, 0, 15, 0, 13, 2.5, 0.0)])
+    s_deb = Scene(**{**BASE, "n_steps": 140}, disp=[disp_entry(c, i, j, k, 2.5, 0.0, [("debye", 20.0, 1e-9)])
+                                                  for c in range(3) for i in range(4, 13) for j in range(0, 15)
+                                                  for k in range(0, 13)])
+    a = oracle.run_oracle(s_inf)["td"][0]
+    b = oracle.run_oracle(s_deb)["td"][0]
+    assert np.argmax(np.abs(b)) >= np.argmax(np.abs(a))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("schedule", [rb.SPLIT, rb.FUSED])
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_device_fp64_matches_oracle_bit_exact(name, schedule):
+    s = SCENES[name]
+    want = oracle.run_oracle(s)
+    got = run_device(s, rb.FP64, schedule)
+    assert np.array_equal(got["td"], want["td"]), np.abs(got["td"] - want["td"]).max()
+    assert np.linalg.norm(got["dft"] - want["dft"]) <= 1e-12 * np.linalg.norm(want["dft"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_device_fp32_close_to_oracle(name):
+    s = SCENES[name]
+    want = oracle.run_oracle(s)
+    got = run_device(s, rb.FP32, rb.FUSED)
+    for p in range(want["td"].shape[0]):
+        scale = np.abs(want["td"][p]).max()
+        assert np.abs(got["td"][p] - want["td"][p]).max() <= 1e-3 * scale
+
+
+@pytest.mark.gpu
+def test_sphere_fractions_partition_volume():
+    # the fractions of all E_z samples of a sphere sum to its volume
+    # (each sample owns one unit cube); 8^3 supersampling error is small
+    import ctypes as C
+
+    lib = rb.load()
+    f = lib.rfb_sphere_fractions
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(C.c_double), C.c_double] + [C.c_int] * 6 + [C.POINTER(C.c_double)] * 2
+    r = 7.3
+    n = 24
+    cen = (C.c_double * 3)(12.2, 11.9, 12.4)
+    fr = np.zeros(3 * n ** 3)
+    n2 = np.zeros(3 * n ** 3)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    assert f(cen, r, 0, 0, 0, n, n, n, dp(fr), dp(n2)) == 0
+    vol = 4.0 / 3.0 * math.pi * r ** 3
+    for c in range(3):
+        assert abs(fr[c::3].sum() - vol) / vol < 2e-3
+    assert fr.min() >= 0.0 and fr.max() <= 1.0
