@@ -1,0 +1,42 @@
+"""Runs a few time steps of a named workload on cuda:0, for profilers.
+
+    python -m rfsyn_b200.profile --workload c2 --steps 16 [--schedule fused|split] [--n N]
+
+The scene is created (and uploaded) first, then `steps` steps are launched
+kernel by kernel; nothing is timed here.  --n rescales the workload to an
+n^3 grid (same recipe) for captures that must stay small.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+
+import rfsyn_b200 as rb  # noqa: E402
+from rfsyn_b200 import scenes  # noqa: E402
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2"])
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--schedule", default="fused", choices=["fused", "split"])
+    ap.add_argument("--n", type=int, default=0)
+    args = ap.parse_args()
+    w = scenes.c2() if args.workload == "c2" else scenes.c1(precision=rb.FP32)
+    if args.n:
+        w = scenes.scaled(w, args.n, max(args.steps, 8))
+    w.schedule = rb.FUSED if args.schedule == "fused" else rb.SPLIT
+    w.n_steps = max(args.steps, 1)
+    setup = scenes.sphere_setup(w)
+    sim = rb.Sim(scenes.run_config(w), setup.ptr if setup else None, None)
+    sweep_ms, other_ms = sim.time_kernels(args.steps)
+    sim.close()
+    print(f"{w.name}: {args.steps} steps, sweep {sweep_ms / args.steps:.3f} ms/step, "
+          f"other {other_ms / args.steps:.3f} ms/step")
+
+
+if __name__ == "__main__":
+    main()
