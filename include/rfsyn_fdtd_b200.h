@@ -183,6 +183,27 @@ typedef struct {
 int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_sphere_t *spheres,
                                     size_t n_spheres, int smoothing);
 
+/* ---- sphere fill fractions without device allocation --------------------------
+ * No counterpart in rfsyn.  For callers that cannot allocate device memory
+ * when they rasterise a sphere: a thread building scenes while another
+ * thread of the process captures a CUDA graph (an allocation would break the
+ * capture), a real-time loop that must not enter the allocator, or a process
+ * whose device memory belongs to another framework's pool allocator.
+ * Computes, for every cell of the box [i0, i0+ni) x [j0, j0+nj) x [k0, k0+nk),
+ * the fill fraction f[3*cell + c] and squared normal component n2[3*cell + c]
+ * of the three E samples, cell = ((i-i0)*nj + (j-j0))*nk + (k-k0), exactly as
+ * fdtd_b200_materials_add_spheres does; f and n2 are host arrays of
+ * 3*ni*nj*nk doubles.  Nothing is allocated: the device staging is a fixed
+ * array of 2^20 samples per output (16 MiB in all) that the library keeps on
+ * every GPU that loads it until the process exits; a box of more than 2^20
+ * samples is rejected with -1.  The first call on a device looks the staging
+ * array up (once per device), so make that first call before any stream
+ * capture.  Every call shares the one array and runs on the default stream:
+ * calls that overlap on the GPU (from several host threads) race, so
+ * serialise them. */
+int fdtd_b200_sphere_fractions_noalloc(const double centre[3], double radius, int i0, int j0, int k0,
+                                       int ni, int nj, int nk, double *f, double *n2);
+
 /* ---- process-wide settings and diagnostics ---------------------------------- */
 /* Precision / schedule used by rfsyn's own entry points (fdtd_simulate_echo,
  * fdtd_stage_create).  Initial values: FP64 and FUSED, or the environment
