@@ -7,6 +7,8 @@
 #include <string.h>
 
 #include <atomic>
+#include <iterator>
+#include <mutex>
 #include <vector>
 
 #include "engine.h"
@@ -354,7 +356,8 @@ struct rfb_engine {
     size_t n_steps = 0, steps_done = 0;
     double *d_omega = nullptr, *d_re = nullptr, *d_im = nullptr;
     size_t dft_cap = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int own_stream = 0;
     int parity = 0;
     static constexpr int CHUNK = 16;
@@ -390,7 +393,13 @@ static void enqueue_step(rfb_engine *e, int par) {
     Args<T> a = engine_args<T>(e, par);
     const rfb_geom_t &g = e->g;
     if (e->sched == RFB_SCHED_FUSED) {
-        launch_fused<T>(a, e->plan, e->stream);
+        // interior and edge sweeps touch disjoint cells: run them side by side
+        cudaEventRecord(e->ev_fork, e->stream);
+        cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
+        launch_interior<T>(a, e->plan, e->stream);
+        launch_edge<T>(a, e->plan, e->stream2);
+        cudaEventRecord(e->ev_join, e->stream2);
+        cudaStreamWaitEvent(e->stream, e->ev_join, 0);
     } else {
         dim3 blk(32, 8);
         dim3 grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
@@ -411,7 +420,7 @@ static void enqueue_step(rfb_engine *e, int par) {
 }
 
 static int count_step_launches(const rfb_engine *e) {
-    int n = (e->sched == RFB_SCHED_FUSED) ? 1 : 2;
+    int n = (e->sched == RFB_SCHED_FUSED) ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) : 2;
     if (e->scene.n_cells) n++;
     return n + 1;
 }
@@ -434,6 +443,170 @@ fail:
     return -1;
 }
 
+// Work lists of the sweep.  Interior items: column tiles of (tj x 32) cells
+// in (j, k) whose cells, halo row and halo column lie outside every CPML
+// slab and PEC boundary (and hold no code-less list cell), over the interior
+// plane range; edge items: (8 x 32) tiles over everything else.
+static void free_plan_lists(FusedPlan &p) {
+    cudaFree(p.d_int);
+    cudaFree(p.d_edge);
+    p.d_int = p.d_edge = nullptr;
+    p.n_int = p.n_edge = 0;
+}
+
+static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int seg_int, int seg_edge) {
+    const rfb_geom_t &g = e->g;
+    const bool px = g.periodic & 1u, py = g.periodic & 2u, pz = g.periodic & 4u;
+    FusedPlan &p = e->plan;
+    free_plan_lists(p);
+    p.tj = tj;
+    p.ns = ns;
+    p.seg_int = seg_int;
+    p.seg_edge = seg_edge;
+    p.d.cj = g.ny + ((active && !py) ? 1 : 0);
+    p.d.ck = g.nz + ((active && !pz) ? 1 : 0);
+    p.d.ci = g.nx + ((active && !px) ? 1 : 0);
+    const bool on = e->cpml.on != 0;
+    int xlo, xhi, ylo, yhi, zlo, zhi;
+    auto ext = [&](int ax, int *lo, int *hi, int n, bool per) {
+        interior_axis(on ? e->cpml.eh[ax].lo : 0, on ? e->cpml.eh[ax].hi : n, on ? e->cpml.em[ax].lo : 0,
+                      on ? e->cpml.em[ax].hi : n + 1, n, per, on, lo, hi);
+    };
+    ext(0, &xlo, &xhi, g.nx, px);
+    ext(1, &ylo, &yhi, g.ny, py);
+    ext(2, &zlo, &zhi, g.nz, pz);
+    const int xa = px ? 0 : xlo + 1, xb = std::max(xa, xhi);
+    std::vector<SweepItem> vi, ve;
+    auto add = [](std::vector<SweepItem> &v, int j0, int k0, int b, int en, int seg) {
+        for (int s = b; s < en; s += seg) v.push_back(SweepItem{j0, k0, s, std::min(en, s + seg)});
+    };
+    auto add_edge = [&](int j0, int rows, int k0, int b, int en) {
+        for (int jj = j0; jj < j0 + rows && jj < p.d.cj; jj += 8) add(ve, jj, k0, b, en, seg_edge);
+    };
+    for (int j0 = 0; j0 < p.d.cj; j0 += tj)
+        for (int k0 = 0; k0 < p.d.ck; k0 += 32) {
+            const bool full = j0 + tj <= p.d.cj && k0 + 32 <= p.d.ck;
+            const bool yok = py ? j0 + tj <= g.ny : (j0 - 1 >= ylo && j0 + tj <= yhi);
+            const bool zok = pz ? k0 + 32 <= g.nz : (k0 - 1 >= zlo && k0 + 32 <= zhi);
+            bool skipcell = false;
+            for (int s = 0; s < e->scene.n_skip; s++) {
+                const long long c = e->scene.skip[s];
+                const int sk = (int)(c % e->pitch), sj = (int)((c / e->pitch) % (g.ny + 1));
+                if (sj >= j0 && sj < j0 + tj && sk >= k0 && sk < k0 + 32) skipcell = true;
+            }
+            if (full && yok && zok && !skipcell && xb > xa) {
+                add(vi, j0, k0, xa, xb, seg_int);
+                add_edge(j0, tj, k0, 0, xa);
+                add_edge(j0, tj, k0, xb, p.d.ci);
+            } else {
+                add_edge(j0, tj, k0, 0, p.d.ci);
+            }
+        }
+    p.n_int = (int)vi.size();
+    p.n_edge = (int)ve.size();
+    if (p.n_int) CK(cudaMalloc(&p.d_int, vi.size() * sizeof(SweepItem)));
+    if (p.n_edge) CK(cudaMalloc(&p.d_edge, ve.size() * sizeof(SweepItem)));
+    if (p.n_int) CK(cudaMemcpy(p.d_int, vi.data(), vi.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
+    if (p.n_edge) CK(cudaMemcpy(p.d_edge, ve.data(), ve.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
+    return 0;
+fail:
+    return -1;
+}
+
+// ---- autotuner ---------------------------------------------------------------
+// Picks the interior variant (rows per tile, ring depth, CTAs per SM) and the
+// segment lengths of both work lists by timing a few sweeps of each candidate
+// on the engine's own scene; the choice is cached per geometry.  Every
+// candidate computes bit-identical fields, so tuning changes speed only.
+struct TunedPlan {
+    int tj, ns, seg_int, seg_edge;
+};
+
+static std::mutex g_tune_mu;
+static std::vector<std::pair<std::vector<long long>, TunedPlan>> g_tune_cache;
+
+template <typename T>
+static void enqueue_sweep(rfb_engine *e, int par) {
+    Args<T> a = engine_args<T>(e, par);
+    cudaEventRecord(e->ev_fork, e->stream);
+    cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
+    launch_interior<T>(a, e->plan, e->stream);
+    launch_edge<T>(a, e->plan, e->stream2);
+    cudaEventRecord(e->ev_join, e->stream2);
+    cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+}
+
+static int autotune(rfb_engine *e, int active) {
+    const rfb_geom_t &g = e->g;
+    std::vector<long long> key = {g.nx, g.ny, g.nz, (long long)g.periodic, e->prec, active, e->cpml.on};
+    if (e->cpml.on)
+        for (int a = 0; a < 3; a++) {
+            key.push_back(e->cpml.eh[a].lo); key.push_back(e->cpml.eh[a].hi);
+            key.push_back(e->cpml.em[a].lo); key.push_back(e->cpml.em[a].hi);
+        }
+    for (int s = 0; s < e->scene.n_skip; s++) key.push_back(e->scene.skip[s]);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (auto &kv : g_tune_cache)
+            if (kv.first == key)
+                return build_sweep_plan(e, active, kv.second.tj, kv.second.ns, kv.second.seg_int, kv.second.seg_edge);
+    }
+    std::vector<InteriorVariant> vars;
+    if (e->prec == RFB_FP32) vars.assign(std::begin(kIntVariantsFp32), std::end(kIntVariantsFp32));
+    else vars.assign(std::begin(kIntVariantsFp64), std::end(kIntVariantsFp64));
+    const int segs_int[] = {32, 64, 128};
+    const int segs_edge[] = {16, 32};
+    TunedPlan best = {vars[0].tj, vars[0].ns, 64, 32};
+    float best_ms = 1e30f;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    {
+        const long long cells = (long long)g.nx * g.ny * g.nz;
+        const int reps = cells > (1 << 22) ? 3 : 6;
+        int par = 0;
+        for (const InteriorVariant &v : vars)
+            for (int si : segs_int)
+                for (int se : segs_edge) {
+                    if (build_sweep_plan(e, active, v.tj, v.ns, si, se) != 0) goto fail;
+                    for (int w = 0; w < 2; w++) {
+                        if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
+                        else enqueue_sweep<float>(e, par);
+                        par ^= 1;
+                    }
+                    CK(cudaEventRecord(t0, e->stream));
+                    for (int w = 0; w < reps; w++) {
+                        if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
+                        else enqueue_sweep<float>(e, par);
+                        par ^= 1;
+                    }
+                    CK(cudaEventRecord(t1, e->stream));
+                    CK(cudaEventSynchronize(t1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, t0, t1));
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = TunedPlan{v.tj, v.ns, si, se};
+                    }
+                }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache.push_back({key, best});
+    }
+    if (build_sweep_plan(e, active, best.tj, best.ns, best.seg_int, best.seg_edge) != 0) return -1;
+    // the tuning sweeps advanced the fields: start from the zero state again
+    if (rfb_engine_reset(e) != 0) return -1;
+    CK(cudaStreamSynchronize(e->stream));
+    return 0;
+fail:
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    return -1;
+}
+
 extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     if (!e) return;
     if (e->stream) cudaStreamSynchronize(e->stream);
@@ -448,6 +621,10 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     cudaFree(e->src_val); cudaFree(e->src_hard);
     cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
+    cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_join) cudaEventDestroy(e->ev_join);
+    if (e->stream2) cudaStreamDestroy(e->stream2);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -465,30 +642,6 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
     e->total = (size_t)(geom->nx + 1) * (geom->ny + 1) * e->pitch;
     e->nbuf = schedule == RFB_SCHED_FUSED ? 2 : 1;
     e->n_steps = n_steps;
-    if (schedule == RFB_SCHED_FUSED) {
-        int active = 0;
-        for (size_t s = 0; s < n_sources; s++) {
-            if ((sources[s].i == geom->nx && !(geom->periodic & 1u)) ||
-                (sources[s].j == geom->ny && !(geom->periodic & 2u)) ||
-                (sources[s].k == geom->nz && !(geom->periodic & 4u)))
-                active = 1;
-        }
-        if (fused_prepare() != 0) {
-            rfb_set_error("cannot configure the fused kernel's shared memory");
-            delete e;
-            return nullptr;
-        }
-        int rc = fused_plan_default(&e->plan, geom, active);
-        const char *ov = getenv("RFSYN_FDTD_PLAN");  // "tj,seg_len": manual tile plan
-        int tj = 0, seg = 0;
-        if (rc == 0 && ov && sscanf(ov, "%d,%d", &tj, &seg) == 2 && (tj == 8 || tj == 16))
-            rc = fused_plan_dims(&e->plan, geom, active, tj, seg);
-        if (rc != 0) {
-            rfb_set_error("grid too large for the fused schedule");
-            delete e;
-            return nullptr;
-        }
-    }
     if (stream) {
         e->stream = (cudaStream_t)stream;
     } else {
@@ -530,6 +683,35 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
     }
     CK(cudaMalloc(&e->d_step, sizeof(int)));
     CK(cudaMemset(e->d_step, 0, sizeof(int)));
+    if (schedule == RFB_SCHED_FUSED) {
+        if (fused_prepare() != 0) {
+            rfb_set_error("cannot configure the sweep kernels' shared memory");
+            goto fail_noset;
+        }
+        int active = 0;
+        for (size_t s = 0; s < n_sources; s++) {
+            if ((sources[s].i == geom->nx && !(geom->periodic & 1u)) ||
+                (sources[s].j == geom->ny && !(geom->periodic & 2u)) ||
+                (sources[s].k == geom->nz && !(geom->periodic & 4u)))
+                active = 1;
+        }
+        CK(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+        // plan: "tj,ns,seg_interior,seg_edge" from RFSYN_FDTD_PLAN, the
+        // autotuner (default) or, with RFSYN_FDTD_TUNE=0, the first variant
+        const char *ov = getenv("RFSYN_FDTD_PLAN");
+        const char *tune = getenv("RFSYN_FDTD_TUNE");
+        int a1 = 0, a2 = 0, a3 = 0, a4 = 0;
+        int rc;
+        if (ov && sscanf(ov, "%d,%d,%d,%d", &a1, &a2, &a3, &a4) == 4 && a3 > 0 && a4 > 0)
+            rc = build_sweep_plan(e, active, a1, a2, a3, a4);
+        else if (tune && !strcmp(tune, "0"))
+            rc = build_sweep_plan(e, active, 8, precision == RFB_FP32 ? 6 : 4, 64, 32);
+        else
+            rc = autotune(e, active);
+        if (rc != 0) goto fail_noset;
+    }
     CK(cudaDeviceSynchronize());
     e->launches_per_step = count_step_launches(e);
     if (scene) {
@@ -622,7 +804,7 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->dispersive = e->n_ade;
     out->h2d_bytes = e->h2d_bytes;
     out->tile_j = e->plan.tj;
-    out->seg_len = e->plan.d.seg_len;
+    out->seg_len = e->plan.seg_int;
     size_t sca = 0;
     if (e->cpml.on) {
         // cells of the swept volume inside the slab of each axis (H profiles)
@@ -650,8 +832,13 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         const rfb_geom_t &g = e->g;
         CK(cudaEventRecord(ev[0], e->stream));
         if (e->sched == RFB_SCHED_FUSED) {
-            launch_fused<T>(a, e->plan, e->stream);
-            g_launches++;
+            cudaEventRecord(e->ev_fork, e->stream);
+            cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
+            launch_interior<T>(a, e->plan, e->stream);
+            launch_edge<T>(a, e->plan, e->stream2);
+            cudaEventRecord(e->ev_join, e->stream2);
+            cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+            g_launches += (e->plan.n_int > 0) + (e->plan.n_edge > 0);
         } else {
             dim3 blk(32, 8), grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
             k_h_split<T><<<grd, blk, 0, e->stream>>>(a);

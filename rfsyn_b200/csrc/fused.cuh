@@ -1,26 +1,32 @@
-// fused.cuh -- one-kernel-per-step H+E sweep (2.5D march along i).
+// fused.cuh -- one-launch-per-step H+E sweep (2.5D march along i).
 //
-// Each CTA owns a (TJ x 32) tile of (j, k) and a segment of i planes and
-// marches the segment plane by plane.  Per plane p a stage of shared memory
-// holds E^n(p) with a one-cell halo in j and k, H^{n-1/2}(p) of the tile plus
-// the low-j / low-k halo cells, and the material codes of the tile.  Stages
-// live in an NS-deep ring filled by cp.async NS-1 planes ahead, so while
-// plane i is computed planes i+1 .. i+NS-1 are in flight from HBM (enough
-// bytes in flight per SM to cover HBM latency at full bandwidth).
+// The grid is cut into column tiles of (TJ x 32) cells in (j, k); a work item
+// is one tile and a range of i planes.  A CTA marches its range plane by
+// plane.  Per plane p a stage of shared memory holds E^n(p) with a one-cell
+// halo in j and k, H^{n-1/2}(p) of the tile plus its low-j / low-k halo cells
+// and the tile's material codes; stages form an NS-deep ring filled by
+// cp.async NS-1 planes ahead, so while plane i is computed the next planes
+// are in flight from HBM.
 //
 // Plane i: H^{n+1/2}(i) is computed for the tile (stored) and for its halo
-// (recomputed redundantly, never stored) from E(i), E(i+1) and H_in(i); then
-// E^{n+1}(i) follows from shared H(i) and the H(i-1) values of the previous
-// plane kept in registers.  Fields and the H-side psi are ping-ponged between
-// two buffers, so a halo recomputation always reads step-n data even when the
-// owning CTA has already written step n+1.  Per cell-step the kernel moves the
+// (recomputed, never stored) from E(i), E(i+1) and H_in(i); E^{n+1}(i) then
+// follows from shared H(i) and the H(i-1) values of the previous plane kept
+// in registers.  Fields and the H-side psi are ping-ponged between two
+// buffers, so a halo recomputation always reads step-n data even when the
+// owning CTA has already written step n+1.  Per cell-step the sweep moves the
 // compulsory 6 reads + 6 writes of the field components (48 B in FP32).
 //
-// A (tile, plane) with no CPML slab, no PEC boundary and no skipped cell takes
-// a branch-free interior path (uniform per CTA, so no divergence); all other
-// planes take the general path with rfsyn's per-component update ranges and
-// the slab-stored psi recursions.  Both evaluate identical arithmetic.
+// Two kernels make up one step's sweep (they run concurrently on two streams
+// and touch disjoint cells):
+//   k_sweep_interior -- items whose tiles and planes lie outside every CPML
+//     slab and PEC boundary: branch-free, no psi;
+//   k_sweep_edge -- all other items: rfsyn's per-component update ranges and
+//     the slab psi recursions, with psi and profile values staged in shared
+//     memory by the same cp.async ring, so no global load sits on the
+//     compute path.
 #pragma once
+#include <algorithm>
+
 #include "engine.h"
 #include "kernels.cuh"
 
@@ -28,13 +34,18 @@ namespace rfb {
 
 struct FusedDims {
     int cj, ck, ci;   // covered extents: j in [0,cj), k in [0,ck), planes [0,ci)
-    int seg_len;      // planes per CTA segment
+};
+
+struct SweepItem {
+    int j0, k0, ib, ie;
 };
 
 struct FusedPlan {
-    int tj = 8;
+    int tj = 8, ns = 6;   // interior variant (rows per tile, ring depth)
     FusedDims d;
-    dim3 grid;
+    int seg_int = 64, seg_edge = 32;
+    int n_int = 0, n_edge = 0;
+    SweepItem *d_int = nullptr, *d_edge = nullptr;  // device work lists
 };
 
 template <typename T>
@@ -59,6 +70,15 @@ struct FusedStage {
     T e[3][TJ + 2][34];   // E^n(p): rows j0-1 .. j0+TJ, cols k0-1 .. k0+32
     T h[3][TJ + 1][33];   // H_in(p): rows j0-1 .. j0+TJ-1, cols k0-1 .. k0+31
     uint32_t code[TJ][8]; // material codes of the tile (32 bytes per row)
+};
+
+// Edge stage: the fields plus the psi of plane p at the positions of h:
+// slots 0-5 hold the H-side psi arrays (hx_y hx_z hy_z hy_x hz_x hz_y),
+// slots 6-11 the E-side ones (ex_y ex_z ey_z ey_x ez_x ez_y, own cells only).
+template <typename T, int TJ>
+struct EdgeStage {
+    FusedStage<T, TJ> f;
+    T psi[12][TJ + 1][33];
 };
 
 __device__ __forceinline__ int wrap_coord(int q, int n, bool periodic, bool &valid) {
@@ -126,7 +146,8 @@ __device__ __forceinline__ IssuePlan make_issue_plan(const Args<T> &a, int j0, i
     return ip;
 }
 
-// Issues the cp.async copies of plane p into stage st (p < 0: zeros).
+// Issues the cp.async copies of the fields of plane p into stage st (p < 0:
+// zeros).
 template <typename T, int TJ>
 __device__ __forceinline__ void fused_issue(const Args<T> &a, FusedStage<T, TJ> &st, int p, const IssuePlan &ip,
                                             int r, int q) {
@@ -158,56 +179,6 @@ __device__ __forceinline__ void fused_issue(const Args<T> &a, FusedStage<T, TJ> 
     }
 }
 
-// General-path H^{n+1/2} of component c at plane i from stage-resident E(i)
-// (cur), E(i+1) (nxt) and H_in(i); (r, q) is the stage position.  Components
-// that rfsyn's loops do not update keep their input value.  store: write the
-// new psi (owner) or only use it (halo).
-template <typename T, int TJ>
-__device__ __forceinline__ T fused_h(const Args<T> &a, int c, int i, int j, int k, const FusedStage<T, TJ> &cur,
-                                     const FusedStage<T, TJ> &nxt, int r, int q, bool store) {
-    const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
-    const T hin = cur.h[c][r][q];
-    T dA, dB;
-    int pA, pB, axA, axB, qA, qB;
-    if (c == 0) {
-        if (!(i < a.nx + (px ? 0 : 1) && j < a.ny && k < a.nz)) return hin;
-        dA = xs(cur.e[2][r + 1][q], cur.e[2][r][q]);
-        dB = xs(cur.e[1][r][q + 1], cur.e[1][r][q]);
-        pA = 0; axA = 1; qA = j;
-        pB = 1; axB = 2; qB = k;
-    } else if (c == 1) {
-        if (!(i < a.nx && j < a.ny + (py ? 0 : 1) && k < a.nz)) return hin;
-        dA = xs(cur.e[0][r][q + 1], cur.e[0][r][q]);
-        dB = xs(nxt.e[2][r][q], cur.e[2][r][q]);
-        pA = 2; axA = 2; qA = k;
-        pB = 3; axB = 0; qB = i;
-    } else {
-        if (!(i < a.nx && j < a.ny && k < a.nz + (pz ? 0 : 1))) return hin;
-        dA = xs(nxt.e[1][r][q], cur.e[1][r][q]);
-        dB = xs(cur.e[0][r + 1][q], cur.e[0][r][q]);
-        pA = 4; axA = 0; qA = i;
-        pB = 5; axB = 1; qB = j;
-    }
-    T tA = dA, tB = dB;
-    if (a.cpml_on) {
-        int s = slab_of(qA, a.lo_h[axA], a.hi_h[axA]);
-        if (s >= 0) {
-            const long long pi = psi_idx(a, axA, a.ns_h[axA], s, i, j, k);
-            T pn;
-            tA = cpml_step(dA, a.kinv_h[axA][qA], a.b_h[axA][qA], a.a_h[axA][qA], a.dx, a.psi_hi[pA][pi], &pn);
-            if (store) a.psi_ho[pA][pi] = pn;
-        }
-        s = slab_of(qB, a.lo_h[axB], a.hi_h[axB]);
-        if (s >= 0) {
-            const long long pi = psi_idx(a, axB, a.ns_h[axB], s, i, j, k);
-            T pn;
-            tB = cpml_step(dB, a.kinv_h[axB][qB], a.b_h[axB][qB], a.a_h[axB][qB], a.dx, a.psi_hi[pB][pi], &pn);
-            if (store) a.psi_ho[pB][pi] = pn;
-        }
-    }
-    return xs(hin, xm(a.cbh, xs(tA, tB)));
-}
-
 __device__ __forceinline__ int plane_after(int i, int nx, bool px) {
     int p = i + 1;
     if (p == nx && px) return 0;
@@ -215,36 +186,156 @@ __device__ __forceinline__ int plane_after(int i, int nx, bool px) {
     return p;
 }
 
-// Range [lo, hi) of a non-periodic axis where both profiles are the identity
-// and every component is swept, for tiles that also read index lo-1.
-__device__ __forceinline__ void interior_range(int lo_h, int hi_h, int lo_m, int hi_m, int n, bool periodic, int cpml,
-                                               int &lo, int &hi) {
-    if (periodic) {
-        lo = 0;
-        hi = n;
-        return;
-    }
-    lo = 1;
-    hi = n;
-    if (cpml) {
-        lo = max(lo, max(lo_h, lo_m));
-        hi = min(hi, min(hi_h, hi_m));
-    }
+// Unstretched H of component c at stage position (r, q).
+template <typename T, int TJ>
+__device__ __forceinline__ T h_interior(int c, T cbh, const FusedStage<T, TJ> &cur, const FusedStage<T, TJ> &nxt,
+                                        int r, int q) {
+    if (c == 0)
+        return xs(cur.h[0][r][q],
+                  xm(cbh, xs(xs(cur.e[2][r + 1][q], cur.e[2][r][q]), xs(cur.e[1][r][q + 1], cur.e[1][r][q]))));
+    if (c == 1)
+        return xs(cur.h[1][r][q],
+                  xm(cbh, xs(xs(cur.e[0][r][q + 1], cur.e[0][r][q]), xs(nxt.e[2][r][q], cur.e[2][r][q]))));
+    return xs(cur.h[2][r][q],
+              xm(cbh, xs(xs(nxt.e[1][r][q], cur.e[1][r][q]), xs(cur.e[0][r + 1][q], cur.e[0][r][q]))));
 }
 
-// NS stages: planes i .. i+NS-2 are resident or in flight while plane i is
-// computed (prefetch distance NS-1).
+// ---------------------------------------------------------------------------
+// Interior sweep: every cell of every plane of the item is updated with the
+// unstretched formulas (the host-built item list guarantees it).
+// ---------------------------------------------------------------------------
 template <typename T, int TJ, int NS, int MINB>
-__global__ void __launch_bounds__(32 * TJ, MINB) k_fused(Args<T> a, FusedDims d) {
+__global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_interior(Args<T> a, FusedDims d, const SweepItem *items) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FusedStage<T, TJ> *stage = reinterpret_cast<FusedStage<T, TJ> *>(smem_raw);
     T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(smem_raw + NS * sizeof(FusedStage<T, TJ>));
     T *s_tab = reinterpret_cast<T *>(smem_raw + NS * sizeof(FusedStage<T, TJ>) + sizeof(T) * 3 * (TJ + 1) * 33);
 
+    const SweepItem it = items[blockIdx.x];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * TJ;
-    const int ib = blockIdx.z * d.seg_len;
-    const int ie = min(ib + d.seg_len, d.ci);
+    const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
+    const bool px = a.per & 1u;
+    const int r = ty + 1, q = tx + 1;
+    const IssuePlan ip = make_issue_plan<T, TJ>(a, j0, k0, tid);
+    (void)d;
+    for (int t = tid; t < 256; t += 32 * TJ) {
+        s_tab[t] = a.tca[t];
+        s_tab[256 + t] = a.tcb[t];
+    }
+    const T cbh = a.cbh;
+    const int pprev = ib > 0 ? ib - 1 : a.nx - 1;  // ib == 0 only on a periodic x axis
+    fused_issue<T, TJ>(a, stage[NS - 1], pprev, ip, r, q);
+    cp_async_commit();
+    int pf = ib;
+#pragma unroll
+    for (int s = 0; s < NS - 1; s++) {
+        if (pf >= 0 && ib + s <= ie) fused_issue<T, TJ>(a, stage[s], pf, ip, r, q);
+        cp_async_commit();
+        if (pf >= 0) pf = plane_after(pf, a.nx, px);
+    }
+    cp_async_wait<NS - 2>();
+    __syncthreads();
+    T prevHy = h_interior<T, TJ>(1, cbh, stage[NS - 1], stage[0], r, q);
+    T prevHz = h_interior<T, TJ>(2, cbh, stage[NS - 1], stage[0], r, q);
+    __syncthreads();
+
+    int sc = 0;
+    for (int i = ib; i < ie; i++) {
+        const int sn = sc == NS - 1 ? 0 : sc + 1;
+        const int sf = sc == 0 ? NS - 1 : sc - 1;
+        if (pf >= 0 && i + NS - 1 <= ie) fused_issue<T, TJ>(a, stage[sf], pf, ip, r, q);
+        cp_async_commit();
+        if (pf >= 0) pf = plane_after(pf, a.nx, px);
+        cp_async_wait<NS - 2>();
+        __syncthreads();
+        const FusedStage<T, TJ> &cur = stage[sc];
+        const FusedStage<T, TJ> &nxt = stage[sn];
+        const T e0 = cur.e[0][r][q], e1 = cur.e[1][r][q], e2 = cur.e[2][r][q];
+        const int code = (int)((cur.code[ty][tx >> 2] >> (8 * (tx & 3))) & 0xffu);
+        const long long c = (long long)i * a.plane + (long long)ip.own_off;
+        const T hx = h_interior<T, TJ>(0, cbh, cur, nxt, r, q);
+        const T hy = h_interior<T, TJ>(1, cbh, cur, nxt, r, q);
+        const T hz = h_interior<T, TJ>(2, cbh, cur, nxt, r, q);
+        a.Ho[0][c] = hx;
+        a.Ho[1][c] = hy;
+        a.Ho[2][c] = hz;
+        sH[0][r][q] = hx;
+        sH[1][r][q] = hy;
+        sH[2][r][q] = hz;
+        if (ty == 0) {
+            sH[0][0][q] = h_interior<T, TJ>(0, cbh, cur, nxt, 0, q);
+            sH[2][0][q] = h_interior<T, TJ>(2, cbh, cur, nxt, 0, q);
+        } else if (ty == 1 && tx < TJ) {
+            sH[0][tx + 1][0] = h_interior<T, TJ>(0, cbh, cur, nxt, tx + 1, 0);
+            sH[1][tx + 1][0] = h_interior<T, TJ>(1, cbh, cur, nxt, tx + 1, 0);
+        }
+        __syncthreads();
+        if (!a.codes || code != LIST_CODE) {
+            const T ca = s_tab[code], cb = s_tab[256 + code];
+            a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(xs(sH[2][r][q], sH[2][r - 1][q]), xs(sH[1][r][q], sH[1][r][q - 1]))));
+            a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(xs(sH[0][r][q], sH[0][r][q - 1]), xs(hz, prevHz))));
+            a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(xs(hy, prevHy), xs(sH[0][r][q], sH[0][r - 1][q]))));
+        }
+        prevHy = hy;
+        prevHz = hz;
+        sc = sn;
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Edge sweep
+// ---------------------------------------------------------------------------
+// Profile triple (kappa_inv, b, a) at index q of an axis profile of length
+// len, identity outside it or when the axis has no CPML.
+template <typename T>
+__device__ __forceinline__ void prof_at(const T *kinv, const T *b, const T *ac, int q, int len, T *out) {
+    if (kinv && q >= 0 && q < len) {
+        out[0] = kinv[q];
+        out[1] = b[q];
+        out[2] = ac[q];
+    } else {
+        out[0] = T(1);
+        out[1] = T(1);
+        out[2] = T(0);
+    }
+}
+
+// Slab index of q, -1 in the unstretched interior or outside [0, len).
+__device__ __forceinline__ int slab_in(int q, int lo, int hi, int len, int on) {
+    if (!on || q < 0 || q >= len) return -1;
+    return slab_of(q, lo, hi);
+}
+
+// Per-CTA profile tables in shared memory.
+template <typename T, int TJ>
+struct EdgeShared {
+    T py[6][TJ + 1];   // y profile (h: kinv b a, m: kinv b a) at rows j0-1 .. j0+TJ-1
+    T pz[6][33];       // z profile at cols k0-1 .. k0+31
+};
+
+// rfsyn's cpml_term with the psi state passed by value: psi_new = b psi +
+// a d (written to *psi_out), returns d kappa_inv + dx psi_new.
+template <typename T>
+__device__ __forceinline__ T stretch(T d, T kinv, T b, T ac, T dx, T psi_old, T *psi_out) {
+    T pn = xa(xm(b, psi_old), xm(ac, d));
+    *psi_out = pn;
+    return xa(xm(d, kinv), xm(dx, pn));
+}
+
+template <typename T, int TJ, int NS, int MINB>
+__global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDims d, const SweepItem *items) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    EdgeStage<T, TJ> *stage = reinterpret_cast<EdgeStage<T, TJ> *>(smem_raw);
+    unsigned char *after = smem_raw + NS * sizeof(EdgeStage<T, TJ>);
+    T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(after);
+    T *s_tab = reinterpret_cast<T *>(after + sizeof(T) * 3 * (TJ + 1) * 33);
+    EdgeShared<T, TJ> &es =
+        *reinterpret_cast<EdgeShared<T, TJ> *>(after + sizeof(T) * 3 * (TJ + 1) * 33 + sizeof(T) * 512);
+
+    const SweepItem it = items[blockIdx.x];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
     const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
     const int j = j0 + ty, k = k0 + tx;
     const bool own = j < d.cj && k < d.ck;
@@ -254,45 +345,183 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_fused(Args<T> a, FusedDims d)
     const int kh = k0 > 0 ? k0 - 1 : a.nz - 1;
     const int r = ty + 1, q = tx + 1;
     const IssuePlan ip = make_issue_plan<T, TJ>(a, j0, k0, tid);
+    const int on = a.cpml_on;
+    const long long ny1 = a.ny + 1;
 
-    // coefficient table in shared memory
     for (int t = tid; t < 256; t += 32 * TJ) {
         s_tab[t] = a.tca[t];
         s_tab[256 + t] = a.tcb[t];
     }
-    // interior test: y / z per CTA, x per plane
-    int ylo, yhi, zlo, zhi, xlo, xhi;
-    interior_range(a.lo_h[1], a.hi_h[1], a.lo_m[1], a.hi_m[1], a.ny, py, a.cpml_on, ylo, yhi);
-    interior_range(a.lo_h[2], a.hi_h[2], a.lo_m[2], a.hi_m[2], a.nz, pz, a.cpml_on, zlo, zhi);
-    interior_range(a.lo_h[0], a.hi_h[0], a.lo_m[0], a.hi_m[0], a.nx, px, a.cpml_on, xlo, xhi);
-    const bool tile_fast = (py ? j0 + TJ <= a.ny : (j0 - 1 >= ylo && j0 + TJ <= yhi)) &&
-                           (pz ? k0 + 32 <= a.nz : (k0 - 1 >= zlo && k0 + 32 <= zhi));
-    // skipped cells (code-less scenes) in this tile: their planes take the general path
-    int skip_plane[MAX_SKIP];
-#pragma unroll
-    for (int s = 0; s < MAX_SKIP; s++) {
-        skip_plane[s] = -1;
-        if (s < a.n_skip) {
-            const long long c = a.skip[s];
-            const int sk = (int)(c % a.pitch), sj = (int)((c / a.pitch) % (a.ny + 1));
-            if (sj >= j0 && sj < j0 + TJ && sk >= k0 && sk < k0 + 32) skip_plane[s] = (int)(c / a.plane);
-        }
+    for (int t = tid; t < TJ + 1; t += 32 * TJ) {
+        const int jj = j0 - 1 + t;
+        T v[3];
+        prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], jj, a.ny, v);
+        es.py[0][t] = v[0]; es.py[1][t] = v[1]; es.py[2][t] = v[2];
+        prof_at(on ? a.kinv_m[1] : (const T *)nullptr, a.b_m[1], a.a_m[1], jj, a.ny + 1, v);
+        es.py[3][t] = v[0]; es.py[4][t] = v[1]; es.py[5][t] = v[2];
     }
+    for (int t = tid; t < 33; t += 32 * TJ) {
+        const int kk = k0 - 1 + t;
+        T v[3];
+        prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], kk, a.nz, v);
+        es.pz[0][t] = v[0]; es.pz[1][t] = v[1]; es.pz[2][t] = v[2];
+        prof_at(on ? a.kinv_m[2] : (const T *)nullptr, a.b_m[2], a.a_m[2], kk, a.nz + 1, v);
+        es.pz[3][t] = v[0]; es.pz[4][t] = v[1]; es.pz[5][t] = v[2];
+    }
+    // slab indices of the own cell (H side: q < n; E side: only swept samples
+    // use them, and those have q < n)
+    const int sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
+    const int skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
+    const int sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
+    const int skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
+    // halo cells: row (j0-1, k) for warp 0, column (j0+tx, k0-1) for warp 1
+    const int sjh_row = slab_in(j0 - 1, a.lo_h[1], a.hi_h[1], a.ny, on);
+    const int jc = j0 + tx;
+    const int sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
+    const int skh_col = slab_in(k0 - 1, a.lo_h[2], a.hi_h[2], a.nz, on);
+    const int nshy = a.ns_h[1], nshz = a.ns_h[2], nsmy = a.ns_m[1], nsmz = a.ns_m[2];
+
+    // psi copies of plane p into stage st
+    auto issue_psi = [&](EdgeStage<T, TJ> &st, int p) {
+        if (!on || p < 0) return;
+        const int sxh = slab_in(p, a.lo_h[0], a.hi_h[0], a.nx, on);
+        const int sxm = slab_in(p, a.lo_m[0], a.hi_m[0], a.nx, on);
+        if (own) {
+            if (sjh >= 0) {
+                const long long o = ((long long)p * nshy + sjh) * a.pitch + k;
+                cp_async(&st.psi[0][r][q], a.psi_hi[0] + o, true);
+                cp_async(&st.psi[5][r][q], a.psi_hi[5] + o, true);
+            }
+            if (skh >= 0) {
+                const long long o = ((long long)p * ny1 + j) * nshz + skh;
+                cp_async(&st.psi[1][r][q], a.psi_hi[1] + o, true);
+                cp_async(&st.psi[2][r][q], a.psi_hi[2] + o, true);
+            }
+            if (sxh >= 0) {
+                const long long o = ((long long)sxh * ny1 + j) * a.pitch + k;
+                cp_async(&st.psi[3][r][q], a.psi_hi[3] + o, true);
+                cp_async(&st.psi[4][r][q], a.psi_hi[4] + o, true);
+            }
+            if (sjm >= 0) {
+                const long long o = ((long long)p * nsmy + sjm) * a.pitch + k;
+                cp_async(&st.psi[6][r][q], a.psi_e[0] + o, true);
+                cp_async(&st.psi[11][r][q], a.psi_e[5] + o, true);
+            }
+            if (skm >= 0) {
+                const long long o = ((long long)p * ny1 + j) * nsmz + skm;
+                cp_async(&st.psi[7][r][q], a.psi_e[1] + o, true);
+                cp_async(&st.psi[8][r][q], a.psi_e[2] + o, true);
+            }
+            if (sxm >= 0) {
+                const long long o = ((long long)sxm * ny1 + j) * a.pitch + k;
+                cp_async(&st.psi[9][r][q], a.psi_e[3] + o, true);
+                cp_async(&st.psi[10][r][q], a.psi_e[4] + o, true);
+            }
+        }
+        if (ty == 0 && row_halo && k < d.ck) {
+            // row halo (j0-1, k): Hx (hx_y, hx_z), Hz (hz_x, hz_y)
+            if (sjh_row >= 0) {
+                const long long o = ((long long)p * nshy + sjh_row) * a.pitch + k;
+                cp_async(&st.psi[0][0][q], a.psi_hi[0] + o, true);
+                cp_async(&st.psi[5][0][q], a.psi_hi[5] + o, true);
+            }
+            if (skh >= 0) {
+                const long long o = ((long long)p * ny1 + jh) * nshz + skh;
+                cp_async(&st.psi[1][0][q], a.psi_hi[1] + o, true);
+            }
+            if (sxh >= 0) {
+                const long long o = ((long long)sxh * ny1 + jh) * a.pitch + k;
+                cp_async(&st.psi[4][0][q], a.psi_hi[4] + o, true);
+            }
+        } else if (ty == 1 && tx < TJ && col_halo && jc < d.cj) {
+            // column halo (j0+tx, k0-1): Hx (hx_y, hx_z), Hy (hy_z, hy_x)
+            if (sjh_col >= 0) {
+                const long long o = ((long long)p * nshy + sjh_col) * a.pitch + kh;
+                cp_async(&st.psi[0][tx + 1][0], a.psi_hi[0] + o, true);
+            }
+            if (skh_col >= 0) {
+                const long long o = ((long long)p * ny1 + jc) * nshz + skh_col;
+                cp_async(&st.psi[1][tx + 1][0], a.psi_hi[1] + o, true);
+                cp_async(&st.psi[2][tx + 1][0], a.psi_hi[2] + o, true);
+            }
+            if (sxh >= 0) {
+                const long long o = ((long long)sxh * ny1 + jc) * a.pitch + kh;
+                cp_async(&st.psi[3][tx + 1][0], a.psi_hi[3] + o, true);
+            }
+        }
+    };
+    auto issue = [&](EdgeStage<T, TJ> &st, int p) {
+        fused_issue<T, TJ>(a, st.f, p, ip, r, q);
+        issue_psi(st, p);
+    };
+
+    // H of component c at plane i for the cell at stage (rr, qq) with
+    // coordinates (jj, kk); sy / sz its H-side y / z slab indices, yi / zi
+    // its rows in the profile tables; store: the owner writes the new psi.
+    auto h_edge = [&](int c, int i, int jj, int kk, int rr, int qq, int sy, int sz, int yi, int zi,
+                      const EdgeStage<T, TJ> &cs, const EdgeStage<T, TJ> &ns, bool store) -> T {
+        const FusedStage<T, TJ> &cur = cs.f, &nxt = ns.f;
+        const T hin = cur.h[c][rr][qq];
+        const int sx = slab_in(i, a.lo_h[0], a.hi_h[0], a.nx, on);
+        T dA, dB;
+        if (c == 0) {
+            if (!(i < a.nx + (px ? 0 : 1) && jj < a.ny && kk < a.nz)) return hin;
+            dA = xs(cur.e[2][rr + 1][qq], cur.e[2][rr][qq]);
+            dB = xs(cur.e[1][rr][qq + 1], cur.e[1][rr][qq]);
+            if (sy >= 0) {
+                T pn;
+                dA = stretch(dA, es.py[0][yi], es.py[1][yi], es.py[2][yi], a.dx, cs.psi[0][rr][qq], &pn);
+                if (store) a.psi_ho[0][((long long)i * nshy + sy) * a.pitch + kk] = pn;
+            }
+            if (sz >= 0) {
+                T pn;
+                dB = stretch(dB, es.pz[0][zi], es.pz[1][zi], es.pz[2][zi], a.dx, cs.psi[1][rr][qq], &pn);
+                if (store) a.psi_ho[1][((long long)i * ny1 + jj) * nshz + sz] = pn;
+            }
+        } else if (c == 1) {
+            if (!(i < a.nx && jj < a.ny + (py ? 0 : 1) && kk < a.nz)) return hin;
+            dA = xs(cur.e[0][rr][qq + 1], cur.e[0][rr][qq]);
+            dB = xs(nxt.e[2][rr][qq], cur.e[2][rr][qq]);
+            if (sz >= 0) {
+                T pn;
+                dA = stretch(dA, es.pz[0][zi], es.pz[1][zi], es.pz[2][zi], a.dx, cs.psi[2][rr][qq], &pn);
+                if (store) a.psi_ho[2][((long long)i * ny1 + jj) * nshz + sz] = pn;
+            }
+            if (sx >= 0) {
+                T pn;
+                dB = stretch(dB, a.kinv_h[0][i], a.b_h[0][i], a.a_h[0][i], a.dx, cs.psi[3][rr][qq], &pn);
+                if (store) a.psi_ho[3][((long long)sx * ny1 + jj) * a.pitch + kk] = pn;
+            }
+        } else {
+            if (!(i < a.nx && jj < a.ny && kk < a.nz + (pz ? 0 : 1))) return hin;
+            dA = xs(nxt.e[1][rr][qq], cur.e[1][rr][qq]);
+            dB = xs(cur.e[0][rr + 1][qq], cur.e[0][rr][qq]);
+            if (sx >= 0) {
+                T pn;
+                dA = stretch(dA, a.kinv_h[0][i], a.b_h[0][i], a.a_h[0][i], a.dx, cs.psi[4][rr][qq], &pn);
+                if (store) a.psi_ho[4][((long long)sx * ny1 + jj) * a.pitch + kk] = pn;
+            }
+            if (sy >= 0) {
+                T pn;
+                dB = stretch(dB, es.py[0][yi], es.py[1][yi], es.py[2][yi], a.dx, cs.psi[5][rr][qq], &pn);
+                if (store) a.psi_ho[5][((long long)i * nshy + sy) * a.pitch + kk] = pn;
+            }
+        }
+        return xs(hin, xm(a.cbh, xs(dA, dB)));
+    };
 
     T prevHy = 0, prevHz = 0;
     int pprev = -1;
     if (ib > 0) pprev = ib - 1;
     else if (px) pprev = a.nx - 1;
-    // one commit group per plane: [pprev], ib, ib+1, ..., ib+NS-2; the
-    // plane before the segment borrows the slot of plane ib+NS-1
     if (pprev >= 0) {
-        fused_issue<T, TJ>(a, stage[NS - 1], pprev, ip, r, q);
+        issue(stage[NS - 1], pprev);
         cp_async_commit();
     }
-    int pf = ib;  // next plane to fetch (in march order, possibly wrapped)
+    int pf = ib;
 #pragma unroll
     for (int s = 0; s < NS - 1; s++) {
-        if (pf >= 0 && ib + s <= ie) fused_issue<T, TJ>(a, stage[s], pf, ip, r, q);
+        if (pf >= 0 && ib + s <= ie) issue(stage[s], pf);
         cp_async_commit();
         if (pf >= 0) pf = plane_after(pf, a.nx, px);
     }
@@ -300,80 +529,48 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_fused(Args<T> a, FusedDims d)
         cp_async_wait<NS - 2>();
         __syncthreads();
         if (own) {
-            prevHy = fused_h<T, TJ>(a, 1, pprev, j, k, stage[NS - 1], stage[0], r, q, false);
-            prevHz = fused_h<T, TJ>(a, 2, pprev, j, k, stage[NS - 1], stage[0], r, q, false);
+            prevHy = h_edge(1, pprev, j, k, r, q, sjh, skh, r, q, stage[NS - 1], stage[0], false);
+            prevHz = h_edge(2, pprev, j, k, r, q, sjh, skh, r, q, stage[NS - 1], stage[0], false);
         }
-        __syncthreads();
     }
+    __syncthreads();  // profile tables visible; prologue slot free
 
     int sc = 0;
     for (int i = ib; i < ie; i++) {
         const int sn = sc == NS - 1 ? 0 : sc + 1;
-        const int sf = sc == 0 ? NS - 1 : sc - 1;  // slot of plane i+NS-1
-        // fetch plane i+NS-1 (needed as E(i+NS-1) by plane i+NS-2 <= ie-1)
-        if (pf >= 0 && i + NS - 1 <= ie) fused_issue<T, TJ>(a, stage[sf], pf, ip, r, q);
+        const int sf = sc == 0 ? NS - 1 : sc - 1;
+        if (pf >= 0 && i + NS - 1 <= ie) issue(stage[sf], pf);
         cp_async_commit();
         if (pf >= 0) pf = plane_after(pf, a.nx, px);
         cp_async_wait<NS - 2>();
         __syncthreads();
-        const FusedStage<T, TJ> &cur = stage[sc];
-        const FusedStage<T, TJ> &nxt = stage[sn];
-        bool fast = tile_fast && i >= xlo && i < xhi;
-#pragma unroll
-        for (int s = 0; s < MAX_SKIP; s++) fast = fast && skip_plane[s] != i;
+        const EdgeStage<T, TJ> &cs = stage[sc];
+        const EdgeStage<T, TJ> &ns = stage[sn];
+        const FusedStage<T, TJ> &cur = cs.f;
         const T e0 = cur.e[0][r][q], e1 = cur.e[1][r][q], e2 = cur.e[2][r][q];
         const int code = (int)((cur.code[ty][tx >> 2] >> (8 * (tx & 3))) & 0xffu);
         const long long c = (long long)i * a.plane + (long long)ip.own_off;
         T hx = 0, hy = 0, hz = 0;
-        if (fast) {
-            const T cbh = a.cbh;
-            hx = xs(cur.h[0][r][q], xm(cbh, xs(xs(cur.e[2][r + 1][q], cur.e[2][r][q]), xs(cur.e[1][r][q + 1], cur.e[1][r][q]))));
-            hy = xs(cur.h[1][r][q], xm(cbh, xs(xs(cur.e[0][r][q + 1], cur.e[0][r][q]), xs(nxt.e[2][r][q], cur.e[2][r][q]))));
-            hz = xs(cur.h[2][r][q], xm(cbh, xs(xs(nxt.e[1][r][q], cur.e[1][r][q]), xs(cur.e[0][r + 1][q], cur.e[0][r][q]))));
+        if (own) {
+            hx = h_edge(0, i, j, k, r, q, sjh, skh, r, q, cs, ns, true);
+            hy = h_edge(1, i, j, k, r, q, sjh, skh, r, q, cs, ns, true);
+            hz = h_edge(2, i, j, k, r, q, sjh, skh, r, q, cs, ns, true);
             a.Ho[0][c] = hx;
             a.Ho[1][c] = hy;
             a.Ho[2][c] = hz;
-            sH[0][r][q] = hx;
-            sH[1][r][q] = hy;
-            sH[2][r][q] = hz;
-            if (ty == 0) {
-                sH[0][0][q] = xs(cur.h[0][0][q], xm(cbh, xs(xs(cur.e[2][1][q], cur.e[2][0][q]), xs(cur.e[1][0][q + 1], cur.e[1][0][q]))));
-                sH[2][0][q] = xs(cur.h[2][0][q], xm(cbh, xs(xs(nxt.e[1][0][q], cur.e[1][0][q]), xs(cur.e[0][1][q], cur.e[0][0][q]))));
-            } else if (ty == 1 && tx < TJ) {
-                const int rr = tx + 1;
-                sH[0][rr][0] = xs(cur.h[0][rr][0], xm(cbh, xs(xs(cur.e[2][rr + 1][0], cur.e[2][rr][0]), xs(cur.e[1][rr][1], cur.e[1][rr][0]))));
-                sH[1][rr][0] = xs(cur.h[1][rr][0], xm(cbh, xs(xs(cur.e[0][rr][1], cur.e[0][rr][0]), xs(nxt.e[2][rr][0], cur.e[2][rr][0]))));
-            }
-        } else {
-            if (own) {
-                hx = fused_h<T, TJ>(a, 0, i, j, k, cur, nxt, r, q, true);
-                hy = fused_h<T, TJ>(a, 1, i, j, k, cur, nxt, r, q, true);
-                hz = fused_h<T, TJ>(a, 2, i, j, k, cur, nxt, r, q, true);
-                a.Ho[0][c] = hx;
-                a.Ho[1][c] = hy;
-                a.Ho[2][c] = hz;
-            }
-            sH[0][r][q] = hx;
-            sH[1][r][q] = hy;
-            sH[2][r][q] = hz;
-            if (ty == 0 && row_halo && k < d.ck) {
-                sH[0][0][q] = fused_h<T, TJ>(a, 0, i, jh, k, cur, nxt, 0, q, false);
-                sH[2][0][q] = fused_h<T, TJ>(a, 2, i, jh, k, cur, nxt, 0, q, false);
-            } else if (ty == 1 && tx < TJ && col_halo && j0 + tx < d.cj) {
-                const int rr = tx + 1;
-                sH[0][rr][0] = fused_h<T, TJ>(a, 0, i, j0 + tx, kh, cur, nxt, rr, 0, false);
-                sH[1][rr][0] = fused_h<T, TJ>(a, 1, i, j0 + tx, kh, cur, nxt, rr, 0, false);
-            }
+        }
+        sH[0][r][q] = hx;
+        sH[1][r][q] = hy;
+        sH[2][r][q] = hz;
+        if (ty == 0 && row_halo && k < d.ck) {
+            sH[0][0][q] = h_edge(0, i, jh, k, 0, q, sjh_row, skh, 0, q, cs, ns, false);
+            sH[2][0][q] = h_edge(2, i, jh, k, 0, q, sjh_row, skh, 0, q, cs, ns, false);
+        } else if (ty == 1 && tx < TJ && col_halo && jc < d.cj) {
+            sH[0][tx + 1][0] = h_edge(0, i, jc, kh, tx + 1, 0, sjh_col, skh_col, tx + 1, 0, cs, ns, false);
+            sH[1][tx + 1][0] = h_edge(1, i, jc, kh, tx + 1, 0, sjh_col, skh_col, tx + 1, 0, cs, ns, false);
         }
         __syncthreads();
-        if (fast) {
-            if (!a.codes || code != LIST_CODE) {
-                const T ca = s_tab[code], cb = s_tab[256 + code];
-                a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(xs(sH[2][r][q], sH[2][r - 1][q]), xs(sH[1][r][q], sH[1][r][q - 1]))));
-                a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(xs(sH[0][r][q], sH[0][r][q - 1]), xs(hz, prevHz))));
-                a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(xs(hy, prevHy), xs(sH[0][r][q], sH[0][r - 1][q]))));
-            }
-        } else if (own && i < a.nx) {
+        if (own && i < a.nx) {
             bool skip;
             if (a.codes) {
                 skip = code == LIST_CODE;
@@ -383,19 +580,50 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_fused(Args<T> a, FusedDims d)
             }
             if (!skip) {
                 const T ca = s_tab[code], cb = s_tab[256 + code];
+                const int sxm = slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on);
                 if (e_updated(a, 0, i, j, k)) {
-                    T tA = e_term(a, 0, 1, j, xs(sH[2][r][q], sH[2][r - 1][q]), i, j, k);
-                    T tB = e_term(a, 1, 2, k, xs(sH[1][r][q], sH[1][r][q - 1]), i, j, k);
+                    T tA = xs(sH[2][r][q], sH[2][r - 1][q]);
+                    T tB = xs(sH[1][r][q], sH[1][r][q - 1]);
+                    if (sjm >= 0) {
+                        T pn;
+                        tA = stretch(tA, es.py[3][r], es.py[4][r], es.py[5][r], a.dx, cs.psi[6][r][q], &pn);
+                        a.psi_e[0][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
+                    }
+                    if (skm >= 0) {
+                        T pn;
+                        tB = stretch(tB, es.pz[3][q], es.pz[4][q], es.pz[5][q], a.dx, cs.psi[7][r][q], &pn);
+                        a.psi_e[1][((long long)i * ny1 + j) * nsmz + skm] = pn;
+                    }
                     a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
                 }
                 if (e_updated(a, 1, i, j, k)) {
-                    T tA = e_term(a, 2, 2, k, xs(sH[0][r][q], sH[0][r][q - 1]), i, j, k);
-                    T tB = e_term(a, 3, 0, i, xs(hz, prevHz), i, j, k);
+                    T tA = xs(sH[0][r][q], sH[0][r][q - 1]);
+                    T tB = xs(hz, prevHz);
+                    if (skm >= 0) {
+                        T pn;
+                        tA = stretch(tA, es.pz[3][q], es.pz[4][q], es.pz[5][q], a.dx, cs.psi[8][r][q], &pn);
+                        a.psi_e[2][((long long)i * ny1 + j) * nsmz + skm] = pn;
+                    }
+                    if (sxm >= 0) {
+                        T pn;
+                        tB = stretch(tB, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, cs.psi[9][r][q], &pn);
+                        a.psi_e[3][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
+                    }
                     a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
                 }
                 if (e_updated(a, 2, i, j, k)) {
-                    T tA = e_term(a, 4, 0, i, xs(hy, prevHy), i, j, k);
-                    T tB = e_term(a, 5, 1, j, xs(sH[0][r][q], sH[0][r - 1][q]), i, j, k);
+                    T tA = xs(hy, prevHy);
+                    T tB = xs(sH[0][r][q], sH[0][r - 1][q]);
+                    if (sxm >= 0) {
+                        T pn;
+                        tA = stretch(tA, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, cs.psi[10][r][q], &pn);
+                        a.psi_e[4][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
+                    }
+                    if (sjm >= 0) {
+                        T pn;
+                        tB = stretch(tB, es.py[3][r], es.py[4][r], es.py[5][r], a.dx, cs.psi[11][r][q], &pn);
+                        a.psi_e[5][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
+                    }
                     a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
                 }
             }
@@ -407,88 +635,98 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_fused(Args<T> a, FusedDims d)
     cp_async_wait<0>();
 }
 
+// ---------------------------------------------------------------------------
+// Instantiations and launch
+// ---------------------------------------------------------------------------
 template <typename T, int TJ, int NS>
-constexpr size_t fused_smem() {
+constexpr size_t interior_smem() {
     return NS * sizeof(FusedStage<T, TJ>) + sizeof(T) * 3 * (TJ + 1) * 33 + sizeof(T) * 512;
 }
+template <typename T, int TJ, int NS>
+constexpr size_t edge_smem() {
+    return NS * sizeof(EdgeStage<T, TJ>) + sizeof(T) * 3 * (TJ + 1) * 33 + sizeof(T) * 512 +
+           sizeof(EdgeShared<T, TJ>);
+}
 
-// Instantiations: FP32 keeps six planes in flight at four CTAs per SM (64
-// registers); FP64 four planes at three CTAs per SM.  TJ = 16 halves the
-// relative halo at the cost of fewer column tiles.
-#define RFB_FUSED_FP32_8 k_fused<float, 8, 6, 4>
-#define RFB_FUSED_FP32_16 k_fused<float, 16, 4, 2>
-#define RFB_FUSED_FP64_8 k_fused<double, 8, 4, 3>
-#define RFB_FUSED_FP64_16 k_fused<double, 16, 3, 1>
+// Interior variants (TJ, NS, CTAs per SM) the autotuner chooses from, and
+// the edge kernels: FP32 edge 3 stages at 3 CTAs/SM, FP64 edge 2 at 2.
+#define RFB_INT_VARIANTS_FP32(X) X(float, 8, 6, 4) X(float, 8, 5, 5) X(float, 16, 4, 3) X(float, 16, 3, 4)
+#define RFB_INT_VARIANTS_FP64(X) X(double, 8, 4, 3) X(double, 16, 2, 2)
+#define RFB_EDGE_FP32 k_sweep_edge<float, 8, 3, 3>
+#define RFB_EDGE_FP64 k_sweep_edge<double, 8, 2, 2>
+
+struct InteriorVariant {
+    int tj, ns, minb;
+};
+static const InteriorVariant kIntVariantsFp32[] = {{8, 6, 4}, {8, 5, 5}, {16, 4, 3}, {16, 3, 4}};
+static const InteriorVariant kIntVariantsFp64[] = {{8, 4, 3}, {16, 2, 2}};
 
 template <typename T>
-void launch_fused(const Args<T> &a, const FusedPlan &p, cudaStream_t st);
+void launch_interior(const Args<T> &a, const FusedPlan &p, cudaStream_t st);
+template <typename T>
+void launch_edge(const Args<T> &a, const FusedPlan &p, cudaStream_t st);
 
+#define RFB_LAUNCH_INT(TT, TJ_, NS_, MB_)                                                                    \
+    if (p.tj == TJ_ && p.ns == NS_)                                                                          \
+        k_sweep_interior<TT, TJ_, NS_, MB_><<<p.n_int, dim3(32, TJ_), interior_smem<TT, TJ_, NS_>(), st>>>( \
+            a, p.d, p.d_int);
 template <>
-inline void launch_fused<float>(const Args<float> &a, const FusedPlan &p, cudaStream_t st) {
-    if (p.tj == 16)
-        RFB_FUSED_FP32_16<<<p.grid, dim3(32, 16), fused_smem<float, 16, 4>(), st>>>(a, p.d);
-    else
-        RFB_FUSED_FP32_8<<<p.grid, dim3(32, 8), fused_smem<float, 8, 6>(), st>>>(a, p.d);
+inline void launch_interior<float>(const Args<float> &a, const FusedPlan &p, cudaStream_t st) {
+    if (!p.n_int) return;
+    RFB_INT_VARIANTS_FP32(RFB_LAUNCH_INT)
+}
+template <>
+inline void launch_interior<double>(const Args<double> &a, const FusedPlan &p, cudaStream_t st) {
+    if (!p.n_int) return;
+    RFB_INT_VARIANTS_FP64(RFB_LAUNCH_INT)
+}
+template <>
+inline void launch_edge<float>(const Args<float> &a, const FusedPlan &p, cudaStream_t st) {
+    if (p.n_edge) RFB_EDGE_FP32<<<p.n_edge, dim3(32, 8), edge_smem<float, 8, 3>(), st>>>(a, p.d, p.d_edge);
+}
+template <>
+inline void launch_edge<double>(const Args<double> &a, const FusedPlan &p, cudaStream_t st) {
+    if (p.n_edge) RFB_EDGE_FP64<<<p.n_edge, dim3(32, 8), edge_smem<double, 8, 2>(), st>>>(a, p.d, p.d_edge);
 }
 
-template <>
-inline void launch_fused<double>(const Args<double> &a, const FusedPlan &p, cudaStream_t st) {
-    if (p.tj == 16)
-        RFB_FUSED_FP64_16<<<p.grid, dim3(32, 16), fused_smem<double, 16, 3>(), st>>>(a, p.d);
-    else
-        RFB_FUSED_FP64_8<<<p.grid, dim3(32, 8), fused_smem<double, 8, 4>(), st>>>(a, p.d);
-}
-
-// Raises the dynamic shared-memory limit of every fused instantiation once.
+// Raises the dynamic shared-memory limit of every sweep instantiation once.
+#define RFB_PREP_INT(TT, TJ_, NS_, MB_)                                                            \
+    if (e == cudaSuccess)                                                                          \
+        e = cudaFuncSetAttribute(k_sweep_interior<TT, TJ_, NS_, MB_>,                             \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)interior_smem<TT, TJ_, NS_>());
 static inline int fused_prepare() {
     static int done = 0;
     if (done) return 0;
-    cudaError_t e = cudaFuncSetAttribute(RFB_FUSED_FP32_8, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fused_smem<float, 8, 6>());
+    cudaError_t e = cudaSuccess;
+    RFB_INT_VARIANTS_FP32(RFB_PREP_INT)
+    RFB_INT_VARIANTS_FP64(RFB_PREP_INT)
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(RFB_FUSED_FP32_16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fused_smem<float, 16, 4>());
+        e = cudaFuncSetAttribute(RFB_EDGE_FP32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)edge_smem<float, 8, 3>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(RFB_FUSED_FP64_8, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fused_smem<double, 8, 4>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(RFB_FUSED_FP64_16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fused_smem<double, 16, 3>());
+        e = cudaFuncSetAttribute(RFB_EDGE_FP64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)edge_smem<double, 8, 2>());
     if (e != cudaSuccess) return -1;
     done = 1;
     return 0;
 }
 
-// Plans the fused sweep.  boundary_active: some source sits on a padded
-// boundary plane (i = nx, j = ny or k = nz of a non-periodic axis), so those
-// planes must be swept too; otherwise they stay zero for the whole run and
-// are skipped.
-static inline int fused_plan_dims(FusedPlan *p, const rfb_geom_t *g, int boundary_active, int tj, int seg_len) {
-    const bool px = g->periodic & 1u, py = g->periodic & 2u, pz = g->periodic & 4u;
-    p->tj = tj;
-    p->d.cj = g->ny + ((boundary_active && !py) ? 1 : 0);
-    p->d.ck = g->nz + ((boundary_active && !pz) ? 1 : 0);
-    p->d.ci = g->nx + ((boundary_active && !px) ? 1 : 0);
-    if (seg_len <= 0 || seg_len > p->d.ci) seg_len = p->d.ci;
-    p->d.seg_len = seg_len;
-    const int nseg = (p->d.ci + seg_len - 1) / seg_len;
-    p->grid = dim3((p->d.ck + 31) / 32, (p->d.cj + tj - 1) / tj, nseg);
-    if (nseg > 65535 || p->grid.y > 65535) return -1;
-    return 0;
-}
-
-// Default plan: TJ = 8 and i-segments sized so the grid holds about
-// eight CTAs per SM of a 148-SM B200.
-static inline int fused_plan_default(FusedPlan *p, const rfb_geom_t *g, int boundary_active) {
-    if (fused_plan_dims(p, g, boundary_active, 8, 0) != 0) return -1;
-    const long long cols = (long long)p->grid.x * p->grid.y;
-    const long long target = 148LL * 8;
-    long long nseg = (target + cols - 1) / cols;
-    long long max_seg = p->d.ci / 8 > 0 ? p->d.ci / 8 : 1;
-    if (nseg > max_seg) nseg = max_seg;
-    if (nseg < 1) nseg = 1;
-    const int seg_len = (int)((p->d.ci + nseg - 1) / nseg);
-    return fused_plan_dims(p, g, boundary_active, 8, seg_len);
+// Interior range [lo, hi) of an axis: indices whose profiles are the identity
+// on both staggered grids and where every component is swept (index >= 1 on a
+// non-periodic axis).
+static inline void interior_axis(int lo_h, int hi_h, int lo_m, int hi_m, int n, bool periodic, bool cpml, int *lo,
+                                 int *hi) {
+    if (periodic) {
+        *lo = 0;
+        *hi = n;
+        return;
+    }
+    *lo = 1;
+    *hi = n;
+    if (cpml) {
+        *lo = std::max(*lo, std::max(lo_h, lo_m));
+        *hi = std::min(*hi, std::min(hi_h, hi_m));
+    }
 }
 
 }  // namespace rfb
