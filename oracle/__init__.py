@@ -171,6 +171,8 @@ def build(ref: bool = True) -> None:
 
 def build_driver() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "driver"], check=True)
+    if Path("/root/reference/engine/fdtd/grid.c").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "validators"], check=True)
 
 
 _libs: dict[str, C.CDLL] = {}

@@ -184,6 +184,13 @@ static void fill_cpml_args(Args<T> &a, const DevCpml &c, int hin, int hout) {
     }
 }
 
+// Contiguous rows of `row` bytes into rows of `pitch` bytes.
+__global__ void k_repack_u8(uint8_t *dst, const uint8_t *src, long long row, long long pitch, long long n) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    dst[(t / row) * pitch + (t % row)] = src[t];
+}
+
 // ---------------------------------------------------------------------------
 // Scene on the device: code volume, coefficient table, interface list.
 // ---------------------------------------------------------------------------
@@ -237,10 +244,26 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
     s.n_cells = img ? (int)img->n_cells : 0;
     if (img && img->codes) {
         if (cudaMalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
-        if (cudaMemcpy2D(s.codes, pitch, img->codes, g->nz + 1, g->nz + 1, (size_t)(g->nx + 1) * (g->ny + 1),
-                         cudaMemcpyHostToDevice) != cudaSuccess) {
-            rfb_set_error("code volume upload failed");
-            return -1;
+        const size_t rows = (size_t)(g->nx + 1) * (g->ny + 1), row = (size_t)g->nz + 1;
+        if (pitch == (long long)row) {
+            if (cudaMemcpy(s.codes, img->codes, rows * row, cudaMemcpyHostToDevice) != cudaSuccess) {
+                rfb_set_error("code volume upload failed");
+                return -1;
+            }
+        } else {
+            // one contiguous upload, then a device-side repack into the
+            // pitched layout (a strided host copy of short rows is slow)
+            uint8_t *tmp = nullptr;
+            if (cudaMalloc(&tmp, rows * row) != cudaSuccess) { rfb_set_error("code volume staging failed"); return -1; }
+            cudaError_t ce = cudaMemcpy(tmp, img->codes, rows * row, cudaMemcpyHostToDevice);
+            if (ce == cudaSuccess) {
+                const long long n = (long long)(rows * row);
+                k_repack_u8<<<(unsigned)((n + 255) / 256), 256>>>(s.codes, tmp, (long long)row, pitch, n);
+                g_launches++;
+                ce = cudaDeviceSynchronize();
+            }
+            cudaFree(tmp);
+            if (ce != cudaSuccess) { rfb_set_error("code volume upload failed"); return -1; }
         }
     }
     if (s.n_cells) {
@@ -1064,10 +1087,14 @@ struct rfb_scene_dev {
     DevScene s;
 };
 
+// The step-wise API keeps rfsyn's own unpadded layout (pitch nz+1) on the
+// device, so each host array moves with one contiguous copy.
+static long long step_pitch(int nz) { return nz + 1; }
+
 extern "C" rfb_fields_t *rfb_fields_create(const rfb_geom_t *geom) {
     rfb_fields *f = new rfb_fields();
     f->g = *geom;
-    f->pitch = pitch_for(geom->nz, 8);
+    f->pitch = step_pitch(geom->nz);
     f->total = (size_t)(geom->nx + 1) * (geom->ny + 1) * f->pitch;
     CK(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
     for (int c = 0; c < 6; c++) CK(cudaMalloc(&f->f[c], f->total * 8));
@@ -1087,7 +1114,7 @@ extern "C" void rfb_fields_destroy(rfb_fields_t *f) {
 extern "C" rfb_cpml_dev_t *rfb_cpml_dev_create(const rfb_geom_t *geom, const rfb_cpml_desc_t *desc) {
     rfb_cpml_dev *c = new rfb_cpml_dev();
     c->nx = geom->nx; c->ny = geom->ny; c->nz = geom->nz;
-    if (devcpml_init(c->c, geom, desc, RFB_FP64, pitch_for(geom->nz, 8), 1) != 0) {
+    if (devcpml_init(c->c, geom, desc, RFB_FP64, step_pitch(geom->nz), 1) != 0) {
         devcpml_free(c->c);
         delete c;
         return nullptr;
@@ -1101,7 +1128,7 @@ extern "C" void rfb_cpml_dev_destroy(rfb_cpml_dev_t *c) {
 }
 extern "C" rfb_scene_dev_t *rfb_scene_dev_create(const rfb_geom_t *geom, const rfb_scene_image_t *img) {
     rfb_scene_dev *s = new rfb_scene_dev();
-    if (devscene_init(s->s, geom, img, RFB_FP64, pitch_for(geom->nz, 8)) != 0) {
+    if (devscene_init(s->s, geom, img, RFB_FP64, step_pitch(geom->nz)) != 0) {
         devscene_free(s->s);
         delete s;
         return nullptr;
@@ -1117,13 +1144,10 @@ extern "C" void rfb_scene_dev_destroy(rfb_scene_dev_t *s) {
 static int fields_xfer(rfb_fields *f, double *const host[6], int first, int count, bool up) {
     const rfb_geom_t &g = f->g;
     const size_t rows = (size_t)(g.nx + 1) * (g.ny + 1);
+    const size_t bytes = rows * (size_t)(g.nz + 1) * 8;
     for (int c = first; c < first + count; c++) {
-        if (up)
-            CK(cudaMemcpy2DAsync(f->f[c], f->pitch * 8, host[c], (g.nz + 1) * 8, (g.nz + 1) * 8, rows,
-                                 cudaMemcpyHostToDevice, f->stream));
-        else
-            CK(cudaMemcpy2DAsync(host[c], (g.nz + 1) * 8, f->f[c], f->pitch * 8, (g.nz + 1) * 8, rows,
-                                 cudaMemcpyDeviceToHost, f->stream));
+        if (up) CK(cudaMemcpyAsync(f->f[c], host[c], bytes, cudaMemcpyHostToDevice, f->stream));
+        else CK(cudaMemcpyAsync(host[c], f->f[c], bytes, cudaMemcpyDeviceToHost, f->stream));
     }
     return 0;
 fail:

@@ -41,7 +41,40 @@ def main() -> None:
     r = oracle.run_ref(c1_scene())
     np.savez_compressed(OUT / "c1.npz", td=r["td"], dft=r["dft"])
     print("c1", r["td"].shape, float(np.abs(r["td"]).max()))
+    validators()
+
+
+# rfsyn's validators and unit tests with the arguments its CTest passes
+# (CMakeLists.txt:266-305; stability at the minimum RFSYN_STABILITY_STEPS)
+VALIDATOR_ARGS = {
+    "simulate_unit": [], "materials_unit": [], "materials_tensor_unit": [], "periodic_materials_unit": [],
+    "periodic_wrapping_unit": [], "validate_cpml": [], "validate_cpml_margin": [], "validate_cpml_planewave": [],
+    "validate_materials_fresnel": [], "validate_probe_dft": [], "validate_materials_energy": [],
+    "validate_cpml_oblique": [], "validate_materials_high_contrast": ["--full"],
+    "validate_long_term_stability": ["--steps", "10000"], "validate_materials_tilted": [],
+    "audit_periodic_energy": [],
+}
+
+
+def validators() -> None:
+    """stdout of rfsyn's validators linked against rfsyn itself."""
+    import subprocess
+    import tempfile
+
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "validators_ref"], check=True)
+    dst = OUT / "validators"
+    dst.mkdir(exist_ok=True)
+    for name, args in VALIDATOR_ARGS.items():
+        with tempfile.TemporaryDirectory() as wd:
+            r = subprocess.run([str(ROOT / "oracle" / "_ref" / "validators_ref" / name), *args], cwd=wd,
+                               capture_output=True, text=True, timeout=1800)
+        assert r.returncode == 0, (name, r.stdout, r.stderr)
+        (dst / f"{name}.txt").write_text(r.stdout)
+        print(name, "ok", len(r.stdout.splitlines()), "lines")
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "validators":
+        validators()
+    else:
+        main()
