@@ -121,7 +121,11 @@ typedef struct {
     size_t slab_cell_axes;   /* sum over cells of the CPML slab axes containing them */
     size_t h2d_bytes;        /* scene bytes uploaded at creation */
     int precision, schedule;
-    int tile_j, seg_len;     /* fused sweep plan */
+    int tile_j, seg_len;     /* fused sweep plan: rows per interior tile, planes per work item */
+    int ring_depth;          /* planes staged per interior CTA */
+    int tma;                 /* 1: interior planes staged by the Tensor Memory Accelerator */
+    int interior_items;      /* work items of the interior sweep (CTAs per step) */
+    int edge_items;          /* work items of the edge sweep */
 } fdtd_b200_sim_info_t;
 
 int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info);

@@ -94,7 +94,9 @@ class Sphere(C.Structure):
 class SimInfo(C.Structure):
     _fields_ = [("cells", C.c_size_t), ("list_cells", C.c_size_t), ("dispersive", C.c_size_t),
                 ("slab_cell_axes", C.c_size_t), ("h2d_bytes", C.c_size_t), ("precision", C.c_int),
-                ("schedule", C.c_int), ("tile_j", C.c_int), ("seg_len", C.c_int)]
+                ("schedule", C.c_int), ("tile_j", C.c_int), ("seg_len", C.c_int),
+                ("ring_depth", C.c_int), ("tma", C.c_int), ("interior_items", C.c_int),
+                ("edge_items", C.c_int)]
 
 
 SETUP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)

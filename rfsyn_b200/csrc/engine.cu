@@ -14,6 +14,7 @@
 #include "engine.h"
 #include "kernels.cuh"
 #include "fused.cuh"
+#include "tma.cuh"
 
 using namespace rfb;
 
@@ -387,6 +388,8 @@ struct rfb_engine {
     cudaGraphExec_t g1[2] = {nullptr, nullptr}, gk[2] = {nullptr, nullptr};
     int launches_per_step = 0;
     FusedPlan plan;
+    TmaMaps tmaps[2];       // tensor maps of the input buffers per parity (TMA interior sweep)
+    int *d_err = nullptr;   // set by a sweep whose copies did not complete in time
     size_t h2d_bytes = 0, n_ade = 0;
 };
 
@@ -411,6 +414,13 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
     return a;
 }
 
+// Interior sweep of the plan: TMA-fed or cp.async-fed variant.
+template <typename T>
+static void launch_int(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
+    if (e->plan.tma) launch_interior_tma<T>(a, e->plan, e->tmaps[e->nbuf == 2 ? par : 0], e->d_err, st);
+    else launch_interior<T>(a, e->plan, st);
+}
+
 template <typename T>
 static void enqueue_step(rfb_engine *e, int par) {
     Args<T> a = engine_args<T>(e, par);
@@ -419,7 +429,7 @@ static void enqueue_step(rfb_engine *e, int par) {
         // interior and edge sweeps touch disjoint cells: run them side by side
         cudaEventRecord(e->ev_fork, e->stream);
         cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
-        launch_interior<T>(a, e->plan, e->stream);
+        launch_int<T>(e, a, par, e->stream);
         launch_edge<T>(a, e->plan, e->stream2);
         cudaEventRecord(e->ev_join, e->stream2);
         cudaStreamWaitEvent(e->stream, e->ev_join, 0);
@@ -477,13 +487,75 @@ static void free_plan_lists(FusedPlan &p) {
     p.n_int = p.n_edge = 0;
 }
 
-static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int seg_int, int seg_edge) {
+// ---- tensor maps of the TMA interior sweep -----------------------------------
+// Each field array (and the code volume) is a 3-D tensor (pitch, ny+1, nx+1),
+// k fastest; boxes are (40 | 36 | 32) x rows x 1 plane.  Out-of-range boxes
+// parts read as zero (no NaN fill).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)f;
+    });
+    return fn;
+}
+
+static int encode_map(CUtensorMap *m, void *base, CUtensorMapDataType dt, size_t esz, const rfb_geom_t &g,
+                      size_t pitch, unsigned box_w, unsigned box_h) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        rfb_set_error("the CUDA driver does not provide cuTensorMapEncodeTiled");
+        return -1;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)g.ny + 1, (cuuint64_t)g.nx + 1};
+    const cuuint64_t strides[2] = {(cuuint64_t)(pitch * esz), (cuuint64_t)(pitch * esz * (g.ny + 1))};
+    const cuuint32_t box[3] = {box_w, box_h, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        rfb_set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return -1;
+    }
+    return 0;
+}
+
+static int build_tma_maps(rfb_engine *e, int tj) {
+    const CUtensorMapDataType dt =
+        e->prec == RFB_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    for (int par = 0; par < 2; par++) {
+        const int in = e->nbuf == 2 ? par : 0;
+        TmaMaps &m = e->tmaps[par];
+        memset(&m, 0, sizeof m);
+        for (int c = 0; c < 3; c++) {
+            if (encode_map(&m.e[c], e->fld[in][c], dt, e->esz, e->g, e->pitch, TMA_EW, tj + 2)) return -1;
+            if (encode_map(&m.h[c], e->fld[in][3 + c], dt, e->esz, e->g, e->pitch, TMA_HW, tj + 1)) return -1;
+        }
+        if (e->scene.codes &&
+            encode_map(&m.code, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 32, tj))
+            return -1;
+    }
+    return 0;
+}
+
+static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge) {
     const rfb_geom_t &g = e->g;
     const bool px = g.periodic & 1u, py = g.periodic & 2u, pz = g.periodic & 4u;
     FusedPlan &p = e->plan;
     free_plan_lists(p);
     p.tj = tj;
     p.ns = ns;
+    p.tma = tma;
     p.seg_int = seg_int;
     p.seg_edge = seg_edge;
     p.d.cj = g.ny + ((active && !py) ? 1 : 0);
@@ -509,8 +581,10 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int seg_i
     for (int j0 = 0; j0 < p.d.cj; j0 += tj)
         for (int k0 = 0; k0 < p.d.ck; k0 += 32) {
             const bool full = j0 + tj <= p.d.cj && k0 + 32 <= p.d.ck;
-            const bool yok = py ? j0 + tj <= g.ny : (j0 - 1 >= ylo && j0 + tj <= yhi);
-            const bool zok = pz ? k0 + 32 <= g.nz : (k0 - 1 >= zlo && k0 + 32 <= zhi);
+            // the interior sweeps read the halo without wrapping it: on a
+            // periodic axis the tiles at either end stay on the edge sweep
+            const bool yok = py ? (j0 >= 1 && j0 + tj < g.ny) : (j0 - 1 >= ylo && j0 + tj <= yhi);
+            const bool zok = pz ? (k0 >= 32 && k0 + 32 < g.nz) : (k0 - 1 >= zlo && k0 + 32 <= zhi);
             bool skipcell = false;
             for (int s = 0; s < e->scene.n_skip; s++) {
                 const long long c = e->scene.skip[s];
@@ -531,9 +605,25 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int seg_i
     if (p.n_edge) CK(cudaMalloc(&p.d_edge, ve.size() * sizeof(SweepItem)));
     if (p.n_int) CK(cudaMemcpy(p.d_int, vi.data(), vi.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_edge) CK(cudaMemcpy(p.d_edge, ve.data(), ve.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
+    if (tma && p.n_int && build_tma_maps(e, tj) != 0) return -1;
     return 0;
 fail:
     return -1;
+}
+
+static bool plan_variant_known(int prec, int tj, int ns, int tma) {
+    const InteriorVariant *v;
+    size_t n;
+    if (prec == RFB_FP32) {
+        v = tma ? kTmaVariantsFp32 : kIntVariantsFp32;
+        n = tma ? std::size(kTmaVariantsFp32) : std::size(kIntVariantsFp32);
+    } else {
+        v = tma ? kTmaVariantsFp64 : kIntVariantsFp64;
+        n = tma ? std::size(kTmaVariantsFp64) : std::size(kIntVariantsFp64);
+    }
+    for (size_t q = 0; q < n; q++)
+        if (v[q].tj == tj && v[q].ns == ns) return true;
+    return false;
 }
 
 // ---- autotuner ---------------------------------------------------------------
@@ -542,7 +632,7 @@ fail:
 // on the engine's own scene; the choice is cached per geometry.  Every
 // candidate computes bit-identical fields, so tuning changes speed only.
 struct TunedPlan {
-    int tj, ns, seg_int, seg_edge;
+    int tj, ns, tma, seg_int, seg_edge;
 };
 
 static std::mutex g_tune_mu;
@@ -553,7 +643,7 @@ static void enqueue_sweep(rfb_engine *e, int par) {
     Args<T> a = engine_args<T>(e, par);
     cudaEventRecord(e->ev_fork, e->stream);
     cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
-    launch_interior<T>(a, e->plan, e->stream);
+    launch_int<T>(e, a, par, e->stream);
     launch_edge<T>(a, e->plan, e->stream2);
     cudaEventRecord(e->ev_join, e->stream2);
     cudaStreamWaitEvent(e->stream, e->ev_join, 0);
@@ -572,14 +662,24 @@ static int autotune(rfb_engine *e, int active) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         for (auto &kv : g_tune_cache)
             if (kv.first == key)
-                return build_sweep_plan(e, active, kv.second.tj, kv.second.ns, kv.second.seg_int, kv.second.seg_edge);
+                return build_sweep_plan(e, active, kv.second.tj, kv.second.ns, kv.second.tma, kv.second.seg_int,
+                                        kv.second.seg_edge);
     }
-    std::vector<InteriorVariant> vars;
-    if (e->prec == RFB_FP32) vars.assign(std::begin(kIntVariantsFp32), std::end(kIntVariantsFp32));
-    else vars.assign(std::begin(kIntVariantsFp64), std::end(kIntVariantsFp64));
+    struct Cand {
+        InteriorVariant v;
+        int tma;
+    };
+    std::vector<Cand> vars;
+    if (e->prec == RFB_FP32) {
+        for (const InteriorVariant &v : kTmaVariantsFp32) vars.push_back({v, 1});
+        for (const InteriorVariant &v : kIntVariantsFp32) vars.push_back({v, 0});
+    } else {
+        for (const InteriorVariant &v : kTmaVariantsFp64) vars.push_back({v, 1});
+        for (const InteriorVariant &v : kIntVariantsFp64) vars.push_back({v, 0});
+    }
     const int segs_int[] = {32, 64, 128};
     const int segs_edge[] = {16, 32};
-    TunedPlan best = {vars[0].tj, vars[0].ns, 64, 32};
+    TunedPlan best = {vars[0].v.tj, vars[0].v.ns, vars[0].tma, 64, 32};
     float best_ms = 1e30f;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     CK(cudaEventCreate(&t0));
@@ -588,10 +688,11 @@ static int autotune(rfb_engine *e, int active) {
         const long long cells = (long long)g.nx * g.ny * g.nz;
         const int reps = cells > (1 << 22) ? 3 : 6;
         int par = 0;
-        for (const InteriorVariant &v : vars)
+        for (const Cand &cv : vars)
             for (int si : segs_int)
                 for (int se : segs_edge) {
-                    if (build_sweep_plan(e, active, v.tj, v.ns, si, se) != 0) goto fail;
+                    const InteriorVariant &v = cv.v;
+                    if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se) != 0) goto fail;
                     for (int w = 0; w < 2; w++) {
                         if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
                         else enqueue_sweep<float>(e, par);
@@ -609,7 +710,7 @@ static int autotune(rfb_engine *e, int active) {
                     CK(cudaEventElapsedTime(&ms, t0, t1));
                     if (ms < best_ms) {
                         best_ms = ms;
-                        best = TunedPlan{v.tj, v.ns, si, se};
+                        best = TunedPlan{v.tj, v.ns, cv.tma, si, se};
                     }
                 }
     }
@@ -619,7 +720,16 @@ static int autotune(rfb_engine *e, int active) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         g_tune_cache.push_back({key, best});
     }
-    if (build_sweep_plan(e, active, best.tj, best.ns, best.seg_int, best.seg_edge) != 0) return -1;
+    if (build_sweep_plan(e, active, best.tj, best.ns, best.tma, best.seg_int, best.seg_edge) != 0) return -1;
+    {
+        // a timed-out copy during tuning would have left the error flag set
+        int err = 0;
+        CK(cudaMemcpy(&err, e->d_err, sizeof err, cudaMemcpyDeviceToHost));
+        if (err) {
+            rfb_set_error("a sweep's tensor copies did not complete in time");
+            return -1;
+        }
+    }
     // the tuning sweeps advanced the fields: start from the zero state again
     if (rfb_engine_reset(e) != 0) return -1;
     CK(cudaStreamSynchronize(e->stream));
@@ -642,7 +752,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     devcpml_free(e->cpml);
     devscene_free(e->scene);
     cudaFree(e->src_val); cudaFree(e->src_hard);
-    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step);
+    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
     cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
@@ -706,6 +816,8 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
     }
     CK(cudaMalloc(&e->d_step, sizeof(int)));
     CK(cudaMemset(e->d_step, 0, sizeof(int)));
+    CK(cudaMalloc(&e->d_err, sizeof(int)));
+    CK(cudaMemset(e->d_err, 0, sizeof(int)));
     if (schedule == RFB_SCHED_FUSED) {
         if (fused_prepare() != 0) {
             rfb_set_error("cannot configure the sweep kernels' shared memory");
@@ -721,16 +833,26 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
         CK(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
-        // plan: "tj,ns,seg_interior,seg_edge" from RFSYN_FDTD_PLAN, the
-        // autotuner (default) or, with RFSYN_FDTD_TUNE=0, the first variant
+        if (tma_prepare() != 0) {
+            rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
+            goto fail_noset;
+        }
+        // plan: "tj,ns,seg_interior,seg_edge[,tma]" from RFSYN_FDTD_PLAN,
+        // the autotuner (default) or, with RFSYN_FDTD_TUNE=0, the first
+        // TMA variant
         const char *ov = getenv("RFSYN_FDTD_PLAN");
         const char *tune = getenv("RFSYN_FDTD_TUNE");
-        int a1 = 0, a2 = 0, a3 = 0, a4 = 0;
+        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
         int rc;
-        if (ov && sscanf(ov, "%d,%d,%d,%d", &a1, &a2, &a3, &a4) == 4 && a3 > 0 && a4 > 0)
-            rc = build_sweep_plan(e, active, a1, a2, a3, a4);
+        const int nov = ov ? sscanf(ov, "%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5) : 0;
+        if (nov >= 4 && a3 > 0 && a4 > 0 && plan_variant_known(precision, a1, a2, nov == 5 ? a5 : 0))
+            rc = build_sweep_plan(e, active, a1, a2, nov == 5 ? a5 : 0, a3, a4);
+        else if (ov)
+            rc = (rfb_set_error("RFSYN_FDTD_PLAN=\"%s\" names no sweep variant", ov), -1);
         else if (tune && !strcmp(tune, "0"))
-            rc = build_sweep_plan(e, active, 8, precision == RFB_FP32 ? 6 : 4, 64, 32);
+            rc = build_sweep_plan(e, active, precision == RFB_FP32 ? kTmaVariantsFp32[0].tj : kTmaVariantsFp64[0].tj,
+                                  precision == RFB_FP32 ? kTmaVariantsFp32[0].ns : kTmaVariantsFp64[0].ns, 1, 64,
+                                  32);
         else
             rc = autotune(e, active);
         if (rc != 0) goto fail_noset;
@@ -828,6 +950,10 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->h2d_bytes = e->h2d_bytes;
     out->tile_j = e->plan.tj;
     out->seg_len = e->plan.seg_int;
+    out->ring_depth = e->plan.ns;
+    out->tma = e->plan.tma;
+    out->interior_items = e->plan.n_int;
+    out->edge_items = e->plan.n_edge;
     size_t sca = 0;
     if (e->cpml.on) {
         // cells of the swept volume inside the slab of each axis (H profiles)
@@ -857,7 +983,7 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         if (e->sched == RFB_SCHED_FUSED) {
             cudaEventRecord(e->ev_fork, e->stream);
             cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
-            launch_interior<T>(a, e->plan, e->stream);
+            launch_int<T>(e, a, par, e->stream);
             launch_edge<T>(a, e->plan, e->stream2);
             cudaEventRecord(e->ev_join, e->stream2);
             cudaStreamWaitEvent(e->stream, e->ev_join, 0);
@@ -912,9 +1038,22 @@ extern "C" int rfb_engine_time_kernels(rfb_engine_t *e, size_t n, double *sweep_
                                : time_kernels_t<float>(e, n, sweep_ms, other_ms);
 }
 
+// After the stream drained: did a sweep give up on its copies?
+static int check_sweep_error(rfb_engine *e) {
+    int err = 0;
+    CK(cudaMemcpy(&err, e->d_err, sizeof err, cudaMemcpyDeviceToHost));
+    if (err) {
+        rfb_set_error("a sweep's tensor copies did not complete in time");
+        return -1;
+    }
+    return 0;
+fail:
+    return -1;
+}
+
 extern "C" int rfb_engine_sync(rfb_engine_t *e) {
     CK(cudaStreamSynchronize(e->stream));
-    return 0;
+    return check_sweep_error(e);
 fail:
     return -1;
 }
@@ -927,6 +1066,7 @@ extern "C" int rfb_engine_read_probes(rfb_engine_t *e, double *out) {
     size_t n = (size_t)e->n_probes * e->n_steps;
     if (!n) return 0;
     CK(cudaStreamSynchronize(e->stream));
+    if (check_sweep_error(e) != 0) return -1;
     if (e->prec == RFB_FP64) {
         CK(cudaMemcpy(out, e->ts, n * 8, cudaMemcpyDeviceToHost));
     } else {
@@ -980,6 +1120,7 @@ extern "C" int rfb_engine_read_field(rfb_engine_t *e, int component, double *hos
     const int buf = e->nbuf == 2 ? e->parity : 0;
     const size_t rows = (size_t)(g.nx + 1) * (g.ny + 1);
     CK(cudaStreamSynchronize(e->stream));
+    if (check_sweep_error(e) != 0) return -1;
     if (e->prec == RFB_FP64) {
         CK(cudaMemcpy2D(host, (g.nz + 1) * 8, e->fld[buf][component], e->pitch * 8, (g.nz + 1) * 8, rows,
                         cudaMemcpyDeviceToHost));

@@ -42,6 +42,7 @@ struct SweepItem {
 
 struct FusedPlan {
     int tj = 8, ns = 6;   // interior variant (rows per tile, ring depth)
+    int tma = 0;          // interior planes staged by the TMA (1) or per-thread cp.async (0)
     FusedDims d;
     int seg_int = 64, seg_edge = 32;
     int n_int = 0, n_edge = 0;

@@ -252,6 +252,10 @@ int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info) {
     info->schedule = sim->schedule;
     info->tile_j = ei.tile_j;
     info->seg_len = ei.seg_len;
+    info->ring_depth = ei.ring_depth;
+    info->tma = ei.tma;
+    info->interior_items = ei.interior_items;
+    info->edge_items = ei.edge_items;
     return 0;
 }
 

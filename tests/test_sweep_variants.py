@@ -1,0 +1,95 @@
+"""Every interior sweep variant the autotuner may pick (TMA-fed and
+cp.async-fed, each tile height and ring depth) on scenes large enough to
+have interior work items: FP64 probe series bit-equal to the CPU oracle.
+
+The sweep variant is forced per session with RFSYN_FDTD_PLAN
+("rows,ring,seg_interior,seg_edge,tma"); the session's info confirms that
+the interior sweep ran with that variant and had work."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+import rfsyn_b200 as rb
+from oracle import Scene
+from rfsyn_b200 import scenes
+from tests.cases import DT1, scene_run_config, workload_to_scene
+
+pytestmark = pytest.mark.gpu
+
+# (rows per tile, ring depth, tma) of every compiled interior variant
+VARIANTS = {
+    rb.FP64: [(8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
+    rb.FP32: [(8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0), (16, 4, 0), (16, 3, 0)],
+}
+
+SCENES = {
+    # the headline recipe at 104^3 (5-cell CPML): interior tiles at k0 = 32, 64
+    "c2_104": workload_to_scene(scenes.scaled(scenes.c2(), 104, 120)),
+    # periodic y and z (the halo of the end tiles would wrap), CPML on x
+    "periodic_yz_cpml_x": Scene(
+        nx=24, ny=41, nz=100, n_steps=80, periodic=6, npml=4,
+        boxes=[(6, 18, 10, 30, 40, 80, 4.0, 0.01)],
+        comps=[(2, 12, 20, 50, 7.0, 0.0), (0, 12, 20, 70, 3.0, 0.02)],
+        sources=[(12, 20, 60, 2, 0, 1.0, 0, 20 * DT1, 5 * DT1, 0.0)],
+        probes=[(14, 22, 62, 2), (12, 0, 3, 0), (8, 30, 45, 1)], freqs=[30e9]),
+    # fully periodic: interior items start at plane 0 and wrap to nx-1
+    "periodic_all": Scene(
+        nx=18, ny=41, nz=100, n_steps=60, periodic=7,
+        boxes=[(3, 12, 10, 25, 35, 70, 2.5, 0.0)],
+        sources=[(9, 15, 50, 1, 0, 1.0, 0, 15 * DT1, 4 * DT1, 0.0)],
+        probes=[(0, 15, 50, 1), (17, 10, 40, 2), (9, 29, 99, 0)]),
+}
+
+
+@pytest.fixture(scope="module")
+def wants():
+    return {name: oracle.run_oracle(s) for name, s in SCENES.items()}
+
+
+def _run(s: Scene, precision: int, variant, monkeypatch):
+    tj, ns, tma = variant
+    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma}")
+    rc = scene_run_config(s, precision, rb.FUSED)
+    cs = s.to_c()
+    needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres)
+    sim = rb.Sim(rc, oracle.device_setup() if needs_setup else None,
+                 C.cast(C.pointer(cs), C.c_void_p) if needs_setup else None)
+    try:
+        info = sim.info()
+        assert (info.tile_j, info.ring_depth, info.tma) == (tj, ns, tma)
+        assert info.interior_items > 0 and info.edge_items > 0
+        sim.advance(s.n_steps)
+        return sim.probes(), sim.dft()
+    finally:
+        sim.close()
+
+
+@pytest.mark.parametrize("variant", VARIANTS[rb.FP64], ids=lambda v: "tj%d_ns%d_%s" % (v[0], v[1], "tma" if v[2] else "cpasync"))
+@pytest.mark.parametrize("name", list(SCENES))
+def test_interior_variant_fp64_bit_exact(wants, name, variant, monkeypatch):
+    td, _ = _run(SCENES[name], rb.FP64, variant, monkeypatch)
+    assert np.array_equal(td, wants[name]["td"])
+
+
+@pytest.mark.parametrize("variant", VARIANTS[rb.FP32], ids=lambda v: "tj%d_ns%d_%s" % (v[0], v[1], "tma" if v[2] else "cpasync"))
+def test_interior_variants_fp32_agree(wants, variant, monkeypatch):
+    """All FP32 variants evaluate the same expressions in the same order:
+    identical probe series; and within the FP32 bound of the FP64 oracle."""
+    s = SCENES["c2_104"]
+    td, _ = _run(s, rb.FP32, variant, monkeypatch)
+    ref, _ = _run(s, rb.FP32, VARIANTS[rb.FP32][-1], monkeypatch)
+    assert np.array_equal(td, ref)
+    want = wants["c2_104"]["td"]
+    err = np.linalg.norm(td - want) / np.linalg.norm(want)
+    assert err < 1e-3, err
+
+
+def test_plan_override_rejects_unknown_variant(monkeypatch):
+    monkeypatch.setenv("RFSYN_FDTD_PLAN", "12,7,32,16,1")
+    s = SCENES["periodic_all"]
+    with pytest.raises(RuntimeError, match="names no sweep variant"):
+        rb.Sim(scene_run_config(s, rb.FP64, rb.FUSED))
