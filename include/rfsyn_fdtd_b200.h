@@ -135,6 +135,26 @@ int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info);
  * kernel(s), *other_ms = the interface-list and probe kernels. */
 int fdtd_b200_sim_time_kernels(fdtd_b200_sim_t *sim, size_t n_steps, double *sweep_ms, double *other_ms);
 
+/* FP64 energy audit of the resident fields after `steps_done` = n steps
+ * (replaces the host loops of validate_long_term_stability.c:166-209 and
+ * audit_periodic_energy.c:43-71): sums over i < nx, j < ny, k < nz of
+ * 0.5 eps E^2 and 0.5 mu0 H^2 times dx^3, eps = dt / (dx Cb) from each
+ * component's scalar Cb (validate_long_term_stability.c:74-75).  FP64
+ * accumulation whatever the field precision; deterministic.  interior_j
+ * covers planes x_lo <= i < x_hi.  With the fused schedule the previous
+ * step's fields are resident too: electric_prev_j is the energy of E^{n-1},
+ * cross_j = 0.5 mu0 H^{n-3/2} . H^{n-1/2} dx^3, and modified_prev_j their sum,
+ * the audit's modified energy at step n-1; NaN with the split schedule or
+ * before the first step. */
+typedef struct {
+    double electric_j, magnetic_j, total_j, interior_j;
+    double electric_prev_j, cross_j, modified_prev_j;
+    double max_abs_e, max_abs_h;
+    size_t nonfinite;
+} fdtd_b200_energy_t;
+
+int fdtd_b200_sim_energy(fdtd_b200_sim_t *sim, int x_lo, int x_hi, fdtd_b200_energy_t *out);
+
 /* ---- dispersive media (auxiliary differential equations) ----------------------
  * rfsyn models only static eps_r and sigma (engine/fdtd/materials.c:92-125);
  * these entry points add per-component dispersive samples integrated with

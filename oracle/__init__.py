@@ -247,6 +247,21 @@ def fields_stepwise(scene: Scene, initial=None):
     return _run_fields(_load(DRIVER_LIB, "scn"), "scn", scene, initial)
 
 
+def energy_oracle(scene: Scene, x_lo: int = 0, x_hi: int | None = None) -> dict:
+    """The oracle's energy audit after the scene's n_steps (orc_energy)."""
+    lib = _load(ORACLE_LIB, "orc")
+    f = lib.orc_energy
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(ScnScene), C.c_int, C.c_int, C.POINTER(C.c_double)]
+    q = (C.c_double * 9)()
+    s = scene.to_c()
+    if f(C.byref(s), x_lo, scene.nx if x_hi is None else x_hi, q) != 0:
+        raise RuntimeError("orc_energy failed")
+    names = ("electric_j", "magnetic_j", "interior_e_j", "interior_h_j", "electric_prev_j", "cross_j",
+             "max_abs_e", "max_abs_h", "nonfinite")
+    return dict(zip(names, list(q)))
+
+
 def device_setup():
     """scn_setup of the product-linked driver as a C function pointer."""
     lib = _load(DRIVER_LIB, "scn")

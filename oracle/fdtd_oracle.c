@@ -548,5 +548,56 @@ out:
     return rc;
 }
 
+/* Energy audit after the scene's n_steps steps, in the loop order of rfsyn's
+ * validate_long_term_stability.c:166-209 (eps = dt / (dx Cb) from the
+ * component's scalar coefficient, :74-75) and, for the modified energy, of
+ * audit_periodic_energy.c:53-62 applied to the last step: E^{n-1} energy and
+ * 0.5 mu0 H^{n-3/2} . H^{n-1/2}.  q: electric, magnetic, electric and
+ * magnetic over planes x_lo <= i < x_hi, electric of E^{n-1}, cross term,
+ * max |E|, max |H|, non-finite count (energies times dx^3). */
+int orc_energy(const scn_scene_t *s, int x_lo, int x_hi, double *q) {
+    orc_t o;
+    int rc = -1;
+    double *prev = NULL;
+    if (orc_init(&o, s) != 0) goto out;
+    prev = malloc(6 * o.total * sizeof(double));
+    if (!prev) goto out;
+    for (size_t n = 0; n < s->n_steps; n++) {
+        if (n + 1 == s->n_steps)
+            for (int c = 0; c < 6; c++) memcpy(prev + c * o.total, field(&o, c), o.total * 8);
+        step(&o, s, n);
+    }
+    for (int v = 0; v < 9; v++) q[v] = 0.0;
+    for (size_t i = 0; i < o.n[0]; i++)
+        for (size_t j = 0; j < o.n[1]; j++)
+            for (size_t k = 0; k < o.n[2]; k++) {
+                size_t w = at(&o, i, j, k);
+                int inside = (int)i >= x_lo && (int)i < x_hi;
+                for (int c = 0; c < 3; c++) {
+                    double cb = o.has_ovr[c][w] ? o.ocb[c][w] : o.tcb[o.id[w]];
+                    double eps = o.dt / (o.dx * cb);
+                    double ev = o.E[c][w], hv = o.H[c][w];
+                    double ep = prev[c * o.total + w], hp = prev[(3 + c) * o.total + w];
+                    if (!isfinite(ev)) q[8] += 1.0;
+                    if (!isfinite(hv)) q[8] += 1.0;
+                    q[6] = fmax(q[6], fabs(ev));
+                    q[7] = fmax(q[7], fabs(hv));
+                    double ue = 0.5 * eps * ev * ev, uh = 0.5 * O_MU0 * hv * hv;
+                    q[0] += ue;
+                    q[1] += uh;
+                    if (inside) q[2] += ue, q[3] += uh;
+                    q[4] += 0.5 * eps * ep * ep;
+                    q[5] += 0.5 * O_MU0 * hp * hv;
+                }
+            }
+    double vol = pow(o.dx, 3.0);
+    for (int v = 0; v < 6; v++) q[v] *= vol;
+    rc = 0;
+out:
+    free(prev);
+    orc_free(&o);
+    return rc;
+}
+
 /* dt of a scene (grid.c:27-28) */
 double orc_dt(double dx, double courant) { return courant * (dx / (O_C0 * sqrt(3.0))); }

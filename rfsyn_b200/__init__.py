@@ -99,6 +99,12 @@ class SimInfo(C.Structure):
                 ("edge_items", C.c_int)]
 
 
+class Energy(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("electric_j", "magnetic_j", "total_j", "interior_j", "electric_prev_j",
+                                           "cross_j", "modified_prev_j", "max_abs_e", "max_abs_h")] + \
+               [("nonfinite", C.c_size_t)]
+
+
 SETUP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
@@ -173,6 +179,7 @@ def load() -> C.CDLL:
         "fdtd_b200_materials_add_spheres": (I, [P, P, C.POINTER(Sphere), S, I]),
         "fdtd_b200_sim_info": (I, [P, C.POINTER(SimInfo)]),
         "fdtd_b200_sim_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
+        "fdtd_b200_sim_energy": (I, [P, I, I, C.POINTER(Energy)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -306,6 +313,14 @@ class Sim:
         if self.lib.fdtd_b200_sim_info(self.h, C.byref(si)) != 0:
             raise RuntimeError(last_error())
         return si
+
+    def energy(self, x_lo: int = 0, x_hi: int | None = None) -> dict:
+        """FP64 energy audit of the resident fields (fdtd_b200_sim_energy)."""
+        en = Energy()
+        hi = self.rc.c.nx if x_hi is None else x_hi
+        if self.lib.fdtd_b200_sim_energy(self.h, x_lo, hi, C.byref(en)) != 0:
+            raise RuntimeError(last_error())
+        return {n: getattr(en, n) for n, _ in Energy._fields_}
 
     def time_kernels(self, n: int) -> tuple[float, float]:
         """Runs n steps kernel by kernel; returns (sweep_ms, other_ms)."""

@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "fused.cuh"
 #include "tma.cuh"
+#include "energy.cuh"
 
 using namespace rfb;
 
@@ -210,6 +211,7 @@ struct DevScene {
     int *t_main = nullptr, *t_nq = nullptr, *t_uv = nullptr, *t_sign = nullptr;
     int n_skip = 0;
     long long skip[MAX_SKIP] = {};
+    double *cb64_tab = nullptr, *cb64_list = nullptr;  // FP64 Cb for the energy audit
 };
 
 static void devscene_free(DevScene &s) {
@@ -218,6 +220,7 @@ static void devscene_free(DevScene &s) {
     cudaFree(s.l_tix); cudaFree(s.l_src); cudaFree(s.l_aix); cudaFree(s.ade_c); cudaFree(s.ade_s);
     cudaFree(s.t_m11); cudaFree(s.t_scale); cudaFree(s.t_w);
     cudaFree(s.t_main); cudaFree(s.t_nq); cudaFree(s.t_uv); cudaFree(s.t_sign);
+    cudaFree(s.cb64_tab); cudaFree(s.cb64_list);
     s = DevScene();
 }
 
@@ -239,7 +242,8 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
     for (int q = 0; q < tc; q++) { tca[q] = img->table_ca[q]; tcb[q] = img->table_cb[q]; }
     s.tca = dev_upload_conv(tca, 256, prec);
     s.tcb = dev_upload_conv(tcb, 256, prec);
-    if (!s.tca || !s.tcb) { rfb_set_error("table upload failed"); return -1; }
+    s.cb64_tab = (double *)dev_upload_conv(tcb, 256, RFB_FP64);
+    if (!s.tca || !s.tcb || !s.cb64_tab) { rfb_set_error("table upload failed"); return -1; }
     const size_t plane_b = (size_t)(g->ny + 1) * pitch;
     const size_t total_b = plane_b * (g->nx + 1);
     s.n_cells = img ? (int)img->n_cells : 0;
@@ -273,10 +277,11 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
         s.l_kind = dev_copy(img->kind, ne);
         s.l_ca = dev_upload_conv(img->ca, ne, prec);
         s.l_cb = dev_upload_conv(img->cb, ne, prec);
+        s.cb64_list = (double *)dev_upload_conv(img->cb, ne, RFB_FP64);
         s.l_tix = dev_copy(img->tix, ne);
         s.l_src = dev_copy(img->src, ne);
         s.l_aix = dev_copy(img->aix, ne);
-        if (!s.lc_ijk || !s.l_kind || !s.l_ca || !s.l_cb || !s.l_tix || !s.l_src || !s.l_aix) {
+        if (!s.lc_ijk || !s.l_kind || !s.l_ca || !s.l_cb || !s.l_tix || !s.l_src || !s.l_aix || !s.cb64_list) {
             rfb_set_error("interface list upload failed");
             return -1;
         }
@@ -390,6 +395,7 @@ struct rfb_engine {
     FusedPlan plan;
     TmaMaps tmaps[2];       // tensor maps of the input buffers per parity (TMA interior sweep)
     int *d_err = nullptr;   // set by a sweep whose copies did not complete in time
+    double *d_energy = nullptr;  // energy audit: block partials + result
     size_t h2d_bytes = 0, n_ade = 0;
 };
 
@@ -752,7 +758,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     devcpml_free(e->cpml);
     devscene_free(e->scene);
     cudaFree(e->src_val); cudaFree(e->src_hard);
-    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err);
+    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
     cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
@@ -1027,6 +1033,55 @@ fail:
     for (int q = 0; q < 4; q++)
         if (ev[q]) cudaEventDestroy(ev[q]);
     return rc;
+}
+
+// ---- energy audit ------------------------------------------------------------
+static int check_sweep_error(rfb_engine *e);
+
+template <typename T>
+static void enqueue_energy(rfb_engine *e, double dt, double dx, int x_lo, int x_hi, bool prev) {
+    EnergyArgs<T> a;
+    memset(&a, 0, sizeof a);
+    const int cur = e->nbuf == 2 ? e->parity : 0;
+    for (int m = 0; m < 3; m++) {
+        a.E[m] = (const T *)e->fld[cur][m];
+        a.H[m] = (const T *)e->fld[cur][3 + m];
+        a.Ep[m] = prev ? (const T *)e->fld[1 - cur][m] : nullptr;
+        a.Hp[m] = prev ? (const T *)e->fld[1 - cur][3 + m] : nullptr;
+    }
+    a.codes = e->scene.codes;
+    a.cb_tab = e->scene.cb64_tab;
+    a.n_cells = e->scene.n_cells;
+    a.lc_ijk = e->scene.lc_ijk;
+    a.cb_list = e->scene.cb64_list;
+    a.n_skip = e->scene.n_skip;
+    for (int q = 0; q < MAX_SKIP; q++) a.skip[q] = e->scene.skip[q];
+    a.nx = e->g.nx;
+    a.ny = e->g.ny;
+    a.nz = e->g.nz;
+    a.pitch = e->pitch;
+    a.x_lo = x_lo;
+    a.x_hi = x_hi;
+    a.dt_over_dx = dt / dx;
+    a.partial = e->d_energy;
+    k_energy<T><<<EN_BLOCKS, EN_THREADS, 0, e->stream>>>(a);
+}
+
+extern "C" int rfb_engine_energy(rfb_engine_t *e, double dt, double dx, int x_lo, int x_hi, double q[RFB_EN_COUNT]) {
+    const bool prev = e->nbuf == 2 && e->steps_done > 0;
+    if (!e->d_energy) CK(cudaMalloc(&e->d_energy, (size_t)(EN_BLOCKS + 1) * RFB_EN_COUNT * sizeof(double)));
+    if (e->prec == RFB_FP64) enqueue_energy<double>(e, dt, dx, x_lo, x_hi, prev);
+    else enqueue_energy<float>(e, dt, dx, x_lo, x_hi, prev);
+    k_energy_final<<<1, 32, 0, e->stream>>>(e->d_energy, EN_BLOCKS, pow(dx, 3.0), prev ? 1 : 0,
+                                            e->d_energy + (size_t)EN_BLOCKS * RFB_EN_COUNT);
+    g_launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(q, e->d_energy + (size_t)EN_BLOCKS * RFB_EN_COUNT, RFB_EN_COUNT * sizeof(double),
+                       cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    return check_sweep_error(e);
+fail:
+    return -1;
 }
 
 extern "C" int rfb_engine_time_kernels(rfb_engine_t *e, size_t n, double *sweep_ms, double *other_ms) {

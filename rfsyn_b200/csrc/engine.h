@@ -159,11 +159,24 @@ int rfb_step_update_h(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *c
 int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cpml_dev_t *cpml,
                       rfb_scene_dev_t *scene, double vacuum_cb, double *const host[6]);
 
-/* FP64 energy audit on the device: returns sum over cells of
- * 0.5*(eps E^2 + mu0 H^2) * dx^3 with eps recovered from Cb
- * (validate_long_term_stability.c:166-209). */
-int rfb_step_energy(rfb_fields_t *f, const rfb_geom_t *geom, rfb_scene_dev_t *scene,
-                    double vacuum_cb, double *const host[6], double *out_energy);
+/* FP64 energy audit of an engine's resident fields (rfsyn
+ * validate_long_term_stability.c:166-209, audit_periodic_energy.c:43-71):
+ * sums over i < nx, j < ny, k < nz of 0.5 eps E^2 and 0.5 mu0 H^2 times
+ * dx^3, eps = dt / (dx Cb) per (cell, component) with Cb the component's
+ * scalar coefficient.  q[] receives RFB_EN_COUNT values (RFB_EN_*). */
+enum {
+    RFB_EN_E = 0,        /* electric energy of the current E (step n)            */
+    RFB_EN_H,            /* magnetic energy of the current H (step n - 1/2)      */
+    RFB_EN_E_INT,        /* electric, planes x_lo <= i < x_hi                    */
+    RFB_EN_H_INT,        /* magnetic, planes x_lo <= i < x_hi                    */
+    RFB_EN_E_PREV,       /* electric energy of E at step n - 1 (ping-pong only)  */
+    RFB_EN_CROSS,        /* 0.5 mu0 H^{n-3/2} . H^{n-1/2} dx^3 (ping-pong only)  */
+    RFB_EN_MAX_E,        /* max |E| (current)                                    */
+    RFB_EN_MAX_H,        /* max |H| (current)                                    */
+    RFB_EN_NONFINITE,    /* number of non-finite current samples                 */
+    RFB_EN_COUNT
+};
+int rfb_engine_energy(rfb_engine_t *e, double dt, double dx, int x_lo, int x_hi, double q[RFB_EN_COUNT]);
 
 /* Fill fractions of a sphere (centre / radius in cell units) for the three E
  * samples of every cell of the box [i0, i0+ni) x [j0, j0+nj) x [k0, k0+nk):

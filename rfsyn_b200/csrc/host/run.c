@@ -67,7 +67,7 @@ void fdtd_b200_config_init(fdtd_b200_config_t *cfg, size_t nx, size_t ny, size_t
 struct fdtd_b200_sim {
     rfb_engine_t *eng;
     size_t n_steps, n_probes, n_freqs;
-    double dt;
+    double dt, dx;
     double *freqs;
     double dft_offset;
     size_t nx, ny, nz;
@@ -185,6 +185,7 @@ fdtd_b200_sim_t *fdtd_b200_sim_create(const fdtd_b200_config_t *cfg, fdtd_materi
     sim->n_steps = nt;
     sim->n_probes = np;
     sim->dt = g.dt;
+    sim->dx = g.dx;
     sim->nx = g.nx; sim->ny = g.ny; sim->nz = g.nz;
     sim->dft_offset = cfg->dft_time_offset_steps;
     sim->precision = cfg->precision;
@@ -262,6 +263,23 @@ int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info) {
 int fdtd_b200_sim_time_kernels(fdtd_b200_sim_t *sim, size_t n, double *sweep_ms, double *other_ms) {
     if (!sim || !sweep_ms || !other_ms) return -1;
     return rfb_engine_time_kernels(sim->eng, n, sweep_ms, other_ms);
+}
+
+int fdtd_b200_sim_energy(fdtd_b200_sim_t *sim, int x_lo, int x_hi, fdtd_b200_energy_t *out) {
+    if (!sim || !out) return -1;
+    double q[RFB_EN_COUNT];
+    if (rfb_engine_energy(sim->eng, sim->dt, sim->dx, x_lo, x_hi, q) != 0) return -1;
+    out->electric_j = q[RFB_EN_E];
+    out->magnetic_j = q[RFB_EN_H];
+    out->total_j = q[RFB_EN_E] + q[RFB_EN_H];
+    out->interior_j = q[RFB_EN_E_INT] + q[RFB_EN_H_INT];
+    out->electric_prev_j = q[RFB_EN_E_PREV];
+    out->cross_j = q[RFB_EN_CROSS];
+    out->modified_prev_j = q[RFB_EN_E_PREV] + q[RFB_EN_CROSS];
+    out->max_abs_e = q[RFB_EN_MAX_E];
+    out->max_abs_h = q[RFB_EN_MAX_H];
+    out->nonfinite = (size_t)q[RFB_EN_NONFINITE];
+    return 0;
 }
 
 int fdtd_b200_sim_read_probes(fdtd_b200_sim_t *sim, double *probe_td) {
