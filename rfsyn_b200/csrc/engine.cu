@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "fused.cuh"
 #include "tma.cuh"
+#include "sweep.cuh"
 #include "energy.cuh"
 
 using namespace rfb;
@@ -420,11 +421,36 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
     return a;
 }
 
-// Interior sweep of the plan: TMA-fed or cp.async-fed variant.
+// Interior sweep of the plan: TMA-fed or cp.async-fed variant, or (mode 2)
+// the persistent work-queue sweep over the interior items.
+template <typename T>
+static void launch_q_t(const Args<T> &a, const FusedPlan &p, bool edge, const TmaMaps &m, int *err, cudaStream_t st);
+template <>
+void launch_q_t<float>(const Args<float> &a, const FusedPlan &p, bool edge, const TmaMaps &m, int *err,
+                       cudaStream_t st) {
+    if (edge) launch_q_f<true>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    else launch_q_f<false>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
+}
+template <>
+void launch_q_t<double>(const Args<double> &a, const FusedPlan &p, bool edge, const TmaMaps &m, int *err,
+                        cudaStream_t st) {
+    if (edge) launch_q_d<true>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    else launch_q_d<false>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
+}
+
 template <typename T>
 static void launch_int(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
-    if (e->plan.tma) launch_interior_tma<T>(a, e->plan, e->tmaps[e->nbuf == 2 ? par : 0], e->d_err, st);
+    const TmaMaps &m = e->tmaps[e->nbuf == 2 ? par : 0];
+    if (e->plan.tma == 2) launch_q_t<T>(a, e->plan, false, m, e->d_err, st);
+    else if (e->plan.tma) launch_interior_tma<T>(a, e->plan, m, e->d_err, st);
     else launch_interior<T>(a, e->plan, st);
+}
+// Everything else of the sweep: the slab / boundary queue (mode 2) and the
+// cp.async-fed edge sweep (the items whose halo wraps, in mode 2).
+template <typename T>
+static void launch_rest(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
+    if (e->plan.tma == 2) launch_q_t<T>(a, e->plan, true, e->tmaps[e->nbuf == 2 ? par : 0], e->d_err, st);
+    launch_edge<T>(a, e->plan, st);
 }
 
 template <typename T>
@@ -436,7 +462,7 @@ static void enqueue_step(rfb_engine *e, int par) {
         cudaEventRecord(e->ev_fork, e->stream);
         cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
         launch_int<T>(e, a, par, e->stream);
-        launch_edge<T>(a, e->plan, e->stream2);
+        launch_rest<T>(e, a, par, e->stream2);
         cudaEventRecord(e->ev_join, e->stream2);
         cudaStreamWaitEvent(e->stream, e->ev_join, 0);
     } else {
@@ -459,7 +485,7 @@ static void enqueue_step(rfb_engine *e, int par) {
 }
 
 static int count_step_launches(const rfb_engine *e) {
-    int n = (e->sched == RFB_SCHED_FUSED) ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) : 2;
+    int n = (e->sched == RFB_SCHED_FUSED) ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) : 2;
     if (e->scene.n_cells) n++;
     return n + 1;
 }
@@ -489,8 +515,9 @@ fail:
 static void free_plan_lists(FusedPlan &p) {
     cudaFree(p.d_int);
     cudaFree(p.d_edge);
-    p.d_int = p.d_edge = nullptr;
-    p.n_int = p.n_edge = 0;
+    cudaFree(p.d_qe);
+    p.d_int = p.d_edge = p.d_qe = nullptr;
+    p.n_int = p.n_edge = p.n_qe = 0;
 }
 
 // ---- tensor maps of the TMA interior sweep -----------------------------------
@@ -577,11 +604,19 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     ext(1, &ylo, &yhi, g.ny, py);
     ext(2, &zlo, &zhi, g.nz, pz);
     const int xa = px ? 0 : xlo + 1, xb = std::max(xa, xhi);
-    std::vector<SweepItem> vi, ve;
+    std::vector<SweepItem> vi, ve, vq;
     auto add = [](std::vector<SweepItem> &v, int j0, int k0, int b, int en, int seg) {
         for (int s = b; s < en; s += seg) v.push_back(SweepItem{j0, k0, s, std::min(en, s + seg)});
     };
     auto add_edge = [&](int j0, int rows, int k0, int b, int en) {
+        // mode 2: tiles whose halo stays inside the grid go to the TMA-fed
+        // slab / boundary queue; tiles whose halo wraps around a periodic
+        // axis to the cp.async-fed edge sweep (8-row tiles)
+        const bool wraps = (py && (j0 == 0 || j0 + rows >= g.ny)) || (pz && (k0 == 0 || k0 + 32 >= g.nz));
+        if (tma == 2 && !wraps) {
+            add(vq, j0, k0, b, en, seg_edge);
+            return;
+        }
         for (int jj = j0; jj < j0 + rows && jj < p.d.cj; jj += 8) add(ve, jj, k0, b, en, seg_edge);
     };
     for (int j0 = 0; j0 < p.d.cj; j0 += tj)
@@ -605,13 +640,24 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
                 add_edge(j0, tj, k0, 0, p.d.ci);
             }
         }
+    // queue order: longest items first, so the last items to start are short
+    std::stable_sort(vq.begin(), vq.end(), [](const SweepItem &x, const SweepItem &y) {
+        return x.ie - x.ib > y.ie - y.ib;
+    });
     p.n_int = (int)vi.size();
     p.n_edge = (int)ve.size();
+    p.n_qe = (int)vq.size();
     if (p.n_int) CK(cudaMalloc(&p.d_int, vi.size() * sizeof(SweepItem)));
     if (p.n_edge) CK(cudaMalloc(&p.d_edge, ve.size() * sizeof(SweepItem)));
+    if (p.n_qe) CK(cudaMalloc(&p.d_qe, vq.size() * sizeof(SweepItem)));
     if (p.n_int) CK(cudaMemcpy(p.d_int, vi.data(), vi.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_edge) CK(cudaMemcpy(p.d_edge, ve.data(), ve.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
-    if (tma && p.n_int && build_tma_maps(e, tj) != 0) return -1;
+    if (p.n_qe) CK(cudaMemcpy(p.d_qe, vq.data(), vq.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
+    if (tma == 2 && !p.d_queue) {
+        CK(cudaMalloc(&p.d_queue, 4 * sizeof(int)));
+        CK(cudaMemset(p.d_queue, 0, 4 * sizeof(int)));
+    }
+    if (tma && (p.n_int || p.n_qe) && build_tma_maps(e, tj) != 0) return -1;
     return 0;
 fail:
     return -1;
@@ -620,7 +666,10 @@ fail:
 static bool plan_variant_known(int prec, int tj, int ns, int tma) {
     const InteriorVariant *v;
     size_t n;
-    if (prec == RFB_FP32) {
+    if (tma == 2) {
+        v = prec == RFB_FP32 ? kQVariantsFp32 : kQVariantsFp64;
+        n = prec == RFB_FP32 ? std::size(kQVariantsFp32) : std::size(kQVariantsFp64);
+    } else if (prec == RFB_FP32) {
         v = tma ? kTmaVariantsFp32 : kIntVariantsFp32;
         n = tma ? std::size(kTmaVariantsFp32) : std::size(kIntVariantsFp32);
     } else {
@@ -650,7 +699,7 @@ static void enqueue_sweep(rfb_engine *e, int par) {
     cudaEventRecord(e->ev_fork, e->stream);
     cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
     launch_int<T>(e, a, par, e->stream);
-    launch_edge<T>(a, e->plan, e->stream2);
+    launch_rest<T>(e, a, par, e->stream2);
     cudaEventRecord(e->ev_join, e->stream2);
     cudaStreamWaitEvent(e->stream, e->ev_join, 0);
 }
@@ -677,9 +726,11 @@ static int autotune(rfb_engine *e, int active) {
     };
     std::vector<Cand> vars;
     if (e->prec == RFB_FP32) {
+        for (const InteriorVariant &v : kQVariantsFp32) vars.push_back({v, 2});
         for (const InteriorVariant &v : kTmaVariantsFp32) vars.push_back({v, 1});
         for (const InteriorVariant &v : kIntVariantsFp32) vars.push_back({v, 0});
     } else {
+        for (const InteriorVariant &v : kQVariantsFp64) vars.push_back({v, 2});
         for (const InteriorVariant &v : kTmaVariantsFp64) vars.push_back({v, 1});
         for (const InteriorVariant &v : kIntVariantsFp64) vars.push_back({v, 0});
     }
@@ -760,7 +811,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     cudaFree(e->src_val); cudaFree(e->src_hard);
     cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
-    cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge);
+    cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_queue);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->stream2) cudaStreamDestroy(e->stream2);
@@ -839,7 +890,7 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
         CK(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
-        if (tma_prepare() != 0) {
+        if (tma_prepare() != 0 || q_prepare() != 0) {
             rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
             goto fail_noset;
         }
@@ -959,7 +1010,7 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->ring_depth = e->plan.ns;
     out->tma = e->plan.tma;
     out->interior_items = e->plan.n_int;
-    out->edge_items = e->plan.n_edge;
+    out->edge_items = e->plan.n_edge + e->plan.n_qe;
     size_t sca = 0;
     if (e->cpml.on) {
         // cells of the swept volume inside the slab of each axis (H profiles)
@@ -990,10 +1041,10 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
             cudaEventRecord(e->ev_fork, e->stream);
             cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
             launch_int<T>(e, a, par, e->stream);
-            launch_edge<T>(a, e->plan, e->stream2);
+            launch_rest<T>(e, a, par, e->stream2);
             cudaEventRecord(e->ev_join, e->stream2);
             cudaStreamWaitEvent(e->stream, e->ev_join, 0);
-            g_launches += (e->plan.n_int > 0) + (e->plan.n_edge > 0);
+            g_launches += (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0);
         } else {
             dim3 blk(32, 8), grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
             k_h_split<T><<<grd, blk, 0, e->stream>>>(a);

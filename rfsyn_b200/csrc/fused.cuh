@@ -42,11 +42,17 @@ struct SweepItem {
 
 struct FusedPlan {
     int tj = 8, ns = 6;   // interior variant (rows per tile, ring depth)
-    int tma = 0;          // interior planes staged by the TMA (1) or per-thread cp.async (0)
+    // interior planes staged per thread by cp.async (0), by the TMA (1), or
+    // (2) interior and slab tiles both by the TMA in the persistent
+    // work-queue sweeps k_sweep_q (sweep.cuh)
+    int tma = 0;
     FusedDims d;
     int seg_int = 64, seg_edge = 32;
     int n_int = 0, n_edge = 0;
     SweepItem *d_int = nullptr, *d_edge = nullptr;  // device work lists
+    int n_qe = 0;                                   // mode 2: slab / boundary items of k_sweep_q<EDGE>
+    SweepItem *d_qe = nullptr;
+    int *d_queue = nullptr;                         // mode 2: counters (interior 0-1, edge 2-3)
 };
 
 template <typename T>

@@ -2,8 +2,10 @@
 //
 // One templated source serves FP64 (bit-for-bit with rfsyn's CPU loops: the
 // same operation order, every multiply and add rounded separately through
-// __dmul_rn/__dadd_rn so nothing is contracted into an FMA) and FP32 (plain
-// operators, the compiler may contract).
+// __dmul_rn/__dadd_rn so nothing is contracted into an FMA) and FP32 (the
+// same order, rounded separately through __fmul_rn/__fadd_rn: every sweep
+// variant the autotuner may pick yields bit-identical FP32 fields, so runs
+// are reproducible whatever variant a process picks).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -13,9 +15,9 @@ namespace rfb {
 __device__ __forceinline__ double xm(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double xa(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ float xm(float a, float b) { return a * b; }
-__device__ __forceinline__ float xa(float a, float b) { return a + b; }
-__device__ __forceinline__ float xs(float a, float b) { return a - b; }
+__device__ __forceinline__ float xm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xs(float a, float b) { return __fsub_rn(a, b); }
 
 constexpr int LIST_CODE = 255;
 constexpr int MAX_SKIP = 4;

@@ -1,0 +1,525 @@
+// sweep.cuh -- persistent, TMA-fed H+E sweep over a device work queue.
+//
+// One step of the fused schedule is two launches of k_sweep_q, side by side
+// on two streams: the interior instantiation (EDGE = false) takes the work
+// items whose tiles, halos and planes lie outside every CPML slab and PEC
+// boundary; the edge instantiation (EDGE = true) takes all other items whose
+// halo does not wrap around a periodic axis, with rfsyn's per-component
+// update ranges (engine/fdtd/cpml.c:176-219, materials.c:911-1060) and the
+// slab-stored psi recursions (cpml.h:46-51).  Items whose halo wraps stay on
+// the cp.async-fed k_sweep_edge (fused.cuh).
+//
+// The grid is sized to the resident CTAs (SM count x CTAs per SM); each CTA
+// pops items from a device counter until the list is exhausted, so uneven
+// items (interior vs slab tiles, segment remainders) balance across SMs.  The
+// last CTA to leave zeroes the counters, so every launch starts from a clean
+// queue whatever ran before it.
+//
+// Per item the march is the one of k_sweep_interior_tma (tma.cuh): per plane
+// one elected thread issues one tiled cp.async.bulk.tensor load per field
+// component and one for the codes into an NS-deep ring of shared-memory
+// stages completing on mbarriers; H of the plane is computed for the tile and
+// its low-j / low-k halo (recomputed, never stored), then E follows from the
+// shared H and the previous plane's H kept in registers.  psi values of slab
+// cells are read with plain loads issued before the plane's barrier wait, so
+// their latency overlaps the wait; profile values of the tile's rows and
+// columns sit in shared memory.  Only slab cells touch psi or profiles, so
+// the bytes moved are the algorithmic ones.
+//
+// Every mbarrier wait is bounded (tma.cuh: mbar_wait); on a timeout the CTA
+// records an error code, lets its own copies in flight land (bounded) and
+// leaves the queue.  No load uses cluster multicast.
+#pragma once
+#include "tma.cuh"
+
+namespace rfb {
+
+template <typename T, int TJ>
+struct TileTables {
+    T tab[512];         // Ca (0..255), Cb (256..511)
+    T py[6][TJ + 1];    // y profiles at rows j0-1 .. j0+TJ-1: H grid (kinv b a), E grid (kinv b a)
+    T pz[6][33];        // z profiles at cols k0-1 .. k0+31
+};
+
+template <typename T, int TJ, int NS>
+struct QLayout {
+    using L = TmaLayout<T, TJ, NS>;
+    static constexpr size_t bars = NS * L::stage;
+    static constexpr size_t sh = bars + round128(8 * NS);
+    static constexpr size_t tabs = sh + round128(sizeof(T) * 3 * (TJ + 1) * 33);
+    static constexpr size_t misc = tabs + round128(sizeof(TileTables<T, TJ>));
+    static constexpr size_t total = misc + 16;
+};
+
+template <typename T, int TJ, int NS, int MINB, bool EDGE>
+__global__ void __launch_bounds__(32 * TJ, MINB)
+    k_sweep_q(Args<T> a, FusedDims d, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps,
+              int *queue, int *err) {
+    static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
+    using L = TmaLayout<T, TJ, NS>;
+    using S = QLayout<T, TJ, NS>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
+    T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(smem_raw + S::sh);
+    TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
+    volatile int *s_item = reinterpret_cast<volatile int *>(smem_raw + S::misc);
+    auto E = [&](int s, int c) { return reinterpret_cast<T(*)[TMA_EW]>(smem_raw + s * L::stage + c * L::ebox); };
+    auto H = [&](int s, int c) {
+        return reinterpret_cast<T(*)[TMA_HW]>(smem_raw + s * L::stage + 3 * L::ebox + c * L::hbox);
+    };
+    auto CODE = [&](int s) {
+        return reinterpret_cast<uint8_t(*)[32]>(smem_raw + s * L::stage + 3 * L::ebox + 3 * L::hbox);
+    };
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
+    const int r = ty + 1, q = tx + 4;  // stage coordinates of the own cell
+    const int qs = tx + 1;             // sH / z-table column of the own cell
+    const bool with_codes = a.codes != nullptr;
+    const unsigned tx_bytes = 3 * L::ebytes + 3 * L::hbytes + (with_codes ? L::cbytes : 0u);
+    const T cbh = a.cbh;
+    const int on = a.cpml_on;
+    const long long ny1 = a.ny + 1;
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; s++) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    for (int t = tid; t < 256; t += 32 * TJ) {
+        tt.tab[t] = a.tca[t];
+        tt.tab[256 + t] = a.tcb[t];
+    }
+    __syncthreads();
+
+    // uniform bookkeeping: phase bit s = parity of slot s's next completion,
+    // pending bit s = slot s has a load in flight that nobody waited for
+    unsigned phase = 0, pending = 0;
+    bool failed = false;
+
+    for (;;) {
+        if (tid == 0) *s_item = atomicAdd(&queue[0], 1);
+        __syncthreads();
+        const int w = *s_item;
+        if (w >= n_items) break;
+        const SweepItem it = items[w];
+        const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
+
+        auto issue = [&](int s, int p) {
+            if (p < 0) return;
+            if (tid == 0) {
+                mbar_expect_tx(&bars[s], tx_bytes);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    tma_load_3d(E(s, c), &maps.e[c], k0 - 4, j0 - 1, p, &bars[s]);
+                    tma_load_3d(H(s, c), &maps.h[c], k0 - 4, j0 - 1, p, &bars[s]);
+                }
+                if (with_codes) tma_load_3d(CODE(s), &maps.code, k0, j0, p, &bars[s]);
+            }
+            pending |= 1u << s;
+        };
+        auto wait_slot = [&](int s) {
+            if (!(pending & (1u << s))) return;
+            if (!mbar_wait(&bars[s], (phase >> s) & 1u)) failed = true;
+            phase ^= 1u << s;
+            pending &= ~(1u << s);
+        };
+
+        // ---- per-thread geometry of the item (EDGE) ----
+        const int j = j0 + ty, k = k0 + tx;
+        const bool own = !EDGE || (j < d.cj && k < d.ck);
+        // component masks at (j, k): bits 0-2 H, 3-5 E (plane conditions apart)
+        unsigned mjk = 0x3f;
+        bool rowh = true, colh = tx < TJ;  // halo cells this thread recomputes
+        int sjh = -1, skh = -1, sjm = -1, skm = -1;
+        int sjh_row = -1, sjh_col = -1, skh_col = -1;
+        const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
+        if constexpr (EDGE) {
+            const int jmin = py ? 0 : 1, kmin = pz ? 0 : 1;
+            mjk = 0;
+            if (own) {
+                if (j < a.ny && k < a.nz) mjk |= 1u;
+                if (j < a.ny + (py ? 0 : 1) && k < a.nz) mjk |= 2u;
+                if (j < a.ny && k < a.nz + (pz ? 0 : 1)) mjk |= 4u;
+                if (j < a.ny && k < a.nz) {
+                    if (j >= jmin && k >= kmin) mjk |= 8u;
+                    if (k >= kmin) mjk |= 16u;
+                    if (j >= jmin) mjk |= 32u;
+                }
+            }
+            rowh = j0 > 0 && k < d.ck;
+            colh = tx < TJ && k0 > 0 && jc < d.cj;
+            sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
+            skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
+            sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
+            skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
+            sjh_row = slab_in(jh, a.lo_h[1], a.hi_h[1], a.ny, on);
+            sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
+            skh_col = slab_in(kh, a.lo_h[2], a.hi_h[2], a.nz, on);
+            for (int t = tid; t < TJ + 1; t += 32 * TJ) {
+                T v[3];
+                prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], j0 - 1 + t, a.ny, v);
+                tt.py[0][t] = v[0]; tt.py[1][t] = v[1]; tt.py[2][t] = v[2];
+                prof_at(on ? a.kinv_m[1] : (const T *)nullptr, a.b_m[1], a.a_m[1], j0 - 1 + t, a.ny + 1, v);
+                tt.py[3][t] = v[0]; tt.py[4][t] = v[1]; tt.py[5][t] = v[2];
+            }
+            for (int t = tid; t < 33; t += 32 * TJ) {
+                T v[3];
+                prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], k0 - 1 + t, a.nz, v);
+                tt.pz[0][t] = v[0]; tt.pz[1][t] = v[1]; tt.pz[2][t] = v[2];
+                prof_at(on ? a.kinv_m[2] : (const T *)nullptr, a.b_m[2], a.a_m[2], k0 - 1 + t, a.nz + 1, v);
+                tt.pz[3][t] = v[0]; tt.pz[4][t] = v[1]; tt.pz[5][t] = v[2];
+            }
+        }
+        const int nshy = a.ns_h[1], nshz = a.ns_h[2], nsmy = a.ns_m[1], nsmz = a.ns_m[2];
+
+        // H of component c at plane i (slots sc / sn) for the cell at stage
+        // position (rr, qq) with coordinates (jj, kk): unstretched, or (EDGE)
+        // with the slab psi recursions; yi / zi are its rows in the profile
+        // tables, sy / sz its H-grid slab indices, sx the plane's.  pA / pB
+        // are the cell's psi inputs of the two terms (used where a slab
+        // applies); the updated psi are stored when `store`.
+        auto hcell = [&](int c, int i, int sc, int sn, int rr, int qq, int jj, int kk, int yi, int zi, int sy,
+                         int sz, int sx, T pA, T pB, bool store) -> T {
+            const T hin = H(sc, c)[rr][qq];
+            T dA, dB;
+            if (c == 0) {
+                dA = xs(E(sc, 2)[rr + 1][qq], E(sc, 2)[rr][qq]);
+                dB = xs(E(sc, 1)[rr][qq + 1], E(sc, 1)[rr][qq]);
+            } else if (c == 1) {
+                dA = xs(E(sc, 0)[rr][qq + 1], E(sc, 0)[rr][qq]);
+                dB = xs(E(sn, 2)[rr][qq], E(sc, 2)[rr][qq]);
+            } else {
+                dA = xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]);
+                dB = xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq]);
+            }
+            if constexpr (EDGE) {
+                T pn;
+                if (c == 0) {
+                    if (sy >= 0) {
+                        dA = stretch(dA, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pA, &pn);
+                        if (store) a.psi_ho[0][((long long)i * nshy + sy) * a.pitch + kk] = pn;
+                    }
+                    if (sz >= 0) {
+                        dB = stretch(dB, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pB, &pn);
+                        if (store) a.psi_ho[1][((long long)i * ny1 + jj) * nshz + sz] = pn;
+                    }
+                } else if (c == 1) {
+                    if (sz >= 0) {
+                        dA = stretch(dA, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pA, &pn);
+                        if (store) a.psi_ho[2][((long long)i * ny1 + jj) * nshz + sz] = pn;
+                    }
+                    if (sx >= 0) {
+                        dB = stretch(dB, a.kinv_h[0][i], a.b_h[0][i], a.a_h[0][i], a.dx, pB, &pn);
+                        if (store) a.psi_ho[3][((long long)sx * ny1 + jj) * a.pitch + kk] = pn;
+                    }
+                } else {
+                    if (sx >= 0) {
+                        dA = stretch(dA, a.kinv_h[0][i], a.b_h[0][i], a.a_h[0][i], a.dx, pA, &pn);
+                        if (store) a.psi_ho[4][((long long)sx * ny1 + jj) * a.pitch + kk] = pn;
+                    }
+                    if (sy >= 0) {
+                        dB = stretch(dB, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pB, &pn);
+                        if (store) a.psi_ho[5][((long long)i * nshy + sy) * a.pitch + kk] = pn;
+                    }
+                }
+            }
+            return xs(hin, xm(cbh, xs(dA, dB)));
+        };
+        // psi inputs of H component c at a cell (zero where no slab applies)
+        auto hpsi = [&](int c, int i, int jj, int kk, int sy, int sz, int sx, T &pA, T &pB) {
+            pA = T(0);
+            pB = T(0);
+            if (c == 0) {
+                if (sy >= 0) pA = a.psi_hi[0][((long long)i * nshy + sy) * a.pitch + kk];
+                if (sz >= 0) pB = a.psi_hi[1][((long long)i * ny1 + jj) * nshz + sz];
+            } else if (c == 1) {
+                if (sz >= 0) pA = a.psi_hi[2][((long long)i * ny1 + jj) * nshz + sz];
+                if (sx >= 0) pB = a.psi_hi[3][((long long)sx * ny1 + jj) * a.pitch + kk];
+            } else {
+                if (sx >= 0) pA = a.psi_hi[4][((long long)sx * ny1 + jj) * a.pitch + kk];
+                if (sy >= 0) pB = a.psi_hi[5][((long long)i * nshy + sy) * a.pitch + kk];
+            }
+        };
+        // plane conditions: H bits (Hx to nx inclusive on a PEC x axis), E bits
+        auto plane_mask = [&](int i) -> unsigned {
+            if constexpr (!EDGE) return 0x3fu;
+            unsigned m = 0;
+            if (i < a.nx + (px ? 0 : 1)) m |= 1u;
+            if (i < a.nx) m |= 2u | 4u | 8u;
+            if (i < a.nx && i >= (px ? 0 : 1)) m |= 16u | 32u;
+            return m;
+        };
+
+        // ---- prologue: previous plane and the first NS-1 planes ----
+        int pprev = ib > 0 ? ib - 1 : (px ? a.nx - 1 : -1);
+        int pf = ib;
+        issue(NS - 1, pprev);
+#pragma unroll
+        for (int s = 0; s < NS - 1; s++) {
+            if (pf >= 0 && ib + s <= ie) issue(s, pf);
+            if (pf >= 0) pf = plane_after(pf, a.nx, px);
+        }
+        wait_slot(NS - 1);
+        wait_slot(0);
+        if (__syncthreads_or(failed)) goto bail;
+        {
+            T prevHy = T(0), prevHz = T(0);
+            if (pprev >= 0) {
+                const unsigned mp = plane_mask(pprev) & mjk;
+                const int sxp = EDGE ? slab_in(pprev, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
+                T pA = T(0), pB = T(0);
+                if constexpr (EDGE) hpsi(1, pprev, j, k, sjh, skh, sxp, pA, pB);
+                prevHy = (mp & 2u) ? hcell(1, pprev, NS - 1, 0, r, q, j, k, r, qs, sjh, skh, sxp, pA, pB, false)
+                                   : H(NS - 1, 1)[r][q];
+                if constexpr (EDGE) hpsi(2, pprev, j, k, sjh, skh, sxp, pA, pB);
+                prevHz = (mp & 4u) ? hcell(2, pprev, NS - 1, 0, r, q, j, k, r, qs, sjh, skh, sxp, pA, pB, false)
+                                   : H(NS - 1, 2)[r][q];
+            }
+            __syncthreads();  // slot NS-1 may now be refilled
+
+            int sc = 0;
+            for (int i = ib; i < ie; i++) {
+                const int sn = sc == NS - 1 ? 0 : sc + 1;
+                const int sf = sc == 0 ? NS - 1 : sc - 1;  // held plane i-1, read by nobody any more
+                if (pf >= 0 && i + NS - 1 <= ie) {
+                    issue(sf, pf);
+                    pf = plane_after(pf, a.nx, px);
+                }
+                const unsigned m = plane_mask(i) & mjk;
+                const int sxh = EDGE ? slab_in(i, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
+                const int sxm = EDGE ? slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on) : -1;
+                // psi inputs of the own cell, loaded before the wait
+                T hp[6], ep[6];
+#pragma unroll
+                for (int t = 0; t < 6; t++) hp[t] = ep[t] = T(0);
+                if constexpr (EDGE) {
+                    if (m & 1u) hpsi(0, i, j, k, sjh, skh, sxh, hp[0], hp[1]);
+                    if (m & 2u) hpsi(1, i, j, k, sjh, skh, sxh, hp[2], hp[3]);
+                    if (m & 4u) hpsi(2, i, j, k, sjh, skh, sxh, hp[4], hp[5]);
+                    if (m & 8u) {
+                        if (sjm >= 0) ep[0] = a.psi_e[0][((long long)i * nsmy + sjm) * a.pitch + k];
+                        if (skm >= 0) ep[1] = a.psi_e[1][((long long)i * ny1 + j) * nsmz + skm];
+                    }
+                    if (m & 16u) {
+                        if (skm >= 0) ep[2] = a.psi_e[2][((long long)i * ny1 + j) * nsmz + skm];
+                        if (sxm >= 0) ep[3] = a.psi_e[3][((long long)sxm * ny1 + j) * a.pitch + k];
+                    }
+                    if (m & 32u) {
+                        if (sxm >= 0) ep[4] = a.psi_e[4][((long long)sxm * ny1 + j) * a.pitch + k];
+                        if (sjm >= 0) ep[5] = a.psi_e[5][((long long)i * nsmy + sjm) * a.pitch + k];
+                    }
+                }
+                wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
+                if (__syncthreads_or(failed)) goto bail;
+                const T e0 = E(sc, 0)[r][q], e1 = E(sc, 1)[r][q], e2 = E(sc, 2)[r][q];
+                const int code = with_codes ? (int)CODE(sc)[ty][tx] : 0;
+                const long long c = (long long)i * a.plane + (long long)j * a.pitch + k;
+                T hx = H(sc, 0)[r][q], hy = H(sc, 1)[r][q], hz = H(sc, 2)[r][q];
+                if (m & 1u) hx = hcell(0, i, sc, sn, r, q, j, k, r, qs, sjh, skh, sxh, hp[0], hp[1], true);
+                if (m & 2u) hy = hcell(1, i, sc, sn, r, q, j, k, r, qs, sjh, skh, sxh, hp[2], hp[3], true);
+                if (m & 4u) hz = hcell(2, i, sc, sn, r, q, j, k, r, qs, sjh, skh, sxh, hp[4], hp[5], true);
+                if (own && (!EDGE || i < d.ci)) {
+                    a.Ho[0][c] = hx;
+                    a.Ho[1][c] = hy;
+                    a.Ho[2][c] = hz;
+                }
+                sH[0][r][qs] = hx;
+                sH[1][r][qs] = hy;
+                sH[2][r][qs] = hz;
+                if (ty == 0) {
+                    if (rowh) {
+                        // row halo (j0-1, k): Hx, Hz
+                        const unsigned mh = plane_mask(i) & (EDGE ? ((k < a.nz ? 1u : 0u) |
+                                                                     (k < a.nz + (pz ? 0 : 1) ? 4u : 0u))
+                                                                  : 5u);
+                        T pA = T(0), pB = T(0);
+                        T v = H(sc, 0)[0][q];
+                        if (mh & 1u) {
+                            if constexpr (EDGE) hpsi(0, i, jh, k, sjh_row, skh, sxh, pA, pB);
+                            v = hcell(0, i, sc, sn, 0, q, jh, k, 0, qs, sjh_row, skh, sxh, pA, pB, false);
+                        }
+                        sH[0][0][qs] = v;
+                        v = H(sc, 2)[0][q];
+                        if (mh & 4u) {
+                            if constexpr (EDGE) hpsi(2, i, jh, k, sjh_row, skh, sxh, pA, pB);
+                            v = hcell(2, i, sc, sn, 0, q, jh, k, 0, qs, sjh_row, skh, sxh, pA, pB, false);
+                        }
+                        sH[2][0][qs] = v;
+                    }
+                } else if (ty == 1 && colh) {
+                    // column halo (j0+tx, k0-1): Hx, Hy
+                    const unsigned mh = plane_mask(i) & (EDGE ? ((jc < a.ny ? 1u : 0u) |
+                                                                 (jc < a.ny + (py ? 0 : 1) ? 2u : 0u))
+                                                              : 3u);
+                    T pA = T(0), pB = T(0);
+                    T v = H(sc, 0)[tx + 1][3];
+                    if (mh & 1u) {
+                        if constexpr (EDGE) hpsi(0, i, jc, kh, sjh_col, skh_col, sxh, pA, pB);
+                        v = hcell(0, i, sc, sn, tx + 1, 3, jc, kh, tx + 1, 0, sjh_col, skh_col, sxh, pA, pB, false);
+                    }
+                    sH[0][tx + 1][0] = v;
+                    v = H(sc, 1)[tx + 1][3];
+                    if (mh & 2u) {
+                        if constexpr (EDGE) hpsi(1, i, jc, kh, sjh_col, skh_col, sxh, pA, pB);
+                        v = hcell(1, i, sc, sn, tx + 1, 3, jc, kh, tx + 1, 0, sjh_col, skh_col, sxh, pA, pB, false);
+                    }
+                    sH[1][tx + 1][0] = v;
+                }
+                __syncthreads();
+                if (!with_codes || code != LIST_CODE) {
+                    bool skip = false;
+                    if constexpr (EDGE) {
+                        if (!with_codes)
+                            for (int s = 0; s < a.n_skip; s++) skip |= a.skip[s] == c;
+                    }
+                    if (!skip) {
+                        const T ca = tt.tab[code], cb = tt.tab[256 + code];
+                        if (m & 8u) {
+                            T tA = xs(sH[2][r][qs], sH[2][r - 1][qs]);
+                            T tB = xs(sH[1][r][qs], sH[1][r][qs - 1]);
+                            if constexpr (EDGE) {
+                                T pn;
+                                if (sjm >= 0) {
+                                    tA = stretch(tA, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[0], &pn);
+                                    a.psi_e[0][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
+                                }
+                                if (skm >= 0) {
+                                    tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
+                                    a.psi_e[1][((long long)i * ny1 + j) * nsmz + skm] = pn;
+                                }
+                            }
+                            a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
+                        }
+                        if (m & 16u) {
+                            T tA = xs(sH[0][r][qs], sH[0][r][qs - 1]);
+                            T tB = xs(hz, prevHz);
+                            if constexpr (EDGE) {
+                                T pn;
+                                if (skm >= 0) {
+                                    tA = stretch(tA, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[2], &pn);
+                                    a.psi_e[2][((long long)i * ny1 + j) * nsmz + skm] = pn;
+                                }
+                                if (sxm >= 0) {
+                                    tB = stretch(tB, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, ep[3], &pn);
+                                    a.psi_e[3][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
+                                }
+                            }
+                            a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
+                        }
+                        if (m & 32u) {
+                            T tA = xs(hy, prevHy);
+                            T tB = xs(sH[0][r][qs], sH[0][r - 1][qs]);
+                            if constexpr (EDGE) {
+                                T pn;
+                                if (sxm >= 0) {
+                                    tA = stretch(tA, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, ep[4], &pn);
+                                    a.psi_e[4][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
+                                }
+                                if (sjm >= 0) {
+                                    tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
+                                    a.psi_e[5][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
+                                }
+                            }
+                            a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
+                        }
+                    }
+                }
+                prevHy = hy;
+                prevHz = hz;
+                sc = sn;
+            }
+        }
+        __syncthreads();  // the ring, the tables and the item slot are free again
+        continue;
+    bail:
+        // a copy did not complete in time: report it, let the copies still in
+        // flight land (bounded) before the shared memory is reused or released
+        if (tid == 0) {
+            atomicExch(err, 1);
+            for (int s = 0; s < NS; s++)
+                if (pending & (1u << s)) mbar_wait(&bars[s], (phase >> s) & 1u);
+        }
+        __syncthreads();
+        break;
+    }
+    // leave the queue; the last CTA out rewinds it for the next launch
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&queue[1], 1) == (int)gridDim.x - 1) {
+            queue[0] = 0;
+            queue[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// Variants (element type, TJ, NS, CTAs per SM): interior and edge share the
+// tile height and ring depth of a plan.
+#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4) X(float, 8, 3, 5) X(float, 16, 3, 2)
+#define RFB_Q_VARIANTS_FP64(X) X(double, 8, 3, 3) X(double, 8, 4, 2)
+
+template <typename T, int TJ, int NS, int MINB, bool EDGE>
+inline int q_grid() {
+    static int g = 0;
+    if (!g) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweep_q<T, TJ, NS, MINB, EDGE>, 32 * TJ,
+                                                      QLayout<T, TJ, NS>::total);
+        g = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
+    }
+    return g;
+}
+
+// Launch of one instantiation over n items; the grid never exceeds the items.
+// q_grid is first evaluated in q_prepare, outside any stream capture.
+#define RFB_LAUNCH_Q(TT, TJ_, NS_, MB_)                                                                      \
+    if (tj == TJ_ && ns == NS_) {                                                                            \
+        const int g = std::min(n, q_grid<TT, TJ_, NS_, MB_, EDGE>());                                        \
+        k_sweep_q<TT, TJ_, NS_, MB_, EDGE><<<g, dim3(32, TJ_), QLayout<TT, TJ_, NS_>::total, st>>>(          \
+            a, d, items, n, m, queue, err);                                                                  \
+    }
+template <typename T, bool EDGE>
+void launch_q(const Args<T> &a, const FusedDims &d, int tj, int ns, const SweepItem *items, int n, const TmaMaps &m,
+              int *queue, int *err, cudaStream_t st);
+template <bool EDGE>
+inline void launch_q_f(const Args<float> &a, const FusedDims &d, int tj, int ns, const SweepItem *items, int n,
+                       const TmaMaps &m, int *queue, int *err, cudaStream_t st) {
+    if (n <= 0) return;
+    RFB_Q_VARIANTS_FP32(RFB_LAUNCH_Q)
+}
+template <bool EDGE>
+inline void launch_q_d(const Args<double> &a, const FusedDims &d, int tj, int ns, const SweepItem *items, int n,
+                       const TmaMaps &m, int *queue, int *err, cudaStream_t st) {
+    if (n <= 0) return;
+    RFB_Q_VARIANTS_FP64(RFB_LAUNCH_Q)
+}
+
+#define RFB_PREP_Q(TT, TJ_, NS_, MB_)                                                                       \
+    if (e == cudaSuccess)                                                                                   \
+        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MB_, false>,                                      \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
+    if (e == cudaSuccess)                                                                                   \
+        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MB_, true>,                                       \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
+    if (e == cudaSuccess) {                                                                                 \
+        (void)q_grid<TT, TJ_, NS_, MB_, false>();                                                          \
+        (void)q_grid<TT, TJ_, NS_, MB_, true>();                                                           \
+    }
+static inline int q_prepare() {
+    static int done = 0;
+    if (done) return 0;
+    cudaError_t e = cudaSuccess;
+    RFB_Q_VARIANTS_FP32(RFB_PREP_Q)
+    RFB_Q_VARIANTS_FP64(RFB_PREP_Q)
+    if (e != cudaSuccess) return -1;
+    done = 1;
+    return 0;
+}
+
+#define RFB_Q_ENTRY(TT, TJ_, NS_, MB_) {TJ_, NS_, MB_},
+static const InteriorVariant kQVariantsFp32[] = {RFB_Q_VARIANTS_FP32(RFB_Q_ENTRY)};
+static const InteriorVariant kQVariantsFp64[] = {RFB_Q_VARIANTS_FP64(RFB_Q_ENTRY)};
+
+}  // namespace rfb

@@ -1,10 +1,14 @@
-"""Every interior sweep variant the autotuner may pick (TMA-fed and
-cp.async-fed, each tile height and ring depth) on scenes large enough to
-have interior work items: FP64 probe series bit-equal to the CPU oracle.
+"""Every sweep variant the autotuner may pick (cp.async-fed, TMA-fed
+interior, and the persistent work-queue sweeps that take interior and slab
+tiles by TMA; each tile height and ring depth): FP64 probe series bit-equal
+to the CPU oracle, on scenes large enough to have interior work items and,
+for the work-queue sweeps, on every small boundary case of tests/cases.py
+(PEC walls with sources on the padded planes, periodic wraps, tensors,
+per-component overrides).
 
 The sweep variant is forced per session with RFSYN_FDTD_PLAN
-("rows,ring,seg_interior,seg_edge,tma"); the session's info confirms that
-the interior sweep ran with that variant and had work."""
+("rows,ring,seg_interior,seg_edge,mode"); the session's info confirms that
+the sweep ran with that variant and had work."""
 from __future__ import annotations
 
 import ctypes as C
@@ -16,15 +20,23 @@ import oracle
 import rfsyn_b200 as rb
 from oracle import Scene
 from rfsyn_b200 import scenes
-from tests.cases import DT1, scene_run_config, workload_to_scene
+from tests.cases import CASES, DT1, scene_run_config, workload_to_scene
 
 pytestmark = pytest.mark.gpu
 
-# (rows per tile, ring depth, tma) of every compiled interior variant
+# (rows per tile, ring depth, mode) of every compiled variant; mode 0
+# cp.async interior, 1 TMA interior, 2 work-queue sweeps
 VARIANTS = {
-    rb.FP64: [(8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
-    rb.FP32: [(8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0), (16, 4, 0), (16, 3, 0)],
+    rb.FP64: [(8, 3, 2), (8, 4, 2), (8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
+    rb.FP32: [(8, 4, 2), (8, 3, 2), (16, 3, 2), (8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0),
+              (16, 4, 0), (16, 3, 0)],
 }
+QUEUE = [v for v in VARIANTS[rb.FP64] if v[2] == 2]
+MODE = {0: "cpasync", 1: "tma", 2: "queue"}
+
+
+def _vid(v):
+    return "tj%d_ns%d_%s" % (v[0], v[1], MODE[v[2]])
 
 SCENES = {
     # the headline recipe at 104^3 (5-cell CPML): interior tiles at k0 = 32, 64
@@ -50,7 +62,7 @@ def wants():
     return {name: oracle.run_oracle(s) for name, s in SCENES.items()}
 
 
-def _run(s: Scene, precision: int, variant, monkeypatch):
+def _run(s: Scene, precision: int, variant, monkeypatch, need_interior=True):
     tj, ns, tma = variant
     monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma}")
     rc = scene_run_config(s, precision, rb.FUSED)
@@ -61,21 +73,23 @@ def _run(s: Scene, precision: int, variant, monkeypatch):
     try:
         info = sim.info()
         assert (info.tile_j, info.ring_depth, info.tma) == (tj, ns, tma)
-        assert info.interior_items > 0 and info.edge_items > 0
+        assert info.edge_items > 0
+        if need_interior:
+            assert info.interior_items > 0
         sim.advance(s.n_steps)
         return sim.probes(), sim.dft()
     finally:
         sim.close()
 
 
-@pytest.mark.parametrize("variant", VARIANTS[rb.FP64], ids=lambda v: "tj%d_ns%d_%s" % (v[0], v[1], "tma" if v[2] else "cpasync"))
+@pytest.mark.parametrize("variant", VARIANTS[rb.FP64], ids=_vid)
 @pytest.mark.parametrize("name", list(SCENES))
 def test_interior_variant_fp64_bit_exact(wants, name, variant, monkeypatch):
     td, _ = _run(SCENES[name], rb.FP64, variant, monkeypatch)
     assert np.array_equal(td, wants[name]["td"])
 
 
-@pytest.mark.parametrize("variant", VARIANTS[rb.FP32], ids=lambda v: "tj%d_ns%d_%s" % (v[0], v[1], "tma" if v[2] else "cpasync"))
+@pytest.mark.parametrize("variant", VARIANTS[rb.FP32], ids=_vid)
 def test_interior_variants_fp32_agree(wants, variant, monkeypatch):
     """All FP32 variants evaluate the same expressions in the same order:
     identical probe series; and within the FP32 bound of the FP64 oracle."""
@@ -86,6 +100,15 @@ def test_interior_variants_fp32_agree(wants, variant, monkeypatch):
     want = wants["c2_104"]["td"]
     err = np.linalg.norm(td - want) / np.linalg.norm(want)
     assert err < 1e-3, err
+
+
+@pytest.mark.parametrize("variant", QUEUE, ids=_vid)
+@pytest.mark.parametrize("name", list(CASES))
+def test_queue_sweep_boundary_cases_fp64_bit_exact(name, variant, monkeypatch):
+    s = CASES[name]
+    want = oracle.run_oracle(s)
+    td, dft = _run(s, rb.FP64, variant, monkeypatch, need_interior=False)
+    assert np.array_equal(td, want["td"])
 
 
 def test_plan_override_rejects_unknown_variant(monkeypatch):
