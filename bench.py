@@ -313,6 +313,8 @@ def run_b200(args) -> None:
                    "probes": len(w.probes), "dft_bins": len(w.freqs), "spheres": len(w.spheres),
                    "list_cells": info.list_cells, "dispersive_samples": info.dispersive,
                    "schedule": "fused" if info.schedule == rb.FUSED else "split", "tile_j": info.tile_j,
+                   "sweep_mode": {0: "cp.async", 1: "tma-interior", 2: "tma-queue", 3: "tma-queue-shifted"}.get(info.tma),
+                   "ring_depth": info.ring_depth,
                    "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
                    "l2": "inputs larger than L2 (fields 6 x 2 x 76 MB per scene)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

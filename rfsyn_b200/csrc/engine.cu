@@ -424,32 +424,36 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
 // Interior sweep of the plan: TMA-fed or cp.async-fed variant, or (mode 2)
 // the persistent work-queue sweep over the interior items.
 template <typename T>
-static void launch_q_t(const Args<T> &a, const FusedPlan &p, bool edge, const TmaMaps &m, int *err, cudaStream_t st);
+static void launch_q_t(const Args<T> &a, const FusedPlan &p, int kind, const TmaMaps &m, int *err, cudaStream_t st);
 template <>
-void launch_q_t<float>(const Args<float> &a, const FusedPlan &p, bool edge, const TmaMaps &m, int *err,
+void launch_q_t<float>(const Args<float> &a, const FusedPlan &p, int kind, const TmaMaps &m, int *err,
                        cudaStream_t st) {
-    if (edge) launch_q_f<true>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
-    else launch_q_f<false>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
+    if (kind == 2) launch_q_f<2>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    else if (kind == 1) launch_q_f<1>(a, p.d, p.tj, p.ns, p.d_qx, p.n_qx, m, p.d_queue + 4, err, st);
+    else launch_q_f<0>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
 }
 template <>
-void launch_q_t<double>(const Args<double> &a, const FusedPlan &p, bool edge, const TmaMaps &m, int *err,
+void launch_q_t<double>(const Args<double> &a, const FusedPlan &p, int kind, const TmaMaps &m, int *err,
                         cudaStream_t st) {
-    if (edge) launch_q_d<true>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
-    else launch_q_d<false>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
+    if (kind == 2) launch_q_d<2>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    else if (kind == 1) launch_q_d<1>(a, p.d, p.tj, p.ns, p.d_qx, p.n_qx, m, p.d_queue + 4, err, st);
+    else launch_q_d<0>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
 }
 
 template <typename T>
 static void launch_int(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
     const TmaMaps &m = e->tmaps[e->nbuf == 2 ? par : 0];
-    if (e->plan.tma == 2) launch_q_t<T>(a, e->plan, false, m, e->d_err, st);
-    else if (e->plan.tma) launch_interior_tma<T>(a, e->plan, m, e->d_err, st);
+    if (e->plan.tma >= 2) {
+        launch_q_t<T>(a, e->plan, 0, m, e->d_err, st);
+        launch_q_t<T>(a, e->plan, 1, m, e->d_err, st);
+    } else if (e->plan.tma) launch_interior_tma<T>(a, e->plan, m, e->d_err, st);
     else launch_interior<T>(a, e->plan, st);
 }
 // Everything else of the sweep: the slab / boundary queue (mode 2) and the
 // cp.async-fed edge sweep (the items whose halo wraps, in mode 2).
 template <typename T>
 static void launch_rest(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
-    if (e->plan.tma == 2) launch_q_t<T>(a, e->plan, true, e->tmaps[e->nbuf == 2 ? par : 0], e->d_err, st);
+    if (e->plan.tma >= 2) launch_q_t<T>(a, e->plan, 2, e->tmaps[e->nbuf == 2 ? par : 0], e->d_err, st);
     launch_edge<T>(a, e->plan, st);
 }
 
@@ -485,7 +489,9 @@ static void enqueue_step(rfb_engine *e, int par) {
 }
 
 static int count_step_launches(const rfb_engine *e) {
-    int n = (e->sched == RFB_SCHED_FUSED) ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) : 2;
+    int n = (e->sched == RFB_SCHED_FUSED)
+                ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0)
+                : 2;
     if (e->scene.n_cells) n++;
     return n + 1;
 }
@@ -516,8 +522,9 @@ static void free_plan_lists(FusedPlan &p) {
     cudaFree(p.d_int);
     cudaFree(p.d_edge);
     cudaFree(p.d_qe);
-    p.d_int = p.d_edge = p.d_qe = nullptr;
-    p.n_int = p.n_edge = p.n_qe = 0;
+    cudaFree(p.d_qx);
+    p.d_int = p.d_edge = p.d_qe = p.d_qx = nullptr;
+    p.n_int = p.n_edge = p.n_qe = p.n_qx = 0;
 }
 
 // ---- tensor maps of the TMA interior sweep -----------------------------------
@@ -581,8 +588,26 @@ static int build_tma_maps(rfb_engine *e, int tj) {
     return 0;
 }
 
+// The work-queue sweeps address psi arrays and field planes with 32-bit
+// offsets: admitted only when each has fewer than 2^31 elements.
+static bool q_fits(const rfb_engine *e) {
+    const long long lim = 1LL << 31;
+    const rfb_geom_t &g = e->g;
+    const long long plane = (long long)(g.ny + 1) * e->pitch;
+    if (plane >= lim) return false;
+    if (!e->cpml.on) return true;
+    const long long x = (long long)e->cpml.eh[0].ns * plane, xm = (long long)e->cpml.em[0].ns * plane;
+    const long long y = (long long)(g.nx + 1) * std::max(e->cpml.eh[1].ns, e->cpml.em[1].ns) * e->pitch;
+    const long long z = (long long)(g.nx + 1) * (g.ny + 1) * std::max(e->cpml.eh[2].ns, e->cpml.em[2].ns);
+    return x < lim && xm < lim && y < lim && z < lim;
+}
+
 static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge) {
     const rfb_geom_t &g = e->g;
+    if (tma >= 2 && !q_fits(e)) {
+        rfb_set_error("grid too large for the work-queue sweep (32-bit offsets)");
+        return -1;
+    }
     const bool px = g.periodic & 1u, py = g.periodic & 2u, pz = g.periodic & 4u;
     FusedPlan &p = e->plan;
     free_plan_lists(p);
@@ -604,24 +629,40 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     ext(1, &ylo, &yhi, g.ny, py);
     ext(2, &zlo, &zhi, g.nz, pz);
     const int xa = px ? 0 : xlo + 1, xb = std::max(xa, xhi);
-    std::vector<SweepItem> vi, ve, vq;
+    std::vector<SweepItem> vi, ve, vq, vx;
     auto add = [](std::vector<SweepItem> &v, int j0, int k0, int b, int en, int seg) {
         for (int s = b; s < en; s += seg) v.push_back(SweepItem{j0, k0, s, std::min(en, s + seg)});
     };
     auto add_edge = [&](int j0, int rows, int k0, int b, int en) {
-        // mode 2: tiles whose halo stays inside the grid go to the TMA-fed
+        // modes 2, 3: tiles whose halo stays inside the grid go to the TMA-fed
         // slab / boundary queue; tiles whose halo wraps around a periodic
         // axis to the cp.async-fed edge sweep (8-row tiles)
-        const bool wraps = (py && (j0 == 0 || j0 + rows >= g.ny)) || (pz && (k0 == 0 || k0 + 32 >= g.nz));
-        if (tma == 2 && !wraps) {
+        const bool wraps = (py && (j0 <= 0 || j0 + rows >= g.ny)) || (pz && (k0 <= 0 || k0 + 32 >= g.nz));
+        if (tma >= 2 && !wraps) {
             add(vq, j0, k0, b, en, seg_edge);
             return;
         }
         for (int jj = j0; jj < j0 + rows && jj < p.d.cj; jj += 8) add(ve, jj, k0, b, en, seg_edge);
     };
-    for (int j0 = 0; j0 < p.d.cj; j0 += tj)
-        for (int k0 = 0; k0 < p.d.ck; k0 += 32) {
-            const bool full = j0 + tj <= p.d.cj && k0 + 32 <= p.d.ck;
+    // tile origins: multiples of (tj, 32) from 0, or in mode 3, on axes
+    // without wrap, shifted so that the first interior tile starts right
+    // after the low slab (j0 any row, k0 a multiple of 16 for the TMA boxes);
+    // the tiles below it may start at negative coordinates, their cells
+    // outside the grid are idle lanes
+    int js = 0, ks = 0;
+    if (tma == 3) {
+        if (!py) {
+            const int ja = ylo + 1;
+            js = ja - tj * ((ja + tj - 1) / tj);
+        }
+        if (!pz) {
+            const int ka = (zlo + 1 + 15) / 16 * 16;
+            ks = ka - 32 * ((ka + 31) / 32);
+        }
+    }
+    for (int j0 = js; j0 < p.d.cj; j0 += tj)
+        for (int k0 = ks; k0 < p.d.ck; k0 += 32) {
+            const bool full = j0 >= 0 && k0 >= 0 && j0 + tj <= p.d.cj && k0 + 32 <= p.d.ck;
             // the interior sweeps read the halo without wrapping it: on a
             // periodic axis the tiles at either end stay on the edge sweep
             const bool yok = py ? (j0 >= 1 && j0 + tj < g.ny) : (j0 - 1 >= ylo && j0 + tj <= yhi);
@@ -632,7 +673,13 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
                 const int sk = (int)(c % e->pitch), sj = (int)((c / e->pitch) % (g.ny + 1));
                 if (sj >= j0 && sj < j0 + tj && sk >= k0 && sk < k0 + 32) skipcell = true;
             }
-            if (full && yok && zok && !skipcell && xb > xa) {
+            if (tma >= 2 && full && yok && zok && !skipcell && xb > xa) {
+                // interior planes to the interior sweep, x-slab and
+                // x-boundary planes to the x-slab sweep
+                add(vi, j0, k0, xa, xb, seg_int);
+                add(vx, j0, k0, 0, xa, seg_edge);
+                add(vx, j0, k0, xb, p.d.ci, seg_edge);
+            } else if (full && yok && zok && !skipcell && xb > xa) {
                 add(vi, j0, k0, xa, xb, seg_int);
                 add_edge(j0, tj, k0, 0, xa);
                 add_edge(j0, tj, k0, xb, p.d.ci);
@@ -647,17 +694,20 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     p.n_int = (int)vi.size();
     p.n_edge = (int)ve.size();
     p.n_qe = (int)vq.size();
+    p.n_qx = (int)vx.size();
     if (p.n_int) CK(cudaMalloc(&p.d_int, vi.size() * sizeof(SweepItem)));
     if (p.n_edge) CK(cudaMalloc(&p.d_edge, ve.size() * sizeof(SweepItem)));
     if (p.n_qe) CK(cudaMalloc(&p.d_qe, vq.size() * sizeof(SweepItem)));
+    if (p.n_qx) CK(cudaMalloc(&p.d_qx, vx.size() * sizeof(SweepItem)));
     if (p.n_int) CK(cudaMemcpy(p.d_int, vi.data(), vi.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_edge) CK(cudaMemcpy(p.d_edge, ve.data(), ve.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_qe) CK(cudaMemcpy(p.d_qe, vq.data(), vq.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
-    if (tma == 2 && !p.d_queue) {
-        CK(cudaMalloc(&p.d_queue, 4 * sizeof(int)));
-        CK(cudaMemset(p.d_queue, 0, 4 * sizeof(int)));
+    if (p.n_qx) CK(cudaMemcpy(p.d_qx, vx.data(), vx.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
+    if (tma >= 2 && !p.d_queue) {
+        CK(cudaMalloc(&p.d_queue, 6 * sizeof(int)));
+        CK(cudaMemset(p.d_queue, 0, 6 * sizeof(int)));
     }
-    if (tma && (p.n_int || p.n_qe) && build_tma_maps(e, tj) != 0) return -1;
+    if (tma && (p.n_int || p.n_qe || p.n_qx) && build_tma_maps(e, tj) != 0) return -1;
     return 0;
 fail:
     return -1;
@@ -666,7 +716,7 @@ fail:
 static bool plan_variant_known(int prec, int tj, int ns, int tma) {
     const InteriorVariant *v;
     size_t n;
-    if (tma == 2) {
+    if (tma >= 2) {
         v = prec == RFB_FP32 ? kQVariantsFp32 : kQVariantsFp64;
         n = prec == RFB_FP32 ? std::size(kQVariantsFp32) : std::size(kQVariantsFp64);
     } else if (prec == RFB_FP32) {
@@ -725,12 +775,15 @@ static int autotune(rfb_engine *e, int active) {
         int tma;
     };
     std::vector<Cand> vars;
+    const bool qok = q_fits(e);
     if (e->prec == RFB_FP32) {
-        for (const InteriorVariant &v : kQVariantsFp32) vars.push_back({v, 2});
+        if (qok)
+            for (const InteriorVariant &v : kQVariantsFp32) vars.push_back({v, 2}), vars.push_back({v, 3});
         for (const InteriorVariant &v : kTmaVariantsFp32) vars.push_back({v, 1});
         for (const InteriorVariant &v : kIntVariantsFp32) vars.push_back({v, 0});
     } else {
-        for (const InteriorVariant &v : kQVariantsFp64) vars.push_back({v, 2});
+        if (qok)
+            for (const InteriorVariant &v : kQVariantsFp64) vars.push_back({v, 2}), vars.push_back({v, 3});
         for (const InteriorVariant &v : kTmaVariantsFp64) vars.push_back({v, 1});
         for (const InteriorVariant &v : kIntVariantsFp64) vars.push_back({v, 0});
     }
@@ -811,7 +864,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     cudaFree(e->src_val); cudaFree(e->src_hard);
     cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
-    cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_queue);
+    cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_qx); cudaFree(e->plan.d_queue);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->stream2) cudaStreamDestroy(e->stream2);
@@ -1010,7 +1063,7 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->ring_depth = e->plan.ns;
     out->tma = e->plan.tma;
     out->interior_items = e->plan.n_int;
-    out->edge_items = e->plan.n_edge + e->plan.n_qe;
+    out->edge_items = e->plan.n_edge + e->plan.n_qe + e->plan.n_qx;
     size_t sca = 0;
     if (e->cpml.on) {
         // cells of the swept volume inside the slab of each axis (H profiles)
@@ -1044,7 +1097,7 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
             launch_rest<T>(e, a, par, e->stream2);
             cudaEventRecord(e->ev_join, e->stream2);
             cudaStreamWaitEvent(e->stream, e->ev_join, 0);
-            g_launches += (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0);
+            g_launches += (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0);
         } else {
             dim3 blk(32, 8), grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
             k_h_split<T><<<grd, blk, 0, e->stream>>>(a);

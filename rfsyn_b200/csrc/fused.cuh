@@ -43,16 +43,17 @@ struct SweepItem {
 struct FusedPlan {
     int tj = 8, ns = 6;   // interior variant (rows per tile, ring depth)
     // interior planes staged per thread by cp.async (0), by the TMA (1), or
-    // (2) interior and slab tiles both by the TMA in the persistent
-    // work-queue sweeps k_sweep_q (sweep.cuh)
+    // (2, 3) interior and slab tiles both by the TMA in the persistent
+    // work-queue sweeps k_sweep_q (sweep.cuh); 3 shifts the tile origins of
+    // axes without wrap so that interior tiles start right after the slab
     int tma = 0;
     FusedDims d;
     int seg_int = 64, seg_edge = 32;
     int n_int = 0, n_edge = 0;
     SweepItem *d_int = nullptr, *d_edge = nullptr;  // device work lists
-    int n_qe = 0;                                   // mode 2: slab / boundary items of k_sweep_q<EDGE>
-    SweepItem *d_qe = nullptr;
-    int *d_queue = nullptr;                         // mode 2: counters (interior 0-1, edge 2-3)
+    int n_qe = 0, n_qx = 0;                         // modes 2, 3: edge and x-slab items of k_sweep_q
+    SweepItem *d_qe = nullptr, *d_qx = nullptr;
+    int *d_queue = nullptr;                         // counters (interior 0-1, edge 2-3, x slab 4-5)
 };
 
 template <typename T>
@@ -148,7 +149,7 @@ __device__ __forceinline__ IssuePlan make_issue_plan(const Args<T> &a, int j0, i
         ip.job_off = (vj && vk) ? jj * (int)a.pitch + kk : -1;
     } else if (ip.job == 4) {
         const int j = j0 + ip.job_r, k = k0 + 4 * ip.job_q;
-        ip.job_off = (a.codes && j <= a.ny && k <= a.nz) ? j * (int)a.pitch + k : -1;
+        ip.job_off = (a.codes && j >= 0 && k >= 0 && j <= a.ny && k <= a.nz) ? j * (int)a.pitch + k : -1;
     }
     return ip;
 }
@@ -345,7 +346,9 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
     const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
     const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
     const int j = j0 + ty, k = k0 + tx;
-    const bool own = j < d.cj && k < d.ck;
+    // tiles may start at negative coordinates on an axis without wrap (the
+    // work-queue plans shift the tile origins); cells outside the grid idle
+    const bool own = j >= 0 && k >= 0 && j < d.cj && k < d.ck;
     const bool row_halo = (j0 > 0 || py);
     const bool col_halo = (k0 > 0 || pz);
     const int jh = j0 > 0 ? j0 - 1 : a.ny - 1;
@@ -425,7 +428,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
                 cp_async(&st.psi[10][r][q], a.psi_e[4] + o, true);
             }
         }
-        if (ty == 0 && row_halo && k < d.ck) {
+        if (ty == 0 && row_halo && k >= 0 && k < d.ck) {
             // row halo (j0-1, k): Hx (hx_y, hx_z), Hz (hz_x, hz_y)
             if (sjh_row >= 0) {
                 const long long o = ((long long)p * nshy + sjh_row) * a.pitch + k;
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
                 const long long o = ((long long)sxh * ny1 + jh) * a.pitch + k;
                 cp_async(&st.psi[4][0][q], a.psi_hi[4] + o, true);
             }
-        } else if (ty == 1 && tx < TJ && col_halo && jc < d.cj) {
+        } else if (ty == 1 && tx < TJ && col_halo && jc >= 0 && jc < d.cj) {
             // column halo (j0+tx, k0-1): Hx (hx_y, hx_z), Hy (hy_z, hy_x)
             if (sjh_col >= 0) {
                 const long long o = ((long long)p * nshy + sjh_col) * a.pitch + kh;
@@ -569,10 +572,10 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
         sH[0][r][q] = hx;
         sH[1][r][q] = hy;
         sH[2][r][q] = hz;
-        if (ty == 0 && row_halo && k < d.ck) {
+        if (ty == 0 && row_halo && k >= 0 && k < d.ck) {
             sH[0][0][q] = h_edge(0, i, jh, k, 0, q, sjh_row, skh, 0, q, cs, ns, false);
             sH[2][0][q] = h_edge(2, i, jh, k, 0, q, sjh_row, skh, 0, q, cs, ns, false);
-        } else if (ty == 1 && tx < TJ && col_halo && jc < d.cj) {
+        } else if (ty == 1 && tx < TJ && col_halo && jc >= 0 && jc < d.cj) {
             sH[0][tx + 1][0] = h_edge(0, i, jc, kh, tx + 1, 0, sjh_col, skh_col, tx + 1, 0, cs, ns, false);
             sH[1][tx + 1][0] = h_edge(1, i, jc, kh, tx + 1, 0, sjh_col, skh_col, tx + 1, 0, cs, ns, false);
         }

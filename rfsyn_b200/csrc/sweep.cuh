@@ -1,13 +1,18 @@
 // sweep.cuh -- persistent, TMA-fed H+E sweep over a device work queue.
 //
-// One step of the fused schedule is two launches of k_sweep_q, side by side
-// on two streams: the interior instantiation (EDGE = false) takes the work
-// items whose tiles, halos and planes lie outside every CPML slab and PEC
-// boundary; the edge instantiation (EDGE = true) takes all other items whose
-// halo does not wrap around a periodic axis, with rfsyn's per-component
-// update ranges (engine/fdtd/cpml.c:176-219, materials.c:911-1060) and the
-// slab-stored psi recursions (cpml.h:46-51).  Items whose halo wraps stay on
-// the cp.async-fed k_sweep_edge (fused.cuh).
+// One step of the fused schedule is three launches of k_sweep_q on two
+// streams, one per kind of work item:
+//   KIND 0 (interior) -- tiles whose cells, halos and planes lie outside
+//     every CPML slab and PEC boundary: branch-free, no psi;
+//   KIND 1 (x slab) -- the same tiles' planes inside the x slab or on an x
+//     boundary: x-slab psi and plane conditions, both uniform per plane;
+//   KIND 2 (edge) -- all other tiles whose halo does not wrap around a
+//     periodic axis, with rfsyn's per-component update ranges
+//     (engine/fdtd/cpml.c:176-219, materials.c:911-1060) and every slab
+//     psi recursion (cpml.h:46-51).
+// Items whose halo wraps stay on the cp.async-fed k_sweep_edge (fused.cuh).
+// Each kind is compiled separately so the interior keeps the lean
+// instruction stream it needs to stay bandwidth-bound.
 //
 // The grid is sized to the resident CTAs (SM count x CTAs per SM); each CTA
 // pops items from a device counter until the list is exhausted, so uneven
@@ -51,11 +56,13 @@ struct QLayout {
     static constexpr size_t total = misc + 16;
 };
 
-template <typename T, int TJ, int NS, int MINB, bool EDGE>
+template <typename T, int TJ, int NS, int MINB, int KIND>
 __global__ void __launch_bounds__(32 * TJ, MINB)
     k_sweep_q(Args<T> a, FusedDims d, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps,
               int *queue, int *err) {
     static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
+    constexpr bool EDGE = KIND == 2;  // per-cell y / z conditions and slabs
+    constexpr bool XS = KIND >= 1;    // x-slab psi and plane conditions
     using L = TmaLayout<T, TJ, NS>;
     using S = QLayout<T, TJ, NS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -124,15 +131,22 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             pending &= ~(1u << s);
         };
 
-        // ---- per-thread geometry of the item (EDGE) ----
+        // ---- per-thread geometry of the item ----
+        // The interior instantiation takes tiles whose cells and halos lie
+        // outside the y / z slabs and boundaries: every component is swept
+        // at every (j, k), only the plane (x) conditions and x-slab psi
+        // remain, both uniform per plane.  The edge instantiation adds the
+        // per-cell y / z conditions and y / z slab psi.
         const int j = j0 + ty, k = k0 + tx;
-        const bool own = !EDGE || (j < d.cj && k < d.ck);
-        // component masks at (j, k): bits 0-2 H, 3-5 E (plane conditions apart)
-        unsigned mjk = 0x3f;
-        bool rowh = true, colh = tx < TJ;  // halo cells this thread recomputes
+        const bool own = !EDGE || (j >= 0 && k >= 0 && j < d.cj && k < d.ck);
+        const int pitch = (int)a.pitch;
+        const int plane32 = (int)a.plane;
+        const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
+        unsigned mjk = 0x3f;                   // bits 0-2 H, 3-5 E at (j, k), plane apart
+        bool rowh = true, colh = tx < TJ;      // halo cells this thread recomputes
         int sjh = -1, skh = -1, sjm = -1, skm = -1;
         int sjh_row = -1, sjh_col = -1, skh_col = -1;
-        const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
+        unsigned mrow_jk = 5u, mcol_jk = 3u;   // halo components at (j, k), plane apart
         if constexpr (EDGE) {
             const int jmin = py ? 0 : 1, kmin = pz ? 0 : 1;
             mjk = 0;
@@ -146,8 +160,10 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                     if (j >= jmin) mjk |= 32u;
                 }
             }
-            rowh = j0 > 0 && k < d.ck;
-            colh = tx < TJ && k0 > 0 && jc < d.cj;
+            rowh = j0 > 0 && k >= 0 && k < d.ck;
+            colh = tx < TJ && k0 > 0 && jc >= 0 && jc < d.cj;
+            mrow_jk = (k < a.nz ? 1u : 0u) | (k < a.nz + (pz ? 0 : 1) ? 4u : 0u);
+            mcol_jk = (jc < a.ny ? 1u : 0u) | (jc < a.ny + (py ? 0 : 1) ? 2u : 0u);
             sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
             skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
             sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
@@ -171,15 +187,49 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             }
         }
         const int nshy = a.ns_h[1], nshz = a.ns_h[2], nsmy = a.ns_m[1], nsmz = a.ns_m[2];
+        // 32-bit element offsets (the plan admits these sweeps only when every
+        // field plane and psi array has fewer than 2^31 elements): in-plane
+        // offsets (x-slab psi arrays are planes of the field layout), y-slab
+        // offsets s*pitch + k, z-slab offsets j*ns + s; per plane a uniform
+        // base is added
+        struct Cell {
+            int ox, oy, oz;  // x-, y-, z-slab array offsets (plane / slab bases apart)
+            int sy, sz;      // H-grid y / z slab indices (-1 outside)
+        };
+        const Cell own_c = {j * pitch + k, sjh * pitch + k, j * nshz + skh, sjh, skh};
+        const Cell row_c = {jh * pitch + k, sjh_row * pitch + k, jh * nshz + skh, sjh_row, skh};
+        const Cell col_c = {jc * pitch + kh, sjh_col * pitch + kh, jc * nshz + skh_col, sjh_col, skh_col};
+        const int oym = sjm * pitch + k, ozm = j * nsmz + skm;
+        // per-plane uniform bases of the H-side psi arrays and the plane's x
+        // profile (kappa_inv, b, a) on the H and E grids
+        struct PlaneB {
+            int by, bz, bx, sx;
+        };
+        auto plane_b = [&](int i) -> PlaneB {
+            const int sx = (XS && on) ? slab_in(i, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
+            return PlaneB{i * nshy * pitch, i * (int)ny1 * nshz, sx * plane32, sx};
+        };
+        T xph[3] = {T(1), T(1), T(0)}, xpm[3] = {T(1), T(1), T(0)};
+        auto load_xprof = [&](int i, int sxh_, int sxm_) {
+            if constexpr (!XS) return;
+            if (sxh_ >= 0) {
+                xph[0] = a.kinv_h[0][i];
+                xph[1] = a.b_h[0][i];
+                xph[2] = a.a_h[0][i];
+            }
+            if (sxm_ >= 0) {
+                xpm[0] = a.kinv_m[0][i];
+                xpm[1] = a.b_m[0][i];
+                xpm[2] = a.a_m[0][i];
+            }
+        };
 
         // H of component c at plane i (slots sc / sn) for the cell at stage
-        // position (rr, qq) with coordinates (jj, kk): unstretched, or (EDGE)
-        // with the slab psi recursions; yi / zi are its rows in the profile
-        // tables, sy / sz its H-grid slab indices, sx the plane's.  pA / pB
-        // are the cell's psi inputs of the two terms (used where a slab
-        // applies); the updated psi are stored when `store`.
-        auto hcell = [&](int c, int i, int sc, int sn, int rr, int qq, int jj, int kk, int yi, int zi, int sy,
-                         int sz, int sx, T pA, T pB, bool store) -> T {
+        // position (rr, qq) described by `cl`; yi / zi are its rows in the
+        // profile tables.  pA / pB are the cell's psi inputs of the two terms
+        // (used where a slab applies); the updated psi are stored when `store`.
+        auto hcell = [&](int c, const PlaneB &pb, int sc, int sn, int rr, int qq, const Cell &cl, int yi, int zi,
+                         T pA, T pB, bool store) -> T {
             const T hin = H(sc, c)[rr][qq];
             T dA, dB;
             if (c == 0) {
@@ -192,57 +242,55 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                 dA = xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]);
                 dB = xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq]);
             }
-            if constexpr (EDGE) {
-                T pn;
-                if (c == 0) {
-                    if (sy >= 0) {
-                        dA = stretch(dA, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pA, &pn);
-                        if (store) a.psi_ho[0][((long long)i * nshy + sy) * a.pitch + kk] = pn;
-                    }
-                    if (sz >= 0) {
-                        dB = stretch(dB, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pB, &pn);
-                        if (store) a.psi_ho[1][((long long)i * ny1 + jj) * nshz + sz] = pn;
-                    }
-                } else if (c == 1) {
-                    if (sz >= 0) {
-                        dA = stretch(dA, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pA, &pn);
-                        if (store) a.psi_ho[2][((long long)i * ny1 + jj) * nshz + sz] = pn;
-                    }
-                    if (sx >= 0) {
-                        dB = stretch(dB, a.kinv_h[0][i], a.b_h[0][i], a.a_h[0][i], a.dx, pB, &pn);
-                        if (store) a.psi_ho[3][((long long)sx * ny1 + jj) * a.pitch + kk] = pn;
-                    }
-                } else {
-                    if (sx >= 0) {
-                        dA = stretch(dA, a.kinv_h[0][i], a.b_h[0][i], a.a_h[0][i], a.dx, pA, &pn);
-                        if (store) a.psi_ho[4][((long long)sx * ny1 + jj) * a.pitch + kk] = pn;
-                    }
-                    if (sy >= 0) {
-                        dB = stretch(dB, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pB, &pn);
-                        if (store) a.psi_ho[5][((long long)i * nshy + sy) * a.pitch + kk] = pn;
-                    }
+            T pn;
+            if (c == 0) {
+                if (EDGE && cl.sy >= 0) {
+                    dA = stretch(dA, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pA, &pn);
+                    if (store) a.psi_ho[0][pb.by + cl.oy] = pn;
+                }
+                if (EDGE && cl.sz >= 0) {
+                    dB = stretch(dB, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pB, &pn);
+                    if (store) a.psi_ho[1][pb.bz + cl.oz] = pn;
+                }
+            } else if (c == 1) {
+                if (EDGE && cl.sz >= 0) {
+                    dA = stretch(dA, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pA, &pn);
+                    if (store) a.psi_ho[2][pb.bz + cl.oz] = pn;
+                }
+                if (pb.sx >= 0) {
+                    dB = stretch(dB, xph[0], xph[1], xph[2], a.dx, pB, &pn);
+                    if (store) a.psi_ho[3][pb.bx + cl.ox] = pn;
+                }
+            } else {
+                if (pb.sx >= 0) {
+                    dA = stretch(dA, xph[0], xph[1], xph[2], a.dx, pA, &pn);
+                    if (store) a.psi_ho[4][pb.bx + cl.ox] = pn;
+                }
+                if (EDGE && cl.sy >= 0) {
+                    dB = stretch(dB, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pB, &pn);
+                    if (store) a.psi_ho[5][pb.by + cl.oy] = pn;
                 }
             }
             return xs(hin, xm(cbh, xs(dA, dB)));
         };
         // psi inputs of H component c at a cell (zero where no slab applies)
-        auto hpsi = [&](int c, int i, int jj, int kk, int sy, int sz, int sx, T &pA, T &pB) {
+        auto hpsi = [&](int c, const PlaneB &pb, const Cell &cl, T &pA, T &pB) {
             pA = T(0);
             pB = T(0);
             if (c == 0) {
-                if (sy >= 0) pA = a.psi_hi[0][((long long)i * nshy + sy) * a.pitch + kk];
-                if (sz >= 0) pB = a.psi_hi[1][((long long)i * ny1 + jj) * nshz + sz];
+                if (EDGE && cl.sy >= 0) pA = a.psi_hi[0][pb.by + cl.oy];
+                if (EDGE && cl.sz >= 0) pB = a.psi_hi[1][pb.bz + cl.oz];
             } else if (c == 1) {
-                if (sz >= 0) pA = a.psi_hi[2][((long long)i * ny1 + jj) * nshz + sz];
-                if (sx >= 0) pB = a.psi_hi[3][((long long)sx * ny1 + jj) * a.pitch + kk];
+                if (EDGE && cl.sz >= 0) pA = a.psi_hi[2][pb.bz + cl.oz];
+                if (pb.sx >= 0) pB = a.psi_hi[3][pb.bx + cl.ox];
             } else {
-                if (sx >= 0) pA = a.psi_hi[4][((long long)sx * ny1 + jj) * a.pitch + kk];
-                if (sy >= 0) pB = a.psi_hi[5][((long long)i * nshy + sy) * a.pitch + kk];
+                if (pb.sx >= 0) pA = a.psi_hi[4][pb.bx + cl.ox];
+                if (EDGE && cl.sy >= 0) pB = a.psi_hi[5][pb.by + cl.oy];
             }
         };
         // plane conditions: H bits (Hx to nx inclusive on a PEC x axis), E bits
         auto plane_mask = [&](int i) -> unsigned {
-            if constexpr (!EDGE) return 0x3fu;
+            if constexpr (!XS) return 0x3fu;
             unsigned m = 0;
             if (i < a.nx + (px ? 0 : 1)) m |= 1u;
             if (i < a.nx) m |= 2u | 4u | 8u;
@@ -266,14 +314,21 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             T prevHy = T(0), prevHz = T(0);
             if (pprev >= 0) {
                 const unsigned mp = plane_mask(pprev) & mjk;
-                const int sxp = EDGE ? slab_in(pprev, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
+                const PlaneB pb = plane_b(pprev);
+                load_xprof(pprev, pb.sx, -1);
+                // psi are read only for components swept at the cell, so
+                // every offset used addresses a cell of the grid
                 T pA = T(0), pB = T(0);
-                if constexpr (EDGE) hpsi(1, pprev, j, k, sjh, skh, sxp, pA, pB);
-                prevHy = (mp & 2u) ? hcell(1, pprev, NS - 1, 0, r, q, j, k, r, qs, sjh, skh, sxp, pA, pB, false)
-                                   : H(NS - 1, 1)[r][q];
-                if constexpr (EDGE) hpsi(2, pprev, j, k, sjh, skh, sxp, pA, pB);
-                prevHz = (mp & 4u) ? hcell(2, pprev, NS - 1, 0, r, q, j, k, r, qs, sjh, skh, sxp, pA, pB, false)
-                                   : H(NS - 1, 2)[r][q];
+                prevHy = H(NS - 1, 1)[r][q];
+                if (mp & 2u) {
+                    hpsi(1, pb, own_c, pA, pB);
+                    prevHy = hcell(1, pb, NS - 1, 0, r, q, own_c, r, qs, pA, pB, false);
+                }
+                prevHz = H(NS - 1, 2)[r][q];
+                if (mp & 4u) {
+                    hpsi(2, pb, own_c, pA, pB);
+                    prevHz = hcell(2, pb, NS - 1, 0, r, q, own_c, r, qs, pA, pB, false);
+                }
             }
             __syncthreads();  // slot NS-1 may now be refilled
 
@@ -285,40 +340,54 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                     issue(sf, pf);
                     pf = plane_after(pf, a.nx, px);
                 }
-                const unsigned m = plane_mask(i) & mjk;
-                const int sxh = EDGE ? slab_in(i, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
-                const int sxm = EDGE ? slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on) : -1;
-                // psi inputs of the own cell, loaded before the wait
-                T hp[6], ep[6];
+                const unsigned mpl = plane_mask(i);
+                const unsigned m = mpl & mjk;
+                const PlaneB pb = plane_b(i);
+                const int sxm = (XS && on) ? slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on) : -1;
+                const int bym = i * nsmy * pitch, bzm = i * (int)ny1 * nsmz, bxm = sxm * plane32;
+                // halo cells recomputed this plane: row (j0-1, k) Hx, Hz;
+                // column (j0+tx, k0-1) Hx, Hy
+                const unsigned mrow = (ty == 0 && rowh) ? (mpl & mrow_jk) : 0u;
+                const unsigned mcol = (ty == 1 && colh) ? (mpl & mcol_jk) : 0u;
+                // psi inputs of the own cell and of the halo cells and the
+                // plane's x profile, all loaded before the wait; psi are read
+                // only for components swept at the cell, so every offset
+                // used addresses a cell of the grid
+                T hp[6], ep[6], hh[4];
 #pragma unroll
                 for (int t = 0; t < 6; t++) hp[t] = ep[t] = T(0);
-                if constexpr (EDGE) {
-                    if (m & 1u) hpsi(0, i, j, k, sjh, skh, sxh, hp[0], hp[1]);
-                    if (m & 2u) hpsi(1, i, j, k, sjh, skh, sxh, hp[2], hp[3]);
-                    if (m & 4u) hpsi(2, i, j, k, sjh, skh, sxh, hp[4], hp[5]);
-                    if (m & 8u) {
-                        if (sjm >= 0) ep[0] = a.psi_e[0][((long long)i * nsmy + sjm) * a.pitch + k];
-                        if (skm >= 0) ep[1] = a.psi_e[1][((long long)i * ny1 + j) * nsmz + skm];
-                    }
-                    if (m & 16u) {
-                        if (skm >= 0) ep[2] = a.psi_e[2][((long long)i * ny1 + j) * nsmz + skm];
-                        if (sxm >= 0) ep[3] = a.psi_e[3][((long long)sxm * ny1 + j) * a.pitch + k];
-                    }
-                    if (m & 32u) {
-                        if (sxm >= 0) ep[4] = a.psi_e[4][((long long)sxm * ny1 + j) * a.pitch + k];
-                        if (sjm >= 0) ep[5] = a.psi_e[5][((long long)i * nsmy + sjm) * a.pitch + k];
-                    }
+#pragma unroll
+                for (int t = 0; t < 4; t++) hh[t] = T(0);
+                load_xprof(i, pb.sx, sxm);
+                if (m & 1u) hpsi(0, pb, own_c, hp[0], hp[1]);
+                if (m & 2u) hpsi(1, pb, own_c, hp[2], hp[3]);
+                if (m & 4u) hpsi(2, pb, own_c, hp[4], hp[5]);
+                if (mrow & 1u) hpsi(0, pb, row_c, hh[0], hh[1]);
+                if (mrow & 4u) hpsi(2, pb, row_c, hh[2], hh[3]);
+                if (mcol & 1u) hpsi(0, pb, col_c, hh[0], hh[1]);
+                if (mcol & 2u) hpsi(1, pb, col_c, hh[2], hh[3]);
+                if (m & 8u) {
+                    if (EDGE && sjm >= 0) ep[0] = a.psi_e[0][bym + oym];
+                    if (EDGE && skm >= 0) ep[1] = a.psi_e[1][bzm + ozm];
+                }
+                if (m & 16u) {
+                    if (EDGE && skm >= 0) ep[2] = a.psi_e[2][bzm + ozm];
+                    if (sxm >= 0) ep[3] = a.psi_e[3][bxm + own_c.ox];
+                }
+                if (m & 32u) {
+                    if (sxm >= 0) ep[4] = a.psi_e[4][bxm + own_c.ox];
+                    if (EDGE && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
                 }
                 wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
                 if (__syncthreads_or(failed)) goto bail;
                 const T e0 = E(sc, 0)[r][q], e1 = E(sc, 1)[r][q], e2 = E(sc, 2)[r][q];
                 const int code = with_codes ? (int)CODE(sc)[ty][tx] : 0;
-                const long long c = (long long)i * a.plane + (long long)j * a.pitch + k;
+                const long long c = (long long)i * a.plane + own_c.ox;
                 T hx = H(sc, 0)[r][q], hy = H(sc, 1)[r][q], hz = H(sc, 2)[r][q];
-                if (m & 1u) hx = hcell(0, i, sc, sn, r, q, j, k, r, qs, sjh, skh, sxh, hp[0], hp[1], true);
-                if (m & 2u) hy = hcell(1, i, sc, sn, r, q, j, k, r, qs, sjh, skh, sxh, hp[2], hp[3], true);
-                if (m & 4u) hz = hcell(2, i, sc, sn, r, q, j, k, r, qs, sjh, skh, sxh, hp[4], hp[5], true);
-                if (own && (!EDGE || i < d.ci)) {
+                if (m & 1u) hx = hcell(0, pb, sc, sn, r, q, own_c, r, qs, hp[0], hp[1], true);
+                if (m & 2u) hy = hcell(1, pb, sc, sn, r, q, own_c, r, qs, hp[2], hp[3], true);
+                if (m & 4u) hz = hcell(2, pb, sc, sn, r, q, own_c, r, qs, hp[4], hp[5], true);
+                if (own) {
                     a.Ho[0][c] = hx;
                     a.Ho[1][c] = hy;
                     a.Ho[2][c] = hz;
@@ -326,43 +395,21 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                 sH[0][r][qs] = hx;
                 sH[1][r][qs] = hy;
                 sH[2][r][qs] = hz;
-                if (ty == 0) {
-                    if (rowh) {
-                        // row halo (j0-1, k): Hx, Hz
-                        const unsigned mh = plane_mask(i) & (EDGE ? ((k < a.nz ? 1u : 0u) |
-                                                                     (k < a.nz + (pz ? 0 : 1) ? 4u : 0u))
-                                                                  : 5u);
-                        T pA = T(0), pB = T(0);
-                        T v = H(sc, 0)[0][q];
-                        if (mh & 1u) {
-                            if constexpr (EDGE) hpsi(0, i, jh, k, sjh_row, skh, sxh, pA, pB);
-                            v = hcell(0, i, sc, sn, 0, q, jh, k, 0, qs, sjh_row, skh, sxh, pA, pB, false);
-                        }
-                        sH[0][0][qs] = v;
-                        v = H(sc, 2)[0][q];
-                        if (mh & 4u) {
-                            if constexpr (EDGE) hpsi(2, i, jh, k, sjh_row, skh, sxh, pA, pB);
-                            v = hcell(2, i, sc, sn, 0, q, jh, k, 0, qs, sjh_row, skh, sxh, pA, pB, false);
-                        }
-                        sH[2][0][qs] = v;
-                    }
+                if (ty == 0 && rowh) {
+                    // row halo (j0-1, k): Hx, Hz
+                    T v = H(sc, 0)[0][q];
+                    if (mrow & 1u) v = hcell(0, pb, sc, sn, 0, q, row_c, 0, qs, hh[0], hh[1], false);
+                    sH[0][0][qs] = v;
+                    v = H(sc, 2)[0][q];
+                    if (mrow & 4u) v = hcell(2, pb, sc, sn, 0, q, row_c, 0, qs, hh[2], hh[3], false);
+                    sH[2][0][qs] = v;
                 } else if (ty == 1 && colh) {
                     // column halo (j0+tx, k0-1): Hx, Hy
-                    const unsigned mh = plane_mask(i) & (EDGE ? ((jc < a.ny ? 1u : 0u) |
-                                                                 (jc < a.ny + (py ? 0 : 1) ? 2u : 0u))
-                                                              : 3u);
-                    T pA = T(0), pB = T(0);
                     T v = H(sc, 0)[tx + 1][3];
-                    if (mh & 1u) {
-                        if constexpr (EDGE) hpsi(0, i, jc, kh, sjh_col, skh_col, sxh, pA, pB);
-                        v = hcell(0, i, sc, sn, tx + 1, 3, jc, kh, tx + 1, 0, sjh_col, skh_col, sxh, pA, pB, false);
-                    }
+                    if (mcol & 1u) v = hcell(0, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[0], hh[1], false);
                     sH[0][tx + 1][0] = v;
                     v = H(sc, 1)[tx + 1][3];
-                    if (mh & 2u) {
-                        if constexpr (EDGE) hpsi(1, i, jc, kh, sjh_col, skh_col, sxh, pA, pB);
-                        v = hcell(1, i, sc, sn, tx + 1, 3, jc, kh, tx + 1, 0, sjh_col, skh_col, sxh, pA, pB, false);
-                    }
+                    if (mcol & 2u) v = hcell(1, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[2], hh[3], false);
                     sH[1][tx + 1][0] = v;
                 }
                 __syncthreads();
@@ -374,51 +421,43 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                     }
                     if (!skip) {
                         const T ca = tt.tab[code], cb = tt.tab[256 + code];
+                        T pn;
                         if (m & 8u) {
                             T tA = xs(sH[2][r][qs], sH[2][r - 1][qs]);
                             T tB = xs(sH[1][r][qs], sH[1][r][qs - 1]);
-                            if constexpr (EDGE) {
-                                T pn;
-                                if (sjm >= 0) {
-                                    tA = stretch(tA, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[0], &pn);
-                                    a.psi_e[0][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
-                                }
-                                if (skm >= 0) {
-                                    tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
-                                    a.psi_e[1][((long long)i * ny1 + j) * nsmz + skm] = pn;
-                                }
+                            if (EDGE && sjm >= 0) {
+                                tA = stretch(tA, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[0], &pn);
+                                a.psi_e[0][bym + oym] = pn;
+                            }
+                            if (EDGE && skm >= 0) {
+                                tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
+                                a.psi_e[1][bzm + ozm] = pn;
                             }
                             a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
                         }
                         if (m & 16u) {
                             T tA = xs(sH[0][r][qs], sH[0][r][qs - 1]);
                             T tB = xs(hz, prevHz);
-                            if constexpr (EDGE) {
-                                T pn;
-                                if (skm >= 0) {
-                                    tA = stretch(tA, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[2], &pn);
-                                    a.psi_e[2][((long long)i * ny1 + j) * nsmz + skm] = pn;
-                                }
-                                if (sxm >= 0) {
-                                    tB = stretch(tB, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, ep[3], &pn);
-                                    a.psi_e[3][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
-                                }
+                            if (EDGE && skm >= 0) {
+                                tA = stretch(tA, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[2], &pn);
+                                a.psi_e[2][bzm + ozm] = pn;
+                            }
+                            if (sxm >= 0) {
+                                tB = stretch(tB, xpm[0], xpm[1], xpm[2], a.dx, ep[3], &pn);
+                                a.psi_e[3][bxm + own_c.ox] = pn;
                             }
                             a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
                         }
                         if (m & 32u) {
                             T tA = xs(hy, prevHy);
                             T tB = xs(sH[0][r][qs], sH[0][r - 1][qs]);
-                            if constexpr (EDGE) {
-                                T pn;
-                                if (sxm >= 0) {
-                                    tA = stretch(tA, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, ep[4], &pn);
-                                    a.psi_e[4][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
-                                }
-                                if (sjm >= 0) {
-                                    tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
-                                    a.psi_e[5][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
-                                }
+                            if (sxm >= 0) {
+                                tA = stretch(tA, xpm[0], xpm[1], xpm[2], a.dx, ep[4], &pn);
+                                a.psi_e[4][bxm + own_c.ox] = pn;
+                            }
+                            if (EDGE && sjm >= 0) {
+                                tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
+                                a.psi_e[5][bym + oym] = pn;
                             }
                             a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
                         }
@@ -453,19 +492,20 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     }
 }
 
-// Variants (element type, TJ, NS, CTAs per SM): interior and edge share the
-// tile height and ring depth of a plan.
-#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4) X(float, 8, 3, 5) X(float, 16, 3, 2)
-#define RFB_Q_VARIANTS_FP64(X) X(double, 8, 3, 3) X(double, 8, 4, 2)
+// Variants (element type, TJ, NS, CTAs per SM of the interior and of the
+// edge instantiation): interior and edge share the tile height and ring
+// depth of a plan.
+#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 4) X(float, 8, 3, 5, 4) X(float, 16, 3, 2, 2)
+#define RFB_Q_VARIANTS_FP64(X) X(double, 8, 3, 3, 2) X(double, 8, 4, 2, 2)
 
-template <typename T, int TJ, int NS, int MINB, bool EDGE>
+template <typename T, int TJ, int NS, int MINB, int KIND>
 inline int q_grid() {
     static int g = 0;
     if (!g) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweep_q<T, TJ, NS, MINB, EDGE>, 32 * TJ,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweep_q<T, TJ, NS, MINB, KIND>, 32 * TJ,
                                                       QLayout<T, TJ, NS>::total);
         g = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
     }
@@ -474,38 +514,43 @@ inline int q_grid() {
 
 // Launch of one instantiation over n items; the grid never exceeds the items.
 // q_grid is first evaluated in q_prepare, outside any stream capture.
-#define RFB_LAUNCH_Q(TT, TJ_, NS_, MB_)                                                                      \
+#define RFB_LAUNCH_Q(TT, TJ_, NS_, MBI_, MBE_)                                                               \
     if (tj == TJ_ && ns == NS_) {                                                                            \
-        const int g = std::min(n, q_grid<TT, TJ_, NS_, MB_, EDGE>());                                        \
-        k_sweep_q<TT, TJ_, NS_, MB_, EDGE><<<g, dim3(32, TJ_), QLayout<TT, TJ_, NS_>::total, st>>>(          \
+        constexpr int MB_ = KIND == 0 ? MBI_ : MBE_;                                                         \
+        const int g = std::min(n, q_grid<TT, TJ_, NS_, MB_, KIND>());                                        \
+        k_sweep_q<TT, TJ_, NS_, MB_, KIND><<<g, dim3(32, TJ_), QLayout<TT, TJ_, NS_>::total, st>>>(          \
             a, d, items, n, m, queue, err);                                                                  \
     }
-template <typename T, bool EDGE>
+template <typename T, int KIND>
 void launch_q(const Args<T> &a, const FusedDims &d, int tj, int ns, const SweepItem *items, int n, const TmaMaps &m,
               int *queue, int *err, cudaStream_t st);
-template <bool EDGE>
+template <int KIND>
 inline void launch_q_f(const Args<float> &a, const FusedDims &d, int tj, int ns, const SweepItem *items, int n,
                        const TmaMaps &m, int *queue, int *err, cudaStream_t st) {
     if (n <= 0) return;
     RFB_Q_VARIANTS_FP32(RFB_LAUNCH_Q)
 }
-template <bool EDGE>
+template <int KIND>
 inline void launch_q_d(const Args<double> &a, const FusedDims &d, int tj, int ns, const SweepItem *items, int n,
                        const TmaMaps &m, int *queue, int *err, cudaStream_t st) {
     if (n <= 0) return;
     RFB_Q_VARIANTS_FP64(RFB_LAUNCH_Q)
 }
 
-#define RFB_PREP_Q(TT, TJ_, NS_, MB_)                                                                       \
+#define RFB_PREP_Q(TT, TJ_, NS_, MBI_, MBE_)                                                                \
     if (e == cudaSuccess)                                                                                   \
-        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MB_, false>,                                      \
+        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MBI_, 0>,                                         \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
     if (e == cudaSuccess)                                                                                   \
-        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MB_, true>,                                       \
+        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MBE_, 1>,                                         \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
+    if (e == cudaSuccess)                                                                                   \
+        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MBE_, 2>,                                         \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
     if (e == cudaSuccess) {                                                                                 \
-        (void)q_grid<TT, TJ_, NS_, MB_, false>();                                                          \
-        (void)q_grid<TT, TJ_, NS_, MB_, true>();                                                           \
+        (void)q_grid<TT, TJ_, NS_, MBI_, 0>();                                                             \
+        (void)q_grid<TT, TJ_, NS_, MBE_, 1>();                                                             \
+        (void)q_grid<TT, TJ_, NS_, MBE_, 2>();                                                             \
     }
 static inline int q_prepare() {
     static int done = 0;
@@ -518,7 +563,7 @@ static inline int q_prepare() {
     return 0;
 }
 
-#define RFB_Q_ENTRY(TT, TJ_, NS_, MB_) {TJ_, NS_, MB_},
+#define RFB_Q_ENTRY(TT, TJ_, NS_, MBI_, MBE_) {TJ_, NS_, MBI_},
 static const InteriorVariant kQVariantsFp32[] = {RFB_Q_VARIANTS_FP32(RFB_Q_ENTRY)};
 static const InteriorVariant kQVariantsFp64[] = {RFB_Q_VARIANTS_FP64(RFB_Q_ENTRY)};
 

@@ -32,6 +32,9 @@ def main() -> None:
     w.n_steps = max(args.steps, 1)
     setup = scenes.sphere_setup(w)
     sim = rb.Sim(scenes.run_config(w), setup.ptr if setup else None, None)
+    info = sim.info()
+    print(f"plan: mode {info.tma}, rows {info.tile_j}, ring {info.ring_depth}, segment {info.seg_len}, "
+          f"interior items {info.interior_items}, edge items {info.edge_items}", flush=True)
     sweep_ms, other_ms = sim.time_kernels(args.steps)
     sim.close()
     print(f"{w.name}: {args.steps} steps, sweep {sweep_ms / args.steps:.3f} ms/step, "

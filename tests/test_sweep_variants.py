@@ -25,14 +25,15 @@ from tests.cases import CASES, DT1, scene_run_config, workload_to_scene
 pytestmark = pytest.mark.gpu
 
 # (rows per tile, ring depth, mode) of every compiled variant; mode 0
-# cp.async interior, 1 TMA interior, 2 work-queue sweeps
+# cp.async interior, 1 TMA interior, 2 work-queue sweeps, 3 work-queue
+# sweeps with tile origins shifted to the slab edges
 VARIANTS = {
-    rb.FP64: [(8, 3, 2), (8, 4, 2), (8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
-    rb.FP32: [(8, 4, 2), (8, 3, 2), (16, 3, 2), (8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0),
-              (16, 4, 0), (16, 3, 0)],
+    rb.FP64: [(8, 3, 2), (8, 4, 2), (8, 3, 3), (8, 4, 3), (8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
+    rb.FP32: [(8, 4, 2), (8, 3, 2), (16, 3, 2), (8, 4, 3), (16, 3, 3), (8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0),
+              (8, 5, 0), (16, 4, 0), (16, 3, 0)],
 }
-QUEUE = [v for v in VARIANTS[rb.FP64] if v[2] == 2]
-MODE = {0: "cpasync", 1: "tma", 2: "queue"}
+QUEUE = [v for v in VARIANTS[rb.FP64] if v[2] >= 2]
+MODE = {0: "cpasync", 1: "tma", 2: "queue", 3: "queue_shifted"}
 
 
 def _vid(v):
