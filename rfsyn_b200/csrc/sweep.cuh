@@ -51,7 +51,7 @@ struct QLayout {
     using L = TmaLayout<T, TJ, NS>;
     static constexpr size_t bars = NS * L::stage;
     static constexpr size_t sh = bars + round128(8 * NS);
-    static constexpr size_t tabs = sh + round128(sizeof(T) * 3 * (TJ + 1) * 33);
+    static constexpr size_t tabs = sh + round128(sizeof(T) * 2 * 3 * (TJ + 1) * 33);
     static constexpr size_t misc = tabs + round128(sizeof(TileTables<T, TJ>));
     static constexpr size_t total = misc + 16;
 };
@@ -61,13 +61,16 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     k_sweep_q(Args<T> a, FusedDims d, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps,
               int *queue, int *err) {
     static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
+    static_assert(TJ >= 3, "warps 0-2 share the halo recomputation");
     constexpr bool EDGE = KIND == 2;  // per-cell y / z conditions and slabs
     constexpr bool XS = KIND >= 1;    // x-slab psi and plane conditions
     using L = TmaLayout<T, TJ, NS>;
     using S = QLayout<T, TJ, NS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
-    T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(smem_raw + S::sh);
+    // H of the current plane (tile + halo), double-buffered by plane parity
+    // so one block barrier per plane separates its writes from its reads
+    T(*sHb)[3][TJ + 1][33] = reinterpret_cast<T(*)[3][TJ + 1][33]>(smem_raw + S::sh);
     TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
     volatile int *s_item = reinterpret_cast<volatile int *>(smem_raw + S::misc);
     auto E = [&](int s, int c) { return reinterpret_cast<T(*)[TMA_EW]>(smem_raw + s * L::stage + c * L::ebox); };
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
         const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
 
         auto issue = [&](int s, int p) {
-            if (p < 0) return;
+            if (p < 0 || failed) return;  // a failed CTA issues no further copies
             if (tid == 0) {
                 mbar_expect_tx(&bars[s], tx_bytes);
 #pragma unroll
@@ -124,9 +127,14 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             }
             pending |= 1u << s;
         };
+        // a wait that timed out marks the CTA failed; later waits return at
+        // once and the item ends with garbage, reported at its end
         auto wait_slot = [&](int s) {
             if (!(pending & (1u << s))) return;
-            if (!mbar_wait(&bars[s], (phase >> s) & 1u)) failed = true;
+            if (failed || !mbar_wait(&bars[s], (phase >> s) & 1u)) {
+                failed = true;
+                return;  // still pending: drained (bounded) on the bail path
+            }
             phase ^= 1u << s;
             pending &= ~(1u << s);
         };
@@ -347,7 +355,9 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                 const int bym = i * nsmy * pitch, bzm = i * (int)ny1 * nsmz, bxm = sxm * plane32;
                 // halo cells recomputed this plane: row (j0-1, k) Hx, Hz;
                 // column (j0+tx, k0-1) Hx, Hy
-                const unsigned mrow = (ty == 0 && rowh) ? (mpl & mrow_jk) : 0u;
+                // row halo: Hx by warp 0, Hz by warp 2
+                const unsigned mrow = (ty == 0 && rowh) ? (mpl & mrow_jk & 1u)
+                                      : (ty == 2 && rowh) ? (mpl & mrow_jk & 4u) : 0u;
                 const unsigned mcol = (ty == 1 && colh) ? (mpl & mcol_jk) : 0u;
                 // psi inputs of the own cell and of the halo cells and the
                 // plane's x profile, all loaded before the wait; psi are read
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                     if (EDGE && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
                 }
                 wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
-                if (__syncthreads_or(failed)) goto bail;
+                T(*sH)[TJ + 1][33] = sHb[(i - ib) & 1];
                 const T e0 = E(sc, 0)[r][q], e1 = E(sc, 1)[r][q], e2 = E(sc, 2)[r][q];
                 const int code = with_codes ? (int)CODE(sc)[ty][tx] : 0;
                 const long long c = (long long)i * a.plane + own_c.ox;
@@ -396,11 +406,13 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                 sH[1][r][qs] = hy;
                 sH[2][r][qs] = hz;
                 if (ty == 0 && rowh) {
-                    // row halo (j0-1, k): Hx, Hz
+                    // row halo (j0-1, k): Hx
                     T v = H(sc, 0)[0][q];
                     if (mrow & 1u) v = hcell(0, pb, sc, sn, 0, q, row_c, 0, qs, hh[0], hh[1], false);
                     sH[0][0][qs] = v;
-                    v = H(sc, 2)[0][q];
+                } else if (ty == 2 && rowh) {
+                    // row halo (j0-1, k): Hz
+                    T v = H(sc, 2)[0][q];
                     if (mrow & 4u) v = hcell(2, pb, sc, sn, 0, q, row_c, 0, qs, hh[2], hh[3], false);
                     sH[2][0][qs] = v;
                 } else if (ty == 1 && colh) {
@@ -468,6 +480,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
                 sc = sn;
             }
         }
+        if (__syncthreads_or(failed)) goto bail;
         __syncthreads();  // the ring, the tables and the item slot are free again
         continue;
     bail:
@@ -495,7 +508,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
 // Variants (element type, TJ, NS, CTAs per SM of the interior and of the
 // edge instantiation): interior and edge share the tile height and ring
 // depth of a plan.
-#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 4) X(float, 8, 3, 5, 4) X(float, 16, 3, 2, 2)
+#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 4) X(float, 8, 3, 5, 3) X(float, 16, 3, 2, 2)
 #define RFB_Q_VARIANTS_FP64(X) X(double, 8, 3, 3, 2) X(double, 8, 4, 2, 2)
 
 template <typename T, int TJ, int NS, int MINB, int KIND>
