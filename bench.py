@@ -29,7 +29,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 PEAKS = ROOT / "MEASURED_PEAKS.json"
-TRAFFIC = ROOT / "profiles" / "fused_sweep_c2.md"
+TRAFFIC = ROOT / "profiles" / "sweep_queue_c2.md"
 METRIC = "Mcell-updates/s"
 
 
@@ -318,7 +318,7 @@ def run_b200(args) -> None:
                    "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
                    "l2": "inputs larger than L2 (fields 6 x 2 x 76 MB per scene)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "kernel": "k_fused (H+E sweep)",
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": "k_sweep_q (one H+E sweep: interior + x-slab + edge launches)",
                      "algorithmic_bytes_per_launch": alg, "launch_ms": sweep_launch_ms,
                      "other_kernels_ms_per_step": other_ms / 200},
         "cpu_baseline": cpu,
