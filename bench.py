@@ -25,6 +25,8 @@ import threading
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -331,6 +333,136 @@ def run_b200(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Batched scenes (--workload c4)
+# ---------------------------------------------------------------------------
+def run_batch(args) -> None:
+    """512 independent uneven scenes (rfsyn_b200.scenes.c4) advanced together
+    by one batch: a step = one full run of every scene (reset + 1500 time
+    steps).  Metric Mcell-updates/s over the whole batch; scenes/s beside it,
+    with the plain one-scene-at-a-time GPU session timed on a sample of the
+    same scenes as the baseline the batch is measured against."""
+    import torch
+
+    import rfsyn_b200 as rb
+    from rfsyn_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    ws = scenes.c4(seed=4 + 1000 * rank, n_scenes=args.scenes)
+    n_steps = ws[0].n_steps
+    cells = sum(w.cells for w in ws)
+    setups = [scenes.scene_setup(w) for w in ws]
+    rcs = [scenes.run_config(w) for w in ws]
+    t0 = time.perf_counter()
+    b = rb.Batch(rcs, [s.ptr if s else None for s in setups])
+    create_s = time.perf_counter() - t0
+    info = b.info()
+    stream = torch.cuda.ExternalStream(b.stream)
+
+    def one_step():
+        b.reset()
+        b.advance(n_steps)
+
+    for _ in range(args.warmup):
+        one_step()
+    b.synchronize()
+    lib = rb.load()
+    launches0 = lib.fdtd_b200_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            one_step()
+        end.record(stream)
+        end.synchronize()
+    b.synchronize()
+    launches = lib.fdtd_b200_launch_count() - launches0
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    value = world * cells * n_steps * args.steps / (ms / 1e3) / 1e6
+    scenes_s = world * len(ws) * args.steps / (ms / 1e3)
+    finite = all(bool(np.all(np.isfinite(b.dft(q)))) for q in range(0, len(ws), max(1, len(ws) // 16)))
+    # sweep kernels alone (CUDA events around the sweep launches of each step)
+    b.reset()
+    sw, ot = b.time_kernels(50)
+    b.close()
+
+    # plain one-scene-at-a-time GPU sessions on a sample of the same scenes
+    sample = ws[: args.plain_sample]
+    plain_ms = 0.0
+    for w, st in zip(sample, setups):
+        sim = rb.Sim(scenes.run_config(w), st.ptr if st else None, None)
+        sim.advance(n_steps)          # warm (graph build)
+        sim.reset()
+        plain_ms += sim.advance_timed(n_steps)
+        sim.close()
+    plain_scenes_s = len(sample) / (plain_ms / 1e3)
+
+    # end to end: scene set-up and upload, the full run, every probe series
+    # and spectrum back on the host
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b2 = rb.Batch(rcs, [s.ptr if s else None for s in setups])
+    b2.advance(n_steps)
+    d2h = 0
+    for q in range(len(ws)):
+        d2h += b2.probes(q).nbytes + b2.dft(q).nbytes
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    b2.close()
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    esz = 4
+    alg = cells * (12 * esz + 1) + info.slab_cell_axes * 8 * esz
+    peak, peak_kind = hbm_peak()
+    sweep_launch_ms = sw / 50
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32 scenes: 0-6 spheres / boxes each)",
+        "config": {"workload": f"c4_batch{len(ws)}_32to96_fp32", "scenes": len(ws), "cells": cells,
+                   "n_steps": n_steps, "npml": 8, "probes_per_scene": 4, "dft_bins": 128,
+                   "plan": {"tile_j": info.tile_j, "ring_depth": info.ring_depth, "mode": info.mode,
+                            "seg_interior": info.seg_interior, "seg_edge": info.seg_edge},
+                   "items": [info.items_interior, info.items_xslab, info.items_edge],
+                   "parallelism": f"scene-batch x{world}", "l2": "inputs larger than L2 (fields 12 x 4 B x 130 M cells)"},
+        "scenes_per_s": scenes_s,
+        "plain_one_at_a_time": {"scenes_per_s": plain_scenes_s, "sample": len(sample),
+                                "speedup_batched": scenes_s / plain_scenes_s / world},
+        "roofline": {"bound": "hbm", "achieved": alg / (sweep_launch_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (sweep_launch_ms / 1e3) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                     "kernel": "k_sweep_qb (one batched H+E sweep: interior + x-slab + edge launches)",
+                     "algorithmic_bytes_per_launch": alg, "launch_ms": sweep_launch_ms,
+                     "other_kernels_ms_per_step": ot / 50},
+        "e2e": {"value": world * cells * n_steps / (e2e_ms / 1e3) / 1e6, "unit": METRIC, "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "includes": "scene set-up and upload"},
+        "create_s": create_s,
+        "gpu_launches": int(launches), "launches_per_time_step": info.launches_per_step,
+        "clocks": clocks, "finite": finite,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -340,11 +472,16 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4"])
+    ap.add_argument("--scenes", type=int, default=512, help="c4: scenes per batch")
+    ap.add_argument("--plain-sample", type=int, default=16, help="c4: scenes timed one at a time")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c4":
+        run_batch(args)
     else:
         run_b200(args)
 

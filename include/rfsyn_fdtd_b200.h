@@ -155,6 +155,50 @@ typedef struct {
 
 int fdtd_b200_sim_energy(fdtd_b200_sim_t *sim, int x_lo, int x_hi, fdtd_b200_energy_t *out);
 
+/* ---- batches of independent scenes ------------------------------------------
+ * No counterpart in rfsyn, whose job loop simulates its examples one after
+ * the other (cli/main.c:362-417).  A batch uploads many scenes -- each with
+ * its own size, CPML, materials (setup callback), sources and probes, as for
+ * fdtd_b200_sim_create -- and advances all of them together: every step is
+ * five kernel launches for the whole batch (three work-queue sweeps over the
+ * tiles of every scene, the interface lists, the probes), replayed from CUDA
+ * graphs.  Every scene yields exactly the probe series and spectra of its own
+ * session (the same kernels, the same arithmetic).  All scenes share the
+ * precision and step count; the FUSED schedule is used whatever the
+ * configuration says; a scene periodic in y or z whose tile halos would wrap
+ * is rejected.  Creation times candidate tile plans on the batch
+ * (RFSYN_FDTD_PLAN "rows,ring,seg_interior,seg_edge,mode" with mode 2 or 3
+ * fixes one).  setups / contexts may be NULL, or hold NULL entries. */
+typedef struct fdtd_b200_batch fdtd_b200_batch_t;
+
+fdtd_b200_batch_t *fdtd_b200_batch_create(size_t n_scenes, const fdtd_b200_config_t *configs,
+                                          const fdtd_material_setup_fn *setups, void *const *contexts,
+                                          void *cuda_stream);
+void fdtd_b200_batch_destroy(fdtd_b200_batch_t *batch);
+size_t fdtd_b200_batch_size(const fdtd_b200_batch_t *batch);
+int fdtd_b200_batch_reset(fdtd_b200_batch_t *batch);
+int fdtd_b200_batch_advance(fdtd_b200_batch_t *batch, size_t n_steps);
+int fdtd_b200_batch_advance_timed(fdtd_b200_batch_t *batch, size_t n_steps, double *ms);
+int fdtd_b200_batch_synchronize(fdtd_b200_batch_t *batch);
+size_t fdtd_b200_batch_steps_done(const fdtd_b200_batch_t *batch);
+void *fdtd_b200_batch_stream(const fdtd_b200_batch_t *batch);
+/* As fdtd_b200_sim_time_kernels, for the whole batch. */
+int fdtd_b200_batch_time_kernels(fdtd_b200_batch_t *batch, size_t n_steps, double *sweep_ms, double *other_ms);
+/* Probe series / spectra of one scene (blocking), as the session calls. */
+int fdtd_b200_batch_read_probes(fdtd_b200_batch_t *batch, size_t scene, double *probe_td);
+int fdtd_b200_batch_dft(fdtd_b200_batch_t *batch, size_t scene, double *dft_re, double *dft_im);
+
+typedef struct {
+    size_t scenes, cells, list_cells, slab_cell_axes;
+    int tile_j, ring_depth;
+    int mode;                    /* 2: tiles from the origin; 3: origins shifted to the slab edges */
+    int seg_interior, seg_edge;  /* planes per work item */
+    int items_interior, items_xslab, items_edge;
+    int launches_per_step;
+} fdtd_b200_batch_info_t;
+
+int fdtd_b200_batch_info(const fdtd_b200_batch_t *batch, fdtd_b200_batch_info_t *info);
+
 /* ---- dispersive media (auxiliary differential equations) ----------------------
  * rfsyn models only static eps_r and sigma (engine/fdtd/materials.c:92-125);
  * these entry points add per-component dispersive samples integrated with

@@ -105,6 +105,13 @@ class Energy(C.Structure):
                [("nonfinite", C.c_size_t)]
 
 
+class BatchInfo(C.Structure):
+    _fields_ = [("scenes", C.c_size_t), ("cells", C.c_size_t), ("list_cells", C.c_size_t),
+                ("slab_cell_axes", C.c_size_t), ("tile_j", C.c_int), ("ring_depth", C.c_int), ("mode", C.c_int),
+                ("seg_interior", C.c_int), ("seg_edge", C.c_int), ("items_interior", C.c_int),
+                ("items_xslab", C.c_int), ("items_edge", C.c_int), ("launches_per_step", C.c_int)]
+
+
 SETUP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
@@ -138,6 +145,29 @@ class SphereSetup:
 
         def cb(grid, mat, ctx):
             return lib.fdtd_b200_materials_add_spheres(mat, grid, self._arr, n, smoothing)
+
+        self.fn = SETUP_FN(cb)
+        self.ptr = C.cast(self.fn, C.c_void_p)
+
+
+class SceneSetup:
+    """An fdtd_material_setup_fn that applies boxes (rfsyn's
+    materials_set_box, in list order) and then spheres
+    (fdtd_b200_materials_add_spheres); keeps the ctypes objects alive.
+    boxes: (i0, i1, j0, j1, k0, k1, eps_r, sigma) half-open cell ranges."""
+
+    def __init__(self, boxes=(), spheres=(), smoothing: int = 1):
+        lib = load()
+        self._spheres = SphereSetup(spheres, smoothing) if spheres else None
+        boxes = list(boxes)
+
+        def cb(grid, mat, ctx):
+            for (i0, i1, j0, j1, k0, k1, eps, sig) in boxes:
+                if lib.materials_set_box(mat, grid, i0, i1, j0, j1, k0, k1, eps, sig) != 0:
+                    return -1
+            if self._spheres is not None:
+                return self._spheres.fn(grid, mat, ctx)
+            return 0
 
         self.fn = SETUP_FN(cb)
         self.ptr = C.cast(self.fn, C.c_void_p)
@@ -177,9 +207,23 @@ def load() -> C.CDLL:
         "fdtd_b200_version": (C.c_char_p, []),
         "cpml_default_params": (CpmlParams, [S]),
         "fdtd_b200_materials_add_spheres": (I, [P, P, C.POINTER(Sphere), S, I]),
+        "materials_set_box": (I, [P, P, S, S, S, S, S, S, D, D]),
         "fdtd_b200_sim_info": (I, [P, C.POINTER(SimInfo)]),
         "fdtd_b200_sim_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_sim_energy": (I, [P, I, I, C.POINTER(Energy)]),
+        "fdtd_b200_batch_create": (P, [S, C.POINTER(B200Config), C.POINTER(P), C.POINTER(P), P]),
+        "fdtd_b200_batch_destroy": (V, [P]),
+        "fdtd_b200_batch_size": (S, [P]),
+        "fdtd_b200_batch_reset": (I, [P]),
+        "fdtd_b200_batch_advance": (I, [P, S]),
+        "fdtd_b200_batch_advance_timed": (I, [P, S, C.POINTER(D)]),
+        "fdtd_b200_batch_synchronize": (I, [P]),
+        "fdtd_b200_batch_steps_done": (S, [P]),
+        "fdtd_b200_batch_stream": (P, [P]),
+        "fdtd_b200_batch_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
+        "fdtd_b200_batch_read_probes": (I, [P, S, C.POINTER(D)]),
+        "fdtd_b200_batch_dft": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
+        "fdtd_b200_batch_info": (I, [P, C.POINTER(BatchInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -365,3 +409,80 @@ class Sim:
 
 def dt_of(dx: float, courant: float = 0.99) -> float:
     return courant * (dx / (C0 * np.sqrt(3.0)))
+
+
+class Batch:
+    """Many independent scenes advanced together (fdtd_b200_batch_*).
+
+    configs: RunConfig per scene (same precision and step count); setups /
+    contexts: one setup pointer (or None) and context (or None) per scene."""
+
+    def __init__(self, configs, setups=None, contexts=None, stream: int | None = None):
+        self.lib = load()
+        self.configs = list(configs)
+        n = len(self.configs)
+        self._cfgs = (B200Config * n)(*[rc.c for rc in self.configs])
+        self._setups = (C.c_void_p * n)(*[(s if s is not None else None) for s in (setups or [None] * n)])
+        self._ctx = (C.c_void_p * n)(*[(x if x is not None else None) for x in (contexts or [None] * n)])
+        self.h = self.lib.fdtd_b200_batch_create(n, self._cfgs, self._setups, self._ctx, stream)
+        if not self.h:
+            raise RuntimeError(f"fdtd_b200_batch_create failed: {last_error()}")
+
+    def __len__(self):
+        return len(self.configs)
+
+    def _ok(self, rc):
+        if rc != 0:
+            raise RuntimeError(last_error())
+
+    def reset(self):
+        self._ok(self.lib.fdtd_b200_batch_reset(self.h))
+
+    def advance(self, n: int):
+        self._ok(self.lib.fdtd_b200_batch_advance(self.h, n))
+
+    def advance_timed(self, n: int) -> float:
+        ms = C.c_double(0.0)
+        self._ok(self.lib.fdtd_b200_batch_advance_timed(self.h, n, C.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        self._ok(self.lib.fdtd_b200_batch_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.fdtd_b200_batch_stream(self.h) or 0
+
+    def info(self) -> BatchInfo:
+        bi = BatchInfo()
+        self._ok(self.lib.fdtd_b200_batch_info(self.h, C.byref(bi)))
+        return bi
+
+    def time_kernels(self, n: int) -> tuple[float, float]:
+        a, b = C.c_double(0), C.c_double(0)
+        self._ok(self.lib.fdtd_b200_batch_time_kernels(self.h, n, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def probes(self, scene: int) -> np.ndarray:
+        c = self.configs[scene].c
+        out = np.zeros((max(c.n_probes, 1), c.n_steps))
+        self._ok(self.lib.fdtd_b200_batch_read_probes(self.h, scene, _dptr(out)))
+        return out[: c.n_probes]
+
+    def dft(self, scene: int) -> np.ndarray:
+        c = self.configs[scene].c
+        re = np.zeros((max(c.n_probes, 1), max(c.n_freqs, 1)))
+        im = np.zeros_like(re)
+        self._ok(self.lib.fdtd_b200_batch_dft(self.h, scene, _dptr(re), _dptr(im)))
+        return (re + 1j * im)[: c.n_probes, : c.n_freqs]
+
+    def close(self):
+        if self.h:
+            self.lib.fdtd_b200_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

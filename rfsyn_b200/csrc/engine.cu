@@ -46,6 +46,12 @@ extern "C" unsigned long long rfb_launch_count(void) { return g_launches.load();
 
 #define MU0_ 1.25663706212e-6
 
+// Device error codes the sweeps record in their error word.
+static const char *sweep_error_text(int err) {
+    return err == 2 ? "a sweep CTA's shared memory did not start on a 128-byte boundary (no copy issued)"
+                    : "a sweep's tensor copies did not complete in time";
+}
+
 static long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
 // Row pitch (elements) of the device layout: a multiple of 32 elements, so
@@ -398,6 +404,8 @@ struct rfb_engine {
     int *d_err = nullptr;   // set by a sweep whose copies did not complete in time
     double *d_energy = nullptr;  // energy audit: block partials + result
     size_t h2d_bytes = 0, n_ade = 0;
+    int active = 0;          // a source sits on a padded boundary plane
+    int member = 0;          // scene of a batch: no plan, graphs or second stream of its own
 };
 
 template <typename T>
@@ -602,23 +610,22 @@ static bool q_fits(const rfb_engine *e) {
     return x < lim && xm < lim && y < lim && z < lim;
 }
 
-static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge) {
+// Work items of a sweep plan (host lists): vi interior, vx x-slab planes of
+// interior tiles (modes 2, 3), vq slab / boundary tiles of the work-queue
+// edge sweep (modes 2, 3), ve tiles of the cp.async-fed edge sweep.
+struct PlanLists {
+    std::vector<SweepItem> vi, vx, vq, ve;
+    FusedDims d;
+};
+
+static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg_int, int seg_edge, PlanLists &out) {
     const rfb_geom_t &g = e->g;
-    if (tma >= 2 && !q_fits(e)) {
-        rfb_set_error("grid too large for the work-queue sweep (32-bit offsets)");
-        return -1;
-    }
     const bool px = g.periodic & 1u, py = g.periodic & 2u, pz = g.periodic & 4u;
-    FusedPlan &p = e->plan;
-    free_plan_lists(p);
-    p.tj = tj;
-    p.ns = ns;
-    p.tma = tma;
-    p.seg_int = seg_int;
-    p.seg_edge = seg_edge;
+    PlanLists &p = out;
     p.d.cj = g.ny + ((active && !py) ? 1 : 0);
     p.d.ck = g.nz + ((active && !pz) ? 1 : 0);
     p.d.ci = g.nx + ((active && !px) ? 1 : 0);
+    std::vector<SweepItem> &vi = p.vi, &ve = p.ve, &vq = p.vq, &vx = p.vx;
     const bool on = e->cpml.on != 0;
     int xlo, xhi, ylo, yhi, zlo, zhi;
     auto ext = [&](int ax, int *lo, int *hi, int n, bool per) {
@@ -629,7 +636,6 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     ext(1, &ylo, &yhi, g.ny, py);
     ext(2, &zlo, &zhi, g.nz, pz);
     const int xa = px ? 0 : xlo + 1, xb = std::max(xa, xhi);
-    std::vector<SweepItem> vi, ve, vq, vx;
     auto add = [](std::vector<SweepItem> &v, int j0, int k0, int b, int en, int seg) {
         for (int s = b; s < en; s += seg) v.push_back(SweepItem{j0, k0, s, std::min(en, s + seg)});
     };
@@ -691,6 +697,24 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     std::stable_sort(vq.begin(), vq.end(), [](const SweepItem &x, const SweepItem &y) {
         return x.ie - x.ib > y.ie - y.ib;
     });
+}
+
+static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge) {
+    if (tma >= 2 && !q_fits(e)) {
+        rfb_set_error("grid too large for the work-queue sweep (32-bit offsets)");
+        return -1;
+    }
+    FusedPlan &p = e->plan;
+    free_plan_lists(p);
+    p.tj = tj;
+    p.ns = ns;
+    p.tma = tma;
+    p.seg_int = seg_int;
+    p.seg_edge = seg_edge;
+    PlanLists pl;
+    plan_items(e, active, tj, tma, seg_int, seg_edge, pl);
+    p.d = pl.d;
+    const std::vector<SweepItem> &vi = pl.vi, &ve = pl.ve, &vq = pl.vq, &vx = pl.vx;
     p.n_int = (int)vi.size();
     p.n_edge = (int)ve.size();
     p.n_qe = (int)vq.size();
@@ -836,7 +860,7 @@ static int autotune(rfb_engine *e, int active) {
         int err = 0;
         CK(cudaMemcpy(&err, e->d_err, sizeof err, cudaMemcpyDeviceToHost));
         if (err) {
-            rfb_set_error("a sweep's tensor copies did not complete in time");
+            rfb_set_error("%s", sweep_error_text(err));
             return -1;
         }
     }
@@ -872,11 +896,12 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     delete e;
 }
 
-extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision, int schedule,
-                                           const rfb_cpml_desc_t *cpml, const rfb_scene_image_t *scene,
-                                           size_t n_sources, const rfb_source_desc_t *sources, size_t n_probes,
-                                           const rfb_probe_desc_t *probes, size_t n_steps, void *stream) {
+static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int schedule, const rfb_cpml_desc_t *cpml,
+                                   const rfb_scene_image_t *scene, size_t n_sources, const rfb_source_desc_t *sources,
+                                   size_t n_probes, const rfb_probe_desc_t *probes, size_t n_steps, void *stream,
+                                   int member) {
     rfb_engine *e = new rfb_engine();
+    e->member = member;
     e->g = *geom;
     e->prec = precision;
     e->sched = schedule;
@@ -940,6 +965,15 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
                 (sources[s].k == geom->nz && !(geom->periodic & 4u)))
                 active = 1;
         }
+        e->active = active;
+        if (member) {
+            // a batch scene: the batch builds the plans and owns the streams
+            if (tma_prepare() != 0 || q_prepare() != 0) {
+                rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
+                goto fail_noset;
+            }
+            goto created;
+        }
         CK(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
@@ -967,6 +1001,7 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
             rc = autotune(e, active);
         if (rc != 0) goto fail_noset;
     }
+created:
     CK(cudaDeviceSynchronize());
     e->launches_per_step = count_step_launches(e);
     if (scene) {
@@ -985,6 +1020,27 @@ fail:
 fail_noset:
     rfb_engine_destroy(e);
     return nullptr;
+}
+
+extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision, int schedule,
+                                           const rfb_cpml_desc_t *cpml, const rfb_scene_image_t *scene,
+                                           size_t n_sources, const rfb_source_desc_t *sources, size_t n_probes,
+                                           const rfb_probe_desc_t *probes, size_t n_steps, void *stream) {
+    return engine_create(geom, precision, schedule, cpml, scene, n_sources, sources, n_probes, probes, n_steps, stream,
+                         0);
+}
+
+extern "C" rfb_engine_t *rfb_engine_create_member(const rfb_geom_t *geom, int precision,
+                                                  const rfb_cpml_desc_t *cpml, const rfb_scene_image_t *scene,
+                                                  size_t n_sources, const rfb_source_desc_t *sources,
+                                                  size_t n_probes, const rfb_probe_desc_t *probes, size_t n_steps,
+                                                  void *stream) {
+    if (!stream) {
+        rfb_set_error("a batch scene needs the batch's stream");
+        return nullptr;
+    }
+    return engine_create(geom, precision, RFB_SCHED_FUSED, cpml, scene, n_sources, sources, n_probes, probes,
+                         n_steps, stream, 1);
 }
 
 extern "C" int rfb_engine_reset(rfb_engine_t *e) {
@@ -1202,7 +1258,7 @@ static int check_sweep_error(rfb_engine *e) {
     int err = 0;
     CK(cudaMemcpy(&err, e->d_err, sizeof err, cudaMemcpyDeviceToHost));
     if (err) {
-        rfb_set_error("a sweep's tensor copies did not complete in time");
+        rfb_set_error("%s", sweep_error_text(err));
         return -1;
     }
     return 0;
@@ -1521,3 +1577,5 @@ out:
     (void)vac;
     return rc;
 }
+
+#include "batch.cuh"

@@ -110,6 +110,38 @@ rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision, int sched
                                 size_t n_probes, const rfb_probe_desc_t *probes,
                                 size_t n_steps, void *stream);
 void rfb_engine_destroy(rfb_engine_t *e);
+/* An engine for one scene of a batch (FUSED schedule): device state only;
+ * the batch builds the sweep plans and owns the kernels' launches.  `stream`
+ * must be the batch's stream. */
+rfb_engine_t *rfb_engine_create_member(const rfb_geom_t *geom, int precision, const rfb_cpml_desc_t *cpml,
+                                       const rfb_scene_image_t *scene, size_t n_sources,
+                                       const rfb_source_desc_t *sources, size_t n_probes,
+                                       const rfb_probe_desc_t *probes, size_t n_steps, void *stream);
+
+/* ---- batches of scenes advanced together (batch.cuh) ----------------------- */
+typedef struct rfb_batch rfb_batch_t;
+typedef struct {
+    size_t scenes, cells, list_cells, slab_cell_axes;
+    int tile_j, ring_depth, mode, seg_interior, seg_edge;
+    int items_interior, items_xslab, items_edge;
+    int launches_per_step;
+} rfb_batch_info_t;
+/* Takes ownership of the members (and of `stream` when own_stream). */
+rfb_batch_t *rfb_batch_create(rfb_engine_t **members, size_t n, void *stream, int own_stream);
+void rfb_batch_destroy(rfb_batch_t *b);
+int rfb_batch_reset(rfb_batch_t *b);
+int rfb_batch_advance(rfb_batch_t *b, size_t n);
+int rfb_batch_advance_timed(rfb_batch_t *b, size_t n, double *ms);
+int rfb_batch_sync(rfb_batch_t *b);
+int rfb_batch_time_kernels(rfb_batch_t *b, size_t n, double *sweep_ms, double *other_ms);
+rfb_engine_t *rfb_batch_member(rfb_batch_t *b, size_t s);
+size_t rfb_batch_size(rfb_batch_t *b);
+size_t rfb_batch_steps_done(rfb_batch_t *b);
+void *rfb_batch_stream(rfb_batch_t *b);
+int rfb_batch_info(rfb_batch_t *b, rfb_batch_info_t *out);
+/* A non-blocking stream (for a batch's members), or NULL. */
+void *rfb_stream_create(void);
+void rfb_stream_destroy(void *stream);
 
 /* Zero fields, psi and ADE state and rewind the step counter (async). */
 int rfb_engine_reset(rfb_engine_t *e);

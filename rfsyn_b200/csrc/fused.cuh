@@ -214,10 +214,10 @@ __device__ __forceinline__ T h_interior(int c, T cbh, const FusedStage<T, TJ> &c
 // ---------------------------------------------------------------------------
 template <typename T, int TJ, int NS, int MINB>
 __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_interior(Args<T> a, FusedDims d, const SweepItem *items) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FusedStage<T, TJ> *stage = reinterpret_cast<FusedStage<T, TJ> *>(smem_raw);
-    T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(smem_raw + NS * sizeof(FusedStage<T, TJ>));
-    T *s_tab = reinterpret_cast<T *>(smem_raw + NS * sizeof(FusedStage<T, TJ>) + sizeof(T) * 3 * (TJ + 1) * 33);
+    extern __shared__ __align__(16) unsigned char smem_cp[];
+    FusedStage<T, TJ> *stage = reinterpret_cast<FusedStage<T, TJ> *>(smem_cp);
+    T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(smem_cp + NS * sizeof(FusedStage<T, TJ>));
+    T *s_tab = reinterpret_cast<T *>(smem_cp + NS * sizeof(FusedStage<T, TJ>) + sizeof(T) * 3 * (TJ + 1) * 33);
 
     const SweepItem it = items[blockIdx.x];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
@@ -333,9 +333,9 @@ __device__ __forceinline__ T stretch(T d, T kinv, T b, T ac, T dx, T psi_old, T 
 
 template <typename T, int TJ, int NS, int MINB>
 __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDims d, const SweepItem *items) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    EdgeStage<T, TJ> *stage = reinterpret_cast<EdgeStage<T, TJ> *>(smem_raw);
-    unsigned char *after = smem_raw + NS * sizeof(EdgeStage<T, TJ>);
+    extern __shared__ __align__(16) unsigned char smem_cp[];
+    EdgeStage<T, TJ> *stage = reinterpret_cast<EdgeStage<T, TJ> *>(smem_cp);
+    unsigned char *after = smem_cp + NS * sizeof(EdgeStage<T, TJ>);
     T(*sH)[TJ + 1][33] = reinterpret_cast<T(*)[TJ + 1][33]>(after);
     T *s_tab = reinterpret_cast<T *>(after + sizeof(T) * 3 * (TJ + 1) * 33);
     EdgeShared<T, TJ> &es =

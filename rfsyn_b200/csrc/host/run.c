@@ -66,6 +66,7 @@ void fdtd_b200_config_init(fdtd_b200_config_t *cfg, size_t nx, size_t ny, size_t
 
 struct fdtd_b200_sim {
     rfb_engine_t *eng;
+    int borrowed;          /* a batch scene: the batch owns the engine */
     size_t n_steps, n_probes, n_freqs;
     double dt, dx;
     double *freqs;
@@ -95,8 +96,10 @@ static double wave_value(const fdtd_b200_source_t *s, double t, size_t n) {
 
 static size_t canon(size_t q, size_t n, int periodic) { return periodic ? q % n : q; }
 
-fdtd_b200_sim_t *fdtd_b200_sim_create(const fdtd_b200_config_t *cfg, fdtd_material_setup_fn setup, void *context,
-                                      void *cuda_stream) {
+/* member: create the engine as a scene of a batch (FUSED, on the batch's
+ * stream, no plan of its own). */
+static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_setup_fn setup, void *context,
+                                   void *cuda_stream, int member) {
     fdtd_grid_t g;
     cpml_t *pml = NULL;
     materials_t *mat = NULL;
@@ -201,8 +204,15 @@ fdtd_b200_sim_t *fdtd_b200_sim_create(const fdtd_b200_config_t *cfg, fdtd_materi
     rfb_geom_from_grid(&g, &geom);
     rfb_cpml_desc_t cd;
     if (pml) rfb_cpml_desc_from(pml, &cd);
-    sim->eng = rfb_engine_create(&geom, cfg->precision, cfg->schedule, pml ? &cd : NULL, &scene.img, ns, sd, np, pd, nt,
-                                 cuda_stream);
+    if (member) {
+        sim->schedule = FDTD_B200_SCHED_FUSED;
+        sim->borrowed = 1;
+        sim->eng = rfb_engine_create_member(&geom, cfg->precision, pml ? &cd : NULL, &scene.img, ns, sd, np, pd, nt,
+                                            cuda_stream);
+    } else {
+        sim->eng = rfb_engine_create(&geom, cfg->precision, cfg->schedule, pml ? &cd : NULL, &scene.img, ns, sd, np,
+                                     pd, nt, cuda_stream);
+    }
     if (!sim->eng) goto fail;
     rfb_scene_build_free(&scene);
     free(vals); free(sd); free(extra); free(pd);
@@ -221,9 +231,14 @@ fail:
     return NULL;
 }
 
+fdtd_b200_sim_t *fdtd_b200_sim_create(const fdtd_b200_config_t *cfg, fdtd_material_setup_fn setup, void *context,
+                                      void *cuda_stream) {
+    return sim_create(cfg, setup, context, cuda_stream, 0);
+}
+
 void fdtd_b200_sim_destroy(fdtd_b200_sim_t *sim) {
     if (!sim) return;
-    rfb_engine_destroy(sim->eng);
+    if (!sim->borrowed) rfb_engine_destroy(sim->eng);
     free(sim->freqs);
     free(sim);
 }
@@ -440,4 +455,136 @@ signal_t *signal_copy(const signal_t *sig) {
     memcpy(c->samples, sig->samples, sig->n_samples * sizeof(rfsyn_float_complex));
     c->metadata = sig->metadata;
     return c;
+}
+
+/* ---- batches of independent scenes ------------------------------------------ */
+struct fdtd_b200_batch {
+    rfb_batch_t *b;
+    size_t n;
+    fdtd_b200_sim_t **sims;   /* per scene: its configuration; engines owned by b */
+};
+
+fdtd_b200_batch_t *fdtd_b200_batch_create(size_t n_scenes, const fdtd_b200_config_t *configs,
+                                          const fdtd_material_setup_fn *setups, void *const *contexts,
+                                          void *cuda_stream) {
+    fdtd_b200_batch_t *bt = NULL;
+    rfb_engine_t **engs = NULL;
+    void *stream = cuda_stream;
+    int own = 0;
+    size_t made = 0;
+    if (!configs || n_scenes == 0) {
+        rfb_set_error("a batch needs at least one scene configuration");
+        return NULL;
+    }
+    for (size_t s = 0; s < n_scenes; s++) {
+        if (configs[s].precision != configs[0].precision || configs[s].n_steps != configs[0].n_steps) {
+            rfb_set_error("batch scene %zu: every scene must share precision and step count", s);
+            return NULL;
+        }
+    }
+    if (!stream) {
+        stream = rfb_stream_create();
+        if (!stream) return NULL;
+        own = 1;
+    }
+    bt = calloc(1, sizeof(*bt));
+    engs = calloc(n_scenes, sizeof(*engs));
+    if (bt) bt->sims = calloc(n_scenes, sizeof(*bt->sims));
+    if (!bt || !engs || !bt->sims) {
+        rfb_set_error("out of host memory");
+        goto fail;
+    }
+    bt->n = n_scenes;
+    for (size_t s = 0; s < n_scenes; s++) {
+        fdtd_material_setup_fn fn = setups ? setups[s] : NULL;
+        void *ctx = contexts ? contexts[s] : NULL;
+        bt->sims[s] = sim_create(&configs[s], fn, ctx, stream, 1);
+        if (!bt->sims[s]) {
+            char msg[400];
+            snprintf(msg, sizeof msg, "batch scene %zu: %s", s, rfb_last_error());
+            rfb_set_error("%s", msg);
+            goto fail;
+        }
+        engs[s] = bt->sims[s]->eng;
+        made = s + 1;
+    }
+    bt->b = rfb_batch_create(engs, n_scenes, stream, own);
+    own = 0;      /* the batch owns the stream now, on failure too */
+    made = 0;     /* ... and the engines */
+    if (!bt->b) goto fail;
+    free(engs);
+    return bt;
+fail:
+    if (bt) {
+        for (size_t s = 0; s < made; s++) rfb_engine_destroy(engs[s]);
+        if (bt->sims)
+            for (size_t s = 0; s < n_scenes; s++) fdtd_b200_sim_destroy(bt->sims[s]);
+        free(bt->sims);
+        free(bt);
+    }
+    free(engs);
+    if (own) rfb_stream_destroy(stream);
+    return NULL;
+}
+
+void fdtd_b200_batch_destroy(fdtd_b200_batch_t *bt) {
+    if (!bt) return;
+    rfb_batch_destroy(bt->b);
+    for (size_t s = 0; s < bt->n; s++) fdtd_b200_sim_destroy(bt->sims[s]);
+    free(bt->sims);
+    free(bt);
+}
+
+size_t fdtd_b200_batch_size(const fdtd_b200_batch_t *bt) { return bt ? bt->n : 0; }
+int fdtd_b200_batch_reset(fdtd_b200_batch_t *bt) { return bt ? rfb_batch_reset(bt->b) : -1; }
+int fdtd_b200_batch_advance(fdtd_b200_batch_t *bt, size_t n) { return bt ? rfb_batch_advance(bt->b, n) : -1; }
+int fdtd_b200_batch_advance_timed(fdtd_b200_batch_t *bt, size_t n, double *ms) {
+    return bt ? rfb_batch_advance_timed(bt->b, n, ms) : -1;
+}
+int fdtd_b200_batch_synchronize(fdtd_b200_batch_t *bt) { return bt ? rfb_batch_sync(bt->b) : -1; }
+size_t fdtd_b200_batch_steps_done(const fdtd_b200_batch_t *bt) { return bt ? rfb_batch_steps_done(bt->b) : 0; }
+void *fdtd_b200_batch_stream(const fdtd_b200_batch_t *bt) { return bt ? rfb_batch_stream(bt->b) : NULL; }
+
+int fdtd_b200_batch_time_kernels(fdtd_b200_batch_t *bt, size_t n, double *sweep_ms, double *other_ms) {
+    if (!bt || !sweep_ms || !other_ms) return -1;
+    return rfb_batch_time_kernels(bt->b, n, sweep_ms, other_ms);
+}
+
+int fdtd_b200_batch_read_probes(fdtd_b200_batch_t *bt, size_t scene, double *probe_td) {
+    if (!bt || scene >= bt->n || !probe_td) {
+        rfb_set_error("batch: bad scene index or output");
+        return -1;
+    }
+    if (rfb_batch_sync(bt->b) != 0) return -1;
+    return rfb_engine_read_probes(bt->sims[scene]->eng, probe_td);
+}
+
+int fdtd_b200_batch_dft(fdtd_b200_batch_t *bt, size_t scene, double *re, double *im) {
+    if (!bt || scene >= bt->n || !re || !im) {
+        rfb_set_error("batch: bad scene index or output");
+        return -1;
+    }
+    if (rfb_batch_sync(bt->b) != 0) return -1;
+    fdtd_b200_sim_t *sim = bt->sims[scene];
+    return rfb_engine_probe_dft(sim->eng, sim->n_freqs, sim->freqs, sim->dft_offset, re, im);
+}
+
+int fdtd_b200_batch_info(const fdtd_b200_batch_t *bt, fdtd_b200_batch_info_t *info) {
+    if (!bt || !info) return -1;
+    rfb_batch_info_t bi;
+    if (rfb_batch_info(bt->b, &bi) != 0) return -1;
+    info->scenes = bi.scenes;
+    info->cells = bi.cells;
+    info->list_cells = bi.list_cells;
+    info->slab_cell_axes = bi.slab_cell_axes;
+    info->tile_j = bi.tile_j;
+    info->ring_depth = bi.ring_depth;
+    info->mode = bi.mode;
+    info->seg_interior = bi.seg_interior;
+    info->seg_edge = bi.seg_edge;
+    info->items_interior = bi.items_interior;
+    info->items_xslab = bi.items_xslab;
+    info->items_edge = bi.items_edge;
+    info->launches_per_step = bi.launches_per_step;
+    return 0;
 }

@@ -262,9 +262,7 @@ __device__ __forceinline__ T e_ade(const Args<T> &a, int e, int comp, int i, int
 // One thread per (cell, component) entry.  Reads E from the input buffers,
 // H from the output buffers (already advanced), writes E output.
 template <typename T>
-__global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= 3 * a.n_cells) return;
+__device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
     const int cell = e / 3, comp = e - 3 * cell;
     const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
     const long long c = cidx(a, i, j, k);
@@ -298,6 +296,13 @@ __global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
         v = e_ade(a, e, comp, i, j, k, v);
     }
     a.Eo[comp][c] = v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * a.n_cells) return;
+    e_list_entry(a, e);
 }
 
 // ---- probes ---------------------------------------------------------------

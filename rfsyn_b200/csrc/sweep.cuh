@@ -56,23 +56,23 @@ struct QLayout {
     static constexpr size_t total = misc + 16;
 };
 
-template <typename T, int TJ, int NS, int MINB, int KIND>
-__global__ void __launch_bounds__(32 * TJ, MINB)
-    k_sweep_q(Args<T> a, FusedDims d, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps,
-              int *queue, int *err) {
-    static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
-    static_assert(TJ >= 3, "warps 0-2 share the halo recomputation");
+// One work item: the march over planes [ib, ie) of the (TJ x 32) tile at
+// (j0, k0) of the scene described by `a`, `d` and `maps`.  `phase`,
+// `pending` and `failed` are the CTA's ring bookkeeping, carried across
+// items.  Returns false when a copy did not complete in time (the caller
+// drains the ring and leaves the queue).
+template <typename T, int TJ, int NS, int KIND>
+__device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, const TmaMaps &maps, const SweepItem &it,
+                                       unsigned char *smem_raw, unsigned &phase, unsigned &pending, bool &failed) {
     constexpr bool EDGE = KIND == 2;  // per-cell y / z conditions and slabs
     constexpr bool XS = KIND >= 1;    // x-slab psi and plane conditions
     using L = TmaLayout<T, TJ, NS>;
     using S = QLayout<T, TJ, NS>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
     // H of the current plane (tile + halo), double-buffered by plane parity
     // so one block barrier per plane separates its writes from its reads
     T(*sHb)[3][TJ + 1][33] = reinterpret_cast<T(*)[3][TJ + 1][33]>(smem_raw + S::sh);
     TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
-    volatile int *s_item = reinterpret_cast<volatile int *>(smem_raw + S::misc);
     auto E = [&](int s, int c) { return reinterpret_cast<T(*)[TMA_EW]>(smem_raw + s * L::stage + c * L::ebox); };
     auto H = [&](int s, int c) {
         return reinterpret_cast<T(*)[TMA_HW]>(smem_raw + s * L::stage + 3 * L::ebox + c * L::hbox);
@@ -80,7 +80,6 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     auto CODE = [&](int s) {
         return reinterpret_cast<uint8_t(*)[32]>(smem_raw + s * L::stage + 3 * L::ebox + 3 * L::hbox);
     };
-
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
     const int r = ty + 1, q = tx + 4;  // stage coordinates of the own cell
@@ -90,412 +89,422 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     const T cbh = a.cbh;
     const int on = a.cpml_on;
     const long long ny1 = a.ny + 1;
+    const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
 
-    if (tid == 0) {
-        for (int s = 0; s < NS; s++) mbar_init(&bars[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    auto issue = [&](int s, int p) {
+        if (p < 0 || failed) return;  // a failed CTA issues no further copies
+        if (tid == 0) {
+            mbar_expect_tx(&bars[s], tx_bytes);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                tma_load_3d(E(s, c), &maps.e[c], k0 - 4, j0 - 1, p, &bars[s]);
+                tma_load_3d(H(s, c), &maps.h[c], k0 - 4, j0 - 1, p, &bars[s]);
+            }
+            if (with_codes) tma_load_3d(CODE(s), &maps.code, k0, j0, p, &bars[s]);
+        }
+        pending |= 1u << s;
+    };
+    // a wait that timed out marks the CTA failed; later waits return at
+    // once and the item ends with garbage, reported at its end
+    auto wait_slot = [&](int s) {
+        if (!(pending & (1u << s))) return;
+        if (failed || !mbar_wait(&bars[s], (phase >> s) & 1u)) {
+            failed = true;
+            return;  // still pending: drained (bounded) on the bail path
+        }
+        phase ^= 1u << s;
+        pending &= ~(1u << s);
+    };
+
+    // ---- per-thread geometry of the item ----
+    // The interior instantiation takes tiles whose cells and halos lie
+    // outside the y / z slabs and boundaries: every component is swept
+    // at every (j, k), only the plane (x) conditions and x-slab psi
+    // remain, both uniform per plane.  The edge instantiation adds the
+    // per-cell y / z conditions and y / z slab psi.
+    const int j = j0 + ty, k = k0 + tx;
+    const bool own = !EDGE || (j >= 0 && k >= 0 && j < d.cj && k < d.ck);
+    const int pitch = (int)a.pitch;
+    const int plane32 = (int)a.plane;
+    const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
+    unsigned mjk = 0x3f;                   // bits 0-2 H, 3-5 E at (j, k), plane apart
+    bool rowh = true, colh = tx < TJ;      // halo cells this thread recomputes
+    int sjh = -1, skh = -1, sjm = -1, skm = -1;
+    int sjh_row = -1, sjh_col = -1, skh_col = -1;
+    unsigned mrow_jk = 5u, mcol_jk = 3u;   // halo components at (j, k), plane apart
+    if constexpr (EDGE) {
+        const int jmin = py ? 0 : 1, kmin = pz ? 0 : 1;
+        mjk = 0;
+        if (own) {
+            if (j < a.ny && k < a.nz) mjk |= 1u;
+            if (j < a.ny + (py ? 0 : 1) && k < a.nz) mjk |= 2u;
+            if (j < a.ny && k < a.nz + (pz ? 0 : 1)) mjk |= 4u;
+            if (j < a.ny && k < a.nz) {
+                if (j >= jmin && k >= kmin) mjk |= 8u;
+                if (k >= kmin) mjk |= 16u;
+                if (j >= jmin) mjk |= 32u;
+            }
+        }
+        rowh = j0 > 0 && k >= 0 && k < d.ck;
+        colh = tx < TJ && k0 > 0 && jc >= 0 && jc < d.cj;
+        mrow_jk = (k < a.nz ? 1u : 0u) | (k < a.nz + (pz ? 0 : 1) ? 4u : 0u);
+        mcol_jk = (jc < a.ny ? 1u : 0u) | (jc < a.ny + (py ? 0 : 1) ? 2u : 0u);
+        sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
+        skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
+        sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
+        skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
+        sjh_row = slab_in(jh, a.lo_h[1], a.hi_h[1], a.ny, on);
+        sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
+        skh_col = slab_in(kh, a.lo_h[2], a.hi_h[2], a.nz, on);
+        for (int t = tid; t < TJ + 1; t += 32 * TJ) {
+            T v[3];
+            prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], j0 - 1 + t, a.ny, v);
+            tt.py[0][t] = v[0]; tt.py[1][t] = v[1]; tt.py[2][t] = v[2];
+            prof_at(on ? a.kinv_m[1] : (const T *)nullptr, a.b_m[1], a.a_m[1], j0 - 1 + t, a.ny + 1, v);
+            tt.py[3][t] = v[0]; tt.py[4][t] = v[1]; tt.py[5][t] = v[2];
+        }
+        for (int t = tid; t < 33; t += 32 * TJ) {
+            T v[3];
+            prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], k0 - 1 + t, a.nz, v);
+            tt.pz[0][t] = v[0]; tt.pz[1][t] = v[1]; tt.pz[2][t] = v[2];
+            prof_at(on ? a.kinv_m[2] : (const T *)nullptr, a.b_m[2], a.a_m[2], k0 - 1 + t, a.nz + 1, v);
+            tt.pz[3][t] = v[0]; tt.pz[4][t] = v[1]; tt.pz[5][t] = v[2];
+        }
     }
+    const int nshy = a.ns_h[1], nshz = a.ns_h[2], nsmy = a.ns_m[1], nsmz = a.ns_m[2];
+    // 32-bit element offsets (the plan admits these sweeps only when every
+    // field plane and psi array has fewer than 2^31 elements): in-plane
+    // offsets (x-slab psi arrays are planes of the field layout), y-slab
+    // offsets s*pitch + k, z-slab offsets j*ns + s; per plane a uniform
+    // base is added
+    struct Cell {
+        int ox, oy, oz;  // x-, y-, z-slab array offsets (plane / slab bases apart)
+        int sy, sz;      // H-grid y / z slab indices (-1 outside)
+    };
+    const Cell own_c = {j * pitch + k, sjh * pitch + k, j * nshz + skh, sjh, skh};
+    const Cell row_c = {jh * pitch + k, sjh_row * pitch + k, jh * nshz + skh, sjh_row, skh};
+    const Cell col_c = {jc * pitch + kh, sjh_col * pitch + kh, jc * nshz + skh_col, sjh_col, skh_col};
+    const int oym = sjm * pitch + k, ozm = j * nsmz + skm;
+    // per-plane uniform bases of the H-side psi arrays and the plane's x
+    // profile (kappa_inv, b, a) on the H and E grids
+    struct PlaneB {
+        int by, bz, bx, sx;
+    };
+    auto plane_b = [&](int i) -> PlaneB {
+        const int sx = (XS && on) ? slab_in(i, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
+        return PlaneB{i * nshy * pitch, i * (int)ny1 * nshz, sx * plane32, sx};
+    };
+    T xph[3] = {T(1), T(1), T(0)}, xpm[3] = {T(1), T(1), T(0)};
+    auto load_xprof = [&](int i, int sxh_, int sxm_) {
+        if constexpr (!XS) return;
+        if (sxh_ >= 0) {
+            xph[0] = a.kinv_h[0][i];
+            xph[1] = a.b_h[0][i];
+            xph[2] = a.a_h[0][i];
+        }
+        if (sxm_ >= 0) {
+            xpm[0] = a.kinv_m[0][i];
+            xpm[1] = a.b_m[0][i];
+            xpm[2] = a.a_m[0][i];
+        }
+    };
+
+    // H of component c at plane i (slots sc / sn) for the cell at stage
+    // position (rr, qq) described by `cl`; yi / zi are its rows in the
+    // profile tables.  pA / pB are the cell's psi inputs of the two terms
+    // (used where a slab applies); the updated psi are stored when `store`.
+    auto hcell = [&](int c, const PlaneB &pb, int sc, int sn, int rr, int qq, const Cell &cl, int yi, int zi,
+                     T pA, T pB, bool store) -> T {
+        const T hin = H(sc, c)[rr][qq];
+        T dA, dB;
+        if (c == 0) {
+            dA = xs(E(sc, 2)[rr + 1][qq], E(sc, 2)[rr][qq]);
+            dB = xs(E(sc, 1)[rr][qq + 1], E(sc, 1)[rr][qq]);
+        } else if (c == 1) {
+            dA = xs(E(sc, 0)[rr][qq + 1], E(sc, 0)[rr][qq]);
+            dB = xs(E(sn, 2)[rr][qq], E(sc, 2)[rr][qq]);
+        } else {
+            dA = xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]);
+            dB = xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq]);
+        }
+        T pn;
+        if (c == 0) {
+            if (EDGE && cl.sy >= 0) {
+                dA = stretch(dA, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pA, &pn);
+                if (store) a.psi_ho[0][pb.by + cl.oy] = pn;
+            }
+            if (EDGE && cl.sz >= 0) {
+                dB = stretch(dB, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pB, &pn);
+                if (store) a.psi_ho[1][pb.bz + cl.oz] = pn;
+            }
+        } else if (c == 1) {
+            if (EDGE && cl.sz >= 0) {
+                dA = stretch(dA, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pA, &pn);
+                if (store) a.psi_ho[2][pb.bz + cl.oz] = pn;
+            }
+            if (pb.sx >= 0) {
+                dB = stretch(dB, xph[0], xph[1], xph[2], a.dx, pB, &pn);
+                if (store) a.psi_ho[3][pb.bx + cl.ox] = pn;
+            }
+        } else {
+            if (pb.sx >= 0) {
+                dA = stretch(dA, xph[0], xph[1], xph[2], a.dx, pA, &pn);
+                if (store) a.psi_ho[4][pb.bx + cl.ox] = pn;
+            }
+            if (EDGE && cl.sy >= 0) {
+                dB = stretch(dB, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pB, &pn);
+                if (store) a.psi_ho[5][pb.by + cl.oy] = pn;
+            }
+        }
+        return xs(hin, xm(cbh, xs(dA, dB)));
+    };
+    // psi inputs of H component c at a cell (zero where no slab applies)
+    auto hpsi = [&](int c, const PlaneB &pb, const Cell &cl, T &pA, T &pB) {
+        pA = T(0);
+        pB = T(0);
+        if (c == 0) {
+            if (EDGE && cl.sy >= 0) pA = a.psi_hi[0][pb.by + cl.oy];
+            if (EDGE && cl.sz >= 0) pB = a.psi_hi[1][pb.bz + cl.oz];
+        } else if (c == 1) {
+            if (EDGE && cl.sz >= 0) pA = a.psi_hi[2][pb.bz + cl.oz];
+            if (pb.sx >= 0) pB = a.psi_hi[3][pb.bx + cl.ox];
+        } else {
+            if (pb.sx >= 0) pA = a.psi_hi[4][pb.bx + cl.ox];
+            if (EDGE && cl.sy >= 0) pB = a.psi_hi[5][pb.by + cl.oy];
+        }
+    };
+    // plane conditions: H bits (Hx to nx inclusive on a PEC x axis), E bits
+    auto plane_mask = [&](int i) -> unsigned {
+        if constexpr (!XS) return 0x3fu;
+        unsigned m = 0;
+        if (i < a.nx + (px ? 0 : 1)) m |= 1u;
+        if (i < a.nx) m |= 2u | 4u | 8u;
+        if (i < a.nx && i >= (px ? 0 : 1)) m |= 16u | 32u;
+        return m;
+    };
+
+    // ---- prologue: previous plane and the first NS-1 planes ----
+    int pprev = ib > 0 ? ib - 1 : (px ? a.nx - 1 : -1);
+    int pf = ib;
+    issue(NS - 1, pprev);
+#pragma unroll
+    for (int s = 0; s < NS - 1; s++) {
+        if (pf >= 0 && ib + s <= ie) issue(s, pf);
+        if (pf >= 0) pf = plane_after(pf, a.nx, px);
+    }
+    wait_slot(NS - 1);
+    wait_slot(0);
+    if (__syncthreads_or(failed)) return false;
+    {
+        T prevHy = T(0), prevHz = T(0);
+        if (pprev >= 0) {
+            const unsigned mp = plane_mask(pprev) & mjk;
+            const PlaneB pb = plane_b(pprev);
+            load_xprof(pprev, pb.sx, -1);
+            // psi are read only for components swept at the cell, so
+            // every offset used addresses a cell of the grid
+            T pA = T(0), pB = T(0);
+            prevHy = H(NS - 1, 1)[r][q];
+            if (mp & 2u) {
+                hpsi(1, pb, own_c, pA, pB);
+                prevHy = hcell(1, pb, NS - 1, 0, r, q, own_c, r, qs, pA, pB, false);
+            }
+            prevHz = H(NS - 1, 2)[r][q];
+            if (mp & 4u) {
+                hpsi(2, pb, own_c, pA, pB);
+                prevHz = hcell(2, pb, NS - 1, 0, r, q, own_c, r, qs, pA, pB, false);
+            }
+        }
+        __syncthreads();  // slot NS-1 may now be refilled
+
+        int sc = 0;
+        for (int i = ib; i < ie; i++) {
+            const int sn = sc == NS - 1 ? 0 : sc + 1;
+            const int sf = sc == 0 ? NS - 1 : sc - 1;  // held plane i-1, read by nobody any more
+            if (pf >= 0 && i + NS - 1 <= ie) {
+                issue(sf, pf);
+                pf = plane_after(pf, a.nx, px);
+            }
+            const unsigned mpl = plane_mask(i);
+            const unsigned m = mpl & mjk;
+            const PlaneB pb = plane_b(i);
+            const int sxm = (XS && on) ? slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on) : -1;
+            const int bym = i * nsmy * pitch, bzm = i * (int)ny1 * nsmz, bxm = sxm * plane32;
+            // halo cells recomputed this plane: row (j0-1, k) Hx, Hz;
+            // column (j0+tx, k0-1) Hx, Hy
+            // row halo: Hx by warp 0, Hz by warp 2
+            const unsigned mrow = (ty == 0 && rowh) ? (mpl & mrow_jk & 1u)
+                                  : (ty == 2 && rowh) ? (mpl & mrow_jk & 4u) : 0u;
+            const unsigned mcol = (ty == 1 && colh) ? (mpl & mcol_jk) : 0u;
+            // psi inputs of the own cell and of the halo cells and the
+            // plane's x profile, all loaded before the wait; psi are read
+            // only for components swept at the cell, so every offset
+            // used addresses a cell of the grid
+            T hp[6], ep[6], hh[4];
+#pragma unroll
+            for (int t = 0; t < 6; t++) hp[t] = ep[t] = T(0);
+#pragma unroll
+            for (int t = 0; t < 4; t++) hh[t] = T(0);
+            load_xprof(i, pb.sx, sxm);
+            if (m & 1u) hpsi(0, pb, own_c, hp[0], hp[1]);
+            if (m & 2u) hpsi(1, pb, own_c, hp[2], hp[3]);
+            if (m & 4u) hpsi(2, pb, own_c, hp[4], hp[5]);
+            if (mrow & 1u) hpsi(0, pb, row_c, hh[0], hh[1]);
+            if (mrow & 4u) hpsi(2, pb, row_c, hh[2], hh[3]);
+            if (mcol & 1u) hpsi(0, pb, col_c, hh[0], hh[1]);
+            if (mcol & 2u) hpsi(1, pb, col_c, hh[2], hh[3]);
+            if (m & 8u) {
+                if (EDGE && sjm >= 0) ep[0] = a.psi_e[0][bym + oym];
+                if (EDGE && skm >= 0) ep[1] = a.psi_e[1][bzm + ozm];
+            }
+            if (m & 16u) {
+                if (EDGE && skm >= 0) ep[2] = a.psi_e[2][bzm + ozm];
+                if (sxm >= 0) ep[3] = a.psi_e[3][bxm + own_c.ox];
+            }
+            if (m & 32u) {
+                if (sxm >= 0) ep[4] = a.psi_e[4][bxm + own_c.ox];
+                if (EDGE && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
+            }
+            wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
+            T(*sH)[TJ + 1][33] = sHb[(i - ib) & 1];
+            const T e0 = E(sc, 0)[r][q], e1 = E(sc, 1)[r][q], e2 = E(sc, 2)[r][q];
+            const int code = with_codes ? (int)CODE(sc)[ty][tx] : 0;
+            const long long c = (long long)i * a.plane + own_c.ox;
+            T hx = H(sc, 0)[r][q], hy = H(sc, 1)[r][q], hz = H(sc, 2)[r][q];
+            if (m & 1u) hx = hcell(0, pb, sc, sn, r, q, own_c, r, qs, hp[0], hp[1], true);
+            if (m & 2u) hy = hcell(1, pb, sc, sn, r, q, own_c, r, qs, hp[2], hp[3], true);
+            if (m & 4u) hz = hcell(2, pb, sc, sn, r, q, own_c, r, qs, hp[4], hp[5], true);
+            if (own) {
+                a.Ho[0][c] = hx;
+                a.Ho[1][c] = hy;
+                a.Ho[2][c] = hz;
+            }
+            sH[0][r][qs] = hx;
+            sH[1][r][qs] = hy;
+            sH[2][r][qs] = hz;
+            if (ty == 0 && rowh) {
+                // row halo (j0-1, k): Hx
+                T v = H(sc, 0)[0][q];
+                if (mrow & 1u) v = hcell(0, pb, sc, sn, 0, q, row_c, 0, qs, hh[0], hh[1], false);
+                sH[0][0][qs] = v;
+            } else if (ty == 2 && rowh) {
+                // row halo (j0-1, k): Hz
+                T v = H(sc, 2)[0][q];
+                if (mrow & 4u) v = hcell(2, pb, sc, sn, 0, q, row_c, 0, qs, hh[2], hh[3], false);
+                sH[2][0][qs] = v;
+            } else if (ty == 1 && colh) {
+                // column halo (j0+tx, k0-1): Hx, Hy
+                T v = H(sc, 0)[tx + 1][3];
+                if (mcol & 1u) v = hcell(0, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[0], hh[1], false);
+                sH[0][tx + 1][0] = v;
+                v = H(sc, 1)[tx + 1][3];
+                if (mcol & 2u) v = hcell(1, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[2], hh[3], false);
+                sH[1][tx + 1][0] = v;
+            }
+            __syncthreads();
+            if (!with_codes || code != LIST_CODE) {
+                bool skip = false;
+                if constexpr (EDGE) {
+                    if (!with_codes)
+                        for (int s = 0; s < a.n_skip; s++) skip |= a.skip[s] == c;
+                }
+                if (!skip) {
+                    const T ca = tt.tab[code], cb = tt.tab[256 + code];
+                    T pn;
+                    if (m & 8u) {
+                        T tA = xs(sH[2][r][qs], sH[2][r - 1][qs]);
+                        T tB = xs(sH[1][r][qs], sH[1][r][qs - 1]);
+                        if (EDGE && sjm >= 0) {
+                            tA = stretch(tA, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[0], &pn);
+                            a.psi_e[0][bym + oym] = pn;
+                        }
+                        if (EDGE && skm >= 0) {
+                            tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
+                            a.psi_e[1][bzm + ozm] = pn;
+                        }
+                        a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
+                    }
+                    if (m & 16u) {
+                        T tA = xs(sH[0][r][qs], sH[0][r][qs - 1]);
+                        T tB = xs(hz, prevHz);
+                        if (EDGE && skm >= 0) {
+                            tA = stretch(tA, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[2], &pn);
+                            a.psi_e[2][bzm + ozm] = pn;
+                        }
+                        if (sxm >= 0) {
+                            tB = stretch(tB, xpm[0], xpm[1], xpm[2], a.dx, ep[3], &pn);
+                            a.psi_e[3][bxm + own_c.ox] = pn;
+                        }
+                        a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
+                    }
+                    if (m & 32u) {
+                        T tA = xs(hy, prevHy);
+                        T tB = xs(sH[0][r][qs], sH[0][r - 1][qs]);
+                        if (sxm >= 0) {
+                            tA = stretch(tA, xpm[0], xpm[1], xpm[2], a.dx, ep[4], &pn);
+                            a.psi_e[4][bxm + own_c.ox] = pn;
+                        }
+                        if (EDGE && sjm >= 0) {
+                            tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
+                            a.psi_e[5][bym + oym] = pn;
+                        }
+                        a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
+                    }
+                }
+            }
+            prevHy = hy;
+            prevHz = hz;
+            sc = sn;
+        }
+    }
+    return !__syncthreads_or(failed);
+}
+
+// Loads the scene's (Ca, Cb) table into the CTA's shared tables.
+template <typename T, int TJ, int NS>
+__device__ __forceinline__ void q_load_table(const Args<T> &a, unsigned char *smem_raw) {
+    using S = QLayout<T, TJ, NS>;
+    TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
+    const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int t = tid; t < 256; t += 32 * TJ) {
         tt.tab[t] = a.tca[t];
         tt.tab[256 + t] = a.tcb[t];
     }
-    __syncthreads();
+}
 
-    // uniform bookkeeping: phase bit s = parity of slot s's next completion,
-    // pending bit s = slot s has a load in flight that nobody waited for
-    unsigned phase = 0, pending = 0;
-    bool failed = false;
+// Tensor copies need their shared destinations on 128-byte boundaries; the
+// layouts keep every box at a multiple of 128 from the dynamic region's
+// start.  A CTA whose region does not start on such a boundary records
+// error 2 and returns before issuing anything.
+__device__ __forceinline__ bool q_misaligned(const unsigned char *smem, int *err) {
+    if ((__cvta_generic_to_shared(smem) & 127u) == 0) return false;
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(err, 2);
+    return true;
+}
 
-    for (;;) {
-        if (tid == 0) *s_item = atomicAdd(&queue[0], 1);
-        __syncthreads();
-        const int w = *s_item;
-        if (w >= n_items) break;
-        const SweepItem it = items[w];
-        const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
-
-        auto issue = [&](int s, int p) {
-            if (p < 0 || failed) return;  // a failed CTA issues no further copies
-            if (tid == 0) {
-                mbar_expect_tx(&bars[s], tx_bytes);
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    tma_load_3d(E(s, c), &maps.e[c], k0 - 4, j0 - 1, p, &bars[s]);
-                    tma_load_3d(H(s, c), &maps.h[c], k0 - 4, j0 - 1, p, &bars[s]);
-                }
-                if (with_codes) tma_load_3d(CODE(s), &maps.code, k0, j0, p, &bars[s]);
-            }
-            pending |= 1u << s;
-        };
-        // a wait that timed out marks the CTA failed; later waits return at
-        // once and the item ends with garbage, reported at its end
-        auto wait_slot = [&](int s) {
-            if (!(pending & (1u << s))) return;
-            if (failed || !mbar_wait(&bars[s], (phase >> s) & 1u)) {
-                failed = true;
-                return;  // still pending: drained (bounded) on the bail path
-            }
-            phase ^= 1u << s;
-            pending &= ~(1u << s);
-        };
-
-        // ---- per-thread geometry of the item ----
-        // The interior instantiation takes tiles whose cells and halos lie
-        // outside the y / z slabs and boundaries: every component is swept
-        // at every (j, k), only the plane (x) conditions and x-slab psi
-        // remain, both uniform per plane.  The edge instantiation adds the
-        // per-cell y / z conditions and y / z slab psi.
-        const int j = j0 + ty, k = k0 + tx;
-        const bool own = !EDGE || (j >= 0 && k >= 0 && j < d.cj && k < d.ck);
-        const int pitch = (int)a.pitch;
-        const int plane32 = (int)a.plane;
-        const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
-        unsigned mjk = 0x3f;                   // bits 0-2 H, 3-5 E at (j, k), plane apart
-        bool rowh = true, colh = tx < TJ;      // halo cells this thread recomputes
-        int sjh = -1, skh = -1, sjm = -1, skm = -1;
-        int sjh_row = -1, sjh_col = -1, skh_col = -1;
-        unsigned mrow_jk = 5u, mcol_jk = 3u;   // halo components at (j, k), plane apart
-        if constexpr (EDGE) {
-            const int jmin = py ? 0 : 1, kmin = pz ? 0 : 1;
-            mjk = 0;
-            if (own) {
-                if (j < a.ny && k < a.nz) mjk |= 1u;
-                if (j < a.ny + (py ? 0 : 1) && k < a.nz) mjk |= 2u;
-                if (j < a.ny && k < a.nz + (pz ? 0 : 1)) mjk |= 4u;
-                if (j < a.ny && k < a.nz) {
-                    if (j >= jmin && k >= kmin) mjk |= 8u;
-                    if (k >= kmin) mjk |= 16u;
-                    if (j >= jmin) mjk |= 32u;
-                }
-            }
-            rowh = j0 > 0 && k >= 0 && k < d.ck;
-            colh = tx < TJ && k0 > 0 && jc >= 0 && jc < d.cj;
-            mrow_jk = (k < a.nz ? 1u : 0u) | (k < a.nz + (pz ? 0 : 1) ? 4u : 0u);
-            mcol_jk = (jc < a.ny ? 1u : 0u) | (jc < a.ny + (py ? 0 : 1) ? 2u : 0u);
-            sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
-            skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
-            sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
-            skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
-            sjh_row = slab_in(jh, a.lo_h[1], a.hi_h[1], a.ny, on);
-            sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
-            skh_col = slab_in(kh, a.lo_h[2], a.hi_h[2], a.nz, on);
-            for (int t = tid; t < TJ + 1; t += 32 * TJ) {
-                T v[3];
-                prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], j0 - 1 + t, a.ny, v);
-                tt.py[0][t] = v[0]; tt.py[1][t] = v[1]; tt.py[2][t] = v[2];
-                prof_at(on ? a.kinv_m[1] : (const T *)nullptr, a.b_m[1], a.a_m[1], j0 - 1 + t, a.ny + 1, v);
-                tt.py[3][t] = v[0]; tt.py[4][t] = v[1]; tt.py[5][t] = v[2];
-            }
-            for (int t = tid; t < 33; t += 32 * TJ) {
-                T v[3];
-                prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], k0 - 1 + t, a.nz, v);
-                tt.pz[0][t] = v[0]; tt.pz[1][t] = v[1]; tt.pz[2][t] = v[2];
-                prof_at(on ? a.kinv_m[2] : (const T *)nullptr, a.b_m[2], a.a_m[2], k0 - 1 + t, a.nz + 1, v);
-                tt.pz[3][t] = v[0]; tt.pz[4][t] = v[1]; tt.pz[5][t] = v[2];
-            }
-        }
-        const int nshy = a.ns_h[1], nshz = a.ns_h[2], nsmy = a.ns_m[1], nsmz = a.ns_m[2];
-        // 32-bit element offsets (the plan admits these sweeps only when every
-        // field plane and psi array has fewer than 2^31 elements): in-plane
-        // offsets (x-slab psi arrays are planes of the field layout), y-slab
-        // offsets s*pitch + k, z-slab offsets j*ns + s; per plane a uniform
-        // base is added
-        struct Cell {
-            int ox, oy, oz;  // x-, y-, z-slab array offsets (plane / slab bases apart)
-            int sy, sz;      // H-grid y / z slab indices (-1 outside)
-        };
-        const Cell own_c = {j * pitch + k, sjh * pitch + k, j * nshz + skh, sjh, skh};
-        const Cell row_c = {jh * pitch + k, sjh_row * pitch + k, jh * nshz + skh, sjh_row, skh};
-        const Cell col_c = {jc * pitch + kh, sjh_col * pitch + kh, jc * nshz + skh_col, sjh_col, skh_col};
-        const int oym = sjm * pitch + k, ozm = j * nsmz + skm;
-        // per-plane uniform bases of the H-side psi arrays and the plane's x
-        // profile (kappa_inv, b, a) on the H and E grids
-        struct PlaneB {
-            int by, bz, bx, sx;
-        };
-        auto plane_b = [&](int i) -> PlaneB {
-            const int sx = (XS && on) ? slab_in(i, a.lo_h[0], a.hi_h[0], a.nx, on) : -1;
-            return PlaneB{i * nshy * pitch, i * (int)ny1 * nshz, sx * plane32, sx};
-        };
-        T xph[3] = {T(1), T(1), T(0)}, xpm[3] = {T(1), T(1), T(0)};
-        auto load_xprof = [&](int i, int sxh_, int sxm_) {
-            if constexpr (!XS) return;
-            if (sxh_ >= 0) {
-                xph[0] = a.kinv_h[0][i];
-                xph[1] = a.b_h[0][i];
-                xph[2] = a.a_h[0][i];
-            }
-            if (sxm_ >= 0) {
-                xpm[0] = a.kinv_m[0][i];
-                xpm[1] = a.b_m[0][i];
-                xpm[2] = a.a_m[0][i];
-            }
-        };
-
-        // H of component c at plane i (slots sc / sn) for the cell at stage
-        // position (rr, qq) described by `cl`; yi / zi are its rows in the
-        // profile tables.  pA / pB are the cell's psi inputs of the two terms
-        // (used where a slab applies); the updated psi are stored when `store`.
-        auto hcell = [&](int c, const PlaneB &pb, int sc, int sn, int rr, int qq, const Cell &cl, int yi, int zi,
-                         T pA, T pB, bool store) -> T {
-            const T hin = H(sc, c)[rr][qq];
-            T dA, dB;
-            if (c == 0) {
-                dA = xs(E(sc, 2)[rr + 1][qq], E(sc, 2)[rr][qq]);
-                dB = xs(E(sc, 1)[rr][qq + 1], E(sc, 1)[rr][qq]);
-            } else if (c == 1) {
-                dA = xs(E(sc, 0)[rr][qq + 1], E(sc, 0)[rr][qq]);
-                dB = xs(E(sn, 2)[rr][qq], E(sc, 2)[rr][qq]);
-            } else {
-                dA = xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]);
-                dB = xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq]);
-            }
-            T pn;
-            if (c == 0) {
-                if (EDGE && cl.sy >= 0) {
-                    dA = stretch(dA, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pA, &pn);
-                    if (store) a.psi_ho[0][pb.by + cl.oy] = pn;
-                }
-                if (EDGE && cl.sz >= 0) {
-                    dB = stretch(dB, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pB, &pn);
-                    if (store) a.psi_ho[1][pb.bz + cl.oz] = pn;
-                }
-            } else if (c == 1) {
-                if (EDGE && cl.sz >= 0) {
-                    dA = stretch(dA, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pA, &pn);
-                    if (store) a.psi_ho[2][pb.bz + cl.oz] = pn;
-                }
-                if (pb.sx >= 0) {
-                    dB = stretch(dB, xph[0], xph[1], xph[2], a.dx, pB, &pn);
-                    if (store) a.psi_ho[3][pb.bx + cl.ox] = pn;
-                }
-            } else {
-                if (pb.sx >= 0) {
-                    dA = stretch(dA, xph[0], xph[1], xph[2], a.dx, pA, &pn);
-                    if (store) a.psi_ho[4][pb.bx + cl.ox] = pn;
-                }
-                if (EDGE && cl.sy >= 0) {
-                    dB = stretch(dB, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pB, &pn);
-                    if (store) a.psi_ho[5][pb.by + cl.oy] = pn;
-                }
-            }
-            return xs(hin, xm(cbh, xs(dA, dB)));
-        };
-        // psi inputs of H component c at a cell (zero where no slab applies)
-        auto hpsi = [&](int c, const PlaneB &pb, const Cell &cl, T &pA, T &pB) {
-            pA = T(0);
-            pB = T(0);
-            if (c == 0) {
-                if (EDGE && cl.sy >= 0) pA = a.psi_hi[0][pb.by + cl.oy];
-                if (EDGE && cl.sz >= 0) pB = a.psi_hi[1][pb.bz + cl.oz];
-            } else if (c == 1) {
-                if (EDGE && cl.sz >= 0) pA = a.psi_hi[2][pb.bz + cl.oz];
-                if (pb.sx >= 0) pB = a.psi_hi[3][pb.bx + cl.ox];
-            } else {
-                if (pb.sx >= 0) pA = a.psi_hi[4][pb.bx + cl.ox];
-                if (EDGE && cl.sy >= 0) pB = a.psi_hi[5][pb.by + cl.oy];
-            }
-        };
-        // plane conditions: H bits (Hx to nx inclusive on a PEC x axis), E bits
-        auto plane_mask = [&](int i) -> unsigned {
-            if constexpr (!XS) return 0x3fu;
-            unsigned m = 0;
-            if (i < a.nx + (px ? 0 : 1)) m |= 1u;
-            if (i < a.nx) m |= 2u | 4u | 8u;
-            if (i < a.nx && i >= (px ? 0 : 1)) m |= 16u | 32u;
-            return m;
-        };
-
-        // ---- prologue: previous plane and the first NS-1 planes ----
-        int pprev = ib > 0 ? ib - 1 : (px ? a.nx - 1 : -1);
-        int pf = ib;
-        issue(NS - 1, pprev);
-#pragma unroll
-        for (int s = 0; s < NS - 1; s++) {
-            if (pf >= 0 && ib + s <= ie) issue(s, pf);
-            if (pf >= 0) pf = plane_after(pf, a.nx, px);
-        }
-        wait_slot(NS - 1);
-        wait_slot(0);
-        if (__syncthreads_or(failed)) goto bail;
-        {
-            T prevHy = T(0), prevHz = T(0);
-            if (pprev >= 0) {
-                const unsigned mp = plane_mask(pprev) & mjk;
-                const PlaneB pb = plane_b(pprev);
-                load_xprof(pprev, pb.sx, -1);
-                // psi are read only for components swept at the cell, so
-                // every offset used addresses a cell of the grid
-                T pA = T(0), pB = T(0);
-                prevHy = H(NS - 1, 1)[r][q];
-                if (mp & 2u) {
-                    hpsi(1, pb, own_c, pA, pB);
-                    prevHy = hcell(1, pb, NS - 1, 0, r, q, own_c, r, qs, pA, pB, false);
-                }
-                prevHz = H(NS - 1, 2)[r][q];
-                if (mp & 4u) {
-                    hpsi(2, pb, own_c, pA, pB);
-                    prevHz = hcell(2, pb, NS - 1, 0, r, q, own_c, r, qs, pA, pB, false);
-                }
-            }
-            __syncthreads();  // slot NS-1 may now be refilled
-
-            int sc = 0;
-            for (int i = ib; i < ie; i++) {
-                const int sn = sc == NS - 1 ? 0 : sc + 1;
-                const int sf = sc == 0 ? NS - 1 : sc - 1;  // held plane i-1, read by nobody any more
-                if (pf >= 0 && i + NS - 1 <= ie) {
-                    issue(sf, pf);
-                    pf = plane_after(pf, a.nx, px);
-                }
-                const unsigned mpl = plane_mask(i);
-                const unsigned m = mpl & mjk;
-                const PlaneB pb = plane_b(i);
-                const int sxm = (XS && on) ? slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on) : -1;
-                const int bym = i * nsmy * pitch, bzm = i * (int)ny1 * nsmz, bxm = sxm * plane32;
-                // halo cells recomputed this plane: row (j0-1, k) Hx, Hz;
-                // column (j0+tx, k0-1) Hx, Hy
-                // row halo: Hx by warp 0, Hz by warp 2
-                const unsigned mrow = (ty == 0 && rowh) ? (mpl & mrow_jk & 1u)
-                                      : (ty == 2 && rowh) ? (mpl & mrow_jk & 4u) : 0u;
-                const unsigned mcol = (ty == 1 && colh) ? (mpl & mcol_jk) : 0u;
-                // psi inputs of the own cell and of the halo cells and the
-                // plane's x profile, all loaded before the wait; psi are read
-                // only for components swept at the cell, so every offset
-                // used addresses a cell of the grid
-                T hp[6], ep[6], hh[4];
-#pragma unroll
-                for (int t = 0; t < 6; t++) hp[t] = ep[t] = T(0);
-#pragma unroll
-                for (int t = 0; t < 4; t++) hh[t] = T(0);
-                load_xprof(i, pb.sx, sxm);
-                if (m & 1u) hpsi(0, pb, own_c, hp[0], hp[1]);
-                if (m & 2u) hpsi(1, pb, own_c, hp[2], hp[3]);
-                if (m & 4u) hpsi(2, pb, own_c, hp[4], hp[5]);
-                if (mrow & 1u) hpsi(0, pb, row_c, hh[0], hh[1]);
-                if (mrow & 4u) hpsi(2, pb, row_c, hh[2], hh[3]);
-                if (mcol & 1u) hpsi(0, pb, col_c, hh[0], hh[1]);
-                if (mcol & 2u) hpsi(1, pb, col_c, hh[2], hh[3]);
-                if (m & 8u) {
-                    if (EDGE && sjm >= 0) ep[0] = a.psi_e[0][bym + oym];
-                    if (EDGE && skm >= 0) ep[1] = a.psi_e[1][bzm + ozm];
-                }
-                if (m & 16u) {
-                    if (EDGE && skm >= 0) ep[2] = a.psi_e[2][bzm + ozm];
-                    if (sxm >= 0) ep[3] = a.psi_e[3][bxm + own_c.ox];
-                }
-                if (m & 32u) {
-                    if (sxm >= 0) ep[4] = a.psi_e[4][bxm + own_c.ox];
-                    if (EDGE && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
-                }
-                wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
-                T(*sH)[TJ + 1][33] = sHb[(i - ib) & 1];
-                const T e0 = E(sc, 0)[r][q], e1 = E(sc, 1)[r][q], e2 = E(sc, 2)[r][q];
-                const int code = with_codes ? (int)CODE(sc)[ty][tx] : 0;
-                const long long c = (long long)i * a.plane + own_c.ox;
-                T hx = H(sc, 0)[r][q], hy = H(sc, 1)[r][q], hz = H(sc, 2)[r][q];
-                if (m & 1u) hx = hcell(0, pb, sc, sn, r, q, own_c, r, qs, hp[0], hp[1], true);
-                if (m & 2u) hy = hcell(1, pb, sc, sn, r, q, own_c, r, qs, hp[2], hp[3], true);
-                if (m & 4u) hz = hcell(2, pb, sc, sn, r, q, own_c, r, qs, hp[4], hp[5], true);
-                if (own) {
-                    a.Ho[0][c] = hx;
-                    a.Ho[1][c] = hy;
-                    a.Ho[2][c] = hz;
-                }
-                sH[0][r][qs] = hx;
-                sH[1][r][qs] = hy;
-                sH[2][r][qs] = hz;
-                if (ty == 0 && rowh) {
-                    // row halo (j0-1, k): Hx
-                    T v = H(sc, 0)[0][q];
-                    if (mrow & 1u) v = hcell(0, pb, sc, sn, 0, q, row_c, 0, qs, hh[0], hh[1], false);
-                    sH[0][0][qs] = v;
-                } else if (ty == 2 && rowh) {
-                    // row halo (j0-1, k): Hz
-                    T v = H(sc, 2)[0][q];
-                    if (mrow & 4u) v = hcell(2, pb, sc, sn, 0, q, row_c, 0, qs, hh[2], hh[3], false);
-                    sH[2][0][qs] = v;
-                } else if (ty == 1 && colh) {
-                    // column halo (j0+tx, k0-1): Hx, Hy
-                    T v = H(sc, 0)[tx + 1][3];
-                    if (mcol & 1u) v = hcell(0, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[0], hh[1], false);
-                    sH[0][tx + 1][0] = v;
-                    v = H(sc, 1)[tx + 1][3];
-                    if (mcol & 2u) v = hcell(1, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[2], hh[3], false);
-                    sH[1][tx + 1][0] = v;
-                }
-                __syncthreads();
-                if (!with_codes || code != LIST_CODE) {
-                    bool skip = false;
-                    if constexpr (EDGE) {
-                        if (!with_codes)
-                            for (int s = 0; s < a.n_skip; s++) skip |= a.skip[s] == c;
-                    }
-                    if (!skip) {
-                        const T ca = tt.tab[code], cb = tt.tab[256 + code];
-                        T pn;
-                        if (m & 8u) {
-                            T tA = xs(sH[2][r][qs], sH[2][r - 1][qs]);
-                            T tB = xs(sH[1][r][qs], sH[1][r][qs - 1]);
-                            if (EDGE && sjm >= 0) {
-                                tA = stretch(tA, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[0], &pn);
-                                a.psi_e[0][bym + oym] = pn;
-                            }
-                            if (EDGE && skm >= 0) {
-                                tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
-                                a.psi_e[1][bzm + ozm] = pn;
-                            }
-                            a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
-                        }
-                        if (m & 16u) {
-                            T tA = xs(sH[0][r][qs], sH[0][r][qs - 1]);
-                            T tB = xs(hz, prevHz);
-                            if (EDGE && skm >= 0) {
-                                tA = stretch(tA, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[2], &pn);
-                                a.psi_e[2][bzm + ozm] = pn;
-                            }
-                            if (sxm >= 0) {
-                                tB = stretch(tB, xpm[0], xpm[1], xpm[2], a.dx, ep[3], &pn);
-                                a.psi_e[3][bxm + own_c.ox] = pn;
-                            }
-                            a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
-                        }
-                        if (m & 32u) {
-                            T tA = xs(hy, prevHy);
-                            T tB = xs(sH[0][r][qs], sH[0][r - 1][qs]);
-                            if (sxm >= 0) {
-                                tA = stretch(tA, xpm[0], xpm[1], xpm[2], a.dx, ep[4], &pn);
-                                a.psi_e[4][bxm + own_c.ox] = pn;
-                            }
-                            if (EDGE && sjm >= 0) {
-                                tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
-                                a.psi_e[5][bym + oym] = pn;
-                            }
-                            a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
-                        }
-                    }
-                }
-                prevHy = hy;
-                prevHz = hz;
-                sc = sn;
-            }
-        }
-        if (__syncthreads_or(failed)) goto bail;
-        __syncthreads();  // the ring, the tables and the item slot are free again
-        continue;
-    bail:
-        // a copy did not complete in time: report it, let the copies still in
-        // flight land (bounded) before the shared memory is reused or released
-        if (tid == 0) {
-            atomicExch(err, 1);
-            for (int s = 0; s < NS; s++)
-                if (pending & (1u << s)) mbar_wait(&bars[s], (phase >> s) & 1u);
-        }
-        __syncthreads();
-        break;
+template <int NS>
+__device__ __forceinline__ void q_init_bars(uint64_t *bars) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        for (int s = 0; s < NS; s++) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    // leave the queue; the last CTA out rewinds it for the next launch
-    if (tid == 0) {
+}
+
+// A copy did not complete in time: report it, let the CTA's copies still in
+// flight land (bounded) before its shared memory is reused or released.
+template <int NS>
+__device__ __forceinline__ void q_bail(uint64_t *bars, unsigned phase, unsigned pending, int *err) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        atomicExch(err, 1);
+        for (int s = 0; s < NS; s++)
+            if (pending & (1u << s)) mbar_wait(&bars[s], (phase >> s) & 1u);
+    }
+    __syncthreads();
+}
+
+// Leaves the queue; the last CTA out rewinds it for the next launch.
+__device__ __forceinline__ void q_leave(int *queue) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
         __threadfence();
         if (atomicAdd(&queue[1], 1) == (int)gridDim.x - 1) {
             queue[0] = 0;
@@ -503,6 +512,38 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             __threadfence();
         }
     }
+}
+
+template <typename T, int TJ, int NS, int MINB, int KIND>
+__global__ void __launch_bounds__(32 * TJ, MINB)
+    k_sweep_q(Args<T> a, FusedDims d, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps,
+              int *queue, int *err) {
+    static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
+    static_assert(TJ >= 3, "warps 0-2 share the halo recomputation");
+    using S = QLayout<T, TJ, NS>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    if (q_misaligned(smem_raw, err)) return;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
+    volatile int *s_item = reinterpret_cast<volatile int *>(smem_raw + S::misc);
+    q_init_bars<NS>(bars);
+    q_load_table<T, TJ, NS>(a, smem_raw);
+    __syncthreads();
+    // ring bookkeeping: phase bit s = parity of slot s's next completion,
+    // pending bit s = slot s has a load in flight that nobody waited for
+    unsigned phase = 0, pending = 0;
+    bool failed = false;
+    for (;;) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) *s_item = atomicAdd(&queue[0], 1);
+        __syncthreads();
+        const int w = *s_item;
+        if (w >= n_items) break;
+        if (!q_item<T, TJ, NS, KIND>(a, d, maps, items[w], smem_raw, phase, pending, failed)) {
+            q_bail<NS>(bars, phase, pending, err);
+            break;
+        }
+        __syncthreads();  // the ring, the tables and the item slot are free again
+    }
+    q_leave(queue);
 }
 
 // Variants (element type, TJ, NS, CTAs per SM of the interior and of the

@@ -152,6 +152,67 @@ def c2(seed: int = 2, precision: int = FP32) -> Workload:
         probes=probes, freqs=list(np.linspace(4e9, 36e9, 256)), spheres=spheres)
 
 
+def c4(seed: int = 4, n_scenes: int = 512, precision: int = FP32, n_steps: int = 1500,
+       lo: int = 32, hi: int = 96, npml: int = 8) -> list[Workload]:
+    """Batched FDTD: n_scenes independent scenes, per-axis sizes uniform in
+    [lo, hi] cells, dx 1 mm, 8-cell CPML (rfsyn's default grading); 0-6
+    scatterers per scene, each a sphere (radius U[3,12] cells) or a box (sides
+    U[4,16] cells) with eps_r U[1,10] and sigma log-U[1e-4,1] S/m, clear of
+    the CPML (radii and sides capped to fit the smallest axis); one soft Ez dipole (Gaussian-modulated sinusoid f0 10 GHz,
+    tau = 2/(pi 8 GHz), t0 = 4 tau) and 4 Ez probes at interior positions;
+    n_steps steps; 128 DFT bins linear over 2..18 GHz.  Scene s draws from
+    PCG32(seed, stream s).  Needs lo >= 2 npml + 12."""
+    if lo < 2 * npml + 12:
+        raise ValueError("c4: the smallest axis must leave room for scatterers between the CPML slabs")
+    tau = 2.0 / (math.pi * 8e9)
+    freqs = list(np.linspace(2e9, 18e9, 128))
+    out = []
+    for sc in range(n_scenes):
+        rng = Pcg32(seed, sc)
+        nx, ny, nz = (rng.randint(lo, hi + 1) for _ in range(3))
+        dims = (nx, ny, nz)
+        boxes, spheres = [], []
+        room = min(dims) - 2 * (npml + 2)   # cells between the CPML margins
+        for _ in range(rng.randint(0, 7)):
+            eps, sig = rng.range(1.0, 10.0), rng.log_range(1e-4, 1.0)
+            if rng.next_u32() & 1:
+                r = rng.range(3.0, min(12.0, room / 2 - 1))
+                c = [rng.range(npml + r + 2, n - npml - r - 2) for n in dims]
+                spheres.append((c[0], c[1], c[2], r, eps, sig, None))
+            else:
+                b = []
+                for n in dims:
+                    side = rng.randint(4, min(17, room))
+                    a0 = rng.randint(npml + 2, n - npml - 2 - side + 1)
+                    b += [a0, a0 + side]
+                boxes.append((*b, eps, sig))
+        m = npml + 3
+
+        def pick():
+            return [rng.randint(m, n - m) for n in dims]
+
+        s = pick()
+        probes = [dict(zip("ijk", pick()), component=FIELD_EZ) for _ in range(4)]
+        out.append(Workload(
+            name=f"c4_scene{sc}", nx=nx, ny=ny, nz=nz, dx=1e-3, n_steps=n_steps, npml=npml, precision=precision,
+            sources=[dict(i=s[0], j=s[1], k=s[2], component=FIELD_EZ, mode=0, amplitude=1.0,
+                          waveform=WAVE_MOD_GAUSSIAN, p0=10e9, p1=4.0 * tau, p2=tau)],
+            probes=probes, freqs=freqs, boxes=boxes, spheres=spheres))
+    return out
+
+
+def scene_setup(w: Workload):
+    """The workload's boxes and spheres as a setup callback (None when it has
+    neither)."""
+    if not w.boxes and not w.spheres:
+        return None
+    from . import SceneSetup, dispersive
+
+    rows = [(cx, cy, cz, r, eps, sig, None if model is None else dispersive(*model))
+            for (cx, cy, cz, r, eps, sig, model) in w.spheres]
+    return SceneSetup(w.boxes, rows, w.smoothing)
+
+
 def scaled(w: Workload, n: int, n_steps: int) -> Workload:
     """The same scene recipe on an n^3 grid (spheres, probes and source scaled
     with the grid) for parity checks at oracle-friendly sizes."""
