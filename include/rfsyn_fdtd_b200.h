@@ -13,6 +13,8 @@
 #ifndef RFSYN_FDTD_B200_H
 #define RFSYN_FDTD_B200_H
 
+#include <stdint.h>
+
 #include "rfsyn_fdtd.h"
 
 #ifdef __cplusplus
@@ -198,6 +200,41 @@ typedef struct {
 } fdtd_b200_batch_info_t;
 
 int fdtd_b200_batch_info(const fdtd_b200_batch_t *batch, fdtd_b200_batch_info_t *info);
+
+/* ---- learned surrogate network -------------------------------------------------
+ * No counterpart in rfsyn.  A multilayer perceptron trained and evaluated on
+ * the GPU by this library's own kernels (BF16 tensor-core GEMMs with FP32
+ * accumulation, fused bias / GELU epilogues, FP32 Adam master weights): the
+ * network of the transfer-function surrogate (rfsyn_b200.surrogate), which
+ * maps a scene's parameter vector to its tx -> rx transfer function.
+ * Layers: n_in -> width (GELU), depth-1 times width -> width (GELU),
+ * width -> n_out.  width and n_out are multiples of 64; the input is padded
+ * with zeros to a multiple of 64.  Training batches are multiples of 64. */
+typedef struct fdtd_b200_mlp fdtd_b200_mlp_t;
+
+/* He-uniform initial weights from splitmix64(seed), zero biases. */
+fdtd_b200_mlp_t *fdtd_b200_mlp_create(int n_in, int width, int depth, int n_out, uint64_t seed);
+void fdtd_b200_mlp_destroy(fdtd_b200_mlp_t *mlp);
+/* Parameters in layer order: W (out x in, row-major; the first layer's in is
+ * the padded input width), then b. */
+size_t fdtd_b200_mlp_n_params(const fdtd_b200_mlp_t *mlp);
+int fdtd_b200_mlp_get_params(fdtd_b200_mlp_t *mlp, float *params);
+int fdtd_b200_mlp_set_params(fdtd_b200_mlp_t *mlp, const float *params);
+/* One forward + backward pass of a batch (X: batch x n_in, Y: batch x
+ * n_out): mean squared error and its gradient in parameter layout. */
+int fdtd_b200_mlp_grad(fdtd_b200_mlp_t *mlp, const float *X, const float *Y, int batch, double *loss,
+                       float *grads);
+/* Uploads the training set (kept on the device). */
+int fdtd_b200_mlp_set_data(fdtd_b200_mlp_t *mlp, const float *X, const float *Y, size_t n);
+/* `steps` Adam steps (betas, eps) of `batch` samples drawn through a
+ * permutation reshuffled every pass (splitmix64(shuffle_seed)), learning
+ * rate lr * 0.5 (1 + cos(pi s / steps)); each step replays one CUDA graph.
+ * final_loss: mean squared error of the last batch. */
+int fdtd_b200_mlp_train(fdtd_b200_mlp_t *mlp, size_t steps, int batch, double lr, double beta1, double beta2,
+                        double eps, uint64_t shuffle_seed, double *final_loss);
+/* Outputs of n inputs (n x n_out). */
+int fdtd_b200_mlp_predict(fdtd_b200_mlp_t *mlp, const float *X, size_t n, float *Y);
+unsigned long long fdtd_b200_mlp_launch_count(const fdtd_b200_mlp_t *mlp);
 
 /* ---- dispersive media (auxiliary differential equations) ----------------------
  * rfsyn models only static eps_r and sigma (engine/fdtd/materials.c:92-125);

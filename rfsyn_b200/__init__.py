@@ -224,6 +224,17 @@ def load() -> C.CDLL:
         "fdtd_b200_batch_read_probes": (I, [P, S, C.POINTER(D)]),
         "fdtd_b200_batch_dft": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_batch_info": (I, [P, C.POINTER(BatchInfo)]),
+        "fdtd_b200_mlp_create": (P, [I, I, I, I, C.c_uint64]),
+        "fdtd_b200_mlp_destroy": (V, [P]),
+        "fdtd_b200_mlp_n_params": (S, [P]),
+        "fdtd_b200_mlp_get_params": (I, [P, C.POINTER(C.c_float)]),
+        "fdtd_b200_mlp_set_params": (I, [P, C.POINTER(C.c_float)]),
+        "fdtd_b200_mlp_grad": (I, [P, C.POINTER(C.c_float), C.POINTER(C.c_float), I, C.POINTER(D),
+                                   C.POINTER(C.c_float)]),
+        "fdtd_b200_mlp_set_data": (I, [P, C.POINTER(C.c_float), C.POINTER(C.c_float), S]),
+        "fdtd_b200_mlp_train": (I, [P, S, I, D, D, D, D, C.c_uint64, C.POINTER(D)]),
+        "fdtd_b200_mlp_predict": (I, [P, C.POINTER(C.c_float), S, C.POINTER(C.c_float)]),
+        "fdtd_b200_mlp_launch_count": (C.c_ulonglong, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -479,6 +490,74 @@ class Batch:
     def close(self):
         if self.h:
             self.lib.fdtd_b200_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """The surrogate's network on the GPU (fdtd_b200_mlp_*)."""
+
+    def __init__(self, n_in: int, width: int, depth: int, n_out: int, seed: int = 0):
+        self.lib = load()
+        self.n_in, self.width, self.depth, self.n_out = n_in, width, depth, n_out
+        self.h = self.lib.fdtd_b200_mlp_create(n_in, width, depth, n_out, seed)
+        if not self.h:
+            raise RuntimeError(f"fdtd_b200_mlp_create failed: {last_error()}")
+
+    def _ok(self, rc):
+        if rc != 0:
+            raise RuntimeError(last_error())
+
+    @property
+    def n_params(self) -> int:
+        return self.lib.fdtd_b200_mlp_n_params(self.h)
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, dtype=np.float32)
+        self._ok(self.lib.fdtd_b200_mlp_get_params(self.h, _fptr(out)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._ok(self.lib.fdtd_b200_mlp_set_params(self.h, _fptr(p)))
+
+    def grad(self, X: np.ndarray, Y: np.ndarray) -> tuple[float, np.ndarray]:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double(0)
+        self._ok(self.lib.fdtd_b200_mlp_grad(self.h, _fptr(X), _fptr(Y), X.shape[0], C.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def set_data(self, X: np.ndarray, Y: np.ndarray):
+        self._X = np.ascontiguousarray(X, dtype=np.float32)
+        self._Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self._ok(self.lib.fdtd_b200_mlp_set_data(self.h, _fptr(self._X), _fptr(self._Y), self._X.shape[0]))
+
+    def train(self, steps: int, batch: int = 256, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,
+              eps: float = 1e-8, seed: int = 0) -> float:
+        loss = C.c_double(0)
+        self._ok(self.lib.fdtd_b200_mlp_train(self.h, steps, batch, lr, beta1, beta2, eps, seed, C.byref(loss)))
+        return loss.value
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((X.shape[0], self.n_out), dtype=np.float32)
+        self._ok(self.lib.fdtd_b200_mlp_predict(self.h, _fptr(X), X.shape[0], _fptr(Y)))
+        return Y
+
+    def close(self):
+        if self.h:
+            self.lib.fdtd_b200_mlp_destroy(self.h)
             self.h = None
 
     def __del__(self):
