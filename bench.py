@@ -463,6 +463,91 @@ def run_batch(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Surrogate (--workload c5)
+# ---------------------------------------------------------------------------
+def run_surrogate(args) -> None:
+    """Transfer-function surrogate: training data from the batched FDTD
+    (48^3 scenes at dx 2 mm, 0-8 spheres, 1 tx + 4 rx each, 1500 steps), a
+    5-member ensemble of 54 -> 512 x 4 (GELU) -> 512 MLPs trained on the GPU
+    (20k Adam steps, batch 256, lr 1e-3 cosine), held-out scenes answered by
+    the ensemble where its spread is <= 2 % of the norm and by the batched
+    FDTD otherwise.  Metric: held-out scenes/s of that path (wall clock, the
+    ensemble's inference plus the fallback FDTD runs), beside the plain
+    one-scene-at-a-time GPU FDTD and the transfer-function error."""
+    import torch
+
+    import rfsyn_b200 as rb
+    from rfsyn_b200 import scenes
+    from rfsyn_b200 import surrogate as sg
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    ws_tr = sg.c5_scenes(seed=51, n_scenes=args.train_scenes)
+    ws_te = sg.c5_scenes(seed=52, n_scenes=args.test_scenes)
+    tm = {}
+    t0 = time.perf_counter()
+    X_tr, H_tr = sg.transfer_functions(ws_tr, timings=tm)
+    gen_s = time.perf_counter() - t0
+    G_tr = sg.scene_transfer_targets(ws_tr, H_tr)
+    sur = sg.Surrogate(members=5, width=512, depth=4, seed=3)
+    t0 = time.perf_counter()
+    losses = sur.fit(X_tr, G_tr, steps=args.train_steps, batch=256, lr=1e-3)
+    train_s = time.perf_counter() - t0
+    # held-out truth from the batched FDTD (also its throughput)
+    tm_te = {}
+    t0 = time.perf_counter()
+    X_te, H_te = sg.transfer_functions(ws_te, timings=tm_te)
+    fdtd_batched_wall = time.perf_counter() - t0
+    fdtd_batched_scenes_s = len(ws_te) / (tm_te["fdtd_ms"] / 1e3)
+    pred = sur.predict(ws_te, X_te)
+    err_all = sg.rel_err(pred.H, H_te)
+    # the surrogate path with fallback, wall clock end to end
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = sg.infer_with_fallback(sur, ws_te, threshold=args.threshold)
+    path_s = time.perf_counter() - t0
+    err = sg.rel_err(res["H"], H_te)
+    fell = set(res["fallback"])
+    acc_rows = np.asarray([q not in fell for q in range(len(ws_te)) for _ in range(4)])
+    # plain one-scene-at-a-time GPU FDTD on a sample
+    plain_ms = 0.0
+    sample = ws_te[: args.plain_sample]
+    for w in sample:
+        st = scenes.scene_setup(w)
+        sim = rb.Sim(scenes.run_config(w), st.ptr if st else None, None)
+        sim.advance(w.n_steps)
+        sim.reset()
+        plain_ms += sim.advance_timed(w.n_steps)
+        sim.close()
+    plain_scenes_s = len(sample) / (plain_ms / 1e3)
+    value = len(ws_te) / path_s
+    line = {
+        "metric": "scenes/s (batched FDTD + surrogate, held-out)", "value": value, "unit": "scenes/s",
+        "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "bf16 GEMMs / fp32 FDTD", "data": "synthetic (seeded PCG32 scenes)",
+        "config": {"workload": "c5_surrogate_48cube_dx2mm", "train_scenes": len(ws_tr), "test_scenes": len(ws_te),
+                   "samples_per_scene": 4, "members": 5, "net": "54-512x4(GELU)-512", "train_steps": args.train_steps,
+                   "batch": 256, "lr": 1e-3, "threshold": args.threshold, "bins": sg.N_BINS},
+        "plain_one_at_a_time_scenes_s": plain_scenes_s, "speedup_vs_plain": value / plain_scenes_s,
+        "batched_fdtd_scenes_s": fdtd_batched_scenes_s,
+        "accepted_scene_frac": 1.0 - len(fell) / len(ws_te),
+        "transfer_rel_err": {"final_median": float(np.median(err)), "final_p95": float(np.percentile(err, 95)),
+                             "final_max": float(err.max()),
+                             "accepted_median": float(np.median(err[acc_rows])) if acc_rows.any() else None,
+                             "accepted_p95": float(np.percentile(err[acc_rows], 95)) if acc_rows.any() else None,
+                             "network_only_median": float(np.median(err_all)),
+                             "network_only_p95": float(np.percentile(err_all, 95))},
+        "timings_s": {"data_generation": gen_s, "data_generation_device": tm["fdtd_ms"] / 1e3, "training": train_s,
+                      "path_surrogate": res["surrogate_s"], "path_fallback_fdtd": res["fdtd_s"],
+                      "heldout_fdtd_wall": fdtd_batched_wall},
+        "final_train_losses": losses,
+    }
+    sur.close()
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -472,7 +557,11 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"])
+    ap.add_argument("--train-scenes", type=int, default=5000, help="c5: training scenes (4 samples each)")
+    ap.add_argument("--test-scenes", type=int, default=500, help="c5: held-out scenes")
+    ap.add_argument("--train-steps", type=int, default=20000, help="c5: Adam steps per member")
+    ap.add_argument("--threshold", type=float, default=0.02, help="c5: ensemble spread that triggers FDTD")
     ap.add_argument("--scenes", type=int, default=512, help="c4: scenes per batch")
     ap.add_argument("--plain-sample", type=int, default=16, help="c4: scenes timed one at a time")
     args = ap.parse_args()
@@ -482,6 +571,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "c4":
         run_batch(args)
+    elif args.workload == "c5":
+        run_surrogate(args)
     else:
         run_b200(args)
 

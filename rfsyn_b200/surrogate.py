@@ -6,12 +6,20 @@ the ensemble disagrees.  rfsyn has no learned component.
 Scene vector (54 values): 8 scatterers x (x, y, z, radius, eps_r, log10
 sigma), zero-padded, then the tx and rx positions, all scaled to O(1).
 Output (512 values): the de-embedded transfer function
-    G(f) = H(f) * d * exp(+j 2 pi f d / c)        (d = tx-rx distance)
+    G(f) = H(f) / Ez_free(f; d, theta)
 at 256 bins, real parts then imaginary parts, divided by one scale learned
 from the training set.  H(f) = P(f) / S(f): the receive probe's spectrum
 over the spectrum of the transmitted waveform, both with the engine's DFT
-convention.  De-embedding the free-space spreading and delay leaves a
-smooth function of frequency for the network.
+convention.  Ez_free is the z component of the free-space field of a
+z-directed elementary dipole at the receiver (distance d, polar angle
+theta from the dipole axis), near, intermediate and far terms:
+    E_r     = cos(theta) / (2 pi d^2) (1 + 1/(jkd)) e^{-jkd}
+    E_theta = j k sin(theta) / (4 pi d) (1 + 1/(jkd) - 1/(kd)^2) e^{-jkd}
+    Ez      = E_r cos(theta) - E_theta sin(theta)
+(constant factors dropped; the soft source is a current element whose
+moment is proportional to the injected value).  Dividing it out removes the
+spreading, delay and near-field structure of the direct path, so the
+network learns what the scatterers and the grid add to it.
 
 The network (forward, backward, Adam) runs on the GPU through
 fdtd_b200_mlp_* (rfsyn_b200/csrc/mlp.cu); every FDTD run goes through the
@@ -90,11 +98,24 @@ def source_spectrum(w: sc.Workload) -> np.ndarray:
     return (v[None, :] * np.exp(-2j * math.pi * f[:, None] * t[None, :])).sum(axis=1) * dt
 
 
-def _deembed(w: sc.Workload, rx: int) -> np.ndarray:
+def ez_free(w: sc.Workload, rx: int) -> np.ndarray:
+    """Ez of a z-directed elementary dipole at the transmitter, observed at
+    receiver rx, over the scene's bins (constant factors dropped)."""
     s, p = w.sources[0], w.probes[rx]
-    d = math.sqrt(sum((s[a] - p[a]) ** 2 for a in "ijk")) * w.dx
-    f = np.asarray(w.freqs)
-    return d * np.exp(2j * math.pi * f * d / C0)
+    v = np.asarray([(p[a] - s[a]) * w.dx for a in "ijk"], dtype=np.float64)
+    d = float(np.linalg.norm(v))
+    ct = v[2] / d
+    st = math.sqrt(max(0.0, 1.0 - ct * ct))
+    k = 2.0 * math.pi * np.asarray(w.freqs) / C0
+    kd = k * d
+    ph = np.exp(-1j * kd)
+    er = ct / (2.0 * math.pi * d * d) * (1.0 + 1.0 / (1j * kd)) * ph
+    eth = 1j * k * st / (4.0 * math.pi * d) * (1.0 + 1.0 / (1j * kd) - 1.0 / (kd * kd)) * ph
+    return er * ct - eth * st
+
+
+def _deembed(w: sc.Workload, rx: int) -> np.ndarray:
+    return 1.0 / ez_free(w, rx)
 
 
 def transfer_functions(ws: list[sc.Workload], chunk: int = 512, timings: dict | None = None):
