@@ -267,6 +267,30 @@ int fdtd_b200_materials_set_component_dispersive(materials_t *mat, const fdtd_gr
 int fdtd_b200_materials_clear_component_dispersive(materials_t *mat, const fdtd_grid_t *g,
                                                    field_component_t component, size_t i, size_t j, size_t k);
 
+/* ---- full 3x3 anisotropic permittivity -----------------------------------------
+ * rfsyn's tensor edges (materials_set_component_tensor, materials.c:658-903)
+ * are 2x2 (Ex, Ey; a z-invariant TM scope).  These samples carry a full row
+ * of the relative inverse permittivity m = eps_r^-1: component c of a cell
+ * is updated as
+ *   E_c += dt/(eps0 dx) (m_cc D_c + sum_{b != c} m_cb <D_b>),
+ * D_b = (curl H)_b dx at the b sample, <D_b> its mean over the four b
+ * samples surrounding the E_c sample (which keeps the coupling reciprocal
+ * for a symmetric m).  Lossless; for cells outside the CPML; on an axis
+ * without wrap the cell lies in [1, n-1].  A 3x3 sample takes precedence
+ * over every other description of the same component; box assignment clears
+ * them.  set_component_tensor3 takes the row (3 values, m_cc > 0);
+ * set_tensor3_box inverts a symmetric positive-definite eps_r (9 values,
+ * row-major) and sets all three components of every cell of the box. */
+int fdtd_b200_materials_set_component_tensor3(materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                              size_t i, size_t j, size_t k, const double row[3]);
+int fdtd_b200_materials_clear_component_tensor3(materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                                size_t i, size_t j, size_t k);
+int fdtd_b200_materials_set_tensor3_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0,
+                                        size_t j1, size_t k0, size_t k1, const double eps_r[9]);
+/* The row of a 3x3 sample: 0, or 1 when the component has none. */
+int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                    size_t i, size_t j, size_t k, double row[3]);
+
 /* ---- spheres with subpixel smoothing -------------------------------------------
  * Rasterises spheres (centre and radius in cell units: the E_x sample of cell
  * (i,j,k) sits at (i+1/2, j, k), E_y at (i, j+1/2, k), E_z at (i, j, k+1/2))

@@ -78,6 +78,11 @@ def disp_entry(comp, i, j, k, eps_inf, sigma, poles):
     return (comp, i, j, k, eps_inf, sigma, len(poles), tuple(kind), tuple(de), tuple(tau), tuple(wp), tuple(gm))
 
 
+class ScnTensor3(C.Structure):
+    _fields_ = [("comp", C.c_int), ("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t),
+                ("m", C.c_double * 3)]
+
+
 class ScnScene(C.Structure):
     _fields_ = [
         ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t), ("dx", C.c_double), ("courant", C.c_double),
@@ -94,6 +99,7 @@ class ScnScene(C.Structure):
         ("n_probes", C.c_size_t), ("probes", C.POINTER(ScnProbe)),
         ("n_freqs", C.c_size_t), ("freqs", C.POINTER(C.c_double)),
         ("src_t_offset", C.c_double), ("dft_t_offset", C.c_double),
+        ("n_tensor3", C.c_size_t), ("tensor3", C.POINTER(ScnTensor3)),
     ]
 
 
@@ -125,6 +131,7 @@ class Scene:
     freqs: list = field(default_factory=list)
     src_t_offset: float = 0.0
     dft_t_offset: float = 1.0
+    tensor3: list = field(default_factory=list)    # (comp,i,j,k,(m0,m1,m2)) rows of eps_r^-1, applied last
 
     @property
     def dt(self) -> float:
@@ -153,6 +160,8 @@ class Scene:
                           (C.c_double * 2)(*tau), (C.c_double * 2)(*wp), (C.c_double * 2)(*gm)))
         s.n_disp, s.disp = arr(ScnDisp, drows)
         s.n_spheres, s.spheres = arr(ScnSphere, self.spheres)
+        s.n_tensor3, s.tensor3 = arr(ScnTensor3, [(c, i, j, k, (C.c_double * 3)(*m))
+                                                  for (c, i, j, k, m) in self.tensor3])
         s.n_sources, s.sources = arr(ScnSource, self.sources)
         s.n_probes, s.probes = arr(ScnProbe, self.probes)
         f = (C.c_double * max(len(self.freqs), 1))(*self.freqs)

@@ -24,6 +24,9 @@
  *                                  and Lorentz polarisation currents)
  *   sphere fill fractions and the diagonal of the smoothed inverse
  *   permittivity (Farjadpour et al., Opt. Lett. 31, 2972 (2006))
+ *   full 3x3 anisotropic samples: the 2x2 tensor edge generalised to a
+ *                                  full row of eps_r^-1, off-diagonal curls
+ *                                  averaged over the four surrounding samples
  * The data structures are the plainest possible (dense per-component override
  * and tensor planes, full-grid psi) so the restatement is easy to audit.
  */
@@ -63,6 +66,9 @@ typedef struct {
     size_t nd, dcap;
     double *drec;   /* 16 per sample */
     double *dst;    /* 5 per sample: J0 J1 J0- J1- E- */
+    /* full 3x3 samples: per component a flag and the row of eps_r^-1 */
+    uint8_t *has_t3[3];
+    double *t3m[3];
 } orc_t;
 
 static int periodic(const orc_t *o, int a) { return (o->per >> a) & 1u; }
@@ -115,7 +121,7 @@ static void orc_free(orc_t *o) {
         free(o->has_ovr[c]); free(o->oca[c]); free(o->ocb[c]);
     }
     for (int c = 0; c < 2; c++) { free(o->has_t[c]); free(o->tm11[c]); free(o->tm12[c]); free(o->tm22[c]); free(o->tscale[c]); }
-    for (int c = 0; c < 3; c++) free(o->dix[c]);
+    for (int c = 0; c < 3; c++) free(o->dix[c]), free(o->has_t3[c]), free(o->t3m[c]);
     free(o->drec);
     free(o->dst);
     free(o->id);
@@ -266,6 +272,11 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
     o->id = calloc(o->total, 1);
     if (!o->id) return -1;
     for (int c = 0; c < 3; c++) {
+        o->has_t3[c] = calloc(o->total, 1);
+        o->t3m[c] = calloc(3 * o->total, 8);
+        if (!o->has_t3[c] || !o->t3m[c]) return -1;
+    }
+    for (int c = 0; c < 3; c++) {
         o->dix[c] = malloc(o->total * sizeof(int));
         if (!o->dix[c]) return -1;
         for (size_t q = 0; q < o->total; q++) o->dix[c][q] = -1;
@@ -329,6 +340,12 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
             if (s->spheres[q].disp < 0 && table_id(o, s->spheres[q].eps_r, s->spheres[q].sigma) < 0) return -1;
         sr_target_t tg = {o, sr_bg, sr_fill, sr_fill_disp, sr_sample, sr_sample_disp};
         if (sr_rasterise(s, o->n, o->per, sr_canon, o, &tg) != 0) return -1;
+    }
+    for (size_t q = 0; q < s->n_tensor3; q++) {
+        const scn_tensor3_t *t = &s->tensor3[q];
+        size_t w = at(o, t->i, t->j, t->k);
+        o->has_t3[t->comp][w] = 1;
+        memcpy(o->t3m[t->comp] + 3 * w, t->m, 3 * sizeof(double));
     }
     return 0;
 }
@@ -411,6 +428,40 @@ static void tensor_edge(orc_t *o, int c, size_t i, size_t j, size_t k) {
     }
 }
 
+/* Curl difference of E component b at cell (i, j, k): the unstretched
+ * (dA - dB) of the E update below. */
+static double curl_d(const orc_t *o, int b, size_t i, size_t j, size_t k) {
+    const int fa = (b + 2) % 3, axa = (b + 1) % 3, fb = (b + 1) % 3, axb = (b + 2) % 3;
+    size_t pa[3] = {i, j, k}, pb[3] = {i, j, k};
+    pa[axa] = back(pa[axa], o->n[axa]);
+    pb[axb] = back(pb[axb], o->n[axb]);
+    double tA = o->H[fa][at(o, i, j, k)] - o->H[fa][at(o, pa[0], pa[1], pa[2])];
+    double tB = o->H[fb][at(o, i, j, k)] - o->H[fb][at(o, pb[0], pb[1], pb[2])];
+    return tA - tB;
+}
+
+/* Full 3x3 sample: value = m_cc D_c, then for each b != c (ascending)
+ * value += m_cb (0.25 (((D_b(w) + D_b(w+e_c)) + D_b(w-e_b)) + D_b(w+e_c-e_b)));
+ * E_c += dt/(eps0 dx) value. */
+static void tensor3(orc_t *o, int c, size_t i, size_t j, size_t k) {
+    size_t w = at(o, i, j, k);
+    const double *r = o->t3m[c] + 3 * w;
+    double value = r[c] * curl_d(o, c, i, j, k);
+    for (int b = 0; b < 3; b++) {
+        if (b == c) continue;
+        size_t p0[3] = {i, j, k}, p1[3] = {i, j, k};
+        p1[c] += 1;
+        size_t p2[3] = {p0[0], p0[1], p0[2]}, p3[3] = {p1[0], p1[1], p1[2]};
+        p2[b] = back(p2[b], o->n[b]);
+        p3[b] = back(p3[b], o->n[b]);
+        double s4 = ((curl_d(o, b, p0[0], p0[1], p0[2]) + curl_d(o, b, p1[0], p1[1], p1[2])) +
+                     curl_d(o, b, p2[0], p2[1], p2[2])) +
+                    curl_d(o, b, p3[0], p3[1], p3[2]);
+        value = value + r[b] * (0.25 * s4);
+    }
+    o->E[c][w] = o->E[c][w] + (o->dt / (O_EPS0 * o->dx)) * value;
+}
+
 /* E update (materials.c:911-1060).  Component c: E_c = Ca E_c + Cb (dA - dB)
  * with A = d H_{c+2} / d x_{c+1}, B = d H_{c+1} / d x_{c+2} (backward);
  * index 0 of an axis other than c is swept only when that axis is periodic. */
@@ -424,6 +475,10 @@ static void update_e(orc_t *o) {
             for (size_t j = lo[1]; j < o->n[1]; j++)
                 for (size_t k = lo[2]; k < o->n[2]; k++) {
                     size_t here = at(o, i, j, k);
+                    if (o->has_t3[c][here]) {
+                        tensor3(o, c, i, j, k);
+                        continue;
+                    }
                     if (c < 2 && o->has_t[c][here]) {
                         tensor_edge(o, c, i, j, k);
                         continue;

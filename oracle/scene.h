@@ -24,6 +24,9 @@
 typedef struct { size_t i0, i1, j0, j1, k0, k1; double eps_r, sigma; } scn_box_t;
 typedef struct { int comp; size_t i, j, k; double eps_r, sigma; } scn_comp_t;
 typedef struct { int comp; size_t i, j, k; double m11, m12, m22; } scn_tensor_t;
+/* full 3x3 sample (no rfsyn counterpart): row `comp` of the relative
+ * inverse permittivity */
+typedef struct { int comp; size_t i, j, k; double m[3]; } scn_tensor3_t;
 /* waveform: 0 Gaussian derivative (p0 t0, p1 tau), 1 Ricker (p0 f0, p1 t0),
  *           2 modulated Gaussian (p0 f, p1 t0, p2 tau).  mode 0 soft, 1 hard. */
 typedef struct { size_t i, j, k; int comp, mode; double amplitude; int waveform; double p0, p1, p2; } scn_source_t;
@@ -61,6 +64,7 @@ typedef struct {
     size_t n_probes;  const scn_probe_t *probes;
     size_t n_freqs;   const double *freqs;
     double src_t_offset, dft_t_offset;
+    size_t n_tensor3; const scn_tensor3_t *tensor3; /* applied last */
 } scn_scene_t;
 
 #endif

@@ -201,7 +201,13 @@ int scn_setup(const fdtd_grid_t *g, materials_t *m, void *ctx) {
         free(md);
         if (rc != 0) return -1;
     }
+    for (size_t q = 0; q < s->n_tensor3; q++) {
+        const scn_tensor3_t *t = &s->tensor3[q];
+        if (fdtd_b200_materials_set_component_tensor3(m, g, comp_of(t->comp), t->i, t->j, t->k, t->m) != 0) return -1;
+    }
 #else
+    /* rfsyn has no 3x3 samples */
+    if (s->n_tensor3) return -1;
     /* rfsyn has no dispersive media: dispersive samples enter rfsyn at their
      * static permittivity eps_inf + sum delta_eps */
     for (size_t q = 0; q < s->n_disp; q++) {

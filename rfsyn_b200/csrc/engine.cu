@@ -216,6 +216,7 @@ struct DevScene {
     size_t ade_s_bytes = 0;
     void *t_m11 = nullptr, *t_scale = nullptr, *t_w = nullptr;
     int *t_main = nullptr, *t_nq = nullptr, *t_uv = nullptr, *t_sign = nullptr;
+    void *t3 = nullptr;
     int n_skip = 0;
     long long skip[MAX_SKIP] = {};
     double *cb64_tab = nullptr, *cb64_list = nullptr;  // FP64 Cb for the energy audit
@@ -227,7 +228,7 @@ static void devscene_free(DevScene &s) {
     cudaFree(s.l_tix); cudaFree(s.l_src); cudaFree(s.l_aix); cudaFree(s.ade_c); cudaFree(s.ade_s);
     cudaFree(s.t_m11); cudaFree(s.t_scale); cudaFree(s.t_w);
     cudaFree(s.t_main); cudaFree(s.t_nq); cudaFree(s.t_uv); cudaFree(s.t_sign);
-    cudaFree(s.cb64_tab); cudaFree(s.cb64_list);
+    cudaFree(s.cb64_tab); cudaFree(s.cb64_list); cudaFree(s.t3);
     s = DevScene();
 }
 
@@ -306,6 +307,13 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
                 return -1;
             }
         }
+        if (img->n_t3) {
+            s.t3 = dev_upload_conv(img->t3, 4 * img->n_t3, prec);
+            if (!s.t3) {
+                rfb_set_error("3x3 tensor upload failed");
+                return -1;
+            }
+        }
         if (img->n_ade) {
             s.ade_c = dev_upload_conv(img->ade_c, img->n_ade * RFB_ADE_NC, prec);
             s.ade_s_bytes = ne * 5 * (prec == RFB_FP64 ? 8 : 4);
@@ -357,6 +365,7 @@ static void fill_scene_args(Args<T> &a, const DevScene &s) {
     a.t_nq = s.t_nq;
     a.t_uv = s.t_uv;
     a.t_sign = s.t_sign;
+    a.t3 = (const T *)s.t3;
 }
 
 template <typename T>

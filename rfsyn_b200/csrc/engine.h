@@ -46,7 +46,8 @@ enum {
     RFB_LK_COPY   = 0,  /* component not updated (PEC or padded): keep value */
     RFB_LK_SCALAR = 1,  /* E = Ca E + Cb (dA - dB) with CPML where present    */
     RFB_LK_TENSOR = 2,  /* rfsyn 2x2 tensor edge (materials.c:847-903)        */
-    RFB_LK_ADE    = 3   /* dispersive (Debye / Lorentz) cell                  */
+    RFB_LK_ADE    = 3,  /* dispersive (Debye / Lorentz) cell                  */
+    RFB_LK_TENSOR3 = 4  /* full 3x3 anisotropic sample (no rfsyn counterpart) */
 };
 
 /* Scene image produced by the host materials description and consumed by the
@@ -78,6 +79,14 @@ typedef struct {
     const double *t_w;          /* 4 per record                               */
     const int32_t *t_uv;        /* 16 per record: ua, va, ub, vb per coupling  */
     const int32_t *t_sign;      /* per record: +1 or -1 applied to couplings   */
+
+    /* 3x3 records: row c of the relative inverse permittivity of the
+     * sample's component c, then dt / (eps0 dx).  The update is
+     *   E_c += s (m_cc D_c + sum_{b != c} m_cb <D_b>)
+     * with D_b the curl difference of component b at its own sample and
+     * <D_b> its mean over the four b samples around the E_c sample. */
+    size_t n_t3;
+    const double *t3;           /* 4 per record                                */
 
     /* ADE records (dispersive cells), see rfb_ade_desc in the engine. */
     size_t n_ade;

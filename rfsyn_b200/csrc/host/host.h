@@ -49,6 +49,7 @@ typedef struct {
     double *t_m11, *t_scale, *t_w;
     int32_t *t_main, *t_nq, *t_uv, *t_sign;
     double *ade_c;
+    double *t3;             /* 3x3 samples: 4 doubles per record */
 } rfb_scene_build_t;
 
 void rfb_ade_record(const double *model, double dt, double dx, double *out);
@@ -66,6 +67,9 @@ void rfb_scene_build_free(rfb_scene_build_t *b);
 rfb_scene_dev_t *materials_device(const materials_t *mat, const fdtd_grid_t *g);
 int materials_matches(const materials_t *mat, const fdtd_grid_t *g);
 
+/* Inverse of a symmetric positive-definite 3x3 matrix (row-major); -1 when
+ * the matrix is not symmetric positive definite. */
+int rfb_spd3_inverse(const double e[9], double out[9]);
 int rfb_default_precision(void);
 int rfb_default_schedule(void);
 

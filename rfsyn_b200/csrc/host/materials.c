@@ -149,6 +149,7 @@ struct materials {
     omap_t scalar;  /* key -> (Ca, Cb) */
     omap_t tensor;  /* key -> (m11, m12, m22, scale) */
     omap_t disp;    /* key -> dispersive model (DISP_W doubles) */
+    omap_t tensor3; /* key -> row of the 3x3 relative inverse permittivity (3 doubles) */
     unsigned long version;
     /* device copy for the step-wise API */
     rfb_scene_dev_t *dev;
@@ -216,6 +217,7 @@ materials_t *materials_create(const fdtd_grid_t *g) {
     omap_init(&mat->scalar, 2);
     omap_init(&mat->tensor, 4);
     omap_init(&mat->disp, DISP_W);
+    omap_init(&mat->tensor3, 3);
     mat->ids = calloc(total, 1);
     if (!mat->ids) {
         materials_destroy(mat);
@@ -235,6 +237,7 @@ void materials_destroy(materials_t *mat) {
     omap_free(&mat->scalar);
     omap_free(&mat->tensor);
     omap_free(&mat->disp);
+    omap_free(&mat->tensor3);
     rfb_scene_dev_destroy(mat->dev);
     free(mat);
 }
@@ -312,6 +315,7 @@ int materials_assign_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size
     clear_box_overrides(mat, &mat->scalar, i0, i1, j0, j1, k0, k1);
     clear_box_overrides(mat, &mat->tensor, i0, i1, j0, j1, k0, k1);
     clear_box_overrides(mat, &mat->disp, i0, i1, j0, j1, k0, k1);
+    clear_box_overrides(mat, &mat->tensor3, i0, i1, j0, j1, k0, k1);
     mat->version++;
     return 0;
 }
@@ -463,6 +467,93 @@ int fdtd_b200_materials_clear_component_dispersive(materials_t *mat, const fdtd_
     int c = component_number(component);
     if (!materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
     omap_del(&mat->disp, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
+    mat->version++;
+    return 0;
+}
+
+/* ---- full 3x3 anisotropic samples ---------------------------------------------
+ * No counterpart in rfsyn, whose tensor edges are 2x2 (materials.c:658-903).
+ * A sample of component c holds row c of the relative inverse permittivity
+ * m = eps_r^-1 (3x3).  Its update needs the H samples of the neighbouring
+ * cells one step away on every axis: on an axis without wrap the cell must
+ * lie in [1, n-1].  Like rfsyn's tensor edges the samples are lossless and
+ * meant for cells outside the CPML. */
+static int tensor3_margin_ok(const fdtd_grid_t *g, size_t i, size_t j, size_t k) {
+    const size_t n[3] = {g->nx, g->ny, g->nz}, p[3] = {i, j, k};
+    for (int a = 0; a < 3; a++)
+        if (!(g->periodic_axes & (1u << a)) && (p[a] < 1 || p[a] + 1 > n[a])) return 0;
+    return 1;
+}
+
+int fdtd_b200_materials_set_component_tensor3(materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                              size_t i, size_t j, size_t k, const double row[3]) {
+    int c = component_number(component);
+    if (c < 0 || c > 2 || !row || !materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    if (!tensor3_margin_ok(g, i, j, k)) return -1;
+    for (int q = 0; q < 3; q++)
+        if (!isfinite(row[q])) return -1;
+    if (!(row[c] > 0.0)) return -1;
+    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, row) != 0) return -1;
+    mat->version++;
+    return 0;
+}
+
+int fdtd_b200_materials_clear_component_tensor3(materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                                size_t i, size_t j, size_t k) {
+    int c = component_number(component);
+    if (c < 0 || c > 2 || !materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    omap_del(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
+    mat->version++;
+    return 0;
+}
+
+int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g, field_component_t component,
+                                     size_t i, size_t j, size_t k, double row[3]) {
+    int c = component_number(component);
+    if (c < 0 || c > 2 || !row || !materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
+    long long q = omap_find(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
+    if (q < 0) return 1;
+    memcpy(row, mat->tensor3.vals + (size_t)q * 3, 3 * sizeof(double));
+    return 0;
+}
+
+/* Inverse of a symmetric positive-definite 3x3 matrix (row-major), by the
+ * adjugate; -1 when the matrix is not symmetric or not positive definite
+ * (leading principal minors). */
+int rfb_spd3_inverse(const double e[9], double out[9]) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            if (!isfinite(e[3 * a + b]) || fabs(e[3 * a + b] - e[3 * b + a]) > 1e-12 * (fabs(e[3 * a + b]) + 1.0))
+                return -1;
+    const double m1 = e[0], m2 = e[0] * e[4] - e[1] * e[3];
+    const double det = e[0] * (e[4] * e[8] - e[5] * e[7]) - e[1] * (e[3] * e[8] - e[5] * e[6]) +
+                       e[2] * (e[3] * e[7] - e[4] * e[6]);
+    if (!(m1 > 0.0 && m2 > 0.0 && det > 0.0)) return -1;
+    out[0] = (e[4] * e[8] - e[5] * e[7]) / det;
+    out[1] = (e[2] * e[7] - e[1] * e[8]) / det;
+    out[2] = (e[1] * e[5] - e[2] * e[4]) / det;
+    out[3] = out[1];
+    out[4] = (e[0] * e[8] - e[2] * e[6]) / det;
+    out[5] = (e[2] * e[3] - e[0] * e[5]) / det;
+    out[6] = out[2];
+    out[7] = out[5];
+    out[8] = (e[0] * e[4] - e[1] * e[3]) / det;
+    return 0;
+}
+
+int fdtd_b200_materials_set_tensor3_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0,
+                                        size_t j1, size_t k0, size_t k1, const double eps_r[9]) {
+    double m[9];
+    if (!eps_r || rfb_spd3_inverse(eps_r, m) != 0) return -1;
+    if (!box_valid(mat, g, i0, i1, j0, j1, k0, k1)) return -1;
+    for (size_t i = i0; i < i1; i++)
+        for (size_t j = j0; j < j1; j++)
+            for (size_t k = k0; k < k1; k++)
+                for (int c = 0; c < 3; c++) {
+                    if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) return -1;
+                    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, m + 3 * c) != 0)
+                        return -1;
+                }
     mat->version++;
     return 0;
 }
@@ -655,6 +746,7 @@ void rfb_scene_build_free(rfb_scene_build_t *b) {
     free(b->tix); free(b->src); free(b->aix);
     free(b->t_m11); free(b->t_scale); free(b->t_w); free(b->t_main); free(b->t_nq); free(b->t_uv); free(b->t_sign);
     free(b->ade_c);
+    free(b->t3);
     memset(b, 0, sizeof(*b));
 }
 
@@ -667,7 +759,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     }
     const size_t nz1 = g->nz + 1;
     /* 1. cells on the interface list (padded linear index) */
-    size_t cap = mat->scalar.count + mat->tensor.count + mat->disp.count + n_extra;
+    size_t cap = mat->scalar.count + mat->tensor.count + mat->disp.count + mat->tensor3.count + n_extra;
     int id255 = 0;
     if (mat->table_count == MATERIAL_LIMIT) {
         /* code 255 marks list cells: cells of material 255 go to the list too */
@@ -683,6 +775,8 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         if (mat->tensor.keys[q] != OMAP_EMPTY) cells[nc++] = mat->tensor.keys[q] / 3;
     for (size_t q = 0; q < mat->disp.cap; q++)
         if (mat->disp.keys[q] != OMAP_EMPTY) cells[nc++] = mat->disp.keys[q] / 3;
+    for (size_t q = 0; q < mat->tensor3.cap; q++)
+        if (mat->tensor3.keys[q] != OMAP_EMPTY) cells[nc++] = mat->tensor3.keys[q] / 3;
     for (size_t q = 0; q < n_extra; q++)
         cells[nc++] = ((uint64_t)extra[q].i * (g->ny + 1) + (uint64_t)extra[q].j) * nz1 + (uint64_t)extra[q].k;
     if (id255)
@@ -729,10 +823,11 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     out->t_nq = calloc(tcap, sizeof(int32_t));
     out->t_uv = calloc(16 * tcap, sizeof(int32_t));
     out->t_sign = calloc(tcap, sizeof(int32_t));
+    out->t3 = malloc((4 * mat->tensor3.count + 4) * sizeof(double));
     if (!out->cell_ijk || !out->kind || !out->ca || !out->cb || !out->tix || !out->src || !out->aix || !out->t_m11 ||
-        !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign)
+        !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign || !out->t3)
         goto oom;
-    size_t nt = 0;
+    size_t nt = 0, nt3 = 0;
     /* ADE records, deduplicated by model */
     size_t n_models = 0, model_cap = 16;
     double *models = malloc(model_cap * DISP_W * sizeof(double));
@@ -758,6 +853,19 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
             out->cb[e] = co.Cb;
             if (!e_swept(g, c, i, j, k)) {
                 out->kind[e] = RFB_LK_COPY;
+                continue;
+            }
+            long long t3 = omap_find(&mat->tensor3, (uint64_t)idx * 3 + (uint64_t)c);
+            if (t3 >= 0) {
+                /* full 3x3 sample: its row of eps_r^-1 and dt / (eps0 dx) */
+                const double *row = mat->tensor3.vals + (size_t)t3 * 3;
+                double *rec = out->t3 + 4 * nt3;
+                rec[0] = row[0];
+                rec[1] = row[1];
+                rec[2] = row[2];
+                rec[3] = mat->dt / (EPS0 * mat->dx);
+                out->kind[e] = RFB_LK_TENSOR3;
+                out->tix[e] = (int32_t)nt3++;
                 continue;
             }
             const double *t = (c < 2) ? tensor_at(mat, idx, c) : NULL;
@@ -860,6 +968,8 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     img->src = out->src;
     img->aix = out->aix;
     img->n_tensors = nt;
+    img->n_t3 = nt3;
+    img->t3 = out->t3;
     img->t_m11 = out->t_m11;
     img->t_scale = out->t_scale;
     img->t_main = out->t_main;

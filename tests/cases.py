@@ -105,6 +105,6 @@ def run_device(s: Scene, precision: int, schedule: int) -> dict:
 
     rc = scene_run_config(s, precision, schedule)
     cs = s.to_c()
-    needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres)
+    needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres or s.tensor3)
     setup = oracle.device_setup() if needs_setup else None
     return rb.run(rc, setup, C.cast(C.pointer(cs), C.c_void_p) if needs_setup else None)

@@ -32,7 +32,7 @@ ENERGY_SCENES = {
 def _sim(s, precision, schedule):
     rc = scene_run_config(s, precision, schedule)
     cs = s.to_c()
-    needs = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres)
+    needs = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres or s.tensor3)
     sim = rb.Sim(rc, oracle.device_setup() if needs else None, C.cast(C.pointer(cs), C.c_void_p) if needs else None)
     sim._keep = cs
     return sim

@@ -68,7 +68,7 @@ def _run(s: Scene, precision: int, variant, monkeypatch, need_interior=True):
     monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma}")
     rc = scene_run_config(s, precision, rb.FUSED)
     cs = s.to_c()
-    needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres)
+    needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres or s.tensor3)
     sim = rb.Sim(rc, oracle.device_setup() if needs_setup else None,
                  C.cast(C.pointer(cs), C.c_void_p) if needs_setup else None)
     try:
