@@ -49,6 +49,30 @@ typedef struct {
     field_component_t component;   /* FIELD_EX..FIELD_HZ */
 } fdtd_b200_probe_t;
 
+/* A plane wave injected by a total-field / scattered-field boundary (no
+ * counterpart in rfsyn, whose validators drive soft sheets or modal lines,
+ * engine/fdtd/validation_common.h:16-18).  Direction k = (sin t cos p,
+ * sin t sin p, cos t) for theta t, phi p (radians); E along
+ * cos(psi) theta_hat + sin(psi) phi_hat; E(t) = amplitude * waveform at the
+ * box corner the wave reaches first (waveform and p0..p2 as for sources,
+ * samples not allowed).  The total field fills the box of sample positions
+ * [i0, i1] x [j0, j1] x [k0, k1] (cell units; the whole axis on a periodic
+ * axis); the box grown by two cells must lie outside the CPML and inside
+ * the grid, in scalar media.  The incident field comes from a 1-D FDTD line
+ * along k with the grid's dx and dt, interpolated linearly at each sample's
+ * projected distance (Taflove & Hagness, Computational Electrodynamics 3rd
+ * ed., ch. 5); at normal incidence the injection is exact, at oblique
+ * incidence the scattered region carries the 1-D / 3-D dispersion mismatch.
+ * On a periodic axis a non-normal wave is not periodic: use normal
+ * incidence there. */
+typedef struct {
+    double theta, phi, psi;
+    double amplitude;
+    int waveform;                  /* fdtd_b200_waveform_t, not SAMPLES */
+    double p0, p1, p2;
+    size_t i0, i1, j0, j1, k0, k1;
+} fdtd_b200_plane_wave_t;
+
 typedef struct {
     size_t nx, ny, nz;
     double dx;
@@ -70,6 +94,9 @@ typedef struct {
     size_t n_freqs;
     const double *freqs_hz;
     double dft_time_offset_steps;
+    /* NULL, or a plane wave injected through a TF/SF boundary (sessions and
+     * fdtd_b200_run; not in batches) */
+    const fdtd_b200_plane_wave_t *plane_wave;
 } fdtd_b200_config_t;
 
 /* Defaults: courant 0.99, cpml = cpml_default_params(npml), FP64, FUSED,

@@ -83,6 +83,13 @@ class ScnTensor3(C.Structure):
                 ("m", C.c_double * 3)]
 
 
+class ScnPlaneWave(C.Structure):
+    _fields_ = [("theta", C.c_double), ("phi", C.c_double), ("psi", C.c_double), ("amplitude", C.c_double),
+                ("waveform", C.c_int), ("p0", C.c_double), ("p1", C.c_double), ("p2", C.c_double),
+                ("i0", C.c_size_t), ("i1", C.c_size_t), ("j0", C.c_size_t), ("j1", C.c_size_t),
+                ("k0", C.c_size_t), ("k1", C.c_size_t)]
+
+
 class ScnScene(C.Structure):
     _fields_ = [
         ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t), ("dx", C.c_double), ("courant", C.c_double),
@@ -100,6 +107,7 @@ class ScnScene(C.Structure):
         ("n_freqs", C.c_size_t), ("freqs", C.POINTER(C.c_double)),
         ("src_t_offset", C.c_double), ("dft_t_offset", C.c_double),
         ("n_tensor3", C.c_size_t), ("tensor3", C.POINTER(ScnTensor3)),
+        ("plane_wave", C.POINTER(ScnPlaneWave)),
     ]
 
 
@@ -132,6 +140,7 @@ class Scene:
     src_t_offset: float = 0.0
     dft_t_offset: float = 1.0
     tensor3: list = field(default_factory=list)    # (comp,i,j,k,(m0,m1,m2)) rows of eps_r^-1, applied last
+    plane_wave: dict | None = None                  # ScnPlaneWave fields by name
 
     @property
     def dt(self) -> float:
@@ -162,6 +171,12 @@ class Scene:
         s.n_spheres, s.spheres = arr(ScnSphere, self.spheres)
         s.n_tensor3, s.tensor3 = arr(ScnTensor3, [(c, i, j, k, (C.c_double * 3)(*m))
                                                   for (c, i, j, k, m) in self.tensor3])
+        if self.plane_wave is not None:
+            pw = ScnPlaneWave()
+            for name, _ in ScnPlaneWave._fields_:
+                setattr(pw, name, self.plane_wave.get(name, 0))
+            keep.append(pw)
+            s.plane_wave = C.pointer(pw)
         s.n_sources, s.sources = arr(ScnSource, self.sources)
         s.n_probes, s.probes = arr(ScnProbe, self.probes)
         f = (C.c_double * max(len(self.freqs), 1))(*self.freqs)

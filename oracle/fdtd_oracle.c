@@ -27,6 +27,10 @@
  *   full 3x3 anisotropic samples: the 2x2 tensor edge generalised to a
  *                                  full row of eps_r^-1, off-diagonal curls
  *                                  averaged over the four surrounding samples
+ *   plane wave, TF/SF boundary ... Taflove & Hagness 3rd ed. ch. 5: a 1-D
+ *                                  incident line, corrections generated from
+ *                                  the update stencils (the product's term
+ *                                  order, restated)
  * The data structures are the plainest possible (dense per-component override
  * and tensor planes, full-grid psi) so the restatement is easy to audit.
  */
@@ -69,6 +73,17 @@ typedef struct {
     /* full 3x3 samples: per component a flag and the row of eps_r^-1 */
     uint8_t *has_t3[3];
     double *t3m[3];
+    /* plane wave: the 1-D line, H targets, per-sample E term ranges, terms */
+    int tf;
+    size_t tf_len;
+    double tf_ce, tf_ch, *tf_e, *tf_h, *tf_src;
+    size_t tf_nh, tf_hcap;
+    size_t *tf_hw;      /* canonical index of each H target */
+    int *tf_hc, *tf_hfirst, *tf_hcount;
+    int *tf_efirst[3], *tf_ecount[3];
+    size_t tf_nt, tf_tcap;
+    double *tf_coef, *tf_w0, *tf_w1;
+    int *tf_idx;
 } orc_t;
 
 static int periodic(const orc_t *o, int a) { return (o->per >> a) & 1u; }
@@ -122,6 +137,9 @@ static void orc_free(orc_t *o) {
     }
     for (int c = 0; c < 2; c++) { free(o->has_t[c]); free(o->tm11[c]); free(o->tm12[c]); free(o->tm22[c]); free(o->tscale[c]); }
     for (int c = 0; c < 3; c++) free(o->dix[c]), free(o->has_t3[c]), free(o->t3m[c]);
+    for (int c = 0; c < 3; c++) free(o->tf_efirst[c]), free(o->tf_ecount[c]);
+    free(o->tf_e); free(o->tf_h); free(o->tf_src); free(o->tf_hw); free(o->tf_hc); free(o->tf_hfirst);
+    free(o->tf_hcount); free(o->tf_coef); free(o->tf_w0); free(o->tf_w1); free(o->tf_idx);
     free(o->drec);
     free(o->dst);
     free(o->id);
@@ -248,6 +266,204 @@ static int table_id(orc_t *o, double eps_r, double sigma) {
     return (int)o->ntab++;
 }
 
+/* ---- plane wave (TF/SF) ---------------------------------------------------- */
+static double wave(const scn_source_t *s, double t);
+
+static void tf_pos(int comp, const long p[3], double out[3]) {
+    for (int a = 0; a < 3; a++) out[a] = (double)p[a];
+    if (comp < 3) out[comp] += 0.5;
+    else
+        for (int a = 0; a < 3; a++)
+            if (a != comp - 3) out[a] += 0.5;
+}
+
+typedef struct {
+    double lo[3], hi[3], k[3], e[3], h[3], ref[3];
+    unsigned per;
+} tf_t;
+
+static int tf_in(const tf_t *t, const double p[3]) {
+    for (int a = 0; a < 3; a++)
+        if (!(t->per & (1u << a)) && (p[a] < t->lo[a] || p[a] > t->hi[a])) return 0;
+    return 1;
+}
+
+static double tf_s(const tf_t *t, const double p[3]) {
+    double s = 0.0;
+    for (int a = 0; a < 3; a++) s += t->k[a] * (p[a] - t->ref[a]);
+    return s + 4.0;
+}
+
+static int tf_term(orc_t *o, double coef, double s) {
+    if (o->tf_nt == o->tf_tcap) {
+        o->tf_tcap = o->tf_tcap ? 2 * o->tf_tcap : 256;
+        o->tf_coef = realloc(o->tf_coef, o->tf_tcap * 8);
+        o->tf_w0 = realloc(o->tf_w0, o->tf_tcap * 8);
+        o->tf_w1 = realloc(o->tf_w1, o->tf_tcap * 8);
+        o->tf_idx = realloc(o->tf_idx, o->tf_tcap * sizeof(int));
+        if (!o->tf_coef || !o->tf_w0 || !o->tf_w1 || !o->tf_idx) return -1;
+    }
+    double f = floor(s);
+    o->tf_coef[o->tf_nt] = coef;
+    o->tf_idx[o->tf_nt] = (int)f;
+    o->tf_w1[o->tf_nt] = s - f;
+    o->tf_w0[o->tf_nt] = 1.0 - (s - f);
+    o->tf_nt++;
+    return 0;
+}
+
+static long tf_wrap(const orc_t *o, int a, long q) {
+    if (!periodic(o, a)) return q;
+    long n = (long)o->n[a];
+    return q < 0 ? q + n : (q >= n ? q - n : q);
+}
+
+static int tf_init(orc_t *o, const scn_scene_t *s) {
+    const scn_plane_wave_t *pw = s->plane_wave;
+    tf_t t;
+    memset(&t, 0, sizeof t);
+    t.per = o->per;
+    double st = sin(pw->theta), ct = cos(pw->theta), sp = sin(pw->phi), cp = cos(pw->phi);
+    t.k[0] = st * cp; t.k[1] = st * sp; t.k[2] = ct;
+    double th[3] = {ct * cp, ct * sp, -st}, ph[3] = {-sp, cp, 0.0};
+    for (int a = 0; a < 3; a++) t.e[a] = cos(pw->psi) * th[a] + sin(pw->psi) * ph[a];
+    t.h[0] = t.k[1] * t.e[2] - t.k[2] * t.e[1];
+    t.h[1] = t.k[2] * t.e[0] - t.k[0] * t.e[2];
+    t.h[2] = t.k[0] * t.e[1] - t.k[1] * t.e[0];
+    const size_t bl[3] = {pw->i0, pw->j0, pw->k0}, bh[3] = {pw->i1, pw->j1, pw->k1};
+    long lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        t.lo[a] = (double)bl[a];
+        t.hi[a] = (double)bh[a];
+        t.ref[a] = periodic(o, a) ? 0.0 : (t.k[a] >= 0.0 ? (double)bl[a] : (double)bh[a]);
+        lo[a] = periodic(o, a) ? 0 : (long)bl[a] - 2;
+        hi[a] = periodic(o, a) ? (long)o->n[a] - 1 : (long)bh[a] + 2;
+    }
+    const double cbh = o->dt / (O_MU0 * o->dx);
+    double smax = 0.0;
+    for (int c = 0; c < 3; c++) {
+        o->tf_efirst[c] = malloc(o->total * sizeof(int));
+        o->tf_ecount[c] = calloc(o->total, sizeof(int));
+        if (!o->tf_efirst[c] || !o->tf_ecount[c]) return -1;
+        for (size_t q = 0; q < o->total; q++) o->tf_efirst[c][q] = -1;
+    }
+    for (long i = lo[0]; i <= hi[0]; i++)
+        for (long j = lo[1]; j <= hi[1]; j++)
+            for (long k = lo[2]; k <= hi[2]; k++) {
+                const long p[3] = {i, j, k};
+                int near = 0;
+                for (int a = 0; a < 3; a++)
+                    if (!periodic(o, a) && (p[a] <= (long)bl[a] + 2 || p[a] >= (long)bh[a] - 2)) near = 1;
+                if (!near) continue;
+                for (int c = 0; c < 3; c++) {
+                    const int fa = (c + 2) % 3, axa = (c + 1) % 3, fb = (c + 1) % 3, axb = (c + 2) % 3;
+                    const int qc[4] = {fa, fa, fb, fb};
+                    const double sg[4] = {1.0, -1.0, -1.0, 1.0};
+                    /* H_c at p */
+                    {
+                        double hp[3];
+                        tf_pos(3 + c, p, hp);
+                        int hin = tf_in(&t, hp);
+                        long q[4][3];
+                        for (int u = 0; u < 4; u++) for (int a = 0; a < 3; a++) q[u][a] = p[a];
+                        q[0][axa] += 1;
+                        q[2][axb] += 1;
+                        size_t first = o->tf_nt;
+                        for (int u = 0; u < 4; u++) {
+                            double ep[3];
+                            tf_pos(qc[u], q[u], ep);
+                            if (tf_in(&t, ep) == hin) continue;
+                            double sv = tf_s(&t, ep);
+                            if (sv > smax) smax = sv;
+                            if (tf_term(o, -cbh * sg[u] * (hin ? 1.0 : -1.0) * t.e[qc[u]], sv) != 0) return -1;
+                        }
+                        if (o->tf_nt > first) {
+                            if (o->tf_nh == o->tf_hcap) {
+                                o->tf_hcap = o->tf_hcap ? 2 * o->tf_hcap : 256;
+                                o->tf_hw = realloc(o->tf_hw, o->tf_hcap * sizeof(size_t));
+                                o->tf_hc = realloc(o->tf_hc, o->tf_hcap * sizeof(int));
+                                o->tf_hfirst = realloc(o->tf_hfirst, o->tf_hcap * sizeof(int));
+                                o->tf_hcount = realloc(o->tf_hcount, o->tf_hcap * sizeof(int));
+                                if (!o->tf_hw || !o->tf_hc || !o->tf_hfirst || !o->tf_hcount) return -1;
+                            }
+                            o->tf_hw[o->tf_nh] = at(o, (size_t)tf_wrap(o, 0, i), (size_t)tf_wrap(o, 1, j),
+                                                    (size_t)tf_wrap(o, 2, k));
+                            o->tf_hc[o->tf_nh] = c;
+                            o->tf_hfirst[o->tf_nh] = (int)first;
+                            o->tf_hcount[o->tf_nh] = (int)(o->tf_nt - first);
+                            o->tf_nh++;
+                        }
+                    }
+                    /* E_c at p */
+                    {
+                        size_t ci = (size_t)tf_wrap(o, 0, i), cj = (size_t)tf_wrap(o, 1, j), ck = (size_t)tf_wrap(o, 2, k);
+                        size_t cc[3] = {ci, cj, ck};
+                        int swept = ci < o->n[0] && cj < o->n[1] && ck < o->n[2];
+                        for (int a = 0; a < 3 && swept; a++)
+                            if (a != c && !periodic(o, a) && cc[a] < 1) swept = 0;
+                        if (!swept) continue;
+                        double epos[3];
+                        tf_pos(c, p, epos);
+                        int ein = tf_in(&t, epos);
+                        long q[4][3];
+                        for (int u = 0; u < 4; u++) for (int a = 0; a < 3; a++) q[u][a] = p[a];
+                        q[1][axa] -= 1;
+                        q[3][axb] -= 1;
+                        size_t w = at(o, ci, cj, ck);
+                        double cb = o->has_ovr[c][w] ? o->ocb[c][w] : o->tcb[o->id[w]];
+                        size_t first = o->tf_nt;
+                        for (int u = 0; u < 4; u++) {
+                            double hq[3];
+                            tf_pos(3 + qc[u], q[u], hq);
+                            if (tf_in(&t, hq) == ein) continue;
+                            double sv = tf_s(&t, hq) - 0.5;
+                            if (sv + 0.5 > smax) smax = sv + 0.5;
+                            if (tf_term(o, cb * sg[u] * (ein ? 1.0 : -1.0) * t.h[qc[u]], sv) != 0) return -1;
+                        }
+                        if (o->tf_nt > first) {
+                            o->tf_efirst[c][w] = (int)first;
+                            o->tf_ecount[c][w] = (int)(o->tf_nt - first);
+                        }
+                    }
+                }
+            }
+    double cps = O_C0 * o->dt / o->dx;
+    o->tf_len = (size_t)ceil(smax) + 4 + (size_t)ceil((double)s->n_steps * cps) + 4;
+    o->tf_ce = o->dt / (O_EPS0 * o->dx);
+    o->tf_ch = cbh;
+    o->tf_e = calloc(o->tf_len, 8);
+    o->tf_h = calloc(o->tf_len, 8);
+    o->tf_src = malloc((s->n_steps + 1) * 8);
+    if (!o->tf_e || !o->tf_h || !o->tf_src) return -1;
+    scn_source_t ws;
+    memset(&ws, 0, sizeof ws);
+    ws.waveform = pw->waveform;
+    ws.p0 = pw->p0; ws.p1 = pw->p1; ws.p2 = pw->p2;
+    for (size_t n = 0; n <= s->n_steps; n++) o->tf_src[n] = pw->amplitude * wave(&ws, (double)n * o->dt);
+    o->tf = 1;
+    return 0;
+}
+
+/* H corrections from the line's E^n, then the line's H to n+1/2 */
+static void tf_after_h(orc_t *o) {
+    for (size_t q = 0; q < o->tf_nh; q++) {
+        double *f = &o->H[o->tf_hc[q]][o->tf_hw[q]];
+        double h = *f;
+        for (int t = o->tf_hfirst[q]; t < o->tf_hfirst[q] + o->tf_hcount[q]; t++) {
+            int m = o->tf_idx[t];
+            h = h + o->tf_coef[t] * (o->tf_w0[t] * o->tf_e[m] + o->tf_w1[t] * o->tf_e[m + 1]);
+        }
+        *f = h;
+    }
+    for (size_t m = 0; m + 1 < o->tf_len; m++) o->tf_h[m] = o->tf_h[m] - o->tf_ch * (o->tf_e[m + 1] - o->tf_e[m]);
+}
+
+/* the line's E to n+1 (hard source at m = 0) */
+static void tf_after_e(orc_t *o, size_t n1, size_t n_steps) {
+    for (size_t m = 1; m + 1 < o->tf_len; m++) o->tf_e[m] = o->tf_e[m] - o->tf_ce * (o->tf_h[m] - o->tf_h[m - 1]);
+    o->tf_e[0] = o->tf_src[n1 < n_steps ? n1 : n_steps];
+}
+
 static int orc_init(orc_t *o, const scn_scene_t *s) {
     memset(o, 0, sizeof(*o));
     o->n[0] = s->nx; o->n[1] = s->ny; o->n[2] = s->nz;
@@ -347,6 +563,7 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
         o->has_t3[t->comp][w] = 1;
         memcpy(o->t3m[t->comp] + 3 * w, t->m, 3 * sizeof(double));
     }
+    if (s->plane_wave && tf_init(o, s) != 0) return -1;
     return 0;
 }
 
@@ -519,6 +736,14 @@ static void update_e(orc_t *o) {
                         continue;
                     }
                     o->E[c][here] = ca * o->E[c][here] + cb * (tA - tB);
+                    if (o->tf && o->tf_efirst[c][here] >= 0) {
+                        double v = o->E[c][here];
+                        for (int t = o->tf_efirst[c][here]; t < o->tf_efirst[c][here] + o->tf_ecount[c][here]; t++) {
+                            int m = o->tf_idx[t];
+                            v = v + o->tf_coef[t] * (o->tf_w0[t] * o->tf_h[m] + o->tf_w1[t] * o->tf_h[m + 1]);
+                        }
+                        o->E[c][here] = v;
+                    }
                 }
     }
 }
@@ -543,6 +768,7 @@ static double *field(orc_t *o, int comp) { return comp < 3 ? o->E[comp] : o->H[c
 
 static void step(orc_t *o, const scn_scene_t *s, size_t n) {
     update_h(o);
+    if (o->tf) tf_after_h(o);
     double t = ((double)n + s->src_t_offset) * o->dt;
     for (size_t q = 0; q < s->n_sources; q++) {
         const scn_source_t *src = &s->sources[q];
@@ -554,6 +780,7 @@ static void step(orc_t *o, const scn_scene_t *s, size_t n) {
         else f[w] = v;
     }
     update_e(o);
+    if (o->tf) tf_after_e(o, n + 1, s->n_steps);
 }
 
 /* Runs the scene; probe_td n_probes*n_steps, dft_re/im n_probes*n_freqs. */

@@ -47,6 +47,16 @@ typedef struct {
     int disp;
 } scn_sphere_t;
 
+/* plane wave through a total-field / scattered-field box (no rfsyn
+ * counterpart): direction theta / phi, E polarisation psi, waveform as a
+ * source's, total field in the box of sample positions [i0,i1]x[j0,j1]x[k0,k1] */
+typedef struct {
+    double theta, phi, psi, amplitude;
+    int waveform;
+    double p0, p1, p2;
+    size_t i0, i1, j0, j1, k0, k1;
+} scn_plane_wave_t;
+
 typedef struct {
     size_t nx, ny, nz;
     double dx, courant;
@@ -65,6 +75,7 @@ typedef struct {
     size_t n_freqs;   const double *freqs;
     double src_t_offset, dft_t_offset;
     size_t n_tensor3; const scn_tensor3_t *tensor3; /* applied last */
+    const scn_plane_wave_t *plane_wave;             /* NULL: none */
 } scn_scene_t;
 
 #endif

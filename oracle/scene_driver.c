@@ -147,6 +147,7 @@ out:
 /* Applies boxes, then scalar overrides, then tensor edges (in list order). */
 int scn_setup(const fdtd_grid_t *g, materials_t *m, void *ctx) {
     const scn_scene_t *s = (const scn_scene_t *)ctx;
+    /* the plane wave is a run option (fdtd_b200_config_t), not a material */
     for (size_t q = 0; q < s->n_boxes; q++) {
         const scn_box_t *b = &s->boxes[q];
         if (materials_set_box(m, g, b->i0, b->i1, b->j0, b->j1, b->k0, b->k1, b->eps_r, b->sigma) != 0) return -1;

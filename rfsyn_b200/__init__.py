@@ -60,6 +60,15 @@ class B200Probe(C.Structure):
     _fields_ = [("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t), ("component", C.c_int)]
 
 
+class PlaneWave(C.Structure):
+    """fdtd_b200_plane_wave_t."""
+
+    _fields_ = [("theta", C.c_double), ("phi", C.c_double), ("psi", C.c_double), ("amplitude", C.c_double),
+                ("waveform", C.c_int), ("p0", C.c_double), ("p1", C.c_double), ("p2", C.c_double),
+                ("i0", C.c_size_t), ("i1", C.c_size_t), ("j0", C.c_size_t), ("j1", C.c_size_t),
+                ("k0", C.c_size_t), ("k1", C.c_size_t)]
+
+
 class B200Config(C.Structure):
     _fields_ = [
         ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
@@ -68,6 +77,7 @@ class B200Config(C.Structure):
         ("n_sources", C.c_size_t), ("sources", C.POINTER(B200Source)), ("source_time_offset_steps", C.c_double),
         ("n_probes", C.c_size_t), ("probes", C.POINTER(B200Probe)),
         ("n_freqs", C.c_size_t), ("freqs_hz", C.POINTER(C.c_double)), ("dft_time_offset_steps", C.c_double),
+        ("plane_wave", C.POINTER(PlaneWave)),
     ]
 
 
@@ -269,7 +279,7 @@ class RunConfig:
 
     def __init__(self, nx, ny, nz, dx, n_steps, npml, *, courant=0.99, periodic=0, precision=FP64,
                  schedule=FUSED, cpml: CpmlParams | None = None, sources=(), probes=(), freqs=(),
-                 source_time_offset=0.0, dft_time_offset=1.0):
+                 source_time_offset=0.0, dft_time_offset=1.0, plane_wave: dict | None = None):
         self.c = B200Config()
         c = self.c
         c.nx, c.ny, c.nz, c.dx, c.n_steps = nx, ny, nz, dx, n_steps
@@ -306,6 +316,13 @@ class RunConfig:
         c.n_freqs = len(self._freqs)
         c.freqs_hz = _dptr(self._freqs) if len(self._freqs) else None
         c.dft_time_offset_steps = dft_time_offset
+        self._pw = None
+        if plane_wave is not None:
+            pw = PlaneWave()
+            for name, _ in PlaneWave._fields_:
+                setattr(pw, name, plane_wave.get(name, 0))
+            self._pw = pw
+            c.plane_wave = C.pointer(pw)
 
 
 def run(rc: RunConfig, setup=None, context=None) -> dict:

@@ -413,6 +413,15 @@ struct rfb_engine {
     int *d_err = nullptr;   // set by a sweep whose copies did not complete in time
     double *d_energy = nullptr;  // energy audit: block partials + result
     size_t h2d_bytes = 0, n_ade = 0;
+    // plane wave (TF/SF): line, H-target terms, per-entry E terms
+    int tf_on = 0, tf_n_h = 0, tf_m_len = 0;
+    double tf_ce = 0, tf_ch = 0;
+    void *tf_inc_e = nullptr, *tf_inc_h = nullptr, *tf_src = nullptr;
+    long long *tf_h_cell = nullptr;
+    int *tf_h_comp = nullptr, *tf_h_first = nullptr, *tf_h_count = nullptr, *tf_h_idx = nullptr;
+    void *tf_h_coef = nullptr, *tf_h_w0 = nullptr, *tf_h_w1 = nullptr;
+    int *tf_e_first = nullptr, *tf_e_count = nullptr, *tf_e_idx = nullptr;
+    void *tf_e_coef = nullptr, *tf_e_w0 = nullptr, *tf_e_w1 = nullptr;
     int active = 0;          // a source sits on a padded boundary plane
     int member = 0;          // scene of a batch: no plan, graphs or second stream of its own
 };
@@ -435,7 +444,59 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
     a.src_hard = e->src_hard;
     a.n_steps = (long long)e->n_steps;
     a.d_step = e->d_step;
+    if (e->tf_on) {
+        a.tf_first = e->tf_e_first;
+        a.tf_count = e->tf_e_count;
+        a.tf_idx = e->tf_e_idx;
+        a.tf_coef = (const T *)e->tf_e_coef;
+        a.tf_w0 = (const T *)e->tf_e_w0;
+        a.tf_w1 = (const T *)e->tf_e_w1;
+        a.inc_h = (const T *)e->tf_inc_h;
+    }
     return a;
+}
+
+template <typename T>
+static TfArgs<T> tf_args(const rfb_engine *e, int par) {
+    TfArgs<T> t;
+    memset(&t, 0, sizeof t);
+    const int out = e->nbuf == 2 ? 1 - par : 0;
+    t.n_h = e->tf_n_h;
+    t.h_cell = e->tf_h_cell;
+    t.h_comp = e->tf_h_comp;
+    t.h_first = e->tf_h_first;
+    t.h_count = e->tf_h_count;
+    t.h_idx = e->tf_h_idx;
+    t.h_coef = (const T *)e->tf_h_coef;
+    t.h_w0 = (const T *)e->tf_h_w0;
+    t.h_w1 = (const T *)e->tf_h_w1;
+    for (int c = 0; c < 3; c++) t.Ho[c] = (T *)e->fld[out][3 + c];
+    t.inc_e = (T *)e->tf_inc_e;
+    t.inc_h = (T *)e->tf_inc_h;
+    t.m_len = e->tf_m_len;
+    t.ce = (T)e->tf_ce;
+    t.ch = (T)e->tf_ch;
+    t.src = (const T *)e->tf_src;
+    t.d_step = e->d_step;
+    t.n_steps = (long long)e->n_steps;
+    return t;
+}
+
+// Plane wave: H corrections from the line's E^n, then the line's H to n+1/2
+// (before the interface list, whose boundary entries read it).
+template <typename T>
+static void tf_before_list(rfb_engine *e, int par) {
+    if (!e->tf_on) return;
+    TfArgs<T> t = tf_args<T>(e, par);
+    if (t.n_h) k_tfsf_h<T><<<(t.n_h + 255) / 256, 256, 0, e->stream>>>(t);
+    k_inc_h<T><<<(t.m_len + 255) / 256, 256, 0, e->stream>>>(t);
+}
+// ... and the line's E to n+1 after the step counter advanced.
+template <typename T>
+static void tf_after_step(rfb_engine *e, int par) {
+    if (!e->tf_on) return;
+    TfArgs<T> t = tf_args<T>(e, par);
+    k_inc_e<T><<<(t.m_len + 255) / 256, 256, 0, e->stream>>>(t);
 }
 
 // Interior sweep of the plan: TMA-fed or cp.async-fed variant, or (mode 2)
@@ -492,6 +553,7 @@ static void enqueue_step(rfb_engine *e, int par) {
         k_h_split<T><<<grd, blk, 0, e->stream>>>(a);
         k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
     }
+    tf_before_list<T>(e, par);
     if (a.n_cells) k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
     ProbeArgs<T> p;
     p.n = e->n_probes;
@@ -503,6 +565,7 @@ static void enqueue_step(rfb_engine *e, int par) {
     p.n_steps = (long long)e->n_steps;
     p.d_step = e->d_step;
     k_probe_gather<T><<<1, 128, 0, e->stream>>>(p);
+    tf_after_step<T>(e, par);
 }
 
 static int count_step_launches(const rfb_engine *e) {
@@ -510,6 +573,7 @@ static int count_step_launches(const rfb_engine *e) {
                 ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0)
                 : 2;
     if (e->scene.n_cells) n++;
+    if (e->tf_on) n += 2 + (e->tf_n_h > 0);
     return n + 1;
 }
 
@@ -898,6 +962,10 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
     cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_qx); cudaFree(e->plan.d_queue);
+    cudaFree(e->tf_inc_e); cudaFree(e->tf_inc_h); cudaFree(e->tf_src); cudaFree(e->tf_h_cell); cudaFree(e->tf_h_comp);
+    cudaFree(e->tf_h_first); cudaFree(e->tf_h_count); cudaFree(e->tf_h_idx); cudaFree(e->tf_h_coef); cudaFree(e->tf_h_w0);
+    cudaFree(e->tf_h_w1); cudaFree(e->tf_e_first); cudaFree(e->tf_e_count); cudaFree(e->tf_e_idx); cudaFree(e->tf_e_coef);
+    cudaFree(e->tf_e_w0); cudaFree(e->tf_e_w1);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->stream2) cudaStreamDestroy(e->stream2);
@@ -1052,6 +1120,71 @@ extern "C" rfb_engine_t *rfb_engine_create_member(const rfb_geom_t *geom, int pr
                          n_steps, stream, 1);
 }
 
+extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
+    if (e->tf_on || e->member) {
+        rfb_set_error("a plane wave is attached once, to a session");
+        return -1;
+    }
+    const int prec = e->prec;
+    const size_t ne = 3 * (size_t)e->scene.n_cells;
+    const rfb_geom_t &g = e->g;
+    std::vector<long long> cell(d->n_h);
+    std::vector<int> comp(d->n_h);
+    for (size_t q = 0; q < d->n_h; q++) {
+        cell[q] = ((long long)d->h_ijkc[4 * q] * (g.ny + 1) + d->h_ijkc[4 * q + 1]) * e->pitch + d->h_ijkc[4 * q + 2];
+        comp[q] = d->h_ijkc[4 * q + 3];
+    }
+    e->tf_m_len = (int)d->m_len;
+    e->tf_ce = d->ce;
+    e->tf_ch = d->ch;
+    e->tf_n_h = (int)d->n_h;
+    CK(cudaMalloc(&e->tf_inc_e, d->m_len * e->esz));
+    CK(cudaMalloc(&e->tf_inc_h, d->m_len * e->esz));
+    CK(cudaMemset(e->tf_inc_e, 0, d->m_len * e->esz));
+    CK(cudaMemset(e->tf_inc_h, 0, d->m_len * e->esz));
+    e->tf_src = dev_upload_conv(d->src, e->n_steps + 1, prec);
+    if (!e->tf_src) goto fail;
+    if (d->n_h) {
+        e->tf_h_cell = dev_copy(cell.data(), d->n_h);
+        e->tf_h_comp = dev_copy(comp.data(), d->n_h);
+        e->tf_h_first = dev_copy(d->h_first, d->n_h);
+        e->tf_h_count = dev_copy(d->h_count, d->n_h);
+        e->tf_h_idx = dev_copy(d->h_idx, d->n_hterms);
+        e->tf_h_coef = dev_upload_conv(d->h_coef, d->n_hterms, prec);
+        e->tf_h_w0 = dev_upload_conv(d->h_w0, d->n_hterms, prec);
+        e->tf_h_w1 = dev_upload_conv(d->h_w1, d->n_hterms, prec);
+        if (!e->tf_h_cell || !e->tf_h_comp || !e->tf_h_first || !e->tf_h_count || !e->tf_h_idx || !e->tf_h_coef ||
+            !e->tf_h_w0 || !e->tf_h_w1)
+            goto fail;
+    }
+    if (ne) {
+        e->tf_e_first = dev_copy(d->entry_first, ne);
+        e->tf_e_count = dev_copy(d->entry_count, ne);
+        if (!e->tf_e_first || !e->tf_e_count) goto fail;
+    }
+    if (d->n_eterms) {
+        e->tf_e_idx = dev_copy(d->e_idx, d->n_eterms);
+        e->tf_e_coef = dev_upload_conv(d->e_coef, d->n_eterms, prec);
+        e->tf_e_w0 = dev_upload_conv(d->e_w0, d->n_eterms, prec);
+        e->tf_e_w1 = dev_upload_conv(d->e_w1, d->n_eterms, prec);
+        if (!e->tf_e_idx || !e->tf_e_coef || !e->tf_e_w0 || !e->tf_e_w1) goto fail;
+    }
+    e->tf_on = 1;
+    // graphs captured before the plane wave would lack its kernels
+    for (int q = 0; q < 2; q++) {
+        if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
+        if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
+        e->g1[q] = e->gk[q] = nullptr;
+    }
+    e->launches_per_step = count_step_launches(e);
+    e->h2d_bytes += (size_t)(e->n_steps + 1) * e->esz + d->n_h * 24 + (d->n_hterms + d->n_eterms) * (3 * e->esz + 4) +
+                    ne * 8;
+    return 0;
+fail:
+    rfb_set_error("plane-wave upload failed");
+    return -1;
+}
+
 extern "C" int rfb_engine_reset(rfb_engine_t *e) {
     for (int b = 0; b < e->nbuf; b++)
         for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(e->fld[b][c], 0, e->total * e->esz, e->stream));
@@ -1061,6 +1194,10 @@ extern "C" int rfb_engine_reset(rfb_engine_t *e) {
             if (e->cpml.psi_h[b][p]) CK(cudaMemsetAsync(e->cpml.psi_h[b][p], 0, e->cpml.psi_h_bytes[p], e->stream));
     }
     if (e->scene.ade_s) CK(cudaMemsetAsync(e->scene.ade_s, 0, e->scene.ade_s_bytes, e->stream));
+    if (e->tf_on) {
+        CK(cudaMemsetAsync(e->tf_inc_e, 0, (size_t)e->tf_m_len * e->esz, e->stream));
+        CK(cudaMemsetAsync(e->tf_inc_h, 0, (size_t)e->tf_m_len * e->esz, e->stream));
+    }
     CK(cudaMemsetAsync(e->d_step, 0, sizeof(int), e->stream));
     e->steps_done = 0;
     e->parity = 0;
@@ -1170,6 +1307,7 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
             g_launches += 2;
         }
         CK(cudaEventRecord(ev[1], e->stream));
+        tf_before_list<T>(e, par);
         if (a.n_cells) {
             k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
             g_launches++;
@@ -1184,7 +1322,8 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         p.n_steps = (long long)e->n_steps;
         p.d_step = e->d_step;
         k_probe_gather<T><<<1, 128, 0, e->stream>>>(p);
-        g_launches++;
+        tf_after_step<T>(e, par);
+        g_launches += 1 + (e->tf_on ? 2 + (e->tf_n_h > 0) : 0);
         CK(cudaEventRecord(ev[2], e->stream));
         CK(cudaEventSynchronize(ev[2]));
         float t1 = 0.f, t2 = 0.f;

@@ -152,6 +152,24 @@ int rfb_batch_info(rfb_batch_t *b, rfb_batch_info_t *out);
 void *rfb_stream_create(void);
 void rfb_stream_destroy(void *stream);
 
+/* Plane wave through a TF/SF boundary: the 1-D incident line and the
+ * correction terms (see tfsf.c).  H targets are corrected after the sweep
+ * from the line's E; E targets are list entries (entry_first / entry_count
+ * per entry of the scene image, -1 / 0 for none) corrected from its H. */
+typedef struct {
+    size_t m_len;
+    double ce, ch;
+    const double *src;                       /* n_steps + 1 */
+    size_t n_h;
+    const int32_t *h_ijkc, *h_first, *h_count;
+    size_t n_hterms, n_eterms;
+    const double *h_coef, *h_w0, *h_w1, *e_coef, *e_w0, *e_w1;
+    const int32_t *h_idx, *e_idx;
+    const int32_t *entry_first, *entry_count;  /* 3 * n_cells of the scene image */
+} rfb_tfsf_desc_t;
+/* Attaches a plane wave to an engine before its first step. */
+int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d);
+
 /* Zero fields, psi and ADE state and rewind the step counter (async). */
 int rfb_engine_reset(rfb_engine_t *e);
 /* Enqueue n steps on the engine stream (CUDA graph replay). */

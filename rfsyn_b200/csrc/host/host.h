@@ -67,6 +67,33 @@ void rfb_scene_build_free(rfb_scene_build_t *b);
 rfb_scene_dev_t *materials_device(const materials_t *mat, const fdtd_grid_t *g);
 int materials_matches(const materials_t *mat, const fdtd_grid_t *g);
 
+/* Component c of canonical cell (i,j,k) is swept by rfsyn's E loops
+ * (materials.c:915-1059). */
+int rfb_e_swept(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k);
+
+/* Plane-wave TF/SF boundary (tfsf.c): the 1-D incident line and the
+ * correction terms of the H samples (applied after the sweep) and of the E
+ * samples (applied by the interface-list kernel). */
+typedef struct {
+    size_t m_len;            /* E samples of the line (H: m_len - 1) */
+    double ce, ch;           /* dt / (eps0 dx), dt / (mu0 dx) */
+    double *src;             /* E1D[0] at steps 0 .. n_steps */
+    size_t n_h;              /* H targets: i, j, k, comp; first term, count */
+    int32_t *h_ijkc, *h_first, *h_count;
+    size_t n_e;              /* E targets, likewise */
+    int32_t *e_ijkc, *e_first, *e_count;
+    size_t n_hterms, n_eterms;
+    double *h_coef, *h_w0, *h_w1, *e_coef, *e_w0, *e_w1;
+    int32_t *h_idx, *e_idx;
+    size_t n_cells;          /* cells whose E samples go on the interface list */
+    int32_t *cells;
+} rfb_tfsf_build_t;
+
+int rfb_tfsf_build(const fdtd_grid_t *g, const materials_t *mat, const fdtd_b200_plane_wave_t *pw, size_t n_steps,
+                   int cpml_npml, rfb_tfsf_build_t *out);
+void rfb_tfsf_free(rfb_tfsf_build_t *b);
+double rfb_wave_value(int waveform, double amplitude, double p0, double p1, double p2, double t);
+
 /* Inverse of a symmetric positive-definite 3x3 matrix (row-major); -1 when
  * the matrix is not symmetric positive definite. */
 int rfb_spd3_inverse(const double e[9], double out[9]);

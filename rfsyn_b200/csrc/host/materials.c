@@ -725,7 +725,7 @@ static size_t next_q(size_t q, size_t n) { return q + 1 == n ? 0 : q + 1; }
 
 /* Component c of canonical cell (i,j,k) is swept by rfsyn's E loops
  * (materials.c:915-1059). */
-static int e_swept(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k) {
+int rfb_e_swept(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k) {
     size_t i0 = (g->periodic_axes & 1u) ? 0 : 1, j0 = (g->periodic_axes & 2u) ? 0 : 1,
            k0 = (g->periodic_axes & 4u) ? 0 : 1;
     if (i >= g->nx || j >= g->ny || k >= g->nz) return 0;
@@ -851,7 +851,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
             material_coeff_t co = lookup(mat, idx, c);
             out->ca[e] = co.Ca;
             out->cb[e] = co.Cb;
-            if (!e_swept(g, c, i, j, k)) {
+            if (!rfb_e_swept(g, c, i, j, k)) {
                 out->kind[e] = RFB_LK_COPY;
                 continue;
             }

@@ -94,6 +94,18 @@ static double wave_value(const fdtd_b200_source_t *s, double t, size_t n) {
     }
 }
 
+/* amplitude * waveform(t) of a plane wave (waveforms 0..2 as for sources) */
+double rfb_wave_value(int waveform, double amplitude, double p0, double p1, double p2, double t) {
+    fdtd_b200_source_t s;
+    memset(&s, 0, sizeof s);
+    s.waveform = waveform;
+    s.amplitude = amplitude;
+    s.p0 = p0;
+    s.p1 = p1;
+    s.p2 = p2;
+    return wave_value(&s, t, 0);
+}
+
 static size_t canon(size_t q, size_t n, int periodic) { return periodic ? q % n : q; }
 
 /* member: create the engine as a scene of a batch (FUSED, on the batch's
@@ -110,6 +122,9 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
     rfb_extra_cell_t *extra = NULL;
     rfb_probe_desc_t *pd = NULL;
     fdtd_b200_sim_t *sim = NULL;
+    rfb_tfsf_build_t tf;
+    int32_t *tf_first = NULL, *tf_count = NULL;
+    memset(&tf, 0, sizeof tf);
 
     if (!cfg) { rfb_set_error("NULL config"); return NULL; }
     if (cfg->n_steps == 0) { rfb_set_error("n_steps must be positive"); return NULL; }
@@ -139,11 +154,26 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
     if (setup && setup(&g, mat, context) != 0) { rfb_set_error("scene setup callback failed"); goto fail; }
 
     const size_t ns = cfg->n_sources, np = cfg->n_probes, nt = cfg->n_steps;
-    if (ns) {
-        vals = malloc(ns * nt * sizeof(double));
-        sd = calloc(ns, sizeof(*sd));
-        extra = calloc(ns, sizeof(*extra));
+    if (cfg->plane_wave) {
+        if (member) {
+            rfb_set_error("a plane wave is not supported in a batch scene");
+            goto fail;
+        }
+        if (rfb_tfsf_build(&g, mat, cfg->plane_wave, nt, pml ? (int)cfg->cpml.npml : 0, &tf) != 0) goto fail;
+    }
+    if (ns || tf.n_cells) {
+        vals = malloc((ns ? ns : 1) * nt * sizeof(double));
+        sd = calloc(ns ? ns : 1, sizeof(*sd));
+        extra = calloc(ns + tf.n_cells, sizeof(*extra));
         if (!vals || !sd || !extra) { rfb_set_error("out of host memory"); goto fail; }
+    }
+    for (size_t q = 0; q < tf.n_cells; q++) {
+        /* cells next to the plane-wave boundary: on the interface list */
+        extra[ns + q].i = tf.cells[3 * q];
+        extra[ns + q].j = tf.cells[3 * q + 1];
+        extra[ns + q].k = tf.cells[3 * q + 2];
+        extra[ns + q].component = -1;
+        extra[ns + q].slot = -1;
     }
     for (size_t s = 0; s < ns; s++) {
         const fdtd_b200_source_t *src = &cfg->sources[s];
@@ -180,8 +210,42 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
         pd[q].k = (int)canon(p->k, g.nz, pz);
         pd[q].component = (int)p->component;
     }
-    if (materials_build_image(mat, &g, ns, extra, &scene) != 0) goto fail;
+    if (materials_build_image(mat, &g, ns + tf.n_cells, extra, &scene) != 0) goto fail;
     have_scene = 1;
+    if (cfg->plane_wave) {
+        /* E corrections per list entry: find each E target's cell */
+        const size_t ne = 3 * scene.img.n_cells;
+        tf_first = malloc((ne + 1) * sizeof(int32_t));
+        tf_count = calloc(ne + 1, sizeof(int32_t));
+        if (!tf_first || !tf_count) { rfb_set_error("out of host memory"); goto fail; }
+        for (size_t e = 0; e < ne; e++) tf_first[e] = -1;
+        const size_t nz1 = g.nz + 1, ny1 = g.ny + 1;
+        for (size_t q = 0; q < tf.n_e; q++) {
+            const size_t key = ((size_t)tf.e_ijkc[4 * q] * ny1 + (size_t)tf.e_ijkc[4 * q + 1]) * nz1 +
+                               (size_t)tf.e_ijkc[4 * q + 2];
+            size_t lo = 0, hi = scene.img.n_cells;
+            while (lo < hi) {
+                const size_t mid = (lo + hi) / 2;
+                const int32_t *c = scene.img.cell_ijk + 3 * mid;
+                const size_t km = ((size_t)c[0] * ny1 + (size_t)c[1]) * nz1 + (size_t)c[2];
+                if (km < key) lo = mid + 1;
+                else hi = mid;
+            }
+            const int32_t *hit = scene.img.cell_ijk + 3 * lo;
+            if (lo == scene.img.n_cells || hit[0] != tf.e_ijkc[4 * q] || hit[1] != tf.e_ijkc[4 * q + 1] ||
+                hit[2] != tf.e_ijkc[4 * q + 2]) {
+                rfb_set_error("plane wave: a boundary sample is not on the list");
+                goto fail;
+            }
+            const size_t e = 3 * lo + (size_t)tf.e_ijkc[4 * q + 3];
+            if (scene.img.kind[e] != RFB_LK_SCALAR) {
+                rfb_set_error("plane wave: the boundary must lie in scalar media");
+                goto fail;
+            }
+            tf_first[e] = tf.e_first[q];
+            tf_count[e] = tf.e_count[q];
+        }
+    }
 
     sim = calloc(1, sizeof(*sim));
     if (!sim) { rfb_set_error("out of host memory"); goto fail; }
@@ -214,6 +278,32 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
                                      pd, nt, cuda_stream);
     }
     if (!sim->eng) goto fail;
+    if (cfg->plane_wave) {
+        rfb_tfsf_desc_t td;
+        memset(&td, 0, sizeof td);
+        td.m_len = tf.m_len;
+        td.ce = tf.ce;
+        td.ch = tf.ch;
+        td.src = tf.src;
+        td.n_h = tf.n_h;
+        td.h_ijkc = tf.h_ijkc;
+        td.h_first = tf.h_first;
+        td.h_count = tf.h_count;
+        td.n_hterms = tf.n_hterms;
+        td.n_eterms = tf.n_eterms;
+        td.h_coef = tf.h_coef; td.h_w0 = tf.h_w0; td.h_w1 = tf.h_w1; td.h_idx = tf.h_idx;
+        td.e_coef = tf.e_coef; td.e_w0 = tf.e_w0; td.e_w1 = tf.e_w1; td.e_idx = tf.e_idx;
+        td.entry_first = tf_first;
+        td.entry_count = tf_count;
+        if (rfb_engine_set_tfsf(sim->eng, &td) != 0) {
+            rfb_engine_destroy(sim->eng);
+            sim->eng = NULL;
+            goto fail;
+        }
+    }
+    rfb_tfsf_free(&tf);
+    free(tf_first);
+    free(tf_count);
     rfb_scene_build_free(&scene);
     free(vals); free(sd); free(extra); free(pd);
     materials_destroy(mat);
@@ -225,6 +315,9 @@ fail:
         free(sim);
     }
     if (have_scene) rfb_scene_build_free(&scene);
+    rfb_tfsf_free(&tf);
+    free(tf_first);
+    free(tf_count);
     free(vals); free(sd); free(extra); free(pd);
     materials_destroy(mat);
     cpml_destroy(pml);

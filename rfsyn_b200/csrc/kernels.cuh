@@ -59,6 +59,11 @@ struct Args {
     const T *t_m11, *t_scale, *t_w;
     const int *t_main, *t_nq, *t_uv, *t_sign;
     const T *t3;             // 3x3 samples: row of eps_r^-1, then dt / (eps0 dx)
+    // plane-wave boundary: per list entry its first correction term (-1:
+    // none) and count; terms coef * (w0 H1D[idx] + w1 H1D[idx + 1])
+    const int *tf_first, *tf_count, *tf_idx;
+    const T *tf_coef, *tf_w0, *tf_w1;
+    const T *inc_h;          // the incident line's H at n + 1/2
     // sources
     const T *src_val;
     const int *src_hard;
@@ -343,7 +348,68 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
         // full 3x3 anisotropic sample
         v = e_tensor3(a, a.t3 + 4 * (long long)a.l_tix[e], comp, i, j, k, v);
     }
+    if (a.tf_first) {
+        // a sample next to the total-field / scattered-field boundary
+        const int f = a.tf_first[e];
+        if (f >= 0)
+            for (int t = f; t < f + a.tf_count[e]; t++) {
+                const int m = a.tf_idx[t];
+                v = xa(v, xm(a.tf_coef[t], xa(xm(a.tf_w0[t], a.inc_h[m]), xm(a.tf_w1[t], a.inc_h[m + 1]))));
+            }
+    }
     a.Eo[comp][c] = v;
+}
+
+// ---- plane wave through a TF/SF boundary -----------------------------------
+template <typename T>
+struct TfArgs {
+    int n_h;
+    const long long *h_cell;
+    const int *h_comp, *h_first, *h_count, *h_idx;
+    const T *h_coef, *h_w0, *h_w1;
+    T *Ho[3];              // H after the sweep of the step
+    T *inc_e, *inc_h;      // the 1-D line
+    int m_len;
+    T ce, ch;
+    const T *src;          // E1D[0] per step, n_steps + 1 values
+    const int *d_step;
+    long long n_steps;
+};
+
+// H samples next to the boundary: H += coef * (w0 E1D[idx] + w1 E1D[idx+1])
+// for each of their terms, in order (E1D at step n).
+template <typename T>
+__global__ void k_tfsf_h(TfArgs<T> a) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.n_h) return;
+    T *f = a.Ho[a.h_comp[q]] + a.h_cell[q];
+    T h = *f;
+    for (int t = a.h_first[q]; t < a.h_first[q] + a.h_count[q]; t++) {
+        const int m = a.h_idx[t];
+        h = xa(h, xm(a.h_coef[t], xa(xm(a.h_w0[t], a.inc_e[m]), xm(a.h_w1[t], a.inc_e[m + 1]))));
+    }
+    *f = h;
+}
+
+// The line's H: H1D[m] -= ch (E1D[m+1] - E1D[m]).
+template <typename T>
+__global__ void k_inc_h(TfArgs<T> a) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < a.m_len - 1; m += gridDim.x * blockDim.x)
+        a.inc_h[m] = xs(a.inc_h[m], xm(a.ch, xs(a.inc_e[m + 1], a.inc_e[m])));
+}
+
+// The line's E: E1D[m] -= ce (H1D[m] - H1D[m-1]); E1D[0] is the hard source
+// of the step just completed (the step counter already advanced).
+template <typename T>
+__global__ void k_inc_e(TfArgs<T> a) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < a.m_len - 1; m += gridDim.x * blockDim.x) {
+        if (m == 0) {
+            const long long n = *a.d_step;
+            a.inc_e[0] = a.src[n < a.n_steps ? n : a.n_steps];
+        } else {
+            a.inc_e[m] = xs(a.inc_e[m], xm(a.ce, xs(a.inc_h[m], a.inc_h[m - 1])));
+        }
+    }
 }
 
 template <typename T>

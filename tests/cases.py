@@ -96,7 +96,7 @@ def scene_run_config(s: Scene, precision: int, schedule: int) -> rb.RunConfig:
         sources=[dict(i=q[0], j=q[1], k=q[2], component=q[3], mode=q[4], amplitude=q[5], waveform=q[6], p0=q[7],
                       p1=q[8], p2=q[9]) for q in s.sources],
         probes=[dict(i=q[0], j=q[1], k=q[2], component=q[3]) for q in s.probes], freqs=s.freqs,
-        source_time_offset=s.src_t_offset, dft_time_offset=s.dft_t_offset)
+        source_time_offset=s.src_t_offset, dft_time_offset=s.dft_t_offset, plane_wave=s.plane_wave)
 
 
 def run_device(s: Scene, precision: int, schedule: int) -> dict:
