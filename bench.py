@@ -219,9 +219,9 @@ def run_b200(args) -> None:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
 
     # each rank simulates its own independent scene (weak scaling, no collective on the data path)
-    w = scenes.c2(seed=2 + rank)
+    w = scenes.c3(seed=3 + rank) if args.workload == "c3" else scenes.c2(seed=2 + rank)
     rc = scenes.run_config(w)
-    setup = scenes.sphere_setup(w)
+    setup = scenes.scene_setup(w)
     sim = rb.Sim(rc, setup.ptr if setup else None, None)
     stream = torch.cuda.ExternalStream(sim.stream)
     info = sim.info()
@@ -294,7 +294,7 @@ def run_b200(args) -> None:
     e2e_value = world * w.cells * w.n_steps / (e2e_ms / 1e3) / 1e6
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
         try:
             cb = cpu_reference(w, args.ref_sample_steps, max(1, min(os.cpu_count() or 1, 16)))
             cb.pop("loop_s", None)
@@ -310,7 +310,9 @@ def run_b200(args) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32 scene: 24 smoothed + 3 Debye spheres)",
+        "vs_baseline": None, "dtype": "f32",
+        "data": ("synthetic (seeded PCG32 scene: 24 smoothed + 3 Debye spheres)" if args.workload == "c2" else
+                 "synthetic (seeded PCG32 cell: TF/SF plane wave, tilted 3x3 slab, 2-pole Lorentz layer)"),
         "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "n_steps": w.n_steps, "npml": w.npml,
                    "probes": len(w.probes), "dft_bins": len(w.freqs), "spheres": len(w.spheres),
                    "list_cells": info.list_cells, "dispersive_samples": info.dispersive,
@@ -557,7 +559,7 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
     ap.add_argument("--train-scenes", type=int, default=5000, help="c5: training scenes (4 samples each)")
     ap.add_argument("--test-scenes", type=int, default=500, help="c5: held-out scenes")
     ap.add_argument("--train-steps", type=int, default=20000, help="c5: Adam steps per member")

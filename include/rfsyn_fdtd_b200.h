@@ -291,6 +291,9 @@ typedef struct {
 int fdtd_b200_materials_set_component_dispersive(materials_t *mat, const fdtd_grid_t *g,
                                                  field_component_t component, size_t i, size_t j, size_t k,
                                                  const fdtd_b200_dispersive_t *model);
+/* Every component of every cell of a half-open box gets the model. */
+int fdtd_b200_materials_set_dispersive_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0,
+                                           size_t j1, size_t k0, size_t k1, const fdtd_b200_dispersive_t *model);
 int fdtd_b200_materials_clear_component_dispersive(materials_t *mat, const fdtd_grid_t *g,
                                                    field_component_t component, size_t i, size_t j, size_t k);
 
@@ -314,6 +317,12 @@ int fdtd_b200_materials_clear_component_tensor3(materials_t *mat, const fdtd_gri
                                                 size_t i, size_t j, size_t k);
 int fdtd_b200_materials_set_tensor3_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0,
                                         size_t j1, size_t k0, size_t k1, const double eps_r[9]);
+/* Every E sample (cell units: Ex of cell (i,j,k) at (i+1/2, j, k), ...)
+ * within thickness / 2 of the plane through `point` with `normal`, and
+ * admitted by the margin rule, gets the row of eps_r^-1 (a staircased
+ * anisotropic slab). */
+int fdtd_b200_materials_set_tensor3_slab(materials_t *mat, const fdtd_grid_t *g, const double point[3],
+                                         const double normal[3], double thickness, const double eps_r[9]);
 /* The row of a 3x3 sample: 0, or 1 when the component has none. */
 int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g, field_component_t component,
                                     size_t i, size_t j, size_t k, double row[3]);

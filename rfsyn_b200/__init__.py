@@ -162,21 +162,35 @@ class SphereSetup:
 
 class SceneSetup:
     """An fdtd_material_setup_fn that applies boxes (rfsyn's
-    materials_set_box, in list order) and then spheres
-    (fdtd_b200_materials_add_spheres); keeps the ctypes objects alive.
-    boxes: (i0, i1, j0, j1, k0, k1, eps_r, sigma) half-open cell ranges."""
+    materials_set_box, in list order), spheres
+    (fdtd_b200_materials_add_spheres), dispersive boxes
+    (fdtd_b200_materials_set_dispersive_box) and last anisotropic slabs
+    (fdtd_b200_materials_set_tensor3_slab); keeps the ctypes objects alive.
+    boxes: (i0, i1, j0, j1, k0, k1, eps_r, sigma) half-open cell ranges;
+    slabs: (point[3], normal[3], thickness, eps_r[9]); disp_boxes:
+    (i0, i1, j0, j1, k0, k1, Dispersive)."""
 
-    def __init__(self, boxes=(), spheres=(), smoothing: int = 1):
+    def __init__(self, boxes=(), spheres=(), smoothing: int = 1, slabs=(), disp_boxes=()):
         lib = load()
         self._spheres = SphereSetup(spheres, smoothing) if spheres else None
         boxes = list(boxes)
+        self._slabs = [((C.c_double * 3)(*p), (C.c_double * 3)(*n), t, (C.c_double * 9)(*e))
+                       for (p, n, t, e) in slabs]
+        self._dboxes = list(disp_boxes)
 
         def cb(grid, mat, ctx):
             for (i0, i1, j0, j1, k0, k1, eps, sig) in boxes:
                 if lib.materials_set_box(mat, grid, i0, i1, j0, j1, k0, k1, eps, sig) != 0:
                     return -1
-            if self._spheres is not None:
-                return self._spheres.fn(grid, mat, ctx)
+            if self._spheres is not None and self._spheres.fn(grid, mat, ctx) != 0:
+                return -1
+            for (i0, i1, j0, j1, k0, k1, model) in self._dboxes:
+                if lib.fdtd_b200_materials_set_dispersive_box(mat, grid, i0, i1, j0, j1, k0, k1,
+                                                              C.byref(model)) != 0:
+                    return -1
+            for (p, n, t, e) in self._slabs:
+                if lib.fdtd_b200_materials_set_tensor3_slab(mat, grid, p, n, t, e) != 0:
+                    return -1
             return 0
 
         self.fn = SETUP_FN(cb)
@@ -218,6 +232,8 @@ def load() -> C.CDLL:
         "cpml_default_params": (CpmlParams, [S]),
         "fdtd_b200_materials_add_spheres": (I, [P, P, C.POINTER(Sphere), S, I]),
         "materials_set_box": (I, [P, P, S, S, S, S, S, S, D, D]),
+        "fdtd_b200_materials_set_dispersive_box": (I, [P, P, S, S, S, S, S, S, P]),
+        "fdtd_b200_materials_set_tensor3_slab": (I, [P, P, C.POINTER(D), C.POINTER(D), D, C.POINTER(D)]),
         "fdtd_b200_sim_info": (I, [P, C.POINTER(SimInfo)]),
         "fdtd_b200_sim_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_sim_energy": (I, [P, I, I, C.POINTER(Energy)]),

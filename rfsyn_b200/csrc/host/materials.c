@@ -507,6 +507,52 @@ int fdtd_b200_materials_clear_component_tensor3(materials_t *mat, const fdtd_gri
     return 0;
 }
 
+int fdtd_b200_materials_set_tensor3_slab(materials_t *mat, const fdtd_grid_t *g, const double point[3],
+                                         const double normal[3], double thickness, const double eps_r[9]) {
+    double m[9];
+    if (!point || !normal || !eps_r || !(thickness > 0.0) || rfb_spd3_inverse(eps_r, m) != 0) return -1;
+    if (!materials_matches(mat, g)) return -1;
+    const double nn = sqrt(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+    if (!(nn > 0.0)) return -1;
+    const double u[3] = {normal[0] / nn, normal[1] / nn, normal[2] / nn};
+    const size_t n[3] = {g->nx, g->ny, g->nz};
+    size_t lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        const int per = (g->periodic_axes >> a) & 1u;
+        lo[a] = per ? 0 : 1;
+        hi[a] = per ? n[a] : n[a];  /* cells [lo, hi): the margin rule keeps index n - 1 at most */
+    }
+    for (size_t i = lo[0]; i < hi[0]; i++)
+        for (size_t j = lo[1]; j < hi[1]; j++)
+            for (size_t k = lo[2]; k < hi[2]; k++)
+                for (int c = 0; c < 3; c++) {
+                    double p[3] = {(double)i, (double)j, (double)k};
+                    p[c] += 0.5;
+                    const double d = u[0] * (p[0] - point[0]) + u[1] * (p[1] - point[1]) + u[2] * (p[2] - point[2]);
+                    if (fabs(d) > 0.5 * thickness) continue;
+                    if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) continue;
+                    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, m + 3 * c) != 0)
+                        return -1;
+                }
+    mat->version++;
+    return 0;
+}
+
+int fdtd_b200_materials_set_dispersive_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0,
+                                           size_t j1, size_t k0, size_t k1, const fdtd_b200_dispersive_t *model) {
+    double v[DISP_W];
+    if (!model || pack_model(model, v) != 0 || !box_valid(mat, g, i0, i1, j0, j1, k0, k1)) return -1;
+    for (size_t i = i0; i < i1; i++)
+        for (size_t j = j0; j < j1; j++)
+            for (size_t k = k0; k < k1; k++)
+                for (int c = 0; c < 3; c++) {
+                    if (!component_valid(g, c, i, j, k)) continue;
+                    if (omap_put(&mat->disp, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, v) != 0) return -1;
+                }
+    mat->version++;
+    return 0;
+}
+
 int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g, field_component_t component,
                                      size_t i, size_t j, size_t k, double row[3]) {
     int c = component_number(component);

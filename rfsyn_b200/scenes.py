@@ -82,6 +82,11 @@ class Workload:
     # None or (eps_inf, sigma, poles) with poles as in rfsyn_b200.dispersive
     spheres: list = field(default_factory=list)
     smoothing: int = 1
+    # staircased anisotropic slabs (point[3], normal[3], thickness, eps_r 3x3),
+    # dispersive boxes (i0,i1,j0,j1,k0,k1, model as for spheres), a plane wave
+    slabs: list = field(default_factory=list)
+    disp_boxes: list = field(default_factory=list)
+    plane_wave: dict | None = None
 
     @property
     def dt(self) -> float:
@@ -202,15 +207,64 @@ def c4(seed: int = 4, n_scenes: int = 512, precision: int = FP32, n_steps: int =
 
 
 def scene_setup(w: Workload):
-    """The workload's boxes and spheres as a setup callback (None when it has
-    neither)."""
-    if not w.boxes and not w.spheres:
+    """The workload's boxes, spheres, dispersive boxes and anisotropic slabs
+    as a setup callback (None when it has none)."""
+    if not (w.boxes or w.spheres or w.slabs or w.disp_boxes):
         return None
     from . import SceneSetup, dispersive
 
     rows = [(cx, cy, cz, r, eps, sig, None if model is None else dispersive(*model))
             for (cx, cy, cz, r, eps, sig, model) in w.spheres]
-    return SceneSetup(w.boxes, rows, w.smoothing)
+    return SceneSetup(w.boxes, rows, w.smoothing, slabs=w.slabs,
+                      disp_boxes=[(*b[:6], dispersive(*b[6])) for b in w.disp_boxes])
+
+
+def _gauss(rng: Pcg32) -> float:
+    """Standard normal from two PCG32 uniforms (Box-Muller)."""
+    u1 = max(rng.uniform(), 1e-12)
+    return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * rng.uniform())
+
+
+def c3(seed: int = 3, precision: int = FP32, nx: int = 128, ny: int = 128, nz: int = 512, n_steps: int = 6000,
+       npml: int = 16, dx: float = 0.5e-3, grid_probes: int = 8) -> Workload:
+    """Periodic unit cell nx x ny x nz (periodic x / y, npml-cell CPML in z),
+    dx 0.5 mm.  A plane wave at normal incidence (a non-normal wave is not
+    periodic in x / y) with a PCG32(seed) polarisation angle, through a TF/SF
+    boundary 4 cells inside the CPML; a Gaussian-modulated sinusoid f0 12 GHz,
+    tau = 2/(pi 16 GHz), t0 = 4 tau.  One tilted slab (seeded normal within
+    45 deg of z, thickness U[20,60] cells, centred at 0.55 nz) of a full 3x3
+    eps_r: eigenvalues U[2,10] rotated by the QR factor of a seeded Gaussian
+    matrix.  A 12-cell 2-pole Lorentz layer at 0.3 nz (f_p U[5,20] GHz,
+    gamma 2 pi U[0.1,1] GHz, delta_eps U[0.5,3]).  Reflection plane (Ex,
+    grid_probes^2 points, scattered region below the boundary) and
+    transmission plane (Ex, grid_probes^2 points near the top); 512 DFT bins
+    over 2..24 GHz; n_steps steps."""
+    rng = Pcg32(seed, 0)
+    psi = rng.range(0.0, math.pi)
+    th, ph = rng.range(0.0, math.pi / 4), rng.range(0.0, 2.0 * math.pi)
+    normal = [math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)]
+    thick = rng.range(20.0, 60.0)
+    lam = [rng.range(2.0, 10.0) for _ in range(3)]
+    G = np.array([[_gauss(rng) for _ in range(3)] for _ in range(3)])
+    Q, _ = np.linalg.qr(G)
+    eps = Q @ np.diag(lam) @ Q.T
+    eps = 0.5 * (eps + eps.T)
+    poles = [("lorentz", rng.range(0.5, 3.0), 2.0 * math.pi * rng.range(5e9, 20e9),
+              2.0 * math.pi * rng.range(0.1e9, 1e9)) for _ in range(2)]
+    zl = int(0.3 * nz)
+    tau = 2.0 / (math.pi * 16e9)
+    k0, k1 = npml + 4, nz - npml - 4
+    pw = dict(theta=0.0, phi=0.0, psi=psi, amplitude=1.0, waveform=WAVE_MOD_GAUSSIAN, p0=12e9, p1=4.0 * tau,
+              p2=tau, i0=0, i1=nx - 1, j0=0, j1=ny - 1, k0=k0, k1=k1)
+    g = grid_probes
+    pts = [(int((a + 0.5) * nx / g), int((b + 0.5) * ny / g)) for a in range(g) for b in range(g)]
+    probes = [dict(i=i, j=j, k=npml + 2, component=FIELD_EX) for (i, j) in pts]
+    probes += [dict(i=i, j=j, k=k1 - 8, component=FIELD_EX) for (i, j) in pts]
+    return Workload(
+        name=f"c3_{nx}x{ny}x{nz}_periodic_tfsf_aniso_lorentz", nx=nx, ny=ny, nz=nz, dx=dx, n_steps=n_steps,
+        npml=npml, periodic=3, precision=precision, probes=probes, freqs=list(np.linspace(2e9, 24e9, 512)),
+        slabs=[([0.5 * nx, 0.5 * ny, 0.55 * nz], normal, thick, eps.ravel().tolist())],
+        disp_boxes=[(0, nx, 0, ny, zl, zl + 12, (1.0, 0.0, poles))], plane_wave=pw)
 
 
 def scaled(w: Workload, n: int, n_steps: int) -> Workload:
@@ -248,4 +302,4 @@ def run_config(w: Workload):
     return RunConfig(w.nx, w.ny, w.nz, w.dx, w.n_steps, w.npml, courant=w.courant, periodic=w.periodic,
                      precision=w.precision, schedule=w.schedule,
                      cpml=CpmlParams(w.npml, w.m, w.ma, w.kappa_max, w.alpha_max, w.r0),
-                     sources=w.sources, probes=w.probes, freqs=w.freqs)
+                     sources=w.sources, probes=w.probes, freqs=w.freqs, plane_wave=w.plane_wave)

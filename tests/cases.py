@@ -64,6 +64,38 @@ def simulate_unit_cfg() -> rb.FdtdSimConfig:
     return c
 
 
+def slab_rows(w: scenes.Workload) -> list:
+    """The 3x3 rows the product's slab helper gives the workload's slabs
+    (host API only), as the oracle's explicit samples."""
+    lib = rb.load()
+    lib.fdtd_grid_create.restype = C.c_void_p
+    lib.fdtd_grid_create.argtypes = [C.c_size_t] * 3 + [C.c_double, C.c_double]
+    lib.fdtd_grid_set_periodic.argtypes = [C.c_void_p, C.c_uint]
+    lib.materials_create.restype = C.c_void_p
+    lib.materials_create.argtypes = [C.c_void_p]
+    lib.materials_destroy.argtypes = [C.c_void_p]
+    lib.fdtd_grid_destroy.argtypes = [C.c_void_p]
+    lib.fdtd_b200_materials_get_tensor3.argtypes = [C.c_void_p, C.c_void_p, C.c_int] + [C.c_size_t] * 3 + \
+        [C.POINTER(C.c_double)]
+    g = lib.fdtd_grid_create(w.nx, w.ny, w.nz, w.dx, w.courant)
+    lib.fdtd_grid_set_periodic(g, w.periodic)
+    m = lib.materials_create(g)
+    st = rb.SceneSetup(slabs=w.slabs)
+    assert st.fn(g, m, None) == 0
+    rows = []
+    row = (C.c_double * 3)()
+    ext = [n + (0 if (w.periodic >> a) & 1 else 1) for a, n in enumerate((w.nx, w.ny, w.nz))]
+    for i in range(ext[0]):
+        for j in range(ext[1]):
+            for k in range(ext[2]):
+                for c in range(3):
+                    if lib.fdtd_b200_materials_get_tensor3(m, g, c, i, j, k, row) == 0:
+                        rows.append((c, i, j, k, tuple(row)))
+    lib.materials_destroy(m)
+    lib.fdtd_grid_destroy(g)
+    return rows
+
+
 def workload_to_scene(w: scenes.Workload) -> Scene:
     from oracle import MODEL_ONLY, disp_entry
 
@@ -74,14 +106,22 @@ def workload_to_scene(w: scenes.Workload) -> Scene:
             idx = len(disp)
             disp.append(disp_entry(0, MODEL_ONLY, 0, 0, model[0], model[1], model[2]))
         spheres.append((cx, cy, cz, r, eps, sig, idx))
-    return Scene(
+    sc = Scene(
         nx=w.nx, ny=w.ny, nz=w.nz, dx=w.dx, courant=w.courant, n_steps=w.n_steps, periodic=w.periodic,
         npml=w.npml, m=w.m, ma=w.ma, kappa_max=w.kappa_max, alpha_max=w.alpha_max, r0=w.r0,
         boxes=list(w.boxes), comps=list(w.comps), disp=disp, spheres=spheres, smoothing=w.smoothing,
         sources=[(s["i"], s["j"], s["k"], s["component"], s["mode"], s["amplitude"], s["waveform"], s["p0"],
                   s["p1"], s.get("p2", 0.0)) for s in w.sources],
         probes=[(p["i"], p["j"], p["k"], p["component"]) for p in w.probes], freqs=list(w.freqs),
-        src_t_offset=0.0, dft_t_offset=1.0)
+        src_t_offset=0.0, dft_t_offset=1.0, plane_wave=w.plane_wave,
+        tensor3=slab_rows(w) if w.slabs else [])
+    for (i0, i1, j0, j1, k0, k1, model) in w.disp_boxes:
+        for i in range(i0, i1):
+            for j in range(j0, j1):
+                for k in range(k0, k1):
+                    for c in range(3):
+                        sc.disp.append(disp_entry(c, i, j, k, model[0], model[1], model[2]))
+    return sc
 
 
 def c1_scene() -> Scene:
