@@ -3,8 +3,13 @@ parameter vector to its complex tx -> rx transfer function, trained on
 data the batched FDTD generates, with plain FDTD as the fallback whenever
 the ensemble disagrees.  rfsyn has no learned component.
 
-Scene vector (54 values): 8 scatterers x (x, y, z, radius, eps_r, log10
-sigma), zero-padded, then the tx and rx positions, all scaled to O(1).
+Scene vector (54 values): 8 scatterers x 6 values, zero-padded, then the
+tx position and the rx - tx vector, all scaled to O(1).  Each scatterer is
+described relative to the tx / rx pair -- its distances to both, its excess
+path length over the direct path, its radius, eps_r and log10 sigma -- and
+the scatterers are sorted by excess path length, so that the network sees a
+canonical order (the field at the receiver does not depend on the order in
+which scatterers are listed).
 Output (512 values): the de-embedded transfer function
     G(f) = H(f) / Ez_free(f; d, theta)
 at 256 bins, real parts then imaginary parts, divided by one scale learned
@@ -78,11 +83,22 @@ def features(w: sc.Workload, rx: int) -> np.ndarray:
     """The 54-value scene vector of receiver rx."""
     n = float(w.nx)
     f = np.zeros(N_FEAT, dtype=np.float64)
-    for q, (cx, cy, cz, r, eps, sig, _) in enumerate(w.spheres[:N_SCAT]):
-        f[6 * q: 6 * q + 6] = (cx / n, cy / n, cz / n, r / n, (eps - 1.0) / 9.0, (math.log10(sig) + 4.0) / 4.0)
     s, p = w.sources[0], w.probes[rx]
-    f[48:51] = (s["i"] / n, s["j"] / n, s["k"] / n)
-    f[51:54] = (p["i"] / n, p["j"] / n, p["k"] / n)
+    tx = np.array([s["i"], s["j"], s["k"]], dtype=np.float64)
+    rv = np.array([p["i"], p["j"], p["k"]], dtype=np.float64)
+    direct = float(np.linalg.norm(rv - tx))
+    rows = []
+    for (cx, cy, cz, r, eps, sig, _) in w.spheres[:N_SCAT]:
+        c = np.array([cx, cy, cz])
+        dt_, dr_ = float(np.linalg.norm(c - tx)), float(np.linalg.norm(c - rv))
+        excess = dt_ + dr_ - direct
+        rows.append((excess, (dt_ / n, dr_ / n, excess / n, r / n, (eps - 1.0) / 9.0,
+                              (math.log10(sig) + 4.0) / 4.0)))
+    rows.sort(key=lambda t: t[0])
+    for q, (_, v) in enumerate(rows):
+        f[6 * q: 6 * q + 6] = v
+    f[48:51] = tx / n
+    f[51:54] = (rv - tx) / n
     return f
 
 
