@@ -35,6 +35,14 @@ TRAFFIC = ROOT / "profiles" / "sweep_queue_c2.md"
 METRIC = "Mcell-updates/s"
 
 
+SWEEP_KERNEL = {
+    0: "k_sweep_interior + k_sweep_edge (one H+E sweep, cp.async ring)",
+    1: "k_sweep_interior_tma + k_sweep_edge (one H+E sweep)",
+    2: "k_sweep_q (one H+E sweep: interior + x-slab + edge launches)",
+    3: "k_sweep_q (one H+E sweep: interior + x-slab + edge launches, shifted tiles)",
+}
+
+
 def hbm_peak() -> tuple[float, str]:
     try:
         return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
@@ -272,7 +280,8 @@ def run_b200(args) -> None:
     alg = algorithmic_bytes_per_sweep(info, esz)
     peak, peak_kind = hbm_peak()
     achieved = alg / (sweep_launch_ms / 1e3) / 1e9
-    traffic = ncu_traffic_per_launch()
+    # the committed ncu capture covers the C2 scene's queue sweep only
+    traffic = ncu_traffic_per_launch() if args.workload == "c2" and info.tma >= 2 else None
     sim.close()
 
     # end to end through the C ABI with host buffers: setup on the host,
@@ -307,6 +316,7 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
     if rank != 0:
         return
+    field_mb = (w.nx + 1) * (w.ny + 1) * (w.nz + 1) * esz / 1e6
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -320,9 +330,9 @@ def run_b200(args) -> None:
                    "sweep_mode": {0: "cp.async", 1: "tma-interior", 2: "tma-queue", 3: "tma-queue-shifted"}.get(info.tma),
                    "ring_depth": info.ring_depth,
                    "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
-                   "l2": "inputs larger than L2 (fields 6 x 2 x 76 MB per scene)"},
+                   "l2": f"inputs larger than L2 (fields 6 x 2 x {field_mb:.0f} MB per scene)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "kernel": "k_sweep_q (one H+E sweep: interior + x-slab + edge launches)",
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": SWEEP_KERNEL.get(info.tma, "k_h_split + k_e_split"),
                      "algorithmic_bytes_per_launch": alg, "launch_ms": sweep_launch_ms,
                      "other_kernels_ms_per_step": other_ms / 200},
         "cpu_baseline": cpu,

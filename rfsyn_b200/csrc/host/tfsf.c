@@ -173,6 +173,16 @@ int rfb_tfsf_build(const fdtd_grid_t *g, const materials_t *mat, const fdtd_b200
     }
     tf_geo_t t;
     tf_geometry(g, pw, &t);
+    for (int a = 0; a < 3; a++) {
+        /* a wave with a component of k along a periodic axis has a phase
+         * shift across the period (Floquet); without that boundary the
+         * wrapped grid would not carry it */
+        if ((t.per & (1u << a)) && fabs(t.k[a]) > 1e-12) {
+            rfb_set_error("plane wave: oblique incidence along periodic axis %d is not supported (normal incidence "
+                          "only along periodic axes)", a);
+            return -1;
+        }
+    }
     const long n[3] = {(long)g->nx, (long)g->ny, (long)g->nz};
     long lo[3], hi[3];
     const size_t bl[3] = {pw->i0, pw->j0, pw->k0}, bh[3] = {pw->i1, pw->j1, pw->k1};

@@ -94,3 +94,15 @@ def test_device_fp32_within_bound():
     got = run_device(s, rb.FP32, rb.FUSED)["td"]
     scale = np.abs(want).max()
     assert np.abs(got - want).max() / scale < 1e-3
+
+
+def test_oblique_incidence_along_a_periodic_axis_is_rejected():
+    # host-side check before any device work (runs without a GPU): a k
+    # component along a wrapped axis would need Floquet boundaries
+    from tests.cases import scene_run_config
+
+    s = Scene(nx=8, ny=6, nz=60, n_steps=10, periodic=3, npml=8,
+              plane_wave=dict(theta=math.radians(20), phi=0.0, psi=0.0, amplitude=1.0, i0=0, i1=7, j0=0, j1=5,
+                              k0=20, k1=40, **GD), probes=[(2, 2, 15, 0)])
+    with pytest.raises(RuntimeError, match="periodic axis 0"):
+        rb.run(scene_run_config(s, rb.FP64, rb.FUSED))
