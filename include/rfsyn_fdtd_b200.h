@@ -53,18 +53,22 @@ typedef struct {
  * counterpart in rfsyn, whose validators drive soft sheets or modal lines,
  * engine/fdtd/validation_common.h:16-18).  Direction k = (sin t cos p,
  * sin t sin p, cos t) for theta t, phi p (radians); E along
- * cos(psi) theta_hat + sin(psi) phi_hat; E(t) = amplitude * waveform at the
- * box corner the wave reaches first (waveform and p0..p2 as for sources,
- * samples not allowed).  The total field fills the box of sample positions
+ * cos(psi) theta_hat + sin(psi) phi_hat; amplitude * waveform(t) drives
+ * the line's source (waveform and p0..p2 as for sources, samples not
+ * allowed).  The total field fills the box of sample positions
  * [i0, i1] x [j0, j1] x [k0, k1] (cell units; the whole axis on a periodic
  * axis); the box grown by two cells must lie outside the CPML and inside
  * the grid, in scalar media.  The incident field comes from a 1-D FDTD line
- * along k with the grid's dx and dt, interpolated linearly at each sample's
- * projected distance (Taflove & Hagness, Computational Electrodynamics 3rd
- * ed., ch. 5); at normal incidence the injection is exact, at oblique
- * incidence the scattered region carries the 1-D / 3-D dispersion mismatch.
- * On a periodic axis a non-normal wave is not periodic: use normal
- * incidence there. */
+ * along k with the grid's dt and spacing dx sqrt(sum_a k_a^4), which gives
+ * it the grid's numerical phase velocity along k to second order in k dx,
+ * read by cubic interpolation at each sample's projected distance (Taflove
+ * & Hagness, Computational Electrodynamics 3rd ed., ch. 5).  At normal
+ * incidence and along a body diagonal the injection is exact; at other
+ * angles the scattered region sees about -60 dB of the incident peak at 17
+ * cells per wavelength.  The line's source sits 8 line cells before the
+ * first corner, so E there is the waveform delayed by that distance.  A
+ * wave with a component of k along a periodic axis is rejected (no Floquet
+ * boundaries). */
 typedef struct {
     double theta, phi, psi;
     double amplitude;

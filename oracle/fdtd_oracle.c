@@ -28,7 +28,10 @@
  *                                  full row of eps_r^-1, off-diagonal curls
  *                                  averaged over the four surrounding samples
  *   plane wave, TF/SF boundary ... Taflove & Hagness 3rd ed. ch. 5: a 1-D
- *                                  incident line, corrections generated from
+ *                                  incident line with spacing
+ *                                  dx sqrt(sum k_a^4) (the grid's dispersion
+ *                                  along k to second order), cubic Lagrange
+ *                                  interpolation, corrections generated from
  *                                  the update stencils (the product's term
  *                                  order, restated)
  * The data structures are the plainest possible (dense per-component override
@@ -82,7 +85,7 @@ typedef struct {
     int *tf_hc, *tf_hfirst, *tf_hcount;
     int *tf_efirst[3], *tf_ecount[3];
     size_t tf_nt, tf_tcap;
-    double *tf_coef, *tf_w0, *tf_w1;
+    double *tf_coef, *tf_w;   /* 4 weights per term */
     int *tf_idx;
 } orc_t;
 
@@ -139,7 +142,7 @@ static void orc_free(orc_t *o) {
     for (int c = 0; c < 3; c++) free(o->dix[c]), free(o->has_t3[c]), free(o->t3m[c]);
     for (int c = 0; c < 3; c++) free(o->tf_efirst[c]), free(o->tf_ecount[c]);
     free(o->tf_e); free(o->tf_h); free(o->tf_src); free(o->tf_hw); free(o->tf_hc); free(o->tf_hfirst);
-    free(o->tf_hcount); free(o->tf_coef); free(o->tf_w0); free(o->tf_w1); free(o->tf_idx);
+    free(o->tf_hcount); free(o->tf_coef); free(o->tf_w); free(o->tf_idx);
     free(o->drec);
     free(o->dst);
     free(o->id);
@@ -279,6 +282,7 @@ static void tf_pos(int comp, const long p[3], double out[3]) {
 
 typedef struct {
     double lo[3], hi[3], k[3], e[3], h[3], ref[3];
+    double r;   /* line spacing / dx */
     unsigned per;
 } tf_t;
 
@@ -291,23 +295,26 @@ static int tf_in(const tf_t *t, const double p[3]) {
 static double tf_s(const tf_t *t, const double p[3]) {
     double s = 0.0;
     for (int a = 0; a < 3; a++) s += t->k[a] * (p[a] - t->ref[a]);
-    return s + 4.0;
+    return s / t->r + 8.0;
 }
 
 static int tf_term(orc_t *o, double coef, double s) {
     if (o->tf_nt == o->tf_tcap) {
         o->tf_tcap = o->tf_tcap ? 2 * o->tf_tcap : 256;
         o->tf_coef = realloc(o->tf_coef, o->tf_tcap * 8);
-        o->tf_w0 = realloc(o->tf_w0, o->tf_tcap * 8);
-        o->tf_w1 = realloc(o->tf_w1, o->tf_tcap * 8);
+        o->tf_w = realloc(o->tf_w, 4 * o->tf_tcap * 8);
         o->tf_idx = realloc(o->tf_idx, o->tf_tcap * sizeof(int));
-        if (!o->tf_coef || !o->tf_w0 || !o->tf_w1 || !o->tf_idx) return -1;
+        if (!o->tf_coef || !o->tf_w || !o->tf_idx) return -1;
     }
-    double f = floor(s);
+    /* cubic Lagrange weights of line samples f-1 .. f+2 at u = s - f */
+    double f = floor(s), u = s - f;
+    double *w = o->tf_w + 4 * o->tf_nt;
     o->tf_coef[o->tf_nt] = coef;
     o->tf_idx[o->tf_nt] = (int)f;
-    o->tf_w1[o->tf_nt] = s - f;
-    o->tf_w0[o->tf_nt] = 1.0 - (s - f);
+    w[0] = -u * (u - 1.0) * (u - 2.0) / 6.0;
+    w[1] = (u + 1.0) * (u - 1.0) * (u - 2.0) / 2.0;
+    w[2] = -(u + 1.0) * u * (u - 2.0) / 2.0;
+    w[3] = (u + 1.0) * u * (u - 1.0) / 6.0;
     o->tf_nt++;
     return 0;
 }
@@ -330,6 +337,8 @@ static int tf_init(orc_t *o, const scn_scene_t *s) {
     t.h[0] = t.k[1] * t.e[2] - t.k[2] * t.e[1];
     t.h[1] = t.k[2] * t.e[0] - t.k[0] * t.e[2];
     t.h[2] = t.k[0] * t.e[1] - t.k[1] * t.e[0];
+    t.r = sqrt(t.k[0] * t.k[0] * (t.k[0] * t.k[0]) + t.k[1] * t.k[1] * (t.k[1] * t.k[1]) +
+               t.k[2] * t.k[2] * (t.k[2] * t.k[2]));
     const size_t bl[3] = {pw->i0, pw->j0, pw->k0}, bh[3] = {pw->i1, pw->j1, pw->k1};
     long lo[3], hi[3];
     for (int a = 0; a < 3; a++) {
@@ -428,9 +437,9 @@ static int tf_init(orc_t *o, const scn_scene_t *s) {
                 }
             }
     double cps = O_C0 * o->dt / o->dx;
-    o->tf_len = (size_t)ceil(smax) + 4 + (size_t)ceil((double)s->n_steps * cps) + 4;
-    o->tf_ce = o->dt / (O_EPS0 * o->dx);
-    o->tf_ch = cbh;
+    o->tf_len = (size_t)ceil(smax) + 4 + (size_t)ceil((double)s->n_steps * cps / t.r) + 4;
+    o->tf_ce = o->dt / (O_EPS0 * (o->dx * t.r));
+    o->tf_ch = o->dt / (O_MU0 * (o->dx * t.r));
     o->tf_e = calloc(o->tf_len, 8);
     o->tf_h = calloc(o->tf_len, 8);
     o->tf_src = malloc((s->n_steps + 1) * 8);
@@ -451,7 +460,9 @@ static void tf_after_h(orc_t *o) {
         double h = *f;
         for (int t = o->tf_hfirst[q]; t < o->tf_hfirst[q] + o->tf_hcount[q]; t++) {
             int m = o->tf_idx[t];
-            h = h + o->tf_coef[t] * (o->tf_w0[t] * o->tf_e[m] + o->tf_w1[t] * o->tf_e[m + 1]);
+            const double *w = o->tf_w + 4 * t;
+            h = h + o->tf_coef[t] * (w[0] * o->tf_e[m - 1] + w[1] * o->tf_e[m] + w[2] * o->tf_e[m + 1] +
+                                     w[3] * o->tf_e[m + 2]);
         }
         *f = h;
     }
@@ -740,7 +751,9 @@ static void update_e(orc_t *o) {
                         double v = o->E[c][here];
                         for (int t = o->tf_efirst[c][here]; t < o->tf_efirst[c][here] + o->tf_ecount[c][here]; t++) {
                             int m = o->tf_idx[t];
-                            v = v + o->tf_coef[t] * (o->tf_w0[t] * o->tf_h[m] + o->tf_w1[t] * o->tf_h[m + 1]);
+                            const double *w = o->tf_w + 4 * t;
+                            v = v + o->tf_coef[t] * (w[0] * o->tf_h[m - 1] + w[1] * o->tf_h[m] +
+                                                     w[2] * o->tf_h[m + 1] + w[3] * o->tf_h[m + 2]);
                         }
                         o->E[c][here] = v;
                     }

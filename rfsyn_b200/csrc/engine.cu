@@ -419,9 +419,9 @@ struct rfb_engine {
     void *tf_inc_e = nullptr, *tf_inc_h = nullptr, *tf_src = nullptr;
     long long *tf_h_cell = nullptr;
     int *tf_h_comp = nullptr, *tf_h_first = nullptr, *tf_h_count = nullptr, *tf_h_idx = nullptr;
-    void *tf_h_coef = nullptr, *tf_h_w0 = nullptr, *tf_h_w1 = nullptr;
+    void *tf_h_coef = nullptr, *tf_h_w = nullptr;
     int *tf_e_first = nullptr, *tf_e_count = nullptr, *tf_e_idx = nullptr;
-    void *tf_e_coef = nullptr, *tf_e_w0 = nullptr, *tf_e_w1 = nullptr;
+    void *tf_e_coef = nullptr, *tf_e_w = nullptr;
     int active = 0;          // a source sits on a padded boundary plane
     int member = 0;          // scene of a batch: no plan, graphs or second stream of its own
 };
@@ -449,8 +449,7 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
         a.tf_count = e->tf_e_count;
         a.tf_idx = e->tf_e_idx;
         a.tf_coef = (const T *)e->tf_e_coef;
-        a.tf_w0 = (const T *)e->tf_e_w0;
-        a.tf_w1 = (const T *)e->tf_e_w1;
+        a.tf_w = (const T *)e->tf_e_w;
         a.inc_h = (const T *)e->tf_inc_h;
     }
     return a;
@@ -468,8 +467,7 @@ static TfArgs<T> tf_args(const rfb_engine *e, int par) {
     t.h_count = e->tf_h_count;
     t.h_idx = e->tf_h_idx;
     t.h_coef = (const T *)e->tf_h_coef;
-    t.h_w0 = (const T *)e->tf_h_w0;
-    t.h_w1 = (const T *)e->tf_h_w1;
+    t.h_w = (const T *)e->tf_h_w;
     for (int c = 0; c < 3; c++) t.Ho[c] = (T *)e->fld[out][3 + c];
     t.inc_e = (T *)e->tf_inc_e;
     t.inc_h = (T *)e->tf_inc_h;
@@ -963,9 +961,9 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
     cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_qx); cudaFree(e->plan.d_queue);
     cudaFree(e->tf_inc_e); cudaFree(e->tf_inc_h); cudaFree(e->tf_src); cudaFree(e->tf_h_cell); cudaFree(e->tf_h_comp);
-    cudaFree(e->tf_h_first); cudaFree(e->tf_h_count); cudaFree(e->tf_h_idx); cudaFree(e->tf_h_coef); cudaFree(e->tf_h_w0);
-    cudaFree(e->tf_h_w1); cudaFree(e->tf_e_first); cudaFree(e->tf_e_count); cudaFree(e->tf_e_idx); cudaFree(e->tf_e_coef);
-    cudaFree(e->tf_e_w0); cudaFree(e->tf_e_w1);
+    cudaFree(e->tf_h_first); cudaFree(e->tf_h_count); cudaFree(e->tf_h_idx); cudaFree(e->tf_h_coef); cudaFree(e->tf_h_w);
+    cudaFree(e->tf_e_first); cudaFree(e->tf_e_count); cudaFree(e->tf_e_idx); cudaFree(e->tf_e_coef);
+    cudaFree(e->tf_e_w);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->stream2) cudaStreamDestroy(e->stream2);
@@ -1151,10 +1149,9 @@ extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
         e->tf_h_count = dev_copy(d->h_count, d->n_h);
         e->tf_h_idx = dev_copy(d->h_idx, d->n_hterms);
         e->tf_h_coef = dev_upload_conv(d->h_coef, d->n_hterms, prec);
-        e->tf_h_w0 = dev_upload_conv(d->h_w0, d->n_hterms, prec);
-        e->tf_h_w1 = dev_upload_conv(d->h_w1, d->n_hterms, prec);
+        e->tf_h_w = dev_upload_conv(d->h_w, 4 * d->n_hterms, prec);
         if (!e->tf_h_cell || !e->tf_h_comp || !e->tf_h_first || !e->tf_h_count || !e->tf_h_idx || !e->tf_h_coef ||
-            !e->tf_h_w0 || !e->tf_h_w1)
+            !e->tf_h_w)
             goto fail;
     }
     if (ne) {
@@ -1165,9 +1162,8 @@ extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
     if (d->n_eterms) {
         e->tf_e_idx = dev_copy(d->e_idx, d->n_eterms);
         e->tf_e_coef = dev_upload_conv(d->e_coef, d->n_eterms, prec);
-        e->tf_e_w0 = dev_upload_conv(d->e_w0, d->n_eterms, prec);
-        e->tf_e_w1 = dev_upload_conv(d->e_w1, d->n_eterms, prec);
-        if (!e->tf_e_idx || !e->tf_e_coef || !e->tf_e_w0 || !e->tf_e_w1) goto fail;
+        e->tf_e_w = dev_upload_conv(d->e_w, 4 * d->n_eterms, prec);
+        if (!e->tf_e_idx || !e->tf_e_coef || !e->tf_e_w) goto fail;
     }
     e->tf_on = 1;
     // graphs captured before the plane wave would lack its kernels
@@ -1177,7 +1173,7 @@ extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
         e->g1[q] = e->gk[q] = nullptr;
     }
     e->launches_per_step = count_step_launches(e);
-    e->h2d_bytes += (size_t)(e->n_steps + 1) * e->esz + d->n_h * 24 + (d->n_hterms + d->n_eterms) * (3 * e->esz + 4) +
+    e->h2d_bytes += (size_t)(e->n_steps + 1) * e->esz + d->n_h * 24 + (d->n_hterms + d->n_eterms) * (5 * e->esz + 4) +
                     ne * 8;
     return 0;
 fail:

@@ -163,7 +163,7 @@ typedef struct {
     size_t n_h;
     const int32_t *h_ijkc, *h_first, *h_count;
     size_t n_hterms, n_eterms;
-    const double *h_coef, *h_w0, *h_w1, *e_coef, *e_w0, *e_w1;
+    const double *h_coef, *h_w, *e_coef, *e_w;  /* w: 4 weights per term */
     const int32_t *h_idx, *e_idx;
     const int32_t *entry_first, *entry_count;  /* 3 * n_cells of the scene image */
 } rfb_tfsf_desc_t;

@@ -76,14 +76,14 @@ int rfb_e_swept(const fdtd_grid_t *g, int c, size_t i, size_t j, size_t k);
  * samples (applied by the interface-list kernel). */
 typedef struct {
     size_t m_len;            /* E samples of the line (H: m_len - 1) */
-    double ce, ch;           /* dt / (eps0 dx), dt / (mu0 dx) */
+    double ce, ch;           /* dt / (eps0 d1), dt / (mu0 d1), d1 the line spacing */
     double *src;             /* E1D[0] at steps 0 .. n_steps */
     size_t n_h;              /* H targets: i, j, k, comp; first term, count */
     int32_t *h_ijkc, *h_first, *h_count;
     size_t n_e;              /* E targets, likewise */
     int32_t *e_ijkc, *e_first, *e_count;
     size_t n_hterms, n_eterms;
-    double *h_coef, *h_w0, *h_w1, *e_coef, *e_w0, *e_w1;
+    double *h_coef, *h_w, *e_coef, *e_w;   /* w: 4 cubic weights per term */
     int32_t *h_idx, *e_idx;
     size_t n_cells;          /* cells whose E samples go on the interface list */
     int32_t *cells;

@@ -291,8 +291,8 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
         td.h_count = tf.h_count;
         td.n_hterms = tf.n_hterms;
         td.n_eterms = tf.n_eterms;
-        td.h_coef = tf.h_coef; td.h_w0 = tf.h_w0; td.h_w1 = tf.h_w1; td.h_idx = tf.h_idx;
-        td.e_coef = tf.e_coef; td.e_w0 = tf.e_w0; td.e_w1 = tf.e_w1; td.e_idx = tf.e_idx;
+        td.h_coef = tf.h_coef; td.h_w = tf.h_w; td.h_idx = tf.h_idx;
+        td.e_coef = tf.e_coef; td.e_w = tf.e_w; td.e_idx = tf.e_idx;
         td.entry_first = tf_first;
         td.entry_count = tf_count;
         if (rfb_engine_set_tfsf(sim->eng, &td) != 0) {

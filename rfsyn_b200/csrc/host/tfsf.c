@@ -3,11 +3,21 @@
  * No counterpart in rfsyn.  The incident field comes from a 1-D FDTD line
  * along the propagation direction k (Taflove & Hagness, Computational
  * Electrodynamics 3rd ed., ch. 5, the incident-field-array method): E1D at
- * integer positions m dx, H1D at (m + 1/2) dx, the same dt and dx as the
- * grid, a hard source at m = 0.  A grid sample at position p (cell units)
- * sees the incident field at s = k . (p - r_ref) + M0 on the line (r_ref the
- * corner of the total-field box the wave reaches first), interpolated
- * linearly.
+ * integer positions m d1, H1D at (m + 1/2) d1, the grid's dt, a hard source
+ * at m = 0.  A grid sample at position p (cell units) sees the incident
+ * field at s = k . (p - r_ref) dx / d1 + M0 on the line (r_ref the corner of
+ * the total-field box the wave reaches first), interpolated by a cubic
+ * Lagrange polynomial through the four line samples around s.
+ *
+ * Line spacing (dispersion matching): the Yee grid's numerical dispersion
+ * along k, 4/dx^2 sum_a sin^2(k k_a dx / 2), expands to
+ * k^2 - k^4 dx^2 / 12 sum_a k_a^4, and the line's to k^2 - k^4 d1^2 / 12, so
+ * d1 = dx sqrt(sum_a k_a^4) gives both the same phase velocity to second
+ * order in k dx; the time-discretisation term is the same for both (same
+ * dt).  Along an axis d1 = dx and every s is a whole or half line cell, so
+ * normal incidence is injected exactly; along a body diagonal d1 = dx / sqrt 3
+ * and the line reproduces the grid exactly as well.  sum_a k_a^4 >= 1/3, so
+ * c dt / d1 <= courant_safety and the line is stable whenever the grid is.
  *
  * Corrections, generated from the update stencils themselves so that edges
  * and corners need no special cases:
@@ -15,18 +25,22 @@
  *   the other side of the boundary: + Cb sigma (+1 inside / -1 outside) H_inc(q);
  *   H_c update (H -= cbh (dA - dB)) of a sample whose E neighbour q lies on
  *   the other side: - cbh sigma (+1 inside / -1 outside) E_inc(q);
- * sigma the sign of q in the stencil.  Each term is coef * (w0 X[idx] +
- * w1 X[idx + 1]) with X the 1-D line's E (for H targets) or H (for E
- * targets) and the unit-vector component folded into coef.  Terms of one
- * target are applied in the order generated here (the oracle restates the
- * same order). */
+ * sigma the sign of q in the stencil.  Each term is
+ * coef * (((w0 X[idx-1] + w1 X[idx]) + w2 X[idx+1]) + w3 X[idx+2]) with X the
+ * 1-D line's E (for H targets) or H (for E targets) and the unit-vector
+ * component folded into coef; its four weights are stored together.  Terms
+ * of one target are applied in the order generated here (the oracle
+ * restates the same order). */
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include "host.h"
 
-#define M0 4.0
+/* line cells between the source and the first box corner: a sample may sit
+ * sqrt(3) cells before that corner, 3 line cells at the smallest d1, and
+ * the cubic stencil reaches one more sample back */
+#define M0 8.0
 #define TF_C0 299792458.0
 #define TF_MU0 1.25663706212e-6
 
@@ -47,6 +61,7 @@ typedef struct {
     unsigned per;
     long n[3];
     double k[3], e[3], h[3], ref[3];
+    double r;   /* line spacing / dx */
 } tf_geo_t;
 
 static int inside(const tf_geo_t *t, const double pos[3]) {
@@ -60,7 +75,7 @@ static int inside(const tf_geo_t *t, const double pos[3]) {
 static double line_pos(const tf_geo_t *t, const double pos[3]) {
     double s = 0.0;
     for (int a = 0; a < 3; a++) s += t->k[a] * (pos[a] - t->ref[a]);
-    return s + M0;
+    return s / t->r + M0;
 }
 
 static void tf_geometry(const fdtd_grid_t *g, const fdtd_b200_plane_wave_t *pw, tf_geo_t *t) {
@@ -80,6 +95,9 @@ static void tf_geometry(const fdtd_grid_t *g, const fdtd_b200_plane_wave_t *pw, 
     t->h[0] = t->k[1] * t->e[2] - t->k[2] * t->e[1];
     t->h[1] = t->k[2] * t->e[0] - t->k[0] * t->e[2];
     t->h[2] = t->k[0] * t->e[1] - t->k[1] * t->e[0];
+    double k4 = 0.0;
+    for (int a = 0; a < 3; a++) k4 += (t->k[a] * t->k[a]) * (t->k[a] * t->k[a]);
+    t->r = sqrt(k4);
     for (int a = 0; a < 3; a++) {
         t->lo[a] = lo[a];
         t->hi[a] = hi[a];
@@ -103,7 +121,7 @@ typedef struct {
 
 typedef struct {
     size_t n, cap;
-    double *coef, *w0, *w1;
+    double *coef, *w;   /* w: 4 weights per term */
     int32_t *idx;
 } terms_t;
 
@@ -112,20 +130,23 @@ static int push_term(terms_t *T, double coef, double s) {
         size_t nc = T->cap ? 2 * T->cap : 256;
         double *a = realloc(T->coef, nc * sizeof(double));
         if (a) T->coef = a;
-        double *b = realloc(T->w0, nc * sizeof(double));
-        if (b) T->w0 = b;
-        double *c = realloc(T->w1, nc * sizeof(double));
-        if (c) T->w1 = c;
+        double *b = realloc(T->w, 4 * nc * sizeof(double));
+        if (b) T->w = b;
         int32_t *d = realloc(T->idx, nc * sizeof(int32_t));
         if (d) T->idx = d;
-        if (!a || !b || !c || !d) return -1;
+        if (!a || !b || !d) return -1;
         T->cap = nc;
     }
-    const double f = floor(s);
+    /* cubic Lagrange weights of the samples idx-1 .. idx+2 at u = s - idx;
+     * u = 0 gives exactly (0, 1, 0, 0) */
+    const double f = floor(s), u = s - f;
+    double *w = T->w + 4 * T->n;
     T->coef[T->n] = coef;
     T->idx[T->n] = (int32_t)f;
-    T->w1[T->n] = s - f;
-    T->w0[T->n] = 1.0 - (s - f);
+    w[0] = -u * (u - 1.0) * (u - 2.0) / 6.0;
+    w[1] = (u + 1.0) * (u - 1.0) * (u - 2.0) / 2.0;
+    w[2] = -(u + 1.0) * u * (u - 2.0) / 2.0;
+    w[3] = (u + 1.0) * u * (u - 1.0) / 6.0;
     T->n++;
     return 0;
 }
@@ -156,8 +177,8 @@ void rfb_tfsf_free(rfb_tfsf_build_t *b) {
     free(b->src);
     free(b->h_ijkc); free(b->h_first); free(b->h_count);
     free(b->e_ijkc); free(b->e_first); free(b->e_count);
-    free(b->h_coef); free(b->h_w0); free(b->h_w1); free(b->h_idx);
-    free(b->e_coef); free(b->e_w0); free(b->e_w1); free(b->e_idx);
+    free(b->h_coef); free(b->h_w); free(b->h_idx);
+    free(b->e_coef); free(b->e_w); free(b->e_idx);
     free(b->cells);
     memset(b, 0, sizeof(*b));
 }
@@ -280,21 +301,21 @@ int rfb_tfsf_build(const fdtd_grid_t *g, const materials_t *mat, const fdtd_b200
             }
     /* every term reads the line inside [0, m_len) */
     for (size_t q = 0; q < HX.n; q++)
-        if (HX.idx[q] < 0) {
+        if (HX.idx[q] < 1) {
             rfb_set_error("plane wave: the line does not reach a boundary sample");
             goto fail;
         }
     for (size_t q = 0; q < EX.n; q++)
-        if (EX.idx[q] < 0) {
+        if (EX.idx[q] < 1) {
             rfb_set_error("plane wave: the line does not reach a boundary sample");
             goto fail;
         }
     {
         const double cells_per_step = TF_C0 * g->dt / g->dx;
-        out->m_len = (size_t)ceil(smax) + 4 + (size_t)ceil((double)n_steps * cells_per_step) + 4;
+        out->m_len = (size_t)ceil(smax) + 4 + (size_t)ceil((double)n_steps * cells_per_step / t.r) + 4;
     }
-    out->ce = g->dt / (8.8541878128e-12 * g->dx);
-    out->ch = cb_h;
+    out->ce = g->dt / (8.8541878128e-12 * (g->dx * t.r));
+    out->ch = g->dt / (TF_MU0 * (g->dx * t.r));
     /* hard source E1D[0] at steps 0..n_steps: amplitude * waveform(n dt) */
     out->src = malloc((n_steps + 1) * sizeof(double));
     if (!out->src) goto oom;
@@ -305,9 +326,9 @@ int rfb_tfsf_build(const fdtd_grid_t *g, const materials_t *mat, const fdtd_b200
     out->n_e = ET.n;
     out->e_ijkc = ET.ijkc; out->e_first = ET.first; out->e_count = ET.count;
     out->n_hterms = HX.n;
-    out->h_coef = HX.coef; out->h_w0 = HX.w0; out->h_w1 = HX.w1; out->h_idx = HX.idx;
+    out->h_coef = HX.coef; out->h_w = HX.w; out->h_idx = HX.idx;
     out->n_eterms = EX.n;
-    out->e_coef = EX.coef; out->e_w0 = EX.w0; out->e_w1 = EX.w1; out->e_idx = EX.idx;
+    out->e_coef = EX.coef; out->e_w = EX.w; out->e_idx = EX.idx;
     /* list cells: every E target, and every E sample reading a corrected H
      * sample: H_c(p) is read by E_{c+1}(p), E_{c+1}(p + e_{c+2}),
      * E_{c+2}(p), E_{c+2}(p + e_{c+1}) */
@@ -340,8 +361,8 @@ oom:
 fail:
     free(HT.ijkc); free(HT.first); free(HT.count);
     free(ET.ijkc); free(ET.first); free(ET.count);
-    free(HX.coef); free(HX.w0); free(HX.w1); free(HX.idx);
-    free(EX.coef); free(EX.w0); free(EX.w1); free(EX.idx);
+    free(HX.coef); free(HX.w); free(HX.idx);
+    free(EX.coef); free(EX.w); free(EX.idx);
     rfb_tfsf_free(out);
     return -1;
 }

@@ -19,6 +19,13 @@ __device__ __forceinline__ float xm(float a, float b) { return __fmul_rn(a, b); 
 __device__ __forceinline__ float xa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float xs(float a, float b) { return __fsub_rn(a, b); }
 
+// The incident line at a TF/SF term: cubic Lagrange interpolation through
+// x[-1] .. x[2] with the term's weights, ((w0 x[-1] + w1 x[0]) + w2 x[1]) + w3 x[2].
+template <typename T>
+__device__ __forceinline__ T tf_interp(const T *w, const T *x) {
+    return xa(xa(xa(xm(w[0], x[-1]), xm(w[1], x[0])), xm(w[2], x[1])), xm(w[3], x[2]));
+}
+
 constexpr int LIST_CODE = 255;
 constexpr int MAX_SKIP = 4;
 
@@ -62,7 +69,7 @@ struct Args {
     // plane-wave boundary: per list entry its first correction term (-1:
     // none) and count; terms coef * (w0 H1D[idx] + w1 H1D[idx + 1])
     const int *tf_first, *tf_count, *tf_idx;
-    const T *tf_coef, *tf_w0, *tf_w1;
+    const T *tf_coef, *tf_w;  // 4 cubic weights per term
     const T *inc_h;          // the incident line's H at n + 1/2
     // sources
     const T *src_val;
@@ -354,7 +361,7 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
         if (f >= 0)
             for (int t = f; t < f + a.tf_count[e]; t++) {
                 const int m = a.tf_idx[t];
-                v = xa(v, xm(a.tf_coef[t], xa(xm(a.tf_w0[t], a.inc_h[m]), xm(a.tf_w1[t], a.inc_h[m + 1]))));
+                v = xa(v, xm(a.tf_coef[t], tf_interp(a.tf_w + 4 * t, a.inc_h + m)));
             }
     }
     a.Eo[comp][c] = v;
@@ -366,7 +373,7 @@ struct TfArgs {
     int n_h;
     const long long *h_cell;
     const int *h_comp, *h_first, *h_count, *h_idx;
-    const T *h_coef, *h_w0, *h_w1;
+    const T *h_coef, *h_w;  // 4 cubic weights per term
     T *Ho[3];              // H after the sweep of the step
     T *inc_e, *inc_h;      // the 1-D line
     int m_len;
@@ -376,8 +383,8 @@ struct TfArgs {
     long long n_steps;
 };
 
-// H samples next to the boundary: H += coef * (w0 E1D[idx] + w1 E1D[idx+1])
-// for each of their terms, in order (E1D at step n).
+// H samples next to the boundary: H += coef * interp(E1D around idx) for
+// each of their terms, in order (E1D at step n).
 template <typename T>
 __global__ void k_tfsf_h(TfArgs<T> a) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -386,7 +393,7 @@ __global__ void k_tfsf_h(TfArgs<T> a) {
     T h = *f;
     for (int t = a.h_first[q]; t < a.h_first[q] + a.h_count[q]; t++) {
         const int m = a.h_idx[t];
-        h = xa(h, xm(a.h_coef[t], xa(xm(a.h_w0[t], a.inc_e[m]), xm(a.h_w1[t], a.inc_e[m + 1]))));
+        h = xa(h, xm(a.h_coef[t], tf_interp(a.h_w + 4 * t, a.inc_e + m)));
     }
     *f = h;
 }

@@ -5,8 +5,11 @@ CPU (oracle), the physics that pins the restatement:
   * normal incidence on a closed box in vacuum: outside the box the field
     stays at rounding level (the line and the grid propagate identically);
     inside, the probe sees the incident pulse;
-  * oblique incidence (30 deg, phi 20 deg, mixed polarisation): leakage into
-    the scattered region below -40 dB of the incident peak;
+  * oblique incidence (several directions, mixed polarisations): leakage
+    into the scattered region below -60 dB of the incident peak for a pulse
+    whose spectrum is 20 dB down at 17 cells per wavelength, below -55 dB at
+    9 cells per wavelength (the dispersion-matched line); along the body
+    diagonal the line reproduces the grid exactly;
   * normal incidence on a dielectric half-space (periodic x / y, eps_r 4):
     the reflected pulse in the scattered region is -1/3 of the incident one.
 GPU: FP64 device runs equal the oracle bit for bit (box with CPML, oblique;
@@ -26,13 +29,22 @@ from tests.cases import DT1, run_device
 GD = dict(waveform=0, p0=40 * DT1, p1=10 * DT1, p2=0.0)
 
 
-def box_scene(theta=0.0, phi=0.0, psi=0.0, n_steps=160):
+def box_scene(theta=0.0, phi=0.0, psi=0.0, n_steps=160, tau=10):
+    gd = dict(waveform=0, p0=4 * tau * DT1, p1=tau * DT1, p2=0.0)
     return Scene(nx=36, ny=34, nz=40, n_steps=n_steps, npml=6,
                  plane_wave=dict(theta=theta, phi=phi, psi=psi, amplitude=1.0, i0=12, i1=24, j0=11, j1=23,
-                                 k0=12, k1=28, **GD),
+                                 k0=12, k1=28, **gd),
                  probes=[(18, 17, 20, 0), (18, 17, 20, 1), (18, 17, 20, 2),      # inside
                          (18, 17, 9, 0), (18, 17, 31, 0), (9, 17, 20, 2),         # outside
-                         (27, 17, 20, 1), (18, 8, 20, 0), (18, 26, 20, 2)])
+                         (27, 17, 20, 1), (18, 8, 20, 0), (18, 26, 20, 2),
+                         (10, 9, 10, 0), (26, 25, 30, 1), (10, 25, 10, 2)])     # outside, near corners
+
+
+def leakage_db(theta, phi, psi, tau):
+    td = oracle.run_oracle(box_scene(theta, phi, psi, n_steps=200, tau=tau))["td"]
+    peak = np.abs(td[:3]).max()
+    assert peak > 0.3
+    return 20 * math.log10(np.abs(td[3:]).max() / peak)
 
 
 def test_normal_incidence_box_has_no_leakage():
@@ -43,12 +55,19 @@ def test_normal_incidence_box_has_no_leakage():
     assert np.abs(td[3:]).max() < 1e-12 * peak    # nothing leaks out
 
 
-def test_oblique_incidence_leakage_below_40db():
-    td = oracle.run_oracle(box_scene(theta=math.radians(30), phi=math.radians(20), psi=0.6, n_steps=200))["td"]
-    peak = np.abs(td[:3]).max()
-    leak = np.abs(td[3:]).max()
-    assert peak > 0.3
-    assert leak < 1e-2 * peak, leak / peak
+OBLIQUE = [(30, 20, 0.6), (45, 45, 0.3), (15, 0, 0.0), (40, -70, 1.2)]
+
+
+@pytest.mark.parametrize("theta,phi,psi", OBLIQUE, ids=[f"t{a}p{b}" for a, b, _ in OBLIQUE])
+def test_oblique_incidence_leakage(theta, phi, psi):
+    # tau 20 dt: spectrum 20 dB down at ~17 cells per wavelength; tau 10 dt: ~9
+    assert leakage_db(math.radians(theta), math.radians(phi), psi, tau=20) < -60.0
+    assert leakage_db(math.radians(theta), math.radians(phi), psi, tau=10) < -55.0
+
+
+def test_body_diagonal_line_is_exact():
+    # along (1,1,1) the grid's dispersion equals the line's at d1 = dx / sqrt 3
+    assert leakage_db(math.atan(math.sqrt(2.0)), math.radians(45), 1.0, tau=10) < -150.0
 
 
 def test_fresnel_half_space_normal_incidence():
