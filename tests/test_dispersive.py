@@ -83,12 +83,13 @@ def half_space_scenes(poles, eps_inf, sigma, nz=600, kz0=60, kint=200, ks=50, n_
     kint - 1 and kint, at z = kint - 1/2).  Scene a records the reflected
     E_x at z = ks in the scattered-field region; scene b (vacuum) records the
     incident E_x at the mirror point 2 (kint - 1/2) - ks, which has travelled
-    exactly as far on the same grid.  The record ends before the wave
-    reflected from the far end of the medium comes back."""
+    exactly as far on the same grid.  The medium ends 10 cells inside the
+    total-field box (the box boundary must lie in scalar media); the record
+    ends before the wave reaches that far face."""
     pw = dict(theta=0.0, phi=0.0, psi=0.0, amplitude=1.0, i0=0, i1=3, j0=0, j1=3, k0=kz0, k1=nz - 30,
               waveform=0, p0=80 * DT, p1=20 * DT, p2=0.0)
     disp = [disp_entry(c, i, j, k, eps_inf, sigma, poles)
-            for c in range(3) for i in range(4) for j in range(4) for k in range(kint, nz - 10)]
+            for c in range(3) for i in range(4) for j in range(4) for k in range(kint, nz - 40)]
     base = dict(nx=4, ny=4, nz=nz, n_steps=n_steps, periodic=3, npml=10, plane_wave=pw)
     return (Scene(**base, disp=disp, probes=[(1, 1, ks, 0)]),
             Scene(**base, probes=[(1, 1, 2 * kint - 1 - ks, 0)]))
