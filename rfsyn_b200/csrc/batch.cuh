@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             __syncthreads();
             cur = bi.scene;
         }
-        if (!q_item<T, TJ, NS, KIND>(sa, dims[bi.scene], maps[bi.scene], bi.t, smem_raw, phase, pending, failed)) {
+        if (!q_run<T, TJ, NS, KIND>(sa, dims[bi.scene], maps[bi.scene], bi.t, smem_raw, phase, pending, failed)) {
             q_bail<NS>(bars, phase, pending, err);
             break;
         }

@@ -707,8 +707,20 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
     ext(1, &ylo, &yhi, g.ny, py);
     ext(2, &zlo, &zhi, g.nz, pz);
     const int xa = px ? 0 : xlo + 1, xb = std::max(xa, xhi);
-    auto add = [](std::vector<SweepItem> &v, int j0, int k0, int b, int en, int seg) {
-        for (int s = b; s < en; s += seg) v.push_back(SweepItem{j0, k0, s, std::min(en, s + seg)});
+    auto add = [](std::vector<SweepItem> &v, int j0, int k0, int b, int en, int seg, int sub = 0) {
+        for (int s = b; s < en; s += seg) v.push_back(SweepItem{j0, k0, s, std::min(en, s + seg), sub});
+    };
+    // does [q0, q1] hold a slab cell of axis ax on the H or the E grid (the
+    // kernels' slab_in: inside [0, len) and outside [lo, hi))
+    auto touches = [&](int ax, int q0, int q1) {
+        if (!on) return false;
+        const int n = ax == 1 ? g.ny : g.nz;
+        const SlabExt &h = e->cpml.eh[ax], &m = e->cpml.em[ax];
+        for (int q = q0; q <= q1; q++) {
+            if (q >= 0 && q < n && (q < h.lo || q >= h.hi)) return true;
+            if (q >= 0 && q < n + 1 && (q < m.lo || q >= m.hi)) return true;
+        }
+        return false;
     };
     auto add_edge = [&](int j0, int rows, int k0, int b, int en) {
         // modes 2, 3: tiles whose halo stays inside the grid go to the TMA-fed
@@ -716,7 +728,10 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
         // axis to the cp.async-fed edge sweep (8-row tiles)
         const bool wraps = (py && (j0 <= 0 || j0 + rows >= g.ny)) || (pz && (k0 <= 0 || k0 + 32 >= g.nz));
         if (tma >= 2 && !wraps) {
-            add(vq, j0, k0, b, en, seg_edge);
+            // rows j0-1 .. j0+rows-1 and columns k0-1 .. k0+31 cover the
+            // tile, its halo row and its halo column
+            const bool ty = touches(1, j0 - 1, j0 + rows - 1), tz = touches(2, k0 - 1, k0 + 31);
+            add(vq, j0, k0, b, en, seg_edge, ty && tz ? 0 : tz ? 2 : 1);
             return;
         }
         for (int jj = j0; jj < j0 + rows && jj < p.d.cj; jj += 8) add(ve, jj, k0, b, en, seg_edge);

@@ -38,6 +38,9 @@ struct FusedDims {
 
 struct SweepItem {
     int j0, k0, ib, ie;
+    // slab / boundary tiles of the work-queue sweep: 0 any (y and z slabs,
+    // boundaries), 1 no z-slab cell in the tile or its halo, 2 no y-slab cell
+    int sub = 0;
 };
 
 struct FusedPlan {

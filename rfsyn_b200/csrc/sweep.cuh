@@ -9,7 +9,10 @@
 //   KIND 2 (edge) -- all other tiles whose halo does not wrap around a
 //     periodic axis, with rfsyn's per-component update ranges
 //     (engine/fdtd/cpml.c:176-219, materials.c:911-1060) and every slab
-//     psi recursion (cpml.h:46-51).
+//     psi recursion (cpml.h:46-51).  An edge item is marched by one of
+//     three bodies chosen by its `sub` field: tiles that touch only the y
+//     slab (KIND 3 body) or only the z slab (KIND 4 body) carry no code
+//     for the other axis; the rest take the full body.
 // Items whose halo wraps stay on the cp.async-fed k_sweep_edge (fused.cuh).
 // Each kind is compiled separately so the interior keeps the lean
 // instruction stream it needs to stay bandwidth-bound.
@@ -64,8 +67,10 @@ struct QLayout {
 template <typename T, int TJ, int NS, int KIND>
 __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, const TmaMaps &maps, const SweepItem &it,
                                        unsigned char *smem_raw, unsigned &phase, unsigned &pending, bool &failed) {
-    constexpr bool EDGE = KIND == 2;  // per-cell y / z conditions and slabs
-    constexpr bool XS = KIND >= 1;    // x-slab psi and plane conditions
+    constexpr bool EDGE = KIND >= 2;             // per-cell y / z conditions
+    constexpr bool YS = KIND == 2 || KIND == 3;  // y-slab psi
+    constexpr bool ZS = KIND == 2 || KIND == 4;  // z-slab psi
+    constexpr bool XS = KIND >= 1;               // x-slab psi and plane conditions
     using L = TmaLayout<T, TJ, NS>;
     using S = QLayout<T, TJ, NS>;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
@@ -149,26 +154,32 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
         colh = tx < TJ && k0 > 0 && jc >= 0 && jc < d.cj;
         mrow_jk = (k < a.nz ? 1u : 0u) | (k < a.nz + (pz ? 0 : 1) ? 4u : 0u);
         mcol_jk = (jc < a.ny ? 1u : 0u) | (jc < a.ny + (py ? 0 : 1) ? 2u : 0u);
-        sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
-        skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
-        sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
-        skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
-        sjh_row = slab_in(jh, a.lo_h[1], a.hi_h[1], a.ny, on);
-        sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
-        skh_col = slab_in(kh, a.lo_h[2], a.hi_h[2], a.nz, on);
-        for (int t = tid; t < TJ + 1; t += 32 * TJ) {
-            T v[3];
-            prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], j0 - 1 + t, a.ny, v);
-            tt.py[0][t] = v[0]; tt.py[1][t] = v[1]; tt.py[2][t] = v[2];
-            prof_at(on ? a.kinv_m[1] : (const T *)nullptr, a.b_m[1], a.a_m[1], j0 - 1 + t, a.ny + 1, v);
-            tt.py[3][t] = v[0]; tt.py[4][t] = v[1]; tt.py[5][t] = v[2];
+        // a body without one axis's slab code serves only tiles whose
+        // cells and halos lie outside that slab (the host classifies them)
+        if constexpr (YS) {
+            sjh = slab_in(j, a.lo_h[1], a.hi_h[1], a.ny, on);
+            sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
+            sjh_row = slab_in(jh, a.lo_h[1], a.hi_h[1], a.ny, on);
+            sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
+            for (int t = tid; t < TJ + 1; t += 32 * TJ) {
+                T v[3];
+                prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], j0 - 1 + t, a.ny, v);
+                tt.py[0][t] = v[0]; tt.py[1][t] = v[1]; tt.py[2][t] = v[2];
+                prof_at(on ? a.kinv_m[1] : (const T *)nullptr, a.b_m[1], a.a_m[1], j0 - 1 + t, a.ny + 1, v);
+                tt.py[3][t] = v[0]; tt.py[4][t] = v[1]; tt.py[5][t] = v[2];
+            }
         }
-        for (int t = tid; t < 33; t += 32 * TJ) {
-            T v[3];
-            prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], k0 - 1 + t, a.nz, v);
-            tt.pz[0][t] = v[0]; tt.pz[1][t] = v[1]; tt.pz[2][t] = v[2];
-            prof_at(on ? a.kinv_m[2] : (const T *)nullptr, a.b_m[2], a.a_m[2], k0 - 1 + t, a.nz + 1, v);
-            tt.pz[3][t] = v[0]; tt.pz[4][t] = v[1]; tt.pz[5][t] = v[2];
+        if constexpr (ZS) {
+            skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
+            skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
+            skh_col = slab_in(kh, a.lo_h[2], a.hi_h[2], a.nz, on);
+            for (int t = tid; t < 33; t += 32 * TJ) {
+                T v[3];
+                prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], k0 - 1 + t, a.nz, v);
+                tt.pz[0][t] = v[0]; tt.pz[1][t] = v[1]; tt.pz[2][t] = v[2];
+                prof_at(on ? a.kinv_m[2] : (const T *)nullptr, a.b_m[2], a.a_m[2], k0 - 1 + t, a.nz + 1, v);
+                tt.pz[3][t] = v[0]; tt.pz[4][t] = v[1]; tt.pz[5][t] = v[2];
+            }
         }
     }
     const int nshy = a.ns_h[1], nshz = a.ns_h[2], nsmy = a.ns_m[1], nsmz = a.ns_m[2];
@@ -229,16 +240,16 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
         }
         T pn;
         if (c == 0) {
-            if (EDGE && cl.sy >= 0) {
+            if (YS && cl.sy >= 0) {
                 dA = stretch(dA, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pA, &pn);
                 if (store) a.psi_ho[0][pb.by + cl.oy] = pn;
             }
-            if (EDGE && cl.sz >= 0) {
+            if (ZS && cl.sz >= 0) {
                 dB = stretch(dB, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pB, &pn);
                 if (store) a.psi_ho[1][pb.bz + cl.oz] = pn;
             }
         } else if (c == 1) {
-            if (EDGE && cl.sz >= 0) {
+            if (ZS && cl.sz >= 0) {
                 dA = stretch(dA, tt.pz[0][zi], tt.pz[1][zi], tt.pz[2][zi], a.dx, pA, &pn);
                 if (store) a.psi_ho[2][pb.bz + cl.oz] = pn;
             }
@@ -251,7 +262,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                 dA = stretch(dA, xph[0], xph[1], xph[2], a.dx, pA, &pn);
                 if (store) a.psi_ho[4][pb.bx + cl.ox] = pn;
             }
-            if (EDGE && cl.sy >= 0) {
+            if (YS && cl.sy >= 0) {
                 dB = stretch(dB, tt.py[0][yi], tt.py[1][yi], tt.py[2][yi], a.dx, pB, &pn);
                 if (store) a.psi_ho[5][pb.by + cl.oy] = pn;
             }
@@ -263,14 +274,14 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
         pA = T(0);
         pB = T(0);
         if (c == 0) {
-            if (EDGE && cl.sy >= 0) pA = a.psi_hi[0][pb.by + cl.oy];
-            if (EDGE && cl.sz >= 0) pB = a.psi_hi[1][pb.bz + cl.oz];
+            if (YS && cl.sy >= 0) pA = a.psi_hi[0][pb.by + cl.oy];
+            if (ZS && cl.sz >= 0) pB = a.psi_hi[1][pb.bz + cl.oz];
         } else if (c == 1) {
-            if (EDGE && cl.sz >= 0) pA = a.psi_hi[2][pb.bz + cl.oz];
+            if (ZS && cl.sz >= 0) pA = a.psi_hi[2][pb.bz + cl.oz];
             if (pb.sx >= 0) pB = a.psi_hi[3][pb.bx + cl.ox];
         } else {
             if (pb.sx >= 0) pA = a.psi_hi[4][pb.bx + cl.ox];
-            if (EDGE && cl.sy >= 0) pB = a.psi_hi[5][pb.by + cl.oy];
+            if (YS && cl.sy >= 0) pB = a.psi_hi[5][pb.by + cl.oy];
         }
     };
     // plane conditions: H bits (Hx to nx inclusive on a PEC x axis), E bits
@@ -354,16 +365,16 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
             if (mcol & 1u) hpsi(0, pb, col_c, hh[0], hh[1]);
             if (mcol & 2u) hpsi(1, pb, col_c, hh[2], hh[3]);
             if (m & 8u) {
-                if (EDGE && sjm >= 0) ep[0] = a.psi_e[0][bym + oym];
-                if (EDGE && skm >= 0) ep[1] = a.psi_e[1][bzm + ozm];
+                if (YS && sjm >= 0) ep[0] = a.psi_e[0][bym + oym];
+                if (ZS && skm >= 0) ep[1] = a.psi_e[1][bzm + ozm];
             }
             if (m & 16u) {
-                if (EDGE && skm >= 0) ep[2] = a.psi_e[2][bzm + ozm];
+                if (ZS && skm >= 0) ep[2] = a.psi_e[2][bzm + ozm];
                 if (sxm >= 0) ep[3] = a.psi_e[3][bxm + own_c.ox];
             }
             if (m & 32u) {
                 if (sxm >= 0) ep[4] = a.psi_e[4][bxm + own_c.ox];
-                if (EDGE && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
+                if (YS && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
             }
             wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
             T(*sH)[TJ + 1][33] = sHb[(i - ib) & 1];
@@ -414,11 +425,11 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                     if (m & 8u) {
                         T tA = xs(sH[2][r][qs], sH[2][r - 1][qs]);
                         T tB = xs(sH[1][r][qs], sH[1][r][qs - 1]);
-                        if (EDGE && sjm >= 0) {
+                        if (YS && sjm >= 0) {
                             tA = stretch(tA, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[0], &pn);
                             a.psi_e[0][bym + oym] = pn;
                         }
-                        if (EDGE && skm >= 0) {
+                        if (ZS && skm >= 0) {
                             tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
                             a.psi_e[1][bzm + ozm] = pn;
                         }
@@ -427,7 +438,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                     if (m & 16u) {
                         T tA = xs(sH[0][r][qs], sH[0][r][qs - 1]);
                         T tB = xs(hz, prevHz);
-                        if (EDGE && skm >= 0) {
+                        if (ZS && skm >= 0) {
                             tA = stretch(tA, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[2], &pn);
                             a.psi_e[2][bzm + ozm] = pn;
                         }
@@ -444,7 +455,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                             tA = stretch(tA, xpm[0], xpm[1], xpm[2], a.dx, ep[4], &pn);
                             a.psi_e[4][bxm + own_c.ox] = pn;
                         }
-                        if (EDGE && sjm >= 0) {
+                        if (YS && sjm >= 0) {
                             tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
                             a.psi_e[5][bym + oym] = pn;
                         }
@@ -458,6 +469,17 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
         }
     }
     return !__syncthreads_or(failed);
+}
+
+// The march of one item: an edge item takes the body its `sub` names.
+template <typename T, int TJ, int NS, int KIND>
+__device__ __forceinline__ bool q_run(const Args<T> &a, const FusedDims &d, const TmaMaps &maps, const SweepItem &it,
+                                      unsigned char *smem_raw, unsigned &phase, unsigned &pending, bool &failed) {
+    if constexpr (KIND == 2) {
+        if (it.sub == 1) return q_item<T, TJ, NS, 3>(a, d, maps, it, smem_raw, phase, pending, failed);
+        if (it.sub == 2) return q_item<T, TJ, NS, 4>(a, d, maps, it, smem_raw, phase, pending, failed);
+    }
+    return q_item<T, TJ, NS, KIND>(a, d, maps, it, smem_raw, phase, pending, failed);
 }
 
 // Loads the scene's (Ca, Cb) table into the CTA's shared tables.
@@ -537,7 +559,8 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
         __syncthreads();
         const int w = *s_item;
         if (w >= n_items) break;
-        if (!q_item<T, TJ, NS, KIND>(a, d, maps, items[w], smem_raw, phase, pending, failed)) {
+        const SweepItem it = items[w];
+        if (!q_run<T, TJ, NS, KIND>(a, d, maps, it, smem_raw, phase, pending, failed)) {
             q_bail<NS>(bars, phase, pending, err);
             break;
         }
@@ -549,7 +572,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
 // Variants (element type, TJ, NS, CTAs per SM of the interior and of the
 // edge instantiation): interior and edge share the tile height and ring
 // depth of a plan.
-#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 4) X(float, 8, 3, 5, 3) X(float, 16, 3, 2, 2)
+#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 3) X(float, 8, 3, 5, 3) X(float, 16, 3, 2, 2)
 #define RFB_Q_VARIANTS_FP64(X) X(double, 8, 3, 3, 2) X(double, 8, 4, 2, 2)
 
 template <typename T, int TJ, int NS, int MINB, int KIND>
