@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
 // Variants (element type, TJ, NS, CTAs per SM of the interior and of the
 // edge instantiation): interior and edge share the tile height and ring
 // depth of a plan.
-#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 3) X(float, 8, 3, 5, 3) X(float, 16, 3, 2, 2)
+#define RFB_Q_VARIANTS_FP32(X) X(float, 8, 4, 4, 4) X(float, 8, 3, 5, 3) X(float, 16, 3, 2, 2)
 #define RFB_Q_VARIANTS_FP64(X) X(double, 8, 3, 3, 2) X(double, 8, 4, 2, 2)
 
 template <typename T, int TJ, int NS, int MINB, int KIND>
