@@ -12,7 +12,7 @@
 //     scene; a CTA switching scenes copies the scene's parameters (Args) and
 //     (Ca, Cb) table into shared memory;
 //   k_e_list_b -- the interface-list entries of every scene, one block per
-//     256 list thread slots of one scene;
+//     256 entries of one scene;
 //   k_probe_gather_b -- every probe of every scene, then the shared step
 //     counter.
 // Steps are captured in CUDA graphs (16 steps per graph), and the tile
@@ -96,16 +96,16 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     q_leave(queue);
 }
 
-// Interface-list entries of many scenes: block b takes the list thread slots
-// blocks[b].y .. +255 (list_entry_of) of scene blocks[b].x.
+// Interface-list entries of many scenes: block b updates entries
+// blocks[b].y .. +255 of scene blocks[b].x.
 template <typename T>
 __global__ void __launch_bounds__(256) k_e_list_b(const Args<T> *args, const int2 *blocks) {
     __shared__ Args<T> sa;
     const int2 b = blocks[blockIdx.x];
     load_args(sa, args + b.x, 256, threadIdx.x);
     __syncthreads();
-    const int e = list_entry_of(b.y + threadIdx.x, sa.n_cells);
-    if (e >= 0) e_list_entry(sa, e);
+    const int e = b.y + threadIdx.x;
+    if (e < 3 * sa.n_cells) e_list_entry(sa, e);
 }
 
 template <typename T>
@@ -458,7 +458,7 @@ static int batch_upload_args(rfb_batch *b) {
     }
     for (size_t s = 0; s < n; s++) {
         rfb_engine *e = b->m[s];
-        const int ne = list_slots(e->scene.n_cells);
+        const int ne = 3 * e->scene.n_cells;
         for (int e0 = 0; e0 < ne; e0 += 256) lblocks.push_back(make_int2((int)s, e0));
         std::vector<long long> cell(e->n_probes);
         std::vector<int> comp(e->n_probes);

@@ -552,7 +552,7 @@ static void enqueue_step(rfb_engine *e, int par) {
         k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
     }
     tf_before_list<T>(e, par);
-    if (a.n_cells) k_e_list<T><<<(list_slots(a.n_cells) + 255) / 256, 256, 0, e->stream>>>(a);
+    if (a.n_cells) k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
     ProbeArgs<T> p;
     p.n = e->n_probes;
     p.cell = e->probe_cell;
@@ -1320,7 +1320,7 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         CK(cudaEventRecord(ev[1], e->stream));
         tf_before_list<T>(e, par);
         if (a.n_cells) {
-            k_e_list<T><<<(list_slots(a.n_cells) + 255) / 256, 256, 0, e->stream>>>(a);
+            k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
             g_launches++;
         }
         ProbeArgs<T> p;
@@ -1722,7 +1722,7 @@ extern "C" int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cp
     g_launches++;
     if (a.n_cells) {
         // the step-wise list carries no sources: d_step is unused
-        k_e_list<double><<<(list_slots(a.n_cells) + 255) / 256, 256, 0, f->stream>>>(a);
+        k_e_list<double><<<(3 * a.n_cells + 255) / 256, 256, 0, f->stream>>>(a);
         g_launches++;
     }
     if (cudaGetLastError() != cudaSuccess) { rfb_set_error("E update launch failed"); goto out; }

@@ -316,18 +316,6 @@ __device__ __forceinline__ T e_tensor3(const Args<T> &a, const T *r, int c, int 
 }
 
 // ---- interface list: overrides, tensor edges, sources --------------------
-// Thread slot t of a list launch -> entry (3 cell + comp): slots come in
-// groups of 96 = 3 warps covering 32 consecutive list cells, one component
-// per warp, so a warp follows one component's code path and its lanes touch
-// neighbouring cells.  -1 past the last cell.
-__host__ __device__ __forceinline__ int list_entry_of(int t, int n_cells) {
-    const int g = t / 96, r = t - 96 * g;
-    const int comp = r >> 5, cell = 32 * g + (r & 31);
-    return cell < n_cells ? 3 * cell + comp : -1;
-}
-// Thread slots a list of n cells needs.
-__host__ __device__ __forceinline__ int list_slots(int n_cells) { return 96 * ((n_cells + 31) / 32); }
-
 // One thread per (cell, component) entry.  Reads E from the input buffers,
 // H from the output buffers (already advanced), writes E output.
 template <typename T>
@@ -433,8 +421,8 @@ __global__ void k_inc_e(TfArgs<T> a) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
-    const int e = list_entry_of(blockIdx.x * blockDim.x + threadIdx.x, a.n_cells);
-    if (e < 0) return;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * a.n_cells) return;
     e_list_entry(a, e);
 }
 
