@@ -40,6 +40,7 @@ SWEEP_KERNEL = {
     1: "k_sweep_interior_tma + k_sweep_edge (one H+E sweep)",
     2: "k_sweep_q (one H+E sweep: interior + x-slab + edge launches)",
     3: "k_sweep_q (one H+E sweep: interior + x-slab + edge launches, shifted tiles)",
+    4: "k_sweep_q (one H+E sweep: interior + x-slab + edge launches, narrow z-slab tiles)",
 }
 
 
@@ -327,7 +328,8 @@ def run_b200(args) -> None:
                    "probes": len(w.probes), "dft_bins": len(w.freqs), "spheres": len(w.spheres),
                    "list_cells": info.list_cells, "dispersive_samples": info.dispersive,
                    "schedule": "fused" if info.schedule == rb.FUSED else "split", "tile_j": info.tile_j,
-                   "sweep_mode": {0: "cp.async", 1: "tma-interior", 2: "tma-queue", 3: "tma-queue-shifted"}.get(info.tma),
+                   "sweep_mode": {0: "cp.async", 1: "tma-interior", 2: "tma-queue", 3: "tma-queue-shifted",
+                                  4: "tma-queue-narrow-z"}.get(info.tma),
                    "ring_depth": info.ring_depth,
                    "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
                    "l2": f"inputs larger than L2 (fields 6 x 2 x {field_mb:.0f} MB per scene)"},

@@ -255,6 +255,10 @@ static int batch_build_plan(rfb_batch *b, int tj, int ns, int mode, int seg_int,
     maps[1].resize(n);
     for (size_t s = 0; s < n; s++) {
         rfb_engine *e = b->m[s];
+        if (mode == 4 && (e->g.periodic & 6u)) {
+            rfb_set_error("batch scene %zu: sweep mode 4 needs non-periodic y and z axes", s);
+            return -1;
+        }
         PlanLists pl;
         plan_items(e, e->active, tj, mode, seg_int, seg_edge, pl);
         if (!pl.ve.empty()) {
@@ -368,8 +372,10 @@ static int batch_autotune(rfb_batch *b) {
     std::vector<Cand> cands;
     const InteriorVariant *v = b->prec == RFB_FP32 ? kQVariantsFp32 : kQVariantsFp64;
     const size_t nv = b->prec == RFB_FP32 ? std::size(kQVariantsFp32) : std::size(kQVariantsFp64);
+    bool wrap_yz = false;
+    for (const rfb_engine *e : b->m) wrap_yz |= (e->g.periodic & 6u) != 0;
     for (size_t q = 0; q < nv; q++)
-        for (int mode = 2; mode <= 3; mode++)
+        for (int mode = 2; mode <= (wrap_yz ? 3 : 4); mode++)
             for (int si : {32, 64})
                 for (int se : {16, 32}) cands.push_back(Cand{v[q].tj, v[q].ns, mode, si, se});
     const char *ov = getenv("RFSYN_FDTD_PLAN");

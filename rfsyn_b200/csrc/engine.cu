@@ -659,9 +659,13 @@ static int build_tma_maps(rfb_engine *e, int tj) {
         for (int c = 0; c < 3; c++) {
             if (encode_map(&m.e[c], e->fld[in][c], dt, e->esz, e->g, e->pitch, TMA_EW, tj + 2)) return -1;
             if (encode_map(&m.h[c], e->fld[in][3 + c], dt, e->esz, e->g, e->pitch, TMA_HW, tj + 1)) return -1;
+            // narrow tiles: 2 tj rows x 16 columns (E 24 x (2 tj + 2), H 20 x (2 tj + 1))
+            if (encode_map(&m.en[c], e->fld[in][c], dt, e->esz, e->g, e->pitch, 24, 2 * tj + 2)) return -1;
+            if (encode_map(&m.hn[c], e->fld[in][3 + c], dt, e->esz, e->g, e->pitch, 20, 2 * tj + 1)) return -1;
         }
         if (e->scene.codes &&
-            encode_map(&m.code, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 32, tj))
+            (encode_map(&m.code, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 32, tj) ||
+             encode_map(&m.coden, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 16, 2 * tj)))
             return -1;
     }
     return 0;
@@ -736,12 +740,26 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
         }
         for (int jj = j0; jj < j0 + rows && jj < p.d.cj; jj += 8) add(ve, jj, k0, b, en, seg_edge);
     };
-    // tile origins: multiples of (tj, 32) from 0, or in mode 3, on axes
-    // without wrap, shifted so that the first interior tile starts right
+    // tile origins: multiples of (tj, 32) from 0, or in modes 3 and 4, on
+    // axes without wrap, shifted so that the first interior tile starts right
     // after the low slab (j0 any row, k0 a multiple of 16 for the TMA boxes);
     // the tiles below it may start at negative coordinates, their cells
-    // outside the grid are idle lanes
+    // outside the grid are idle lanes.  Mode 4 (no periodic y / z) covers
+    // the z-slab columns with narrow (2 tj x 16) tiles instead: 32-wide
+    // columns only where they are z-interior, 16-wide columns below and
+    // above them.
     int js = 0, ks = 0;
+    std::vector<std::pair<int, int>> cols;  // (k0, width)
+    if (tma == 4) {
+        const int ja = ylo + 1;
+        js = ja - tj * ((ja + tj - 1) / tj);
+        const int ka = (zlo + 1 + 15) / 16 * 16;
+        int kb = ka;
+        while (kb + 32 <= std::min(zhi, p.d.ck)) kb += 32;
+        for (int k0 = ka - 16; k0 + 16 > 0; k0 -= 16) cols.push_back({k0, 16});
+        for (int k0 = ka; k0 < kb; k0 += 32) cols.push_back({k0, 32});
+        for (int k0 = kb; k0 < p.d.ck; k0 += 16) cols.push_back({k0, 16});
+    }
     if (tma == 3) {
         if (!py) {
             const int ja = ylo + 1;
@@ -752,8 +770,17 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
             ks = ka - 32 * ((ka + 31) / 32);
         }
     }
-    for (int j0 = js; j0 < p.d.cj; j0 += tj)
-        for (int k0 = ks; k0 < p.d.ck; k0 += 32) {
+    if (tma != 4)
+        for (int k0 = ks; k0 < p.d.ck; k0 += 32) cols.push_back({k0, 32});
+    for (const auto &cw : cols) {
+        const int k0 = cw.first;
+        if (cw.second == 16) {
+            // narrow z-slab tiles: always slab / boundary work
+            for (int j0 = 0; j0 < p.d.cj; j0 += 2 * tj)
+                add(vq, j0, k0, 0, p.d.ci, seg_edge, touches(1, j0 - 1, j0 + 2 * tj - 1) ? 4 : 3);
+            continue;
+        }
+        for (int j0 = js; j0 < p.d.cj; j0 += tj) {
             const bool full = j0 >= 0 && k0 >= 0 && j0 + tj <= p.d.cj && k0 + 32 <= p.d.ck;
             // the interior sweeps read the halo without wrapping it: on a
             // periodic axis the tiles at either end stay on the edge sweep
@@ -779,6 +806,7 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
                 add_edge(j0, tj, k0, 0, p.d.ci);
             }
         }
+    }
     // queue order: longest items first, so the last items to start are short
     std::stable_sort(vq.begin(), vq.end(), [](const SweepItem &x, const SweepItem &y) {
         return x.ie - x.ib > y.ie - y.ib;
@@ -788,6 +816,10 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
 static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge) {
     if (tma >= 2 && !q_fits(e)) {
         rfb_set_error("grid too large for the work-queue sweep (32-bit offsets)");
+        return -1;
+    }
+    if (tma == 4 && (e->g.periodic & 6u)) {
+        rfb_set_error("sweep mode 4 (narrow z-slab tiles) needs non-periodic y and z axes");
         return -1;
     }
     FusedPlan &p = e->plan;
@@ -826,6 +858,7 @@ fail:
 static bool plan_variant_known(int prec, int tj, int ns, int tma) {
     const InteriorVariant *v;
     size_t n;
+    if (tma < 0 || tma > 4) return false;
     if (tma >= 2) {
         v = prec == RFB_FP32 ? kQVariantsFp32 : kQVariantsFp64;
         n = prec == RFB_FP32 ? std::size(kQVariantsFp32) : std::size(kQVariantsFp64);
@@ -885,15 +918,19 @@ static int autotune(rfb_engine *e, int active) {
         int tma;
     };
     std::vector<Cand> vars;
-    const bool qok = q_fits(e);
+    const bool qok = q_fits(e), narrow = qok && !(e->g.periodic & 6u);
     if (e->prec == RFB_FP32) {
         if (qok)
             for (const InteriorVariant &v : kQVariantsFp32) vars.push_back({v, 2}), vars.push_back({v, 3});
+        if (narrow)
+            for (const InteriorVariant &v : kQVariantsFp32) vars.push_back({v, 4});
         for (const InteriorVariant &v : kTmaVariantsFp32) vars.push_back({v, 1});
         for (const InteriorVariant &v : kIntVariantsFp32) vars.push_back({v, 0});
     } else {
         if (qok)
             for (const InteriorVariant &v : kQVariantsFp64) vars.push_back({v, 2}), vars.push_back({v, 3});
+        if (narrow)
+            for (const InteriorVariant &v : kQVariantsFp64) vars.push_back({v, 4});
         for (const InteriorVariant &v : kTmaVariantsFp64) vars.push_back({v, 1});
         for (const InteriorVariant &v : kIntVariantsFp64) vars.push_back({v, 0});
     }

@@ -44,51 +44,78 @@ namespace rfb {
 
 template <typename T, int TJ>
 struct TileTables {
-    T tab[512];         // Ca (0..255), Cb (256..511)
-    T py[6][TJ + 1];    // y profiles at rows j0-1 .. j0+TJ-1: H grid (kinv b a), E grid (kinv b a)
-    T pz[6][33];        // z profiles at cols k0-1 .. k0+31
+    T tab[512];           // Ca (0..255), Cb (256..511)
+    T py[6][2 * TJ + 1];  // y profiles at rows j0-1 .. j0+rows-1: H grid (kinv b a), E grid (kinv b a)
+    T pz[6][33];          // z profiles at cols k0-1 .. k0+cols-1
 };
+
+// Boxes of one stage for a tile of TR rows x W columns: E rows j0-1 ..
+// j0+TR, columns k0-4 .. k0+W+3; H rows j0-1 .. j0+TR-1, columns k0-4 ..
+// k0+W-1; codes TR x W.  Wide tiles are (TJ x 32), one row per warp;
+// narrow tiles (2 TJ x 16), two rows per warp.
+template <typename T, int TR, int W>
+struct QShape {
+    static constexpr int EW = W + 8, HW = W + 4;
+    static constexpr unsigned ebytes = sizeof(T) * EW * (TR + 2);
+    static constexpr unsigned hbytes = sizeof(T) * HW * (TR + 1);
+    static constexpr unsigned cbytes = W * TR;
+    static constexpr size_t ebox = round128(ebytes);
+    static constexpr size_t hbox = round128(hbytes);
+    static constexpr size_t cbox = round128(cbytes);
+    static constexpr size_t stage = 3 * ebox + 3 * hbox + cbox;
+};
+
+__host__ __device__ constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
 
 template <typename T, int TJ, int NS>
 struct QLayout {
-    using L = TmaLayout<T, TJ, NS>;
-    static constexpr size_t bars = NS * L::stage;
+    using Wd = QShape<T, TJ, 32>;
+    using Nr = QShape<T, 2 * TJ, 16>;
+    static constexpr size_t stage = cmax(Wd::stage, Nr::stage);
+    static constexpr size_t bars = NS * stage;
     static constexpr size_t sh = bars + round128(8 * NS);
-    static constexpr size_t tabs = sh + round128(sizeof(T) * 2 * 3 * (TJ + 1) * 33);
+    static constexpr size_t tabs = sh + round128(sizeof(T) * 2 * 3 * cmax((TJ + 1) * 33, (2 * TJ + 1) * 17));
     static constexpr size_t misc = tabs + round128(sizeof(TileTables<T, TJ>));
     static constexpr size_t total = misc + 16;
 };
 
-// One work item: the march over planes [ib, ie) of the (TJ x 32) tile at
-// (j0, k0) of the scene described by `a`, `d` and `maps`.  `phase`,
+// One work item: the march over planes [ib, ie) of the (TJ x 32) tile (W =
+// 32) or the (2 TJ x 16) tile (W = 16) at (j0, k0) of the scene described by
+// `a`, `d` and `maps`.  `phase`,
 // `pending` and `failed` are the CTA's ring bookkeeping, carried across
 // items.  Returns false when a copy did not complete in time (the caller
 // drains the ring and leaves the queue).
-template <typename T, int TJ, int NS, int KIND>
+template <typename T, int TJ, int NS, int KIND, int W = 32>
 __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, const TmaMaps &maps, const SweepItem &it,
                                        unsigned char *smem_raw, unsigned &phase, unsigned &pending, bool &failed) {
     constexpr bool EDGE = KIND >= 2;             // per-cell y / z conditions
     constexpr bool YS = KIND == 2 || KIND == 3;  // y-slab psi
     constexpr bool ZS = KIND == 2 || KIND == 4;  // z-slab psi
     constexpr bool XS = KIND >= 1;               // x-slab psi and plane conditions
-    using L = TmaLayout<T, TJ, NS>;
+    static_assert(W == 32 || (W == 16 && KIND >= 2), "narrow tiles are edge tiles");
+    constexpr int RPW = 32 / W;       // tile rows per warp
+    constexpr int TR = TJ * RPW;      // tile rows
+    using L = QShape<T, TR, W>;
     using S = QLayout<T, TJ, NS>;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
     // H of the current plane (tile + halo), double-buffered by plane parity
     // so one block barrier per plane separates its writes from its reads
-    T(*sHb)[3][TJ + 1][33] = reinterpret_cast<T(*)[3][TJ + 1][33]>(smem_raw + S::sh);
+    T(*sHb)[3][TR + 1][W + 1] = reinterpret_cast<T(*)[3][TR + 1][W + 1]>(smem_raw + S::sh);
     TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
-    auto E = [&](int s, int c) { return reinterpret_cast<T(*)[TMA_EW]>(smem_raw + s * L::stage + c * L::ebox); };
+    auto E = [&](int s, int c) { return reinterpret_cast<T(*)[L::EW]>(smem_raw + s * S::stage + c * L::ebox); };
     auto H = [&](int s, int c) {
-        return reinterpret_cast<T(*)[TMA_HW]>(smem_raw + s * L::stage + 3 * L::ebox + c * L::hbox);
+        return reinterpret_cast<T(*)[L::HW]>(smem_raw + s * S::stage + 3 * L::ebox + c * L::hbox);
     };
     auto CODE = [&](int s) {
-        return reinterpret_cast<uint8_t(*)[32]>(smem_raw + s * L::stage + 3 * L::ebox + 3 * L::hbox);
+        return reinterpret_cast<uint8_t(*)[W]>(smem_raw + s * S::stage + 3 * L::ebox + 3 * L::hbox);
     };
+    const CUtensorMap *me = W == 32 ? maps.e : maps.en, *mh = W == 32 ? maps.h : maps.hn;
+    const CUtensorMap *mc = W == 32 ? &maps.code : &maps.coden;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const bool px = a.per & 1u, py = a.per & 2u, pz = a.per & 4u;
-    const int r = ty + 1, q = tx + 4;  // stage coordinates of the own cell
-    const int qs = tx + 1;             // sH / z-table column of the own cell
+    const int row = ty * RPW + (RPW > 1 ? tx / W : 0), col = RPW > 1 ? tx % W : tx;  // own cell in the tile
+    const int r = row + 1, q = col + 4;  // stage coordinates of the own cell
+    const int qs = col + 1;              // sH / z-table column of the own cell
     const bool with_codes = a.codes != nullptr;
     const unsigned tx_bytes = 3 * L::ebytes + 3 * L::hbytes + (with_codes ? L::cbytes : 0u);
     const T cbh = a.cbh;
@@ -102,10 +129,10 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
             mbar_expect_tx(&bars[s], tx_bytes);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                tma_load_3d(E(s, c), &maps.e[c], k0 - 4, j0 - 1, p, &bars[s]);
-                tma_load_3d(H(s, c), &maps.h[c], k0 - 4, j0 - 1, p, &bars[s]);
+                tma_load_3d(E(s, c), &me[c], k0 - 4, j0 - 1, p, &bars[s]);
+                tma_load_3d(H(s, c), &mh[c], k0 - 4, j0 - 1, p, &bars[s]);
             }
-            if (with_codes) tma_load_3d(CODE(s), &maps.code, k0, j0, p, &bars[s]);
+            if (with_codes) tma_load_3d(CODE(s), mc, k0, j0, p, &bars[s]);
         }
         pending |= 1u << s;
     };
@@ -127,13 +154,16 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
     // at every (j, k), only the plane (x) conditions and x-slab psi
     // remain, both uniform per plane.  The edge instantiation adds the
     // per-cell y / z conditions and y / z slab psi.
-    const int j = j0 + ty, k = k0 + tx;
+    const int j = j0 + row, k = k0 + col;
     const bool own = !EDGE || (j >= 0 && k >= 0 && j < d.cj && k < d.ck);
     const int pitch = (int)a.pitch;
     const int plane32 = (int)a.plane;
+    // halo cells recomputed per plane: the row (j0-1, k0 .. k0+W-1), Hx by
+    // warp 0 and Hz by warp 2, the column (j0 .. j0+TR-1, k0-1), Hx and Hy
+    // by warp 1; lane tx takes halo column tx / halo row tx
     const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
     unsigned mjk = 0x3f;                   // bits 0-2 H, 3-5 E at (j, k), plane apart
-    bool rowh = true, colh = tx < TJ;      // halo cells this thread recomputes
+    bool rowh = tx < W, colh = tx < TR;    // halo cells this thread recomputes
     int sjh = -1, skh = -1, sjm = -1, skm = -1;
     int sjh_row = -1, sjh_col = -1, skh_col = -1;
     unsigned mrow_jk = 5u, mcol_jk = 3u;   // halo components at (j, k), plane apart
@@ -150,8 +180,8 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                 if (j >= jmin) mjk |= 32u;
             }
         }
-        rowh = j0 > 0 && k >= 0 && k < d.ck;
-        colh = tx < TJ && k0 > 0 && jc >= 0 && jc < d.cj;
+        rowh = tx < W && j0 > 0 && k >= 0 && k < d.ck;
+        colh = tx < TR && k0 > 0 && jc >= 0 && jc < d.cj;
         mrow_jk = (k < a.nz ? 1u : 0u) | (k < a.nz + (pz ? 0 : 1) ? 4u : 0u);
         mcol_jk = (jc < a.ny ? 1u : 0u) | (jc < a.ny + (py ? 0 : 1) ? 2u : 0u);
         // a body without one axis's slab code serves only tiles whose
@@ -161,7 +191,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
             sjm = slab_in(j, a.lo_m[1], a.hi_m[1], a.ny, on);
             sjh_row = slab_in(jh, a.lo_h[1], a.hi_h[1], a.ny, on);
             sjh_col = slab_in(jc, a.lo_h[1], a.hi_h[1], a.ny, on);
-            for (int t = tid; t < TJ + 1; t += 32 * TJ) {
+            for (int t = tid; t < TR + 1; t += 32 * TJ) {
                 T v[3];
                 prof_at(on ? a.kinv_h[1] : (const T *)nullptr, a.b_h[1], a.a_h[1], j0 - 1 + t, a.ny, v);
                 tt.py[0][t] = v[0]; tt.py[1][t] = v[1]; tt.py[2][t] = v[2];
@@ -173,7 +203,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
             skh = slab_in(k, a.lo_h[2], a.hi_h[2], a.nz, on);
             skm = slab_in(k, a.lo_m[2], a.hi_m[2], a.nz, on);
             skh_col = slab_in(kh, a.lo_h[2], a.hi_h[2], a.nz, on);
-            for (int t = tid; t < 33; t += 32 * TJ) {
+            for (int t = tid; t < W + 1; t += 32 * TJ) {
                 T v[3];
                 prof_at(on ? a.kinv_h[2] : (const T *)nullptr, a.b_h[2], a.a_h[2], k0 - 1 + t, a.nz, v);
                 tt.pz[0][t] = v[0]; tt.pz[1][t] = v[1]; tt.pz[2][t] = v[2];
@@ -377,9 +407,9 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                 if (YS && sjm >= 0) ep[5] = a.psi_e[5][bym + oym];
             }
             wait_slot(sn);  // plane i+1 (plane i landed before the previous barrier)
-            T(*sH)[TJ + 1][33] = sHb[(i - ib) & 1];
+            T(*sH)[TR + 1][W + 1] = sHb[(i - ib) & 1];
             const T e0 = E(sc, 0)[r][q], e1 = E(sc, 1)[r][q], e2 = E(sc, 2)[r][q];
-            const int code = with_codes ? (int)CODE(sc)[ty][tx] : 0;
+            const int code = with_codes ? (int)CODE(sc)[row][col] : 0;
             const long long c = (long long)i * a.plane + own_c.ox;
             T hx = H(sc, 0)[r][q], hy = H(sc, 1)[r][q], hz = H(sc, 2)[r][q];
             if (m & 1u) hx = hcell(0, pb, sc, sn, r, q, own_c, r, qs, hp[0], hp[1], true);
@@ -478,6 +508,8 @@ __device__ __forceinline__ bool q_run(const Args<T> &a, const FusedDims &d, cons
     if constexpr (KIND == 2) {
         if (it.sub == 1) return q_item<T, TJ, NS, 3>(a, d, maps, it, smem_raw, phase, pending, failed);
         if (it.sub == 2) return q_item<T, TJ, NS, 4>(a, d, maps, it, smem_raw, phase, pending, failed);
+        if (it.sub == 3) return q_item<T, TJ, NS, 4, 16>(a, d, maps, it, smem_raw, phase, pending, failed);
+        if (it.sub == 4) return q_item<T, TJ, NS, 2, 16>(a, d, maps, it, smem_raw, phase, pending, failed);
     }
     return q_item<T, TJ, NS, KIND>(a, d, maps, it, smem_raw, phase, pending, failed);
 }

@@ -25,9 +25,11 @@
 
 namespace rfb {
 
-// One tensor map per input array of one buffer parity.
+// One tensor map per input array of one buffer parity, for the wide (TJ x
+// 32) tiles and for the narrow (2 TJ x 16) tiles of the work-queue sweep.
 struct TmaMaps {
     CUtensorMap e[3], h[3], code;
+    CUtensorMap en[3], hn[3], coden;
 };
 
 constexpr int TMA_EW = 40;  // E box width (k0-4 .. k0+35)
