@@ -330,7 +330,7 @@ def run_b200(args) -> None:
                    "schedule": "fused" if info.schedule == rb.FUSED else "split", "tile_j": info.tile_j,
                    "sweep_mode": {0: "cp.async", 1: "tma-interior", 2: "tma-queue", 3: "tma-queue-shifted",
                                   4: "tma-queue-narrow-z"}.get(info.tma),
-                   "ring_depth": info.ring_depth,
+                   "ring_depth": info.ring_depth, "single_queue": bool(info.unified),
                    "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
                    "l2": f"inputs larger than L2 (fields 6 x 2 x {field_mb:.0f} MB per scene)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

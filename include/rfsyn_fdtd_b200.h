@@ -159,6 +159,7 @@ typedef struct {
     int tma;                 /* 1: interior planes staged by the Tensor Memory Accelerator */
     int interior_items;      /* work items of the interior sweep (CTAs per step) */
     int edge_items;          /* work items of the edge sweep */
+    int unified;             /* 1: every sweep item in one work queue, one launch per step */
 } fdtd_b200_sim_info_t;
 
 int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info);

@@ -504,14 +504,16 @@ static void launch_q_t(const Args<T> &a, const FusedPlan &p, int kind, const Tma
 template <>
 void launch_q_t<float>(const Args<float> &a, const FusedPlan &p, int kind, const TmaMaps &m, int *err,
                        cudaStream_t st) {
-    if (kind == 2) launch_q_f<2>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    if (kind == 2 && p.uni) launch_q_f<5>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    else if (kind == 2) launch_q_f<2>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
     else if (kind == 1) launch_q_f<1>(a, p.d, p.tj, p.ns, p.d_qx, p.n_qx, m, p.d_queue + 4, err, st);
     else launch_q_f<0>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
 }
 template <>
 void launch_q_t<double>(const Args<double> &a, const FusedPlan &p, int kind, const TmaMaps &m, int *err,
                         cudaStream_t st) {
-    if (kind == 2) launch_q_d<2>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    if (kind == 2 && p.uni) launch_q_d<5>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
+    else if (kind == 2) launch_q_d<2>(a, p.d, p.tj, p.ns, p.d_qe, p.n_qe, m, p.d_queue + 2, err, st);
     else if (kind == 1) launch_q_d<1>(a, p.d, p.tj, p.ns, p.d_qx, p.n_qx, m, p.d_queue + 4, err, st);
     else launch_q_d<0>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
 }
@@ -813,7 +815,8 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
     });
 }
 
-static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge) {
+static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge,
+                            int uni = 0) {
     if (tma >= 2 && !q_fits(e)) {
         rfb_set_error("grid too large for the work-queue sweep (32-bit offsets)");
         return -1;
@@ -829,9 +832,22 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     p.tma = tma;
     p.seg_int = seg_int;
     p.seg_edge = seg_edge;
+    p.uni = tma >= 2 ? uni : 0;
     PlanLists pl;
     plan_items(e, active, tj, tma, seg_int, seg_edge, pl);
     p.d = pl.d;
+    if (p.uni) {
+        // one queue: interior and x-slab items join the slab / boundary
+        // items, costliest first (a slab or boundary plane costs about four
+        // interior planes)
+        for (SweepItem it : pl.vi) it.sub = 5, pl.vq.push_back(it);
+        for (SweepItem it : pl.vx) it.sub = 6, pl.vq.push_back(it);
+        pl.vi.clear();
+        pl.vx.clear();
+        auto cost = [](const SweepItem &x) { return (x.ie - x.ib) * (x.sub == 5 ? 1 : 4); };
+        std::stable_sort(pl.vq.begin(), pl.vq.end(),
+                         [&](const SweepItem &x, const SweepItem &y) { return cost(x) > cost(y); });
+    }
     const std::vector<SweepItem> &vi = pl.vi, &ve = pl.ve, &vq = pl.vq, &vx = pl.vx;
     p.n_int = (int)vi.size();
     p.n_edge = (int)ve.size();
@@ -880,7 +896,7 @@ static bool plan_variant_known(int prec, int tj, int ns, int tma) {
 // on the engine's own scene; the choice is cached per geometry.  Every
 // candidate computes bit-identical fields, so tuning changes speed only.
 struct TunedPlan {
-    int tj, ns, tma, seg_int, seg_edge;
+    int tj, ns, tma, seg_int, seg_edge, uni;
 };
 
 static std::mutex g_tune_mu;
@@ -911,7 +927,7 @@ static int autotune(rfb_engine *e, int active) {
         for (auto &kv : g_tune_cache)
             if (kv.first == key)
                 return build_sweep_plan(e, active, kv.second.tj, kv.second.ns, kv.second.tma, kv.second.seg_int,
-                                        kv.second.seg_edge);
+                                        kv.second.seg_edge, kv.second.uni);
     }
     struct Cand {
         InteriorVariant v;
@@ -936,7 +952,7 @@ static int autotune(rfb_engine *e, int active) {
     }
     const int segs_int[] = {32, 64, 128};
     const int segs_edge[] = {16, 32};
-    TunedPlan best = {vars[0].v.tj, vars[0].v.ns, vars[0].tma, 64, 32};
+    TunedPlan best = {vars[0].v.tj, vars[0].v.ns, vars[0].tma, 64, 32, 0};
     float best_ms = 1e30f;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     CK(cudaEventCreate(&t0));
@@ -947,9 +963,10 @@ static int autotune(rfb_engine *e, int active) {
         int par = 0;
         for (const Cand &cv : vars)
             for (int si : segs_int)
-                for (int se : segs_edge) {
+                for (int se : segs_edge)
+                    for (int uni = 0; uni <= (cv.tma >= 2 ? 1 : 0); uni++) {
                     const InteriorVariant &v = cv.v;
-                    if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se) != 0) goto fail;
+                    if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se, uni) != 0) goto fail;
                     for (int w = 0; w < 2; w++) {
                         if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
                         else enqueue_sweep<float>(e, par);
@@ -967,7 +984,7 @@ static int autotune(rfb_engine *e, int active) {
                     CK(cudaEventElapsedTime(&ms, t0, t1));
                     if (ms < best_ms) {
                         best_ms = ms;
-                        best = TunedPlan{v.tj, v.ns, cv.tma, si, se};
+                        best = TunedPlan{v.tj, v.ns, cv.tma, si, se, uni};
                     }
                 }
     }
@@ -977,7 +994,8 @@ static int autotune(rfb_engine *e, int active) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         g_tune_cache.push_back({key, best});
     }
-    if (build_sweep_plan(e, active, best.tj, best.ns, best.tma, best.seg_int, best.seg_edge) != 0) return -1;
+    if (build_sweep_plan(e, active, best.tj, best.ns, best.tma, best.seg_int, best.seg_edge, best.uni) != 0)
+        return -1;
     {
         // a timed-out copy during tuning would have left the error flag set
         int err = 0;
@@ -1108,16 +1126,17 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
             rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
             goto fail_noset;
         }
-        // plan: "tj,ns,seg_interior,seg_edge[,tma]" from RFSYN_FDTD_PLAN,
+        // plan: "tj,ns,seg_interior,seg_edge[,mode[,single_queue]]" from RFSYN_FDTD_PLAN,
         // the autotuner (default) or, with RFSYN_FDTD_TUNE=0, the first
         // TMA variant
         const char *ov = getenv("RFSYN_FDTD_PLAN");
         const char *tune = getenv("RFSYN_FDTD_TUNE");
-        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
         int rc;
-        const int nov = ov ? sscanf(ov, "%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5) : 0;
-        if (nov >= 4 && a3 > 0 && a4 > 0 && plan_variant_known(precision, a1, a2, nov == 5 ? a5 : 0))
-            rc = build_sweep_plan(e, active, a1, a2, nov == 5 ? a5 : 0, a3, a4);
+        const int nov = ov ? sscanf(ov, "%d,%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5, &a6) : 0;
+        if (nov >= 4 && a3 > 0 && a4 > 0 && plan_variant_known(precision, a1, a2, nov >= 5 ? a5 : 0) &&
+            (a6 == 0 || (a6 == 1 && a5 >= 2)))
+            rc = build_sweep_plan(e, active, a1, a2, nov >= 5 ? a5 : 0, a3, a4, a6);
         else if (ov)
             rc = (rfb_set_error("RFSYN_FDTD_PLAN=\"%s\" names no sweep variant", ov), -1);
         else if (tune && !strcmp(tune, "0"))
@@ -1312,6 +1331,7 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->seg_len = e->plan.seg_int;
     out->ring_depth = e->plan.ns;
     out->tma = e->plan.tma;
+    out->unified = e->plan.uni;
     out->interior_items = e->plan.n_int;
     out->edge_items = e->plan.n_edge + e->plan.n_qe + e->plan.n_qx;
     size_t sca = 0;

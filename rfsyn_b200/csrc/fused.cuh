@@ -39,7 +39,9 @@ struct FusedDims {
 struct SweepItem {
     int j0, k0, ib, ie;
     // slab / boundary tiles of the work-queue sweep: 0 any (y and z slabs,
-    // boundaries), 1 no z-slab cell in the tile or its halo, 2 no y-slab cell
+    // boundaries), 1 no z-slab cell in the tile or its halo, 2 no y-slab
+    // cell, 3 narrow tile without y-slab cells, 4 any narrow tile; in the
+    // single-queue sweep also 5 interior and 6 x-slab items
     int sub = 0;
 };
 
@@ -54,6 +56,9 @@ struct FusedPlan {
     int seg_int = 64, seg_edge = 32;
     int n_int = 0, n_edge = 0;
     SweepItem *d_int = nullptr, *d_edge = nullptr;  // device work lists
+    // modes >= 2, uni = 1: every item (interior sub 5, x slab sub 6, slab /
+    // boundary subs 0-4) in the one edge list, one launch of k_sweep_q<KIND 5>
+    int uni = 0;
     int n_qe = 0, n_qx = 0;                         // modes 2, 3: edge and x-slab items of k_sweep_q
     SweepItem *d_qe = nullptr, *d_qx = nullptr;
     int *d_queue = nullptr;                         // counters (interior 0-1, edge 2-3, x slab 4-5)

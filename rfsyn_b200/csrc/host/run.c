@@ -363,6 +363,7 @@ int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info) {
     info->seg_len = ei.seg_len;
     info->ring_depth = ei.ring_depth;
     info->tma = ei.tma;
+    info->unified = ei.unified;
     info->interior_items = ei.interior_items;
     info->edge_items = ei.edge_items;
     return 0;

@@ -501,10 +501,23 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
     return !__syncthreads_or(failed);
 }
 
-// The march of one item: an edge item takes the body its `sub` names.
+// The march of one item: an edge item takes the body its `sub` names; KIND 5
+// (the single-queue sweep) takes interior (sub 5) and x-slab (sub 6) items
+// too.
 template <typename T, int TJ, int NS, int KIND>
 __device__ __forceinline__ bool q_run(const Args<T> &a, const FusedDims &d, const TmaMaps &maps, const SweepItem &it,
                                       unsigned char *smem_raw, unsigned &phase, unsigned &pending, bool &failed) {
+    if constexpr (KIND == 5) {
+        switch (it.sub) {
+            case 5: return q_item<T, TJ, NS, 0>(a, d, maps, it, smem_raw, phase, pending, failed);
+            case 6: return q_item<T, TJ, NS, 1>(a, d, maps, it, smem_raw, phase, pending, failed);
+            case 1: return q_item<T, TJ, NS, 3>(a, d, maps, it, smem_raw, phase, pending, failed);
+            case 2: return q_item<T, TJ, NS, 4>(a, d, maps, it, smem_raw, phase, pending, failed);
+            case 3: return q_item<T, TJ, NS, 4, 16>(a, d, maps, it, smem_raw, phase, pending, failed);
+            case 4: return q_item<T, TJ, NS, 2, 16>(a, d, maps, it, smem_raw, phase, pending, failed);
+            default: return q_item<T, TJ, NS, 2>(a, d, maps, it, smem_raw, phase, pending, failed);
+        }
+    }
     if constexpr (KIND == 2) {
         if (it.sub == 1) return q_item<T, TJ, NS, 3>(a, d, maps, it, smem_raw, phase, pending, failed);
         if (it.sub == 2) return q_item<T, TJ, NS, 4>(a, d, maps, it, smem_raw, phase, pending, failed);
@@ -656,10 +669,14 @@ inline void launch_q_d(const Args<double> &a, const FusedDims &d, int tj, int ns
     if (e == cudaSuccess)                                                                                   \
         e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MBE_, 2>,                                         \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
+    if (e == cudaSuccess)                                                                                   \
+        e = cudaFuncSetAttribute(k_sweep_q<TT, TJ_, NS_, MBE_, 5>,                                         \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QLayout<TT, TJ_, NS_>::total); \
     if (e == cudaSuccess) {                                                                                 \
         (void)q_grid<TT, TJ_, NS_, MBI_, 0>();                                                             \
         (void)q_grid<TT, TJ_, NS_, MBE_, 1>();                                                             \
         (void)q_grid<TT, TJ_, NS_, MBE_, 2>();                                                             \
+        (void)q_grid<TT, TJ_, NS_, MBE_, 5>();                                                             \
     }
 static inline int q_prepare() {
     static int done = 0;

@@ -27,19 +27,21 @@ pytestmark = pytest.mark.gpu
 # (rows per tile, ring depth, mode) of every compiled variant; mode 0
 # cp.async interior, 1 TMA interior, 2 work-queue sweeps, 3 work-queue
 # sweeps with tile origins shifted to the slab edges, 4 work-queue sweeps
-# with narrow (2 tj x 16) tiles over the z slabs (no periodic y / z)
+# with narrow (2 tj x 16) tiles over the z slabs (no periodic y / z); a
+# fourth value 1 puts every item of modes 2-4 in one queue (one launch)
 VARIANTS = {
-    rb.FP64: [(8, 3, 2), (8, 4, 2), (8, 3, 3), (8, 4, 3), (8, 3, 4), (8, 4, 4), (8, 3, 1), (8, 4, 1), (8, 4, 0),
-              (16, 2, 0)],
-    rb.FP32: [(8, 4, 2), (8, 3, 2), (16, 3, 2), (8, 4, 3), (16, 3, 3), (8, 4, 4), (8, 3, 4), (16, 3, 4), (8, 4, 1),
-              (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0), (16, 4, 0), (16, 3, 0)],
+    rb.FP64: [(8, 3, 2), (8, 4, 2), (8, 3, 3), (8, 4, 3), (8, 3, 4), (8, 4, 4), (8, 4, 2, 1), (8, 3, 4, 1),
+              (8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
+    rb.FP32: [(8, 4, 2), (8, 3, 2), (16, 3, 2), (8, 4, 3), (16, 3, 3), (8, 4, 4), (8, 3, 4), (16, 3, 4),
+              (8, 4, 2, 1), (8, 4, 4, 1), (16, 3, 4, 1), (8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0),
+              (16, 4, 0), (16, 3, 0)],
 }
 QUEUE = [v for v in VARIANTS[rb.FP64] if v[2] >= 2]
 MODE = {0: "cpasync", 1: "tma", 2: "queue", 3: "queue_shifted", 4: "queue_narrow"}
 
 
 def _vid(v):
-    return "tj%d_ns%d_%s" % (v[0], v[1], MODE[v[2]])
+    return "tj%d_ns%d_%s%s" % (v[0], v[1], MODE[v[2]], "_single" if len(v) > 3 and v[3] else "")
 
 SCENES = {
     # the headline recipe at 104^3 (5-cell CPML): interior tiles at k0 = 32, 64
@@ -66,8 +68,9 @@ def wants():
 
 
 def _run(s: Scene, precision: int, variant, monkeypatch, need_interior=True):
-    tj, ns, tma = variant
-    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma}")
+    tj, ns, tma = variant[:3]
+    uni = variant[3] if len(variant) > 3 else 0
+    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma},{uni}")
     rc = scene_run_config(s, precision, rb.FUSED)
     cs = s.to_c()
     needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres or s.tensor3)
@@ -75,9 +78,9 @@ def _run(s: Scene, precision: int, variant, monkeypatch, need_interior=True):
                  C.cast(C.pointer(cs), C.c_void_p) if needs_setup else None)
     try:
         info = sim.info()
-        assert (info.tile_j, info.ring_depth, info.tma) == (tj, ns, tma)
+        assert (info.tile_j, info.ring_depth, info.tma, info.unified) == (tj, ns, tma, uni)
         assert info.edge_items > 0
-        if need_interior:
+        if need_interior and not uni:
             assert info.interior_items > 0
         sim.advance(s.n_steps)
         return sim.probes(), sim.dft()
@@ -89,7 +92,7 @@ def _narrow_on_wrap(s: Scene, variant, monkeypatch) -> bool:
     """Mode 4 on a scene with periodic y or z: the session must refuse it."""
     if variant[2] != 4 or not (s.periodic & 6):
         return False
-    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{variant[0]},{variant[1]},32,16,4")
+    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{variant[0]},{variant[1]},32,16,4,{variant[3] if len(variant) > 3 else 0}")
     with pytest.raises(RuntimeError, match="non-periodic y and z"):
         rb.Sim(scene_run_config(s, rb.FP64, rb.FUSED))
     return True
