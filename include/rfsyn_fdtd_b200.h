@@ -225,10 +225,12 @@ int fdtd_b200_batch_dft(fdtd_b200_batch_t *batch, size_t scene, double *dft_re, 
 typedef struct {
     size_t scenes, cells, list_cells, slab_cell_axes;
     int tile_j, ring_depth;
-    int mode;                    /* 2: tiles from the origin; 3: origins shifted to the slab edges */
+    int mode;                    /* 2: tiles from the origin; 3: origins shifted to the slab edges;
+                                    4: narrow tiles over the z slabs */
     int seg_interior, seg_edge;  /* planes per work item */
     int items_interior, items_xslab, items_edge;
     int launches_per_step;
+    int unified;                 /* 1: every sweep item in one work queue, one launch per step */
 } fdtd_b200_batch_info_t;
 
 int fdtd_b200_batch_info(const fdtd_b200_batch_t *batch, fdtd_b200_batch_info_t *info);

@@ -119,7 +119,8 @@ class BatchInfo(C.Structure):
     _fields_ = [("scenes", C.c_size_t), ("cells", C.c_size_t), ("list_cells", C.c_size_t),
                 ("slab_cell_axes", C.c_size_t), ("tile_j", C.c_int), ("ring_depth", C.c_int), ("mode", C.c_int),
                 ("seg_interior", C.c_int), ("seg_edge", C.c_int), ("items_interior", C.c_int),
-                ("items_xslab", C.c_int), ("items_edge", C.c_int), ("launches_per_step", C.c_int)]
+                ("items_xslab", C.c_int), ("items_edge", C.c_int), ("launches_per_step", C.c_int),
+                ("unified", C.c_int)]
 
 
 SETUP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)

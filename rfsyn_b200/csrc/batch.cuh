@@ -177,7 +177,11 @@ inline void launch_qb(const Args<T> *args, const FusedDims *dims, const TmaMaps 
     if (e == cudaSuccess)                                                                                   \
         e = cudaFuncSetAttribute(k_sweep_qb<TT, TJ_, NS_, RFB_QB_MINB(TT, TJ_, MBI_, MBE_, 2), 2>,                   \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QBLayout<TT, TJ_, NS_>::total); \
+    if (e == cudaSuccess)                                                                                   \
+        e = cudaFuncSetAttribute(k_sweep_qb<TT, TJ_, NS_, RFB_QB_MINB(TT, TJ_, MBI_, MBE_, 5), 5>,                   \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QBLayout<TT, TJ_, NS_>::total); \
     if (e == cudaSuccess) {                                                                                 \
+        (void)qb_grid<TT, TJ_, NS_, RFB_QB_MINB(TT, TJ_, MBI_, MBE_, 5), 5>();                                       \
         (void)qb_grid<TT, TJ_, NS_, RFB_QB_MINB(TT, TJ_, MBI_, MBE_, 0), 0>();                                       \
         (void)qb_grid<TT, TJ_, NS_, RFB_QB_MINB(TT, TJ_, MBI_, MBE_, 1), 1>();                                       \
         (void)qb_grid<TT, TJ_, NS_, RFB_QB_MINB(TT, TJ_, MBI_, MBE_, 2), 2>();                                       \
@@ -210,8 +214,9 @@ struct rfb_batch {
     void *d_args[2] = {};          // Args<T>[n] per parity
     FusedDims *d_dims = nullptr;
     TmaMaps *d_maps[2] = {};
-    BatchItem *d_items[3] = {};    // interior, x slab, edge
+    BatchItem *d_items[3] = {};    // interior, x slab, edge (uni: every item in the edge list)
     int n_items[3] = {};
+    int uni = 0;
     int2 *d_lblocks = nullptr;
     int n_lblocks = 0;
     void *d_probes = nullptr;
@@ -240,11 +245,12 @@ static void batch_free_plan(rfb_batch *b) {
 }
 
 // Work lists and per-scene tensor maps / dims of one plan.
-static int batch_build_plan(rfb_batch *b, int tj, int ns, int mode, int seg_int, int seg_edge) {
+static int batch_build_plan(rfb_batch *b, int tj, int ns, int mode, int seg_int, int seg_edge, int uni = 0) {
     batch_free_plan(b);
     b->tj = tj;
     b->ns = ns;
     b->mode = mode;
+    b->uni = uni;
     b->seg_int = seg_int;
     b->seg_edge = seg_edge;
     const size_t n = b->m.size();
@@ -273,11 +279,19 @@ static int batch_build_plan(rfb_batch *b, int tj, int ns, int mode, int seg_int,
         maps[0][s] = e->tmaps[0];
         maps[1][s] = e->tmaps[1];
     }
+    if (uni) {
+        // one queue for every item (interior sub 5, x slab sub 6)
+        for (BatchItem it : lists[0]) it.t.sub = 5, lists[2].push_back(it);
+        for (BatchItem it : lists[1]) it.t.sub = 6, lists[2].push_back(it);
+        lists[0].clear();
+        lists[1].clear();
+    }
     for (int k = 0; k < 3; k++) {
-        // longest items first across the whole batch
-        std::stable_sort(lists[k].begin(), lists[k].end(), [](const BatchItem &x, const BatchItem &y) {
-            return x.t.ie - x.t.ib > y.t.ie - y.t.ib;
-        });
+        // costliest items first across the whole batch (a slab or boundary
+        // plane costs about four interior planes)
+        auto cost = [](const BatchItem &x) { return (x.t.ie - x.t.ib) * (x.t.sub == 5 ? 1 : 4); };
+        std::stable_sort(lists[k].begin(), lists[k].end(),
+                         [&](const BatchItem &x, const BatchItem &y) { return cost(x) > cost(y); });
         b->n_items[k] = (int)lists[k].size();
         if (b->n_items[k]) {
             CK(cudaMalloc(&b->d_items[k], lists[k].size() * sizeof(BatchItem)));
@@ -300,6 +314,11 @@ template <typename T>
 static void batch_sweep(rfb_batch *b, int par) {
     const Args<T> *args = (const Args<T> *)b->d_args[par];
     const TmaMaps *maps = b->d_maps[par];
+    if (b->uni) {
+        launch_qb<5, T>(args, b->d_dims, maps, b->tj, b->ns, b->d_items[2], b->n_items[2], b->d_queue + 2, b->d_err,
+                        b->stream);
+        return;
+    }
     cudaEventRecord(b->ev_fork, b->stream);
     cudaStreamWaitEvent(b->stream2, b->ev_fork, 0);
     launch_qb<0, T>(args, b->d_dims, maps, b->tj, b->ns, b->d_items[0], b->n_items[0], b->d_queue, b->d_err,
@@ -367,7 +386,7 @@ fail:
 // bit-identical fields, so the choice changes speed only.
 static int batch_autotune(rfb_batch *b) {
     struct Cand {
-        int tj, ns, mode, si, se;
+        int tj, ns, mode, si, se, uni;
     };
     std::vector<Cand> cands;
     const InteriorVariant *v = b->prec == RFB_FP32 ? kQVariantsFp32 : kQVariantsFp64;
@@ -377,16 +396,17 @@ static int batch_autotune(rfb_batch *b) {
     for (size_t q = 0; q < nv; q++)
         for (int mode = 2; mode <= (wrap_yz ? 3 : 4); mode++)
             for (int si : {32, 64})
-                for (int se : {16, 32}) cands.push_back(Cand{v[q].tj, v[q].ns, mode, si, se});
+                for (int se : {16, 32})
+                    for (int uni : {0, 1}) cands.push_back(Cand{v[q].tj, v[q].ns, mode, si, se, uni});
     const char *ov = getenv("RFSYN_FDTD_PLAN");
     if (ov) {
-        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
-        if (sscanf(ov, "%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5) != 5 || a5 < 2 || a3 <= 0 || a4 <= 0 ||
-            !plan_variant_known(b->prec, a1, a2, a5)) {
+        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
+        const int nov = sscanf(ov, "%d,%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5, &a6);
+        if (nov < 5 || a5 < 2 || a3 <= 0 || a4 <= 0 || a6 < 0 || a6 > 1 || !plan_variant_known(b->prec, a1, a2, a5)) {
             rfb_set_error("RFSYN_FDTD_PLAN=\"%s\" names no work-queue sweep variant", ov);
             return -1;
         }
-        return batch_build_plan(b, a1, a2, a5, a3, a4);
+        return batch_build_plan(b, a1, a2, a5, a3, a4, a6);
     }
     Cand best = cands[0];
     float best_ms = 1e30f;
@@ -395,7 +415,7 @@ static int batch_autotune(rfb_batch *b) {
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     for (const Cand &c : cands) {
-        if (batch_build_plan(b, c.tj, c.ns, c.mode, c.si, c.se) != 0) goto fail;
+        if (batch_build_plan(b, c.tj, c.ns, c.mode, c.si, c.se, c.uni) != 0) goto fail;
         for (int w = 0; w < 5; w++) {
             if (w == 2) CK(cudaEventRecord(t0, b->stream));
             if (b->prec == RFB_FP64) batch_sweep<double>(b, par);
@@ -421,7 +441,7 @@ static int batch_autotune(rfb_batch *b) {
             return -1;
         }
     }
-    if (batch_build_plan(b, best.tj, best.ns, best.mode, best.si, best.se) != 0) return -1;
+    if (batch_build_plan(b, best.tj, best.ns, best.mode, best.si, best.se, best.uni) != 0) return -1;
     // the tuning sweeps advanced the fields: start from the zero state again
     if (rfb_batch_reset(b) != 0) return -1;
     CK(cudaStreamSynchronize(b->stream));
@@ -695,6 +715,7 @@ extern "C" int rfb_batch_info(rfb_batch_t *b, rfb_batch_info_t *out) {
     out->tile_j = b->tj;
     out->ring_depth = b->ns;
     out->mode = b->mode;
+    out->unified = b->uni;
     out->seg_interior = b->seg_int;
     out->seg_edge = b->seg_edge;
     out->items_interior = b->n_items[0];

@@ -965,28 +965,28 @@ static int autotune(rfb_engine *e, int active) {
             for (int si : segs_int)
                 for (int se : segs_edge)
                     for (int uni = 0; uni <= (cv.tma >= 2 ? 1 : 0); uni++) {
-                    const InteriorVariant &v = cv.v;
-                    if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se, uni) != 0) goto fail;
-                    for (int w = 0; w < 2; w++) {
-                        if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
-                        else enqueue_sweep<float>(e, par);
-                        par ^= 1;
+                        const InteriorVariant &v = cv.v;
+                        if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se, uni) != 0) goto fail;
+                        for (int w = 0; w < 2; w++) {
+                            if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
+                            else enqueue_sweep<float>(e, par);
+                            par ^= 1;
+                        }
+                        CK(cudaEventRecord(t0, e->stream));
+                        for (int w = 0; w < reps; w++) {
+                            if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
+                            else enqueue_sweep<float>(e, par);
+                            par ^= 1;
+                        }
+                        CK(cudaEventRecord(t1, e->stream));
+                        CK(cudaEventSynchronize(t1));
+                        float ms = 0.f;
+                        CK(cudaEventElapsedTime(&ms, t0, t1));
+                        if (ms < best_ms) {
+                            best_ms = ms;
+                            best = TunedPlan{v.tj, v.ns, cv.tma, si, se, uni};
+                        }
                     }
-                    CK(cudaEventRecord(t0, e->stream));
-                    for (int w = 0; w < reps; w++) {
-                        if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
-                        else enqueue_sweep<float>(e, par);
-                        par ^= 1;
-                    }
-                    CK(cudaEventRecord(t1, e->stream));
-                    CK(cudaEventSynchronize(t1));
-                    float ms = 0.f;
-                    CK(cudaEventElapsedTime(&ms, t0, t1));
-                    if (ms < best_ms) {
-                        best_ms = ms;
-                        best = TunedPlan{v.tj, v.ns, cv.tma, si, se, uni};
-                    }
-                }
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);

@@ -134,6 +134,7 @@ typedef struct {
     int tile_j, ring_depth, mode, seg_interior, seg_edge;
     int items_interior, items_xslab, items_edge;
     int launches_per_step;
+    int unified;
 } rfb_batch_info_t;
 /* Takes ownership of the members (and of `stream` when own_stream). */
 rfb_batch_t *rfb_batch_create(rfb_engine_t **members, size_t n, void *stream, int own_stream);

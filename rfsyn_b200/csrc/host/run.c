@@ -680,5 +680,6 @@ int fdtd_b200_batch_info(const fdtd_b200_batch_t *bt, fdtd_b200_batch_info_t *in
     info->items_xslab = bi.items_xslab;
     info->items_edge = bi.items_edge;
     info->launches_per_step = bi.launches_per_step;
+    info->unified = bi.unified;
     return 0;
 }
