@@ -271,45 +271,44 @@ __device__ __forceinline__ T e_ade(const Args<T> &a, int e, int comp, int i, int
     return en;
 }
 
-// Curl difference of E component b at cell (i, j, k) from the advanced H:
-// (H_{b+2}(p) - H_{b+2}(p - e_{b+1})) - (H_{b+1}(p) - H_{b+1}(p - e_{b+2})),
-// the unstretched terms of the E update (materials.c:920-1059), indices
-// wrapped on periodic axes.
-template <typename T>
-__device__ __forceinline__ T curl_diff(const Args<T> &a, int b, int i, int j, int k) {
-    const int fa = (b + 2) % 3, axa = (b + 1) % 3, fb = (b + 1) % 3, axb = (b + 2) % 3;
-    int pa[3] = {i, j, k}, pb[3] = {i, j, k};
-    const int n[3] = {a.nx, a.ny, a.nz};
-    pa[axa] = pa[axa] == 0 ? n[axa] - 1 : pa[axa] - 1;
-    pb[axb] = pb[axb] == 0 ? n[axb] - 1 : pb[axb] - 1;
-    const T tA = xs(a.Ho[fa][cidx(a, i, j, k)], a.Ho[fa][cidx(a, pa[0], pa[1], pa[2])]);
-    const T tB = xs(a.Ho[fb][cidx(a, i, j, k)], a.Ho[fb][cidx(a, pb[0], pb[1], pb[2])]);
-    return xs(tA, tB);
-}
-
 // Full 3x3 sample of component c at (i, j, k), record r = (m_c0, m_c1, m_c2,
 // s): value = m_cc D_c, then for b = 0, 1, 2 (b != c) value += m_cb (0.25
 // (((D_b(w) + D_b(w + e_c)) + D_b(w - e_b)) + D_b(w + e_c - e_b))); the
-// result is E + s value.  Neighbours wrap on periodic axes only (the host
+// result is E + s value.  D_b(p) is the curl difference of E component b
+// from the advanced H, (H_{b+2}(p) - H_{b+2}(p - e_{b+1})) - (H_{b+1}(p) -
+// H_{b+1}(p - e_{b+2})), the unstretched terms of the E update
+// (materials.c:920-1059).  Neighbours wrap on periodic axes only (the host
 // admits samples in [1, n-1] on the other axes, so every index used is in
 // the padded grid: a step back never leaves it, a step forward reaches at
 // most the padded boundary sample n).
 template <typename T>
 __device__ __forceinline__ T e_tensor3(const Args<T> &a, const T *r, int c, int i, int j, int k, T v) {
+    // linear indices by strides from the sample's own; a step back from
+    // coordinate 0 wraps to n - 1 (reached only on periodic axes)
     const int n[3] = {a.nx, a.ny, a.nz};
-    T value = xm(r[c], curl_diff(a, c, i, j, k));
+    const long long st[3] = {(long long)(a.ny + 1) * a.pitch, a.pitch, 1};
+    auto curl_at = [&](int b, long long q, const int p[3]) {
+        const int fa = (b + 2) % 3, axa = (b + 1) % 3, fb = (b + 1) % 3, axb = (b + 2) % 3;
+        const long long qa = p[axa] == 0 ? q + (long long)(n[axa] - 1) * st[axa] : q - st[axa];
+        const long long qb = p[axb] == 0 ? q + (long long)(n[axb] - 1) * st[axb] : q - st[axb];
+        return xs(xs(a.Ho[fa][q], a.Ho[fa][qa]), xs(a.Ho[fb][q], a.Ho[fb][qb]));
+    };
+    const int p0[3] = {i, j, k};
+    const long long c0 = cidx(a, i, j, k);
+    T value = xm(r[c], curl_at(c, c0, p0));
+    const bool wrap = ((a.per >> c) & 1u) && p0[c] + 1 == n[c];
+    int p1[3] = {i, j, k};
+    p1[c] = wrap ? 0 : p1[c] + 1;
+    const long long c1 = wrap ? c0 - (long long)(n[c] - 1) * st[c] : c0 + st[c];
     for (int b = 0; b < 3; b++) {
         if (b == c) continue;
-        int p0[3] = {i, j, k};
-        int p1[3] = {i, j, k};
-        p1[c] = ((a.per >> c) & 1u) && p1[c] + 1 == n[c] ? 0 : p1[c] + 1;
         int p2[3] = {p0[0], p0[1], p0[2]};
         p2[b] = p2[b] == 0 ? n[b] - 1 : p2[b] - 1;
         int p3[3] = {p1[0], p1[1], p1[2]};
         p3[b] = p3[b] == 0 ? n[b] - 1 : p3[b] - 1;
-        const T s4 = xa(xa(xa(curl_diff(a, b, p0[0], p0[1], p0[2]), curl_diff(a, b, p1[0], p1[1], p1[2])),
-                           curl_diff(a, b, p2[0], p2[1], p2[2])),
-                        curl_diff(a, b, p3[0], p3[1], p3[2]));
+        const long long back = p0[b] == 0 ? (long long)(n[b] - 1) * st[b] : -st[b];
+        const T s4 = xa(xa(xa(curl_at(b, c0, p0), curl_at(b, c1, p1)), curl_at(b, c0 + back, p2)),
+                        curl_at(b, c1 + back, p3));
         value = xa(value, xm(r[b], xm(T(0.25), s4)));
     }
     return xa(v, xm(r[3], value));
