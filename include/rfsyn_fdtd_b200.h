@@ -355,6 +355,35 @@ typedef struct {
 int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_sphere_t *spheres,
                                     size_t n_spheres, int smoothing);
 
+/* ---- heightmap world -----------------------------------------------------------
+ * rfsyn's terrain description (engine/world/world.h:10-17, world.c:49-135):
+ * column (i, j) is solid material column_materials[i ny + j] up to height
+ * heights_m[i ny + j] (0 .. nz dx; air columns have height 0).  rfsyn loads
+ * such worlds and a material catalog but never applies them to an FDTD grid
+ * (cli/main.c:325-333).  This maps one onto the materials of a grid with the
+ * same cells: media[id] gives eps_r and sigma of world material id (for
+ * example rfsyn's material_catalog_evaluate at the simulation frequency).
+ * Cells take world.c's bulk id (solid where the solid fraction is >= 1/2);
+ * with smoothing, every E component of a cell cut by the surface gets the
+ * diagonal of the smoothed inverse permittivity along the world's surface
+ * normal, the rule fdtd_b200_materials_add_spheres uses.  Box assignment
+ * semantics: the columns' earlier descriptions are replaced.  Returns 0 (and
+ * the number of cut cells in *mixed_out) or -1 with fdtd_b200_last_error(),
+ * rejecting what world_create_heightmap rejects. */
+typedef struct {
+    size_t nx, ny, nz;                 /* world cells: the grid's */
+    double dx;                         /* the grid's */
+    const double *heights_m;           /* nx * ny */
+    const uint8_t *column_materials;   /* nx * ny world material ids */
+    uint8_t air_id;
+} fdtd_b200_heightmap_t;
+typedef struct {
+    double eps_r, sigma;
+} fdtd_b200_medium_t;
+int fdtd_b200_materials_apply_heightmap(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_heightmap_t *hm,
+                                        const fdtd_b200_medium_t *media, size_t n_media, int smoothing,
+                                        size_t *mixed_out);
+
 /* ---- sphere fill fractions without device allocation --------------------------
  * No counterpart in rfsyn.  For callers that cannot allocate device memory
  * when they rasterise a sphere: a thread building scenes while another

@@ -197,6 +197,45 @@ class SceneSetup:
         self.fn = SETUP_FN(cb)
         self.ptr = C.cast(self.fn, C.c_void_p)
 
+class Heightmap(C.Structure):
+    _fields_ = [("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t), ("dx", C.c_double),
+                ("heights_m", C.POINTER(C.c_double)), ("column_materials", C.POINTER(C.c_uint8)),
+                ("air_id", C.c_uint8)]
+
+
+class Medium(C.Structure):
+    _fields_ = [("eps_r", C.c_double), ("sigma", C.c_double)]
+
+
+class HeightmapSetup:
+    """An fdtd_material_setup_fn that maps a heightmap world onto the grid
+    (fdtd_b200_materials_apply_heightmap).  heights: (nx, ny) metres;
+    columns: (nx, ny) world material ids; media: [(eps_r, sigma)] per id.
+    After the setup ran, `mixed` holds the number of cells cut by the
+    surface."""
+
+    def __init__(self, heights, columns, media, nz: int, dx: float, air_id: int = 0, smoothing: int = 1):
+        lib = load()
+        h = np.ascontiguousarray(heights, dtype=np.float64)
+        ids = np.ascontiguousarray(columns, dtype=np.uint8)
+        self._h, self._ids = h, ids
+        self._media = (Medium * len(media))(*[Medium(e, s) for (e, s) in media])
+        self.mixed = None
+        mixed = C.c_size_t(0)
+
+        def cb(grid, mat, ctx):
+            hm = Heightmap(h.shape[0], h.shape[1], nz, dx, _dptr(h), ids.ctypes.data_as(C.POINTER(C.c_uint8)),
+                           air_id)
+            if lib.fdtd_b200_materials_apply_heightmap(mat, grid, C.byref(hm), self._media, len(media), smoothing,
+                                                        C.byref(mixed)) != 0:
+                return -1
+            self.mixed = mixed.value
+            return 0
+
+        self.fn = SETUP_FN(cb)
+        self.ptr = C.cast(self.fn, C.c_void_p)
+
+
 _lib = None
 
 
@@ -232,6 +271,8 @@ def load() -> C.CDLL:
         "fdtd_b200_version": (C.c_char_p, []),
         "cpml_default_params": (CpmlParams, [S]),
         "fdtd_b200_materials_add_spheres": (I, [P, P, C.POINTER(Sphere), S, I]),
+        "fdtd_b200_materials_apply_heightmap": (I, [P, P, C.POINTER(Heightmap), C.POINTER(Medium), S, I,
+                                                    C.POINTER(C.c_size_t)]),
         "materials_set_box": (I, [P, P, S, S, S, S, S, S, D, D]),
         "fdtd_b200_materials_set_dispersive_box": (I, [P, P, S, S, S, S, S, S, P]),
         "fdtd_b200_materials_set_tensor3_slab": (I, [P, P, C.POINTER(D), C.POINTER(D), D, C.POINTER(D)]),

@@ -756,6 +756,138 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
     return 0;
 }
 
+/* ---- heightmap world -> materials --------------------------------------------
+ * rfsyn describes terrain as a heightmap world (engine/world/world.c:49-135):
+ * column (i, j) holds solid material column_materials[i ny + j] up to height
+ * h; cell (i, j, k) has the solid fraction f = clamp(h/dx - k, 0, 1) (height
+ * clipped to the domain, world.c:23-28, :94-95), its bulk id is the solid
+ * where f >= 0.5 and air elsewhere (:98), and a cell with 0 < f < 1 carries
+ * the surface normal (-gx, -gy, 1) / |.| from central differences of the
+ * heights, one-sided at the edges (:30-47).  rfsyn never applies a world to
+ * its FDTD grid (cli/main.c:325-333); this maps it onto the materials: bulk
+ * ids per column run, and with smoothing, every E component of a mixed cell
+ * gets the diagonal of the smoothed inverse permittivity used for spheres,
+ *   1/eps_c = n_c^2 (f/eps_s + (1-f)/eps_a) + (1 - n_c^2) / (f eps_s + (1-f) eps_a),
+ *   sigma_c = f sigma_s + (1 - f) sigma_a. */
+static double hm_fraction(double hc, size_t k) {
+    double f = hc - (double)k;
+    if (f <= 0.0) return 0.0;
+    if (f >= 1.0) return 1.0;
+    return f;
+}
+
+static int hm_normal(const fdtd_b200_heightmap_t *hm, size_t i, size_t j, double n[3]) {
+    const size_t il = i ? i - 1 : i, ir = i + 1 < hm->nx ? i + 1 : i;
+    const size_t jl = j ? j - 1 : j, jr = j + 1 < hm->ny ? j + 1 : j;
+    double gx = 0.0, gy = 0.0;
+    if (ir != il) gx = (hm->heights_m[ir * hm->ny + j] - hm->heights_m[il * hm->ny + j]) / ((double)(ir - il) * hm->dx);
+    if (jr != jl) gy = (hm->heights_m[i * hm->ny + jr] - hm->heights_m[i * hm->ny + jl]) / ((double)(jr - jl) * hm->dx);
+    const double len = hypot(hypot(gx, gy), 1.0);
+    if (!isfinite(len) || len <= 0.0) return -1;
+    n[0] = -gx / len;
+    n[1] = -gy / len;
+    n[2] = 1.0 / len;
+    return 0;
+}
+
+int fdtd_b200_materials_apply_heightmap(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_heightmap_t *hm,
+                                        const fdtd_b200_medium_t *media, size_t n_media, int smoothing,
+                                        size_t *mixed_out) {
+    if (mixed_out) *mixed_out = 0;
+    if (!materials_matches(mat, g) || !hm || !hm->heights_m || !hm->column_materials || !media) {
+        rfb_set_error("heightmap: NULL argument or materials of another grid");
+        return -1;
+    }
+    if (hm->nx != g->nx || hm->ny != g->ny || hm->nz != g->nz || !isfinite(hm->dx) || hm->dx <= 0.0 ||
+        fabs(hm->dx - g->dx) > 1e-12 * g->dx) {
+        rfb_set_error("heightmap: its cells must be the grid's (nx, ny, nz, dx)");
+        return -1;
+    }
+    if ((size_t)hm->air_id >= n_media) {
+        rfb_set_error("heightmap: no medium for the air id %d", (int)hm->air_id);
+        return -1;
+    }
+    const size_t cols = hm->nx * hm->ny;
+    const double top = (double)hm->nz * hm->dx;
+    for (size_t q = 0; q < cols; q++) {
+        const double h = hm->heights_m[q];
+        if (!isfinite(h) || h < 0.0 || h > top || (h > 0.0 && hm->column_materials[q] == hm->air_id) ||
+            (size_t)hm->column_materials[q] >= n_media) {
+            rfb_set_error("heightmap: column %zu has an invalid height or material", q);
+            return -1;
+        }
+    }
+    /* media -> material ids, registered on first use */
+    int id_of[256];
+    for (int q = 0; q < 256; q++) id_of[q] = -1;
+    for (size_t q = 0; q <= cols; q++) {
+        const uint8_t w = q < cols ? hm->column_materials[q] : hm->air_id;
+        if (id_of[w] >= 0) continue;
+        material_id_t id;
+        if (materials_register(mat, media[w].eps_r, media[w].sigma, &id) != 0) {
+            rfb_set_error("heightmap: medium %d rejected (eps_r >= 1, sigma >= 0, at most 256 materials)", (int)w);
+            return -1;
+        }
+        id_of[w] = id;
+    }
+    /* bulk ids: the solid run below, air above (box assignment clears any
+     * description the cells had) */
+    for (size_t i = 0; i < hm->nx; i++)
+        for (size_t j = 0; j < hm->ny; j++) {
+            const size_t q = i * hm->ny + j;
+            const double hc = fmin(hm->heights_m[q] / hm->dx, (double)hm->nz);
+            size_t kb = 0;
+            while (kb < hm->nz && hm_fraction(hc, kb) >= 0.5) kb++;
+            if (kb > 0 &&
+                materials_assign_box(mat, g, i, i + 1, j, j + 1, 0, kb, (material_id_t)id_of[hm->column_materials[q]]))
+                return -1;
+            if (kb < hm->nz &&
+                materials_assign_box(mat, g, i, i + 1, j, j + 1, kb, hm->nz, (material_id_t)id_of[hm->air_id]))
+                return -1;
+        }
+    /* mixed cells */
+    size_t mixed = 0;
+    const fdtd_b200_medium_t air = media[hm->air_id];
+    for (size_t i = 0; i < hm->nx; i++)
+        for (size_t j = 0; j < hm->ny; j++) {
+            const size_t q = i * hm->ny + j;
+            const double hc = fmin(hm->heights_m[q] / hm->dx, (double)hm->nz);
+            const fdtd_b200_medium_t sol = media[hm->column_materials[q]];
+            for (size_t k = 0; k < hm->nz; k++) {
+                const double f = hm_fraction(hc, k);
+                if (!(f > 0.0 && f < 1.0)) continue;
+                mixed++;
+                if (!smoothing) continue;
+                double n[3];
+                if (hm_normal(hm, i, j, n) != 0) {
+                    rfb_set_error("heightmap: no surface normal at column %zu", q);
+                    return -1;
+                }
+                const size_t w = fdtd_index(g, i, j, k);
+                for (int c = 0; c < 3; c++) {
+                    if (!sample_valid(g, c, i, j, k)) continue;
+                    const double n2 = n[c] * n[c];
+                    const double mean = f * sol.eps_r + (1.0 - f) * air.eps_r;
+                    const double minv = f / sol.eps_r + (1.0 - f) / air.eps_r;
+                    const double inv = n2 * minv + (1.0 - n2) / mean;
+                    material_coeff_t co;
+                    if (make_coeff(mat, 1.0 / inv, f * sol.sigma + (1.0 - f) * air.sigma, &co) != 0) {
+                        rfb_set_error("heightmap: smoothed medium out of range");
+                        return -1;
+                    }
+                    const double v[2] = {co.Ca, co.Cb};
+                    if (omap_put(&mat->scalar, (uint64_t)w * 3 + (uint64_t)c, v) != 0) {
+                        rfb_set_error("out of host memory mapping the heightmap");
+                        return -1;
+                    }
+                }
+            }
+        }
+    mat->version++;
+    if (mixed_out) *mixed_out = mixed;
+    return 0;
+}
+
 /* Symmetric Ex/Ey coupling weight of two tensor edges (materials.c:836-845):
  * 0.25 * rho * sqrt(m11_x) * sqrt(m11_y) with rho the mean normalised
  * off-diagonal correlation; evaluated in the same order for bit parity. */
