@@ -141,6 +141,24 @@ void *fdtd_b200_sim_stream(const fdtd_b200_sim_t *sim);
 int fdtd_b200_sim_read_probes(fdtd_b200_sim_t *sim, double *probe_td);
 /* n_probes * n_freqs each, over the steps done so far (blocking). */
 int fdtd_b200_sim_dft(fdtd_b200_sim_t *sim, double *dft_re, double *dft_im);
+
+/* ---- the stage's output signal, AWGN and .iq files ---------------------------
+ * rfsyn's CLI chain after the FDTD stage: the probe series becomes a complex
+ * float signal (float)td[n] + 0i (cli/fdtd_stage.c:23-24), awgn_create(snr_db,
+ * seed, stream) adds white Gaussian noise of per-axis deviation
+ * sqrt(P / 10^(snr_db/10) / 2), P the mean power, drawn with rfsyn's PCG32
+ * stream and Box-Muller pair per sample (engine/noise/awgn.c:16-44), and
+ * write_signal stores the samples as interleaved float32 I/Q
+ * (cli/main.c:70-85).  fdtd_b200_sim_read_iq computes the same samples on
+ * the GPU from the resident probe series and returns 2 n_steps floats (I, Q
+ * per sample); awgn NULL leaves the noise out.  fdtd_b200_iq_write writes n
+ * samples to a file as write_signal does (0, or -1). */
+typedef struct {
+    float snr_db;
+    uint64_t seed, stream;
+} fdtd_b200_awgn_t;
+int fdtd_b200_sim_read_iq(fdtd_b200_sim_t *sim, size_t probe, const fdtd_b200_awgn_t *awgn, float *iq_out);
+int fdtd_b200_iq_write(const char *path, const float *iq, size_t n_samples);
 /* One field component in rfsyn's padded layout, (nx+1)(ny+1)(nz+1) doubles. */
 int fdtd_b200_sim_read_field(fdtd_b200_sim_t *sim, field_component_t component, double *host);
 /* Kernels launched per time step by this session. */

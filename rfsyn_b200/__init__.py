@@ -197,6 +197,10 @@ class SceneSetup:
         self.fn = SETUP_FN(cb)
         self.ptr = C.cast(self.fn, C.c_void_p)
 
+class Awgn(C.Structure):
+    _fields_ = [("snr_db", C.c_float), ("seed", C.c_uint64), ("stream", C.c_uint64)]
+
+
 class Heightmap(C.Structure):
     _fields_ = [("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t), ("dx", C.c_double),
                 ("heights_m", C.POINTER(C.c_double)), ("column_materials", C.POINTER(C.c_uint8)),
@@ -261,6 +265,8 @@ def load() -> C.CDLL:
         "fdtd_b200_sim_steps_done": (S, [P]),
         "fdtd_b200_sim_stream": (P, [P]),
         "fdtd_b200_sim_read_probes": (I, [P, C.POINTER(D)]),
+        "fdtd_b200_sim_read_iq": (I, [P, S, C.POINTER(Awgn), C.POINTER(C.c_float)]),
+        "fdtd_b200_iq_write": (I, [C.c_char_p, C.POINTER(C.c_float), S]),
         "fdtd_b200_sim_dft": (I, [P, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_sim_read_field": (I, [P, I, C.POINTER(D)]),
         "fdtd_b200_sim_launches_per_step": (I, [P]),
@@ -465,6 +471,16 @@ class Sim:
         if self.lib.fdtd_b200_sim_read_probes(self.h, _dptr(out)) != 0:
             raise RuntimeError(last_error())
         return out[: c.n_probes]
+
+    def read_iq(self, probe: int, snr_db: float | None = None, seed: int = 0, stream: int = 0) -> np.ndarray:
+        """The stage's complex64 signal of one probe, with rfsyn's AWGN when
+        snr_db is given (fdtd_b200_sim_read_iq)."""
+        n = self.rc.c.n_steps
+        out = np.zeros(2 * n, dtype=np.float32)
+        awgn = C.byref(Awgn(snr_db, seed, stream)) if snr_db is not None else None
+        if self.lib.fdtd_b200_sim_read_iq(self.h, probe, awgn, out.ctypes.data_as(C.POINTER(C.c_float))) != 0:
+            raise RuntimeError(last_error())
+        return out.view(np.complex64)
 
     def dft(self) -> np.ndarray:
         c = self.rc.c

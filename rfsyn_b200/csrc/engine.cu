@@ -17,6 +17,7 @@
 #include "tma.cuh"
 #include "sweep.cuh"
 #include "energy.cuh"
+#include "iq.cuh"
 
 using namespace rfb;
 
@@ -412,6 +413,7 @@ struct rfb_engine {
     TmaMaps tmaps[2];       // tensor maps of the input buffers per parity (TMA interior sweep)
     int *d_err = nullptr;   // set by a sweep whose copies did not complete in time
     double *d_energy = nullptr;  // energy audit: block partials + result
+    float *d_iq = nullptr;       // stage output: n_steps I/Q pairs, then the noise scale (a double)
     size_t h2d_bytes = 0, n_ade = 0;
     // plane wave (TF/SF): line, H-target terms, per-entry E terms
     int tf_on = 0, tf_n_h = 0, tf_m_len = 0;
@@ -1027,7 +1029,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     devcpml_free(e->cpml);
     devscene_free(e->scene);
     cudaFree(e->src_val); cudaFree(e->src_hard);
-    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy);
+    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy); cudaFree(e->d_iq);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
     cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_qx); cudaFree(e->plan.d_queue);
     cudaFree(e->tf_inc_e); cudaFree(e->tf_inc_h); cudaFree(e->tf_src); cudaFree(e->tf_h_cell); cudaFree(e->tf_h_comp);
@@ -1492,6 +1494,41 @@ fail:
 extern "C" void *rfb_engine_stream(rfb_engine_t *e) { return (void *)e->stream; }
 extern "C" size_t rfb_engine_steps_done(rfb_engine_t *e) { return e->steps_done; }
 extern "C" int rfb_engine_launches_per_step(rfb_engine_t *e) { return e->launches_per_step; }
+
+// The FDTD stage's signal of one probe, optionally with rfsyn's AWGN, as
+// interleaved float I/Q (2 n_steps floats) in host memory.
+extern "C" int rfb_engine_read_iq(rfb_engine_t *e, int probe, int noise, double snr_linear, unsigned long long seed,
+                                  unsigned long long stream, float *out) {
+    const long long n = (long long)e->n_steps;
+    if (probe < 0 || probe >= e->n_probes || !out) {
+        rfb_set_error("read_iq: no probe %d", probe);
+        return -1;
+    }
+    // samples, then the noise scale in an 8-byte slot at float offset 2 n + 2
+    if (!e->d_iq) CK(cudaMalloc(&e->d_iq, (size_t)(2 * n + 4) * sizeof(float)));
+    {
+        double *d_std = noise ? reinterpret_cast<double *>(e->d_iq + 2 * n + 2) : nullptr;
+        const size_t off = (size_t)probe * (size_t)n * e->esz;
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        if (e->prec == RFB_FP64) {
+            const double *x = reinterpret_cast<const double *>(reinterpret_cast<const char *>(e->ts) + off);
+            if (noise) k_iq_power<double><<<1, 1, 0, e->stream>>>(x, n, snr_linear, d_std);
+            k_iq_noise<double><<<blocks, 256, 0, e->stream>>>(x, n, d_std, seed, stream, e->d_iq);
+        } else {
+            const float *x = reinterpret_cast<const float *>(reinterpret_cast<const char *>(e->ts) + off);
+            if (noise) k_iq_power<float><<<1, 1, 0, e->stream>>>(x, n, snr_linear, d_std);
+            k_iq_noise<float><<<blocks, 256, 0, e->stream>>>(x, n, d_std, seed, stream, e->d_iq);
+        }
+        g_launches += 1 + (noise ? 1 : 0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, e->d_iq, (size_t)(2 * n) * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+        CK(cudaStreamSynchronize(e->stream));
+        if (check_sweep_error(e) != 0) return -1;
+    }
+    return 0;
+fail:
+    return -1;
+}
 
 extern "C" int rfb_engine_read_probes(rfb_engine_t *e, double *out) {
     size_t n = (size_t)e->n_probes * e->n_steps;

@@ -178,6 +178,10 @@ int rfb_engine_advance(rfb_engine_t *e, size_t n);
 /* Blocking copy of the probe time series (n_probes * n_steps doubles, probe
  * major).  Only the first `steps_done` samples of each probe are valid. */
 int rfb_engine_read_probes(rfb_engine_t *e, double *out);
+/* One probe's stage signal as interleaved float I/Q (2 n_steps floats),
+ * with rfsyn's AWGN when noise != 0 (snr_linear = 10^(snr_db/10)). */
+int rfb_engine_read_iq(rfb_engine_t *e, int probe, int noise, double snr_linear, unsigned long long seed,
+                       unsigned long long stream, float *out);
 /* Running DFT of every probe series over bins freqs (Kahan-compensated FP32
  * accumulation in FP32 runs, FP64 otherwise; FP64 phase recurrence); sample n
  * is taken at t = (n + t_offset_steps) * dt and weighted by dt. */

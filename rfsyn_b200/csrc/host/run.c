@@ -396,6 +396,26 @@ int fdtd_b200_sim_read_probes(fdtd_b200_sim_t *sim, double *probe_td) {
     return rfb_engine_read_probes(sim->eng, probe_td);
 }
 
+int fdtd_b200_sim_read_iq(fdtd_b200_sim_t *sim, size_t probe, const fdtd_b200_awgn_t *awgn, float *iq_out) {
+    if (!sim || !iq_out) {
+        rfb_set_error("read_iq: NULL argument");
+        return -1;
+    }
+    /* awgn.c:28: snr_linear from the float snr_db, in double */
+    const double snr_linear = awgn ? pow(10.0, (double)awgn->snr_db / 10.0) : 0.0;
+    return rfb_engine_read_iq(sim->eng, (int)probe, awgn != NULL, snr_linear, awgn ? awgn->seed : 0,
+                              awgn ? awgn->stream : 0, iq_out);
+}
+
+int fdtd_b200_iq_write(const char *path, const float *iq, size_t n_samples) {
+    if (!path || (n_samples && !iq)) return -1;
+    FILE *f = fopen(path, "wb");
+    if (!f) return -1;
+    const size_t written = n_samples ? fwrite(iq, 2 * sizeof(float), n_samples, f) : 0;
+    const int closed = fclose(f);
+    return (written == n_samples && closed == 0) ? 0 : -1;
+}
+
 int fdtd_b200_sim_dft(fdtd_b200_sim_t *sim, double *re, double *im) {
     if (!sim || !re || !im) return -1;
     return rfb_engine_probe_dft(sim->eng, sim->n_freqs, sim->freqs, sim->dft_offset, re, im);
