@@ -238,6 +238,9 @@ void *fdtd_b200_batch_stream(const fdtd_b200_batch_t *batch);
 int fdtd_b200_batch_time_kernels(fdtd_b200_batch_t *batch, size_t n_steps, double *sweep_ms, double *other_ms);
 /* Probe series / spectra of one scene (blocking), as the session calls. */
 int fdtd_b200_batch_read_probes(fdtd_b200_batch_t *batch, size_t scene, double *probe_td);
+/* fdtd_b200_sim_read_iq for one scene of the batch (2 n_steps floats). */
+int fdtd_b200_batch_read_iq(fdtd_b200_batch_t *batch, size_t scene, size_t probe, const fdtd_b200_awgn_t *awgn,
+                            float *iq_out);
 int fdtd_b200_batch_dft(fdtd_b200_batch_t *batch, size_t scene, double *dft_re, double *dft_im);
 
 typedef struct {

@@ -296,6 +296,7 @@ def load() -> C.CDLL:
         "fdtd_b200_batch_stream": (P, [P]),
         "fdtd_b200_batch_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_batch_read_probes": (I, [P, S, C.POINTER(D)]),
+        "fdtd_b200_batch_read_iq": (I, [P, S, S, C.POINTER(Awgn), C.POINTER(C.c_float)]),
         "fdtd_b200_batch_dft": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_batch_info": (I, [P, C.POINTER(BatchInfo)]),
         "fdtd_b200_mlp_create": (P, [I, I, I, I, C.c_uint64]),
@@ -570,6 +571,16 @@ class Batch:
         out = np.zeros((max(c.n_probes, 1), c.n_steps))
         self._ok(self.lib.fdtd_b200_batch_read_probes(self.h, scene, _dptr(out)))
         return out[: c.n_probes]
+
+    def read_iq(self, scene: int, probe: int, snr_db: float | None = None, seed: int = 0,
+                stream: int = 0) -> np.ndarray:
+        """complex64 stage signal of one probe of one scene, with rfsyn's AWGN
+        when snr_db is given (fdtd_b200_batch_read_iq)."""
+        n = self.configs[scene].c.n_steps
+        out = np.zeros(2 * n, dtype=np.float32)
+        awgn = C.byref(Awgn(snr_db, seed, stream)) if snr_db is not None else None
+        self._ok(self.lib.fdtd_b200_batch_read_iq(self.h, scene, probe, awgn, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.view(np.complex64)
 
     def dft(self, scene: int) -> np.ndarray:
         c = self.configs[scene].c

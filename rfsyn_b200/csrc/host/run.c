@@ -673,6 +673,16 @@ int fdtd_b200_batch_read_probes(fdtd_b200_batch_t *bt, size_t scene, double *pro
     return rfb_engine_read_probes(bt->sims[scene]->eng, probe_td);
 }
 
+int fdtd_b200_batch_read_iq(fdtd_b200_batch_t *bt, size_t scene, size_t probe, const fdtd_b200_awgn_t *awgn,
+                            float *iq_out) {
+    if (!bt || scene >= bt->n || !iq_out) {
+        rfb_set_error("batch: bad scene index or output");
+        return -1;
+    }
+    if (rfb_batch_sync(bt->b) != 0) return -1;
+    return fdtd_b200_sim_read_iq(bt->sims[scene], probe, awgn, iq_out);
+}
+
 int fdtd_b200_batch_dft(fdtd_b200_batch_t *bt, size_t scene, double *re, double *im) {
     if (!bt || scene >= bt->n || !re || !im) {
         rfb_set_error("batch: bad scene index or output");

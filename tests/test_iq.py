@@ -143,3 +143,26 @@ def test_device_iq_equals_rfsyn_chain(precision):
                     assert np.mean(part == w) >= 0.99
     finally:
         sim.close()
+
+
+@pytest.mark.gpu
+def test_batch_scene_iq_equals_single_scene():
+    from rfsyn_b200 import scenes
+
+    ws = scenes.c4(seed=11, n_scenes=3, precision=rb.FP32, n_steps=120, lo=20, hi=40, npml=4)
+    setups = [scenes.scene_setup(w) for w in ws]
+    b = rb.Batch([scenes.run_config(w) for w in ws], [s.ptr if s else None for s in setups])
+    try:
+        b.advance(ws[0].n_steps)
+        b.synchronize()
+        for q, w in enumerate(ws):
+            sim = rb.Sim(scenes.run_config(w), setups[q].ptr if setups[q] else None)
+            try:
+                sim.advance(w.n_steps)
+                for p in (0, 3):
+                    assert np.array_equal(b.read_iq(q, p, 6.0, 9, q), sim.read_iq(p, 6.0, 9, q))
+                    assert np.array_equal(b.read_iq(q, p), sim.read_iq(p))
+            finally:
+                sim.close()
+    finally:
+        b.close()
