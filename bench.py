@@ -457,7 +457,8 @@ def run_batch(args) -> None:
         "config": {"workload": f"c4_batch{len(ws)}_32to96_fp32", "scenes": len(ws), "cells": cells,
                    "n_steps": n_steps, "npml": 8, "probes_per_scene": 4, "dft_bins": 128,
                    "plan": {"tile_j": info.tile_j, "ring_depth": info.ring_depth, "mode": info.mode,
-                            "seg_interior": info.seg_interior, "seg_edge": info.seg_edge},
+                            "seg_interior": info.seg_interior, "seg_edge": info.seg_edge,
+                            "single_queue": bool(info.unified)},
                    "items": [info.items_interior, info.items_xslab, info.items_edge],
                    "parallelism": f"scene-batch x{world}", "l2": "inputs larger than L2 (fields 12 x 4 B x 130 M cells)"},
         "scenes_per_s": scenes_s,
