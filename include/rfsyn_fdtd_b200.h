@@ -159,6 +159,15 @@ typedef struct {
 } fdtd_b200_awgn_t;
 int fdtd_b200_sim_read_iq(fdtd_b200_sim_t *sim, size_t probe, const fdtd_b200_awgn_t *awgn, float *iq_out);
 int fdtd_b200_iq_write(const char *path, const float *iq, size_t n_samples);
+
+/* ---- failure detection ----------------------------------------------------------
+ * Every wait of the sweeps on a tensor copy is bounded (~2e9 SM cycles); a
+ * copy that never completes makes the sweep record an error that the next
+ * blocking call returns as -1 with its text.  This runs the same wait on an
+ * mbarrier armed for a copy that is never issued, with the given limit
+ * (cycles, at most 4e9): *timed_out = 1 and *cycles the time waited.  No
+ * copy is in flight, so the device stays usable. */
+int fdtd_b200_selftest_bounded_wait(long long limit_cycles, int *timed_out, long long *cycles);
 /* One field component in rfsyn's padded layout, (nx+1)(ny+1)(nz+1) doubles. */
 int fdtd_b200_sim_read_field(fdtd_b200_sim_t *sim, field_component_t component, double *host);
 /* Kernels launched per time step by this session. */

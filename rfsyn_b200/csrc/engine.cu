@@ -1530,6 +1530,49 @@ fail:
     return -1;
 }
 
+// Failure-path check of the sweeps' bounded wait: one thread arms an mbarrier
+// for 16 bytes of a copy that is never issued and waits on it with the given
+// cycle limit; the wait gives up, the thread records it and the kernel ends
+// (no copy is in flight, so nothing lands after the exit).
+__global__ void k_wait_selftest(long long limit, int *status, long long *cycles) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    mbar_expect_tx(&bar, 16);
+    const long long t0 = clock64();
+    const bool done = mbar_wait_for(&bar, 0, limit);
+    *cycles = clock64() - t0;
+    *status = done ? 0 : 1;
+}
+
+extern "C" int fdtd_b200_selftest_bounded_wait(long long limit_cycles, int *timed_out, long long *cycles) {
+    int *d_status = nullptr;
+    long long *d_cycles = nullptr;
+    int rc = -1;
+    if (!timed_out || !cycles || limit_cycles <= 0 || limit_cycles > 4000000000LL) {
+        rfb_set_error("selftest: limit must lie in (0, 4e9] cycles");
+        return -1;
+    }
+    if (cudaMalloc(&d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&d_cycles, sizeof(long long)) != cudaSuccess) {
+        rfb_set_error("selftest: device allocation failed");
+        goto out;
+    }
+    k_wait_selftest<<<1, 32>>>(limit_cycles, d_status, d_cycles);
+    g_launches++;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(timed_out, d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(cycles, d_cycles, sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        rfb_set_error("selftest: %s", cudaGetErrorString(cudaGetLastError()));
+        goto out;
+    }
+    rc = 0;
+out:
+    cudaFree(d_status);
+    cudaFree(d_cycles);
+    return rc;
+}
+
 extern "C" int rfb_engine_read_probes(rfb_engine_t *e, double *out) {
     size_t n = (size_t)e->n_probes * e->n_steps;
     if (!n) return 0;

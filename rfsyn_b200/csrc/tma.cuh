@@ -77,13 +77,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
     return ok != 0;
 }
 // Bounded wait for the completion of the phase with the given parity: false
-// after ~2e9 SM cycles without it.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+// after `limit` SM cycles without it (every sweep waits ~2e9 cycles, about a
+// second, before it reports a stalled copy).
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, unsigned parity, long long limit) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > 2000000000LL) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    return mbar_wait_for(bar, parity, 2000000000LL);
 }
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
     asm volatile(
