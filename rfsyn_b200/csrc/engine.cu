@@ -811,9 +811,11 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
             }
         }
     }
-    // queue order: longest items first, so the last items to start are short
+    // queue order: longest items first, so the last items to start are
+    // short; among equal lengths, items of one body together
     std::stable_sort(vq.begin(), vq.end(), [](const SweepItem &x, const SweepItem &y) {
-        return x.ie - x.ib > y.ie - y.ib;
+        if (x.ie - x.ib != y.ie - y.ib) return x.ie - x.ib > y.ie - y.ib;
+        return x.sub < y.sub;
     });
 }
 
@@ -846,9 +848,13 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
         for (SweepItem it : pl.vx) it.sub = 6, pl.vq.push_back(it);
         pl.vi.clear();
         pl.vx.clear();
+        // among equal costs, items of one body together (fewer
+        // instruction-fetch stalls)
         auto cost = [](const SweepItem &x) { return (x.ie - x.ib) * (x.sub == 5 ? 1 : 4); };
-        std::stable_sort(pl.vq.begin(), pl.vq.end(),
-                         [&](const SweepItem &x, const SweepItem &y) { return cost(x) > cost(y); });
+        std::stable_sort(pl.vq.begin(), pl.vq.end(), [&](const SweepItem &x, const SweepItem &y) {
+            if (cost(x) != cost(y)) return cost(x) > cost(y);
+            return x.sub < y.sub;
+        });
     }
     const std::vector<SweepItem> &vi = pl.vi, &ve = pl.ve, &vq = pl.vq, &vx = pl.vx;
     p.n_int = (int)vi.size();
