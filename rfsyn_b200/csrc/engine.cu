@@ -48,6 +48,20 @@ extern "C" unsigned long long rfb_launch_count(void) { return g_launches.load();
 #define MU0_ 1.25663706212e-6
 
 // Device error codes the sweeps record in their error word.
+extern "C" double rfb_now(void) {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+extern "C" void rfb_trace(const char *phase, double t0) {
+    static const int on = [] {
+        const char *v = getenv("RFSYN_FDTD_TRACE");
+        return v && v[0] == '1';
+    }();
+    if (on) fprintf(stderr, "rfsyn_b200 trace: %s %.3f ms\n", phase, 1e3 * (rfb_now() - t0));
+}
+
 static const char *sweep_error_text(int err) {
     return err == 2 ? "a sweep CTA's shared memory did not start on a 128-byte boundary (no copy issued)"
                     : "a sweep's tensor copies did not complete in time";
@@ -1069,13 +1083,20 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
         CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
         e->own_stream = 1;
     }
+    double t_phase;
+    t_phase = rfb_now();
     for (int b = 0; b < e->nbuf; b++)
         for (int c = 0; c < 6; c++) {
             CK(cudaMalloc(&e->fld[b][c], e->total * e->esz));
             CK(cudaMemset(e->fld[b][c], 0, e->total * e->esz));
         }
+    rfb_trace("engine: field buffers", t_phase);
+    t_phase = rfb_now();
     if (cpml && devcpml_init(e->cpml, geom, cpml, precision, e->pitch, e->nbuf) != 0) goto fail_noset;
+    rfb_trace("engine: cpml", t_phase);
+    t_phase = rfb_now();
     if (devscene_init(e->scene, geom, scene, precision, e->pitch) != 0) goto fail_noset;
+    rfb_trace("engine: scene upload", t_phase);
     e->n_src = (int)n_sources;
     if (n_sources) {
         std::vector<double> vals(n_sources * n_steps);
@@ -1151,8 +1172,11 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
             rc = build_sweep_plan(e, active, precision == RFB_FP32 ? kTmaVariantsFp32[0].tj : kTmaVariantsFp64[0].tj,
                                   precision == RFB_FP32 ? kTmaVariantsFp32[0].ns : kTmaVariantsFp64[0].ns, 1, 64,
                                   32);
-        else
+        else {
+            const double t_tune = rfb_now();
             rc = autotune(e, active);
+            rfb_trace("engine: plan (autotune or cached)", t_tune);
+        }
         if (rc != 0) goto fail_noset;
     }
 created:

@@ -254,6 +254,11 @@ int rfb_sphere_fractions(const double centre[3], double radius, int i0, int j0, 
 const char *rfb_last_error(void);
 void rfb_set_error(const char *fmt, ...);
 
+/* Host wall clock (s) and, with RFSYN_FDTD_TRACE=1 in the environment, one
+ * stderr line "rfsyn_b200 trace: <phase> <ms>" per traced phase. */
+double rfb_now(void);
+void rfb_trace(const char *phase, double t0);
+
 /* Number of kernels this process has launched through the engine. */
 unsigned long long rfb_launch_count(void);
 

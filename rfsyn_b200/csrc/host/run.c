@@ -151,7 +151,9 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
     }
     mat = materials_create(&g);
     if (!mat) { rfb_set_error("materials_create failed"); goto fail; }
+    double t_phase = rfb_now();
     if (setup && setup(&g, mat, context) != 0) { rfb_set_error("scene setup callback failed"); goto fail; }
+    rfb_trace("create: setup callback", t_phase);
 
     const size_t ns = cfg->n_sources, np = cfg->n_probes, nt = cfg->n_steps;
     if (cfg->plane_wave) {
@@ -210,8 +212,11 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
         pd[q].k = (int)canon(p->k, g.nz, pz);
         pd[q].component = (int)p->component;
     }
+    t_phase = rfb_now();
     if (materials_build_image(mat, &g, ns + tf.n_cells, extra, &scene) != 0) goto fail;
     have_scene = 1;
+    rfb_trace("create: scene image", t_phase);
+    t_phase = rfb_now();
     if (cfg->plane_wave) {
         /* E corrections per list entry: find each E target's cell */
         const size_t ne = 3 * scene.img.n_cells;
@@ -278,6 +283,7 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
                                      pd, nt, cuda_stream);
     }
     if (!sim->eng) goto fail;
+    rfb_trace("create: engine", t_phase);
     if (cfg->plane_wave) {
         rfb_tfsf_desc_t td;
         memset(&td, 0, sizeof td);
@@ -429,20 +435,28 @@ int fdtd_b200_sim_read_field(fdtd_b200_sim_t *sim, field_component_t c, double *
 int fdtd_b200_run(const fdtd_b200_config_t *cfg, fdtd_material_setup_fn setup, void *context,
                   fdtd_b200_result_t *result) {
     if (!result) { rfb_set_error("NULL result"); return -1; }
+    double t_phase = rfb_now();
     fdtd_b200_sim_t *sim = fdtd_b200_sim_create(cfg, setup, context, NULL);
+    rfb_trace("run: create", t_phase);
     if (!sim) return -1;
     int rc = -1;
     double ms = 0.0;
+    t_phase = rfb_now();
     if (rfb_engine_advance_timed(sim->eng, cfg->n_steps, &ms) != 0) goto out;
+    rfb_trace("run: time loop", t_phase);
+    t_phase = rfb_now();
     if (result->probe_td && rfb_engine_read_probes(sim->eng, result->probe_td) != 0) goto out;
     if (result->dft_re && result->dft_im && sim->n_freqs &&
         rfb_engine_probe_dft(sim->eng, sim->n_freqs, sim->freqs, sim->dft_offset, result->dft_re, result->dft_im) != 0)
         goto out;
+    rfb_trace("run: series + spectra", t_phase);
     result->sample_rate_hz = 1.0 / sim->dt;
     result->device_ms = ms;
     rc = 0;
 out:
+    t_phase = rfb_now();
     fdtd_b200_sim_destroy(sim);
+    rfb_trace("run: destroy", t_phase);
     return rc;
 }
 
