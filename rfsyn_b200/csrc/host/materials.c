@@ -29,6 +29,7 @@ typedef struct {
     uint64_t *keys;    /* UINT64_MAX = empty */
     double *vals;      /* vw doubles per slot */
     size_t cap, count, vw;
+    uint8_t *mark;     /* per-cell flag set by every put of key cell * 3 + c (or NULL) */
 } omap_t;
 
 #define OMAP_EMPTY UINT64_MAX
@@ -48,6 +49,7 @@ static int omap_init(omap_t *m, size_t vw) {
     m->count = 0;
     m->keys = NULL;
     m->vals = NULL;
+    m->mark = NULL;
     return 0;
 }
 
@@ -98,6 +100,7 @@ static int omap_grow(omap_t *m, size_t want_cap) {
 }
 
 static int omap_put(omap_t *m, uint64_t key, const double *val) {
+    if (m->mark) m->mark[key / 3] = 1;
     long at = omap_find(m, key);
     if (at >= 0) {
         memcpy(m->vals + (size_t)at * m->vw, val, m->vw * sizeof(double));
@@ -144,6 +147,9 @@ struct materials {
     size_t nx, ny, nz, total;
     double dx, dt;
     uint8_t *ids;
+    /* 1 for every cell that ever held a per-component description (set by
+     * the maps' puts, never cleared): cells without it need no map lookups */
+    uint8_t *touched;
     mat_entry_t table[MATERIAL_LIMIT];
     size_t table_count;
     omap_t scalar;  /* key -> (Ca, Cb) */
@@ -219,10 +225,12 @@ materials_t *materials_create(const fdtd_grid_t *g) {
     omap_init(&mat->disp, DISP_W);
     omap_init(&mat->tensor3, 3);
     mat->ids = calloc(total, 1);
-    if (!mat->ids) {
+    mat->touched = calloc(total, 1);
+    if (!mat->ids || !mat->touched) {
         materials_destroy(mat);
         return NULL;
     }
+    mat->scalar.mark = mat->tensor.mark = mat->disp.mark = mat->tensor3.mark = mat->touched;
     material_id_t vacuum;
     if (materials_register(mat, 1.0, 0.0, &vacuum) != 0) {
         materials_destroy(mat);
@@ -234,6 +242,7 @@ materials_t *materials_create(const fdtd_grid_t *g) {
 void materials_destroy(materials_t *mat) {
     if (!mat) return;
     free(mat->ids);
+    free(mat->touched);
     omap_free(&mat->scalar);
     omap_free(&mat->tensor);
     omap_free(&mat->disp);
@@ -700,11 +709,13 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                     for (int c = 0; c < 3; c++) valid[c] = sample_valid(g, c, i, j, k);
                     const size_t w = fdtd_index(g, i, j, k);
                     if (fc[0] == 1.0 && fc[1] == 1.0 && fc[2] == 1.0 && valid[0] && valid[1] && valid[2]) {
-                        for (int c = 0; c < 3; c++) {
-                            omap_del(&mat->scalar, (uint64_t)w * 3 + (uint64_t)c);
-                            omap_del(&mat->disp, (uint64_t)w * 3 + (uint64_t)c);
+                        if (mat->touched[w]) {
+                            for (int c = 0; c < 3; c++) {
+                                omap_del(&mat->scalar, (uint64_t)w * 3 + (uint64_t)c);
+                                omap_del(&mat->disp, (uint64_t)w * 3 + (uint64_t)c);
+                            }
+                            for (int c = 0; c < 2; c++) omap_del(&mat->tensor, (uint64_t)w * 3 + (uint64_t)c);
                         }
-                        for (int c = 0; c < 2; c++) omap_del(&mat->tensor, (uint64_t)w * 3 + (uint64_t)c);
                         if (sp->model) {
                             for (int c = 0; c < 3; c++)
                                 if (omap_put(&mat->disp, (uint64_t)w * 3 + (uint64_t)c, dmodel) != 0) goto oom;
@@ -960,11 +971,32 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     if (id255)
         for (size_t q = 0; q < mat->total; q++)
             if (mat->ids[q] == 255) cells[nc++] = q;
-    qsort(cells, nc, sizeof(uint64_t), cmp_u64);
-    size_t nu = 0;
-    for (size_t q = 0; q < nc; q++)
-        if (nu == 0 || cells[nu - 1] != cells[q]) cells[nu++] = cells[q];
-    nc = nu;
+    /* sorted, unique: by a sort for few candidates, else through a byte per
+     * cell scanned in order (linear in the grid, no n log n sort of the
+     * three keys per override) */
+    uint8_t *mask = nc > 4096 ? calloc(mat->total, 1) : NULL;
+    if (mask) {
+        for (size_t q = 0; q < nc; q++) mask[cells[q]] = 1;
+        size_t nu = 0;
+        const size_t words = mat->total / 8;
+        for (size_t w8 = 0; w8 < words; w8++) {
+            uint64_t v;
+            memcpy(&v, mask + 8 * w8, 8);
+            if (!v) continue;
+            for (size_t b = 0; b < 8; b++)
+                if (mask[8 * w8 + b]) cells[nu++] = 8 * w8 + b;
+        }
+        for (size_t q = 8 * words; q < mat->total; q++)
+            if (mask[q]) cells[nu++] = q;
+        nc = nu;
+        free(mask);
+    } else {
+        qsort(cells, nc, sizeof(uint64_t), cmp_u64);
+        size_t nu = 0;
+        for (size_t q = 0; q < nc; q++)
+            if (nu == 0 || cells[nu - 1] != cells[q]) cells[nu++] = cells[q];
+        nc = nu;
+    }
 
     /* 2. code volume: needed when any cell uses a non-vacuum material or the
      *    list is long; otherwise the engine works code-less */
