@@ -207,13 +207,10 @@ template <typename T, int TJ>
 __device__ __forceinline__ T h_interior(int c, T cbh, const FusedStage<T, TJ> &cur, const FusedStage<T, TJ> &nxt,
                                         int r, int q) {
     if (c == 0)
-        return xs(cur.h[0][r][q],
-                  xm(cbh, xs(xs(cur.e[2][r + 1][q], cur.e[2][r][q]), xs(cur.e[1][r][q + 1], cur.e[1][r][q]))));
+        return upd_h(cur.h[0][r][q], cbh, xs(xs(cur.e[2][r + 1][q], cur.e[2][r][q]), xs(cur.e[1][r][q + 1], cur.e[1][r][q])));
     if (c == 1)
-        return xs(cur.h[1][r][q],
-                  xm(cbh, xs(xs(cur.e[0][r][q + 1], cur.e[0][r][q]), xs(nxt.e[2][r][q], cur.e[2][r][q]))));
-    return xs(cur.h[2][r][q],
-              xm(cbh, xs(xs(nxt.e[1][r][q], cur.e[1][r][q]), xs(cur.e[0][r + 1][q], cur.e[0][r][q]))));
+        return upd_h(cur.h[1][r][q], cbh, xs(xs(cur.e[0][r][q + 1], cur.e[0][r][q]), xs(nxt.e[2][r][q], cur.e[2][r][q])));
+    return upd_h(cur.h[2][r][q], cbh, xs(xs(nxt.e[1][r][q], cur.e[1][r][q]), xs(cur.e[0][r + 1][q], cur.e[0][r][q])));
 }
 
 // ---------------------------------------------------------------------------
@@ -288,9 +285,9 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_interior(Args<T> a, Fus
         __syncthreads();
         if (!a.codes || code != LIST_CODE) {
             const T ca = s_tab[code], cb = s_tab[256 + code];
-            a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(xs(sH[2][r][q], sH[2][r - 1][q]), xs(sH[1][r][q], sH[1][r][q - 1]))));
-            a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(xs(sH[0][r][q], sH[0][r][q - 1]), xs(hz, prevHz))));
-            a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(xs(hy, prevHy), xs(sH[0][r][q], sH[0][r - 1][q]))));
+            a.Eo[0][c] = upd_e(ca, e0, cb, xs(xs(sH[2][r][q], sH[2][r - 1][q]), xs(sH[1][r][q], sH[1][r][q - 1])));
+            a.Eo[1][c] = upd_e(ca, e1, cb, xs(xs(sH[0][r][q], sH[0][r][q - 1]), xs(hz, prevHz)));
+            a.Eo[2][c] = upd_e(ca, e2, cb, xs(xs(hy, prevHy), xs(sH[0][r][q], sH[0][r - 1][q])));
         }
         prevHy = hy;
         prevHz = hz;
@@ -334,9 +331,9 @@ struct EdgeShared {
 // a d (written to *psi_out), returns d kappa_inv + dx psi_new.
 template <typename T>
 __device__ __forceinline__ T stretch(T d, T kinv, T b, T ac, T dx, T psi_old, T *psi_out) {
-    T pn = xa(xm(b, psi_old), xm(ac, d));
+    T pn = cpml_psi(b, psi_old, ac, d);
     *psi_out = pn;
-    return xa(xm(d, kinv), xm(dx, pn));
+    return cpml_out(d, kinv, dx, pn);
 }
 
 template <typename T, int TJ, int NS, int MINB>
@@ -525,7 +522,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
                 if (store) a.psi_ho[5][((long long)i * nshy + sy) * a.pitch + kk] = pn;
             }
         }
-        return xs(hin, xm(a.cbh, xs(dA, dB)));
+        return upd_h(hin, a.cbh, xs(dA, dB));
     };
 
     T prevHy = 0, prevHz = 0;
@@ -612,7 +609,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
                         tB = stretch(tB, es.pz[3][q], es.pz[4][q], es.pz[5][q], a.dx, cs.psi[7][r][q], &pn);
                         a.psi_e[1][((long long)i * ny1 + j) * nsmz + skm] = pn;
                     }
-                    a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
+                    a.Eo[0][c] = upd_e(ca, e0, cb, xs(tA, tB));
                 }
                 if (e_updated(a, 1, i, j, k)) {
                     T tA = xs(sH[0][r][q], sH[0][r][q - 1]);
@@ -627,7 +624,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
                         tB = stretch(tB, a.kinv_m[0][i], a.b_m[0][i], a.a_m[0][i], a.dx, cs.psi[9][r][q], &pn);
                         a.psi_e[3][((long long)sxm * ny1 + j) * a.pitch + k] = pn;
                     }
-                    a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
+                    a.Eo[1][c] = upd_e(ca, e1, cb, xs(tA, tB));
                 }
                 if (e_updated(a, 2, i, j, k)) {
                     T tA = xs(hy, prevHy);
@@ -642,7 +639,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB) k_sweep_edge(Args<T> a, FusedDi
                         tB = stretch(tB, es.py[3][r], es.py[4][r], es.py[5][r], a.dx, cs.psi[11][r][q], &pn);
                         a.psi_e[5][((long long)i * nsmy + sjm) * a.pitch + k] = pn;
                     }
-                    a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
+                    a.Eo[2][c] = upd_e(ca, e2, cb, xs(tA, tB));
                 }
             }
         }

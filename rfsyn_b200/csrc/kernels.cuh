@@ -19,6 +19,21 @@ __device__ __forceinline__ float xm(float a, float b) { return __fmul_rn(a, b); 
 __device__ __forceinline__ float xa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float xs(float a, float b) { return __fsub_rn(a, b); }
 
+// The update expressions H - cbh d, Ca E + Cb t and rfsyn's cpml_term
+// (psi' = b psi + a d, result d kappa_inv + dx psi'), every product and sum
+// rounded on its own in rfsyn's operation order (FP64 bit-exact with rfsyn;
+// FP32 identical in every kernel, so all sweep variants agree bit for bit).
+// Contracting the FP32 forms into fused multiply-adds measured no faster on
+// B200: the edge sweep gained register spills.
+template <typename T>
+__device__ __forceinline__ T upd_h(T h, T cbh, T d) { return xs(h, xm(cbh, d)); }
+template <typename T>
+__device__ __forceinline__ T upd_e(T ca, T e, T cb, T t) { return xa(xm(ca, e), xm(cb, t)); }
+template <typename T>
+__device__ __forceinline__ T cpml_psi(T b, T psi, T ac, T d) { return xa(xm(b, psi), xm(ac, d)); }
+template <typename T>
+__device__ __forceinline__ T cpml_out(T d, T kinv, T dx, T p) { return xa(xm(d, kinv), xm(dx, p)); }
+
 // The incident line at a TF/SF term: cubic Lagrange interpolation through
 // x[-1] .. x[2] with the term's weights, ((w0 x[-1] + w1 x[0]) + w2 x[1]) + w3 x[2].
 template <typename T>
@@ -99,9 +114,9 @@ __device__ __forceinline__ long long psi_idx(const Args<T> &a, int axis, int ns,
 // returns diff kappa_inv + dx psi.
 template <typename T>
 __device__ __forceinline__ T cpml_step(T diff, T kinv, T b, T ac, T dx, T psi_old, T *psi_new) {
-    T p = xa(xm(b, psi_old), xm(ac, diff));
+    T p = cpml_psi(b, psi_old, ac, diff);
     *psi_new = p;
-    return xa(xm(diff, kinv), xm(dx, p));
+    return cpml_out(diff, kinv, dx, p);
 }
 
 // Stretched difference for an H component along `axis` at position q, using
@@ -145,21 +160,21 @@ __device__ __forceinline__ void h_cell(const Args<T> &a, int i, int j, int k) {
         T dB = xs(a.E[1][cidx(a, i, j, kp)], a.E[1][c]);
         T tA = h_term(a, 0, 1, j, dA, i, j, k);
         T tB = h_term(a, 1, 2, k, dB, i, j, k);
-        a.Ho[0][c] = xs(a.H[0][c], xm(a.cbh, xs(tA, tB)));
+        a.Ho[0][c] = upd_h(a.H[0][c], a.cbh, xs(tA, tB));
     }
     if (i < a.nx && j < a.ny + (py ? 0 : 1) && k < a.nz) {
         T dA = xs(a.E[0][cidx(a, i, j, kp)], a.E[0][c]);
         T dB = xs(a.E[2][cidx(a, ip, j, k)], a.E[2][c]);
         T tA = h_term(a, 2, 2, k, dA, i, j, k);
         T tB = h_term(a, 3, 0, i, dB, i, j, k);
-        a.Ho[1][c] = xs(a.H[1][c], xm(a.cbh, xs(tA, tB)));
+        a.Ho[1][c] = upd_h(a.H[1][c], a.cbh, xs(tA, tB));
     }
     if (i < a.nx && j < a.ny && k < a.nz + (pz ? 0 : 1)) {
         T dA = xs(a.E[1][cidx(a, ip, j, k)], a.E[1][c]);
         T dB = xs(a.E[0][cidx(a, i, jp, k)], a.E[0][c]);
         T tA = h_term(a, 4, 0, i, dA, i, j, k);
         T tB = h_term(a, 5, 1, j, dB, i, j, k);
-        a.Ho[2][c] = xs(a.H[2][c], xm(a.cbh, xs(tA, tB)));
+        a.Ho[2][c] = upd_h(a.H[2][c], a.cbh, xs(tA, tB));
     }
 }
 
@@ -191,7 +206,7 @@ __device__ __forceinline__ T e_scalar(const Args<T> &a, int comp, int i, int j, 
         tA = e_term(a, 4, 0, i, xs(a.Ho[1][c], a.Ho[1][cidx(a, im, j, k)]), i, j, k);
         tB = e_term(a, 5, 1, j, xs(a.Ho[0][c], a.Ho[0][cidx(a, i, jm, k)]), i, j, k);
     }
-    return xa(xm(ca, v), xm(cb, xs(tA, tB)));
+    return upd_e(ca, v, cb, xs(tA, tB));
 }
 
 template <typename T>

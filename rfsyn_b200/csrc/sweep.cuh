@@ -297,7 +297,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                 if (store) a.psi_ho[5][pb.by + cl.oy] = pn;
             }
         }
-        return xs(hin, xm(cbh, xs(dA, dB)));
+        return upd_h(hin, cbh, xs(dA, dB));
     };
     // psi inputs of H component c at a cell (zero where no slab applies)
     auto hpsi = [&](int c, const PlaneB &pb, const Cell &cl, T &pA, T &pB) {
@@ -463,7 +463,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                             tB = stretch(tB, tt.pz[3][qs], tt.pz[4][qs], tt.pz[5][qs], a.dx, ep[1], &pn);
                             a.psi_e[1][bzm + ozm] = pn;
                         }
-                        a.Eo[0][c] = xa(xm(ca, e0), xm(cb, xs(tA, tB)));
+                        a.Eo[0][c] = upd_e(ca, e0, cb, xs(tA, tB));
                     }
                     if (m & 16u) {
                         T tA = xs(sH[0][r][qs], sH[0][r][qs - 1]);
@@ -476,7 +476,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                             tB = stretch(tB, xpm[0], xpm[1], xpm[2], a.dx, ep[3], &pn);
                             a.psi_e[3][bxm + own_c.ox] = pn;
                         }
-                        a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(tA, tB)));
+                        a.Eo[1][c] = upd_e(ca, e1, cb, xs(tA, tB));
                     }
                     if (m & 32u) {
                         T tA = xs(hy, prevHy);
@@ -489,7 +489,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                             tB = stretch(tB, tt.py[3][r], tt.py[4][r], tt.py[5][r], a.dx, ep[5], &pn);
                             a.psi_e[5][bym + oym] = pn;
                         }
-                        a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(tA, tB)));
+                        a.Eo[2][c] = upd_e(ca, e2, cb, xs(tA, tB));
                     }
                 }
             }

@@ -172,13 +172,13 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
         // plane in slot sc (the plane after it is in slot sn)
         auto hval = [&](int c, int sc, int sn, int rr, int qq) -> T {
             if (c == 0)
-                return xs(H(sc, 0)[rr][qq], xm(cbh, xs(xs(E(sc, 2)[rr + 1][qq], E(sc, 2)[rr][qq]),
-                                                      xs(E(sc, 1)[rr][qq + 1], E(sc, 1)[rr][qq]))));
+                return upd_h(H(sc, 0)[rr][qq], cbh, xs(xs(E(sc, 2)[rr + 1][qq], E(sc, 2)[rr][qq]),
+                                                      xs(E(sc, 1)[rr][qq + 1], E(sc, 1)[rr][qq])));
             if (c == 1)
-                return xs(H(sc, 1)[rr][qq], xm(cbh, xs(xs(E(sc, 0)[rr][qq + 1], E(sc, 0)[rr][qq]),
-                                                      xs(E(sn, 2)[rr][qq], E(sc, 2)[rr][qq]))));
-            return xs(H(sc, 2)[rr][qq], xm(cbh, xs(xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]),
-                                                  xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq]))));
+                return upd_h(H(sc, 1)[rr][qq], cbh, xs(xs(E(sc, 0)[rr][qq + 1], E(sc, 0)[rr][qq]),
+                                                      xs(E(sn, 2)[rr][qq], E(sc, 2)[rr][qq])));
+            return upd_h(H(sc, 2)[rr][qq], cbh, xs(xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]),
+                                                  xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq])));
         };
         T prevHy = hval(1, NS - 1, 0, r, q);
         T prevHz = hval(2, NS - 1, 0, r, q);
@@ -215,10 +215,9 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
             __syncthreads();
             if (!with_codes || code != LIST_CODE) {
                 const T ca = s_tab[code], cb = s_tab[256 + code];
-                a.Eo[0][c] = xa(xm(ca, e0),
-                                xm(cb, xs(xs(sH[2][r][qs], sH[2][r - 1][qs]), xs(sH[1][r][qs], sH[1][r][qs - 1]))));
-                a.Eo[1][c] = xa(xm(ca, e1), xm(cb, xs(xs(sH[0][r][qs], sH[0][r][qs - 1]), xs(hz, prevHz))));
-                a.Eo[2][c] = xa(xm(ca, e2), xm(cb, xs(xs(hy, prevHy), xs(sH[0][r][qs], sH[0][r - 1][qs]))));
+                a.Eo[0][c] = upd_e(ca, e0, cb, xs(xs(sH[2][r][qs], sH[2][r - 1][qs]), xs(sH[1][r][qs], sH[1][r][qs - 1])));
+                a.Eo[1][c] = upd_e(ca, e1, cb, xs(xs(sH[0][r][qs], sH[0][r][qs - 1]), xs(hz, prevHz)));
+                a.Eo[2][c] = upd_e(ca, e2, cb, xs(xs(hy, prevHy), xs(sH[0][r][qs], sH[0][r - 1][qs])));
             }
             prevHy = hy;
             prevHz = hz;
