@@ -215,20 +215,17 @@ def run_reference(args) -> None:
 # ---------------------------------------------------------------------------
 def run_b200(args) -> None:
     import torch
-    import torch.distributed as dist
-
     import rfsyn_b200 as rb
-    from rfsyn_b200 import scenes
+    from rfsyn_b200 import ranks, scenes
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rk = ranks.from_env()
+    world, rank, local = rk.world, rk.rank, rk.local
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    ranks.init(rk, "nccl", 120)
 
     # each rank simulates its own independent scene (weak scaling, no collective on the data path)
-    w = scenes.c3(seed=3 + rank) if args.workload == "c3" else scenes.c2(seed=2 + rank)
+    w = (scenes.c3(seed=ranks.scene_seed(3, rk)) if args.workload == "c3"
+         else scenes.c2(seed=ranks.scene_seed(2, rk)))
     rc = scenes.run_config(w)
     setup = scenes.scene_setup(w)
     sim = rb.Sim(rc, setup.ptr if setup else None, None)
@@ -246,8 +243,7 @@ def run_b200(args) -> None:
     lib = rb.load()
     launches0 = lib.fdtd_b200_launch_count()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
+    ranks.barrier(rk)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         start.record(stream)
@@ -257,16 +253,10 @@ def run_b200(args) -> None:
         end.synchronize()
     torch.cuda.synchronize()
     launches = lib.fdtd_b200_launch_count() - launches0
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        if world > 1:
-            dist.barrier()
+    ms = ranks.max_over(rk, start.elapsed_time(end))
+    ranks.barrier(rk)
     clocks = clk.summary()
-    cells_total = world * w.cells * w.n_steps * args.steps
-    value = cells_total / (ms / 1e3) / 1e6
+    value = ranks.weak_rate(w.cells * w.n_steps * args.steps, ms, rk) / 1e6
 
     # results of the last timed step: probes and spectra (correctness guard)
     dft = sim.dft()
@@ -296,12 +286,8 @@ def run_b200(args) -> None:
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         d2h = r["td"].nbytes + r["dft"].nbytes
     h2d = info.h2d_bytes
-    e2e_ms = sum(e2e_ms) / len(e2e_ms)  # mean of the end-to-end calls (host set-up times vary)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * w.cells * w.n_steps / (e2e_ms / 1e3) / 1e6
+    e2e_ms = ranks.max_over(rk, sum(e2e_ms) / len(e2e_ms))  # mean of the calls (host set-up times vary)
+    e2e_value = ranks.weak_rate(w.cells * w.n_steps, e2e_ms, rk) / 1e6
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
@@ -312,9 +298,7 @@ def run_b200(args) -> None:
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "unavailable", "sample": str(exc)}
 
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.finish(rk)
     if rank != 0:
         return
     field_mb = (w.nx + 1) * (w.ny + 1) * (w.nz + 1) * esz / 1e6
@@ -359,18 +343,13 @@ def run_batch(args) -> None:
     import torch
 
     import rfsyn_b200 as rb
-    from rfsyn_b200 import scenes
+    from rfsyn_b200 import ranks, scenes
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rk = ranks.from_env()
+    world, rank, local = rk.world, rk.rank, rk.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    ws = scenes.c4(seed=4 + 1000 * rank, n_scenes=args.scenes)
+    ranks.init(rk, "nccl", 300)
+    ws = scenes.c4(seed=ranks.scene_seed(4, rk, 1000), n_scenes=args.scenes)
     n_steps = ws[0].n_steps
     cells = sum(w.cells for w in ws)
     setups = [scenes.scene_setup(w) for w in ws]
@@ -391,8 +370,7 @@ def run_batch(args) -> None:
     lib = rb.load()
     launches0 = lib.fdtd_b200_launch_count()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
+    ranks.barrier(rk)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         start.record(stream)
@@ -402,14 +380,12 @@ def run_batch(args) -> None:
         end.synchronize()
     b.synchronize()
     launches = lib.fdtd_b200_launch_count() - launches0
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = ranks.max_over(rk, start.elapsed_time(end))
     clocks = clk.summary()
-    value = world * cells * n_steps * args.steps / (ms / 1e3) / 1e6
-    scenes_s = world * len(ws) * args.steps / (ms / 1e3)
+    # every rank's scenes differ: the whole job's cells are summed over ranks
+    cells_all = ranks.sum_over(rk, float(cells))
+    value = cells_all * n_steps * args.steps / (ms / 1e3) / 1e6
+    scenes_s = ranks.weak_rate(len(ws) * args.steps, ms, rk)
     finite = all(bool(np.all(np.isfinite(b.dft(q)))) for q in range(0, len(ws), max(1, len(ws) // 16)))
     # sweep kernels alone (CUDA events around the sweep launches of each step)
     b.reset()
@@ -436,14 +412,9 @@ def run_batch(args) -> None:
     d2h = 0
     for q in range(len(ws)):
         d2h += b2.probes(q).nbytes + b2.dft(q).nbytes
-    e2e_ms = (time.perf_counter() - t0) * 1e3
+    e2e_ms = ranks.max_over(rk, (time.perf_counter() - t0) * 1e3)
     b2.close()
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.finish(rk)
     if rank != 0:
         return
     esz = 4
@@ -469,7 +440,7 @@ def run_batch(args) -> None:
                      "kernel": "k_sweep_qb (one batched H+E sweep: interior + x-slab + edge launches)",
                      "algorithmic_bytes_per_launch": alg, "launch_ms": sweep_launch_ms,
                      "other_kernels_ms_per_step": ot / 50},
-        "e2e": {"value": world * cells * n_steps / (e2e_ms / 1e3) / 1e6, "unit": METRIC, "h2d_bytes_per_step": None,
+        "e2e": {"value": cells_all * n_steps / (e2e_ms / 1e3) / 1e6, "unit": METRIC, "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "includes": "scene set-up and upload"},
         "create_s": create_s,
         "gpu_launches": int(launches), "launches_per_time_step": info.launches_per_step,
