@@ -551,18 +551,25 @@ static void launch_rest(rfb_engine *e, const Args<T> &a, int par, cudaStream_t s
     launch_edge<T>(a, e->plan, st);
 }
 
+// One fused sweep: the interior kinds on the engine stream, the slab /
+// boundary kinds on the second stream, side by side (they touch disjoint
+// cells).  A third stream for the x-slab kind measured slower on C2.
+template <typename T>
+static void launch_sweep(rfb_engine *e, const Args<T> &a, int par) {
+    cudaEventRecord(e->ev_fork, e->stream);
+    cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
+    launch_int<T>(e, a, par, e->stream);
+    launch_rest<T>(e, a, par, e->stream2);
+    cudaEventRecord(e->ev_join, e->stream2);
+    cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+}
+
 template <typename T>
 static void enqueue_step(rfb_engine *e, int par) {
     Args<T> a = engine_args<T>(e, par);
     const rfb_geom_t &g = e->g;
     if (e->sched == RFB_SCHED_FUSED) {
-        // interior and edge sweeps touch disjoint cells: run them side by side
-        cudaEventRecord(e->ev_fork, e->stream);
-        cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
-        launch_int<T>(e, a, par, e->stream);
-        launch_rest<T>(e, a, par, e->stream2);
-        cudaEventRecord(e->ev_join, e->stream2);
-        cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+        launch_sweep<T>(e, a, par);
     } else {
         dim3 blk(32, 8);
         dim3 grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
@@ -927,12 +934,7 @@ static std::vector<std::pair<std::vector<long long>, TunedPlan>> g_tune_cache;
 template <typename T>
 static void enqueue_sweep(rfb_engine *e, int par) {
     Args<T> a = engine_args<T>(e, par);
-    cudaEventRecord(e->ev_fork, e->stream);
-    cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
-    launch_int<T>(e, a, par, e->stream);
-    launch_rest<T>(e, a, par, e->stream2);
-    cudaEventRecord(e->ev_join, e->stream2);
-    cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+    launch_sweep<T>(e, a, par);
 }
 
 static int autotune(rfb_engine *e, int active) {
@@ -1393,12 +1395,7 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         const rfb_geom_t &g = e->g;
         CK(cudaEventRecord(ev[0], e->stream));
         if (e->sched == RFB_SCHED_FUSED) {
-            cudaEventRecord(e->ev_fork, e->stream);
-            cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
-            launch_int<T>(e, a, par, e->stream);
-            launch_rest<T>(e, a, par, e->stream2);
-            cudaEventRecord(e->ev_join, e->stream2);
-            cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+            launch_sweep<T>(e, a, par);
             g_launches += (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0);
         } else {
             dim3 blk(32, 8), grd((g.nz + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nx + 1);
