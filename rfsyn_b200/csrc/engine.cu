@@ -428,6 +428,13 @@ struct rfb_engine {
     int *d_err = nullptr;   // set by a sweep whose copies did not complete in time
     double *d_energy = nullptr;  // energy audit: block partials + result
     float *d_iq = nullptr;       // stage output: n_steps I/Q pairs, then the noise scale (a double)
+    // cells whose three E samples are 3x3 samples without source or TF/SF
+    // term, updated per cell by k_t3_cells (their list entries are kind 5);
+    // t3_kinds keeps the image's kinds to undo it
+    int *t3_cells = nullptr;
+    int n_t3_cells = 0;
+    std::vector<uint8_t> t3_kinds;
+    std::vector<int> t3_host;
     size_t h2d_bytes = 0, n_ade = 0;
     // plane wave (TF/SF): line, H-target terms, per-entry E terms
     int tf_on = 0, tf_n_h = 0, tf_m_len = 0;
@@ -578,6 +585,7 @@ static void enqueue_step(rfb_engine *e, int par) {
     }
     tf_before_list<T>(e, par);
     if (a.n_cells) k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
+    if (e->n_t3_cells) k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
     ProbeArgs<T> p;
     p.n = e->n_probes;
     p.cell = e->probe_cell;
@@ -596,6 +604,7 @@ static int count_step_launches(const rfb_engine *e) {
                 ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0)
                 : 2;
     if (e->scene.n_cells) n++;
+    if (e->n_t3_cells) n++;
     if (e->tf_on) n += 2 + (e->tf_n_h > 0);
     return n + 1;
 }
@@ -1052,6 +1061,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     devscene_free(e->scene);
     cudaFree(e->src_val); cudaFree(e->src_hard);
     cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy); cudaFree(e->d_iq);
+    cudaFree(e->t3_cells);
     cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
     cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_qx); cudaFree(e->plan.d_queue);
     cudaFree(e->tf_inc_e); cudaFree(e->tf_inc_h); cudaFree(e->tf_src); cudaFree(e->tf_h_cell); cudaFree(e->tf_h_comp);
@@ -1063,6 +1073,44 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     if (e->stream2) cudaStreamDestroy(e->stream2);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
+}
+
+// Cells whose three list entries are 3x3 samples without a source go to the
+// per-cell kernel; their entries become kind 5, which the list kernel skips.
+static int group_t3_cells(rfb_engine *e, const rfb_scene_image_t *img) {
+    const size_t ne = 3 * (size_t)img->n_cells;
+    std::vector<int> cells;
+    for (size_t q = 0; q < (size_t)img->n_cells; q++) {
+        bool all = true;
+        for (int c = 0; c < 3; c++) all &= img->kind[3 * q + c] == RFB_LK_TENSOR3 && img->src[3 * q + c] < 0;
+        if (all) cells.push_back((int)q);
+    }
+    if (cells.empty()) return 0;
+    e->t3_kinds.assign(img->kind, img->kind + ne);
+    std::vector<uint8_t> kinds = e->t3_kinds;
+    for (int q : cells)
+        for (int c = 0; c < 3; c++) kinds[3 * (size_t)q + c] = RFB_LK_CELL3;
+    e->t3_cells = dev_copy(cells.data(), cells.size());
+    if (!e->t3_cells) {
+        rfb_set_error("3x3 cell list upload failed");
+        return -1;
+    }
+    CK(cudaMemcpy(e->scene.l_kind, kinds.data(), ne, cudaMemcpyHostToDevice));
+    e->n_t3_cells = (int)cells.size();
+    e->t3_host = cells;
+    return 0;
+fail:
+    return -1;
+}
+
+// Gives every 3x3 cell back to the list kernel (a TF/SF term landed on one).
+static int ungroup_t3_cells(rfb_engine *e) {
+    if (!e->n_t3_cells) return 0;
+    CK(cudaMemcpy(e->scene.l_kind, e->t3_kinds.data(), e->t3_kinds.size(), cudaMemcpyHostToDevice));
+    e->n_t3_cells = 0;
+    return 0;
+fail:
+    return -1;
 }
 
 static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int schedule, const rfb_cpml_desc_t *cpml,
@@ -1098,6 +1146,7 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
     rfb_trace("engine: cpml", t_phase);
     t_phase = rfb_now();
     if (devscene_init(e->scene, geom, scene, precision, e->pitch) != 0) goto fail_noset;
+    if (!member && scene && scene->n_cells && group_t3_cells(e, scene) != 0) goto fail_noset;
     rfb_trace("engine: scene upload", t_phase);
     e->n_src = (int)n_sources;
     if (n_sources) {
@@ -1236,6 +1285,13 @@ extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
     for (size_t q = 0; q < d->n_h; q++) {
         cell[q] = ((long long)d->h_ijkc[4 * q] * (g.ny + 1) + d->h_ijkc[4 * q + 1]) * e->pitch + d->h_ijkc[4 * q + 2];
         comp[q] = d->h_ijkc[4 * q + 3];
+    }
+    // a 3x3 cell that carries a TF/SF E term stays with the list kernel
+    if (e->n_t3_cells && d->entry_first) {
+        bool hit = false;
+        for (int q : e->t3_host)
+            for (int c = 0; c < 3; c++) hit |= d->entry_first[3 * (size_t)q + c] >= 0;
+        if (hit && ungroup_t3_cells(e) != 0) goto fail;
     }
     e->tf_m_len = (int)d->m_len;
     e->tf_ce = d->ce;
@@ -1407,6 +1463,10 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         tf_before_list<T>(e, par);
         if (a.n_cells) {
             k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
+            if (e->n_t3_cells) {
+                k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
+                g_launches++;
+            }
             g_launches++;
         }
         ProbeArgs<T> p;

@@ -329,6 +329,57 @@ __device__ __forceinline__ T e_tensor3(const Args<T> &a, const T *r, int c, int 
     return xa(v, xm(r[3], value));
 }
 
+// The three components of a cell whose samples are all 3x3 samples (no
+// source, no TF/SF term): e_tensor3 for c = 0, 1, 2 with the same operation
+// order, the curl differences they share computed once -- D_b at the cell
+// and at the cell one step back along b serve both components c != b -- so
+// a cell takes 18 curl evaluations instead of 27.
+template <typename T>
+__device__ __forceinline__ void t3_cell(const Args<T> &a, int cell) {
+    const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
+    const int n[3] = {a.nx, a.ny, a.nz};
+    const long long st[3] = {(long long)(a.ny + 1) * a.pitch, a.pitch, 1};
+    auto curl_at = [&](int b, long long q, const int p[3]) {
+        const int fa = (b + 2) % 3, axa = (b + 1) % 3, fb = (b + 1) % 3, axb = (b + 2) % 3;
+        const long long qa = p[axa] == 0 ? q + (long long)(n[axa] - 1) * st[axa] : q - st[axa];
+        const long long qb = p[axb] == 0 ? q + (long long)(n[axb] - 1) * st[axb] : q - st[axb];
+        return xs(xs(a.Ho[fa][q], a.Ho[fa][qa]), xs(a.Ho[fb][q], a.Ho[fb][qb]));
+    };
+    const int p0[3] = {i, j, k};
+    const long long c0 = cidx(a, i, j, k);
+    T dw[3], dm[3];
+    long long back[3];
+    for (int b = 0; b < 3; b++) {
+        dw[b] = curl_at(b, c0, p0);
+        int p2[3] = {i, j, k};
+        p2[b] = p2[b] == 0 ? n[b] - 1 : p2[b] - 1;
+        back[b] = p0[b] == 0 ? (long long)(n[b] - 1) * st[b] : -st[b];
+        dm[b] = curl_at(b, c0 + back[b], p2);
+    }
+    for (int c = 0; c < 3; c++) {
+        const T *r = a.t3 + 4 * (long long)a.l_tix[3 * cell + c];
+        T value = xm(r[c], dw[c]);
+        const bool wrap = ((a.per >> c) & 1u) && p0[c] + 1 == n[c];
+        int p1[3] = {i, j, k};
+        p1[c] = wrap ? 0 : p1[c] + 1;
+        const long long c1 = wrap ? c0 - (long long)(n[c] - 1) * st[c] : c0 + st[c];
+        for (int b = 0; b < 3; b++) {
+            if (b == c) continue;
+            int p3[3] = {p1[0], p1[1], p1[2]};
+            p3[b] = p3[b] == 0 ? n[b] - 1 : p3[b] - 1;
+            const T s4 = xa(xa(xa(dw[b], curl_at(b, c1, p1)), dm[b]), curl_at(b, c1 + back[b], p3));
+            value = xa(value, xm(r[b], xm(T(0.25), s4)));
+        }
+        a.Eo[c][c0] = xa(a.E[c][c0], xm(r[3], value));
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_t3_cells(Args<T> a, const int *cells, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) t3_cell(a, cells[t]);
+}
+
 // ---- interface list: overrides, tensor edges, sources --------------------
 // One thread per (cell, component) entry.  Reads E from the input buffers,
 // H from the output buffers (already advanced), writes E output.
@@ -337,6 +388,8 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
     const int cell = e / 3, comp = e - 3 * cell;
     const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
     const long long c = cidx(a, i, j, k);
+    const int kind = a.l_kind[e];
+    if (kind == 5) return;  // a 3x3 cell: k_t3_cells updates its three components
     T v = a.E[comp][c];
     const int s = a.l_src[e];
     if (s >= 0) {
@@ -344,7 +397,6 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
         const T sv = (n < a.n_steps) ? a.src_val[(long long)s * a.n_steps + n] : T(0);
         v = a.src_hard[s] ? sv : xa(v, sv);
     }
-    const int kind = a.l_kind[e];
     if (kind == 1) {
         v = e_scalar(a, comp, i, j, k, v, a.l_ca[e], a.l_cb[e]);
     } else if (kind == 2) {
