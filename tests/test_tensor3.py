@@ -2,6 +2,9 @@
 edges are 2x2, materials.c:658-903).
 
 CPU (oracle only), the physics that pins the restatement:
+  * in the scope of rfsyn's 2x2 tensor edges (z-invariant TM field, uniform
+    medium filling a periodic domain) the 3x3 update equals rfsyn's to
+    rounding;
   * a diagonal 3x3 sample is the scalar medium (relative 1e-10 over the run);
   * a plane wave in a uniform rotated uniaxial medium keeps the polarisation
     of its eigenvector and travels at c / sqrt(eps) of that eigenvalue;
@@ -122,6 +125,35 @@ def test_random_tensor_cavity_stays_bounded():
     early = np.abs(td[:, 300:1000]).max()
     late = np.abs(td[:, 2000:]).max()
     assert late < 2.0 * early
+
+
+def test_reduces_to_rfsyn_2x2_tensor_in_its_scope():
+    """rfsyn's tensor edges (materials.c:847-903) are the 2x2 (Ex, Ey)
+    inverse permittivity of a z-invariant TM field, coupled to the four
+    surrounding samples with the pair weight 0.25 rho sqrt(m11 m11'); in a
+    uniform medium that fills a fully periodic domain the weight is 0.25 m12
+    and the 3x3 rows (m11, m12, 0), (m12, m22, 0), (0, 0, 1/eps_z) describe
+    the same update.  Driven z-invariantly (an Ex / Ey sheet along z), the two
+    agree to rounding (1e-10 of the peak) at every probe."""
+    eps = np.array([[4.0, 1.2], [1.2, 2.5]])
+    m = np.linalg.inv(eps)
+    eps_z = 3.0
+    n, nz = 12, 3
+    base = dict(nx=n, ny=n, nz=nz, n_steps=240, periodic=7,
+                sources=[(5, 6, k, c, 0, 1.0 if c == 0 else 0.6, *_gd(25, 6)) for k in range(nz) for c in (0, 1)],
+                probes=[(8, 4, 1, 0), (2, 9, 1, 1), (6, 6, 2, 5), (10, 10, 0, 0)])
+    cells = [(i, j, k) for i in range(n) for j in range(n) for k in range(nz)]
+    a = Scene(boxes=[(0, n, 0, n, 0, nz, eps_z, 0.0)],
+              tensors=[(0, i, j, k, m[0, 0], m[0, 1], m[1, 1]) for (i, j, k) in cells] +
+                      [(1, i, j, k, m[1, 1], m[0, 1], m[0, 0]) for (i, j, k) in cells], **base)
+    b = Scene(**base)
+    b.tensor3 = ([(0, i, j, k, (m[0, 0], m[0, 1], 0.0)) for (i, j, k) in cells] +
+                 [(1, i, j, k, (m[0, 1], m[1, 1], 0.0)) for (i, j, k) in cells] +
+                 [(2, i, j, k, (0.0, 0.0, 1.0 / eps_z)) for (i, j, k) in cells])
+    ta, tb = oracle.run_oracle(a)["td"], oracle.run_oracle(b)["td"]
+    peak = np.abs(ta).max()
+    assert peak > 0
+    assert np.abs(ta - tb).max() <= 1e-10 * peak, np.abs(ta - tb).max() / peak
 
 
 def test_box_helper_inverts_eps():
