@@ -1787,24 +1787,54 @@ __global__ void k_sphere_fractions(double cx, double cy, double cz, double r, in
     n2[t] = nn;
 }
 
+// Sphere set-up runs once per sphere of every scene (tens of thousands of
+// calls when a batch of scenes is built): the device results and their
+// pinned host staging are kept per device and grown on demand, so a call is
+// one launch, two copies and one synchronisation.
+namespace {
+struct FracScratch {
+    double *dev = nullptr, *host = nullptr;
+    size_t cap = 0;  // doubles per output
+};
+std::mutex g_frac_mu;
+FracScratch g_frac[64];
+}  // namespace
+
 extern "C" int rfb_sphere_fractions(const double centre[3], double radius, int i0, int j0, int k0, int ni, int nj,
                                     int nk, double *f, double *n2) {
     const size_t n = 3 * (size_t)ni * nj * nk;
-    double *df = nullptr, *dn = nullptr;
-    int rc = -1;
+    int rc = -1, dev = 0;
     if (!n) return 0;
-    CK(cudaMalloc(&df, n * 8));
-    CK(cudaMalloc(&dn, n * 8));
-    k_sphere_fractions<<<(unsigned)((n + 255) / 256), 256>>>(centre[0], centre[1], centre[2], radius, i0, j0, k0, ni,
-                                                             nj, nk, df, dn);
-    g_launches++;
-    CK(cudaGetLastError());
-    CK(cudaMemcpy(f, df, n * 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(n2, dn, n * 8, cudaMemcpyDeviceToHost));
+    std::lock_guard<std::mutex> lock(g_frac_mu);
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        rfb_set_error("sphere fractions: device index %d out of range", dev);
+        return -1;
+    }
+    {
+        FracScratch &s = g_frac[dev];
+        if (s.cap < n) {
+            cudaFree(s.dev);
+            cudaFreeHost(s.host);
+            s.dev = nullptr;
+            s.host = nullptr;
+            s.cap = 0;
+            const size_t want = std::max(n, (size_t)1 << 18);
+            CK(cudaMalloc(&s.dev, 2 * want * sizeof(double)));
+            CK(cudaMallocHost(&s.host, 2 * want * sizeof(double)));
+            s.cap = want;
+        }
+        k_sphere_fractions<<<(unsigned)((n + 255) / 256), 256>>>(centre[0], centre[1], centre[2], radius, i0, j0, k0,
+                                                                 ni, nj, nk, s.dev, s.dev + s.cap);
+        g_launches++;
+        CK(cudaGetLastError());
+        CK(cudaMemcpy(s.host, s.dev, n * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(s.host + s.cap, s.dev + s.cap, n * 8, cudaMemcpyDeviceToHost));
+        memcpy(f, s.host, n * 8);
+        memcpy(n2, s.host + s.cap, n * 8);
+    }
     rc = 0;
 fail:
-    cudaFree(df);
-    cudaFree(dn);
     return rc;
 }
 
