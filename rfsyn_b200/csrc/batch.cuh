@@ -390,20 +390,41 @@ fail:
 // Picks the plan (tile height, ring depth, tile origins, segment lengths) by
 // timing a few batched sweeps of each candidate; every candidate computes
 // bit-identical fields, so the choice changes speed only.
+// Plans chosen for batches of the same scene geometries (in order), so that
+// a batch built again -- the next set of examples of a stage, an end-to-end
+// run -- skips the tuning.
+struct BatchCand {
+    int tj, ns, mode, si, se, uni;
+};
+static std::mutex g_btune_mu;
+static std::vector<std::pair<std::vector<long long>, BatchCand>> g_btune_cache;
+
+static std::vector<long long> batch_key(const rfb_batch *b) {
+    std::vector<long long> key = {b->prec, (long long)b->m.size()};
+    for (const rfb_engine *e : b->m) {
+        const rfb_geom_t &g = e->g;
+        key.insert(key.end(), {g.nx, g.ny, g.nz, (long long)g.periodic, e->active, e->cpml.on});
+        if (e->cpml.on)
+            for (int a = 0; a < 3; a++)
+                key.insert(key.end(), {e->cpml.eh[a].lo, e->cpml.eh[a].hi, e->cpml.em[a].lo, e->cpml.em[a].hi});
+        key.push_back(e->scene.n_skip);
+        for (int s = 0; s < e->scene.n_skip; s++) key.push_back(e->scene.skip[s]);
+    }
+    return key;
+}
+
 static int batch_autotune(rfb_batch *b) {
-    struct Cand {
-        int tj, ns, mode, si, se, uni;
-    };
+    using Cand = BatchCand;
     std::vector<Cand> cands;
     const InteriorVariant *v = b->prec == RFB_FP32 ? kQVariantsFp32 : kQVariantsFp64;
     const size_t nv = b->prec == RFB_FP32 ? std::size(kQVariantsFp32) : std::size(kQVariantsFp64);
     bool wrap_yz = false;
     for (const rfb_engine *e : b->m) wrap_yz |= (e->g.periodic & 6u) != 0;
+    // two stages: variant, tile origins and queue form at (64, 32)-plane
+    // items, then the segment lengths of the winner
     for (size_t q = 0; q < nv; q++)
         for (int mode = 2; mode <= (wrap_yz ? 3 : 4); mode++)
-            for (int si : {32, 64})
-                for (int se : {16, 32})
-                    for (int uni : {0, 1}) cands.push_back(Cand{v[q].tj, v[q].ns, mode, si, se, uni});
+            for (int uni : {0, 1}) cands.push_back(Cand{v[q].tj, v[q].ns, mode, 64, 32, uni});
     const char *ov = getenv("RFSYN_FDTD_PLAN");
     if (ov) {
         int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
@@ -414,13 +435,24 @@ static int batch_autotune(rfb_batch *b) {
         }
         return batch_build_plan(b, a1, a2, a5, a3, a4, a6);
     }
+    const std::vector<long long> key = batch_key(b);
+    {
+        std::lock_guard<std::mutex> lock(g_btune_mu);
+        for (const auto &kv : g_btune_cache)
+            if (kv.first == key) {
+                const Cand &c = kv.second;
+                return batch_build_plan(b, c.tj, c.ns, c.mode, c.si, c.se, c.uni);
+            }
+    }
     Cand best = cands[0];
+    const size_t first_stage = cands.size();
     float best_ms = 1e30f;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     int par = 0;
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
-    for (const Cand &c : cands) {
+    for (size_t ci = 0; ci < cands.size(); ci++) {
+        const Cand c = cands[ci];
         if (batch_build_plan(b, c.tj, c.ns, c.mode, c.si, c.se, c.uni) != 0) goto fail;
         for (int w = 0; w < 5; w++) {
             if (w == 2) CK(cudaEventRecord(t0, b->stream));
@@ -436,6 +468,11 @@ static int batch_autotune(rfb_batch *b) {
             best_ms = ms;
             best = c;
         }
+        if (ci + 1 == first_stage)
+            for (int si : {32, 64})
+                for (int se : {16, 32})
+                    if (si != best.si || se != best.se)
+                        cands.push_back(Cand{best.tj, best.ns, best.mode, si, se, best.uni});
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
@@ -446,6 +483,10 @@ static int batch_autotune(rfb_batch *b) {
             rfb_set_error("batch: %s", sweep_error_text(err));
             return -1;
         }
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_btune_mu);
+        g_btune_cache.push_back({key, best});
     }
     if (batch_build_plan(b, best.tj, best.ns, best.mode, best.si, best.se, best.uni) != 0) return -1;
     // the tuning sweeps advanced the fields: start from the zero state again
