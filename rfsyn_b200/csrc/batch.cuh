@@ -624,7 +624,12 @@ extern "C" rfb_batch_t *rfb_batch_create(rfb_engine_t **members, size_t n, void 
         }
     if ((b->prec == RFB_FP64 ? batch_upload_args<double>(b) : batch_upload_args<float>(b)) != 0) goto fail;
     CK(cudaDeviceSynchronize());
-    if (batch_autotune(b) != 0) goto fail;
+    {
+        const double t_tune = rfb_now();
+        const int rc = batch_autotune(b);
+        rfb_trace("batch: plan (tuned or cached)", t_tune);
+        if (rc != 0) goto fail;
+    }
     return b;
 fail:
     rfb_batch_destroy(b);

@@ -623,6 +623,7 @@ fdtd_b200_batch_t *fdtd_b200_batch_create(size_t n_scenes, const fdtd_b200_confi
         goto fail;
     }
     bt->n = n_scenes;
+    const double t_members = rfb_now();
     for (size_t s = 0; s < n_scenes; s++) {
         fdtd_material_setup_fn fn = setups ? setups[s] : NULL;
         void *ctx = contexts ? contexts[s] : NULL;
@@ -636,6 +637,7 @@ fdtd_b200_batch_t *fdtd_b200_batch_create(size_t n_scenes, const fdtd_b200_confi
         engs[s] = bt->sims[s]->eng;
         made = s + 1;
     }
+    rfb_trace("batch: member scenes", t_members);
     bt->b = rfb_batch_create(engs, n_scenes, stream, own);
     own = 0;      /* the batch owns the stream now, on failure too */
     made = 0;     /* ... and the engines */
