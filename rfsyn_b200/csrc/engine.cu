@@ -402,6 +402,7 @@ struct rfb_engine {
     long long pitch;
     size_t esz, total;
     void *fld[2][6] = {};
+    void *fld_base = nullptr;  // one allocation holds every field buffer
     int nbuf = 1;
     DevCpml cpml;
     DevScene scene;
@@ -1055,8 +1056,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
         if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
         if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
     }
-    for (int b = 0; b < 2; b++)
-        for (int c = 0; c < 6; c++) cudaFree(e->fld[b][c]);
+    cudaFree(e->fld_base);
     devcpml_free(e->cpml);
     devscene_free(e->scene);
     cudaFree(e->src_val); cudaFree(e->src_hard);
@@ -1135,11 +1135,15 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
     }
     double t_phase;
     t_phase = rfb_now();
-    for (int b = 0; b < e->nbuf; b++)
-        for (int c = 0; c < 6; c++) {
-            CK(cudaMalloc(&e->fld[b][c], e->total * e->esz));
-            CK(cudaMemset(e->fld[b][c], 0, e->total * e->esz));
-        }
+    {
+        // every buffer is a multiple of 128 bytes (whole pitched rows), so
+        // the sub-buffers keep the alignment the tensor copies need
+        const size_t one = e->total * e->esz;
+        CK(cudaMalloc(&e->fld_base, one * 6 * e->nbuf));
+        CK(cudaMemsetAsync(e->fld_base, 0, one * 6 * e->nbuf, e->stream));
+        for (int b = 0; b < e->nbuf; b++)
+            for (int c = 0; c < 6; c++) e->fld[b][c] = static_cast<char *>(e->fld_base) + (size_t)(6 * b + c) * one;
+    }
     rfb_trace("engine: field buffers", t_phase);
     t_phase = rfb_now();
     if (cpml && devcpml_init(e->cpml, geom, cpml, precision, e->pitch, e->nbuf) != 0) goto fail_noset;
