@@ -272,6 +272,8 @@ def load() -> C.CDLL:
         "fdtd_b200_sim_launches_per_step": (I, [P]),
         "fdtd_b200_last_error": (C.c_char_p, []),
         "fdtd_b200_launch_count": (C.c_ulonglong, []),
+        "fdtd_b200_cached_bytes": (C.c_ulonglong, []),
+        "fdtd_b200_release_cached_memory": (None, []),
         "fdtd_b200_set_default_precision": (I, [I]),
         "fdtd_b200_set_default_schedule": (I, [I]),
         "fdtd_b200_version": (C.c_char_p, []),
@@ -321,6 +323,16 @@ def load() -> C.CDLL:
 
 def last_error() -> str:
     return load().fdtd_b200_last_error().decode()
+
+
+def cached_bytes() -> int:
+    """Device memory the library keeps from destroyed simulations for reuse."""
+    return int(load().fdtd_b200_cached_bytes())
+
+
+def release_cached_memory() -> None:
+    """Returns the library's cached device memory to the driver."""
+    load().fdtd_b200_release_cached_memory()
 
 
 def _dptr(a: np.ndarray):

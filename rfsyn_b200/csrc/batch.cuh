@@ -231,7 +231,7 @@ struct rfb_batch {
 
 static void batch_free_plan(rfb_batch *b) {
     for (int k = 0; k < 3; k++) {
-        cudaFree(b->d_items[k]);
+        dfree(b->d_items[k]);
         b->d_items[k] = nullptr;
         b->n_items[k] = 0;
     }
@@ -239,10 +239,10 @@ static void batch_free_plan(rfb_batch *b) {
         if (b->g1[q]) cudaGraphExecDestroy(b->g1[q]);
         if (b->gk[q]) cudaGraphExecDestroy(b->gk[q]);
         b->g1[q] = b->gk[q] = nullptr;
-        cudaFree(b->d_maps[q]);
+        dfree(b->d_maps[q]);
         b->d_maps[q] = nullptr;
     }
-    cudaFree(b->d_dims);
+    dfree(b->d_dims);
     b->d_dims = nullptr;
 }
 
@@ -300,15 +300,15 @@ static int batch_build_plan(rfb_batch *b, int tj, int ns, int mode, int seg_int,
         });
         b->n_items[k] = (int)lists[k].size();
         if (b->n_items[k]) {
-            CK(cudaMalloc(&b->d_items[k], lists[k].size() * sizeof(BatchItem)));
+            CK(dmalloc(&b->d_items[k], lists[k].size() * sizeof(BatchItem)));
             CK(cudaMemcpy(b->d_items[k], lists[k].data(), lists[k].size() * sizeof(BatchItem),
                           cudaMemcpyHostToDevice));
         }
     }
-    CK(cudaMalloc(&b->d_dims, n * sizeof(FusedDims)));
+    CK(dmalloc(&b->d_dims, n * sizeof(FusedDims)));
     CK(cudaMemcpy(b->d_dims, dims.data(), n * sizeof(FusedDims), cudaMemcpyHostToDevice));
     for (int q = 0; q < 2; q++) {
-        CK(cudaMalloc(&b->d_maps[q], n * sizeof(TmaMaps)));
+        CK(dmalloc(&b->d_maps[q], n * sizeof(TmaMaps)));
         CK(cudaMemcpy(b->d_maps[q], maps[q].data(), n * sizeof(TmaMaps), cudaMemcpyHostToDevice));
     }
     return 0;
@@ -504,9 +504,9 @@ extern "C" void rfb_batch_destroy(rfb_batch_t *b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     batch_free_plan(b);
     for (rfb_engine *e : b->m) rfb_engine_destroy(e);
-    cudaFree(b->d_step); cudaFree(b->d_err); cudaFree(b->d_queue);
-    cudaFree(b->d_args[0]); cudaFree(b->d_args[1]);
-    cudaFree(b->d_lblocks); cudaFree(b->d_probes);
+    dfree(b->d_step); dfree(b->d_err); dfree(b->d_queue);
+    dfree(b->d_args[0]); dfree(b->d_args[1]);
+    dfree(b->d_lblocks); dfree(b->d_probes);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (b->stream2) cudaStreamDestroy(b->stream2);
@@ -526,7 +526,7 @@ static int batch_upload_args(rfb_batch *b) {
             a[par][s] = engine_args<T>(b->m[s], par);
             a[par][s].d_step = b->d_step;
         }
-        CK(cudaMalloc(&b->d_args[par], n * sizeof(Args<T>)));
+        CK(dmalloc(&b->d_args[par], n * sizeof(Args<T>)));
         CK(cudaMemcpy(b->d_args[par], a[par].data(), n * sizeof(Args<T>), cudaMemcpyHostToDevice));
     }
     for (size_t s = 0; s < n; s++) {
@@ -550,12 +550,12 @@ static int batch_upload_args(rfb_batch *b) {
     }
     b->n_lblocks = (int)lblocks.size();
     if (b->n_lblocks) {
-        CK(cudaMalloc(&b->d_lblocks, lblocks.size() * sizeof(int2)));
+        CK(dmalloc(&b->d_lblocks, lblocks.size() * sizeof(int2)));
         CK(cudaMemcpy(b->d_lblocks, lblocks.data(), lblocks.size() * sizeof(int2), cudaMemcpyHostToDevice));
     }
     b->n_probes = (int)probes.size();
     if (b->n_probes) {
-        CK(cudaMalloc(&b->d_probes, probes.size() * sizeof(ProbeRefB<T>)));
+        CK(dmalloc(&b->d_probes, probes.size() * sizeof(ProbeRefB<T>)));
         CK(cudaMemcpy(b->d_probes, probes.data(), probes.size() * sizeof(ProbeRefB<T>), cudaMemcpyHostToDevice));
     }
     return 0;
@@ -607,11 +607,11 @@ extern "C" rfb_batch_t *rfb_batch_create(rfb_engine_t **members, size_t n, void 
     CK(cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
-    CK(cudaMalloc(&b->d_step, sizeof(int)));
+    CK(dmalloc(&b->d_step, sizeof(int)));
     CK(cudaMemset(b->d_step, 0, sizeof(int)));
-    CK(cudaMalloc(&b->d_err, sizeof(int)));
+    CK(dmalloc(&b->d_err, sizeof(int)));
     CK(cudaMemset(b->d_err, 0, sizeof(int)));
-    CK(cudaMalloc(&b->d_queue, 6 * sizeof(int)));
+    CK(dmalloc(&b->d_queue, 6 * sizeof(int)));
     CK(cudaMemset(b->d_queue, 0, 6 * sizeof(int)));
     if (qb_prepare() != 0) {
         rfb_set_error("cannot configure the batched sweep kernels' shared memory");

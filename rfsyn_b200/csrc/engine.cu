@@ -8,7 +8,9 @@
 
 #include <atomic>
 #include <iterator>
+#include <map>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -46,6 +48,127 @@ extern "C" unsigned long long rfb_launch_count(void) { return g_launches.load();
     } while (0)
 
 #define MU0_ 1.25663706212e-6
+
+// ---------------------------------------------------------------------------
+// Device memory cache.  cudaMalloc / cudaFree of megabyte blocks cost one to
+// a few milliseconds each on B200 (measured), and one scene holds dozens of
+// them, so a process that creates and destroys simulations again and again
+// (end-to-end runs, batches, sweeps of scenes) spent most of its set-up time
+// in the driver.  Blocks of 1 MB and more are rounded up to 2 MB and, when
+// freed, kept per device for the next allocation of a size within a quarter
+// of theirs.  A freed block enters the cache after a device synchronisation,
+// the same implicit synchronisation cudaFree performs, so no pending work
+// can still touch it when it is handed out again.  The cache holds at most a
+// quarter of the device's memory; an allocation that fails empties the
+// cache and retries.
+// ---------------------------------------------------------------------------
+namespace {
+struct MemCache {
+    std::mutex mu;
+    std::multimap<size_t, void *> free_blocks[64];  // per device, by size
+    size_t free_bytes[64] = {};
+    size_t cap[64] = {};
+    std::unordered_map<void *, std::pair<int, size_t>> live;  // cached-class block -> device, size
+};
+MemCache &mem_cache() {
+    static MemCache *c = new MemCache();  // never destroyed: frees may run at exit
+    return *c;
+}
+constexpr size_t MC_MIN = 1ull << 20, MC_GRAIN = 2ull << 20;
+
+void mc_release_device(MemCache &c, int dev) {
+    for (auto &kv : c.free_blocks[dev]) cudaFree(kv.second);
+    c.free_blocks[dev].clear();
+    c.free_bytes[dev] = 0;
+}
+}  // namespace
+
+static cudaError_t dmalloc_raw(void **p, size_t n) {
+    *p = nullptr;
+    if (n < MC_MIN) return cudaMalloc(p, n);
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess) return ce;
+    if (dev < 0 || dev >= 64) return cudaMalloc(p, n);
+    const size_t want = (n + MC_GRAIN - 1) / MC_GRAIN * MC_GRAIN;
+    MemCache &c = mem_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    auto &fb = c.free_blocks[dev];
+    auto it = fb.lower_bound(want);
+    if (it != fb.end() && it->first <= want + want / 4) {
+        *p = it->second;
+        c.free_bytes[dev] -= it->first;
+        c.live[*p] = {dev, it->first};
+        fb.erase(it);
+        return cudaSuccess;
+    }
+    ce = cudaMalloc(p, want);
+    if (ce == cudaErrorMemoryAllocation && c.free_bytes[dev]) {
+        cudaGetLastError();
+        mc_release_device(c, dev);
+        ce = cudaMalloc(p, want);
+    }
+    if (ce != cudaSuccess) {
+        *p = nullptr;
+        return ce;
+    }
+    c.live[*p] = {dev, want};
+    return cudaSuccess;
+}
+
+template <typename X>
+static cudaError_t dmalloc(X **p, size_t n) {
+    return dmalloc_raw(reinterpret_cast<void **>(p), n);
+}
+
+static cudaError_t dfree(void *p) {
+    if (!p) return cudaSuccess;
+    MemCache &c = mem_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    auto it = c.live.find(p);
+    if (it == c.live.end()) return cudaFree(p);
+    const int dev = it->second.first;
+    const size_t size = it->second.second;
+    c.live.erase(it);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaError_t ce = cudaDeviceSynchronize();
+    if (!c.cap[dev]) {
+        size_t fr = 0, tot = 0;
+        c.cap[dev] = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? tot / 4 : 0;
+    }
+    if (ce == cudaSuccess && c.free_bytes[dev] + size <= c.cap[dev]) {
+        c.free_blocks[dev].emplace(size, p);
+        c.free_bytes[dev] += size;
+    } else {
+        ce = cudaFree(p);
+    }
+    if (cur != dev) cudaSetDevice(cur);
+    return ce;
+}
+
+// Returns every cached block of every device to the driver.
+extern "C" void rfb_release_cached_memory(void) {
+    MemCache &c = mem_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int d = 0; d < 64; d++)
+        if (!c.free_blocks[d].empty()) {
+            cudaSetDevice(d);
+            mc_release_device(c, d);
+        }
+    cudaSetDevice(cur);
+}
+
+extern "C" unsigned long long rfb_cached_bytes(void) {
+    MemCache &c = mem_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    unsigned long long s = 0;
+    for (int d = 0; d < 64; d++) s += c.free_bytes[d];
+    return s;
+}
 
 // Device error codes the sweeps record in their error word.
 extern "C" double rfb_now(void) {
@@ -113,31 +236,32 @@ struct DevCpml {
     void *psi_e[6] = {};
     void *psi_h[2][6] = {};
     size_t psi_e_bytes[6] = {}, psi_h_bytes[6] = {};
+    // the profiles share one allocation and the psi arrays another, each
+    // array starting on a 256-byte boundary
+    void *prof_base = nullptr, *psi_base = nullptr;
+    size_t psi_total = 0;
 };
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 static void *dev_upload_conv(const double *src, size_t n, int prec) {
     void *d = nullptr;
     size_t esz = prec == RFB_FP64 ? 8 : 4;
-    if (cudaMalloc(&d, n * esz) != cudaSuccess) return nullptr;
+    if (dmalloc(&d, n * esz) != cudaSuccess) return nullptr;
     if (prec == RFB_FP64) {
-        if (cudaMemcpy(d, src, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+        if (cudaMemcpy(d, src, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) { dfree(d); return nullptr; }
     } else {
         std::vector<float> tmp(n);
         for (size_t q = 0; q < n; q++) tmp[q] = (float)src[q];
-        if (cudaMemcpy(d, tmp.data(), n * 4, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+        if (cudaMemcpy(d, tmp.data(), n * 4, cudaMemcpyHostToDevice) != cudaSuccess) { dfree(d); return nullptr; }
     }
     return d;
 }
 
 static void devcpml_free(DevCpml &c) {
-    for (int a = 0; a < 3; a++)
-        for (int q = 0; q < 6; q++) cudaFree(c.prof[a][q]), c.prof[a][q] = nullptr;
-    for (int p = 0; p < 6; p++) {
-        cudaFree(c.psi_e[p]); c.psi_e[p] = nullptr;
-        cudaFree(c.psi_h[0][p]); c.psi_h[0][p] = nullptr;
-        cudaFree(c.psi_h[1][p]); c.psi_h[1][p] = nullptr;
-    }
-    c.on = 0;
+    dfree(c.prof_base);
+    dfree(c.psi_base);
+    c = DevCpml();
 }
 
 // nbuf_h: 1 for in-place schedules, 2 for ping-pong H psi.
@@ -147,15 +271,37 @@ static int devcpml_init(DevCpml &c, const rfb_geom_t *g, const rfb_cpml_desc_t *
     c.on = 1;
     const int n[3] = {g->nx, g->ny, g->nz};
     const size_t esz = prec == RFB_FP64 ? 8 : 4;
-    for (int a = 0; a < 3; a++) {
-        const double *src[6] = {d->kinv_m[a], d->b_m[a], d->a_m[a], d->kinv_h[a], d->b_h[a], d->a_h[a]};
+    // profiles: staged in the run precision on the host, one upload
+    size_t prof_off[3][6], prof_bytes = 0;
+    for (int a = 0; a < 3; a++)
         for (int q = 0; q < 6; q++) {
-            size_t len = q < 3 ? (size_t)n[a] + 1 : (size_t)n[a];
-            c.prof[a][q] = dev_upload_conv(src[q], len, prec);
-            if (!c.prof[a][q]) { rfb_set_error("cpml profile upload failed"); return -1; }
+            prof_off[a][q] = prof_bytes;
+            prof_bytes += align256((q < 3 ? (size_t)n[a] + 1 : (size_t)n[a]) * esz);
         }
-        c.em[a] = slab_extent(d->kinv_m[a], d->b_m[a], d->a_m[a], n[a] + 1);
-        c.eh[a] = slab_extent(d->kinv_h[a], d->b_h[a], d->a_h[a], n[a]);
+    {
+        std::vector<unsigned char> stage(prof_bytes, 0);
+        for (int a = 0; a < 3; a++) {
+            const double *src[6] = {d->kinv_m[a], d->b_m[a], d->a_m[a], d->kinv_h[a], d->b_h[a], d->a_h[a]};
+            for (int q = 0; q < 6; q++) {
+                const size_t len = q < 3 ? (size_t)n[a] + 1 : (size_t)n[a];
+                unsigned char *dst = stage.data() + prof_off[a][q];
+                if (prec == RFB_FP64) {
+                    memcpy(dst, src[q], len * 8);
+                } else {
+                    float *f = reinterpret_cast<float *>(dst);
+                    for (size_t k = 0; k < len; k++) f[k] = (float)src[q][k];
+                }
+            }
+            c.em[a] = slab_extent(d->kinv_m[a], d->b_m[a], d->a_m[a], n[a] + 1);
+            c.eh[a] = slab_extent(d->kinv_h[a], d->b_h[a], d->a_h[a], n[a]);
+        }
+        if (dmalloc(&c.prof_base, prof_bytes) != cudaSuccess ||
+            cudaMemcpy(c.prof_base, stage.data(), prof_bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            rfb_set_error("cpml profile upload failed");
+            return -1;
+        }
+        for (int a = 0; a < 3; a++)
+            for (int q = 0; q < 6; q++) c.prof[a][q] = static_cast<char *>(c.prof_base) + prof_off[a][q];
     }
     // extents of a psi array with slab axis ax and ns slab cells
     auto bytes = [&](int ax, int ns) -> size_t {
@@ -165,23 +311,30 @@ static int devcpml_init(DevCpml &c, const rfb_geom_t *g, const rfb_cpml_desc_t *
         else e = (size_t)(g->nx + 1) * (g->ny + 1) * ns;
         return e * esz;
     };
+    // psi: offsets first, then one allocation cleared once
+    size_t off_e[6], off_h[2][6], total = 0;
     for (int p = 0; p < 6; p++) {
-        int ax = psi_axis_e(p);
-        size_t be = bytes(ax, c.em[ax].ns);
-        c.psi_e_bytes[p] = be;
-        if (be) {
-            if (cudaMalloc(&c.psi_e[p], be) != cudaSuccess) { rfb_set_error("psi alloc failed"); return -1; }
-            cudaMemset(c.psi_e[p], 0, be);
+        const int ax = psi_axis_e(p), ah = psi_axis_h(p);
+        c.psi_e_bytes[p] = bytes(ax, c.em[ax].ns);
+        c.psi_h_bytes[p] = bytes(ah, c.eh[ah].ns);
+        off_e[p] = total;
+        total += align256(c.psi_e_bytes[p]);
+        for (int b = 0; b < nbuf_h; b++) {
+            off_h[b][p] = total;
+            total += align256(c.psi_h_bytes[p]);
         }
-        int ah = psi_axis_h(p);
-        size_t bh = bytes(ah, c.eh[ah].ns);
-        c.psi_h_bytes[p] = bh;
-        if (bh) {
-            for (int b = 0; b < nbuf_h; b++) {
-                if (cudaMalloc(&c.psi_h[b][p], bh) != cudaSuccess) { rfb_set_error("psi alloc failed"); return -1; }
-                cudaMemset(c.psi_h[b][p], 0, bh);
-            }
-            if (nbuf_h == 1) c.psi_h[1][p] = nullptr;
+    }
+    c.psi_total = total;
+    if (total) {
+        if (dmalloc(&c.psi_base, total) != cudaSuccess || cudaMemset(c.psi_base, 0, total) != cudaSuccess) {
+            rfb_set_error("psi alloc failed");
+            return -1;
+        }
+        char *base = static_cast<char *>(c.psi_base);
+        for (int p = 0; p < 6; p++) {
+            if (c.psi_e_bytes[p]) c.psi_e[p] = base + off_e[p];
+            if (c.psi_h_bytes[p])
+                for (int b = 0; b < nbuf_h; b++) c.psi_h[b][p] = base + off_h[b][p];
         }
     }
     return 0;
@@ -238,12 +391,12 @@ struct DevScene {
 };
 
 static void devscene_free(DevScene &s) {
-    cudaFree(s.codes); cudaFree(s.tca); cudaFree(s.tcb);
-    cudaFree(s.lc_ijk); cudaFree(s.l_kind); cudaFree(s.l_ca); cudaFree(s.l_cb);
-    cudaFree(s.l_tix); cudaFree(s.l_src); cudaFree(s.l_aix); cudaFree(s.ade_c); cudaFree(s.ade_s);
-    cudaFree(s.t_m11); cudaFree(s.t_scale); cudaFree(s.t_w);
-    cudaFree(s.t_main); cudaFree(s.t_nq); cudaFree(s.t_uv); cudaFree(s.t_sign);
-    cudaFree(s.cb64_tab); cudaFree(s.cb64_list); cudaFree(s.t3);
+    dfree(s.codes); dfree(s.tca); dfree(s.tcb);
+    dfree(s.lc_ijk); dfree(s.l_kind); dfree(s.l_ca); dfree(s.l_cb);
+    dfree(s.l_tix); dfree(s.l_src); dfree(s.l_aix); dfree(s.ade_c); dfree(s.ade_s);
+    dfree(s.t_m11); dfree(s.t_scale); dfree(s.t_w);
+    dfree(s.t_main); dfree(s.t_nq); dfree(s.t_uv); dfree(s.t_sign);
+    dfree(s.cb64_tab); dfree(s.cb64_list); dfree(s.t3);
     s = DevScene();
 }
 
@@ -251,8 +404,8 @@ template <typename X>
 static X *dev_copy(const X *src, size_t n) {
     if (!n || !src) return nullptr;
     X *d = nullptr;
-    if (cudaMalloc(&d, n * sizeof(X)) != cudaSuccess) return nullptr;
-    if (cudaMemcpy(d, src, n * sizeof(X), cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    if (dmalloc(&d, n * sizeof(X)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, src, n * sizeof(X), cudaMemcpyHostToDevice) != cudaSuccess) { dfree(d); return nullptr; }
     return d;
 }
 
@@ -271,7 +424,7 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
     const size_t total_b = plane_b * (g->nx + 1);
     s.n_cells = img ? (int)img->n_cells : 0;
     if (img && img->codes) {
-        if (cudaMalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
+        if (dmalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
         const size_t rows = (size_t)(g->nx + 1) * (g->ny + 1), row = (size_t)g->nz + 1;
         if (pitch == (long long)row) {
             if (cudaMemcpy(s.codes, img->codes, rows * row, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -282,7 +435,7 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
             // one contiguous upload, then a device-side repack into the
             // pitched layout (a strided host copy of short rows is slow)
             uint8_t *tmp = nullptr;
-            if (cudaMalloc(&tmp, rows * row) != cudaSuccess) { rfb_set_error("code volume staging failed"); return -1; }
+            if (dmalloc(&tmp, rows * row) != cudaSuccess) { rfb_set_error("code volume staging failed"); return -1; }
             cudaError_t ce = cudaMemcpy(tmp, img->codes, rows * row, cudaMemcpyHostToDevice);
             if (ce == cudaSuccess) {
                 const long long n = (long long)(rows * row);
@@ -290,7 +443,7 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
                 g_launches++;
                 ce = cudaDeviceSynchronize();
             }
-            cudaFree(tmp);
+            dfree(tmp);
             if (ce != cudaSuccess) { rfb_set_error("code volume upload failed"); return -1; }
         }
     }
@@ -332,7 +485,7 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
         if (img->n_ade) {
             s.ade_c = dev_upload_conv(img->ade_c, img->n_ade * RFB_ADE_NC, prec);
             s.ade_s_bytes = ne * 5 * (prec == RFB_FP64 ? 8 : 4);
-            if (!s.ade_c || cudaMalloc(&s.ade_s, s.ade_s_bytes) != cudaSuccess) {
+            if (!s.ade_c || dmalloc(&s.ade_s, s.ade_s_bytes) != cudaSuccess) {
                 rfb_set_error("dispersive state allocation failed");
                 return -1;
             }
@@ -345,7 +498,7 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
                     s.skip[q] = ((long long)img->cell_ijk[3 * q] * (g->ny + 1) + img->cell_ijk[3 * q + 1]) * pitch +
                                 img->cell_ijk[3 * q + 2];
             } else {
-                if (cudaMalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
+                if (dmalloc(&s.codes, total_b) != cudaSuccess) { rfb_set_error("code volume alloc failed"); return -1; }
                 cudaMemset(s.codes, 0, total_b);
                 k_mark_list<<<(s.n_cells + 255) / 256, 256>>>(s.codes, s.lc_ijk, s.n_cells, g->ny, pitch);
                 g_launches++;
@@ -633,10 +786,10 @@ fail:
 // slab and PEC boundary (and hold no code-less list cell), over the interior
 // plane range; edge items: (8 x 32) tiles over everything else.
 static void free_plan_lists(FusedPlan &p) {
-    cudaFree(p.d_int);
-    cudaFree(p.d_edge);
-    cudaFree(p.d_qe);
-    cudaFree(p.d_qx);
+    dfree(p.d_int);
+    dfree(p.d_edge);
+    dfree(p.d_qe);
+    dfree(p.d_qx);
     p.d_int = p.d_edge = p.d_qe = p.d_qx = nullptr;
     p.n_int = p.n_edge = p.n_qe = p.n_qx = 0;
 }
@@ -892,16 +1045,16 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     p.n_edge = (int)ve.size();
     p.n_qe = (int)vq.size();
     p.n_qx = (int)vx.size();
-    if (p.n_int) CK(cudaMalloc(&p.d_int, vi.size() * sizeof(SweepItem)));
-    if (p.n_edge) CK(cudaMalloc(&p.d_edge, ve.size() * sizeof(SweepItem)));
-    if (p.n_qe) CK(cudaMalloc(&p.d_qe, vq.size() * sizeof(SweepItem)));
-    if (p.n_qx) CK(cudaMalloc(&p.d_qx, vx.size() * sizeof(SweepItem)));
+    if (p.n_int) CK(dmalloc(&p.d_int, vi.size() * sizeof(SweepItem)));
+    if (p.n_edge) CK(dmalloc(&p.d_edge, ve.size() * sizeof(SweepItem)));
+    if (p.n_qe) CK(dmalloc(&p.d_qe, vq.size() * sizeof(SweepItem)));
+    if (p.n_qx) CK(dmalloc(&p.d_qx, vx.size() * sizeof(SweepItem)));
     if (p.n_int) CK(cudaMemcpy(p.d_int, vi.data(), vi.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_edge) CK(cudaMemcpy(p.d_edge, ve.data(), ve.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_qe) CK(cudaMemcpy(p.d_qe, vq.data(), vq.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (p.n_qx) CK(cudaMemcpy(p.d_qx, vx.data(), vx.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
     if (tma >= 2 && !p.d_queue) {
-        CK(cudaMalloc(&p.d_queue, 6 * sizeof(int)));
+        CK(dmalloc(&p.d_queue, 6 * sizeof(int)));
         CK(cudaMemset(p.d_queue, 0, 6 * sizeof(int)));
     }
     if (tma && (p.n_int || p.n_qe || p.n_qx) && build_tma_maps(e, tj) != 0) return -1;
@@ -1056,18 +1209,18 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
         if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
         if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
     }
-    cudaFree(e->fld_base);
+    dfree(e->fld_base);
     devcpml_free(e->cpml);
     devscene_free(e->scene);
-    cudaFree(e->src_val); cudaFree(e->src_hard);
-    cudaFree(e->probe_cell); cudaFree(e->probe_comp); cudaFree(e->ts); cudaFree(e->d_step); cudaFree(e->d_err); cudaFree(e->d_energy); cudaFree(e->d_iq);
-    cudaFree(e->t3_cells);
-    cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
-    cudaFree(e->plan.d_int); cudaFree(e->plan.d_edge); cudaFree(e->plan.d_qe); cudaFree(e->plan.d_qx); cudaFree(e->plan.d_queue);
-    cudaFree(e->tf_inc_e); cudaFree(e->tf_inc_h); cudaFree(e->tf_src); cudaFree(e->tf_h_cell); cudaFree(e->tf_h_comp);
-    cudaFree(e->tf_h_first); cudaFree(e->tf_h_count); cudaFree(e->tf_h_idx); cudaFree(e->tf_h_coef); cudaFree(e->tf_h_w);
-    cudaFree(e->tf_e_first); cudaFree(e->tf_e_count); cudaFree(e->tf_e_idx); cudaFree(e->tf_e_coef);
-    cudaFree(e->tf_e_w);
+    dfree(e->src_val); dfree(e->src_hard);
+    dfree(e->probe_cell); dfree(e->probe_comp); dfree(e->ts); dfree(e->d_step); dfree(e->d_err); dfree(e->d_energy); dfree(e->d_iq);
+    dfree(e->t3_cells);
+    dfree(e->d_omega); dfree(e->d_re); dfree(e->d_im);
+    dfree(e->plan.d_int); dfree(e->plan.d_edge); dfree(e->plan.d_qe); dfree(e->plan.d_qx); dfree(e->plan.d_queue);
+    dfree(e->tf_inc_e); dfree(e->tf_inc_h); dfree(e->tf_src); dfree(e->tf_h_cell); dfree(e->tf_h_comp);
+    dfree(e->tf_h_first); dfree(e->tf_h_count); dfree(e->tf_h_idx); dfree(e->tf_h_coef); dfree(e->tf_h_w);
+    dfree(e->tf_e_first); dfree(e->tf_e_count); dfree(e->tf_e_idx); dfree(e->tf_e_coef);
+    dfree(e->tf_e_w);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->stream2) cudaStreamDestroy(e->stream2);
@@ -1139,7 +1292,7 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
         // every buffer is a multiple of 128 bytes (whole pitched rows), so
         // the sub-buffers keep the alignment the tensor copies need
         const size_t one = e->total * e->esz;
-        CK(cudaMalloc(&e->fld_base, one * 6 * e->nbuf));
+        CK(dmalloc(&e->fld_base, one * 6 * e->nbuf));
         CK(cudaMemsetAsync(e->fld_base, 0, one * 6 * e->nbuf, e->stream));
         for (int b = 0; b < e->nbuf; b++)
             for (int c = 0; c < 6; c++) e->fld[b][c] = static_cast<char *>(e->fld_base) + (size_t)(6 * b + c) * one;
@@ -1174,13 +1327,13 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
         }
         e->probe_cell = dev_copy(cell.data(), n_probes);
         e->probe_comp = dev_copy(comp.data(), n_probes);
-        CK(cudaMalloc(&e->ts, n_probes * n_steps * e->esz));
+        CK(dmalloc(&e->ts, n_probes * n_steps * e->esz));
         CK(cudaMemset(e->ts, 0, n_probes * n_steps * e->esz));
         if (!e->probe_cell || !e->probe_comp) { rfb_set_error("probe upload failed"); goto fail_noset; }
     }
-    CK(cudaMalloc(&e->d_step, sizeof(int)));
+    CK(dmalloc(&e->d_step, sizeof(int)));
     CK(cudaMemset(e->d_step, 0, sizeof(int)));
-    CK(cudaMalloc(&e->d_err, sizeof(int)));
+    CK(dmalloc(&e->d_err, sizeof(int)));
     CK(cudaMemset(e->d_err, 0, sizeof(int)));
     if (schedule == RFB_SCHED_FUSED) {
         if (fused_prepare() != 0) {
@@ -1301,8 +1454,8 @@ extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
     e->tf_ce = d->ce;
     e->tf_ch = d->ch;
     e->tf_n_h = (int)d->n_h;
-    CK(cudaMalloc(&e->tf_inc_e, d->m_len * e->esz));
-    CK(cudaMalloc(&e->tf_inc_h, d->m_len * e->esz));
+    CK(dmalloc(&e->tf_inc_e, d->m_len * e->esz));
+    CK(dmalloc(&e->tf_inc_h, d->m_len * e->esz));
     CK(cudaMemset(e->tf_inc_e, 0, d->m_len * e->esz));
     CK(cudaMemset(e->tf_inc_h, 0, d->m_len * e->esz));
     e->tf_src = dev_upload_conv(d->src, e->n_steps + 1, prec);
@@ -1347,13 +1500,8 @@ fail:
 }
 
 extern "C" int rfb_engine_reset(rfb_engine_t *e) {
-    for (int b = 0; b < e->nbuf; b++)
-        for (int c = 0; c < 6; c++) CK(cudaMemsetAsync(e->fld[b][c], 0, e->total * e->esz, e->stream));
-    for (int p = 0; p < 6; p++) {
-        if (e->cpml.psi_e[p]) CK(cudaMemsetAsync(e->cpml.psi_e[p], 0, e->cpml.psi_e_bytes[p], e->stream));
-        for (int b = 0; b < 2; b++)
-            if (e->cpml.psi_h[b][p]) CK(cudaMemsetAsync(e->cpml.psi_h[b][p], 0, e->cpml.psi_h_bytes[p], e->stream));
-    }
+    CK(cudaMemsetAsync(e->fld_base, 0, e->total * e->esz * 6 * e->nbuf, e->stream));
+    if (e->cpml.psi_base) CK(cudaMemsetAsync(e->cpml.psi_base, 0, e->cpml.psi_total, e->stream));
     if (e->scene.ade_s) CK(cudaMemsetAsync(e->scene.ade_s, 0, e->scene.ade_s_bytes, e->stream));
     if (e->tf_on) {
         CK(cudaMemsetAsync(e->tf_inc_e, 0, (size_t)e->tf_m_len * e->esz, e->stream));
@@ -1538,7 +1686,7 @@ static void enqueue_energy(rfb_engine *e, double dt, double dx, int x_lo, int x_
 
 extern "C" int rfb_engine_energy(rfb_engine_t *e, double dt, double dx, int x_lo, int x_hi, double q[RFB_EN_COUNT]) {
     const bool prev = e->nbuf == 2 && e->steps_done > 0;
-    if (!e->d_energy) CK(cudaMalloc(&e->d_energy, (size_t)(EN_BLOCKS + 1) * RFB_EN_COUNT * sizeof(double)));
+    if (!e->d_energy) CK(dmalloc(&e->d_energy, (size_t)(EN_BLOCKS + 1) * RFB_EN_COUNT * sizeof(double)));
     if (e->prec == RFB_FP64) enqueue_energy<double>(e, dt, dx, x_lo, x_hi, prev);
     else enqueue_energy<float>(e, dt, dx, x_lo, x_hi, prev);
     k_energy_final<<<1, 32, 0, e->stream>>>(e->d_energy, EN_BLOCKS, pow(dx, 3.0), prev ? 1 : 0,
@@ -1596,7 +1744,7 @@ extern "C" int rfb_engine_read_iq(rfb_engine_t *e, int probe, int noise, double 
         return -1;
     }
     // samples, then the noise scale in an 8-byte slot at float offset 2 n + 2
-    if (!e->d_iq) CK(cudaMalloc(&e->d_iq, (size_t)(2 * n + 4) * sizeof(float)));
+    if (!e->d_iq) CK(dmalloc(&e->d_iq, (size_t)(2 * n + 4) * sizeof(float)));
     {
         double *d_std = noise ? reinterpret_cast<double *>(e->d_iq + 2 * n + 2) : nullptr;
         const size_t off = (size_t)probe * (size_t)n * e->esz;
@@ -1645,7 +1793,7 @@ extern "C" int fdtd_b200_selftest_bounded_wait(long long limit_cycles, int *time
         rfb_set_error("selftest: limit must lie in (0, 4e9] cycles");
         return -1;
     }
-    if (cudaMalloc(&d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&d_cycles, sizeof(long long)) != cudaSuccess) {
+    if (dmalloc(&d_status, sizeof(int)) != cudaSuccess || dmalloc(&d_cycles, sizeof(long long)) != cudaSuccess) {
         rfb_set_error("selftest: device allocation failed");
         goto out;
     }
@@ -1659,8 +1807,8 @@ extern "C" int fdtd_b200_selftest_bounded_wait(long long limit_cycles, int *time
     }
     rc = 0;
 out:
-    cudaFree(d_status);
-    cudaFree(d_cycles);
+    dfree(d_status);
+    dfree(d_cycles);
     return rc;
 }
 
@@ -1688,11 +1836,11 @@ extern "C" int rfb_engine_probe_dft(rfb_engine_t *e, size_t n_freqs, const doubl
     const size_t nout = (size_t)e->n_probes * n_freqs;
     for (size_t f = 0; f < n_freqs; f++) om[f] = 2.0 * 3.14159265358979323846 * freqs_hz[f];
     if (e->dft_cap < n_freqs || !e->d_re) {
-        cudaFree(e->d_omega); cudaFree(e->d_re); cudaFree(e->d_im);
+        dfree(e->d_omega); dfree(e->d_re); dfree(e->d_im);
         e->d_omega = e->d_re = e->d_im = nullptr;
-        CK(cudaMalloc(&e->d_omega, n_freqs * 8));
-        CK(cudaMalloc(&e->d_re, nout * 8));
-        CK(cudaMalloc(&e->d_im, nout * 8));
+        CK(dmalloc(&e->d_omega, n_freqs * 8));
+        CK(dmalloc(&e->d_re, nout * 8));
+        CK(dmalloc(&e->d_im, nout * 8));
         e->dft_cap = n_freqs;
     }
     CK(cudaMemcpyAsync(e->d_omega, om.data(), n_freqs * 8, cudaMemcpyHostToDevice, e->stream));
@@ -1818,13 +1966,13 @@ extern "C" int rfb_sphere_fractions(const double centre[3], double radius, int i
     {
         FracScratch &s = g_frac[dev];
         if (s.cap < n) {
-            cudaFree(s.dev);
+            dfree(s.dev);
             cudaFreeHost(s.host);
             s.dev = nullptr;
             s.host = nullptr;
             s.cap = 0;
             const size_t want = std::max(n, (size_t)1 << 18);
-            CK(cudaMalloc(&s.dev, 2 * want * sizeof(double)));
+            CK(dmalloc(&s.dev, 2 * want * sizeof(double)));
             CK(cudaMallocHost(&s.host, 2 * want * sizeof(double)));
             s.cap = want;
         }
@@ -1870,7 +2018,7 @@ extern "C" rfb_fields_t *rfb_fields_create(const rfb_geom_t *geom) {
     f->pitch = step_pitch(geom->nz);
     f->total = (size_t)(geom->nx + 1) * (geom->ny + 1) * f->pitch;
     CK(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
-    for (int c = 0; c < 6; c++) CK(cudaMalloc(&f->f[c], f->total * 8));
+    for (int c = 0; c < 6; c++) CK(dmalloc(&f->f[c], f->total * 8));
     return f;
 fail:
     rfb_fields_destroy(f);
@@ -1879,7 +2027,7 @@ fail:
 
 extern "C" void rfb_fields_destroy(rfb_fields_t *f) {
     if (!f) return;
-    for (int c = 0; c < 6; c++) cudaFree(f->f[c]);
+    for (int c = 0; c < 6; c++) dfree(f->f[c]);
     if (f->stream) cudaStreamDestroy(f->stream);
     delete f;
 }
@@ -1969,7 +2117,7 @@ extern "C" int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cp
         double one = 1.0;
         vca = dev_copy(&one, 1);
         vcb = dev_copy(&vacuum_cb, 1);
-        if (!vca || !vcb) { rfb_set_error("vacuum table upload failed"); cudaFree(vca); cudaFree(vcb); return -1; }
+        if (!vca || !vcb) { rfb_set_error("vacuum table upload failed"); dfree(vca); dfree(vcb); return -1; }
         a.tca = vca;
         a.tcb = vcb;
     }
@@ -1989,8 +2137,8 @@ extern "C" int rfb_step_update_e(rfb_fields_t *f, const rfb_geom_t *geom, rfb_cp
     rc = 0;
 out:
     cudaStreamSynchronize(f->stream);
-    cudaFree(vca);
-    cudaFree(vcb);
+    dfree(vca);
+    dfree(vcb);
     (void)vac;
     return rc;
 }

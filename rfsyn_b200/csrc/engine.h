@@ -262,6 +262,8 @@ void rfb_trace(const char *phase, double t0);
 
 /* Number of kernels this process has launched through the engine. */
 unsigned long long rfb_launch_count(void);
+unsigned long long rfb_cached_bytes(void);
+void rfb_release_cached_memory(void);
 
 #ifdef __cplusplus
 }

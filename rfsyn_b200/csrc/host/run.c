@@ -46,6 +46,8 @@ int fdtd_b200_set_default_schedule(int schedule) {
 
 const char *fdtd_b200_last_error(void) { return rfb_last_error(); }
 unsigned long long fdtd_b200_launch_count(void) { return rfb_launch_count(); }
+unsigned long long fdtd_b200_cached_bytes(void) { return rfb_cached_bytes(); }
+void fdtd_b200_release_cached_memory(void) { rfb_release_cached_memory(); }
 const char *fdtd_b200_version(void) { return "rfsyn-b200 0.1 (sm_100a)"; }
 
 void fdtd_b200_config_init(fdtd_b200_config_t *cfg, size_t nx, size_t ny, size_t nz, double dx, size_t n_steps,
