@@ -43,6 +43,15 @@ static uint64_t mix64(uint64_t x) {
     return x;
 }
 
+/* Home slot of a key.  Keys are cell * 3 + component, and scenes describe
+ * cells in runs along k, so runs of 32 consecutive keys keep consecutive
+ * slots and only the run is hashed: filling or reading a slab, a box or a
+ * shell walks the table (and its values) nearly sequentially instead of
+ * taking a cache miss per key. */
+static size_t omap_home(uint64_t key, size_t mask) {
+    return (size_t)((mix64(key >> 5) << 5) | (key & 31u)) & mask;
+}
+
 static int omap_init(omap_t *m, size_t vw) {
     m->vw = vw;
     m->cap = 0;
@@ -63,7 +72,7 @@ static void omap_free(omap_t *m) {
 
 static long omap_find(const omap_t *m, uint64_t key) {
     if (!m->cap) return -1;
-    size_t mask = m->cap - 1, h = mix64(key) & mask;
+    size_t mask = m->cap - 1, h = omap_home(key, mask);
     for (;;) {
         if (m->keys[h] == OMAP_EMPTY) return -1;
         if (m->keys[h] == key) return (long)h;
@@ -86,7 +95,7 @@ static int omap_grow(omap_t *m, size_t want_cap) {
     size_t mask = want_cap - 1;
     for (size_t q = 0; q < ocap; q++) {
         if (ok[q] == OMAP_EMPTY) continue;
-        size_t h = mix64(ok[q]) & mask;
+        size_t h = omap_home(ok[q], mask);
         while (nk[h] != OMAP_EMPTY) h = (h + 1) & mask;
         nk[h] = ok[q];
         memcpy(nv + h * m->vw, ov + q * m->vw, m->vw * sizeof(double));
@@ -99,21 +108,29 @@ static int omap_grow(omap_t *m, size_t want_cap) {
     return 0;
 }
 
+/* Room for n_more new keys without a rehash on the way (a bulk setter
+ * reserves once instead of growing through every power of two). */
+static int omap_reserve(omap_t *m, size_t n_more) {
+    const size_t need = 2 * (m->count + n_more);
+    if (need <= m->cap) return 0;
+    size_t cap = m->cap ? m->cap : 64;
+    while (cap < need) cap *= 2;
+    return omap_grow(m, cap);
+}
+
 static int omap_put(omap_t *m, uint64_t key, const double *val) {
     if (m->mark) m->mark[key / 3] = 1;
-    long at = omap_find(m, key);
-    if (at >= 0) {
-        memcpy(m->vals + (size_t)at * m->vw, val, m->vw * sizeof(double));
-        return 0;
-    }
     if ((m->count + 1) * 2 > m->cap) {
         if (omap_grow(m, m->cap ? m->cap * 2 : 64) != 0) return -1;
     }
-    size_t mask = m->cap - 1, h = mix64(key) & mask;
-    while (m->keys[h] != OMAP_EMPTY) h = (h + 1) & mask;
-    m->keys[h] = key;
+    /* one probe: the key's slot, or the empty slot that ends its chain */
+    size_t mask = m->cap - 1, h = omap_home(key, mask);
+    while (m->keys[h] != OMAP_EMPTY && m->keys[h] != key) h = (h + 1) & mask;
+    if (m->keys[h] == OMAP_EMPTY) {
+        m->keys[h] = key;
+        m->count++;
+    }
     memcpy(m->vals + h * m->vw, val, m->vw * sizeof(double));
-    m->count++;
     return 0;
 }
 
@@ -123,7 +140,7 @@ static void omap_del_slot(omap_t *m, size_t h) {
     size_t hole = h;
     size_t q = (h + 1) & mask;
     while (m->keys[q] != OMAP_EMPTY) {
-        size_t home = mix64(m->keys[q]) & mask;
+        size_t home = omap_home(m->keys[q], mask);
         /* can the entry at q move into the hole? (home not in (hole, q]) */
         int movable = (q > hole) ? (home <= hole || home > q) : (home <= hole && home > q);
         if (movable) {
@@ -531,18 +548,43 @@ int fdtd_b200_materials_set_tensor3_slab(materials_t *mat, const fdtd_grid_t *g,
         lo[a] = per ? 0 : 1;
         hi[a] = per ? n[a] : n[a];  /* cells [lo, hi): the margin rule keeps index n - 1 at most */
     }
-    for (size_t i = lo[0]; i < hi[0]; i++)
-        for (size_t j = lo[1]; j < hi[1]; j++)
-            for (size_t k = lo[2]; k < hi[2]; k++)
-                for (int c = 0; c < 3; c++) {
-                    double p[3] = {(double)i, (double)j, (double)k};
-                    p[c] += 0.5;
-                    const double d = u[0] * (p[0] - point[0]) + u[1] * (p[1] - point[1]) + u[2] * (p[2] - point[2]);
-                    if (fabs(d) > 0.5 * thickness) continue;
-                    if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) continue;
-                    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, m + 3 * c) != 0)
-                        return -1;
+    /* Per (i, j) column only the k range the slab can reach is tested: the
+     * sample offsets move d by at most 0.5 (|u0| + |u1| + |u2|), and a cell
+     * of margin on each side keeps the bound conservative; every sample
+     * then passes the exact test below.  Pass 0 counts, pass 1 stores. */
+    const double half = 0.5 * thickness, slack = 0.5 * (fabs(u[0]) + fabs(u[1]) + fabs(u[2]));
+    for (int pass = 0; pass < 2; pass++) {
+        size_t count = 0;
+        for (size_t i = lo[0]; i < hi[0]; i++)
+            for (size_t j = lo[1]; j < hi[1]; j++) {
+                size_t ka = lo[2], kb = hi[2];
+                if (fabs(u[2]) > 1e-9) {
+                    const double r0 = u[0] * ((double)i - point[0]) + u[1] * ((double)j - point[1]) - u[2] * point[2];
+                    double a = (-half - slack - r0) / u[2], b = (half + slack - r0) / u[2];
+                    if (a > b) { const double s = a; a = b; b = s; }
+                    a = floor(a) - 1.0;
+                    b = ceil(b) + 2.0;
+                    if (a > (double)ka) ka = a >= (double)hi[2] ? hi[2] : (size_t)a;
+                    if (b < (double)kb) kb = b <= (double)ka ? ka : (size_t)b;
                 }
+                for (size_t k = ka; k < kb; k++)
+                    for (int c = 0; c < 3; c++) {
+                        double p[3] = {(double)i, (double)j, (double)k};
+                        p[c] += 0.5;
+                        const double d =
+                            u[0] * (p[0] - point[0]) + u[1] * (p[1] - point[1]) + u[2] * (p[2] - point[2]);
+                        if (fabs(d) > half) continue;
+                        if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) continue;
+                        if (pass == 0) {
+                            count++;
+                        } else if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c,
+                                            m + 3 * c) != 0) {
+                            return -1;
+                        }
+                    }
+            }
+        if (pass == 0 && omap_reserve(&mat->tensor3, count) != 0) return -1;
+    }
     mat->version++;
     return 0;
 }
@@ -551,6 +593,7 @@ int fdtd_b200_materials_set_dispersive_box(materials_t *mat, const fdtd_grid_t *
                                            size_t j1, size_t k0, size_t k1, const fdtd_b200_dispersive_t *model) {
     double v[DISP_W];
     if (!model || pack_model(model, v) != 0 || !box_valid(mat, g, i0, i1, j0, j1, k0, k1)) return -1;
+    if (omap_reserve(&mat->disp, 3 * (i1 - i0) * (j1 - j0) * (k1 - k0)) != 0) return -1;
     for (size_t i = i0; i < i1; i++)
         for (size_t j = j0; j < j1; j++)
             for (size_t k = k0; k < k1; k++)
