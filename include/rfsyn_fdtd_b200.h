@@ -454,6 +454,25 @@ const char *fdtd_b200_version(void);
 unsigned long long fdtd_b200_cached_bytes(void);
 void fdtd_b200_release_cached_memory(void);
 
+/* ---- fdtd.gpu.* settings ------------------------------------------------------
+ * The config surface's GPU section.  rfsyn's pipeline config keeps the FDTD
+ * stage's keys in its "fdtd" section (cli/settings.c:6-33); the GPU options
+ * sit beside them as "gpu.<name>" (set with `config set fdtd.gpu.<name> v`,
+ * cli/main.c:233-290).  key: "fdtd.gpu.<name>", "gpu.<name>" or "<name>";
+ * value as text (a boolean as true/false or 1/0):
+ *   precision  fp32 | fp64          default precision of rfsyn's entry points
+ *   schedule   fused | split        default schedule of rfsyn's entry points
+ *   plan       auto | tj,ns,seg_interior,seg_edge[,mode[,single_queue]]
+ *                                   the sweep plan (auto = the autotuner)
+ *   tune       true | false         false: the first tensor-copy variant, no tuning
+ *   trace      true | false         per-phase host times on stderr
+ * "default" restores a setting's initial state (its RFSYN_FDTD_* environment
+ * variable decides).  Returns 0, or -1 with fdtd_b200_last_error() for an
+ * unknown key or a value it does not accept (the setting is unchanged).
+ * fdtd_b200_get_setting writes the current value as text. */
+int fdtd_b200_apply_setting(const char *key, const char *value);
+int fdtd_b200_get_setting(const char *key, char *buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

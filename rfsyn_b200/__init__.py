@@ -274,6 +274,8 @@ def load() -> C.CDLL:
         "fdtd_b200_launch_count": (C.c_ulonglong, []),
         "fdtd_b200_cached_bytes": (C.c_ulonglong, []),
         "fdtd_b200_release_cached_memory": (None, []),
+        "fdtd_b200_apply_setting": (I, [C.c_char_p, C.c_char_p]),
+        "fdtd_b200_get_setting": (I, [C.c_char_p, C.c_char_p, S]),
         "fdtd_b200_set_default_precision": (I, [I]),
         "fdtd_b200_set_default_schedule": (I, [I]),
         "fdtd_b200_version": (C.c_char_p, []),
@@ -323,6 +325,15 @@ def load() -> C.CDLL:
 
 def last_error() -> str:
     return load().fdtd_b200_last_error().decode()
+
+
+def iq_write(path, iq: np.ndarray) -> None:
+    """Writes complex64 samples as rfsyn's .iq file (interleaved float32 I/Q,
+    fdtd_b200_iq_write)."""
+    a = np.ascontiguousarray(iq, dtype=np.complex64)
+    ptr = a.view(np.float32).ctypes.data_as(C.POINTER(C.c_float)) if a.size else None
+    if load().fdtd_b200_iq_write(os.fsencode(path), ptr, a.size) != 0:
+        raise OSError(f"could not write {path}: {last_error()}")
 
 
 def cached_bytes() -> int:

@@ -425,12 +425,12 @@ static int batch_autotune(rfb_batch *b) {
     for (size_t q = 0; q < nv; q++)
         for (int mode = 2; mode <= (wrap_yz ? 3 : 4); mode++)
             for (int uni : {0, 1}) cands.push_back(Cand{v[q].tj, v[q].ns, mode, 64, 32, uni});
-    const char *ov = getenv("RFSYN_FDTD_PLAN");
+    const char *ov = rfb_plan_override();
     if (ov) {
         int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
         const int nov = sscanf(ov, "%d,%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5, &a6);
         if (nov < 5 || a5 < 2 || a3 <= 0 || a4 <= 0 || a6 < 0 || a6 > 1 || !plan_variant_known(b->prec, a1, a2, a5)) {
-            rfb_set_error("RFSYN_FDTD_PLAN=\"%s\" names no work-queue sweep variant", ov);
+            rfb_set_error("sweep plan \"%s\" names no work-queue sweep variant", ov);
             return -1;
         }
         return batch_build_plan(b, a1, a2, a5, a3, a4, a6);

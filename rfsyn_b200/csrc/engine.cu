@@ -177,12 +177,25 @@ extern "C" double rfb_now(void) {
     return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
 
-extern "C" void rfb_trace(const char *phase, double t0) {
-    static const int on = [] {
+// -1 until first read: RFSYN_FDTD_TRACE=1 or the trace setting turns it on
+static std::atomic<int> g_trace{-1};
+
+extern "C" int rfb_trace_enabled(void) {
+    int on = g_trace.load();
+    if (on < 0) {
         const char *v = getenv("RFSYN_FDTD_TRACE");
-        return v && v[0] == '1';
-    }();
-    if (on) fprintf(stderr, "rfsyn_b200 trace: %s %.3f ms\n", phase, 1e3 * (rfb_now() - t0));
+        on = v && v[0] == '1';
+        int expect = -1;
+        g_trace.compare_exchange_strong(expect, on);
+        on = g_trace.load();
+    }
+    return on;
+}
+
+extern "C" void rfb_set_trace(int on) { g_trace.store(on < 0 ? -1 : on ? 1 : 0); }
+
+extern "C" void rfb_trace(const char *phase, double t0) {
+    if (rfb_trace_enabled()) fprintf(stderr, "rfsyn_b200 trace: %s %.3f ms\n", phase, 1e3 * (rfb_now() - t0));
 }
 
 static const char *sweep_error_text(int err) {
@@ -1366,8 +1379,7 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
         // plan: "tj,ns,seg_interior,seg_edge[,mode[,single_queue]]" from RFSYN_FDTD_PLAN,
         // the autotuner (default) or, with RFSYN_FDTD_TUNE=0, the first
         // TMA variant
-        const char *ov = getenv("RFSYN_FDTD_PLAN");
-        const char *tune = getenv("RFSYN_FDTD_TUNE");
+        const char *ov = rfb_plan_override();
         int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
         int rc;
         const int nov = ov ? sscanf(ov, "%d,%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5, &a6) : 0;
@@ -1375,8 +1387,8 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
             (a6 == 0 || (a6 == 1 && a5 >= 2)))
             rc = build_sweep_plan(e, active, a1, a2, nov >= 5 ? a5 : 0, a3, a4, a6);
         else if (ov)
-            rc = (rfb_set_error("RFSYN_FDTD_PLAN=\"%s\" names no sweep variant", ov), -1);
-        else if (tune && !strcmp(tune, "0"))
+            rc = (rfb_set_error("sweep plan \"%s\" names no sweep variant", ov), -1);
+        else if (!rfb_tune_enabled())
             rc = build_sweep_plan(e, active, precision == RFB_FP32 ? kTmaVariantsFp32[0].tj : kTmaVariantsFp64[0].tj,
                                   precision == RFB_FP32 ? kTmaVariantsFp32[0].ns : kTmaVariantsFp64[0].ns, 1, 64,
                                   32);

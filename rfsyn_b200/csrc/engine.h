@@ -263,6 +263,11 @@ void rfb_trace(const char *phase, double t0);
 /* Number of kernels this process has launched through the engine. */
 unsigned long long rfb_launch_count(void);
 unsigned long long rfb_cached_bytes(void);
+/* process-wide settings (host/run.c, engine.cu) */
+const char *rfb_plan_override(void);
+int rfb_tune_enabled(void);
+void rfb_set_trace(int on);
+int rfb_trace_enabled(void);
 void rfb_release_cached_memory(void);
 
 #ifdef __cplusplus

@@ -44,6 +44,123 @@ int fdtd_b200_set_default_schedule(int schedule) {
     return 0;
 }
 
+/* ---- fdtd.gpu.* settings ------------------------------------------------------
+ * rfsyn's pipeline config keeps the FDTD stage's keys in its "fdtd" section
+ * (cli/settings.c:6-33, read with config.c's typed getters); the GPU options
+ * live beside them as "gpu.<name>" keys, which rfsyn's `config set
+ * fdtd.gpu.<name> <value>` (cli/main.c:233-290) stores as text, a number or
+ * a boolean.  These are the process-wide ones; the per-run ones (DFT bins,
+ * batching, per-example scenes) are read by the job runner above the ABI. */
+static char g_plan[96];
+static int g_plan_set = 0;  /* 0: RFSYN_FDTD_PLAN decides; 1: g_plan ("" = autotune) */
+static int g_tune = -1;     /* -1: RFSYN_FDTD_TUNE decides */
+
+const char *rfb_plan_override(void) { return g_plan_set ? (g_plan[0] ? g_plan : NULL) : getenv("RFSYN_FDTD_PLAN"); }
+
+int rfb_tune_enabled(void) {
+    if (g_tune >= 0) return g_tune;
+    const char *v = getenv("RFSYN_FDTD_TUNE");
+    return !(v && !strcmp(v, "0"));
+}
+
+static const char *setting_name(const char *key) {
+    if (!strncmp(key, "fdtd.", 5)) key += 5;
+    if (!strncmp(key, "gpu.", 4)) key += 4;
+    return key;
+}
+
+static int parse_flag(const char *v, int *out) {
+    if (!strcmp(v, "1") || !strcmp(v, "true")) return *out = 1, 0;
+    if (!strcmp(v, "0") || !strcmp(v, "false")) return *out = 0, 0;
+    return -1;
+}
+
+/* 4 to 6 comma-separated integers >= 0, nothing else */
+static int plan_text_ok(const char *v) {
+    int n = 0;
+    const char *p = v;
+    while (*p) {
+        if (*p < '0' || *p > '9') return 0;
+        while (*p >= '0' && *p <= '9') p++;
+        n++;
+        if (*p == ',') {
+            p++;
+            if (!*p) return 0;
+        } else if (*p) {
+            return 0;
+        }
+    }
+    return n >= 4 && n <= 6;
+}
+
+int fdtd_b200_apply_setting(const char *key, const char *value) {
+    if (!key || !value) {
+        rfb_set_error("NULL setting key or value");
+        return -1;
+    }
+    const char *k = setting_name(key);
+    int flag = 0;
+    if (!strcmp(value, "default")) {
+        /* back to the initial state: the environment variable decides */
+        if (!strcmp(k, "precision")) return g_prec = -1, 0;
+        if (!strcmp(k, "schedule")) return g_sched = -1, 0;
+        if (!strcmp(k, "plan")) return g_plan_set = 0, 0;
+        if (!strcmp(k, "tune")) return g_tune = -1, 0;
+        if (!strcmp(k, "trace")) return rfb_set_trace(-1), 0;
+    }
+    if (!strcmp(k, "precision")) {
+        if (!strcmp(value, "fp32") || !strcmp(value, "FP32")) return fdtd_b200_set_default_precision(FDTD_B200_FP32);
+        if (!strcmp(value, "fp64") || !strcmp(value, "FP64")) return fdtd_b200_set_default_precision(FDTD_B200_FP64);
+    } else if (!strcmp(k, "schedule")) {
+        if (!strcmp(value, "fused")) return fdtd_b200_set_default_schedule(FDTD_B200_SCHED_FUSED);
+        if (!strcmp(value, "split")) return fdtd_b200_set_default_schedule(FDTD_B200_SCHED_SPLIT);
+    } else if (!strcmp(k, "plan")) {
+        if (!strcmp(value, "auto")) {
+            g_plan[0] = '\0';
+            g_plan_set = 1;
+            return 0;
+        }
+        if (strlen(value) < sizeof g_plan && plan_text_ok(value)) {
+            strcpy(g_plan, value);
+            g_plan_set = 1;
+            return 0;
+        }
+    } else if (!strcmp(k, "tune")) {
+        if (parse_flag(value, &flag) == 0) return g_tune = flag, 0;
+    } else if (!strcmp(k, "trace")) {
+        if (parse_flag(value, &flag) == 0) return rfb_set_trace(flag), 0;
+    } else {
+        rfb_set_error("unknown setting \"%s\"", key);
+        return -1;
+    }
+    rfb_set_error("invalid value \"%s\" for setting \"%s\"", value, key);
+    return -1;
+}
+
+int fdtd_b200_get_setting(const char *key, char *buf, size_t len) {
+    if (!key || !buf || !len) {
+        rfb_set_error("NULL setting key or buffer");
+        return -1;
+    }
+    const char *k = setting_name(key);
+    const char *v;
+    if (!strcmp(k, "precision")) v = rfb_default_precision() == RFB_FP32 ? "fp32" : "fp64";
+    else if (!strcmp(k, "schedule")) v = rfb_default_schedule() == RFB_SCHED_SPLIT ? "split" : "fused";
+    else if (!strcmp(k, "plan")) v = rfb_plan_override() ? rfb_plan_override() : "auto";
+    else if (!strcmp(k, "tune")) v = rfb_tune_enabled() ? "true" : "false";
+    else if (!strcmp(k, "trace")) v = rfb_trace_enabled() ? "true" : "false";
+    else {
+        rfb_set_error("unknown setting \"%s\"", key);
+        return -1;
+    }
+    if (strlen(v) + 1 > len) {
+        rfb_set_error("buffer too short for setting \"%s\"", key);
+        return -1;
+    }
+    strcpy(buf, v);
+    return 0;
+}
+
 const char *fdtd_b200_last_error(void) { return rfb_last_error(); }
 unsigned long long fdtd_b200_launch_count(void) { return rfb_launch_count(); }
 unsigned long long fdtd_b200_cached_bytes(void) { return rfb_cached_bytes(); }

@@ -176,21 +176,7 @@ def c4(seed: int = 4, n_scenes: int = 512, precision: int = FP32, n_steps: int =
         rng = Pcg32(seed, sc)
         nx, ny, nz = (rng.randint(lo, hi + 1) for _ in range(3))
         dims = (nx, ny, nz)
-        boxes, spheres = [], []
-        room = min(dims) - 2 * (npml + 2)   # cells between the CPML margins
-        for _ in range(rng.randint(0, 7)):
-            eps, sig = rng.range(1.0, 10.0), rng.log_range(1e-4, 1.0)
-            if rng.next_u32() & 1:
-                r = rng.range(3.0, min(12.0, room / 2 - 1))
-                c = [rng.range(npml + r + 2, n - npml - r - 2) for n in dims]
-                spheres.append((c[0], c[1], c[2], r, eps, sig, None))
-            else:
-                b = []
-                for n in dims:
-                    side = rng.randint(4, min(17, room))
-                    a0 = rng.randint(npml + 2, n - npml - 2 - side + 1)
-                    b += [a0, a0 + side]
-                boxes.append((*b, eps, sig))
+        boxes, spheres = draw_scatterers(rng, dims, npml)
         m = npml + 3
 
         def pick():
@@ -204,6 +190,30 @@ def c4(seed: int = 4, n_scenes: int = 512, precision: int = FP32, n_steps: int =
                           waveform=WAVE_MOD_GAUSSIAN, p0=10e9, p1=4.0 * tau, p2=tau)],
             probes=probes, freqs=freqs, boxes=boxes, spheres=spheres))
     return out
+
+
+def draw_scatterers(rng: Pcg32, dims, npml: int) -> tuple[list, list]:
+    """0-6 scatterers clear of the CPML, each a sphere (radius U[3,12] cells)
+    or a box (sides U[4,16] cells) with eps_r U[1,10] and sigma log-U[1e-4,1]
+    S/m (radii and sides capped to fit the smallest axis), drawn from rng.
+    Returns (boxes, spheres) in the Workload's forms.  Needs
+    min(dims) >= 2 npml + 12."""
+    boxes, spheres = [], []
+    room = min(dims) - 2 * (npml + 2)   # cells between the CPML margins
+    for _ in range(rng.randint(0, 7)):
+        eps, sig = rng.range(1.0, 10.0), rng.log_range(1e-4, 1.0)
+        if rng.next_u32() & 1:
+            r = rng.range(3.0, min(12.0, room / 2 - 1))
+            c = [rng.range(npml + r + 2, n - npml - r - 2) for n in dims]
+            spheres.append((c[0], c[1], c[2], r, eps, sig, None))
+        else:
+            b = []
+            for n in dims:
+                side = rng.randint(4, min(17, room))
+                a0 = rng.randint(npml + 2, n - npml - 2 - side + 1)
+                b += [a0, a0 + side]
+            boxes.append((*b, eps, sig))
+    return boxes, spheres
 
 
 def scene_setup(w: Workload):
