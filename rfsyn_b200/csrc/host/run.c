@@ -280,7 +280,9 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
             rfb_set_error("a plane wave is not supported in a batch scene");
             goto fail;
         }
+        t_phase = rfb_now();
         if (rfb_tfsf_build(&g, mat, cfg->plane_wave, nt, pml ? (int)cfg->cpml.npml : 0, &tf) != 0) goto fail;
+        rfb_trace("create: plane wave", t_phase);
     }
     if (ns || tf.n_cells) {
         vals = malloc((ns ? ns : 1) * nt * sizeof(double));
@@ -369,6 +371,7 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
             tf_first[e] = tf.e_first[q];
             tf_count[e] = tf.e_count[q];
         }
+        rfb_trace("create: plane-wave targets", t_phase);
     }
 
     sim = calloc(1, sizeof(*sim));
