@@ -8,6 +8,9 @@
  * the step kernels, sources are injected by the interface-list kernel and
  * probes are gathered on the device; only the time series comes back. */
 #include <math.h>
+#include <pthread.h>
+#include <stdatomic.h>
+#include <unistd.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -708,6 +711,75 @@ signal_t *signal_copy(const signal_t *sig) {
 }
 
 /* ---- batches of independent scenes ------------------------------------------ */
+/* Member scenes are built by a few host threads: each scene's set-up
+ * callback, material maps, interface list and device buffers are its own,
+ * and the engine's shared state (memory cache, launch counter, fill-fraction
+ * scratch) is locked or atomic.  The error reported is the one of the
+ * lowest-numbered scene that failed, as a sequential loop would report:
+ * scenes are taken in increasing order, so every lower scene was tried. */
+typedef struct {
+    const fdtd_b200_config_t *configs;
+    const fdtd_material_setup_fn *setups;
+    void *const *contexts;
+    void *stream;
+    fdtd_b200_sim_t **sims;
+    size_t n;
+    atomic_size_t next;
+    atomic_int failed;
+    size_t fail_at;
+    char msg[480];
+    pthread_mutex_t mu;
+} member_job_t;
+
+static void *member_worker(void *arg) {
+    member_job_t *j = (member_job_t *)arg;
+    while (!atomic_load(&j->failed)) {
+        const size_t s = atomic_fetch_add(&j->next, 1);
+        if (s >= j->n) break;
+        fdtd_material_setup_fn fn = j->setups ? j->setups[s] : NULL;
+        void *ctx = j->contexts ? j->contexts[s] : NULL;
+        j->sims[s] = sim_create(&j->configs[s], fn, ctx, j->stream, 1);
+        if (!j->sims[s]) {
+            pthread_mutex_lock(&j->mu);
+            if (!atomic_load(&j->failed) || s < j->fail_at) {
+                j->fail_at = s;
+                snprintf(j->msg, sizeof j->msg, "batch scene %zu: %s", s, rfb_last_error());
+            }
+            atomic_store(&j->failed, 1);
+            pthread_mutex_unlock(&j->mu);
+        }
+    }
+    return NULL;
+}
+
+/* Threads for member creation: RFSYN_FDTD_CREATE_THREADS, else the online
+ * cores up to 16, never more than the scenes. */
+static size_t member_threads(size_t n) {
+    long t = 0;
+    const char *v = getenv("RFSYN_FDTD_CREATE_THREADS");
+    if (v && *v) t = strtol(v, NULL, 10);
+    if (t <= 0) {
+        t = sysconf(_SC_NPROCESSORS_ONLN);
+        if (t > 16) t = 16;
+    }
+    if (t < 1) t = 1;
+    return (size_t)t < n ? (size_t)t : n;
+}
+
+static int create_members(member_job_t *j) {
+    pthread_t th[64];
+    size_t nt = member_threads(j->n);
+    if (nt > 64) nt = 64;
+    size_t started = 0;
+    for (size_t q = 1; q < nt; q++) {
+        if (pthread_create(&th[q], NULL, member_worker, j) != 0) break;
+        started = q;
+    }
+    member_worker(j);  /* the calling thread works too */
+    for (size_t q = 1; q <= started; q++) pthread_join(th[q], NULL);
+    return atomic_load(&j->failed) ? -1 : 0;
+}
+
 struct fdtd_b200_batch {
     rfb_batch_t *b;
     size_t n;
@@ -746,18 +818,26 @@ fdtd_b200_batch_t *fdtd_b200_batch_create(size_t n_scenes, const fdtd_b200_confi
     }
     bt->n = n_scenes;
     const double t_members = rfb_now();
-    for (size_t s = 0; s < n_scenes; s++) {
-        fdtd_material_setup_fn fn = setups ? setups[s] : NULL;
-        void *ctx = contexts ? contexts[s] : NULL;
-        bt->sims[s] = sim_create(&configs[s], fn, ctx, stream, 1);
-        if (!bt->sims[s]) {
-            char msg[400];
-            snprintf(msg, sizeof msg, "batch scene %zu: %s", s, rfb_last_error());
-            rfb_set_error("%s", msg);
+    {
+        member_job_t job;
+        memset(&job, 0, sizeof job);
+        job.configs = configs;
+        job.setups = setups;
+        job.contexts = contexts;
+        job.stream = stream;
+        job.sims = bt->sims;
+        job.n = n_scenes;
+        atomic_init(&job.next, 0);
+        atomic_init(&job.failed, 0);
+        pthread_mutex_init(&job.mu, NULL);
+        const int rc = create_members(&job);
+        pthread_mutex_destroy(&job.mu);
+        for (size_t s = 0; s < n_scenes; s++) engs[s] = bt->sims[s] ? bt->sims[s]->eng : NULL;
+        made = n_scenes;  /* engines of the scenes that were made (NULL elsewhere) */
+        if (rc != 0) {
+            rfb_set_error("%s", job.msg);
             goto fail;
         }
-        engs[s] = bt->sims[s]->eng;
-        made = s + 1;
     }
     rfb_trace("batch: member scenes", t_members);
     bt->b = rfb_batch_create(engs, n_scenes, stream, own);

@@ -112,3 +112,28 @@ def test_batch_rejects_unsupported():
     with pytest.raises(RuntimeError, match="past the configured step count"):
         b.advance(1)
     b.close()
+
+
+def test_members_built_on_threads_match_one_thread(monkeypatch):
+    ws = _small_batch(rb.FP32, n=8, steps=40)
+
+    def run():
+        setups = [scenes.scene_setup(w) for w in ws]
+        b = rb.Batch([scenes.run_config(w) for w in ws], [s.ptr if s else None for s in setups])
+        try:
+            b.advance(40)
+            return [b.probes(q) for q in range(len(ws))]
+        finally:
+            b.close()
+
+    monkeypatch.setenv("RFSYN_FDTD_CREATE_THREADS", "1")
+    one = run()
+    monkeypatch.setenv("RFSYN_FDTD_CREATE_THREADS", "8")
+    many = run()
+    assert all(np.array_equal(x, y) for x, y in zip(one, many))
+    # the error names the lowest-numbered failing scene, as one thread would
+    bad = copy.deepcopy(ws)
+    for q in (5, 2, 6):
+        bad[q].sources[0]["i"] = bad[q].nx + 3
+    with pytest.raises(RuntimeError, match="batch scene 2: source 0 outside the grid"):
+        rb.Batch([scenes.run_config(w) for w in bad])
