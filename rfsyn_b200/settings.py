@@ -72,7 +72,10 @@ def _no_constant(name):
 def load(path: str | os.PathLike) -> dict:
     """config.json as a dict (config_load, cli/config.c:24-60); raises
     ValueError where rfsyn's parser refuses the text (NaN and Infinity
-    included)."""
+    included).  One difference, loud rather than silent: number literals
+    that JSON forbids but cJSON hands to strtod (leading zeros, a trailing
+    point, "-.5") are read by rfsyn and refused here.  Files written by
+    rfsyn's `config set` (cJSON_Print) never hold them."""
     with open(path, "rb") as f:
         return json.loads(f.read().decode("utf-8"), object_pairs_hook=_first_wins, parse_constant=_no_constant)
 
@@ -94,10 +97,19 @@ def get(cfg, section: str, key: str):
     return v if isinstance(v, str) else None
 
 
+def _as_double(v) -> float:
+    """A JSON number as cJSON's strtod reads it (integer literals beyond the
+    double range become +-inf, as Python's float() would refuse)."""
+    try:
+        return float(v)
+    except OverflowError:
+        return math.inf if v > 0 else -math.inf
+
+
 def get_double(cfg, section: str, key: str, default: float) -> float:
     """config_get_double: a JSON number, else the default."""
     v = _item(cfg, section, key)
-    return float(v) if _is_number(v) else default
+    return _as_double(v) if _is_number(v) else default
 
 
 def get_long(cfg, section: str, key: str, default: int) -> int:
@@ -106,10 +118,7 @@ def get_long(cfg, section: str, key: str, default: int) -> int:
     v = _item(cfg, section, key)
     if not _is_number(v):
         return default
-    try:
-        d = float(v)
-    except OverflowError:
-        return default
+    d = _as_double(v)
     if not math.isfinite(d) or d != math.floor(d) or d < float(LONG_MIN) or d > float(LONG_MAX):
         return default
     if d == 2.0 ** 63:

@@ -85,6 +85,8 @@ RAW = [
     '{"fdtd": {"nx": 30, "nx": 40, "t0": 1.5, "t0": 9}, "fdtd": {"ny": 99}}',
     # integers beyond double precision, exponents, negative zero
     '{"fdtd": {"nx": 9007199254740993, "ny": 1E2, "nz": -0, "dx": 2.5e-3, "tau": -0.0}}',
+    # literals beyond the double range
+    '{"fdtd": {"dx": 1' + '0' * 400 + ', "t0": -1' + '0' * 400 + ', "tau": 1e400, "nx": 1' + '0' * 30 + '}}',
 ]
 KEYS = [("fdtd", k) for k in ("nx", "ny", "nz", "dx", "courant", "n_steps", "npml", "src_i", "src_j", "src_k",
                               "probe_i", "probe_j", "probe_k", "t0", "tau", "enabled", "gpu.precision")] + \
@@ -125,6 +127,20 @@ def test_getters_equal_rfsyn(tmp_path):
                 assert settings.get(mine, sec, key) == (g.decode() if g is not None else None), (p, key)
         finally:
             ref.config_destroy(rc)
+
+
+@needs_ref
+def test_lenient_number_literals_are_refused_loudly(tmp_path):
+    # cJSON reads these through strtod; strict JSON (and this module) refuses
+    ref = _ref()
+    for q, lit in enumerate(["007", "5.", "-.5"]):
+        p = tmp_path / f"lenient{q}.json"
+        p.write_text('{"fdtd": {"nx": %s}}' % lit)
+        rc = ref.config_load(str(p).encode())
+        assert rc
+        ref.config_destroy(rc)
+        with pytest.raises(ValueError):
+            settings.load(p)
 
 
 @needs_ref
