@@ -83,8 +83,21 @@ void mc_release_device(MemCache &c, int dev) {
 }
 }  // namespace
 
+// Host-side fault injection (no device fault): RFSYN_FDTD_FAIL_ALLOC=n makes
+// the n-th device allocation of each single-scene engine creation report
+// cudaErrorMemoryAllocation without calling the driver, so every error path
+// of creation can be driven from a test.  Armed at the start of a creation,
+// disarmed at its end; unset or 0: off.
+static std::atomic<long long> g_fail_countdown{0};
+
+static void arm_alloc_failure(bool on) {
+    const char *v = on ? getenv("RFSYN_FDTD_FAIL_ALLOC") : nullptr;
+    g_fail_countdown.store(v ? atoll(v) : 0);
+}
+
 static cudaError_t dmalloc_raw(void **p, size_t n) {
     *p = nullptr;
+    if (g_fail_countdown.load() > 0 && g_fail_countdown.fetch_sub(1) == 1) return cudaErrorMemoryAllocation;
     if (n < MC_MIN) return cudaMalloc(p, n);
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
@@ -1424,8 +1437,11 @@ extern "C" rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision
                                            const rfb_cpml_desc_t *cpml, const rfb_scene_image_t *scene,
                                            size_t n_sources, const rfb_source_desc_t *sources, size_t n_probes,
                                            const rfb_probe_desc_t *probes, size_t n_steps, void *stream) {
-    return engine_create(geom, precision, schedule, cpml, scene, n_sources, sources, n_probes, probes, n_steps, stream,
-                         0);
+    arm_alloc_failure(true);
+    rfb_engine_t *e = engine_create(geom, precision, schedule, cpml, scene, n_sources, sources, n_probes, probes,
+                                    n_steps, stream, 0);
+    arm_alloc_failure(false);
+    return e;
 }
 
 extern "C" rfb_engine_t *rfb_engine_create_member(const rfb_geom_t *geom, int precision,
