@@ -299,3 +299,16 @@ def test_examples_batched_equal_single_and_rfsyn(restore_settings, tmp_path):
     paths = settings.write_examples(seeded, [2], tmp_path)
     assert Path(paths[0]).name == "example_000002.iq"
     assert np.array_equal(np.fromfile(paths[0], dtype=np.complex64), single[2])
+
+
+def test_setting_text_and_disabled_stage():
+    assert settings.setting_text(True) == "true" and settings.setting_text(False) == "false"
+    assert settings.setting_text(0) == "0" and settings.setting_text(4.0) == "4"
+    assert settings.setting_text(2.5) == "2.5" and settings.setting_text("8,4,128,32,2") == "8,4,128,32,2"
+    with pytest.raises(ValueError):
+        settings.setting_text(None)
+    with pytest.raises(ValueError, match="fdtd.enabled"):
+        settings.run_examples({"fdtd": {"enabled": False}}, [0])
+    # the AWGN stage of example i: (float) snr, seed as uint64, stream i
+    assert settings.awgn_of({"awgn": {"snr_db": 7.3, "seed": -1}}, 5) == (float(np.float32(7.3)), (1 << 64) - 1, 5)
+    assert settings.awgn_of({"awgn": {"enabled": False}}, 0) is None
