@@ -3,7 +3,7 @@
 Workload: the 256^3 FP32 scene with 24 subpixel-smoothed dielectric spheres,
 3 Debye spheres, 12-cell CPML, 16 probes x 256 DFT bins and 4000 steps
 (rfsyn_b200.scenes.c2).  A bench "step" is one full simulation of that scene
-(reset + 4000 time steps + probe DFT on the device).  Metric:
+(reset + 4000 time steps; the probe series stay on the device).  Metric:
 Mcell-updates/s = nx*ny*nz*n_steps*K / seconds, whole job.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
@@ -21,7 +21,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from pathlib import Path
 
@@ -136,49 +135,120 @@ def algorithmic_bytes_per_sweep(info, esz: int) -> float:
 # ---------------------------------------------------------------------------
 # CPU reference arm
 # ---------------------------------------------------------------------------
-def cpu_reference(workload, steps: int, threads: int) -> dict:
-    """rfsyn's own CPU loop (oracle/_ref) on `threads` independent copies of
-    the scene, `steps` time steps each; throughput over the slowest copy."""
+COPY_BYTES_PER_CELL = 170  # rfsyn's resident copy of a scene: 6 fields, 12 psi, materials, driver state
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def mem_available() -> int:
+    try:
+        for line in Path("/proc/meminfo").read_text().splitlines():
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except (OSError, ValueError):
+        pass
+    return 0
+
+
+def cpu_copies(workload) -> int:
+    """Independent copies run side by side: one per host core, as many as
+    60 % of the available memory holds."""
+    cores = os.cpu_count() or 1
+    per = max(1, (workload.nx + 1) * (workload.ny + 1) * (workload.nz + 1) * COPY_BYTES_PER_CELL)
+    avail = mem_available()
+    return max(1, min(cores, int(0.6 * avail) // per if avail else cores))
+
+
+def _cpu_worker(workload, steps, samples, warm, barrier, conn) -> None:
+    """One process: builds rfsyn's copy of the scene, runs `warm` untimed
+    steps (first touch of the calloc'd fields and psi), then `samples` timed
+    samples of `steps` steps, each started together with the other copies."""
     import ctypes as C
 
     import oracle
     from tests.cases import workload_to_scene
 
-    kind = "reference" if oracle.ref_available() else "port"
-    scene = workload_to_scene(workload)
-    scene.n_steps = steps
-    scene.probes, scene.freqs = [], []
-    cs = scene.to_c()
-    if kind == "reference":
+    try:
+        scene = workload_to_scene(workload)
+        scene.probes, scene.freqs = [], []
+        cs = scene.to_c()
         lib = C.CDLL(str(oracle.REF_LIB))
-        fn = lib.scn_time
-        fn.restype = C.c_int
-        fn.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double)]
-        results = [None] * threads
+        lib.scn_bench_create.restype = C.c_void_p
+        lib.scn_bench_create.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.scn_bench_steps.restype = C.c_int
+        lib.scn_bench_steps.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_double)]
+        lib.scn_bench_destroy.argtypes = [C.c_void_p]
+        setup = C.c_double(0)
+        h = lib.scn_bench_create(C.byref(cs), C.byref(setup))
+        t = C.c_double(0)
+        ok = bool(h) and lib.scn_bench_steps(h, warm, C.byref(t)) == 0
+        times = []
+        for _ in range(samples):
+            barrier.wait()
+            ok = ok and lib.scn_bench_steps(h, steps, C.byref(t)) == 0
+            times.append(t.value)
+        barrier.wait()
+        lib.scn_bench_destroy(h)
+        conn.send({"ok": ok, "setup_s": setup.value, "times": times})
+    except Exception as exc:  # report, and keep the barrier going for the others
+        barrier.abort()
+        conn.send({"ok": False, "error": repr(exc)})
 
-        def work(q):
-            a, b = C.c_double(0), C.c_double(0)
-            rc = fn(C.byref(cs), steps, C.byref(a), C.byref(b))
-            results[q] = (rc, a.value, b.value)
 
-        ts = [threading.Thread(target=work, args=(q,)) for q in range(threads)]
-        for t in ts:
-            t.start()
-        for t in ts:
-            t.join()
-        if any(r is None or r[0] != 0 for r in results):
-            raise RuntimeError("reference CPU run failed")
-        loop = max(r[2] for r in results)
-    else:
-        threads = 1
+def cpu_reference(workload, steps: int, samples: int, copies: int | None = None, warm: int = 1) -> dict:
+    """rfsyn's own CPU loop (oracle/_ref) on `copies` independent processes,
+    each with its own copy of the scene: per sample every copy runs `steps`
+    time steps after a common barrier; the sample's rate is all copies'
+    cell-updates over the slowest copy's time.  Returns the median rate over
+    the samples, the per-copy rate and the host it ran on.  Without the
+    compiled reference, the oracle port times one copy."""
+    import multiprocessing as mp
+
+    import oracle
+
+    model, cores = cpu_model(), os.cpu_count() or 1
+    if not oracle.ref_available():
+        from tests.cases import workload_to_scene
+
+        scene = workload_to_scene(workload)
+        scene.n_steps, scene.probes, scene.freqs = steps, [], []
         t0 = time.perf_counter()
         oracle.run_oracle(scene)
         loop = time.perf_counter() - t0
-    value = threads * workload.cells * steps / loop / 1e6
-    return {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": f"{threads} independent copies of the {workload.nx}^3 scene x {steps} of its "
-                      f"{workload.n_steps} steps (FP64; Debye spheres at their static permittivity)",
-            "loop_s": loop}
+        v = workload.cells * steps / loop / 1e6
+        return {"value": v, "unit": METRIC, "cores": 1, "kind": "port", "per_copy": v, "samples": [v],
+                "cpu_model": model, "nproc": cores,
+                "sample": f"1 copy of the {workload.nx}^3 scene x {steps} of its {workload.n_steps} steps (FP64)"}
+    copies = copies or cpu_copies(workload)
+    ctx = mp.get_context("spawn")  # never fork a process that holds a CUDA context
+    barrier = ctx.Barrier(copies, timeout=1800)
+    pipes = [ctx.Pipe(duplex=False) for _ in range(copies)]
+    procs = [ctx.Process(target=_cpu_worker, args=(workload, steps, samples, warm, barrier, w), daemon=True)
+             for (_, w) in pipes]
+    for pr in procs:
+        pr.start()
+    res = [r.recv() for (r, _) in pipes]
+    for pr in procs:
+        pr.join()
+    if not all(r.get("ok") for r in res):
+        raise RuntimeError(f"reference CPU run failed: {[r.get('error') for r in res if not r.get('ok')]}")
+    rates = [copies * workload.cells * steps / max(r["times"][s] for r in res) / 1e6 for s in range(samples)]
+    value = statistics.median(rates)
+    return {"value": value, "unit": METRIC, "cores": copies, "kind": "reference", "per_copy": value / copies,
+            "samples": rates, "cpu_model": model, "nproc": cores,
+            "setup_s": max(r["setup_s"] for r in res),
+            "sample": (f"{copies} independent processes (one per core, of {cores}), each its own copy of the "
+                       f"{workload.nx}^3 scene: {warm} untimed warm-up step, then {samples} samples of {steps} of "
+                       f"its {workload.n_steps} steps started together (FP64; Debye spheres at their static "
+                       f"permittivity; median sample)")}
 
 
 def run_reference(args) -> None:
@@ -188,16 +258,12 @@ def run_reference(args) -> None:
     from rfsyn_b200 import scenes
 
     w = scenes.c2()
-    threads = max(1, min(os.cpu_count() or 1, 16))
-    res = []
-    for s in range(args.warmup + args.steps):
-        r = cpu_reference(w, args.ref_sample_steps, threads)
-        if s >= args.warmup:
-            res.append(r)
-    value = statistics.median(r["value"] for r in res)
-    cb = dict(res[-1])
-    cb["value"] = value
-    cb.pop("loop_s", None)
+    # one resident copy per process: the warm-up samples are the bench's
+    # warm-up steps, the timed samples its steps
+    cb = cpu_reference(w, args.ref_sample_steps, args.warmup + args.steps)
+    rates = cb.pop("samples")[args.warmup:]
+    value = statistics.median(rates)
+    cb["value"], cb["per_copy"] = value, value / cb["cores"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -213,6 +279,52 @@ def run_reference(args) -> None:
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def traced_call(fn):
+    """Runs fn() with the library's phase trace on and its stderr lines
+    captured; returns (fn's result, {phase: ms})."""
+    import rfsyn_b200 as rb
+
+    lib = rb.load()
+    sys.stderr.flush()
+    saved = os.dup(2)
+    with tempfile.TemporaryFile(mode="w+b") as tmp:
+        os.dup2(tmp.fileno(), 2)
+        try:
+            lib.fdtd_b200_apply_setting(b"trace", b"true")
+            out = fn()
+        finally:
+            lib.fdtd_b200_apply_setting(b"trace", b"default")
+            os.dup2(saved, 2)
+            os.close(saved)
+        tmp.seek(0)
+        text = tmp.read().decode(errors="replace")
+    phases = {}
+    for line in text.splitlines():
+        if line.startswith("rfsyn_b200 trace: ") and line.endswith(" ms"):
+            name, ms = line[len("rfsyn_b200 trace: "):-3].rsplit(" ", 1)
+            phases[name] = phases.get(name, 0.0) + float(ms)
+    return out, phases
+
+
+def fp64_reference_run(w, setup) -> dict:
+    """The workload in FP64 on the device: one warm-up run, one timed run
+    (CUDA events); returns its spectra and the loop's milliseconds."""
+    import dataclasses
+
+    import rfsyn_b200 as rb
+    from rfsyn_b200 import scenes
+
+    w64 = dataclasses.replace(w, precision=rb.FP64)
+    sim = rb.Sim(scenes.run_config(w64), setup.ptr if setup else None, None)
+    try:
+        sim.advance(w64.n_steps)
+        sim.reset()
+        ms = sim.advance_timed(w64.n_steps)
+        return {"dft": sim.dft(), "ms": ms}
+    finally:
+        sim.close()
+
+
 def run_b200(args) -> None:
     import torch
     import rfsyn_b200 as rb
@@ -260,8 +372,6 @@ def run_b200(args) -> None:
 
     # results of the last timed step: probes and spectra (correctness guard)
     dft = sim.dft()
-    import numpy as np
-
     finite = bool(np.all(np.isfinite(dft)))
 
     # live per-kernel timing of the dominant sweep kernel (same scene)
@@ -287,16 +397,27 @@ def run_b200(args) -> None:
         d2h = r["td"].nbytes + r["dft"].nbytes
     h2d = info.h2d_bytes
     e2e_ms = ranks.max_over(rk, sum(e2e_ms) / len(e2e_ms))  # mean of the calls (host set-up times vary)
+    # where one end-to-end call spends its time (host phase trace of one more call)
+    _, phases = traced_call(lambda: rb.run(rc, setup.ptr if setup else None, None))
     e2e_value = ranks.weak_rate(w.cells * w.n_steps, e2e_ms, rk) / 1e6
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
         try:
-            cb = cpu_reference(w, args.ref_sample_steps, max(1, min(os.cpu_count() or 1, 16)))
-            cb.pop("loop_s", None)
+            cb = cpu_reference(w, args.ref_sample_steps, 3)
+            cb.pop("samples", None)
             cpu = cb
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "unavailable", "sample": str(exc)}
+
+    # accuracy of the measured FP32 run: the same scene in FP64 on the GPU
+    # (bit-exact with rfsyn's double-precision loop wherever that runs),
+    # timed as well for the like-for-like precision figure
+    fp64 = fp64_reference_run(w, setup)
+    err = np.linalg.norm(dft - fp64["dft"], axis=1) / np.linalg.norm(fp64["dft"], axis=1)
+    parity = {"spec_l2_max": float(err.max()), "spec_l2_median": float(np.median(err)), "bound": 1e-4,
+              "probes": int(err.size), "bins": int(dft.shape[1]),
+              "vs": "fp64-gpu (the FP64 device loop: bit-exact with rfsyn's FP64 loop and the oracle at their sizes)"}
 
     ranks.finish(rk)
     if rank != 0:
@@ -323,10 +444,14 @@ def run_b200(args) -> None:
                      "other_kernels_ms_per_step": other_ms / 200},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": e2e_ms, "calls_averaged": max(1, args.e2e_steps)},
+                "ms_per_step": e2e_ms, "calls_averaged": max(1, args.e2e_steps),
+                "phases_ms": {k: round(v, 3) for k, v in phases.items()}},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "finite": finite,
+        "parity": parity,
+        "fp64": {"value": w.cells * w.n_steps / (fp64["ms"] / 1e3) / 1e6, "unit": METRIC, "ms_per_step": fp64["ms"],
+                 "note": "the same scene and step loop in FP64 on the device, one run after a warm-up run"},
     }
     print(json.dumps(line), flush=True)
 
@@ -534,6 +659,50 @@ def run_surrogate(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Profiling runs (--profile-steps N): a few steps launched kernel by kernel
+# ---------------------------------------------------------------------------
+def run_profile(args) -> None:
+    """Creates the workload's scene (or batch) on cuda:0, then launches
+    `--profile-steps` time steps kernel by kernel with CUDA events around the
+    sweep and the rest, for profilers (ncu); prints the plan and the times.
+    --n rescales the C2 recipe to an n^3 grid for captures that must stay
+    small."""
+    import rfsyn_b200 as rb
+    from rfsyn_b200 import scenes
+
+    steps = max(1, args.profile_steps)
+    if args.workload == "c4":
+        ws = scenes.c4(seed=4, n_scenes=args.scenes)
+        setups = [scenes.scene_setup(x) for x in ws]
+        b = rb.Batch([scenes.run_config(x) for x in ws], [st.ptr if st else None for st in setups])
+        bi = b.info()
+        print(f"batch plan: rows {bi.tile_j}, ring {bi.ring_depth}, scenes {bi.scenes}, cells {bi.cells}", flush=True)
+        sweep_ms, other_ms = b.time_kernels(steps)
+        b.close()
+        print(f"c4 x{args.scenes}: {steps} steps, sweep {sweep_ms / steps:.3f} ms/step, other {other_ms / steps:.3f} ms/step")
+        return
+    if args.workload == "c3":
+        w = scenes.c3()
+    elif args.workload == "c1":
+        w = scenes.c1(precision=rb.FP32)
+    else:
+        w = scenes.c2()
+        if args.n:
+            w = scenes.scaled(w, args.n, max(steps, 8))
+    w.schedule = rb.FUSED if args.schedule == "fused" else rb.SPLIT
+    w.n_steps = steps
+    setup = scenes.scene_setup(w)
+    sim = rb.Sim(scenes.run_config(w), setup.ptr if setup else None, None)
+    info = sim.info()
+    print(f"plan: mode {info.tma}, rows {info.tile_j}, ring {info.ring_depth}, segment {info.seg_len}, "
+          f"interior items {info.interior_items}, edge items {info.edge_items}, list cells {info.list_cells}",
+          flush=True)
+    sweep_ms, other_ms = sim.time_kernels(steps)
+    sim.close()
+    print(f"{w.name}: {steps} steps, sweep {sweep_ms / steps:.3f} ms/step, other {other_ms / steps:.3f} ms/step")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -543,14 +712,21 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=3, help="end-to-end calls averaged for e2e")
     ap.add_argument("--ref-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--train-scenes", type=int, default=5000, help="c5: training scenes (4 samples each)")
     ap.add_argument("--test-scenes", type=int, default=500, help="c5: held-out scenes")
     ap.add_argument("--train-steps", type=int, default=20000, help="c5: Adam steps per member")
     ap.add_argument("--threshold", type=float, default=0.02, help="c5: ensemble spread that triggers FDTD")
     ap.add_argument("--scenes", type=int, default=512, help="c4: scenes per batch")
     ap.add_argument("--plain-sample", type=int, default=16, help="c4: scenes timed one at a time")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling run: create the scene, launch this many steps kernel by kernel, print times")
+    ap.add_argument("--n", type=int, default=0, help="profiling run, c2: rescale the recipe to an n^3 grid")
+    ap.add_argument("--schedule", default="fused", choices=["fused", "split"], help="profiling run: schedule")
     args = ap.parse_args()
+    if args.profile_steps:
+        run_profile(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

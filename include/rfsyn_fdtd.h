@@ -183,6 +183,45 @@ int materials_clear_component_tensor(materials_t *mat, const fdtd_grid_t *g, fie
 int materials_get_tensor(const materials_t *mat, const fdtd_grid_t *g, field_component_t component,
                          size_t i, size_t j, size_t k, material_tensor_t *out);
 
+/* ---- 2-D subpixel helpers: engine/fdtd/subpixel_te.h:4-71 --------------------
+ * Set-up helpers rfsyn's tilted-interface validator calls directly
+ * (engine/fdtd/validate_materials_tilted.c:163-241): the share of a sample's
+ * dx x dy cell covered by a rotated rectangle, the covered share of an edge
+ * segment, and arithmetic, harmonic and normal-aligned 2x2 tensor mixes of
+ * two relative permittivities.  Same status codes, argument checks and
+ * output conventions (outputs untouched on failure). */
+typedef enum {
+    SUBPIXEL_TE_OK = 0,
+    SUBPIXEL_TE_INVALID_ARGUMENT = -1,
+    SUBPIXEL_TE_NUMERIC_ERROR = -2
+} subpixel_te_status_t;
+
+typedef struct {
+    double center_x, center_y;
+    double size_u, size_v;   /* full side lengths along the rotated axes */
+    double angle_rad;        /* rotation of the u axis from x */
+} subpixel_te_rectangle_t;
+
+/* subpixel_te.h:18-25 */
+int subpixel_te_rectangle_fraction(const subpixel_te_rectangle_t *rectangle, double sample_x, double sample_y,
+                                   double dx, double dy, double *fraction_out);
+/* subpixel_te.h:27-34: edge from the sample along +x (axis 1) or +y (2) */
+int subpixel_te_rectangle_edge_fraction(const subpixel_te_rectangle_t *rectangle, double sample_x, double sample_y,
+                                        int edge_axis, double length, double *fraction_out);
+/* subpixel_te.h:37-42: 1 / ((1-f)/eps_bg + f/eps_in) */
+int subpixel_te_mix_epsilon_harmonic(double fraction, double eps_background, double eps_inside,
+                                     double *epsilon_r_out);
+/* subpixel_te.h:44-49: (1-f) eps_bg + f eps_in */
+int subpixel_te_mix_epsilon(double fraction, double eps_background, double eps_inside, double *epsilon_r_out);
+/* subpixel_te.h:51-61 */
+int subpixel_te_rectangle_epsilon(const subpixel_te_rectangle_t *rectangle, double sample_x, double sample_y,
+                                  double dx, double dy, double eps_background, double eps_inside,
+                                  double *fraction_out, double *epsilon_r_out);
+/* subpixel_te.h:63-71: inverse-permittivity tensor harmonic along the normal
+ * at angle normal_rad, 1/arithmetic along the interface */
+int subpixel_te_mix_epsilon_tensor(double fraction, double eps_background, double eps_inside, double normal_rad,
+                                   double *minv_xx, double *minv_xy, double *minv_yy);
+
 /* ---- sources: engine/fdtd/source.h:8-35 --------------------------------- */
 typedef enum {
     SRC_SOFT,

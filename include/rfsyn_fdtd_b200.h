@@ -385,6 +385,24 @@ typedef struct {
 int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, const fdtd_b200_sphere_t *spheres,
                                     size_t n_spheres, int smoothing);
 
+/* ---- three-dimensional subpixel smoothing -------------------------------------
+ * rfsyn's tensor mix (subpixel_te_mix_epsilon_tensor, engine/fdtd/
+ * subpixel_te.c:106-132) is two-dimensional: an interface normal in the
+ * (x, y) plane and isotropic media.  fdtd_b200_subpixel_tensor3 gives the
+ * smoothed relative inverse permittivity M (9 values, row-major) of a cell of
+ * which a share `fraction` holds eps_inside behind an interface of normal
+ * `normal` (any length > 0), the rest eps_background; both permittivities are
+ * symmetric positive-definite 3x3 matrices (row-major), so anisotropic media
+ * are allowed.  It averages Kottke, Farjadpour and Johnson's tau transform of
+ * eps in the frame of the normal (Phys. Rev. E 77, 036611, 2008), which for
+ * two isotropic media is M = <1/eps> n n^T + (1/<eps>) (I - n n^T), rfsyn's
+ * rule in three dimensions: with n in the (x, y) plane the (x, y) block of M
+ * is rfsyn's (m_xx, m_xy, m_yy).  Returns SUBPIXEL_TE_OK, or
+ * SUBPIXEL_TE_INVALID_ARGUMENT (NULL, fraction outside [0, 1], zero normal, a
+ * permittivity that is not symmetric positive definite). */
+int fdtd_b200_subpixel_tensor3(double fraction, const double eps_background[9], const double eps_inside[9],
+                               const double normal[3], double minv_out[9]);
+
 /* ---- heightmap world -----------------------------------------------------------
  * rfsyn's terrain description (engine/world/world.h:10-17, world.c:49-135):
  * column (i, j) is solid material column_materials[i ny + j] up to height
@@ -427,11 +445,16 @@ int fdtd_b200_materials_apply_heightmap(materials_t *mat, const fdtd_grid_t *g, 
  * 3*ni*nj*nk doubles.  Nothing is allocated: the device staging is a fixed
  * array of 2^20 samples per output (16 MiB in all) that the library keeps on
  * every GPU that loads it until the process exits; a box of more than 2^20
- * samples is rejected with -1.  The first call on a device looks the staging
- * array up (once per device), so make that first call before any stream
- * capture.  Every call shares the one array and runs on the default stream:
- * calls that overlap on the GPU (from several host threads) race, so
- * serialise them. */
+ * samples is rejected with -1.  The first call on a device sets that device
+ * up (once): it looks the staging array up, which may load the part of the
+ * library that holds it and so commit its 16 MiB at that moment, and it
+ * creates the non-blocking stream the calls run on.  Make that first call at
+ * start-up: before any stream capture, and before another framework's pool
+ * takes the device's memory.  Later calls launch on that stream and copy back
+ * with asynchronous copies on it, so they never wait on the legacy default
+ * stream or on a stream another thread is capturing.  Every call shares the
+ * one array: calls that overlap on the GPU (from several host threads) race,
+ * so serialise them. */
 int fdtd_b200_sphere_fractions_noalloc(const double centre[3], double radius, int i0, int j0, int k0,
                                        int ni, int nj, int nk, double *f, double *n2);
 

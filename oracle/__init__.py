@@ -15,6 +15,7 @@ product's device time loop.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -22,6 +23,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
+# rfsyn's source tree, read (never written) only to compile rfsyn and its
+# validators for the checker; the Makefile takes the same directory as REF
+REFERENCE = Path(os.environ.get("RFSYN_REFERENCE_DIR", "/root/reference"))
 ORACLE_LIB = HERE / "lib" / "liboracle.so"
 DRIVER_LIB = HERE / "lib" / "libscene_driver_b200.so"
 REF_LIB = HERE / "_ref" / "librfsyn_ref.so"
@@ -189,14 +193,14 @@ class Scene:
 def build(ref: bool = True) -> None:
     """Builds liboracle.so (and rfsyn's own sources into _ref when present)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if ref and Path("/root/reference/engine/fdtd/grid.c").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    if ref and (REFERENCE / "engine/fdtd/grid.c").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE}", "ref"], check=True)
 
 
 def build_driver() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "driver"], check=True)
-    if Path("/root/reference/engine/fdtd/grid.c").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "validators"], check=True)
+    if (REFERENCE / "engine/fdtd/grid.c").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE}", "validators"], check=True)
 
 
 _libs: dict[str, C.CDLL] = {}

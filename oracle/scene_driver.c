@@ -344,53 +344,76 @@ static double now_s(void) {
     return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
 
-/* Builds the scene, then times `steps` steps of the loop (H, sources, E)
- * without probes: *setup_s and *loop_s are wall-clock seconds. */
-int scn_time(const scn_scene_t *s, size_t steps, double *setup_s, double *loop_s) {
-    int rc = -1;
-    double t0 = now_s();
-    fdtd_grid_t *g = fdtd_grid_create(s->nx, s->ny, s->nz, s->dx, s->courant);
-    cpml_t *p = NULL;
-    materials_t *m = NULL;
+/* A resident copy of the scene for timing rfsyn's loop (H, sources, E,
+ * without probes): scn_bench_create builds it (grid, CPML, materials and the
+ * first source) and returns the build's wall-clock seconds in *setup_s;
+ * scn_bench_steps advances `steps` more steps and returns their wall-clock
+ * seconds in *loop_s.  rfsyn allocates its fields and the twelve full-grid
+ * psi arrays with calloc (engine/fdtd/grid.c, engine/fdtd/cpml.c:126-138),
+ * so the first step over them pays the page faults of first touch: callers
+ * run untimed warm-up steps before the timed ones. */
+typedef struct {
+    const scn_scene_t *s;
+    fdtd_grid_t *g;
+    cpml_t *p;
+    materials_t *m;
     source_t src;
     source_modulated_gaussian_params_t mg;
     source_gaussian_deriv_params_t gd;
-    if (!g) return -1;
-    if (fdtd_grid_set_periodic(g, s->periodic) != 0) goto out;
+    size_t n;
+} scn_bench_t;
+
+void scn_bench_destroy(scn_bench_t *b) {
+    if (!b) return;
+    materials_destroy(b->m);
+    cpml_destroy(b->p);
+    fdtd_grid_destroy(b->g);
+    free(b);
+}
+
+scn_bench_t *scn_bench_create(const scn_scene_t *s, double *setup_s) {
+    double t0 = now_s();
+    scn_bench_t *b = calloc(1, sizeof *b);
+    if (!b) return NULL;
+    b->s = s;
+    b->g = fdtd_grid_create(s->nx, s->ny, s->nz, s->dx, s->courant);
+    if (!b->g || fdtd_grid_set_periodic(b->g, s->periodic) != 0) goto fail;
     if (s->npml) {
         cpml_params_t cp = {s->npml, s->m, s->ma, s->kappa_max, s->alpha_max, s->r0};
-        p = cpml_create(g, cp);
-        if (!p) goto out;
+        b->p = cpml_create(b->g, cp);
+        if (!b->p) goto fail;
     }
-    m = materials_create(g);
-    if (!m || scn_setup(g, m, (void *)s) != 0) goto out;
+    b->m = materials_create(b->g);
+    if (!b->m || scn_setup(b->g, b->m, (void *)s) != 0) goto fail;
     if (s->n_sources) {
         const scn_source_t *d = &s->sources[0];
         if (d->waveform == 2) {
-            mg.freq_hz = d->p0; mg.t0 = d->p1; mg.tau = d->p2;
-            src = source_make_point(d->i, d->j, d->k, comp_of(d->comp), SRC_SOFT, d->amplitude,
-                                    source_waveform_modulated_gaussian, &mg);
+            b->mg.freq_hz = d->p0; b->mg.t0 = d->p1; b->mg.tau = d->p2;
+            b->src = source_make_point(d->i, d->j, d->k, comp_of(d->comp), SRC_SOFT, d->amplitude,
+                                       source_waveform_modulated_gaussian, &b->mg);
         } else {
-            gd.t0 = d->p0; gd.tau = d->p1;
-            src = source_make_point(d->i, d->j, d->k, comp_of(d->comp), SRC_SOFT, d->amplitude,
-                                    source_waveform_gaussian_derivative, &gd);
+            b->gd.t0 = d->p0; b->gd.tau = d->p1;
+            b->src = source_make_point(d->i, d->j, d->k, comp_of(d->comp), SRC_SOFT, d->amplitude,
+                                       source_waveform_gaussian_derivative, &b->gd);
         }
     }
-    double t1 = now_s();
-    for (size_t n = 0; n < steps; n++) {
-        if (p) fdtd_update_h_cpml(g, p);
-        else fdtd_update_h(g);
-        if (s->n_sources) source_apply(&src, g, (double)n * g->dt);
-        if (p) fdtd_update_e_cpml_materials(g, p, m);
-        else fdtd_update_e_materials(g, m);
+    if (setup_s) *setup_s = now_s() - t0;
+    return b;
+fail:
+    scn_bench_destroy(b);
+    return NULL;
+}
+
+int scn_bench_steps(scn_bench_t *b, size_t steps, double *loop_s) {
+    if (!b) return -1;
+    double t0 = now_s();
+    for (size_t q = 0; q < steps; q++, b->n++) {
+        if (b->p) fdtd_update_h_cpml(b->g, b->p);
+        else fdtd_update_h(b->g);
+        if (b->s->n_sources) source_apply(&b->src, b->g, (double)b->n * b->g->dt);
+        if (b->p) fdtd_update_e_cpml_materials(b->g, b->p, b->m);
+        else fdtd_update_e_materials(b->g, b->m);
     }
-    double t2 = now_s();
-    if (setup_s) *setup_s = t1 - t0;
-    if (loop_s) *loop_s = t2 - t1;
-    rc = 0;
-out:
-    materials_destroy(m);
-    cpml_destroy(p);
-    fdtd_grid_destroy(g);
-    return rc;
+    if (loop_s) *loop_s = now_s() - t0;
+    return 0;
 }

@@ -37,6 +37,7 @@ extern "C" void rfb_set_error(const char *fmt, ...) {
 }
 extern "C" const char *rfb_last_error(void) { return g_err; }
 extern "C" unsigned long long rfb_launch_count(void) { return g_launches.load(); }
+extern "C" void rfb_count_launch(void) { g_launches++; }
 
 #define CK(call)                                                                        \
     do {                                                                                \
@@ -84,20 +85,24 @@ void mc_release_device(MemCache &c, int dev) {
 }  // namespace
 
 // Host-side fault injection (no device fault): RFSYN_FDTD_FAIL_ALLOC=n makes
-// the n-th device allocation of each single-scene engine creation report
-// cudaErrorMemoryAllocation without calling the driver, so every error path
-// of creation can be driven from a test.  Armed at the start of a creation,
-// disarmed at its end; unset or 0: off.
-static std::atomic<long long> g_fail_countdown{0};
+// the n-th device allocation that the creating thread makes inside one
+// single-scene engine creation (rfb_engine_create: field buffers, CPML,
+// scene upload, plan, graphs) report cudaErrorMemoryAllocation without
+// calling the driver, so every error path of engine creation can be driven
+// from a test.  The countdown belongs to the creating thread, so allocations
+// other threads make meanwhile never take the injected failure; allocations
+// made before the engine exists (host scene building, the sphere
+// rasteriser's staging) are outside the armed window.  Unset or 0: off.
+static thread_local long long g_fail_countdown = 0;
 
 static void arm_alloc_failure(bool on) {
     const char *v = on ? getenv("RFSYN_FDTD_FAIL_ALLOC") : nullptr;
-    g_fail_countdown.store(v ? atoll(v) : 0);
+    g_fail_countdown = v ? atoll(v) : 0;
 }
 
 static cudaError_t dmalloc_raw(void **p, size_t n) {
     *p = nullptr;
-    if (g_fail_countdown.load() > 0 && g_fail_countdown.fetch_sub(1) == 1) return cudaErrorMemoryAllocation;
+    if (g_fail_countdown > 0 && --g_fail_countdown == 0) return cudaErrorMemoryAllocation;
     if (n < MC_MIN) return cudaMalloc(p, n);
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);

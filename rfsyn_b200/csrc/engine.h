@@ -260,8 +260,10 @@ void rfb_set_error(const char *fmt, ...);
 double rfb_now(void);
 void rfb_trace(const char *phase, double t0);
 
-/* Number of kernels this process has launched through the engine. */
+/* Number of kernels this process has launched through the engine;
+ * rfb_count_launch adds one for a launch made outside engine.cu. */
 unsigned long long rfb_launch_count(void);
+void rfb_count_launch(void);
 unsigned long long rfb_cached_bytes(void);
 /* process-wide settings (host/run.c, engine.cu) */
 const char *rfb_plan_override(void);

@@ -9,6 +9,11 @@
 // allocation there would invalidate the capture), a real-time loop that must
 // never enter the allocator, or a process whose device memory is owned by a
 // pool allocator of another framework.
+//
+// Work is issued on a stream of this file's own, created non-blocking, so it
+// never synchronises with the legacy default stream (and through it with a
+// stream another thread is capturing), and the results come back with
+// asynchronous copies on that stream followed by a wait on that stream only.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -25,29 +30,45 @@ __global__ void k_sphere_fractions(double cx, double cy, double cz, double r, in
 #define RFB_NOALLOC_MAX_SAMPLES (1u << 20)
 static __device__ __align__(256) double g_sphere_scratch[2 * (size_t)RFB_NOALLOC_MAX_SAMPLES];
 
-// Device address of the staging array, looked up once per device with that
-// device current (the host-side name is only a stand-in, not an address).
+// Per device, looked up once with that device current: the staging array's
+// device address (the host-side name is only a stand-in, not an address) and
+// the non-blocking stream the calls run on.
 #define RFB_NOALLOC_MAX_DEVICES 64
-static std::mutex g_setup_mu;
-static double *g_scratch_addr[RFB_NOALLOC_MAX_DEVICES];
+namespace {
+struct NoallocDevice {
+    double *scratch = nullptr;
+    cudaStream_t stream = nullptr;
+};
+std::mutex g_setup_mu;
+NoallocDevice g_dev[RFB_NOALLOC_MAX_DEVICES];
+}  // namespace
 
-static double *scratch_for_current_device() {
+static const NoallocDevice *setup_current_device() {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= RFB_NOALLOC_MAX_DEVICES) {
         rfb_set_error("fdtd_b200_sphere_fractions_noalloc: no usable current CUDA device");
         return nullptr;
     }
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    NoallocDevice &d = g_dev[dev];
+    if (!d.scratch) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_sphere_scratch);
         if (e != cudaSuccess || !p) {
             rfb_set_error("fdtd_b200_sphere_fractions_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
             return nullptr;
         }
-        g_scratch_addr[dev] = (double *)p;
+        d.scratch = (double *)p;
     }
-    return g_scratch_addr[dev];
+    if (!d.stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            d.stream = nullptr;
+            rfb_set_error("fdtd_b200_sphere_fractions_noalloc: stream creation failed: %s", cudaGetErrorString(e));
+            return nullptr;
+        }
+    }
+    return &d;
 }
 
 extern "C" int fdtd_b200_sphere_fractions_noalloc(const double centre[3], double radius, int i0, int j0, int k0,
@@ -62,16 +83,18 @@ extern "C" int fdtd_b200_sphere_fractions_noalloc(const double centre[3], double
                       n, (unsigned)RFB_NOALLOC_MAX_SAMPLES);
         return -1;
     }
-    double *scratch = scratch_for_current_device();
-    if (!scratch) return -1;
-    double *sf = scratch, *sn = scratch + RFB_NOALLOC_MAX_SAMPLES;
+    const NoallocDevice *d = setup_current_device();
+    if (!d) return -1;
+    double *sf = d->scratch, *sn = d->scratch + RFB_NOALLOC_MAX_SAMPLES;
     // every one of the n samples of both arrays is written by the kernel, so
     // nothing left by an earlier call needs clearing
-    k_sphere_fractions<<<(unsigned)((n + 255) / 256), 256>>>(centre[0], centre[1], centre[2], radius, i0, j0, k0, ni,
-                                                             nj, nk, sf, sn);
+    k_sphere_fractions<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(centre[0], centre[1], centre[2], radius,
+                                                                           i0, j0, k0, ni, nj, nk, sf, sn);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(f, sf, n * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(n2, sn, n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) rfb_count_launch();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(f, sf, n * sizeof(double), cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(n2, sn, n * sizeof(double), cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
     if (e != cudaSuccess) {
         rfb_set_error("fdtd_b200_sphere_fractions_noalloc: %s", cudaGetErrorString(e));
         return -1;

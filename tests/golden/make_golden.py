@@ -52,7 +52,7 @@ VALIDATOR_ARGS = {
     "validate_materials_fresnel": [], "validate_probe_dft": [], "validate_materials_energy": [],
     "validate_cpml_oblique": [], "validate_materials_high_contrast": ["--full"],
     "validate_long_term_stability": ["--steps", "10000"], "validate_materials_tilted": [],
-    "audit_periodic_energy": [],
+    "audit_periodic_energy": [], "subpixel_te_unit": [],
 }
 
 

@@ -3,7 +3,7 @@ slab of a full 3x3 eps_r, 2-pole Lorentz layer, reflection / transmission
 probe planes) at a size the oracle runs in seconds: FP64 device runs equal
 the CPU oracle bit for bit, through the oracle's explicit samples and
 through the product's own slab / dispersive-box helpers alike; FP32 probe
-spectra within the FP32 bound of the FP64 oracle."""
+spectra within 1e-4 relative L2 of the FP64 oracle, probe by probe."""
 from __future__ import annotations
 
 import numpy as np
@@ -14,7 +14,7 @@ import rfsyn_b200 as rb
 from rfsyn_b200 import scenes
 from tests.cases import run_device, workload_to_scene
 
-FP32_SPEC_L2 = 1e-3
+FP32_SPEC_L2 = 1e-4
 
 
 def _workload(precision):
@@ -53,6 +53,6 @@ def test_fp32_spectra_within_bound(want):
     w = _workload(rb.FP32)
     st = scenes.scene_setup(w)
     r = rb.run(scenes.run_config(w), st.ptr, None)
-    num = np.linalg.norm(r["dft"] - want["dft"], axis=1)
-    den = np.linalg.norm(want["dft"], axis=1)
-    assert np.all(num <= FP32_SPEC_L2 * den.max()), (num / den.max()).max()
+    # each probe against its own FP64 norm (no normalisation by the largest)
+    err = np.linalg.norm(r["dft"] - want["dft"], axis=1) / np.linalg.norm(want["dft"], axis=1)
+    assert err.max() <= FP32_SPEC_L2, (int(err.argmax()), float(err.max()))

@@ -1,4 +1,4 @@
-"""Failure detection without a GPU fault (SURVEY section 5).
+"""Failure detection without a GPU fault.
 
 Every sweep waits on its tensor copies with a bounded wait and reports a
 stalled copy as an error the host returns; these tests make that wait run

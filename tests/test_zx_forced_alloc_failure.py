@@ -1,10 +1,13 @@
 """Host-side fault injection: a forced device-allocation failure.
 
-RFSYN_FDTD_FAIL_ALLOC=n makes the n-th device allocation of a single-scene
-engine creation report out-of-memory without calling the driver (no device
-fault).  Creating a small scene with n = 1, 2, ... walks every allocation of
-creation: each attempt must fail with an error the host reads, free what it
-had built and leave the device usable, until n passes the number of
+RFSYN_FDTD_FAIL_ALLOC=n makes the n-th device allocation that the creating
+thread makes inside a single-scene engine creation (field buffers, CPML,
+scene upload, plan, graphs) report out-of-memory without calling the driver
+(no device fault).  Creating a small scene with n = 1, 2, ... walks every
+allocation of engine creation (the host-side scene building before it, and
+the sphere rasteriser's staging, are not walked): each attempt must fail
+with an error the host reads, free what it had built and leave the device
+usable, until n passes the number of
 allocations and creation succeeds.  The scene built afterwards, partly on
 memory the failed attempts released, gives the same probe series and
 spectra bit for bit as before the failures.  Collected late, so a fault
