@@ -3,7 +3,8 @@
 Workload: the 256^3 FP32 scene with 24 subpixel-smoothed dielectric spheres,
 3 Debye spheres, 12-cell CPML, 16 probes x 256 DFT bins and 4000 steps
 (rfsyn_b200.scenes.c2).  A bench "step" is one full simulation of that scene
-(reset + 4000 time steps; the probe series stay on the device).  Metric:
+(reset + 4000 time steps, the probe spectra accumulating on the device as
+the steps run).  Metric:
 Mcell-updates/s = nx*ny*nz*n_steps*K / seconds, whole job.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]

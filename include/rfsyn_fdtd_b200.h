@@ -77,6 +77,19 @@ typedef struct {
     size_t i0, i1, j0, j1, k0, k1;
 } fdtd_b200_plane_wave_t;
 
+/* A plane probe: every step, the mean of one field component over a whole
+ * grid plane -- axis (0 = x, 1 = y, 2 = z) at cell index `index`, every
+ * cell of the other two axes (u < n_u, v < n_v).  In a cell periodic across
+ * the plane, at normal incidence, that mean is the amplitude of the
+ * specular reflected or transmitted wave, so a plane probe's running DFT is
+ * a reflection / transmission spectrum.  No counterpart in rfsyn (its
+ * probes are single cells, engine/fdtd/probe.h:8-39). */
+typedef struct {
+    int axis;
+    size_t index;
+    field_component_t component;   /* FIELD_EX..FIELD_HZ */
+} fdtd_b200_plane_probe_t;
+
 typedef struct {
     size_t nx, ny, nz;
     double dx;
@@ -94,13 +107,23 @@ typedef struct {
     size_t n_probes;
     const fdtd_b200_probe_t *probes;
     /* Probe DFT bins (shared by every probe).  Sample n (recorded after the
-     * E update of step n) enters at t = (n + dft_time_offset_steps) dt. */
+     * E update of step n) enters at t = (n + dft_time_offset_steps) dt.  In
+     * sessions the sums accumulate on the GPU as the steps run (FP64 runs:
+     * FP64 sums with direct sincos, rfsyn's probe_dft_record arithmetic,
+     * engine/fdtd/probe.c:78-92; FP32 runs: Kahan-compensated FP32 sums with
+     * an FP64 phase recurrence); batches transform the stored series when
+     * read. */
     size_t n_freqs;
     const double *freqs_hz;
     double dft_time_offset_steps;
     /* NULL, or a plane wave injected through a TF/SF boundary (sessions and
      * fdtd_b200_run; not in batches) */
     const fdtd_b200_plane_wave_t *plane_wave;
+    /* Plane probes (sessions and fdtd_b200_run; not in batches): their
+     * series and spectra follow the point probes', so every probe output
+     * holds n_probes + n_planes series. */
+    size_t n_planes;
+    const fdtd_b200_plane_probe_t *planes;
 } fdtd_b200_config_t;
 
 /* Defaults: courant 0.99, cpml = cpml_default_params(npml), FP64, FUSED,
@@ -109,8 +132,8 @@ void fdtd_b200_config_init(fdtd_b200_config_t *cfg, size_t nx, size_t ny, size_t
                            size_t n_steps, size_t npml);
 
 typedef struct {
-    double *probe_td;              /* n_probes * n_steps, probe-major, or NULL */
-    double *dft_re, *dft_im;       /* n_probes * n_freqs, or NULL */
+    double *probe_td;              /* (n_probes + n_planes) * n_steps, probe-major, or NULL */
+    double *dft_re, *dft_im;       /* (n_probes + n_planes) * n_freqs, or NULL */
     double sample_rate_hz;         /* 1 / dt */
     double device_ms;              /* GPU time of the step loop (CUDA events) */
 } fdtd_b200_result_t;
@@ -137,9 +160,9 @@ int fdtd_b200_sim_synchronize(fdtd_b200_sim_t *sim);
 int fdtd_b200_sim_advance_timed(fdtd_b200_sim_t *sim, size_t n_steps, double *ms);
 size_t fdtd_b200_sim_steps_done(const fdtd_b200_sim_t *sim);
 void *fdtd_b200_sim_stream(const fdtd_b200_sim_t *sim);
-/* n_probes * n_steps doubles, probe-major (blocking). */
+/* (n_probes + n_planes) * n_steps doubles, probe-major (blocking). */
 int fdtd_b200_sim_read_probes(fdtd_b200_sim_t *sim, double *probe_td);
-/* n_probes * n_freqs each, over the steps done so far (blocking). */
+/* (n_probes + n_planes) * n_freqs each, over the steps done so far (blocking). */
 int fdtd_b200_sim_dft(fdtd_b200_sim_t *sim, double *dft_re, double *dft_im);
 
 /* ---- the stage's output signal, AWGN and .iq files ---------------------------
@@ -342,7 +365,8 @@ int fdtd_b200_materials_clear_component_dispersive(materials_t *mat, const fdtd_
  *   E_c += dt/(eps0 dx) (m_cc D_c + sum_{b != c} m_cb <D_b>),
  * D_b = (curl H)_b dx at the b sample, <D_b> its mean over the four b
  * samples surrounding the E_c sample (which keeps the coupling reciprocal
- * for a symmetric m).  Lossless; for cells outside the CPML; on an axis
+ * for a symmetric m).  Lossless as set here (spheres smoothed with smoothing 2
+ * carry a loss, see below); for cells outside the CPML; on an axis
  * without wrap the cell lies in [1, n-1].  A 3x3 sample takes precedence
  * over every other description of the same component; box assignment clears
  * them.  set_component_tensor3 takes the row (3 values, m_cc > 0);
@@ -360,6 +384,15 @@ int fdtd_b200_materials_set_tensor3_box(materials_t *mat, const fdtd_grid_t *g, 
  * anisotropic slab). */
 int fdtd_b200_materials_set_tensor3_slab(materials_t *mat, const fdtd_grid_t *g, const double point[3],
                                          const double normal[3], double thickness, const double eps_r[9]);
+/* The same slab with its faces smoothed: samples whose unit cube lies inside
+ * get the row of eps_r^-1 as above; samples whose cube a face may cut get,
+ * when their fill fraction f (8^3 lattice) is positive, the row of the
+ * smoothed inverse permittivity between the cell's table material and eps_r
+ * along the normal (fdtd_b200_subpixel_tensor3, Kottke et al.'s average for
+ * the anisotropic slab), with sigma (1 - f) sigma_table, built on the GPU in
+ * FP64.  The margin rule applies. */
+int fdtd_b200_materials_set_tensor3_slab_smoothed(materials_t *mat, const fdtd_grid_t *g, const double point[3],
+                                                  const double normal[3], double thickness, const double eps_r[9]);
 /* The row of a 3x3 sample: 0, or 1 when the component has none. */
 int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g, field_component_t component,
                                     size_t i, size_t j, size_t k, double row[3]);
@@ -370,12 +403,21 @@ int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g
  * in list order, later spheres over earlier ones.  The fill fraction f of the
  * unit cube around every E sample near a surface is computed on the GPU in
  * FP64 (supersampled, 8^3 points).  A cell whose three samples are inside
- * takes the sphere's material id; samples cut by the surface get a scalar
- * override with the diagonal of the smoothed inverse permittivity
- *   1/eps_c = n_c^2 <1/eps> + (1 - n_c^2) / <eps>,  <.> weighted by f,
- * n the outward surface normal, sigma mixed by f (smoothing = 1), or the
- * inside material when f >= 1/2 (smoothing = 0).  Dispersive spheres
- * (model != NULL) are always staircased onto dispersive samples. */
+ * takes the sphere's material id; a sample cut by the surface gets, by
+ * `smoothing`:
+ *   0  the inside material when f >= 1/2 (staircase);
+ *   1  a scalar override with the diagonal of the smoothed inverse
+ *      permittivity 1/eps_c = n_c^2 <1/eps> + (1 - n_c^2) / <eps>;
+ *   2  the full row of the smoothed inverse permittivity as a 3x3 sample,
+ *      M = <1/eps> n n^T + (1/<eps>) (I - n n^T) (fdtd_b200_subpixel_tensor3
+ *      with two isotropic media), built on the GPU in FP64, off-diagonal
+ *      terms included; where the 3x3 update cannot run (the margin rule of
+ *      fdtd_b200_materials_set_component_tensor3) its diagonal as in 1;
+ * with <.> weighted by f against the cell's table material, n the outward
+ * surface normal at the sample, and sigma mixed by f (a lossy 3x3 sample
+ * takes its loss at the component's permittivity 1/M_cc, as rfsyn's
+ * make_coeff does for a scalar one).  Dispersive spheres (model != NULL) are
+ * always staircased onto dispersive samples. */
 typedef struct {
     double cx, cy, cz, radius;
     double eps_r, sigma;
@@ -452,7 +494,10 @@ int fdtd_b200_materials_apply_heightmap(materials_t *mat, const fdtd_grid_t *g, 
  * start-up: before any stream capture, and before another framework's pool
  * takes the device's memory.  Later calls launch on that stream and copy back
  * with asynchronous copies on it, so they never wait on the legacy default
- * stream or on a stream another thread is capturing.  Every call shares the
+ * stream or on a stream another thread is capturing; for the duration of a
+ * call the calling thread's capture mode is thread-local, so a capture
+ * another thread runs in the global mode is not disturbed by it (the
+ * caller's mode is restored on return).  Every call shares the
  * one array: calls that overlap on the GPU (from several host threads) race,
  * so serialise them. */
 int fdtd_b200_sphere_fractions_noalloc(const double centre[3], double radius, int i0, int j0, int k0,

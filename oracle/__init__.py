@@ -82,9 +82,13 @@ def disp_entry(comp, i, j, k, eps_inf, sigma, poles):
     return (comp, i, j, k, eps_inf, sigma, len(poles), tuple(kind), tuple(de), tuple(tau), tuple(wp), tuple(gm))
 
 
+class ScnPlane(C.Structure):
+    _fields_ = [("axis", C.c_int), ("index", C.c_size_t), ("comp", C.c_int)]
+
+
 class ScnTensor3(C.Structure):
     _fields_ = [("comp", C.c_int), ("i", C.c_size_t), ("j", C.c_size_t), ("k", C.c_size_t),
-                ("m", C.c_double * 3)]
+                ("m", C.c_double * 3), ("sigma", C.c_double)]
 
 
 class ScnPlaneWave(C.Structure):
@@ -112,6 +116,7 @@ class ScnScene(C.Structure):
         ("src_t_offset", C.c_double), ("dft_t_offset", C.c_double),
         ("n_tensor3", C.c_size_t), ("tensor3", C.POINTER(ScnTensor3)),
         ("plane_wave", C.POINTER(ScnPlaneWave)),
+        ("n_planes", C.c_size_t), ("planes", C.POINTER(ScnPlane)),
     ]
 
 
@@ -140,10 +145,11 @@ class Scene:
     smoothing: int = 1
     sources: list = field(default_factory=list)    # (i,j,k,comp,mode,amp,waveform,p0,p1,p2)
     probes: list = field(default_factory=list)     # (i,j,k,comp)
+    planes: list = field(default_factory=list)     # (axis,index,comp) plane probes, series after the probes
     freqs: list = field(default_factory=list)
     src_t_offset: float = 0.0
     dft_t_offset: float = 1.0
-    tensor3: list = field(default_factory=list)    # (comp,i,j,k,(m0,m1,m2)) rows of eps_r^-1, applied last
+    tensor3: list = field(default_factory=list)    # (comp,i,j,k,(m0,m1,m2)[,sigma]) rows of eps_r^-1, applied last
     plane_wave: dict | None = None                  # ScnPlaneWave fields by name
 
     @property
@@ -173,8 +179,8 @@ class Scene:
                           (C.c_double * 2)(*tau), (C.c_double * 2)(*wp), (C.c_double * 2)(*gm)))
         s.n_disp, s.disp = arr(ScnDisp, drows)
         s.n_spheres, s.spheres = arr(ScnSphere, self.spheres)
-        s.n_tensor3, s.tensor3 = arr(ScnTensor3, [(c, i, j, k, (C.c_double * 3)(*m))
-                                                  for (c, i, j, k, m) in self.tensor3])
+        s.n_tensor3, s.tensor3 = arr(ScnTensor3, [(t[0], t[1], t[2], t[3], (C.c_double * 3)(*t[4]),
+                                                   t[5] if len(t) > 5 else 0.0) for t in self.tensor3])
         if self.plane_wave is not None:
             pw = ScnPlaneWave()
             for name, _ in ScnPlaneWave._fields_:
@@ -183,6 +189,7 @@ class Scene:
             s.plane_wave = C.pointer(pw)
         s.n_sources, s.sources = arr(ScnSource, self.sources)
         s.n_probes, s.probes = arr(ScnProbe, self.probes)
+        s.n_planes, s.planes = arr(ScnPlane, self.planes)
         f = (C.c_double * max(len(self.freqs), 1))(*self.freqs)
         keep.append(f)
         s.n_freqs, s.freqs = len(self.freqs), f
@@ -228,7 +235,7 @@ def ref_available() -> bool:
 
 def _run(lib: C.CDLL, prefix: str, scene: Scene):
     s = scene.to_c()
-    npb, nf, nt = len(scene.probes), len(scene.freqs), scene.n_steps
+    npb, nf, nt = len(scene.probes) + len(scene.planes), len(scene.freqs), scene.n_steps
     td = np.zeros(max(npb * nt, 1))
     re = np.zeros(max(npb * nf, 1))
     im = np.zeros(max(npb * nf, 1))

@@ -75,7 +75,7 @@ typedef struct {
     double *dst;    /* 5 per sample: J0 J1 J0- J1- E- */
     /* full 3x3 samples: per component a flag and the row of eps_r^-1 */
     uint8_t *has_t3[3];
-    double *t3m[3];
+    double *t3m[3], *t3s[3];
     /* plane wave: the 1-D line, H targets, per-sample E term ranges, terms */
     int tf;
     size_t tf_len;
@@ -139,7 +139,7 @@ static void orc_free(orc_t *o) {
         free(o->has_ovr[c]); free(o->oca[c]); free(o->ocb[c]);
     }
     for (int c = 0; c < 2; c++) { free(o->has_t[c]); free(o->tm11[c]); free(o->tm12[c]); free(o->tm22[c]); free(o->tscale[c]); }
-    for (int c = 0; c < 3; c++) free(o->dix[c]), free(o->has_t3[c]), free(o->t3m[c]);
+    for (int c = 0; c < 3; c++) free(o->dix[c]), free(o->has_t3[c]), free(o->t3m[c]), free(o->t3s[c]);
     for (int c = 0; c < 3; c++) free(o->tf_efirst[c]), free(o->tf_ecount[c]);
     free(o->tf_e); free(o->tf_h); free(o->tf_src); free(o->tf_hw); free(o->tf_hc); free(o->tf_hfirst);
     free(o->tf_hcount); free(o->tf_coef); free(o->tf_w); free(o->tf_idx);
@@ -218,7 +218,7 @@ static void sr_bg(void *ctx, size_t w, double *eps, double *sig) {
     *sig = o->tsig[o->id[w]];
 }
 static void clear_samples(orc_t *o, size_t w) {
-    for (int c = 0; c < 3; c++) o->has_ovr[c][w] = 0, o->dix[c][w] = -1;
+    for (int c = 0; c < 3; c++) o->has_ovr[c][w] = 0, o->dix[c][w] = -1, o->has_t3[c][w] = 0;
     for (int c = 0; c < 2; c++) o->has_t[c][w] = 0;
 }
 static int sr_fill(void *ctx, size_t w, const scn_sphere_t *sp) {
@@ -241,10 +241,21 @@ static int sr_sample(void *ctx, size_t w, int c, double eps, double sig) {
     if (coeff(o, eps, sig, &o->oca[c][w], &o->ocb[c][w]) != 0) return -1;
     o->has_ovr[c][w] = 1;
     o->dix[c][w] = -1;
+    o->has_t3[c][w] = 0;
     return 0;
 }
 static int sr_sample_disp(void *ctx, size_t w, int c, const scn_disp_t *d) {
     return set_disp((orc_t *)ctx, c, w, d);
+}
+static int sr_sample_t3(void *ctx, size_t w, int c, const double row[3], double sigma) {
+    orc_t *o = (orc_t *)ctx;
+    o->has_ovr[c][w] = 0;
+    o->dix[c][w] = -1;
+    if (c < 2) o->has_t[c][w] = 0;
+    o->has_t3[c][w] = 1;
+    memcpy(o->t3m[c] + 3 * w, row, 3 * sizeof(double));
+    o->t3s[c][w] = sigma;
+    return 0;
 }
 static size_t sr_canon(const void *geo, size_t i, size_t j, size_t k) { return at((const orc_t *)geo, i, j, k); }
 
@@ -501,7 +512,8 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
     for (int c = 0; c < 3; c++) {
         o->has_t3[c] = calloc(o->total, 1);
         o->t3m[c] = calloc(3 * o->total, 8);
-        if (!o->has_t3[c] || !o->t3m[c]) return -1;
+        o->t3s[c] = calloc(o->total, 8);
+        if (!o->has_t3[c] || !o->t3m[c] || !o->t3s[c]) return -1;
     }
     for (int c = 0; c < 3; c++) {
         o->dix[c] = malloc(o->total * sizeof(int));
@@ -565,7 +577,7 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
     if (s->n_spheres) {
         for (size_t q = 0; q < s->n_spheres; q++)
             if (s->spheres[q].disp < 0 && table_id(o, s->spheres[q].eps_r, s->spheres[q].sigma) < 0) return -1;
-        sr_target_t tg = {o, sr_bg, sr_fill, sr_fill_disp, sr_sample, sr_sample_disp};
+        sr_target_t tg = {o, sr_bg, sr_fill, sr_fill_disp, sr_sample, sr_sample_disp, sr_sample_t3};
         if (sr_rasterise(s, o->n, o->per, sr_canon, o, &tg) != 0) return -1;
     }
     for (size_t q = 0; q < s->n_tensor3; q++) {
@@ -573,6 +585,7 @@ static int orc_init(orc_t *o, const scn_scene_t *s) {
         size_t w = at(o, t->i, t->j, t->k);
         o->has_t3[t->comp][w] = 1;
         memcpy(o->t3m[t->comp] + 3 * w, t->m, 3 * sizeof(double));
+        o->t3s[t->comp][w] = t->sigma;
     }
     if (s->plane_wave && tf_init(o, s) != 0) return -1;
     return 0;
@@ -670,7 +683,10 @@ static double curl_d(const orc_t *o, int b, size_t i, size_t j, size_t k) {
 
 /* Full 3x3 sample: value = m_cc D_c, then for each b != c (ascending)
  * value += m_cb (0.25 (((D_b(w) + D_b(w+e_c)) + D_b(w-e_b)) + D_b(w+e_c-e_b)));
- * E_c += dt/(eps0 dx) value. */
+ * E_c = ca E_c + s value with the loss of sigma at the component's
+ * permittivity 1/m_cc (rfsyn's make_coeff form, materials.c:92-125):
+ * loss = sigma dt / (2 eps0 / m_cc), s = dt/(eps0 dx) / (1 + loss),
+ * ca = (1 - loss) / (1 + loss). */
 static void tensor3(orc_t *o, int c, size_t i, size_t j, size_t k) {
     size_t w = at(o, i, j, k);
     const double *r = o->t3m[c] + 3 * w;
@@ -687,7 +703,9 @@ static void tensor3(orc_t *o, int c, size_t i, size_t j, size_t k) {
                     curl_d(o, b, p3[0], p3[1], p3[2]);
         value = value + r[b] * (0.25 * s4);
     }
-    o->E[c][w] = o->E[c][w] + (o->dt / (O_EPS0 * o->dx)) * value;
+    const double loss = (o->t3s[c][w] * o->dt) / (2.0 * (O_EPS0 / r[c]));
+    const double sc = (o->dt / (O_EPS0 * o->dx)) / (1.0 + loss), ca = (1.0 - loss) / (1.0 + loss);
+    o->E[c][w] = ca * o->E[c][w] + sc * value;
 }
 
 /* E update (materials.c:911-1060).  Component c: E_c = Ca E_c + Cb (dA - dB)
@@ -796,21 +814,57 @@ static void step(orc_t *o, const scn_scene_t *s, size_t n) {
     if (o->tf) tf_after_e(o, n + 1, s->n_steps);
 }
 
-/* Runs the scene; probe_td n_probes*n_steps, dft_re/im n_probes*n_freqs. */
+/* Mean of one component over a whole plane (plane probe), FP64, summed in
+ * the order of the GPU's reduction so FP64 runs compare bit for bit: the
+ * points t = u n_v + v (u outer) are dealt to 1024 partial sums, point t to
+ * partial t mod 1024 in increasing t; each group of 32 partials is reduced by
+ * halving (p[l] += p[l + h] for h = 16, 8, 4, 2, 1); the 32 group sums are
+ * added in order; the total is divided by n_u n_v. */
+static double plane_mean(const orc_t *o, const scn_plane_t *pl) {
+    const int a = pl->axis, u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
+    const double *f = field((orc_t *)o, pl->comp);
+    const size_t nu = o->n[u], nv = o->n[v], npts = nu * nv;
+    double part[1024];
+    for (int t = 0; t < 1024; t++) part[t] = 0.0;
+    for (size_t t = 0; t < npts; t++) {
+        size_t ijk[3];
+        ijk[a] = pl->index;
+        ijk[u] = t / nv;
+        ijk[v] = t % nv;
+        part[t % 1024] = part[t % 1024] + f[at(o, ijk[0], ijk[1], ijk[2])];
+    }
+    double sum = 0.0;
+    for (int w = 0; w < 32; w++) {
+        double *g = part + 32 * w;
+        for (int h = 16; h > 0; h >>= 1)
+            for (int l = 0; l < 32 - h; l++) g[l] = g[l] + g[l + h];
+        sum = sum + g[0];
+    }
+    return sum / (double)npts;
+}
+
+/* Runs the scene; probe_td (n_probes + n_planes) * n_steps, dft_re/im
+ * (n_probes + n_planes) * n_freqs: point probes, then plane probes. */
 int orc_run(const scn_scene_t *s, double *probe_td, double *dft_re, double *dft_im) {
     orc_t o;
     int rc = -1;
+    const size_t ns = s->n_probes + s->n_planes;
     if (orc_init(&o, s) != 0) goto out;
     if (dft_re && dft_im && s->n_freqs) {
-        memset(dft_re, 0, s->n_probes * s->n_freqs * 8);
-        memset(dft_im, 0, s->n_probes * s->n_freqs * 8);
+        memset(dft_re, 0, ns * s->n_freqs * 8);
+        memset(dft_im, 0, ns * s->n_freqs * 8);
     }
     for (size_t n = 0; n < s->n_steps; n++) {
         step(&o, s, n);
         double td = ((double)n + s->dft_t_offset) * o.dt;
-        for (size_t q = 0; q < s->n_probes; q++) {
-            const scn_probe_t *p = &s->probes[q];
-            double v = field(&o, p->comp)[at(&o, p->i, p->j, p->k)];
+        for (size_t q = 0; q < ns; q++) {
+            double v;
+            if (q < s->n_probes) {
+                const scn_probe_t *p = &s->probes[q];
+                v = field(&o, p->comp)[at(&o, p->i, p->j, p->k)];
+            } else {
+                v = plane_mean(&o, &s->planes[q - s->n_probes]);
+            }
             if (probe_td) probe_td[q * s->n_steps + n] = v;
             if (dft_re && dft_im)
                 for (size_t f = 0; f < s->n_freqs; f++) {

@@ -26,11 +26,13 @@ typedef struct { int comp; size_t i, j, k; double eps_r, sigma; } scn_comp_t;
 typedef struct { int comp; size_t i, j, k; double m11, m12, m22; } scn_tensor_t;
 /* full 3x3 sample (no rfsyn counterpart): row `comp` of the relative
  * inverse permittivity */
-typedef struct { int comp; size_t i, j, k; double m[3]; } scn_tensor3_t;
+typedef struct { int comp; size_t i, j, k; double m[3]; double sigma; } scn_tensor3_t;
 /* waveform: 0 Gaussian derivative (p0 t0, p1 tau), 1 Ricker (p0 f0, p1 t0),
  *           2 modulated Gaussian (p0 f, p1 t0, p2 tau).  mode 0 soft, 1 hard. */
 typedef struct { size_t i, j, k; int comp, mode; double amplitude; int waveform; double p0, p1, p2; } scn_source_t;
 typedef struct { size_t i, j, k; int comp; } scn_probe_t;
+/* mean of component comp over the whole plane axis = index (cells u < n_u, v < n_v) */
+typedef struct { int axis; size_t index; int comp; } scn_plane_t;
 /* dispersive sample (no rfsyn counterpart): kind 0 Debye (tau), 1 Lorentz
  * (omega_p, gamma) per pole */
 typedef struct {
@@ -69,13 +71,14 @@ typedef struct {
     size_t n_tensors; const scn_tensor_t *tensors;  /* then tensor edges */
     size_t n_disp;    const scn_disp_t *disp;       /* then dispersive samples */
     size_t n_spheres; const scn_sphere_t *spheres;  /* then spheres, in order */
-    int smoothing;                                  /* sphere smoothing on/off */
+    int smoothing;                                  /* sphere smoothing: 0 off, 1 diagonal, 2 full 3x3 */
     size_t n_sources; const scn_source_t *sources;
     size_t n_probes;  const scn_probe_t *probes;
     size_t n_freqs;   const double *freqs;
     double src_t_offset, dft_t_offset;
     size_t n_tensor3; const scn_tensor3_t *tensor3; /* applied last */
     const scn_plane_wave_t *plane_wave;             /* NULL: none */
+    size_t n_planes;  const scn_plane_t *planes;    /* plane probes: series after the point probes */
 } scn_scene_t;
 
 #endif

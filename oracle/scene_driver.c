@@ -204,6 +204,8 @@ int scn_setup(const fdtd_grid_t *g, materials_t *m, void *ctx) {
     }
     for (size_t q = 0; q < s->n_tensor3; q++) {
         const scn_tensor3_t *t = &s->tensor3[q];
+        /* the public setter takes lossless rows */
+        if (t->sigma != 0.0) return -1;
         if (fdtd_b200_materials_set_component_tensor3(m, g, comp_of(t->comp), t->i, t->j, t->k, t->m) != 0) return -1;
     }
 #else
@@ -231,6 +233,7 @@ typedef union {
  * dft_re/dft_im: n_probes * n_freqs (may be NULL). */
 int scn_run(const scn_scene_t *s, double *probe_td, double *dft_re, double *dft_im) {
     int rc = -1;
+    if (s->n_planes) return -1; /* rfsyn's probes are single cells */
     fdtd_grid_t *g = fdtd_grid_create(s->nx, s->ny, s->nz, s->dx, s->courant);
     cpml_t *p = NULL;
     materials_t *m = NULL;

@@ -2,7 +2,9 @@
  * sphere_raster.h -- TEST INFRASTRUCTURE (oracle).  CPU restatement of the
  * sphere rasteriser (fill fraction of the unit cube around each E sample by
  * 8^3 supersampling, FP64; diagonal of the smoothed inverse permittivity,
- * Farjadpour et al., Opt. Lett. 31, 2972 (2006)) into a dense per-sample
+ * Farjadpour et al., Opt. Lett. 31, 2972 (2006), or with smoothing 2 its
+ * full row, eps^-1 = <1/eps> n n^T + (1/<eps>) (I - n n^T), where the 3x3
+ * update may run) into a dense per-sample
  * state, sphere by sphere in list order.  Shared by the oracle and by the
  * scene driver built over rfsyn (which then hands the state to rfsyn's own
  * materials API).
@@ -53,6 +55,9 @@ typedef struct {
     /* sample c of cell w: scalar override (clears a dispersive sample) */
     int (*set_sample)(void *ctx, size_t w, int c, double eps_r, double sigma);
     int (*set_sample_disp)(void *ctx, size_t w, int c, const scn_disp_t *d);
+    /* sample c of cell w: row of a 3x3 sample with loss sigma (clears the
+     * sample's other descriptions); NULL: not supported */
+    int (*set_sample_t3)(void *ctx, size_t w, int c, const double row[3], double sigma);
 } sr_target_t;
 
 /* Rasterises every sphere of s into the target.  n: nx, ny, nz; periodic
@@ -98,7 +103,36 @@ static int sr_rasterise(const scn_scene_t *s, const size_t n[3], unsigned period
                             continue;
                         }
                         double eps_c, sig_c;
-                        if (!s->smoothing || f[c] == 1.0) {
+                        if (s->smoothing == 2 && f[c] < 1.0) {
+                            /* full row; the 3x3 update needs the cell in
+                             * [1, n-1] on every axis without wrap */
+                            double eb, sb;
+                            t->background(t->ctx, w, &eb, &sb);
+                            const double p[3] = {(double)i + (c == 0 ? 0.5 : 0.0), (double)j + (c == 1 ? 0.5 : 0.0),
+                                                 (double)k + (c == 2 ? 0.5 : 0.0)};
+                            double nv[3] = {p[0] - sp->cx, p[1] - sp->cy, p[2] - sp->cz};
+                            const double d = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+                            if (d > 0.0) {
+                                nv[0] /= d; nv[1] /= d; nv[2] /= d;
+                            } else {
+                                nv[0] = nv[1] = nv[2] = 0.0;
+                                nv[c] = 1.0;
+                            }
+                            const double lam_n = (1.0 - f[c]) / eb + f[c] / sp->eps_r;
+                            const double lam_t = 1.0 / ((1.0 - f[c]) * eb + f[c] * sp->eps_r);
+                            double row[3];
+                            for (int b = 0; b < 3; b++) row[b] = (lam_n - lam_t) * nv[c] * nv[b] + (b == c ? lam_t : 0.0);
+                            sig_c = f[c] * sp->sigma + (1.0 - f[c]) * sb;
+                            const long pi[3] = {i, j, k};
+                            int margin = 1;
+                            for (int a = 0; a < 3; a++)
+                                if (!(periodic & (1u << a)) && (pi[a] < 1 || pi[a] + 1 > (long)n[a])) margin = 0;
+                            if (margin) {
+                                if (!t->set_sample_t3 || t->set_sample_t3(t->ctx, w, c, row, sig_c) != 0) return -1;
+                                continue;
+                            }
+                            eps_c = 1.0 / row[c];
+                        } else if (!s->smoothing || f[c] == 1.0) {
                             if (f[c] < 0.5) continue;
                             eps_c = sp->eps_r;
                             sig_c = sp->sigma;

@@ -69,6 +69,10 @@ class PlaneWave(C.Structure):
                 ("k0", C.c_size_t), ("k1", C.c_size_t)]
 
 
+class B200Plane(C.Structure):
+    _fields_ = [("axis", C.c_int), ("index", C.c_size_t), ("component", C.c_int)]
+
+
 class B200Config(C.Structure):
     _fields_ = [
         ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
@@ -78,6 +82,7 @@ class B200Config(C.Structure):
         ("n_probes", C.c_size_t), ("probes", C.POINTER(B200Probe)),
         ("n_freqs", C.c_size_t), ("freqs_hz", C.POINTER(C.c_double)), ("dft_time_offset_steps", C.c_double),
         ("plane_wave", C.POINTER(PlaneWave)),
+        ("n_planes", C.c_size_t), ("planes", C.POINTER(B200Plane)),
     ]
 
 
@@ -166,13 +171,17 @@ class SceneSetup:
     materials_set_box, in list order), spheres
     (fdtd_b200_materials_add_spheres), dispersive boxes
     (fdtd_b200_materials_set_dispersive_box) and last anisotropic slabs
-    (fdtd_b200_materials_set_tensor3_slab); keeps the ctypes objects alive.
+    (fdtd_b200_materials_set_tensor3_slab, or with slab_smoothing
+    fdtd_b200_materials_set_tensor3_slab_smoothed); keeps the ctypes objects
+    alive.
     boxes: (i0, i1, j0, j1, k0, k1, eps_r, sigma) half-open cell ranges;
     slabs: (point[3], normal[3], thickness, eps_r[9]); disp_boxes:
     (i0, i1, j0, j1, k0, k1, Dispersive)."""
 
-    def __init__(self, boxes=(), spheres=(), smoothing: int = 1, slabs=(), disp_boxes=()):
+    def __init__(self, boxes=(), spheres=(), smoothing: int = 1, slabs=(), disp_boxes=(), slab_smoothing: int = 0):
         lib = load()
+        set_slab = (lib.fdtd_b200_materials_set_tensor3_slab_smoothed if slab_smoothing
+                    else lib.fdtd_b200_materials_set_tensor3_slab)
         self._spheres = SphereSetup(spheres, smoothing) if spheres else None
         boxes = list(boxes)
         self._slabs = [((C.c_double * 3)(*p), (C.c_double * 3)(*n), t, (C.c_double * 9)(*e))
@@ -190,7 +199,7 @@ class SceneSetup:
                                                               C.byref(model)) != 0:
                     return -1
             for (p, n, t, e) in self._slabs:
-                if lib.fdtd_b200_materials_set_tensor3_slab(mat, grid, p, n, t, e) != 0:
+                if set_slab(mat, grid, p, n, t, e) != 0:
                     return -1
             return 0
 
@@ -286,6 +295,8 @@ def load() -> C.CDLL:
         "materials_set_box": (I, [P, P, S, S, S, S, S, S, D, D]),
         "fdtd_b200_materials_set_dispersive_box": (I, [P, P, S, S, S, S, S, S, P]),
         "fdtd_b200_materials_set_tensor3_slab": (I, [P, P, C.POINTER(D), C.POINTER(D), D, C.POINTER(D)]),
+        "fdtd_b200_materials_set_tensor3_slab_smoothed": (I, [P, P, C.POINTER(D), C.POINTER(D), D, C.POINTER(D)]),
+        "fdtd_b200_subpixel_tensor3": (I, [D, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_sim_info": (I, [P, C.POINTER(SimInfo)]),
         "fdtd_b200_sim_time_kernels": (I, [P, S, C.POINTER(D), C.POINTER(D)]),
         "fdtd_b200_sim_energy": (I, [P, I, I, C.POINTER(Energy)]),
@@ -367,7 +378,7 @@ class RunConfig:
 
     def __init__(self, nx, ny, nz, dx, n_steps, npml, *, courant=0.99, periodic=0, precision=FP64,
                  schedule=FUSED, cpml: CpmlParams | None = None, sources=(), probes=(), freqs=(),
-                 source_time_offset=0.0, dft_time_offset=1.0, plane_wave: dict | None = None):
+                 source_time_offset=0.0, dft_time_offset=1.0, plane_wave: dict | None = None, planes=()):
         self.c = B200Config()
         c = self.c
         c.nx, c.ny, c.nz, c.dx, c.n_steps = nx, ny, nz, dx, n_steps
@@ -411,14 +422,26 @@ class RunConfig:
                 setattr(pw, name, plane_wave.get(name, 0))
             self._pw = pw
             c.plane_wave = C.pointer(pw)
+        self._planes = (B200Plane * max(len(planes), 1))()
+        for q, pl in enumerate(planes):
+            self._planes[q].axis, self._planes[q].index = pl["axis"], pl["index"]
+            self._planes[q].component = pl.get("component", FIELD_EX)
+        c.n_planes = len(planes)
+        c.planes = self._planes
+
+    @property
+    def n_series(self) -> int:
+        """Point probes, then plane probes."""
+        return self.c.n_probes + self.c.n_planes
 
 
 def run(rc: RunConfig, setup=None, context=None) -> dict:
     """fdtd_b200_run: one full run; returns probe series, DFT and GPU time."""
     lib = load()
     c = rc.c
-    td = np.zeros((max(c.n_probes, 1), c.n_steps))
-    re = np.zeros((max(c.n_probes, 1), max(c.n_freqs, 1)))
+    ns = rc.n_series
+    td = np.zeros((max(ns, 1), c.n_steps))
+    re = np.zeros((max(ns, 1), max(c.n_freqs, 1)))
     im = np.zeros_like(re)
     res = B200Result()
     res.probe_td = _dptr(td)
@@ -427,7 +450,7 @@ def run(rc: RunConfig, setup=None, context=None) -> dict:
     status = lib.fdtd_b200_run(C.byref(c), setup, context, C.byref(res))
     if status != 0:
         raise RuntimeError(f"fdtd_b200_run failed: {last_error()}")
-    return {"td": td[: c.n_probes], "dft": (re + 1j * im)[: c.n_probes, : c.n_freqs],
+    return {"td": td[:ns], "dft": (re + 1j * im)[:ns, : c.n_freqs],
             "fs": res.sample_rate_hz, "device_ms": res.device_ms}
 
 
@@ -490,11 +513,11 @@ class Sim:
         return a.value, b.value
 
     def probes(self) -> np.ndarray:
-        c = self.rc.c
-        out = np.zeros((max(c.n_probes, 1), c.n_steps))
+        c, ns = self.rc.c, self.rc.n_series
+        out = np.zeros((max(ns, 1), c.n_steps))
         if self.lib.fdtd_b200_sim_read_probes(self.h, _dptr(out)) != 0:
             raise RuntimeError(last_error())
-        return out[: c.n_probes]
+        return out[:ns]
 
     def read_iq(self, probe: int, snr_db: float | None = None, seed: int = 0, stream: int = 0) -> np.ndarray:
         """The stage's complex64 signal of one probe, with rfsyn's AWGN when
@@ -507,12 +530,12 @@ class Sim:
         return out.view(np.complex64)
 
     def dft(self) -> np.ndarray:
-        c = self.rc.c
-        re = np.zeros((max(c.n_probes, 1), max(c.n_freqs, 1)))
+        c, ns = self.rc.c, self.rc.n_series
+        re = np.zeros((max(ns, 1), max(c.n_freqs, 1)))
         im = np.zeros_like(re)
         if self.lib.fdtd_b200_sim_dft(self.h, _dptr(re), _dptr(im)) != 0:
             raise RuntimeError(last_error())
-        return (re + 1j * im)[: c.n_probes, : c.n_freqs]
+        return (re + 1j * im)[:ns, : c.n_freqs]
 
     def field(self, component: int) -> np.ndarray:
         c = self.rc.c

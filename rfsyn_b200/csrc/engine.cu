@@ -20,6 +20,7 @@
 #include "sweep.cuh"
 #include "energy.cuh"
 #include "iq.cuh"
+#include "sphere_frac.cuh"
 
 using namespace rfb;
 
@@ -507,7 +508,7 @@ static int devscene_init(DevScene &s, const rfb_geom_t *g, const rfb_scene_image
             }
         }
         if (img->n_t3) {
-            s.t3 = dev_upload_conv(img->t3, 4 * img->n_t3, prec);
+            s.t3 = dev_upload_conv(img->t3, 5 * img->n_t3, prec);
             if (!s.t3) {
                 rfb_set_error("3x3 tensor upload failed");
                 return -1;
@@ -601,6 +602,17 @@ struct rfb_engine {
     size_t n_steps = 0, steps_done = 0;
     double *d_omega = nullptr, *d_re = nullptr, *d_im = nullptr;
     size_t dft_cap = 0;
+    // plane probes: series n_probes .. n_probes + n_planes - 1 of ts
+    int n_planes = 0;
+    PlaneDesc *d_planes = nullptr;
+    void **d_fout[2] = {nullptr, nullptr};  // per parity: the six output components, for the plane gather
+    // running DFT of every series: the bins (rad/s), t offset (steps), the
+    // per (series, bin) sums (FP64: re, im; FP32: re, im, compensations)
+    int n_freqs = 0;
+    std::vector<double> dft_freqs;
+    double dft_t_off = 0.0;
+    double *d_run_omega = nullptr;
+    void *d_acc = nullptr;
     cudaStream_t stream = nullptr, stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int own_stream = 0;
@@ -756,6 +768,16 @@ static void launch_sweep(rfb_engine *e, const Args<T> &a, int par) {
     cudaStreamWaitEvent(e->stream, e->ev_join, 0);
 }
 
+// Plane probes of the step: their means join the series before the point
+// probes advance the step counter.
+template <typename T>
+static void launch_plane_gather(rfb_engine *e, int par) {
+    if (!e->n_planes) return;
+    const int out = e->nbuf == 2 ? 1 - par : 0;
+    k_plane_gather<T><<<e->n_planes, 1024, 0, e->stream>>>(e->d_planes, e->n_planes, (const T *const *)e->d_fout[out],
+                                                          (T *)e->ts, e->n_probes, (long long)e->n_steps, e->d_step);
+}
+
 template <typename T>
 static void enqueue_step(rfb_engine *e, int par) {
     Args<T> a = engine_args<T>(e, par);
@@ -780,8 +802,19 @@ static void enqueue_step(rfb_engine *e, int par) {
     p.ts = (T *)e->ts;
     p.n_steps = (long long)e->n_steps;
     p.d_step = e->d_step;
+    launch_plane_gather<T>(e, par);
     k_probe_gather<T><<<1, 128, 0, e->stream>>>(p);
     tf_after_step<T>(e, par);
+}
+
+// The running DFT over the last `count` recorded samples of every series.
+template <typename T>
+static void launch_dft_run(rfb_engine *e, int count) {
+    const int ns = e->n_probes + e->n_planes;
+    if (!e->n_freqs || !ns) return;
+    dim3 grd((unsigned)((e->n_freqs + 127) / 128), (unsigned)ns);
+    k_dft_run<T><<<grd, 128, 0, e->stream>>>((const T *)e->ts, ns, (long long)e->n_steps, e->d_step, count,
+                                             e->n_freqs, e->d_run_omega, e->g.dt, e->dft_t_off, e->d_acc);
 }
 
 static int count_step_launches(const rfb_engine *e) {
@@ -791,6 +824,7 @@ static int count_step_launches(const rfb_engine *e) {
     if (e->scene.n_cells) n++;
     if (e->n_t3_cells) n++;
     if (e->tf_on) n += 2 + (e->tf_n_h > 0);
+    if (e->n_planes) n++;
     return n + 1;
 }
 
@@ -803,6 +837,8 @@ static int build_graph(rfb_engine *e, int par, int steps, cudaGraphExec_t *out) 
         else enqueue_step<float>(e, p);
         if (e->nbuf == 2) p ^= 1;
     }
+    if (e->prec == RFB_FP64) launch_dft_run<double>(e, steps);
+    else launch_dft_run<float>(e, steps);
     CK(cudaStreamEndCapture(e->stream, &graph));
     CK(cudaGraphInstantiate(out, graph, 0));
     cudaGraphDestroy(graph);
@@ -1246,6 +1282,11 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     dfree(e->src_val); dfree(e->src_hard);
     dfree(e->probe_cell); dfree(e->probe_comp); dfree(e->ts); dfree(e->d_step); dfree(e->d_err); dfree(e->d_energy); dfree(e->d_iq);
     dfree(e->t3_cells);
+    dfree(e->d_planes);
+    dfree(e->d_fout[0]);
+    dfree(e->d_fout[1]);
+    dfree(e->d_run_omega);
+    dfree(e->d_acc);
     dfree(e->d_omega); dfree(e->d_re); dfree(e->d_im);
     dfree(e->plan.d_int); dfree(e->plan.d_edge); dfree(e->plan.d_qe); dfree(e->plan.d_qx); dfree(e->plan.d_queue);
     dfree(e->tf_inc_e); dfree(e->tf_inc_h); dfree(e->tf_src); dfree(e->tf_h_cell); dfree(e->tf_h_comp);
@@ -1540,6 +1581,8 @@ extern "C" int rfb_engine_reset(rfb_engine_t *e) {
         CK(cudaMemsetAsync(e->tf_inc_e, 0, (size_t)e->tf_m_len * e->esz, e->stream));
         CK(cudaMemsetAsync(e->tf_inc_h, 0, (size_t)e->tf_m_len * e->esz, e->stream));
     }
+    if (e->d_acc)
+        CK(cudaMemsetAsync(e->d_acc, 0, (size_t)(e->n_probes + e->n_planes) * e->n_freqs * 4 * e->esz, e->stream));
     CK(cudaMemsetAsync(e->d_step, 0, sizeof(int), e->stream));
     e->steps_done = 0;
     e->parity = 0;
@@ -1547,6 +1590,9 @@ extern "C" int rfb_engine_reset(rfb_engine_t *e) {
 fail:
     return -1;
 }
+
+// Running-DFT launches per replayed graph (one, after its steps).
+static unsigned dft_launches(const rfb_engine *e) { return (e->n_freqs && (e->n_probes + e->n_planes)) ? 1u : 0u; }
 
 extern "C" int rfb_engine_advance(rfb_engine_t *e, size_t n) {
     if (e->steps_done + n > e->n_steps) {
@@ -1559,14 +1605,14 @@ extern "C" int rfb_engine_advance(rfb_engine_t *e, size_t n) {
         if (n >= (size_t)rfb_engine::CHUNK) {
             if (!e->gk[par] && build_graph(e, par, rfb_engine::CHUNK, &e->gk[par]) != 0) return -1;
             CK(cudaGraphLaunch(e->gk[par], e->stream));
-            g_launches += (unsigned long long)rfb_engine::CHUNK * e->launches_per_step;
+            g_launches += (unsigned long long)rfb_engine::CHUNK * e->launches_per_step + dft_launches(e);
             n -= rfb_engine::CHUNK;
             e->steps_done += rfb_engine::CHUNK;
             // CHUNK is even: parity unchanged
         } else {
             if (!e->g1[par] && build_graph(e, par, 1, &e->g1[par]) != 0) return -1;
             CK(cudaGraphLaunch(e->g1[par], e->stream));
-            g_launches += e->launches_per_step;
+            g_launches += e->launches_per_step + dft_launches(e);
             n -= 1;
             e->steps_done += 1;
             if (per_parity == 2) e->parity ^= 1;
@@ -1663,9 +1709,11 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         p.ts = (T *)e->ts;
         p.n_steps = (long long)e->n_steps;
         p.d_step = e->d_step;
+        launch_plane_gather<T>(e, par);
         k_probe_gather<T><<<1, 128, 0, e->stream>>>(p);
         tf_after_step<T>(e, par);
-        g_launches += 1 + (e->tf_on ? 2 + (e->tf_n_h > 0) : 0);
+        launch_dft_run<T>(e, 1);
+        g_launches += 1 + (e->tf_on ? 2 + (e->tf_n_h > 0) : 0) + (e->n_planes > 0) + dft_launches(e);
         CK(cudaEventRecord(ev[2], e->stream));
         CK(cudaEventSynchronize(ev[2]));
         float t1 = 0.f, t2 = 0.f;
@@ -1772,7 +1820,7 @@ extern "C" int rfb_engine_launches_per_step(rfb_engine_t *e) { return e->launche
 extern "C" int rfb_engine_read_iq(rfb_engine_t *e, int probe, int noise, double snr_linear, unsigned long long seed,
                                   unsigned long long stream, float *out) {
     const long long n = (long long)e->n_steps;
-    if (probe < 0 || probe >= e->n_probes || !out) {
+    if (probe < 0 || probe >= e->n_probes + e->n_planes || !out) {
         rfb_set_error("read_iq: no probe %d", probe);
         return -1;
     }
@@ -1846,7 +1894,7 @@ out:
 }
 
 extern "C" int rfb_engine_read_probes(rfb_engine_t *e, double *out) {
-    size_t n = (size_t)e->n_probes * e->n_steps;
+    size_t n = (size_t)(e->n_probes + e->n_planes) * e->n_steps;
     if (!n) return 0;
     CK(cudaStreamSynchronize(e->stream));
     if (check_sweep_error(e) != 0) return -1;
@@ -1862,11 +1910,144 @@ fail:
     return -1;
 }
 
+// Plane probes (axis 0..2, index, component 0..5 of ex..hz): their series
+// follow the point probes'.  Before the first step only.
+extern "C" int rfb_engine_set_planes(rfb_engine_t *e, size_t n, const int *axis_index_comp) {
+    std::vector<PlaneDesc> pd(n);
+    const int nn[3] = {e->g.nx, e->g.ny, e->g.nz};
+    const long long st[3] = {(long long)(e->g.ny + 1) * e->pitch, e->pitch, 1};
+    const size_t ns = (size_t)e->n_probes + n;
+    if (e->steps_done) {
+        rfb_set_error("plane probes must be set before the first step");
+        return -1;
+    }
+    for (size_t q = 0; q < n; q++) {
+        const int a = axis_index_comp[3 * q], idx = axis_index_comp[3 * q + 1], c = axis_index_comp[3 * q + 2];
+        if (a < 0 || a > 2 || idx < 0 || idx > nn[a] || c < 0 || c > 5) {
+            rfb_set_error("plane probe %zu: axis %d, index %d, component %d out of range", q, a, idx, c);
+            return -1;
+        }
+        const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
+        pd[q] = PlaneDesc{(long long)idx * st[a], st[u], st[v], nn[u], nn[v], c};
+    }
+    for (int q = 0; q < 2; q++) {
+        if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
+        if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
+        e->g1[q] = e->gk[q] = nullptr;
+    }
+    dfree(e->d_planes);
+    e->d_planes = nullptr;
+    e->n_planes = 0;
+    if (n) {
+        e->d_planes = dev_copy(pd.data(), n);
+        if (!e->d_planes) {
+            rfb_set_error("plane probe upload failed");
+            return -1;
+        }
+        for (int b = 0; b < e->nbuf; b++) {
+            void *ptrs[6];
+            for (int c = 0; c < 6; c++) ptrs[c] = e->fld[e->nbuf == 2 ? b : 0][c];
+            dfree(e->d_fout[b]);
+            e->d_fout[b] = dev_copy(ptrs, 6);
+            if (!e->d_fout[b]) {
+                rfb_set_error("plane probe upload failed");
+                return -1;
+            }
+        }
+        if (e->nbuf == 1) e->d_fout[1] = nullptr;
+        // the pass over stored series sizes its buffers by the series count
+        dfree(e->d_omega); dfree(e->d_re); dfree(e->d_im);
+        e->d_omega = e->d_re = e->d_im = nullptr;
+        e->dft_cap = 0;
+        // series of every probe, point and plane
+        dfree(e->ts);
+        e->ts = nullptr;
+        CK(dmalloc(&e->ts, ns * e->n_steps * e->esz));
+        CK(cudaMemset(e->ts, 0, ns * e->n_steps * e->esz));
+    }
+    e->n_planes = (int)n;
+    e->launches_per_step = count_step_launches(e);
+    if (e->n_freqs) {
+        // the sums follow the series: resize them
+        std::vector<double> f = e->dft_freqs;
+        return rfb_engine_set_dft(e, f.size(), f.data(), e->dft_t_off);
+    }
+    return 0;
+fail:
+    return -1;
+}
+
+// Bins of the running DFT (Hz) and the time offset of sample n, t = (n +
+// t_off) dt.  Before the first step only; 0 bins: no running DFT.
+extern "C" int rfb_engine_set_dft(rfb_engine_t *e, size_t n_freqs, const double *freqs_hz, double t_offset_steps) {
+    const size_t ns = (size_t)e->n_probes + e->n_planes;
+    if (e->steps_done) {
+        rfb_set_error("DFT bins must be set before the first step");
+        return -1;
+    }
+    for (int q = 0; q < 2; q++) {
+        if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
+        if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
+        e->g1[q] = e->gk[q] = nullptr;
+    }
+    dfree(e->d_run_omega);
+    dfree(e->d_acc);
+    e->d_run_omega = nullptr;
+    e->d_acc = nullptr;
+    e->n_freqs = 0;
+    e->dft_freqs.assign(freqs_hz, freqs_hz + n_freqs);
+    e->dft_t_off = t_offset_steps;
+    if (n_freqs && ns) {
+        std::vector<double> om(n_freqs);
+        for (size_t f = 0; f < n_freqs; f++) om[f] = 2.0 * 3.14159265358979323846 * freqs_hz[f];
+        e->d_run_omega = dev_copy(om.data(), n_freqs);
+        if (!e->d_run_omega) {
+            rfb_set_error("DFT bin upload failed");
+            return -1;
+        }
+        CK(dmalloc(&e->d_acc, ns * n_freqs * 4 * e->esz));
+        CK(cudaMemset(e->d_acc, 0, ns * n_freqs * 4 * e->esz));
+        e->n_freqs = (int)n_freqs;
+    }
+    return 0;
+fail:
+    return -1;
+}
+
+// The running sums, accumulated with the steps.
+static int read_running_dft(rfb_engine *e, size_t nout, double *out_re, double *out_im) {
+    CK(cudaStreamSynchronize(e->stream));
+    if (check_sweep_error(e) != 0) return -1;
+    if (e->prec == RFB_FP64) {
+        std::vector<double> acc(2 * nout);
+        CK(cudaMemcpy(acc.data(), e->d_acc, 2 * nout * sizeof(double), cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < nout; q++) {
+            out_re[q] = acc[2 * q];
+            out_im[q] = acc[2 * q + 1];
+        }
+    } else {
+        std::vector<float> acc(4 * nout);
+        CK(cudaMemcpy(acc.data(), e->d_acc, 4 * nout * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < nout; q++) {
+            out_re[q] = acc[4 * q];
+            out_im[q] = acc[4 * q + 1];
+        }
+    }
+    return 0;
+fail:
+    return -1;
+}
+
 extern "C" int rfb_engine_probe_dft(rfb_engine_t *e, size_t n_freqs, const double *freqs_hz, double t_offset_steps,
                                     double *out_re, double *out_im) {
-    if (!e->n_probes || !n_freqs) return 0;
+    const size_t n_series = (size_t)e->n_probes + e->n_planes;
+    if (!n_series || !n_freqs) return 0;
+    if ((size_t)e->n_freqs == n_freqs && e->dft_t_off == t_offset_steps &&
+        memcmp(e->dft_freqs.data(), freqs_hz, n_freqs * sizeof(double)) == 0)
+        return read_running_dft(e, n_series * n_freqs, out_re, out_im);
+    // other bins: a pass over the stored series
     std::vector<double> om(n_freqs);
-    const size_t nout = (size_t)e->n_probes * n_freqs;
+    const size_t nout = n_series * n_freqs;
     for (size_t f = 0; f < n_freqs; f++) om[f] = 2.0 * 3.14159265358979323846 * freqs_hz[f];
     if (e->dft_cap < n_freqs || !e->d_re) {
         dfree(e->d_omega); dfree(e->d_re); dfree(e->d_im);
@@ -1878,13 +2059,13 @@ extern "C" int rfb_engine_probe_dft(rfb_engine_t *e, size_t n_freqs, const doubl
     }
     CK(cudaMemcpyAsync(e->d_omega, om.data(), n_freqs * 8, cudaMemcpyHostToDevice, e->stream));
     {
-        dim3 grd((unsigned)((n_freqs + 127) / 128), e->n_probes);
+        dim3 grd((unsigned)((n_freqs + 127) / 128), (unsigned)n_series);
         if (e->prec == RFB_FP64)
-            k_probe_dft<double><<<grd, 128, 0, e->stream>>>((const double *)e->ts, (long long)e->n_steps, e->n_probes,
+            k_probe_dft<double><<<grd, 128, 0, e->stream>>>((const double *)e->ts, (long long)e->n_steps, (int)n_series,
                                                             (int)e->steps_done, (int)n_freqs, e->d_omega, e->g.dt,
                                                             t_offset_steps, e->d_re, e->d_im);
         else
-            k_probe_dft<float><<<grd, 128, 0, e->stream>>>((const float *)e->ts, (long long)e->n_steps, e->n_probes,
+            k_probe_dft<float><<<grd, 128, 0, e->stream>>>((const float *)e->ts, (long long)e->n_steps, (int)n_series,
                                                            (int)e->steps_done, (int)n_freqs, e->d_omega, e->g.dt,
                                                            t_offset_steps, e->d_re, e->d_im);
         g_launches++;
@@ -1921,9 +2102,6 @@ fail:
 // ---------------------------------------------------------------------------
 // Sphere fill fractions (FP64 subpixel construction on the GPU)
 // ---------------------------------------------------------------------------
-// Unit cube around the sample: exact 0 / 1 when the half diagonal sqrt(3)/2
-// clears the surface, else the share of an 8^3 lattice of points at offsets
-// (a + 1/2)/8 - 1/2 whose squared distance is <= r^2.
 __global__ void k_sphere_fractions(double cx, double cy, double cz, double r, int i0, int j0, int k0, int ni, int nj,
                                    int nk, double *f, double *n2) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1934,42 +2112,11 @@ __global__ void k_sphere_fractions(double cx, double cy, double cz, double r, in
     const int k = k0 + (int)(cell % nk);
     const int j = j0 + (int)((cell / nk) % nj);
     const int i = i0 + (int)(cell / ((long long)nk * nj));
-    const double x = __dadd_rn((double)i, comp == 0 ? 0.5 : 0.0);
-    const double y = __dadd_rn((double)j, comp == 1 ? 0.5 : 0.0);
-    const double z = __dadd_rn((double)k, comp == 2 ? 0.5 : 0.0);
-    const double dx = __dsub_rn(x, cx), dy = __dsub_rn(y, cy), dz = __dsub_rn(z, cz);
-    const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-    const double cc = comp == 0 ? dx : comp == 1 ? dy : dz;
-    double nn = 0.0;
-    if (d > 0.0) {
-        const double u = __ddiv_rn(cc, d);
-        nn = __dmul_rn(u, u);
-    }
-    const double h = 0.8660254037844386;
-    double frac;
-    if (__dadd_rn(d, h) <= r) {
-        frac = 1.0;
-    } else if (__dsub_rn(d, h) >= r) {
-        frac = 0.0;
-    } else {
-        const double r2 = __dmul_rn(r, r);
-        int count = 0;
-        for (int a = 0; a < 8; a++) {
-            const double px = __dsub_rn(__dadd_rn(x, __dsub_rn(__ddiv_rn(__dadd_rn((double)a, 0.5), 8.0), 0.5)), cx);
-            for (int b = 0; b < 8; b++) {
-                const double py = __dsub_rn(__dadd_rn(y, __dsub_rn(__ddiv_rn(__dadd_rn((double)b, 0.5), 8.0), 0.5)), cy);
-                for (int e = 0; e < 8; e++) {
-                    const double pz =
-                        __dsub_rn(__dadd_rn(z, __dsub_rn(__ddiv_rn(__dadd_rn((double)e, 0.5), 8.0), 0.5)), cz);
-                    const double q = __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz));
-                    count += q <= r2;
-                }
-            }
-        }
-        frac = __ddiv_rn((double)count, 512.0);
-    }
-    f[t] = frac;
-    n2[t] = nn;
+    double p[3];
+    rfb_sample_pos(i, j, k, comp, p);
+    double nrm[3];
+    f[t] = rfb_sphere_cube_fraction(p, cx, cy, cz, r, nrm);
+    n2[t] = __dmul_rn(nrm[comp], nrm[comp]);
 }
 
 // Sphere set-up runs once per sphere of every scene (tens of thousands of

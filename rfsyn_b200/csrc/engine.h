@@ -87,7 +87,7 @@ typedef struct {
      * with D_b the curl difference of component b at its own sample and
      * <D_b> its mean over the four b samples around the E_c sample. */
     size_t n_t3;
-    const double *t3;           /* 4 per record                                */
+    const double *t3;           /* 5 per record                                */
 
     /* ADE records (dispersive cells), see rfb_ade_desc in the engine. */
     size_t n_ade;
@@ -120,6 +120,13 @@ rfb_engine_t *rfb_engine_create(const rfb_geom_t *geom, int precision, int sched
                                 size_t n_probes, const rfb_probe_desc_t *probes,
                                 size_t n_steps, void *stream);
 void rfb_engine_destroy(rfb_engine_t *e);
+/* Plane probes, n triples (axis 0..2, index, component 0..5 = ex..hz): each
+ * records the mean of the component over the whole grid plane every step,
+ * as series n_probes .. n_probes + n - 1.  Bins (Hz) of the running DFT of
+ * every series, accumulated with the steps, sample n at t = (n + t_off) dt.
+ * Both before the first step. */
+int rfb_engine_set_planes(rfb_engine_t *e, size_t n, const int *axis_index_comp);
+int rfb_engine_set_dft(rfb_engine_t *e, size_t n_freqs, const double *freqs_hz, double t_offset_steps);
 /* An engine for one scene of a batch (FUSED schedule): device state only;
  * the batch builds the sweep plans and owns the kernels' launches.  `stream`
  * must be the batch's stream. */
@@ -250,6 +257,19 @@ int rfb_engine_energy(rfb_engine_t *e, double dt, double dx, int x_lo, int x_hi,
  * GPU, every operation rounded separately (bit-identical to the oracle). */
 int rfb_sphere_fractions(const double centre[3], double radius, int i0, int j0, int k0, int ni, int nj, int nk,
                          double *f, double *n2);
+
+/* Smoothed permittivity of cut cells, FP64 on the GPU (smooth.cu).
+ * rfb_sphere_rows: for every cell of the box as rfb_sphere_fractions, the
+ * fill fraction f[3 cell + c] of each E sample and row c of the smoothed
+ * relative inverse permittivity rows[9 cell + 3 c + b] between the cell's
+ * isotropic background eps_bg[cell] and eps_in, along the sphere's normal.
+ * rfb_slab_rows: the same for n listed samples ijkc[4 s ..] = (i, j, k, c)
+ * against the slab |(x - point) . u| <= thickness / 2 (u unit) holding the
+ * 3x3 eps_in: f[s], rows[3 s + b]. */
+int rfb_sphere_rows(const double centre[3], double radius, double eps_in, int i0, int j0, int k0, int ni, int nj,
+                    int nk, const double *eps_bg, double *f, double *rows);
+int rfb_slab_rows(const double point[3], const double unit_normal[3], double thickness, const double eps_in[9],
+                  const int *ijkc, const double *eps_bg, int n, double *f, double *rows);
 
 /* Last error message of the calling thread ("" if none). */
 const char *rfb_last_error(void);

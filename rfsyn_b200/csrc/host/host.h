@@ -49,7 +49,7 @@ typedef struct {
     double *t_m11, *t_scale, *t_w;
     int32_t *t_main, *t_nq, *t_uv, *t_sign;
     double *ade_c;
-    double *t3;             /* 3x3 samples: 4 doubles per record */
+    double *t3;             /* 3x3 samples: 5 doubles per record */
 } rfb_scene_build_t;
 
 void rfb_ade_record(const double *model, double dt, double dx, double *out);

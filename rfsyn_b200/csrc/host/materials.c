@@ -172,7 +172,7 @@ struct materials {
     omap_t scalar;  /* key -> (Ca, Cb) */
     omap_t tensor;  /* key -> (m11, m12, m22, scale) */
     omap_t disp;    /* key -> dispersive model (DISP_W doubles) */
-    omap_t tensor3; /* key -> row of the 3x3 relative inverse permittivity (3 doubles) */
+    omap_t tensor3; /* key -> row of the 3x3 relative inverse permittivity, then sigma (4 doubles) */
     unsigned long version;
     /* device copy for the step-wise API */
     rfb_scene_dev_t *dev;
@@ -240,7 +240,7 @@ materials_t *materials_create(const fdtd_grid_t *g) {
     omap_init(&mat->scalar, 2);
     omap_init(&mat->tensor, 4);
     omap_init(&mat->disp, DISP_W);
-    omap_init(&mat->tensor3, 3);
+    omap_init(&mat->tensor3, 4);
     mat->ids = calloc(total, 1);
     mat->touched = calloc(total, 1);
     if (!mat->ids || !mat->touched) {
@@ -519,7 +519,8 @@ int fdtd_b200_materials_set_component_tensor3(materials_t *mat, const fdtd_grid_
     for (int q = 0; q < 3; q++)
         if (!isfinite(row[q])) return -1;
     if (!(row[c] > 0.0)) return -1;
-    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, row) != 0) return -1;
+    const double v[4] = {row[0], row[1], row[2], 0.0};
+    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, v) != 0) return -1;
     mat->version++;
     return 0;
 }
@@ -575,10 +576,11 @@ int fdtd_b200_materials_set_tensor3_slab(materials_t *mat, const fdtd_grid_t *g,
                             u[0] * (p[0] - point[0]) + u[1] * (p[1] - point[1]) + u[2] * (p[2] - point[2]);
                         if (fabs(d) > half) continue;
                         if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) continue;
+                        const double v[4] = {m[3 * c], m[3 * c + 1], m[3 * c + 2], 0.0};
                         if (pass == 0) {
                             count++;
-                        } else if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c,
-                                            m + 3 * c) != 0) {
+                        } else if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, v) !=
+                                   0) {
                             return -1;
                         }
                     }
@@ -587,6 +589,124 @@ int fdtd_b200_materials_set_tensor3_slab(materials_t *mat, const fdtd_grid_t *g,
     }
     mat->version++;
     return 0;
+}
+
+/* The slab with subpixel smoothing of its faces.  Every valid E sample
+ * (component_valid, tensor3_margin_ok) whose unit cube lies inside the slab
+ * -- |d| + r <= thickness / 2, d the sample's signed distance from the mid
+ * plane and r = (|u0| + |u1| + |u2|) / 2 the cube's reach along the normal u
+ * -- gets the row of eps_r^-1 as the staircased slab gives it; every sample
+ * whose cube the faces may cut (|d| - r <= thickness / 2 < |d| + r) gets, when
+ * its fill fraction f (8^3 lattice) is positive, the row of the smoothed
+ * inverse permittivity between the cell's table material (isotropic, the
+ * background) and eps_r along u, with sigma (1 - f) sigma_background; both
+ * computed on the GPU in FP64 (rfb_slab_rows).  Samples outside stay as
+ * they are. */
+int fdtd_b200_materials_set_tensor3_slab_smoothed(materials_t *mat, const fdtd_grid_t *g, const double point[3],
+                                                  const double normal[3], double thickness, const double eps_r[9]) {
+    double m[9];
+    if (!point || !normal || !eps_r || !(thickness > 0.0) || rfb_spd3_inverse(eps_r, m) != 0) return -1;
+    if (!materials_matches(mat, g)) return -1;
+    const double nn = sqrt(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+    if (!(nn > 0.0)) return -1;
+    const double u[3] = {normal[0] / nn, normal[1] / nn, normal[2] / nn};
+    const size_t n[3] = {g->nx, g->ny, g->nz};
+    size_t lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        lo[a] = ((g->periodic_axes >> a) & 1u) ? 0 : 1;
+        hi[a] = n[a];
+    }
+    const double half = 0.5 * thickness;
+    const double reach = 0.5 * ((fabs(u[0]) + fabs(u[1])) + fabs(u[2]));
+    /* column k ranges as the staircased slab, widened by the cube's reach */
+    const double slack = reach + reach;
+    size_t n_in = 0, cap_in = 1024, n_cut = 0, cap_cut = 1024;
+    uint64_t *in_keys = malloc(cap_in * sizeof(uint64_t));
+    int32_t *cut = malloc(4 * cap_cut * sizeof(int32_t));
+    double *cut_bg = NULL, *f = NULL, *rows = NULL;
+    int rc = -1, gpu_failed = 0;
+    if (!in_keys || !cut) goto out;
+    for (size_t i = lo[0]; i < hi[0]; i++)
+        for (size_t j = lo[1]; j < hi[1]; j++) {
+            size_t ka = lo[2], kb = hi[2];
+            if (fabs(u[2]) > 1e-9) {
+                const double r0 = u[0] * ((double)i - point[0]) + u[1] * ((double)j - point[1]) - u[2] * point[2];
+                double a = (-half - slack - r0) / u[2], b = (half + slack - r0) / u[2];
+                if (a > b) { const double t = a; a = b; b = t; }
+                a = floor(a) - 1.0;
+                b = ceil(b) + 2.0;
+                if (a > (double)ka) ka = a >= (double)hi[2] ? hi[2] : (size_t)a;
+                if (b < (double)kb) kb = b <= (double)ka ? ka : (size_t)b;
+            }
+            for (size_t k = ka; k < kb; k++)
+                for (int c = 0; c < 3; c++) {
+                    double p[3] = {(double)i, (double)j, (double)k};
+                    p[c] += 0.5;
+                    /* the device's operation order (sphere_frac.cuh) */
+                    const double d = (u[0] * (p[0] - point[0]) + u[1] * (p[1] - point[1])) + u[2] * (p[2] - point[2]);
+                    const double ad = fabs(d);
+                    if (ad - reach > half) continue;
+                    if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) continue;
+                    const uint64_t key = (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c;
+                    if (ad + reach <= half) {
+                        if (n_in == cap_in) {
+                            cap_in *= 2;
+                            uint64_t *nk2 = realloc(in_keys, cap_in * sizeof(uint64_t));
+                            if (!nk2) goto out;
+                            in_keys = nk2;
+                        }
+                        in_keys[n_in++] = key;
+                    } else {
+                        if (n_cut == cap_cut) {
+                            cap_cut *= 2;
+                            int32_t *nc = realloc(cut, 4 * cap_cut * sizeof(int32_t));
+                            if (!nc) goto out;
+                            cut = nc;
+                        }
+                        cut[4 * n_cut] = (int32_t)i;
+                        cut[4 * n_cut + 1] = (int32_t)j;
+                        cut[4 * n_cut + 2] = (int32_t)k;
+                        cut[4 * n_cut + 3] = c;
+                        n_cut++;
+                    }
+                }
+        }
+    if (n_cut > (size_t)INT32_MAX) goto out;
+    cut_bg = malloc((n_cut + 1) * sizeof(double));
+    f = malloc((n_cut + 1) * sizeof(double));
+    rows = malloc((3 * n_cut + 1) * sizeof(double));
+    if (!cut_bg || !f || !rows) goto out;
+    for (size_t q = 0; q < n_cut; q++) {
+        const size_t w = fdtd_index(g, (size_t)cut[4 * q], (size_t)cut[4 * q + 1], (size_t)cut[4 * q + 2]);
+        cut_bg[q] = mat->table[mat->ids[w]].eps_r;
+    }
+    if (rfb_slab_rows(point, u, thickness, eps_r, cut, cut_bg, (int)n_cut, f, rows) != 0) {
+        gpu_failed = 1;
+        goto out;
+    }
+    if (omap_reserve(&mat->tensor3, n_in + n_cut) != 0) goto out;
+    for (size_t q = 0; q < n_in; q++) {
+        const int c = (int)(in_keys[q] % 3);
+        const double v[4] = {m[3 * c], m[3 * c + 1], m[3 * c + 2], 0.0};
+        if (omap_put(&mat->tensor3, in_keys[q], v) != 0) goto out;
+    }
+    for (size_t q = 0; q < n_cut; q++) {
+        if (!(f[q] > 0.0)) continue;
+        const size_t w = fdtd_index(g, (size_t)cut[4 * q], (size_t)cut[4 * q + 1], (size_t)cut[4 * q + 2]);
+        const double v[4] = {rows[3 * q], rows[3 * q + 1], rows[3 * q + 2],
+                             (1.0 - f[q]) * mat->table[mat->ids[w]].sigma};
+        if (omap_put(&mat->tensor3, (uint64_t)w * 3 + (uint64_t)cut[4 * q + 3], v) != 0) goto out;
+    }
+    rc = 0;
+out:
+    if (rc != 0 && !gpu_failed) rfb_set_error("smoothed slab: out of host memory");
+    free(in_keys);
+    free(cut);
+    free(cut_bg);
+    free(f);
+    free(rows);
+    mat->version++;
+    return rc;
 }
 
 int fdtd_b200_materials_set_dispersive_box(materials_t *mat, const fdtd_grid_t *g, size_t i0, size_t i1, size_t j0,
@@ -611,7 +731,7 @@ int fdtd_b200_materials_get_tensor3(const materials_t *mat, const fdtd_grid_t *g
     if (c < 0 || c > 2 || !row || !materials_matches(mat, g) || !component_valid(g, c, i, j, k)) return -1;
     long long q = omap_find(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c);
     if (q < 0) return 1;
-    memcpy(row, mat->tensor3.vals + (size_t)q * 3, 3 * sizeof(double));
+    memcpy(row, mat->tensor3.vals + (size_t)q * 4, 3 * sizeof(double));
     return 0;
 }
 
@@ -649,7 +769,8 @@ int fdtd_b200_materials_set_tensor3_box(materials_t *mat, const fdtd_grid_t *g, 
             for (size_t k = k0; k < k1; k++)
                 for (int c = 0; c < 3; c++) {
                     if (!component_valid(g, c, i, j, k) || !tensor3_margin_ok(g, i, j, k)) return -1;
-                    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, m + 3 * c) != 0)
+                    const double v[4] = {m[3 * c], m[3 * c + 1], m[3 * c + 2], 0.0};
+                    if (omap_put(&mat->tensor3, (uint64_t)fdtd_index(g, i, j, k) * 3 + (uint64_t)c, v) != 0)
                         return -1;
                 }
     mat->version++;
@@ -736,8 +857,28 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
         if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
         const int ni = (int)(hi[0] - lo[0] + 1), nj = (int)(hi[1] - lo[1] + 1), nk = (int)(hi[2] - lo[2] + 1);
         const size_t ncell = (size_t)ni * nj * nk;
-        double *f = malloc(3 * ncell * sizeof(double)), *n2 = malloc(3 * ncell * sizeof(double));
-        if (!f || !n2 || rfb_sphere_fractions(cen, sp->radius, (int)lo[0], (int)lo[1], (int)lo[2], ni, nj, nk, f, n2)) {
+        /* smoothing 2 (full tensor) on a plain dielectric: fractions and the
+         * rows of the smoothed inverse permittivity against each cell's
+         * table material, from the GPU; otherwise fractions and squared
+         * normal components */
+        const int full = smoothing == 2 && !sp->model;
+        double *f = malloc(3 * ncell * sizeof(double)), *n2 = malloc((full ? 9 : 3) * ncell * sizeof(double));
+        double *ebg = full ? malloc(ncell * sizeof(double)) : NULL;
+        int frc = !f || !n2 || (full && !ebg);
+        if (!frc && full) {
+            for (int di = 0; di < ni; di++)
+                for (int dj = 0; dj < nj; dj++)
+                    for (int dk = 0; dk < nk; dk++)
+                        ebg[((size_t)di * nj + (size_t)dj) * nk + (size_t)dk] =
+                            mat->table[mat->ids[fdtd_index(g, (size_t)(lo[0] + di), (size_t)(lo[1] + dj),
+                                                            (size_t)(lo[2] + dk))]].eps_r;
+            frc = rfb_sphere_rows(cen, sp->radius, sp->eps_r, (int)lo[0], (int)lo[1], (int)lo[2], ni, nj, nk, ebg, f,
+                                  n2);
+        } else if (!frc) {
+            frc = rfb_sphere_fractions(cen, sp->radius, (int)lo[0], (int)lo[1], (int)lo[2], ni, nj, nk, f, n2);
+        }
+        free(ebg);
+        if (frc) {
             free(f);
             free(n2);
             return -1;
@@ -747,7 +888,7 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                 for (int dk = 0; dk < nk; dk++) {
                     const size_t i = (size_t)(lo[0] + di), j = (size_t)(lo[1] + dj), k = (size_t)(lo[2] + dk);
                     const size_t cell = ((size_t)di * nj + (size_t)dj) * nk + (size_t)dk;
-                    const double *fc = f + 3 * cell, *nc = n2 + 3 * cell;
+                    const double *fc = f + 3 * cell, *nc = n2 + (full ? 9 : 3) * cell;
                     int valid[3];
                     for (int c = 0; c < 3; c++) valid[c] = sample_valid(g, c, i, j, k);
                     const size_t w = fdtd_index(g, i, j, k);
@@ -756,6 +897,7 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                             for (int c = 0; c < 3; c++) {
                                 omap_del(&mat->scalar, (uint64_t)w * 3 + (uint64_t)c);
                                 omap_del(&mat->disp, (uint64_t)w * 3 + (uint64_t)c);
+                                omap_del(&mat->tensor3, (uint64_t)w * 3 + (uint64_t)c);
                             }
                             for (int c = 0; c < 2; c++) omap_del(&mat->tensor, (uint64_t)w * 3 + (uint64_t)c);
                         }
@@ -775,7 +917,22 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                             continue;
                         }
                         double eps_c, sig_c;
-                        if (!smoothing || fc[c] == 1.0) {
+                        if (full && fc[c] < 1.0) {
+                            /* the row of the smoothed tensor where the 3x3
+                             * update may run, else its diagonal */
+                            const double *row = nc + 3 * c;
+                            const double eb = mat->table[mat->ids[w]].eps_r, sb = mat->table[mat->ids[w]].sigma;
+                            sig_c = fc[c] * sp->sigma + (1.0 - fc[c]) * sb;
+                            if (tensor3_margin_ok(g, i, j, k)) {
+                                const double v[4] = {row[0], row[1], row[2], sig_c};
+                                if (omap_put(&mat->tensor3, key, v) != 0) goto oom;
+                                omap_del(&mat->scalar, key);
+                                omap_del(&mat->disp, key);
+                                if (c < 2) omap_del(&mat->tensor, key);
+                                continue;
+                            }
+                            eps_c = row[c] > 0.0 ? 1.0 / row[c] : eb;
+                        } else if (!smoothing || fc[c] == 1.0) {
                             if (fc[c] < 0.5) continue;
                             eps_c = sp->eps_r;
                             sig_c = sp->sigma;
@@ -793,6 +950,7 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                         double v[2] = {co.Ca, co.Cb};
                         if (omap_put(&mat->scalar, key, v) != 0) goto oom;
                         omap_del(&mat->disp, key);
+                        omap_del(&mat->tensor3, key);
                     }
                 }
         free(f);
@@ -1076,7 +1234,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     out->t_nq = calloc(tcap, sizeof(int32_t));
     out->t_uv = calloc(16 * tcap, sizeof(int32_t));
     out->t_sign = calloc(tcap, sizeof(int32_t));
-    out->t3 = malloc((4 * mat->tensor3.count + 4) * sizeof(double));
+    out->t3 = malloc((5 * mat->tensor3.count + 5) * sizeof(double));
     if (!out->cell_ijk || !out->kind || !out->ca || !out->cb || !out->tix || !out->src || !out->aix || !out->t_m11 ||
         !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign || !out->t3)
         goto oom;
@@ -1110,13 +1268,21 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
             }
             long long t3 = omap_find(&mat->tensor3, (uint64_t)idx * 3 + (uint64_t)c);
             if (t3 >= 0) {
-                /* full 3x3 sample: its row of eps_r^-1 and dt / (eps0 dx) */
-                const double *row = mat->tensor3.vals + (size_t)t3 * 3;
-                double *rec = out->t3 + 4 * nt3;
+                /* full 3x3 sample: its row of eps_r^-1, then the update's
+                 * coefficients E+ = ca E + s value with the loss of sigma
+                 * taken at the component's own permittivity 1/m_cc, as
+                 * make_coeff takes it for a scalar sample:
+                 * s = dt/(eps0 dx) / (1 + loss), ca = (1 - loss)/(1 + loss),
+                 * loss = sigma dt / (2 eps0 / m_cc); lossless: s = dt/(eps0
+                 * dx), ca = 1 */
+                const double *row = mat->tensor3.vals + (size_t)t3 * 4;
+                double *rec = out->t3 + 5 * nt3;
                 rec[0] = row[0];
                 rec[1] = row[1];
                 rec[2] = row[2];
-                rec[3] = mat->dt / (EPS0 * mat->dx);
+                const double loss = (row[3] * mat->dt) / (2.0 * (EPS0 / row[c]));
+                rec[3] = (mat->dt / (EPS0 * mat->dx)) / (1.0 + loss);
+                rec[4] = (1.0 - loss) / (1.0 + loss);
                 out->kind[e] = RFB_LK_TENSOR3;
                 out->tix[e] = (int32_t)nt3++;
                 continue;

@@ -409,6 +409,26 @@ static fdtd_b200_sim_t *sim_create(const fdtd_b200_config_t *cfg, fdtd_material_
     }
     if (!sim->eng) goto fail;
     rfb_trace("create: engine", t_phase);
+    if (cfg->n_planes) {
+        if (member) { rfb_set_error("plane probes are not supported in batches"); goto fail; }
+        if (!cfg->planes) { rfb_set_error("n_planes without planes"); goto fail; }
+        int *aic = malloc(3 * cfg->n_planes * sizeof(int));
+        if (!aic) { rfb_set_error("out of host memory"); goto fail; }
+        for (size_t q = 0; q < cfg->n_planes; q++) {
+            aic[3 * q] = cfg->planes[q].axis;
+            aic[3 * q + 1] = cfg->planes[q].index > (size_t)INT32_MAX ? -1 : (int)cfg->planes[q].index;
+            aic[3 * q + 2] = (int)cfg->planes[q].component;
+        }
+        const int prc = rfb_engine_set_planes(sim->eng, cfg->n_planes, aic);
+        free(aic);
+        if (prc != 0) goto fail;
+        sim->n_probes += cfg->n_planes;
+    }
+    /* the probe spectra accumulate with the steps (sessions; a batch's
+     * scenes transform their stored series when read) */
+    if (!member && cfg->n_freqs &&
+        rfb_engine_set_dft(sim->eng, cfg->n_freqs, cfg->freqs_hz, cfg->dft_time_offset_steps) != 0)
+        goto fail;
     if (cfg->plane_wave) {
         rfb_tfsf_desc_t td;
         memset(&td, 0, sizeof td);

@@ -80,7 +80,7 @@ struct Args {
     T *ade_s;                // 5 state values per list entry: J0 J1 J0- J1- E-
     const T *t_m11, *t_scale, *t_w;
     const int *t_main, *t_nq, *t_uv, *t_sign;
-    const T *t3;             // 3x3 samples: row of eps_r^-1, then dt / (eps0 dx)
+    const T *t3;             // 3x3 samples: row of eps_r^-1, then s and ca of E+ = ca E + s value
     // plane-wave boundary: per list entry its first correction term (-1:
     // none) and count; terms coef * (w0 H1D[idx] + w1 H1D[idx + 1])
     const int *tf_first, *tf_count, *tf_idx;
@@ -287,9 +287,9 @@ __device__ __forceinline__ T e_ade(const Args<T> &a, int e, int comp, int i, int
 }
 
 // Full 3x3 sample of component c at (i, j, k), record r = (m_c0, m_c1, m_c2,
-// s): value = m_cc D_c, then for b = 0, 1, 2 (b != c) value += m_cb (0.25
+// s, ca): value = m_cc D_c, then for b = 0, 1, 2 (b != c) value += m_cb (0.25
 // (((D_b(w) + D_b(w + e_c)) + D_b(w - e_b)) + D_b(w + e_c - e_b))); the
-// result is E + s value.  D_b(p) is the curl difference of E component b
+// result is ca E + s value (a lossless sample has ca = 1, s = dt/(eps0 dx)).  D_b(p) is the curl difference of E component b
 // from the advanced H, (H_{b+2}(p) - H_{b+2}(p - e_{b+1})) - (H_{b+1}(p) -
 // H_{b+1}(p - e_{b+2})), the unstretched terms of the E update
 // (materials.c:920-1059).  Neighbours wrap on periodic axes only (the host
@@ -326,7 +326,7 @@ __device__ __forceinline__ T e_tensor3(const Args<T> &a, const T *r, int c, int 
                         curl_at(b, c1 + back, p3));
         value = xa(value, xm(r[b], xm(T(0.25), s4)));
     }
-    return xa(v, xm(r[3], value));
+    return xa(xm(r[4], v), xm(r[3], value));
 }
 
 // The three components of a cell whose samples are all 3x3 samples (no
@@ -357,7 +357,7 @@ __device__ __forceinline__ void t3_cell(const Args<T> &a, int cell) {
         dm[b] = curl_at(b, c0 + back[b], p2);
     }
     for (int c = 0; c < 3; c++) {
-        const T *r = a.t3 + 4 * (long long)a.l_tix[3 * cell + c];
+        const T *r = a.t3 + 5 * (long long)a.l_tix[3 * cell + c];
         T value = xm(r[c], dw[c]);
         const bool wrap = ((a.per >> c) & 1u) && p0[c] + 1 == n[c];
         int p1[3] = {i, j, k};
@@ -370,7 +370,7 @@ __device__ __forceinline__ void t3_cell(const Args<T> &a, int cell) {
             const T s4 = xa(xa(xa(dw[b], curl_at(b, c1, p1)), dm[b]), curl_at(b, c1 + back[b], p3));
             value = xa(value, xm(r[b], xm(T(0.25), s4)));
         }
-        a.Eo[c][c0] = xa(a.E[c][c0], xm(r[3], value));
+        a.Eo[c][c0] = xa(xm(r[4], a.E[c][c0]), xm(r[3], value));
     }
 }
 
@@ -419,7 +419,7 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
         v = e_ade(a, e, comp, i, j, k, v);
     } else if (kind == 4) {
         // full 3x3 anisotropic sample
-        v = e_tensor3(a, a.t3 + 4 * (long long)a.l_tix[e], comp, i, j, k, v);
+        v = e_tensor3(a, a.t3 + 5 * (long long)a.l_tix[e], comp, i, j, k, v);
     }
     if (a.tf_first) {
         // a sample next to the total-field / scattered-field boundary
@@ -516,6 +516,106 @@ __global__ void k_probe_gather(ProbeArgs<T> p) {
             p.ts[(long long)q * p.n_steps + n] = p.F[p.comp[q]][p.cell[q]];
     __syncthreads();
     if (threadIdx.x == 0) *p.d_step = n + 1;
+}
+
+// ---- plane probes ------------------------------------------------------------
+// Sample n of a plane probe is the mean of one field component over a whole
+// grid plane (axis a at index q: every (u, v) of the other two axes, u < n_u,
+// v < n_v): for a periodic cell at normal incidence, the amplitude of the
+// specular (zeroth-order) reflected or transmitted wave.  One block per
+// plane; each thread sums its points in FP64 in a fixed order, then warp
+// shuffles and one pass over the warps' sums reduce them in a fixed tree, so
+// the mean is deterministic.  Runs before k_probe_gather (same step index).
+struct PlaneDesc {
+    long long base, su, sv;  // element offset of (u, v) = (0, 0) and the strides
+    int nu, nv, comp;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_plane_gather(const PlaneDesc *planes, int n_planes, const T *const *F,
+                                                       T *ts, int series0, long long n_steps, const int *d_step) {
+    __shared__ double warp_sum[32];
+    const int q = blockIdx.x;
+    if (q >= n_planes) return;
+    const int n = *d_step;
+    if (n >= n_steps) return;
+    const PlaneDesc pd = planes[q];
+    const T *f = F[pd.comp];
+    const long long npts = (long long)pd.nu * pd.nv;
+    double acc = 0.0;
+    for (long long t = threadIdx.x; t < npts; t += blockDim.x) {
+        const long long u = t / pd.nv, v = t - u * pd.nv;
+        acc = __dadd_rn(acc, (double)f[pd.base + u * pd.su + v * pd.sv]);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc = __dadd_rn(acc, __shfl_down_sync(0xffffffffu, acc, off));
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = __dadd_rn(s, warp_sum[w]);
+        ts[(long long)(series0 + q) * n_steps + n] = (T)__ddiv_rn(s, (double)npts);
+    }
+}
+
+// ---- running DFT --------------------------------------------------------------
+// Accumulates the DFT bins of every series (point probes, then plane probes)
+// over the `count` samples the step loop recorded last, [step - count, step),
+// into acc: rfsyn's running sums re += v cos(w t) dt, im -= v sin(w t) dt
+// with t = (n + t_off) dt (engine/fdtd/probe.c:78-92).  Thread per (series,
+// bin); launched once per replayed chunk of steps, so the sums advance with
+// the run instead of in a pass over the stored series afterwards.  FP64 runs:
+// FP64 sums with direct sincos (the order and arithmetic of rfsyn's loop).
+// FP32 runs: Kahan-compensated FP32 sums (acc holds re, im and their
+// compensations), the phasor advanced by an FP64 recurrence anchored with a
+// direct sincos at the first sample of each launch.
+template <typename T>
+__global__ void k_dft_run(const T *ts, int n_series, long long n_steps, const int *d_step, int count, int n_freqs,
+                          const double *omega, double dt, double t_off, void *acc) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (f >= n_freqs || p >= n_series) return;
+    const int n1 = min((long long)*d_step, n_steps), n0 = max(n1 - count, 0);
+    const T *s = ts + (long long)p * n_steps;
+    const double w = omega[f];
+    const long long a = (long long)p * n_freqs + f;
+    if (sizeof(T) == 8) {
+        double *r = static_cast<double *>(acc) + 2 * a;
+        double re = r[0], im = r[1];
+        for (int n = n0; n < n1; n++) {
+            double t = ((double)n + t_off) * dt;
+            double sn, cn;
+            sincos(w * t, &sn, &cn);
+            double v = (double)s[n];
+            re = __dadd_rn(re, __dmul_rn(__dmul_rn(v, cn), dt));
+            im = __dsub_rn(im, __dmul_rn(__dmul_rn(v, sn), dt));
+        }
+        r[0] = re;
+        r[1] = im;
+    } else {
+        float4 *r = static_cast<float4 *>(acc) + a;
+        float4 st = *r;  // re, im, Kahan compensations of re and im
+        if (n1 > n0) {
+            double cw, sw, cn, sn;
+            sincos(w * dt, &sw, &cw);
+            sincos(w * (((double)n0 + t_off) * dt), &sn, &cn);
+            const float fdt = (float)dt;
+            for (int n = n0; n < n1; n++) {
+                const float v = (float)s[n] * fdt;
+                const float yr = v * (float)cn - st.z;
+                const float tr = st.x + yr;
+                st.z = (tr - st.x) - yr;
+                st.x = tr;
+                const float yi = -v * (float)sn - st.w;
+                const float ti = st.y + yi;
+                st.w = (ti - st.y) - yi;
+                st.y = ti;
+                const double c2 = cn * cw - sn * sw;
+                sn = sn * cw + cn * sw;
+                cn = c2;
+            }
+        }
+        *r = st;
+    }
 }
 
 // ---- running DFT of the probe series -------------------------------------

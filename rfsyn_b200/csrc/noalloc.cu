@@ -86,15 +86,26 @@ extern "C" int fdtd_b200_sphere_fractions_noalloc(const double centre[3], double
     const NoallocDevice *d = setup_current_device();
     if (!d) return -1;
     double *sf = d->scratch, *sn = d->scratch + RFB_NOALLOC_MAX_SAMPLES;
+    // This thread's capture mode becomes thread-local for the call: a graph
+    // capture another thread runs in the global mode then ignores the call's
+    // copies (to pageable host memory) and its wait, which touch only this
+    // file's own stream; the caller's mode is restored before returning.
+    cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    cudaError_t e = cudaThreadExchangeStreamCaptureMode(&mode);
+    if (e != cudaSuccess) {
+        rfb_set_error("fdtd_b200_sphere_fractions_noalloc: %s", cudaGetErrorString(e));
+        return -1;
+    }
     // every one of the n samples of both arrays is written by the kernel, so
     // nothing left by an earlier call needs clearing
     k_sphere_fractions<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(centre[0], centre[1], centre[2], radius,
                                                                            i0, j0, k0, ni, nj, nk, sf, sn);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e == cudaSuccess) rfb_count_launch();
     if (e == cudaSuccess) e = cudaMemcpyAsync(f, sf, n * sizeof(double), cudaMemcpyDeviceToHost, d->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(n2, sn, n * sizeof(double), cudaMemcpyDeviceToHost, d->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    cudaThreadExchangeStreamCaptureMode(&mode);
     if (e != cudaSuccess) {
         rfb_set_error("fdtd_b200_sphere_fractions_noalloc: %s", cudaGetErrorString(e));
         return -1;

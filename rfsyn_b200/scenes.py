@@ -74,6 +74,7 @@ class Workload:
     schedule: int = FUSED
     sources: list = field(default_factory=list)   # dicts: i j k component mode amplitude waveform p0 p1 p2
     probes: list = field(default_factory=list)    # dicts: i j k component
+    planes: list = field(default_factory=list)    # plane probes, dicts: axis index component
     freqs: list = field(default_factory=list)
     # scene pieces applied by a setup callback: boxes, component overrides
     boxes: list = field(default_factory=list)     # (i0,i1,j0,j1,k0,k1,eps,sigma)
@@ -87,6 +88,8 @@ class Workload:
     slabs: list = field(default_factory=list)
     disp_boxes: list = field(default_factory=list)
     plane_wave: dict | None = None
+    # slabs: 0 staircased, 1 faces smoothed (fdtd_b200_materials_set_tensor3_slab_smoothed)
+    slab_smoothing: int = 0
 
     @property
     def dt(self) -> float:
@@ -226,7 +229,7 @@ def scene_setup(w: Workload):
     rows = [(cx, cy, cz, r, eps, sig, None if model is None else dispersive(*model))
             for (cx, cy, cz, r, eps, sig, model) in w.spheres]
     return SceneSetup(w.boxes, rows, w.smoothing, slabs=w.slabs,
-                      disp_boxes=[(*b[:6], dispersive(*b[6])) for b in w.disp_boxes])
+                      disp_boxes=[(*b[:6], dispersive(*b[6])) for b in w.disp_boxes], slab_smoothing=w.slab_smoothing)
 
 
 def _gauss(rng: Pcg32) -> float:
@@ -236,7 +239,7 @@ def _gauss(rng: Pcg32) -> float:
 
 
 def c3(seed: int = 3, precision: int = FP32, nx: int = 128, ny: int = 128, nz: int = 512, n_steps: int = 6000,
-       npml: int = 16, dx: float = 0.5e-3, grid_probes: int = 8) -> Workload:
+       npml: int = 16, dx: float = 0.5e-3, grid_probes: int = 8, slab_smoothing: int = 1) -> Workload:
     """Periodic unit cell nx x ny x nz (periodic x / y, npml-cell CPML in z),
     dx 0.5 mm.  A plane wave at normal incidence (a non-normal wave is not
     periodic in x / y) with a PCG32(seed) polarisation angle, through a TF/SF
@@ -244,11 +247,15 @@ def c3(seed: int = 3, precision: int = FP32, nx: int = 128, ny: int = 128, nz: i
     tau = 2/(pi 16 GHz), t0 = 4 tau.  One tilted slab (seeded normal within
     45 deg of z, thickness U[20,60] cells, centred at 0.55 nz) of a full 3x3
     eps_r: eigenvalues U[2,10] rotated by the QR factor of a seeded Gaussian
-    matrix.  A 12-cell 2-pole Lorentz layer at 0.3 nz (f_p U[5,20] GHz,
-    gamma 2 pi U[0.1,1] GHz, delta_eps U[0.5,3]).  Reflection plane (Ex,
-    grid_probes^2 points, scattered region below the boundary) and
-    transmission plane (Ex, grid_probes^2 points near the top); 512 DFT bins
-    over 2..24 GHz; n_steps steps."""
+    matrix, its faces subpixel-smoothed (slab_smoothing 1; 0 staircases
+    them).  A 12-cell 2-pole Lorentz layer at 0.3 nz (f_p U[5,20] GHz,
+    gamma 2 pi U[0.1,1] GHz, delta_eps U[0.5,3]).  Reflection plane (in the
+    scattered region below the boundary) and transmission plane (near the
+    top): each a plane probe of Ex and one of Ey (the mean over the whole
+    plane, the specular wave) and grid_probes^2 Ex point probes; 512 DFT bins
+    over 2..24 GHz, accumulated as the steps run; n_steps steps.  Series:
+    the 2 grid_probes^2 point probes, then the planes (reflection Ex, Ey,
+    transmission Ex, Ey)."""
     rng = Pcg32(seed, 0)
     psi = rng.range(0.0, math.pi)
     th, ph = rng.range(0.0, math.pi / 4), rng.range(0.0, 2.0 * math.pi)
@@ -270,11 +277,13 @@ def c3(seed: int = 3, precision: int = FP32, nx: int = 128, ny: int = 128, nz: i
     pts = [(int((a + 0.5) * nx / g), int((b + 0.5) * ny / g)) for a in range(g) for b in range(g)]
     probes = [dict(i=i, j=j, k=npml + 2, component=FIELD_EX) for (i, j) in pts]
     probes += [dict(i=i, j=j, k=k1 - 8, component=FIELD_EX) for (i, j) in pts]
+    planes = [dict(axis=2, index=k, component=c) for k in (npml + 2, k1 - 8) for c in (FIELD_EX, FIELD_EY)]
     return Workload(
         name=f"c3_{nx}x{ny}x{nz}_periodic_tfsf_aniso_lorentz", nx=nx, ny=ny, nz=nz, dx=dx, n_steps=n_steps,
-        npml=npml, periodic=3, precision=precision, probes=probes, freqs=list(np.linspace(2e9, 24e9, 512)),
+        npml=npml, periodic=3, precision=precision, probes=probes, planes=planes,
+        freqs=list(np.linspace(2e9, 24e9, 512)),
         slabs=[([0.5 * nx, 0.5 * ny, 0.55 * nz], normal, thick, eps.ravel().tolist())],
-        disp_boxes=[(0, nx, 0, ny, zl, zl + 12, (1.0, 0.0, poles))], plane_wave=pw)
+        disp_boxes=[(0, nx, 0, ny, zl, zl + 12, (1.0, 0.0, poles))], plane_wave=pw, slab_smoothing=slab_smoothing)
 
 
 def scaled(w: Workload, n: int, n_steps: int) -> Workload:
@@ -312,4 +321,4 @@ def run_config(w: Workload):
     return RunConfig(w.nx, w.ny, w.nz, w.dx, w.n_steps, w.npml, courant=w.courant, periodic=w.periodic,
                      precision=w.precision, schedule=w.schedule,
                      cpml=CpmlParams(w.npml, w.m, w.ma, w.kappa_max, w.alpha_max, w.r0),
-                     sources=w.sources, probes=w.probes, freqs=w.freqs, plane_wave=w.plane_wave)
+                     sources=w.sources, probes=w.probes, freqs=w.freqs, plane_wave=w.plane_wave, planes=w.planes)

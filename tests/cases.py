@@ -3,6 +3,7 @@ and the product's run configuration."""
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 
 import rfsyn_b200 as rb
 from oracle import Scene
@@ -65,8 +66,15 @@ def simulate_unit_cfg() -> rb.FdtdSimConfig:
 
 
 def slab_rows(w: scenes.Workload) -> list:
-    """The 3x3 rows the product's slab helper gives the workload's slabs
-    (host API only), as the oracle's explicit samples."""
+    """The 3x3 rows the product's slab helper gives the workload's slabs, as
+    the oracle's explicit samples (the staircased helper runs on the host;
+    the smoothed one builds its rows on the GPU)."""
+    return product_t3_rows(dataclasses.replace(w, boxes=[], spheres=[], disp_boxes=[]))
+
+
+def product_t3_rows(w: scenes.Workload) -> list:
+    """Every 3x3 sample the product's set-up of the workload creates (its
+    materials built through the host API on a bare grid)."""
     lib = rb.load()
     lib.fdtd_grid_create.restype = C.c_void_p
     lib.fdtd_grid_create.argtypes = [C.c_size_t] * 3 + [C.c_double, C.c_double]
@@ -80,8 +88,8 @@ def slab_rows(w: scenes.Workload) -> list:
     g = lib.fdtd_grid_create(w.nx, w.ny, w.nz, w.dx, w.courant)
     lib.fdtd_grid_set_periodic(g, w.periodic)
     m = lib.materials_create(g)
-    st = rb.SceneSetup(slabs=w.slabs)
-    assert st.fn(g, m, None) == 0
+    st = scenes.scene_setup(w)
+    assert st is not None and st.fn(g, m, None) == 0
     rows = []
     row = (C.c_double * 3)()
     ext = [n + (0 if (w.periodic >> a) & 1 else 1) for a, n in enumerate((w.nx, w.ny, w.nz))]
@@ -96,7 +104,25 @@ def slab_rows(w: scenes.Workload) -> list:
     return rows
 
 
-def workload_to_scene(w: scenes.Workload) -> Scene:
+def oracle_slab_rows(w: scenes.Workload) -> list:
+    """The oracle's own rows of the workload's slabs (uniform vacuum
+    background): the staircased rule, or the smoothed faces of
+    oracle.subpixel_oracle.slab_rows."""
+    from oracle.subpixel_oracle import slab_rows as smooth_rows
+
+    rows = []
+    for (point, normal, thick, eps) in w.slabs:
+        if w.slab_smoothing:
+            rows += smooth_rows(w.nx, w.ny, w.nz, w.periodic, point, normal, thick, eps)
+        else:
+            rows += slab_rows(dataclasses.replace(w, slabs=[(point, normal, thick, eps)]))
+    return rows
+
+
+def workload_to_scene(w: scenes.Workload, slab_source: str = "oracle") -> Scene:
+    """The workload as the oracle's scene.  Slab samples: the oracle's own
+    rows (slab_source "oracle"), or the rows the product's helper built
+    ("product": a smoothed slab then needs the GPU)."""
     from oracle import MODEL_ONLY, disp_entry
 
     disp, spheres = [], []
@@ -113,8 +139,9 @@ def workload_to_scene(w: scenes.Workload) -> Scene:
         sources=[(s["i"], s["j"], s["k"], s["component"], s["mode"], s["amplitude"], s["waveform"], s["p0"],
                   s["p1"], s.get("p2", 0.0)) for s in w.sources],
         probes=[(p["i"], p["j"], p["k"], p["component"]) for p in w.probes], freqs=list(w.freqs),
+        planes=[(p["axis"], p["index"], p["component"]) for p in w.planes],
         src_t_offset=0.0, dft_t_offset=1.0, plane_wave=w.plane_wave,
-        tensor3=slab_rows(w) if w.slabs else [])
+        tensor3=(slab_rows(w) if slab_source == "product" else oracle_slab_rows(w)) if w.slabs else [])
     for (i0, i1, j0, j1, k0, k1, model) in w.disp_boxes:
         for i in range(i0, i1):
             for j in range(j0, j1):
@@ -136,7 +163,8 @@ def scene_run_config(s: Scene, precision: int, schedule: int) -> rb.RunConfig:
         sources=[dict(i=q[0], j=q[1], k=q[2], component=q[3], mode=q[4], amplitude=q[5], waveform=q[6], p0=q[7],
                       p1=q[8], p2=q[9]) for q in s.sources],
         probes=[dict(i=q[0], j=q[1], k=q[2], component=q[3]) for q in s.probes], freqs=s.freqs,
-        source_time_offset=s.src_t_offset, dft_time_offset=s.dft_t_offset, plane_wave=s.plane_wave)
+        source_time_offset=s.src_t_offset, dft_time_offset=s.dft_t_offset, plane_wave=s.plane_wave,
+        planes=[dict(axis=a, index=i, component=c) for (a, i, c) in s.planes])
 
 
 def run_device(s: Scene, precision: int, schedule: int) -> dict:
