@@ -475,7 +475,10 @@ def run_batch(args) -> None:
     world, rank, local = rk.world, rk.rank, rk.local
     torch.cuda.set_device(local)
     ranks.init(rk, "nccl", 300)
-    ws = scenes.c4(seed=ranks.scene_seed(4, rk, 1000), n_scenes=args.scenes)
+    # one set of args.scenes scenes, each rank batching its contiguous shard
+    # (strong scaling: the job's work is fixed as ranks are added)
+    ws_all = scenes.c4(seed=4, n_scenes=args.scenes)
+    ws = [ws_all[q] for q in ranks.shard(len(ws_all), rk)]
     n_steps = ws[0].n_steps
     cells = sum(w.cells for w in ws)
     setups = [scenes.scene_setup(w) for w in ws]
@@ -508,10 +511,10 @@ def run_batch(args) -> None:
     launches = lib.fdtd_b200_launch_count() - launches0
     ms = ranks.max_over(rk, start.elapsed_time(end))
     clocks = clk.summary()
-    # every rank's scenes differ: the whole job's cells are summed over ranks
+    # the ranks' shards partition the set: the whole job's cells are summed
     cells_all = ranks.sum_over(rk, float(cells))
     value = cells_all * n_steps * args.steps / (ms / 1e3) / 1e6
-    scenes_s = ranks.weak_rate(len(ws) * args.steps, ms, rk)
+    scenes_s = len(ws_all) * args.steps / (ms / 1e3)
     finite = all(bool(np.all(np.isfinite(b.dft(q)))) for q in range(0, len(ws), max(1, len(ws) // 16)))
     # sweep kernels alone (CUDA events around the sweep launches of each step)
     b.reset()
@@ -549,18 +552,19 @@ def run_batch(args) -> None:
     sweep_launch_ms = sw / 50
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32 scenes: 0-6 spheres / boxes each)",
-        "config": {"workload": f"c4_batch{len(ws)}_32to96_fp32", "scenes": len(ws), "cells": cells,
+        "config": {"workload": f"c4_batch{len(ws_all)}_32to96_fp32", "scenes": len(ws_all),
+                   "scenes_per_rank": len(ws), "cells": int(cells_all),
                    "n_steps": n_steps, "npml": 8, "probes_per_scene": 4, "dft_bins": 128,
                    "plan": {"tile_j": info.tile_j, "ring_depth": info.ring_depth, "mode": info.mode,
                             "seg_interior": info.seg_interior, "seg_edge": info.seg_edge,
                             "single_queue": bool(info.unified)},
                    "items": [info.items_interior, info.items_xslab, info.items_edge],
-                   "parallelism": f"scene-batch x{world}", "l2": "inputs larger than L2 (fields 12 x 4 B x 130 M cells)"},
+                   "parallelism": f"scene shards x{world}", "l2": "inputs larger than L2 (fields 12 x 4 B x 130 M cells)"},
         "scenes_per_s": scenes_s,
         "plain_one_at_a_time": {"scenes_per_s": plain_scenes_s, "sample": len(sample),
-                                "speedup_batched": scenes_s / plain_scenes_s / world},
+                                "speedup_batched": scenes_s / world / plain_scenes_s},
         "roofline": {"bound": "hbm", "achieved": alg / (sweep_launch_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (sweep_launch_ms / 1e3) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
                      "kernel": "k_sweep_qb (one batched H+E sweep: interior + x-slab + edge launches)",
@@ -586,62 +590,74 @@ def run_surrogate(args) -> None:
     the ensemble where its spread is <= 2 % of the norm and by the batched
     FDTD otherwise.  Metric: held-out scenes/s of that path (wall clock, the
     ensemble's inference plus the fallback FDTD runs), beside the plain
-    one-scene-at-a-time GPU FDTD and the transfer-function error."""
+    one-scene-at-a-time GPU FDTD and the transfer-function error.  With
+    several ranks the scene sets are sharded (each rank runs its block of
+    scenes, the rows are gathered on every rank), the members split over
+    the ranks and their predictions gathered; times are the slowest rank's."""
     import torch
 
     import rfsyn_b200 as rb
-    from rfsyn_b200 import scenes
+    from rfsyn_b200 import ranks, scenes
     from rfsyn_b200 import surrogate as sg
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    if int(os.environ.get("RANK", "0")) != 0:
-        return
+    rk = ranks.from_env()
+    torch.cuda.set_device(rk.local)
+    ranks.init(rk, "nccl", 1800)
     ws_tr = sg.c5_scenes(seed=51, n_scenes=args.train_scenes)
     ws_te = sg.c5_scenes(seed=52, n_scenes=args.test_scenes)
     tm = {}
+    ranks.barrier(rk)
     t0 = time.perf_counter()
-    X_tr, H_tr = sg.transfer_functions(ws_tr, timings=tm)
-    gen_s = time.perf_counter() - t0
+    X_tr, H_tr = sg.sharded_transfer_functions(ws_tr, rk, timings=tm)
+    gen_s = ranks.max_over(rk, time.perf_counter() - t0)
     G_tr = sg.scene_transfer_targets(ws_tr, H_tr)
-    sur = sg.Surrogate(members=5, width=512, depth=4, seed=3)
+    sur = sg.Surrogate(members=5, width=512, depth=4, seed=3, r=rk)
     t0 = time.perf_counter()
     losses = sur.fit(X_tr, G_tr, steps=args.train_steps, batch=256, lr=1e-3)
-    train_s = time.perf_counter() - t0
+    train_s = ranks.max_over(rk, time.perf_counter() - t0)
     # held-out truth from the batched FDTD (also its throughput)
     tm_te = {}
     t0 = time.perf_counter()
-    X_te, H_te = sg.transfer_functions(ws_te, timings=tm_te)
-    fdtd_batched_wall = time.perf_counter() - t0
-    fdtd_batched_scenes_s = len(ws_te) / (tm_te["fdtd_ms"] / 1e3)
+    X_te, H_te = sg.sharded_transfer_functions(ws_te, rk, timings=tm_te)
+    fdtd_batched_wall = ranks.max_over(rk, time.perf_counter() - t0)
+    fdtd_batched_scenes_s = len(ws_te) / (ranks.max_over(rk, tm_te.get("fdtd_ms", 0.0)) / 1e3)
     pred = sur.predict(ws_te, X_te)
     err_all = sg.rel_err(pred.H, H_te)
     # the surrogate path with fallback, wall clock end to end
     torch.cuda.synchronize()
+    ranks.barrier(rk)
     t0 = time.perf_counter()
     res = sg.infer_with_fallback(sur, ws_te, threshold=args.threshold)
-    path_s = time.perf_counter() - t0
+    path_s = ranks.max_over(rk, time.perf_counter() - t0)
     err = sg.rel_err(res["H"], H_te)
     fell = set(res["fallback"])
     acc_rows = np.asarray([q not in fell for q in range(len(ws_te)) for _ in range(4)])
-    # plain one-scene-at-a-time GPU FDTD on a sample
-    plain_ms = 0.0
-    sample = ws_te[: args.plain_sample]
-    for w in sample:
-        st = scenes.scene_setup(w)
-        sim = rb.Sim(scenes.run_config(w), st.ptr if st else None, None)
-        sim.advance(w.n_steps)
-        sim.reset()
-        plain_ms += sim.advance_timed(w.n_steps)
-        sim.close()
-    plain_scenes_s = len(sample) / (plain_ms / 1e3)
+    # plain one-scene-at-a-time GPU FDTD on a sample (rank 0's GPU)
+    plain_scenes_s = None
+    if rk.rank == 0:
+        plain_ms = 0.0
+        sample = ws_te[: args.plain_sample]
+        for w in sample:
+            st = scenes.scene_setup(w)
+            sim = rb.Sim(scenes.run_config(w), st.ptr if st else None, None)
+            sim.advance(w.n_steps)
+            sim.reset()
+            plain_ms += sim.advance_timed(w.n_steps)
+            sim.close()
+        plain_scenes_s = len(sample) / (plain_ms / 1e3)
+    sur.close()
+    ranks.finish(rk)
+    if rk.rank != 0:
+        return
     value = len(ws_te) / path_s
     line = {
         "metric": "scenes/s (batched FDTD + surrogate, held-out)", "value": value, "unit": "scenes/s",
-        "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "bf16 GEMMs / fp32 FDTD", "data": "synthetic (seeded PCG32 scenes)",
+        "n_gpus": rk.world, "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "bf16 GEMMs / fp32 FDTD", "data": "synthetic (seeded PCG32 scenes)",
         "config": {"workload": "c5_surrogate_48cube_dx2mm", "train_scenes": len(ws_tr), "test_scenes": len(ws_te),
                    "samples_per_scene": 4, "members": 5, "net": "54-512x4(GELU)-512", "train_steps": args.train_steps,
-                   "batch": 256, "lr": 1e-3, "threshold": args.threshold, "bins": sg.N_BINS},
+                   "batch": 256, "lr": 1e-3, "threshold": args.threshold, "bins": sg.N_BINS,
+                   "parallelism": f"scene shards + ensemble members x{rk.world}"},
         "plain_one_at_a_time_scenes_s": plain_scenes_s, "speedup_vs_plain": value / plain_scenes_s,
         "batched_fdtd_scenes_s": fdtd_batched_scenes_s,
         "accepted_scene_frac": 1.0 - len(fell) / len(ws_te),
@@ -651,12 +667,11 @@ def run_surrogate(args) -> None:
                              "accepted_p95": float(np.percentile(err[acc_rows], 95)) if acc_rows.any() else None,
                              "network_only_median": float(np.median(err_all)),
                              "network_only_p95": float(np.percentile(err_all, 95))},
-        "timings_s": {"data_generation": gen_s, "data_generation_device": tm["fdtd_ms"] / 1e3, "training": train_s,
-                      "path_surrogate": res["surrogate_s"], "path_fallback_fdtd": res["fdtd_s"],
+        "timings_s": {"data_generation": gen_s, "data_generation_device": tm.get("fdtd_ms", 0.0) / 1e3,
+                      "training": train_s, "path_surrogate": res["surrogate_s"], "path_fallback_fdtd": res["fdtd_s"],
                       "heldout_fdtd_wall": fdtd_batched_wall},
         "final_train_losses": losses,
     }
-    sur.close()
     print(json.dumps(line), flush=True)
 
 

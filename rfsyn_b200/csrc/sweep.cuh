@@ -123,9 +123,11 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
     const long long ny1 = a.ny + 1;
     const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
 
+    // warps 0-3 recompute the halo H of the plane (one piece each); warp 4
+    // issues the copies, so no warp carries two extra jobs per plane
     auto issue = [&](int s, int p) {
         if (p < 0 || failed) return;  // a failed CTA issues no further copies
-        if (tid == 0) {
+        if (tid == 4 * 32) {
             mbar_expect_tx(&bars[s], tx_bytes);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -159,8 +161,8 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
     const int pitch = (int)a.pitch;
     const int plane32 = (int)a.plane;
     // halo cells recomputed per plane: the row (j0-1, k0 .. k0+W-1), Hx by
-    // warp 0 and Hz by warp 2, the column (j0 .. j0+TR-1, k0-1), Hx and Hy
-    // by warp 1; lane tx takes halo column tx / halo row tx
+    // warp 0 and Hz by warp 2, the column (j0 .. j0+TR-1, k0-1), Hx by warp
+    // 1 and Hy by warp 3; lane tx takes halo column tx / halo row tx
     const int jh = j0 - 1, jc = j0 + tx, kh = k0 - 1;
     unsigned mjk = 0x3f;                   // bits 0-2 H, 3-5 E at (j, k), plane apart
     bool rowh = tx < W, colh = tx < TR;    // halo cells this thread recomputes
@@ -371,12 +373,12 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
             const PlaneB pb = plane_b(i);
             const int sxm = (XS && on) ? slab_in(i, a.lo_m[0], a.hi_m[0], a.nx, on) : -1;
             const int bym = i * nsmy * pitch, bzm = i * (int)ny1 * nsmz, bxm = sxm * plane32;
-            // halo cells recomputed this plane: row (j0-1, k) Hx, Hz;
-            // column (j0+tx, k0-1) Hx, Hy
-            // row halo: Hx by warp 0, Hz by warp 2
+            // halo cells recomputed this plane: row (j0-1, k) Hx by warp 0,
+            // Hz by warp 2; column (j0+tx, k0-1) Hx by warp 1, Hy by warp 3
             const unsigned mrow = (ty == 0 && rowh) ? (mpl & mrow_jk & 1u)
                                   : (ty == 2 && rowh) ? (mpl & mrow_jk & 4u) : 0u;
-            const unsigned mcol = (ty == 1 && colh) ? (mpl & mcol_jk) : 0u;
+            const unsigned mcol = (ty == 1 && colh) ? (mpl & mcol_jk & 1u)
+                                  : (ty == 3 && colh) ? (mpl & mcol_jk & 2u) : 0u;
             // psi inputs of the own cell and of the halo cells and the
             // plane's x profile, all loaded before the wait; psi are read
             // only for components swept at the cell, so every offset
@@ -434,11 +436,13 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
                 if (mrow & 4u) v = hcell(2, pb, sc, sn, 0, q, row_c, 0, qs, hh[2], hh[3], false);
                 sH[2][0][qs] = v;
             } else if (ty == 1 && colh) {
-                // column halo (j0+tx, k0-1): Hx, Hy
+                // column halo (j0+tx, k0-1): Hx
                 T v = H(sc, 0)[tx + 1][3];
                 if (mcol & 1u) v = hcell(0, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[0], hh[1], false);
                 sH[0][tx + 1][0] = v;
-                v = H(sc, 1)[tx + 1][3];
+            } else if (ty == 3 && colh) {
+                // column halo (j0+tx, k0-1): Hy
+                T v = H(sc, 1)[tx + 1][3];
                 if (mcol & 2u) v = hcell(1, pb, sc, sn, tx + 1, 3, col_c, tx + 1, 0, hh[2], hh[3], false);
                 sH[1][tx + 1][0] = v;
             }
@@ -586,7 +590,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     k_sweep_q(Args<T> a, FusedDims d, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps,
               int *queue, int *err) {
     static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
-    static_assert(TJ >= 3, "warps 0-2 share the halo recomputation");
+    static_assert(TJ >= 5, "warps 0-3 share the halo recomputation, warp 4 issues the copies");
     using S = QLayout<T, TJ, NS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (q_misaligned(smem_raw, err)) return;

@@ -1,10 +1,14 @@
 """One process per GPU over scenes: the multi-GPU plumbing of the benches.
 
 The FDTD path shards by scene -- every scene is an independent unit with no
-exchange between ranks -- so the only collectives are a barrier around the
-timed region and the max over ranks of the elapsed time (a weak-scaling
-throughput is every rank's units over the slowest rank's time).  The backend
-is NCCL on GPUs; the same functions run over gloo on CPU, which is how the
+exchange between ranks -- so around the time loop the only collectives are
+a barrier around the timed region and the max over ranks of the elapsed
+time (a weak-scaling throughput is every rank's units over the slowest
+rank's time).  The surrogate's pipeline shards its scene set the same way
+and then exchanges data: the training rows every rank generated are
+gathered on every rank (gather_rows), the ensemble's members are split over
+the ranks (members_of) and their predictions gathered.  The backend is NCCL
+on GPUs; the same functions run over gloo on CPU, which is how the
 multi-rank logic is tested without several GPUs.
 """
 from __future__ import annotations
@@ -93,3 +97,36 @@ def weak_rate(units_per_rank: float, ms_max: float, r: Ranks) -> float:
     """Whole-job throughput (units per second) of ranks that each processed
     units_per_rank, timed by the slowest rank."""
     return r.world * units_per_rank / (ms_max / 1e3)
+
+
+def gather_rows(r: Ranks, a, device: str = "cuda"):
+    """Every rank's block of rows of a (numpy, any row count, the same
+    trailing shape and dtype on every rank), concatenated in rank order on
+    every rank: with contiguous shards (shard()) that is the global order."""
+    import numpy as np
+
+    if r.world == 1:
+        return a
+    import torch
+    import torch.distributed as dist
+
+    a = np.ascontiguousarray(a)
+    n = torch.tensor([a.shape[0]], dtype=torch.int64, device=device)
+    sizes = [torch.zeros_like(n) for _ in range(r.world)]
+    dist.all_gather(sizes, n)
+    sizes = [int(x.item()) for x in sizes]
+    m = max(sizes)
+    row = int(np.prod(a.shape[1:], dtype=np.int64)) if a.ndim > 1 else 1
+    raw = a.view(np.uint8).reshape(a.shape[0], row * a.dtype.itemsize)
+    buf = np.zeros((m, row * a.dtype.itemsize), dtype=np.uint8)
+    buf[: a.shape[0]] = raw
+    t = torch.from_numpy(buf).to(device)
+    parts = [torch.empty_like(t) for _ in range(r.world)]
+    dist.all_gather(parts, t)
+    out = np.concatenate([p.cpu().numpy()[:k] for p, k in zip(parts, sizes)], axis=0)
+    return out.reshape(-1).view(a.dtype).reshape((sum(sizes),) + a.shape[1:])
+
+
+def members_of(n_members: int, r: Ranks) -> list[int]:
+    """The ensemble members rank r trains and evaluates (round robin)."""
+    return [q for q in range(n_members) if q % r.world == r.rank]

@@ -39,6 +39,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import C0, FIELD_EZ, FP32, WAVE_MOD_GAUSSIAN, Batch, Mlp
+from . import ranks as rk
 from . import scenes as sc
 
 N_SCAT = 8
@@ -156,6 +157,16 @@ def transfer_functions(ws: list[sc.Workload], chunk: int = 512, timings: dict | 
     return np.asarray(X), np.asarray(H)
 
 
+def sharded_transfer_functions(ws: list[sc.Workload], r: rk.Ranks, device: str = "cuda", timings: dict | None = None,
+                               tf=transfer_functions):
+    """transfer_functions over several ranks: rank r runs its contiguous
+    shard of the scenes, then every rank receives all rows in scene order."""
+    mine = [ws[q] for q in rk.shard(len(ws), r)]
+    X, H = tf(mine, timings=timings) if mine else (np.zeros((0, N_FEAT)), np.zeros((0, N_BINS), complex))
+    return rk.gather_rows(r, np.asarray(X, dtype=np.float64), device), \
+        rk.gather_rows(r, np.asarray(H, dtype=np.complex128), device)
+
+
 def scene_transfer_targets(ws: list[sc.Workload], H: np.ndarray) -> np.ndarray:
     """G = H * deembed for every (scene, receiver) row of H (complex)."""
     D = np.asarray([_deembed(w, rx) for w in ws for rx in range(len(w.probes))])
@@ -174,10 +185,16 @@ class Prediction:
 
 
 class Surrogate:
-    """An ensemble of GPU MLPs over the de-embedded transfer function."""
+    """An ensemble of GPU MLPs over the de-embedded transfer function.  With
+    several ranks each rank holds, trains and evaluates its share of the
+    members (ranks.members_of); predictions are gathered on every rank."""
 
-    def __init__(self, members: int = 5, width: int = 512, depth: int = 4, seed: int = 0):
-        self.nets = [Mlp(N_FEAT, width, depth, 2 * N_BINS, seed=seed + 7919 * q) for q in range(members)]
+    def __init__(self, members: int = 5, width: int = 512, depth: int = 4, seed: int = 0,
+                 r: rk.Ranks | None = None, device: str = "cuda"):
+        self.r = r or rk.Ranks(0, 1, 0)
+        self.device = device
+        self.members = rk.members_of(members, self.r)
+        self.nets = [Mlp(N_FEAT, width, depth, 2 * N_BINS, seed=seed + 7919 * q) for q in self.members]
         self.scale = 1.0
         self.seed = seed
 
@@ -192,13 +209,15 @@ class Surrogate:
         self.scale = float(np.sqrt(np.mean(np.abs(G) ** 2)))
         T = self._enc(G).astype(np.float32)
         losses = []
-        for q, net in enumerate(self.nets):
+        for q, net in zip(self.members, self.nets):
             net.set_data(X.astype(np.float32), T)
             losses.append(net.train(steps, batch=batch, lr=lr, seed=self.seed + 104729 * q + 1))
-        return losses
+        return list(rk.gather_rows(self.r, np.asarray(losses, dtype=np.float64), self.device))
 
     def predict_g(self, X: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-        outs = np.stack([self._dec(net.predict(X.astype(np.float32)).astype(np.float64)) for net in self.nets])
+        local = np.stack([self._dec(net.predict(X.astype(np.float32)).astype(np.float64)) for net in self.nets]) \
+            if self.nets else np.zeros((0, len(X), N_BINS), complex)
+        outs = rk.gather_rows(self.r, local, self.device)
         mean = outs.mean(axis=0)
         spread = np.sqrt(np.mean(np.sum(np.abs(outs - mean) ** 2, axis=-1), axis=0)) / np.maximum(
             np.linalg.norm(mean, axis=-1), 1e-300)
@@ -219,8 +238,8 @@ class Surrogate:
 def infer_with_fallback(sur: Surrogate, ws: list[sc.Workload], threshold: float = 0.02) -> dict:
     """Transfer functions of every (scene, receiver): the ensemble mean where
     the ensemble agrees (spread <= threshold for all the scene's receivers),
-    the batched FDTD otherwise.  Returns H, which scenes fell back and the
-    wall time of each part."""
+    the batched FDTD otherwise (the fallback scenes sharded over the ranks).
+    Returns H, which scenes fell back and the wall time of each part."""
     t0 = time.perf_counter()
     pred = sur.predict(ws)
     t_sur = time.perf_counter() - t0
@@ -231,7 +250,7 @@ def infer_with_fallback(sur: Surrogate, ws: list[sc.Workload], threshold: float 
     t1 = time.perf_counter()
     timings: dict = {}
     if fall:
-        _, Hf = transfer_functions([ws[q] for q in fall], timings=timings)
+        _, Hf = sharded_transfer_functions([ws[q] for q in fall], sur.r, sur.device, timings=timings)
         r = 0
         for q in fall:
             H[rows[q]:rows[q + 1]] = Hf[r:r + nrx[q]]
