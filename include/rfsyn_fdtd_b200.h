@@ -210,6 +210,8 @@ typedef struct {
     int interior_items;      /* work items of the interior sweep (CTAs per step) */
     int edge_items;          /* work items of the edge sweep */
     int unified;             /* 1: every sweep item in one work queue, one launch per step */
+    int interior_ring2;      /* 0, or the ring depth of the interior sweep whose threads own two
+                                rows of a 2 tile_j-row tile */
 } fdtd_b200_sim_info_t;
 
 int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info);
@@ -530,7 +532,7 @@ void fdtd_b200_release_cached_memory(void);
  * value as text (a boolean as true/false or 1/0):
  *   precision  fp32 | fp64          default precision of rfsyn's entry points
  *   schedule   fused | split        default schedule of rfsyn's entry points
- *   plan       auto | tj,ns,seg_interior,seg_edge[,mode[,single_queue]]
+ *   plan       auto | tj,ns,seg_interior,seg_edge[,mode[,single_queue[,two_rows_ring]]]
  *                                   the sweep plan (auto = the autotuner)
  *   tune       true | false         false: the first tensor-copy variant, no tuning
  *   trace      true | false         per-phase host times on stderr

@@ -738,11 +738,18 @@ void launch_q_t<double>(const Args<double> &a, const FusedPlan &p, int kind, con
     else launch_q_d<0>(a, p.d, p.tj, p.ns, p.d_int, p.n_int, m, p.d_queue, err, st);
 }
 
+// The two-rows interior sweep (FP32 plans only).
+static void launch_interior_i2(const Args<float> &a, const FusedPlan &p, const TmaMaps &m, int *err, cudaStream_t st) {
+    launch_q_i2(a, p.i2, p.d_int, p.n_int, m, p.d_queue, err, st);
+}
+static void launch_interior_i2(const Args<double> &, const FusedPlan &, const TmaMaps &, int *, cudaStream_t) {}
+
 template <typename T>
 static void launch_int(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
     const TmaMaps &m = e->tmaps[e->nbuf == 2 ? par : 0];
     if (e->plan.tma >= 2) {
-        launch_q_t<T>(a, e->plan, 0, m, e->d_err, st);
+        if (e->plan.i2) launch_interior_i2(a, e->plan, m, e->d_err, st);
+        else launch_q_t<T>(a, e->plan, 0, m, e->d_err, st);
         launch_q_t<T>(a, e->plan, 1, m, e->d_err, st);
     } else if (e->plan.tma) launch_interior_tma<T>(a, e->plan, m, e->d_err, st);
     else launch_interior<T>(a, e->plan, st);
@@ -918,9 +925,15 @@ static int build_tma_maps(rfb_engine *e, int tj) {
             if (encode_map(&m.en[c], e->fld[in][c], dt, e->esz, e->g, e->pitch, 24, 2 * tj + 2)) return -1;
             if (encode_map(&m.hn[c], e->fld[in][3 + c], dt, e->esz, e->g, e->pitch, 20, 2 * tj + 1)) return -1;
         }
+        // interior tiles of 2 tj rows x 32 columns (two rows per thread)
+        for (int c = 0; c < 3; c++) {
+            if (encode_map(&m.e2[c], e->fld[in][c], dt, e->esz, e->g, e->pitch, TMA_EW, 2 * tj + 2)) return -1;
+            if (encode_map(&m.h2[c], e->fld[in][3 + c], dt, e->esz, e->g, e->pitch, TMA_HW, 2 * tj + 1)) return -1;
+        }
         if (e->scene.codes &&
             (encode_map(&m.code, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 32, tj) ||
-             encode_map(&m.coden, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 16, 2 * tj)))
+             encode_map(&m.coden, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 16, 2 * tj) ||
+             encode_map(&m.code2, e->scene.codes, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e->g, e->pitch, 32, 2 * tj)))
             return -1;
     }
     return 0;
@@ -948,7 +961,8 @@ struct PlanLists {
     FusedDims d;
 };
 
-static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg_int, int seg_edge, PlanLists &out) {
+static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg_int, int seg_edge, PlanLists &out,
+                       int i2 = 0) {
     const rfb_geom_t &g = e->g;
     const bool px = g.periodic & 1u, py = g.periodic & 2u, pz = g.periodic & 4u;
     PlanLists &p = out;
@@ -1062,6 +1076,32 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
             }
         }
     }
+    if (i2) {
+        // two-rows interior: pair each interior tile with the one below it
+        // (same column, same planes) into one item of 2 tj rows; a tile
+        // left without a partner goes to the slab / boundary queue, whose
+        // full body sweeps any tile
+        std::vector<SweepItem> paired;
+        std::vector<bool> used(vi.size(), false);
+        for (size_t a = 0; a < vi.size(); a++) {
+            if (used[a]) continue;
+            size_t b = a + 1;
+            for (; b < vi.size(); b++)
+                if (!used[b] && vi[b].k0 == vi[a].k0 && vi[b].j0 == vi[a].j0 + tj && vi[b].ib == vi[a].ib &&
+                    vi[b].ie == vi[a].ie)
+                    break;
+            used[a] = true;
+            if (b < vi.size()) {
+                used[b] = true;
+                paired.push_back(vi[a]);
+            } else {
+                SweepItem it = vi[a];
+                it.sub = 0;
+                vq.push_back(it);
+            }
+        }
+        vi.swap(paired);
+    }
     // queue order: longest items first, so the last items to start are
     // short; among equal lengths, items of one body together
     std::stable_sort(vq.begin(), vq.end(), [](const SweepItem &x, const SweepItem &y) {
@@ -1071,7 +1111,12 @@ static void plan_items(const rfb_engine *e, int active, int tj, int tma, int seg
 }
 
 static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, int seg_int, int seg_edge,
-                            int uni = 0) {
+                            int uni = 0, int i2 = 0) {
+    if (i2 && (tma < 2 || uni || e->prec != RFB_FP32 || tj != 8 || (i2 != 3 && i2 != 4))) {
+        rfb_set_error("the two-rows interior sweep needs an FP32 plan of mode 2 or 3, three launches, 8-row tiles "
+                      "and ring depth 3 or 4");
+        return -1;
+    }
     if (tma >= 2 && !q_fits(e)) {
         rfb_set_error("grid too large for the work-queue sweep (32-bit offsets)");
         return -1;
@@ -1088,8 +1133,9 @@ static int build_sweep_plan(rfb_engine *e, int active, int tj, int ns, int tma, 
     p.seg_int = seg_int;
     p.seg_edge = seg_edge;
     p.uni = tma >= 2 ? uni : 0;
+    p.i2 = i2;
     PlanLists pl;
-    plan_items(e, active, tj, tma, seg_int, seg_edge, pl);
+    plan_items(e, active, tj, tma, seg_int, seg_edge, pl, i2);
     p.d = pl.d;
     if (p.uni) {
         // one queue: interior and x-slab items join the slab / boundary
@@ -1155,7 +1201,7 @@ static bool plan_variant_known(int prec, int tj, int ns, int tma) {
 // on the engine's own scene; the choice is cached per geometry.  Every
 // candidate computes bit-identical fields, so tuning changes speed only.
 struct TunedPlan {
-    int tj, ns, tma, seg_int, seg_edge, uni;
+    int tj, ns, tma, seg_int, seg_edge, uni, i2;
 };
 
 static std::mutex g_tune_mu;
@@ -1181,7 +1227,7 @@ static int autotune(rfb_engine *e, int active) {
         for (auto &kv : g_tune_cache)
             if (kv.first == key)
                 return build_sweep_plan(e, active, kv.second.tj, kv.second.ns, kv.second.tma, kv.second.seg_int,
-                                        kv.second.seg_edge, kv.second.uni);
+                                        kv.second.seg_edge, kv.second.uni, kv.second.i2);
     }
     struct Cand {
         InteriorVariant v;
@@ -1206,7 +1252,7 @@ static int autotune(rfb_engine *e, int active) {
     }
     const int segs_int[] = {32, 64, 128};
     const int segs_edge[] = {16, 32};
-    TunedPlan best = {vars[0].v.tj, vars[0].v.ns, vars[0].tma, 64, 32, 0};
+    TunedPlan best = {vars[0].v.tj, vars[0].v.ns, vars[0].tma, 64, 32, 0, 0};
     float best_ms = 1e30f;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     CK(cudaEventCreate(&t0));
@@ -1218,9 +1264,13 @@ static int autotune(rfb_engine *e, int active) {
         for (const Cand &cv : vars)
             for (int si : segs_int)
                 for (int se : segs_edge)
-                    for (int uni = 0; uni <= (cv.tma >= 2 ? 1 : 0); uni++) {
+                    for (int form = 0; form <= (cv.tma >= 2 ? 3 : 0); form++) {
+                        // form 0: three launches; 1: one queue; 2, 3: three
+                        // launches, two-rows interior of ring depth 3, 4
                         const InteriorVariant &v = cv.v;
-                        if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se, uni) != 0) goto fail;
+                        const int uni = form == 1, i2 = form >= 2 ? form + 1 : 0;
+                        if (i2 && (e->prec != RFB_FP32 || v.tj != 8)) continue;
+                        if (build_sweep_plan(e, active, v.tj, v.ns, cv.tma, si, se, uni, i2) != 0) goto fail;
                         for (int w = 0; w < 2; w++) {
                             if (e->prec == RFB_FP64) enqueue_sweep<double>(e, par);
                             else enqueue_sweep<float>(e, par);
@@ -1238,7 +1288,7 @@ static int autotune(rfb_engine *e, int active) {
                         CK(cudaEventElapsedTime(&ms, t0, t1));
                         if (ms < best_ms) {
                             best_ms = ms;
-                            best = TunedPlan{v.tj, v.ns, cv.tma, si, se, uni};
+                            best = TunedPlan{v.tj, v.ns, cv.tma, si, se, uni, i2};
                         }
                     }
     }
@@ -1248,7 +1298,7 @@ static int autotune(rfb_engine *e, int active) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         g_tune_cache.push_back({key, best});
     }
-    if (build_sweep_plan(e, active, best.tj, best.ns, best.tma, best.seg_int, best.seg_edge, best.uni) != 0)
+    if (build_sweep_plan(e, active, best.tj, best.ns, best.tma, best.seg_int, best.seg_edge, best.uni, best.i2) != 0)
         return -1;
     {
         // a timed-out copy during tuning would have left the error flag set
@@ -1422,7 +1472,7 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
         e->active = active;
         if (member) {
             // a batch scene: the batch builds the plans and owns the streams
-            if (tma_prepare() != 0 || q_prepare() != 0) {
+            if (tma_prepare() != 0 || q_prepare() != 0 || qi2_prepare() != 0) {
                 rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
                 goto fail_noset;
             }
@@ -1431,20 +1481,20 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
         CK(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
-        if (tma_prepare() != 0 || q_prepare() != 0) {
+        if (tma_prepare() != 0 || q_prepare() != 0 || qi2_prepare() != 0) {
             rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
             goto fail_noset;
         }
-        // plan: "tj,ns,seg_interior,seg_edge[,mode[,single_queue]]" from RFSYN_FDTD_PLAN,
+        // plan: "tj,ns,seg_interior,seg_edge[,mode[,single_queue[,i2]]]" from RFSYN_FDTD_PLAN,
         // the autotuner (default) or, with RFSYN_FDTD_TUNE=0, the first
         // TMA variant
         const char *ov = rfb_plan_override();
-        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
+        int a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0, a7 = 0;
         int rc;
-        const int nov = ov ? sscanf(ov, "%d,%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5, &a6) : 0;
+        const int nov = ov ? sscanf(ov, "%d,%d,%d,%d,%d,%d,%d", &a1, &a2, &a3, &a4, &a5, &a6, &a7) : 0;
         if (nov >= 4 && a3 > 0 && a4 > 0 && plan_variant_known(precision, a1, a2, nov >= 5 ? a5 : 0) &&
             (a6 == 0 || (a6 == 1 && a5 >= 2)))
-            rc = build_sweep_plan(e, active, a1, a2, nov >= 5 ? a5 : 0, a3, a4, a6);
+            rc = build_sweep_plan(e, active, a1, a2, nov >= 5 ? a5 : 0, a3, a4, a6, a7);
         else if (ov)
             rc = (rfb_set_error("sweep plan \"%s\" names no sweep variant", ov), -1);
         else if (!rfb_tune_enabled())
@@ -1653,6 +1703,7 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->ring_depth = e->plan.ns;
     out->tma = e->plan.tma;
     out->unified = e->plan.uni;
+    out->interior_ring2 = e->plan.i2;
     out->interior_items = e->plan.n_int;
     out->edge_items = e->plan.n_edge + e->plan.n_qe + e->plan.n_qx;
     size_t sca = 0;

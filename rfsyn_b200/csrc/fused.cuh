@@ -59,6 +59,10 @@ struct FusedPlan {
     // modes >= 2, uni = 1: every item (interior sub 5, x slab sub 6, slab /
     // boundary subs 0-4) in the one edge list, one launch of k_sweep_q<KIND 5>
     int uni = 0;
+    // modes 2, 3, FP32: 0, or the ring depth of the interior sweep whose
+    // threads own two rows of a 2 tj-row tile (k_sweep_q_i2); its interior
+    // items are then 2 tj rows high
+    int i2 = 0;
     int n_qe = 0, n_qx = 0;                         // modes 2, 3: edge and x-slab items of k_sweep_q
     SweepItem *d_qe = nullptr, *d_qx = nullptr;
     int *d_queue = nullptr;                         // counters (interior 0-1, edge 2-3, x slab 4-5)

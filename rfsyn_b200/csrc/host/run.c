@@ -78,7 +78,7 @@ static int parse_flag(const char *v, int *out) {
     return -1;
 }
 
-/* 4 to 6 comma-separated integers >= 0, nothing else */
+/* 4 to 7 comma-separated integers >= 0, nothing else */
 static int plan_text_ok(const char *v) {
     int n = 0;
     const char *p = v;
@@ -93,7 +93,7 @@ static int plan_text_ok(const char *v) {
             return 0;
         }
     }
-    return n >= 4 && n <= 6;
+    return n >= 4 && n <= 7;
 }
 
 int fdtd_b200_apply_setting(const char *key, const char *value) {
@@ -517,6 +517,7 @@ int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info) {
     info->unified = ei.unified;
     info->interior_items = ei.interior_items;
     info->edge_items = ei.edge_items;
+    info->interior_ring2 = ei.interior_ring2;
     return 0;
 }
 

@@ -618,6 +618,260 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     q_leave(queue);
 }
 
+// ---- interior tiles of two rows per thread ---------------------------------------
+// The interior march of q_item (KIND 0: no slab, no boundary) over a tile of
+// 2 TJ rows x 32 columns with TJ warps: thread (tx, ty) owns the cells of
+// rows ty and ty + TJ, so the plane's fixed work -- the copy wait, the block
+// barrier, the ring bookkeeping, the halo row and column -- is shared by
+// twice the cells, and each thread has two independent cells' arithmetic to
+// interleave.  Same operations in the same order per cell as q_item, so the
+// results are bit-identical.
+template <typename T, int TJ, int NS>
+struct QLayoutI2 {
+    using S = QShape<T, 2 * TJ, 32>;
+    static constexpr size_t stage = S::stage;
+    static constexpr size_t bars = NS * stage;
+    static constexpr size_t sh = bars + round128(8 * NS);
+    static constexpr size_t tabs = sh + round128(sizeof(T) * 2 * 3 * (2 * TJ + 1) * 33);
+    static constexpr size_t misc = tabs + round128(sizeof(TileTables<T, TJ>));
+    static constexpr size_t total = misc + 16;
+};
+
+template <typename T, int TJ, int NS>
+__device__ __forceinline__ bool q_item_i2(const Args<T> &a, const TmaMaps &maps, const SweepItem &it,
+                                          unsigned char *smem_raw, unsigned &phase, unsigned &pending, bool &failed) {
+    constexpr int TR = 2 * TJ;
+    using L = QShape<T, TR, 32>;
+    using S = QLayoutI2<T, TJ, NS>;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
+    T(*sHb)[3][TR + 1][33] = reinterpret_cast<T(*)[3][TR + 1][33]>(smem_raw + S::sh);
+    TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
+    auto E = [&](int s, int c) { return reinterpret_cast<T(*)[L::EW]>(smem_raw + s * S::stage + c * L::ebox); };
+    auto H = [&](int s, int c) {
+        return reinterpret_cast<T(*)[L::HW]>(smem_raw + s * S::stage + 3 * L::ebox + c * L::hbox);
+    };
+    auto CODE = [&](int s) {
+        return reinterpret_cast<uint8_t(*)[32]>(smem_raw + s * S::stage + 3 * L::ebox + 3 * L::hbox);
+    };
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const bool px = a.per & 1u;
+    const bool with_codes = a.codes != nullptr;
+    const unsigned tx_bytes = 3 * L::ebytes + 3 * L::hbytes + (with_codes ? L::cbytes : 0u);
+    const T cbh = a.cbh;
+    const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
+    const int q = tx + 4, qs = tx + 1;
+    const bool colh = tx < TR;
+
+    auto issue = [&](int s, int p) {
+        if (p < 0 || failed) return;
+        if (tid == 4 * 32) {
+            mbar_expect_tx(&bars[s], tx_bytes);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                tma_load_3d(E(s, c), &maps.e2[c], k0 - 4, j0 - 1, p, &bars[s]);
+                tma_load_3d(H(s, c), &maps.h2[c], k0 - 4, j0 - 1, p, &bars[s]);
+            }
+            if (with_codes) tma_load_3d(CODE(s), &maps.code2, k0, j0, p, &bars[s]);
+        }
+        pending |= 1u << s;
+    };
+    auto wait_slot = [&](int s) {
+        if (!(pending & (1u << s))) return;
+        if (failed || !mbar_wait(&bars[s], (phase >> s) & 1u)) {
+            failed = true;
+            return;
+        }
+        phase ^= 1u << s;
+        pending &= ~(1u << s);
+    };
+    // unstretched H of component c at stage position (rr, qq) of the plane
+    // in slot sc (the plane after it in slot sn): q_item's arithmetic
+    auto hval = [&](int c, int sc, int sn, int rr, int qq) -> T {
+        T dA, dB;
+        if (c == 0) {
+            dA = xs(E(sc, 2)[rr + 1][qq], E(sc, 2)[rr][qq]);
+            dB = xs(E(sc, 1)[rr][qq + 1], E(sc, 1)[rr][qq]);
+        } else if (c == 1) {
+            dA = xs(E(sc, 0)[rr][qq + 1], E(sc, 0)[rr][qq]);
+            dB = xs(E(sn, 2)[rr][qq], E(sc, 2)[rr][qq]);
+        } else {
+            dA = xs(E(sn, 1)[rr][qq], E(sc, 1)[rr][qq]);
+            dB = xs(E(sc, 0)[rr + 1][qq], E(sc, 0)[rr][qq]);
+        }
+        return upd_h(H(sc, c)[rr][qq], cbh, xs(dA, dB));
+    };
+
+    int pprev = ib > 0 ? ib - 1 : (px ? a.nx - 1 : -1);
+    int pf = ib;
+    issue(NS - 1, pprev);
+#pragma unroll
+    for (int s = 0; s < NS - 1; s++) {
+        if (pf >= 0 && ib + s <= ie) issue(s, pf);
+        if (pf >= 0) pf = plane_after(pf, a.nx, px);
+    }
+    wait_slot(NS - 1);
+    wait_slot(0);
+    if (__syncthreads_or(failed)) return false;
+    T prevHy[2] = {T(0), T(0)}, prevHz[2] = {T(0), T(0)};
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        const int r = ty + u * TJ + 1;
+        prevHy[u] = H(NS - 1, 1)[r][q];
+        prevHz[u] = H(NS - 1, 2)[r][q];
+        if (pprev >= 0) {
+            prevHy[u] = hval(1, NS - 1, 0, r, q);
+            prevHz[u] = hval(2, NS - 1, 0, r, q);
+        }
+    }
+    __syncthreads();  // slot NS-1 may now be refilled
+
+    int sc = 0;
+    for (int i = ib; i < ie; i++) {
+        const int sn = sc == NS - 1 ? 0 : sc + 1;
+        const int sf = sc == 0 ? NS - 1 : sc - 1;
+        if (pf >= 0 && i + NS - 1 <= ie) {
+            issue(sf, pf);
+            pf = plane_after(pf, a.nx, px);
+        }
+        wait_slot(sn);
+        T(*sH)[TR + 1][33] = sHb[(i - ib) & 1];
+        T e0[2], e1[2], e2[2], hy[2], hz[2];
+        int code[2];
+        long long c[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int row = ty + u * TJ, r = row + 1;
+            e0[u] = E(sc, 0)[r][q];
+            e1[u] = E(sc, 1)[r][q];
+            e2[u] = E(sc, 2)[r][q];
+            code[u] = with_codes ? (int)CODE(sc)[row][tx] : 0;
+            c[u] = (long long)i * a.plane + (long long)(j0 + row) * a.pitch + (k0 + tx);
+            const T hx = hval(0, sc, sn, r, q);
+            hy[u] = hval(1, sc, sn, r, q);
+            hz[u] = hval(2, sc, sn, r, q);
+            a.Ho[0][c[u]] = hx;
+            a.Ho[1][c[u]] = hy[u];
+            a.Ho[2][c[u]] = hz[u];
+            sH[0][r][qs] = hx;
+            sH[1][r][qs] = hy[u];
+            sH[2][r][qs] = hz[u];
+        }
+        // halo: row (j0-1) Hx by warp 0, Hz by warp 2; column (k0-1) Hx by
+        // warp 1, Hy by warp 3 (lanes of the tile's 2 TJ rows)
+        if (ty == 0) sH[0][0][qs] = hval(0, sc, sn, 0, q);
+        else if (ty == 2) sH[2][0][qs] = hval(2, sc, sn, 0, q);
+        else if (ty == 1 && colh) sH[0][tx + 1][0] = hval(0, sc, sn, tx + 1, 3);
+        else if (ty == 3 && colh) sH[1][tx + 1][0] = hval(1, sc, sn, tx + 1, 3);
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int r = ty + u * TJ + 1;
+            if (!with_codes || code[u] != LIST_CODE) {
+                const T ca = tt.tab[code[u]], cb = tt.tab[256 + code[u]];
+                a.Eo[0][c[u]] = upd_e(ca, e0[u], cb, xs(xs(sH[2][r][qs], sH[2][r - 1][qs]),
+                                                          xs(sH[1][r][qs], sH[1][r][qs - 1])));
+                a.Eo[1][c[u]] = upd_e(ca, e1[u], cb, xs(xs(sH[0][r][qs], sH[0][r][qs - 1]), xs(hz[u], prevHz[u])));
+                a.Eo[2][c[u]] = upd_e(ca, e2[u], cb, xs(xs(hy[u], prevHy[u]), xs(sH[0][r][qs], sH[0][r - 1][qs])));
+            }
+            prevHy[u] = hy[u];
+            prevHz[u] = hz[u];
+        }
+        sc = sn;
+    }
+    return !__syncthreads_or(failed);
+}
+
+// The interior queue with tiles of two rows per thread (KIND 0 items of
+// 2 TJ rows).
+template <typename T, int TJ, int NS, int MINB>
+__global__ void __launch_bounds__(32 * TJ, MINB)
+    k_sweep_q_i2(Args<T> a, const SweepItem *items, int n_items, const __grid_constant__ TmaMaps maps, int *queue,
+                 int *err) {
+    static_assert(NS >= 3 && TJ >= 5, "ring of three planes; warps 0-3 recompute halos, warp 4 issues copies");
+    using S = QLayoutI2<T, TJ, NS>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    if (q_misaligned(smem_raw, err)) return;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::bars);
+    volatile int *s_item = reinterpret_cast<volatile int *>(smem_raw + S::misc);
+    q_init_bars<NS>(bars);
+    {
+        TileTables<T, TJ> &tt = *reinterpret_cast<TileTables<T, TJ> *>(smem_raw + S::tabs);
+        const int tid = threadIdx.y * 32 + threadIdx.x;
+        for (int t = tid; t < 256; t += 32 * TJ) {
+            tt.tab[t] = a.tca[t];
+            tt.tab[256 + t] = a.tcb[t];
+        }
+    }
+    __syncthreads();
+    unsigned phase = 0, pending = 0;
+    bool failed = false;
+    for (;;) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) *s_item = atomicAdd(&queue[0], 1);
+        __syncthreads();
+        const int w = *s_item;
+        if (w >= n_items) break;
+        const SweepItem it = items[w];
+        if (!q_item_i2<T, TJ, NS>(a, maps, it, smem_raw, phase, pending, failed)) {
+            q_bail<NS>(bars, phase, pending, err);
+            break;
+        }
+        __syncthreads();
+    }
+    q_leave(queue);
+}
+
+// Variants of the two-rows interior (FP32 only): (TJ, NS, CTAs per SM).
+#define RFB_QI2_VARIANTS(X) X(8, 3, 3) X(8, 4, 2)
+
+template <typename T>
+inline int qi2_grid(int ns) {
+    static int g[8] = {};
+    int &gv = g[ns & 7];
+    if (!gv) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+#define RFB_QI2_OCC(TJ_, NS_, MB_)                                                                         \
+        if (ns == NS_)                                                                                     \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweep_q_i2<float, TJ_, NS_, MB_>, 32 * TJ_, \
+                                                          QLayoutI2<float, TJ_, NS_>::total);
+        RFB_QI2_VARIANTS(RFB_QI2_OCC)
+#undef RFB_QI2_OCC
+        gv = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
+    }
+    return gv;
+}
+
+// Launch over n two-row interior items (FP32; plan variant `ns`).
+inline void launch_q_i2(const Args<float> &a, int ns, const SweepItem *items, int n, const TmaMaps &m, int *queue,
+                        int *err, cudaStream_t st) {
+    if (n <= 0) return;
+#define RFB_QI2_LAUNCH(TJ_, NS_, MB_)                                                                      \
+    if (ns == NS_) {                                                                                       \
+        const int g = std::min(n, qi2_grid<float>(NS_));                                                   \
+        k_sweep_q_i2<float, TJ_, NS_, MB_><<<g, dim3(32, TJ_), QLayoutI2<float, TJ_, NS_>::total, st>>>(    \
+            a, items, n, m, queue, err);                                                                   \
+    }
+    RFB_QI2_VARIANTS(RFB_QI2_LAUNCH)
+#undef RFB_QI2_LAUNCH
+}
+
+static inline int qi2_prepare() {
+    static int done = 0;
+    if (done) return 0;
+    cudaError_t e = cudaSuccess;
+#define RFB_QI2_PREP(TJ_, NS_, MB_)                                                                        \
+    if (e == cudaSuccess)                                                                                  \
+        e = cudaFuncSetAttribute(k_sweep_q_i2<float, TJ_, NS_, MB_>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)QLayoutI2<float, TJ_, NS_>::total);                                  \
+    if (e == cudaSuccess) (void)qi2_grid<float>(NS_);
+    RFB_QI2_VARIANTS(RFB_QI2_PREP)
+#undef RFB_QI2_PREP
+    if (e != cudaSuccess) return -1;
+    done = 1;
+    return 0;
+}
+
 // Variants (element type, TJ, NS, CTAs per SM of the interior and of the
 // edge instantiation): interior and edge share the tile height and ring
 // depth of a plan.

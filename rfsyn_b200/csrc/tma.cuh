@@ -30,6 +30,7 @@ namespace rfb {
 struct TmaMaps {
     CUtensorMap e[3], h[3], code;
     CUtensorMap en[3], hn[3], coden;
+    CUtensorMap e2[3], h2[3], code2;  // interior tiles of 2 TJ rows x 32 columns
 };
 
 constexpr int TMA_EW = 40;  // E box width (k0-4 .. k0+35)

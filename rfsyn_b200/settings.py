@@ -12,7 +12,7 @@ the "gpu.<name>" keys of the "fdtd" section, which rfsyn's own
 
   process-wide (applied through fdtd_b200_apply_setting):
     gpu.precision  "fp32" | "fp64"     gpu.schedule  "fused" | "split"
-    gpu.plan       "auto" | "tj,ns,seg_interior,seg_edge[,mode[,single_queue]]"
+    gpu.plan       "auto" | "tj,ns,seg_interior,seg_edge[,mode[,single_queue[,two_rows_ring]]]"
     gpu.tune       bool                gpu.trace     bool
   per run (read by run_examples):
     gpu.batch       examples simulated together in one batch (default 1)

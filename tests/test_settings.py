@@ -201,7 +201,7 @@ def test_process_settings_round_trip(restore_settings, monkeypatch):
     settings.apply_setting("trace", "0")
     assert settings.get_setting("trace") == "false"
     # refused values name the setting and leave it unchanged
-    for key, bad in [("precision", "fp16"), ("schedule", "fast"), ("plan", "8,4"), ("plan", "8,4,32,16,4,1,0"),
+    for key, bad in [("precision", "fp16"), ("schedule", "fast"), ("plan", "8,4"), ("plan", "8,4,32,16,4,1,0,0"),
                      ("plan", "8,-4,32,16"), ("plan", "8,4,32,16,"), ("plan", "a,b,c,d"), ("tune", "yes"),
                      ("trace", "")]:
         before = settings.get_setting(key)

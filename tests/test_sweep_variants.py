@@ -28,20 +28,23 @@ pytestmark = pytest.mark.gpu
 # cp.async interior, 1 TMA interior, 2 work-queue sweeps, 3 work-queue
 # sweeps with tile origins shifted to the slab edges, 4 work-queue sweeps
 # with narrow (2 tj x 16) tiles over the z slabs (no periodic y / z); a
-# fourth value 1 puts every item of modes 2-4 in one queue (one launch)
+# fourth value 1 puts every item of modes 2-4 in one queue (one launch); a
+# fifth value 3 or 4 gives the interior tiles of modes 2, 3 to the sweep
+# whose threads own two rows (FP32; that value is its ring depth)
 VARIANTS = {
     rb.FP64: [(8, 3, 2), (8, 4, 2), (8, 3, 3), (8, 4, 3), (8, 3, 4), (8, 4, 4), (8, 4, 2, 1), (8, 3, 4, 1),
               (8, 3, 1), (8, 4, 1), (8, 4, 0), (16, 2, 0)],
     rb.FP32: [(8, 4, 2), (8, 3, 2), (16, 3, 2), (8, 4, 3), (16, 3, 3), (8, 4, 4), (8, 3, 4), (16, 3, 4),
               (8, 4, 2, 1), (8, 4, 4, 1), (16, 3, 4, 1), (8, 4, 1), (8, 3, 1), (16, 3, 1), (8, 6, 0), (8, 5, 0),
-              (16, 4, 0), (16, 3, 0)],
+              (8, 4, 2, 0, 3), (8, 4, 2, 0, 4), (8, 3, 3, 0, 3), (16, 4, 0), (16, 3, 0)],
 }
 QUEUE = [v for v in VARIANTS[rb.FP64] if v[2] >= 2]
 MODE = {0: "cpasync", 1: "tma", 2: "queue", 3: "queue_shifted", 4: "queue_narrow"}
 
 
 def _vid(v):
-    return "tj%d_ns%d_%s%s" % (v[0], v[1], MODE[v[2]], "_single" if len(v) > 3 and v[3] else "")
+    return "tj%d_ns%d_%s%s%s" % (v[0], v[1], MODE[v[2]], "_single" if len(v) > 3 and v[3] else "",
+                                 "_tworows%d" % v[4] if len(v) > 4 and v[4] else "")
 
 SCENES = {
     # the headline recipe at 104^3 (5-cell CPML): interior tiles at k0 = 32, 64
@@ -70,7 +73,8 @@ def wants():
 def _run(s: Scene, precision: int, variant, monkeypatch, need_interior=True):
     tj, ns, tma = variant[:3]
     uni = variant[3] if len(variant) > 3 else 0
-    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma},{uni}")
+    i2 = variant[4] if len(variant) > 4 else 0
+    monkeypatch.setenv("RFSYN_FDTD_PLAN", f"{tj},{ns},32,16,{tma},{uni},{i2}")
     rc = scene_run_config(s, precision, rb.FUSED)
     cs = s.to_c()
     needs_setup = bool(s.boxes or s.comps or s.tensors or s.disp or s.spheres or s.tensor3)
@@ -78,7 +82,7 @@ def _run(s: Scene, precision: int, variant, monkeypatch, need_interior=True):
                  C.cast(C.pointer(cs), C.c_void_p) if needs_setup else None)
     try:
         info = sim.info()
-        assert (info.tile_j, info.ring_depth, info.tma, info.unified) == (tj, ns, tma, uni)
+        assert (info.tile_j, info.ring_depth, info.tma, info.unified, info.interior_ring2) == (tj, ns, tma, uni, i2)
         assert info.edge_items > 0
         if need_interior and not uni:
             assert info.interior_items > 0
@@ -129,6 +133,12 @@ def test_queue_sweep_boundary_cases_fp64_bit_exact(name, variant, monkeypatch):
     want = oracle.run_oracle(s)
     td, dft = _run(s, rb.FP64, variant, monkeypatch, need_interior=False)
     assert np.array_equal(td, want["td"])
+
+
+def test_two_rows_interior_is_fp32_only(monkeypatch):
+    monkeypatch.setenv("RFSYN_FDTD_PLAN", "8,4,32,16,2,0,4")
+    with pytest.raises(RuntimeError, match="two-rows interior"):
+        rb.Sim(scene_run_config(SCENES["c2_104"], rb.FP64, rb.FUSED))
 
 
 def test_plan_override_rejects_unknown_variant(monkeypatch):
