@@ -1321,11 +1321,14 @@ fail:
 
 extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     if (!e) return;
+    double t_phase = rfb_now();
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (int q = 0; q < 2; q++) {
         if (e->g1[q]) cudaGraphExecDestroy(e->g1[q]);
         if (e->gk[q]) cudaGraphExecDestroy(e->gk[q]);
     }
+    rfb_trace("destroy: graphs", t_phase);
+    t_phase = rfb_now();
     dfree(e->fld_base);
     devcpml_free(e->cpml);
     devscene_free(e->scene);
@@ -1343,11 +1346,14 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     dfree(e->tf_h_first); dfree(e->tf_h_count); dfree(e->tf_h_idx); dfree(e->tf_h_coef); dfree(e->tf_h_w);
     dfree(e->tf_e_first); dfree(e->tf_e_count); dfree(e->tf_e_idx); dfree(e->tf_e_coef);
     dfree(e->tf_e_w);
+    rfb_trace("destroy: device buffers", t_phase);
+    t_phase = rfb_now();
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->stream2) cudaStreamDestroy(e->stream2);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
+    rfb_trace("destroy: streams and host state", t_phase);
 }
 
 // Cells whose three list entries are 3x3 samples without a source go to the
