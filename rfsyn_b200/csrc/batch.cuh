@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
     k_sweep_qb(const Args<T> *args, const FusedDims *dims, const TmaMaps *maps, const BatchItem *items, int n_items,
                int *queue, int *err) {
     static_assert(NS >= 3, "the ring must hold the current, the next and one prefetched plane");
-    static_assert(TJ >= 3, "warps 0-2 share the halo recomputation");
+    static_assert(TJ >= 5, "warps 0-3 share the halo recomputation, warp 4 issues the copies");
     using S = QLayout<T, TJ, NS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     if (q_misaligned(smem_raw, err)) return;
@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(32 * TJ, MINB)
         const BatchItem bi = items[w];
         if (bi.scene != cur) {
             load_args(sa, args + bi.scene, 32 * TJ, tid);
-            if (tid == 0) tensormap_acquire(maps + bi.scene);
+            // the fence orders the maps for the thread that issues the copies
+            if (tid == kCopyIssueTid) tensormap_acquire(maps + bi.scene);
             __syncthreads();
             q_load_table<T, TJ, NS>(sa, smem_raw);
             __syncthreads();

@@ -630,6 +630,9 @@ struct rfb_engine {
     // t3_kinds keeps the image's kinds to undo it
     int *t3_cells = nullptr;
     int n_t3_cells = 0;
+    // the list entries outside those cells (k_e_list's work), or none
+    int *list_work = nullptr;
+    int n_list_work = 0;
     std::vector<uint8_t> t3_kinds;
     std::vector<int> t3_host;
     size_t h2d_bytes = 0, n_ade = 0;
@@ -662,6 +665,10 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
     fill_scene_args(a, e->scene);
     a.src_val = (const T *)e->src_val;
     a.src_hard = e->src_hard;
+    if (e->n_t3_cells) {
+        a.l_work = e->list_work;
+        a.n_work = e->n_list_work;
+    }
     a.n_steps = (long long)e->n_steps;
     a.d_step = e->d_step;
     if (e->tf_on) {
@@ -775,6 +782,12 @@ static void launch_sweep(rfb_engine *e, const Args<T> &a, int par) {
     cudaStreamWaitEvent(e->stream, e->ev_join, 0);
 }
 
+// Threads of the interface-list launch: its work entries, or every entry.
+template <typename T>
+static int list_launch_n(const Args<T> &a) {
+    return a.l_work ? a.n_work : 3 * a.n_cells;
+}
+
 // Plane probes of the step: their means join the series before the point
 // probes advance the step counter.
 template <typename T>
@@ -798,7 +811,7 @@ static void enqueue_step(rfb_engine *e, int par) {
         k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
     }
     tf_before_list<T>(e, par);
-    if (a.n_cells) k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
+    if (a.n_cells && list_launch_n(a)) k_e_list<T><<<(list_launch_n(a) + 255) / 256, 256, 0, e->stream>>>(a);
     if (e->n_t3_cells) k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
     ProbeArgs<T> p;
     p.n = e->n_probes;
@@ -828,7 +841,7 @@ static int count_step_launches(const rfb_engine *e) {
     int n = (e->sched == RFB_SCHED_FUSED)
                 ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0)
                 : 2;
-    if (e->scene.n_cells) n++;
+    if (e->scene.n_cells && (!e->n_t3_cells || e->n_list_work)) n++;
     if (e->n_t3_cells) n++;
     if (e->tf_on) n += 2 + (e->tf_n_h > 0);
     if (e->n_planes) n++;
@@ -1335,6 +1348,7 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     dfree(e->src_val); dfree(e->src_hard);
     dfree(e->probe_cell); dfree(e->probe_comp); dfree(e->ts); dfree(e->d_step); dfree(e->d_err); dfree(e->d_energy); dfree(e->d_iq);
     dfree(e->t3_cells);
+    dfree(e->list_work);
     dfree(e->d_planes);
     dfree(e->d_fout[0]);
     dfree(e->d_fout[1]);
@@ -1376,6 +1390,21 @@ static int group_t3_cells(rfb_engine *e, const rfb_scene_image_t *img) {
         rfb_set_error("3x3 cell list upload failed");
         return -1;
     }
+    {
+        // the list kernel runs only over the entries left to it
+        std::vector<int> work;
+        work.reserve(ne - 3 * cells.size());
+        for (size_t q = 0; q < ne; q++)
+            if (kinds[q] != RFB_LK_CELL3) work.push_back((int)q);
+        if (!work.empty()) {
+            e->list_work = dev_copy(work.data(), work.size());
+            if (!e->list_work) {
+                rfb_set_error("list work upload failed");
+                return -1;
+            }
+        }
+        e->n_list_work = (int)work.size();
+    }
     CK(cudaMemcpy(e->scene.l_kind, kinds.data(), ne, cudaMemcpyHostToDevice));
     e->n_t3_cells = (int)cells.size();
     e->t3_host = cells;
@@ -1389,6 +1418,9 @@ static int ungroup_t3_cells(rfb_engine *e) {
     if (!e->n_t3_cells) return 0;
     CK(cudaMemcpy(e->scene.l_kind, e->t3_kinds.data(), e->t3_kinds.size(), cudaMemcpyHostToDevice));
     e->n_t3_cells = 0;
+    dfree(e->list_work);
+    e->list_work = nullptr;
+    e->n_list_work = 0;
     return 0;
 fail:
     return -1;
@@ -1750,12 +1782,14 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         CK(cudaEventRecord(ev[1], e->stream));
         tf_before_list<T>(e, par);
         if (a.n_cells) {
-            k_e_list<T><<<(3 * a.n_cells + 255) / 256, 256, 0, e->stream>>>(a);
+            if (list_launch_n(a)) {
+                k_e_list<T><<<(list_launch_n(a) + 255) / 256, 256, 0, e->stream>>>(a);
+                g_launches++;
+            }
             if (e->n_t3_cells) {
                 k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
                 g_launches++;
             }
-            g_launches++;
         }
         ProbeArgs<T> p;
         p.n = e->n_probes;

@@ -1140,6 +1140,39 @@ void rfb_scene_build_free(rfb_scene_build_t *b) {
     memset(b, 0, sizeof(*b));
 }
 
+
+/* Record dedupe of 3x3 samples: an open-addressing table over the records
+ * built so far, keyed by their five values' bits. */
+typedef struct {
+    int32_t *slot;  /* record index + 1, 0 empty */
+    size_t mask;
+} t3_dedupe_t;
+
+static uint64_t t3_hash(const double *r) {
+    uint64_t h = 1469598103934665603ull;
+    for (int q = 0; q < 5; q++) {
+        uint64_t b;
+        memcpy(&b, &r[q], sizeof b);
+        h = (h ^ b) * 1099511628211ull;
+        h ^= h >> 29;
+    }
+    return h;
+}
+
+/* The index of the record just written at recs[5 * *n]: an earlier equal
+ * record's, or *n (then *n grows). */
+static int32_t t3_record_index(t3_dedupe_t *d, double *recs, size_t *n) {
+    const double *r = recs + 5 * *n;
+    for (size_t h = t3_hash(r) & d->mask;; h = (h + 1) & d->mask) {
+        const int32_t s = d->slot[h];
+        if (!s) {
+            d->slot[h] = (int32_t)(*n + 1);
+            return (int32_t)(*n)++;
+        }
+        if (!memcmp(recs + 5 * (size_t)(s - 1), r, 5 * sizeof(double))) return s - 1;
+    }
+}
+
 int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n_extra, const rfb_extra_cell_t *extra,
                           rfb_scene_build_t *out) {
     memset(out, 0, sizeof(*out));
@@ -1147,6 +1180,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         rfb_set_error("materials do not match the grid");
         return -1;
     }
+    t3_dedupe_t t3d = {NULL, 0};
     const size_t nz1 = g->nz + 1;
     /* 1. cells on the interface list (padded linear index) */
     size_t cap = mat->scalar.count + mat->tensor.count + mat->disp.count + mat->tensor3.count + n_extra;
@@ -1235,8 +1269,12 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     out->t_uv = calloc(16 * tcap, sizeof(int32_t));
     out->t_sign = calloc(tcap, sizeof(int32_t));
     out->t3 = malloc((5 * mat->tensor3.count + 5) * sizeof(double));
+    size_t t3cap = 2;
+    while (t3cap < 2 * mat->tensor3.count + 2) t3cap *= 2;
+    t3d.slot = calloc(t3cap, sizeof(int32_t));
+    t3d.mask = t3cap - 1;
     if (!out->cell_ijk || !out->kind || !out->ca || !out->cb || !out->tix || !out->src || !out->aix || !out->t_m11 ||
-        !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign || !out->t3)
+        !out->t_scale || !out->t_w || !out->t_main || !out->t_nq || !out->t_uv || !out->t_sign || !out->t3 || !t3d.slot)
         goto oom;
     size_t nt = 0, nt3 = 0;
     /* ADE records, deduplicated by model */
@@ -1284,7 +1322,10 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
                 rec[3] = (mat->dt / (EPS0 * mat->dx)) / (1.0 + loss);
                 rec[4] = (1.0 - loss) / (1.0 + loss);
                 out->kind[e] = RFB_LK_TENSOR3;
-                out->tix[e] = (int32_t)nt3++;
+                /* samples with the same record share it (a uniform anisotropic
+                 * region is one record per component): fewer record bytes
+                 * for the list kernels to read */
+                out->tix[e] = t3_record_index(&t3d, out->t3, &nt3);
                 continue;
             }
             const double *t = (c < 2) ? tensor_at(mat, idx, c) : NULL;
@@ -1369,6 +1410,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
             rfb_set_error("two sources on the same field sample");
             free(models);
             free(cells);
+            free(t3d.slot);
             rfb_scene_build_free(out);
             return -1;
         }
@@ -1396,9 +1438,11 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
     img->t_w = out->t_w;
     img->t_uv = out->t_uv;
     img->t_sign = out->t_sign;
+    free(t3d.slot);
     return 0;
 oom:
     free(cells);
+    free(t3d.slot);
     rfb_scene_build_free(out);
     rfb_set_error("out of host memory building the scene image");
     return -1;

@@ -72,6 +72,10 @@ struct Args {
     long long skip[MAX_SKIP];
     // interface list
     int n_cells;
+    // NULL, or the n_work entries k_e_list updates (the others belong to
+    // cells k_t3_cells updates whole)
+    const int *l_work;
+    int n_work;
     const int *lc_ijk;
     const uint8_t *l_kind;
     const T *l_ca, *l_cb;
@@ -487,9 +491,13 @@ __global__ void k_inc_e(TfArgs<T> a) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= 3 * a.n_cells) return;
-    e_list_entry(a, e);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.l_work) {
+        if (t < a.n_work) e_list_entry(a, a.l_work[t]);
+        return;
+    }
+    if (t >= 3 * a.n_cells) return;
+    e_list_entry(a, t);
 }
 
 // ---- probes ---------------------------------------------------------------

@@ -42,6 +42,12 @@
 
 namespace rfb {
 
+// The thread that issues a CTA's tensor copies (warp 4, lane 0; warps 0-3
+// recompute the halo H).  Where the tensor maps live in global memory (the
+// batched sweep), this thread is also the one that acquires them through the
+// tensormap proxy before its first copy of a scene.
+constexpr int kCopyIssueTid = 4 * 32;
+
 template <typename T, int TJ>
 struct TileTables {
     T tab[512];           // Ca (0..255), Cb (256..511)
@@ -127,7 +133,7 @@ __device__ __forceinline__ bool q_item(const Args<T> &a, const FusedDims &d, con
     // issues the copies, so no warp carries two extra jobs per plane
     auto issue = [&](int s, int p) {
         if (p < 0 || failed) return;  // a failed CTA issues no further copies
-        if (tid == 4 * 32) {
+        if (tid == kCopyIssueTid) {
             mbar_expect_tx(&bars[s], tx_bytes);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -664,7 +670,7 @@ __device__ __forceinline__ bool q_item_i2(const Args<T> &a, const TmaMaps &maps,
 
     auto issue = [&](int s, int p) {
         if (p < 0 || failed) return;
-        if (tid == 4 * 32) {
+        if (tid == kCopyIssueTid) {
             mbar_expect_tx(&bars[s], tx_bytes);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
