@@ -437,7 +437,10 @@ def run_b200(args) -> None:
                    "sweep_mode": {0: "cp.async", 1: "tma-interior", 2: "tma-queue", 3: "tma-queue-shifted",
                                   4: "tma-queue-narrow-z"}.get(info.tma),
                    "ring_depth": info.ring_depth, "single_queue": bool(info.unified),
-                   "seg_len": info.seg_len, "parallelism": f"scene-replicas x{world}",
+                   "seg_len": info.seg_len, "seg_edge": info.seg_edge, "two_rows_ring": info.interior_ring2,
+                   "plan": f"{info.tile_j},{info.ring_depth},{info.seg_len},{info.seg_edge},{info.tma},"
+                           f"{info.unified},{info.interior_ring2}",
+                   "parallelism": f"scene-replicas x{world}",
                    "l2": f"inputs larger than L2 (fields 6 x 2 x {field_mb:.0f} MB per scene)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": SWEEP_KERNEL.get(info.tma, "k_h_split + k_e_split"),
@@ -711,7 +714,8 @@ def run_profile(args) -> None:
     setup = scenes.scene_setup(w)
     sim = rb.Sim(scenes.run_config(w), setup.ptr if setup else None, None)
     info = sim.info()
-    print(f"plan: mode {info.tma}, rows {info.tile_j}, ring {info.ring_depth}, segment {info.seg_len}, "
+    print(f"plan: {info.tile_j},{info.ring_depth},{info.seg_len},{info.seg_edge},{info.tma},{info.unified},"
+          f"{info.interior_ring2} (rows, ring, interior / edge segments, mode, single queue, two-rows ring); "
           f"interior items {info.interior_items}, edge items {info.edge_items}, list cells {info.list_cells}",
           flush=True)
     sweep_ms, other_ms = sim.time_kernels(steps)

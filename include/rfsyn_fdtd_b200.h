@@ -212,6 +212,7 @@ typedef struct {
     int unified;             /* 1: every sweep item in one work queue, one launch per step */
     int interior_ring2;      /* 0, or the ring depth of the interior sweep whose threads own two
                                 rows of a 2 tile_j-row tile */
+    int seg_edge;            /* planes per slab / boundary work item */
 } fdtd_b200_sim_info_t;
 
 int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info);

@@ -111,7 +111,7 @@ class SimInfo(C.Structure):
                 ("slab_cell_axes", C.c_size_t), ("h2d_bytes", C.c_size_t), ("precision", C.c_int),
                 ("schedule", C.c_int), ("tile_j", C.c_int), ("seg_len", C.c_int),
                 ("ring_depth", C.c_int), ("tma", C.c_int), ("interior_items", C.c_int),
-                ("edge_items", C.c_int), ("unified", C.c_int), ("interior_ring2", C.c_int)]
+                ("edge_items", C.c_int), ("unified", C.c_int), ("interior_ring2", C.c_int), ("seg_edge", C.c_int)]
 
 
 class Energy(C.Structure):

@@ -1742,6 +1742,7 @@ extern "C" int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out) {
     out->tma = e->plan.tma;
     out->unified = e->plan.uni;
     out->interior_ring2 = e->plan.i2;
+    out->seg_edge = e->plan.seg_edge;
     out->interior_items = e->plan.n_int;
     out->edge_items = e->plan.n_edge + e->plan.n_qe + e->plan.n_qx;
     size_t sca = 0;

@@ -207,6 +207,7 @@ typedef struct {
     size_t list_cells, dispersive, slab_cell_axes, h2d_bytes;
     int tile_j, seg_len, ring_depth, tma, interior_items, edge_items, unified;
     int interior_ring2;  /* 0, or the ring depth of the two-rows interior sweep */
+    int seg_edge;        /* planes per slab / boundary work item */
 } rfb_engine_info_t;
 int rfb_engine_info(rfb_engine_t *e, rfb_engine_info_t *out);
 int rfb_engine_time_kernels(rfb_engine_t *e, size_t n, double *sweep_ms, double *other_ms);

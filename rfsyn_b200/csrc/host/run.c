@@ -518,6 +518,7 @@ int fdtd_b200_sim_info(const fdtd_b200_sim_t *sim, fdtd_b200_sim_info_t *info) {
     info->interior_items = ei.interior_items;
     info->edge_items = ei.edge_items;
     info->interior_ring2 = ei.interior_ring2;
+    info->seg_edge = ei.seg_edge;
     return 0;
 }
 
