@@ -816,31 +816,38 @@ static void step(orc_t *o, const scn_scene_t *s, size_t n) {
 
 /* Mean of one component over a whole plane (plane probe), FP64, summed in
  * the order of the GPU's reduction so FP64 runs compare bit for bit: the
- * points t = u n_v + v (u outer) are dealt to 1024 partial sums, point t to
- * partial t mod 1024 in increasing t; each group of 32 partials is reduced by
- * halving (p[l] += p[l + h] for h = 16, 8, 4, 2, 1); the 32 group sums are
- * added in order; the total is divided by n_u n_v. */
+ * points t = u n_v + v (u outer) are cut into chunks of 1024; within a
+ * chunk, point t goes to partial sum (t - chunk start) mod 256 in increasing
+ * t; each group of 32 partials is reduced by halving (p[l] += p[l + h] for
+ * h = 16, 8, 4, 2, 1) and the 8 group sums are added in order, giving the
+ * chunk's sum; the chunks' sums are added in chunk order; the total is
+ * divided by n_u n_v. */
 static double plane_mean(const orc_t *o, const scn_plane_t *pl) {
     const int a = pl->axis, u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
     const double *f = field((orc_t *)o, pl->comp);
     const size_t nu = o->n[u], nv = o->n[v], npts = nu * nv;
-    double part[1024];
-    for (int t = 0; t < 1024; t++) part[t] = 0.0;
-    for (size_t t = 0; t < npts; t++) {
-        size_t ijk[3];
-        ijk[a] = pl->index;
-        ijk[u] = t / nv;
-        ijk[v] = t % nv;
-        part[t % 1024] = part[t % 1024] + f[at(o, ijk[0], ijk[1], ijk[2])];
+    double total = 0.0;
+    for (size_t t0 = 0; t0 < npts; t0 += 1024) {
+        const size_t t1 = t0 + 1024 < npts ? t0 + 1024 : npts;
+        double part[256];
+        for (int t = 0; t < 256; t++) part[t] = 0.0;
+        for (size_t t = t0; t < t1; t++) {
+            size_t ijk[3];
+            ijk[a] = pl->index;
+            ijk[u] = t / nv;
+            ijk[v] = t % nv;
+            part[(t - t0) % 256] = part[(t - t0) % 256] + f[at(o, ijk[0], ijk[1], ijk[2])];
+        }
+        double chunk = 0.0;
+        for (int w = 0; w < 8; w++) {
+            double *g = part + 32 * w;
+            for (int h = 16; h > 0; h >>= 1)
+                for (int l = 0; l < 32 - h; l++) g[l] = g[l] + g[l + h];
+            chunk = chunk + g[0];
+        }
+        total = total + chunk;
     }
-    double sum = 0.0;
-    for (int w = 0; w < 32; w++) {
-        double *g = part + 32 * w;
-        for (int h = 16; h > 0; h >>= 1)
-            for (int l = 0; l < 32 - h; l++) g[l] = g[l] + g[l + h];
-        sum = sum + g[0];
-    }
-    return sum / (double)npts;
+    return total / (double)npts;
 }
 
 /* Runs the scene; probe_td (n_probes + n_planes) * n_steps, dft_re/im

@@ -605,6 +605,11 @@ struct rfb_engine {
     // plane probes: series n_probes .. n_probes + n_planes - 1 of ts
     int n_planes = 0;
     PlaneDesc *d_planes = nullptr;
+    // the gather's per-chunk sums (n_planes x plane_chunks) and per-plane
+    // counters of finished chunks (zero between launches)
+    int plane_chunks = 0;
+    double *d_plane_part = nullptr;
+    int *d_plane_count = nullptr;
     void **d_fout[2] = {nullptr, nullptr};  // per parity: the six output components, for the plane gather
     // running DFT of every series: the bins (rad/s), t offset (steps), the
     // per (series, bin) sums (FP64: re, im; FP32: re, im, compensations)
@@ -630,6 +635,12 @@ struct rfb_engine {
     // t3_kinds keeps the image's kinds to undo it
     int *t3_cells = nullptr;
     int n_t3_cells = 0;
+    // cells whose three E samples are dispersive samples outside the CPML
+    // without source or TF/SF term, updated per cell by k_ade_cells (their
+    // list entries are kind 6)
+    int *ade_cells = nullptr;
+    int n_ade_cells = 0;
+    std::vector<int> ade_host;
     // the list entries outside those cells (k_e_list's work), or none
     int *list_work = nullptr;
     int n_list_work = 0;
@@ -665,7 +676,7 @@ static Args<T> engine_args(const rfb_engine *e, int par) {
     fill_scene_args(a, e->scene);
     a.src_val = (const T *)e->src_val;
     a.src_hard = e->src_hard;
-    if (e->n_t3_cells) {
+    if (e->n_t3_cells || e->n_ade_cells) {
         a.l_work = e->list_work;
         a.n_work = e->n_list_work;
     }
@@ -782,10 +793,10 @@ static void launch_sweep(rfb_engine *e, const Args<T> &a, int par) {
     cudaStreamWaitEvent(e->stream, e->ev_join, 0);
 }
 
-// Threads of the interface-list launch: its work entries, or every entry.
-template <typename T>
-static int list_launch_n(const Args<T> &a) {
-    return a.l_work ? a.n_work : 3 * a.n_cells;
+// Threads of the interface-list launch: the entries left to it when some
+// cells go to the per-cell kernels (none when all do), else every entry.
+static int list_threads(const rfb_engine *e) {
+    return (e->n_t3_cells || e->n_ade_cells) ? e->n_list_work : 3 * e->scene.n_cells;
 }
 
 // Plane probes of the step: their means join the series before the point
@@ -794,8 +805,9 @@ template <typename T>
 static void launch_plane_gather(rfb_engine *e, int par) {
     if (!e->n_planes) return;
     const int out = e->nbuf == 2 ? 1 - par : 0;
-    k_plane_gather<T><<<e->n_planes, 1024, 0, e->stream>>>(e->d_planes, e->n_planes, (const T *const *)e->d_fout[out],
-                                                          (T *)e->ts, e->n_probes, (long long)e->n_steps, e->d_step);
+    k_plane_gather<T><<<dim3(e->plane_chunks, e->n_planes), kPlaneThreads, 0, e->stream>>>(
+        e->d_planes, e->n_planes, (const T *const *)e->d_fout[out], (T *)e->ts, e->n_probes, (long long)e->n_steps,
+        e->d_step, e->d_plane_part, e->d_plane_count, e->plane_chunks);
 }
 
 template <typename T>
@@ -811,8 +823,10 @@ static void enqueue_step(rfb_engine *e, int par) {
         k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
     }
     tf_before_list<T>(e, par);
-    if (a.n_cells && list_launch_n(a)) k_e_list<T><<<(list_launch_n(a) + 255) / 256, 256, 0, e->stream>>>(a);
+    if (a.n_cells && list_threads(e)) k_e_list<T><<<(list_threads(e) + 255) / 256, 256, 0, e->stream>>>(a);
     if (e->n_t3_cells) k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
+    if (e->n_ade_cells)
+        k_ade_cells<T><<<(e->n_ade_cells + 255) / 256, 256, 0, e->stream>>>(a, e->ade_cells, e->n_ade_cells);
     ProbeArgs<T> p;
     p.n = e->n_probes;
     p.cell = e->probe_cell;
@@ -841,8 +855,9 @@ static int count_step_launches(const rfb_engine *e) {
     int n = (e->sched == RFB_SCHED_FUSED)
                 ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0)
                 : 2;
-    if (e->scene.n_cells && (!e->n_t3_cells || e->n_list_work)) n++;
+    if (e->scene.n_cells && list_threads(e)) n++;
     if (e->n_t3_cells) n++;
+    if (e->n_ade_cells) n++;
     if (e->tf_on) n += 2 + (e->tf_n_h > 0);
     if (e->n_planes) n++;
     return n + 1;
@@ -1348,8 +1363,11 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     dfree(e->src_val); dfree(e->src_hard);
     dfree(e->probe_cell); dfree(e->probe_comp); dfree(e->ts); dfree(e->d_step); dfree(e->d_err); dfree(e->d_energy); dfree(e->d_iq);
     dfree(e->t3_cells);
+    dfree(e->ade_cells);
     dfree(e->list_work);
     dfree(e->d_planes);
+    dfree(e->d_plane_part);
+    dfree(e->d_plane_count);
     dfree(e->d_fout[0]);
     dfree(e->d_fout[1]);
     dfree(e->d_run_omega);
@@ -1374,28 +1392,44 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
 // per-cell kernel; their entries become kind 5, which the list kernel skips.
 static int group_t3_cells(rfb_engine *e, const rfb_scene_image_t *img) {
     const size_t ne = 3 * (size_t)img->n_cells;
-    std::vector<int> cells;
+    // an E sample outside every CPML slab (the list kernel's e_term is then
+    // the plain difference)
+    auto outside = [&](int ax, int q) {
+        return !e->cpml.on || (q >= e->cpml.em[ax].lo && q < e->cpml.em[ax].hi);
+    };
+    std::vector<int> cells, ade;
     for (size_t q = 0; q < (size_t)img->n_cells; q++) {
-        bool all = true;
-        for (int c = 0; c < 3; c++) all &= img->kind[3 * q + c] == RFB_LK_TENSOR3 && img->src[3 * q + c] < 0;
-        if (all) cells.push_back((int)q);
+        bool all3 = true, allade = true;
+        for (int c = 0; c < 3; c++) {
+            all3 &= img->kind[3 * q + c] == RFB_LK_TENSOR3 && img->src[3 * q + c] < 0;
+            allade &= img->kind[3 * q + c] == RFB_LK_ADE && img->src[3 * q + c] < 0 && img->aix[3 * q + c] >= 0;
+        }
+        if (all3) cells.push_back((int)q);
+        else if (allade && outside(0, img->cell_ijk[3 * q]) && outside(1, img->cell_ijk[3 * q + 1]) &&
+                 outside(2, img->cell_ijk[3 * q + 2]))
+            ade.push_back((int)q);
     }
-    if (cells.empty()) return 0;
+    if (cells.empty() && ade.empty()) return 0;
     e->t3_kinds.assign(img->kind, img->kind + ne);
     std::vector<uint8_t> kinds = e->t3_kinds;
     for (int q : cells)
         for (int c = 0; c < 3; c++) kinds[3 * (size_t)q + c] = RFB_LK_CELL3;
-    e->t3_cells = dev_copy(cells.data(), cells.size());
-    if (!e->t3_cells) {
+    for (int q : ade)
+        for (int c = 0; c < 3; c++) kinds[3 * (size_t)q + c] = RFB_LK_CELLADE;
+    if (!cells.empty() && !(e->t3_cells = dev_copy(cells.data(), cells.size()))) {
         rfb_set_error("3x3 cell list upload failed");
+        return -1;
+    }
+    if (!ade.empty() && !(e->ade_cells = dev_copy(ade.data(), ade.size()))) {
+        rfb_set_error("dispersive cell list upload failed");
         return -1;
     }
     {
         // the list kernel runs only over the entries left to it
         std::vector<int> work;
-        work.reserve(ne - 3 * cells.size());
+        work.reserve(ne - 3 * (cells.size() + ade.size()));
         for (size_t q = 0; q < ne; q++)
-            if (kinds[q] != RFB_LK_CELL3) work.push_back((int)q);
+            if (kinds[q] != RFB_LK_CELL3 && kinds[q] != RFB_LK_CELLADE) work.push_back((int)q);
         if (!work.empty()) {
             e->list_work = dev_copy(work.data(), work.size());
             if (!e->list_work) {
@@ -1408,6 +1442,8 @@ static int group_t3_cells(rfb_engine *e, const rfb_scene_image_t *img) {
     CK(cudaMemcpy(e->scene.l_kind, kinds.data(), ne, cudaMemcpyHostToDevice));
     e->n_t3_cells = (int)cells.size();
     e->t3_host = cells;
+    e->n_ade_cells = (int)ade.size();
+    e->ade_host = ade;
     return 0;
 fail:
     return -1;
@@ -1415,9 +1451,10 @@ fail:
 
 // Gives every 3x3 cell back to the list kernel (a TF/SF term landed on one).
 static int ungroup_t3_cells(rfb_engine *e) {
-    if (!e->n_t3_cells) return 0;
+    if (!e->n_t3_cells && !e->n_ade_cells) return 0;
     CK(cudaMemcpy(e->scene.l_kind, e->t3_kinds.data(), e->t3_kinds.size(), cudaMemcpyHostToDevice));
     e->n_t3_cells = 0;
+    e->n_ade_cells = 0;
     dfree(e->list_work);
     e->list_work = nullptr;
     e->n_list_work = 0;
@@ -1605,10 +1642,13 @@ extern "C" int rfb_engine_set_tfsf(rfb_engine_t *e, const rfb_tfsf_desc_t *d) {
         cell[q] = ((long long)d->h_ijkc[4 * q] * (g.ny + 1) + d->h_ijkc[4 * q + 1]) * e->pitch + d->h_ijkc[4 * q + 2];
         comp[q] = d->h_ijkc[4 * q + 3];
     }
-    // a 3x3 cell that carries a TF/SF E term stays with the list kernel
-    if (e->n_t3_cells && d->entry_first) {
+    // a 3x3 or dispersive cell that carries a TF/SF E term stays with the
+    // list kernel
+    if ((e->n_t3_cells || e->n_ade_cells) && d->entry_first) {
         bool hit = false;
         for (int q : e->t3_host)
+            for (int c = 0; c < 3; c++) hit |= d->entry_first[3 * (size_t)q + c] >= 0;
+        for (int q : e->ade_host)
             for (int c = 0; c < 3; c++) hit |= d->entry_first[3 * (size_t)q + c] >= 0;
         if (hit && ungroup_t3_cells(e) != 0) goto fail;
     }
@@ -1783,12 +1823,16 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         CK(cudaEventRecord(ev[1], e->stream));
         tf_before_list<T>(e, par);
         if (a.n_cells) {
-            if (list_launch_n(a)) {
-                k_e_list<T><<<(list_launch_n(a) + 255) / 256, 256, 0, e->stream>>>(a);
+            if (list_threads(e)) {
+                k_e_list<T><<<(list_threads(e) + 255) / 256, 256, 0, e->stream>>>(a);
                 g_launches++;
             }
             if (e->n_t3_cells) {
                 k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
+                g_launches++;
+            }
+            if (e->n_ade_cells) {
+                k_ade_cells<T><<<(e->n_ade_cells + 255) / 256, 256, 0, e->stream>>>(a, e->ade_cells, e->n_ade_cells);
                 g_launches++;
             }
         }
@@ -2028,11 +2072,26 @@ extern "C" int rfb_engine_set_planes(rfb_engine_t *e, size_t n, const int *axis_
         e->g1[q] = e->gk[q] = nullptr;
     }
     dfree(e->d_planes);
+    dfree(e->d_plane_part);
+    dfree(e->d_plane_count);
     e->d_planes = nullptr;
+    e->d_plane_part = nullptr;
+    e->d_plane_count = nullptr;
     e->n_planes = 0;
+    e->plane_chunks = 0;
     if (n) {
         e->d_planes = dev_copy(pd.data(), n);
         if (!e->d_planes) {
+            rfb_set_error("plane probe upload failed");
+            return -1;
+        }
+        for (size_t q = 0; q < n; q++) {
+            const long long npts = (long long)pd[q].nu * pd[q].nv;
+            e->plane_chunks = std::max(e->plane_chunks, (int)((npts + kPlaneChunk - 1) / kPlaneChunk));
+        }
+        if (dmalloc(&e->d_plane_part, n * e->plane_chunks * sizeof(double)) != cudaSuccess ||
+            dmalloc(&e->d_plane_count, n * sizeof(int)) != cudaSuccess ||
+            cudaMemset(e->d_plane_count, 0, n * sizeof(int)) != cudaSuccess) {
             rfb_set_error("plane probe upload failed");
             return -1;
         }

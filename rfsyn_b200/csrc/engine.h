@@ -48,7 +48,8 @@ enum {
     RFB_LK_TENSOR = 2,  /* rfsyn 2x2 tensor edge (materials.c:847-903)        */
     RFB_LK_ADE    = 3,  /* dispersive (Debye / Lorentz) cell                  */
     RFB_LK_TENSOR3 = 4, /* full 3x3 anisotropic sample (no rfsyn counterpart) */
-    RFB_LK_CELL3  = 5   /* 3x3 sample updated by the per-cell kernel, not here */
+    RFB_LK_CELL3  = 5,  /* 3x3 sample updated by the per-cell kernel, not here */
+    RFB_LK_CELLADE = 6  /* dispersive sample updated by the per-cell kernel    */
 };
 
 /* Scene image produced by the host materials description and consumed by the

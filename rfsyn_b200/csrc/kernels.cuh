@@ -250,6 +250,36 @@ __global__ void __launch_bounds__(256) k_e_split(Args<T> a) {
 // Dispersive E update (record layout of rfb_ade_record):
 //   E+ = ca E + cb (dA - dB) + ce E- - sum_p (cj J_p + cjm J_p-)
 //   J_p+ = aJ J_p + aJm J_p- + aE (E+ - E_ref), E_ref = E (Debye), E- (Lorentz)
+// The ADE update of one dispersive sample from its two curl terms: r is
+// the model's record (Ca-like, Cb-like and E-history coefficients, the pole
+// count, 6 per pole), v the sample's E before the step, st its 5 state
+// values (pole currents now and one step back, E one step back), updated in
+// place.  At most two poles (RFB_ADE_NC = 4 + 6 x 2).
+template <typename T>
+__device__ __forceinline__ T ade_core(const T *r, T v, T tA, T tB, T *st) {
+    const T em = st[4];
+    T en = xa(xm(r[0], v), xm(r[1], xs(tA, tB)));
+    en = xa(en, xm(r[2], em));
+    const int np = (int)r[3];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        if (p >= np) break;
+        const T *w = r + 4 + 6 * p;
+        en = xs(en, xa(xm(w[1], st[p]), xm(w[2], st[2 + p])));
+    }
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        if (p >= np) break;
+        const T *w = r + 4 + 6 * p;
+        const T eref = (w[0] != T(0)) ? em : v;
+        const T jn = xa(xa(xm(w[3], st[p]), xm(w[4], st[2 + p])), xm(w[5], xs(en, eref)));
+        st[2 + p] = st[p];
+        st[p] = jn;
+    }
+    st[4] = v;
+    return en;
+}
+
 template <typename T>
 __device__ __forceinline__ T e_ade(const Args<T> &a, int e, int comp, int i, int j, int k, T v) {
     const T *r = a.ade_c + 16 * a.l_aix[e];
@@ -271,23 +301,7 @@ __device__ __forceinline__ T e_ade(const Args<T> &a, int e, int comp, int i, int
         tA = e_term(a, 4, 0, i, xs(a.Ho[1][c], a.Ho[1][cidx(a, im, j, k)]), i, j, k);
         tB = e_term(a, 5, 1, j, xs(a.Ho[0][c], a.Ho[0][cidx(a, i, jm, k)]), i, j, k);
     }
-    const T em = st[4];
-    T en = xa(xm(r[0], v), xm(r[1], xs(tA, tB)));
-    en = xa(en, xm(r[2], em));
-    const int np = (int)r[3];
-    for (int p = 0; p < np; p++) {
-        const T *w = r + 4 + 6 * p;
-        en = xs(en, xa(xm(w[1], st[p]), xm(w[2], st[2 + p])));
-    }
-    for (int p = 0; p < np; p++) {
-        const T *w = r + 4 + 6 * p;
-        const T eref = (w[0] != T(0)) ? em : v;
-        const T jn = xa(xa(xm(w[3], st[p]), xm(w[4], st[2 + p])), xm(w[5], xs(en, eref)));
-        st[2 + p] = st[p];
-        st[p] = jn;
-    }
-    st[4] = v;
-    return en;
+    return ade_core(r, v, tA, tB, st);
 }
 
 // Full 3x3 sample of component c at (i, j, k), record r = (m_c0, m_c1, m_c2,
@@ -384,6 +398,43 @@ __global__ void __launch_bounds__(256) k_t3_cells(Args<T> a, const int *cells, i
     if (t < n) t3_cell(a, cells[t]);
 }
 
+// Cells whose three samples are dispersive (ADE) samples outside every CPML
+// slab, with no source and no TF/SF term: one thread per cell takes its
+// three components -- the nine H values they read loaded once, the 15 state
+// values of the cell's samples (contiguous) loaded together -- with the
+// operations of e_ade per sample (ade_core), so the results are
+// bit-identical to the per-entry form.
+template <typename T>
+__global__ void __launch_bounds__(256) k_ade_cells(Args<T> a, const int *cells, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int cell = cells[t];
+    const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
+    const long long c = cidx(a, i, j, k);
+    const int im = i == 0 ? a.nx - 1 : i - 1;
+    const int jm = j == 0 ? a.ny - 1 : j - 1;
+    const int km = k == 0 ? a.nz - 1 : k - 1;
+    const long long ci = cidx(a, im, j, k), cj = cidx(a, i, jm, k), ck = cidx(a, i, j, km);
+    const T hx = a.Ho[0][c], hy = a.Ho[1][c], hz = a.Ho[2][c];
+    const T hx_j = a.Ho[0][cj], hx_k = a.Ho[0][ck], hy_k = a.Ho[1][ck], hy_i = a.Ho[1][ci], hz_j = a.Ho[2][cj],
+            hz_i = a.Ho[2][ci];
+    const T e0 = a.E[0][c], e1 = a.E[1][c], e2 = a.E[2][c];
+    const T *r0 = a.ade_c + 16 * a.l_aix[3 * cell], *r1 = a.ade_c + 16 * a.l_aix[3 * cell + 1],
+            *r2 = a.ade_c + 16 * a.l_aix[3 * cell + 2];
+    T *st = a.ade_s + 15 * (long long)cell;
+    T s[15];
+#pragma unroll
+    for (int q = 0; q < 15; q++) s[q] = st[q];
+    const T n0 = ade_core(r0, e0, xs(hz, hz_j), xs(hy, hy_k), s);
+    const T n1 = ade_core(r1, e1, xs(hx, hx_k), xs(hz, hz_i), s + 5);
+    const T n2 = ade_core(r2, e2, xs(hy, hy_i), xs(hx, hx_j), s + 10);
+#pragma unroll
+    for (int q = 0; q < 15; q++) st[q] = s[q];
+    a.Eo[0][c] = n0;
+    a.Eo[1][c] = n1;
+    a.Eo[2][c] = n2;
+}
+
 // ---- interface list: overrides, tensor edges, sources --------------------
 // One thread per (cell, component) entry.  Reads E from the input buffers,
 // H from the output buffers (already advanced), writes E output.
@@ -393,7 +444,7 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
     const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
     const long long c = cidx(a, i, j, k);
     const int kind = a.l_kind[e];
-    if (kind == 5) return;  // a 3x3 cell: k_t3_cells updates its three components
+    if (kind == 5 || kind == 6) return;  // a 3x3 / ADE cell: k_t3_cells / k_ade_cells updates it
     T v = a.E[comp][c];
     const int s = a.l_src[e];
     if (s >= 0) {
@@ -530,28 +581,39 @@ __global__ void k_probe_gather(ProbeArgs<T> p) {
 // Sample n of a plane probe is the mean of one field component over a whole
 // grid plane (axis a at index q: every (u, v) of the other two axes, u < n_u,
 // v < n_v): for a periodic cell at normal incidence, the amplitude of the
-// specular (zeroth-order) reflected or transmitted wave.  One block per
-// plane; each thread sums its points in FP64 in a fixed order, then warp
-// shuffles and one pass over the warps' sums reduce them in a fixed tree, so
-// the mean is deterministic.  Runs before k_probe_gather (same step index).
+// specular (zeroth-order) reflected or transmitted wave.  The plane's points
+// t = u n_v + v are cut into chunks of kPlaneChunk, one block each (grid:
+// chunks x planes), so the gather spreads over the SMs.  Each thread sums
+// its points of the chunk (t0 + x, t0 + x + kPlaneThreads, ...) in FP64,
+// warp shuffles and one pass over the warps' sums reduce the block in a
+// fixed tree, and the last block of the plane to finish (a per-plane
+// counter, reset by that block) adds the chunks' sums in chunk order: the
+// mean is deterministic.  Runs before k_probe_gather (same step index).
 struct PlaneDesc {
     long long base, su, sv;  // element offset of (u, v) = (0, 0) and the strides
     int nu, nv, comp;
 };
 
+constexpr int kPlaneChunk = 1024, kPlaneThreads = 256;
+
 template <typename T>
-__global__ void __launch_bounds__(1024) k_plane_gather(const PlaneDesc *planes, int n_planes, const T *const *F,
-                                                       T *ts, int series0, long long n_steps, const int *d_step) {
-    __shared__ double warp_sum[32];
-    const int q = blockIdx.x;
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_gather(const PlaneDesc *planes, int n_planes,
+                                                                const T *const *F, T *ts, int series0,
+                                                                long long n_steps, const int *d_step, double *part,
+                                                                int *count, int max_chunks) {
+    __shared__ double warp_sum[kPlaneThreads / 32];
+    const int q = blockIdx.y, b = blockIdx.x;
     if (q >= n_planes) return;
     const int n = *d_step;
     if (n >= n_steps) return;
     const PlaneDesc pd = planes[q];
-    const T *f = F[pd.comp];
     const long long npts = (long long)pd.nu * pd.nv;
+    const int nchunk = (int)((npts + kPlaneChunk - 1) / kPlaneChunk);
+    if (b >= nchunk) return;
+    const T *f = F[pd.comp];
+    const long long t0 = (long long)b * kPlaneChunk, t1 = t0 + kPlaneChunk < npts ? t0 + kPlaneChunk : npts;
     double acc = 0.0;
-    for (long long t = threadIdx.x; t < npts; t += blockDim.x) {
+    for (long long t = t0 + threadIdx.x; t < t1; t += kPlaneThreads) {
         const long long u = t / pd.nv, v = t - u * pd.nv;
         acc = __dadd_rn(acc, (double)f[pd.base + u * pd.su + v * pd.sv]);
     }
@@ -560,8 +622,19 @@ __global__ void __launch_bounds__(1024) k_plane_gather(const PlaneDesc *planes, 
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = __dadd_rn(s, warp_sum[w]);
-        ts[(long long)(series0 + q) * n_steps + n] = (T)__ddiv_rn(s, (double)npts);
+        for (int w = 0; w < kPlaneThreads / 32; w++) s = __dadd_rn(s, warp_sum[w]);
+        part[(long long)q * max_chunks + b] = s;
+        __threadfence();
+        if (atomicAdd(&count[q], 1) == nchunk - 1) {
+            // every chunk's sum is visible: the other blocks fenced before
+            // their increments
+            __threadfence();
+            const volatile double *pp = part + (long long)q * max_chunks;
+            double m = 0.0;
+            for (int c = 0; c < nchunk; c++) m = __dadd_rn(m, pp[c]);
+            ts[(long long)(series0 + q) * n_steps + n] = (T)__ddiv_rn(m, (double)npts);
+            count[q] = 0;
+        }
     }
 }
 
