@@ -631,12 +631,12 @@ struct rfb_engine {
     double *d_energy = nullptr;  // energy audit: block partials + result
     float *d_iq = nullptr;       // stage output: n_steps I/Q pairs, then the noise scale (a double)
     // cells whose three E samples are 3x3 samples without source or TF/SF
-    // term, updated per cell by k_t3_cells (their list entries are kind 5);
+    // term, updated per cell by k_list_cells (their list entries are kind 5);
     // t3_kinds keeps the image's kinds to undo it
     int *t3_cells = nullptr;
     int n_t3_cells = 0;
     // cells whose three E samples are dispersive samples outside the CPML
-    // without source or TF/SF term, updated per cell by k_ade_cells (their
+    // without source or TF/SF term, updated per cell by k_list_cells (their
     // list entries are kind 6)
     int *ade_cells = nullptr;
     int n_ade_cells = 0;
@@ -799,6 +799,24 @@ static int list_threads(const rfb_engine *e) {
     return (e->n_t3_cells || e->n_ade_cells) ? e->n_list_work : 3 * e->scene.n_cells;
 }
 
+// Launches of the step's interface list: one (k_list_cells when some cells
+// have per-cell updates, else k_e_list), or none without list work.
+static int list_launches(const rfb_engine *e) {
+    return (e->scene.n_cells && list_threads(e)) || e->n_t3_cells || e->n_ade_cells ? 1 : 0;
+}
+
+template <typename T>
+static void launch_list(rfb_engine *e, const Args<T> &a) {
+    if (e->n_t3_cells || e->n_ade_cells) {
+        const int nb3 = (e->n_t3_cells + 255) / 256, nba = (e->n_ade_cells + 255) / 256;
+        const int nbl = (list_threads(e) + 255) / 256;
+        k_list_cells<T><<<nb3 + nba + nbl, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells, nb3, e->ade_cells,
+                                                                e->n_ade_cells, nba);
+    } else if (a.n_cells && list_threads(e)) {
+        k_e_list<T><<<(list_threads(e) + 255) / 256, 256, 0, e->stream>>>(a);
+    }
+}
+
 // Plane probes of the step: their means join the series before the point
 // probes advance the step counter.
 template <typename T>
@@ -823,10 +841,7 @@ static void enqueue_step(rfb_engine *e, int par) {
         k_e_split<T><<<grd, blk, 0, e->stream>>>(a);
     }
     tf_before_list<T>(e, par);
-    if (a.n_cells && list_threads(e)) k_e_list<T><<<(list_threads(e) + 255) / 256, 256, 0, e->stream>>>(a);
-    if (e->n_t3_cells) k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
-    if (e->n_ade_cells)
-        k_ade_cells<T><<<(e->n_ade_cells + 255) / 256, 256, 0, e->stream>>>(a, e->ade_cells, e->n_ade_cells);
+    launch_list<T>(e, a);
     ProbeArgs<T> p;
     p.n = e->n_probes;
     p.cell = e->probe_cell;
@@ -855,9 +870,7 @@ static int count_step_launches(const rfb_engine *e) {
     int n = (e->sched == RFB_SCHED_FUSED)
                 ? (e->plan.n_int > 0) + (e->plan.n_edge > 0) + (e->plan.n_qe > 0) + (e->plan.n_qx > 0)
                 : 2;
-    if (e->scene.n_cells && list_threads(e)) n++;
-    if (e->n_t3_cells) n++;
-    if (e->n_ade_cells) n++;
+    n += list_launches(e);
     if (e->tf_on) n += 2 + (e->tf_n_h > 0);
     if (e->n_planes) n++;
     return n + 1;
@@ -1822,20 +1835,8 @@ static int time_kernels_t(rfb_engine *e, size_t n, double *sweep_ms, double *oth
         }
         CK(cudaEventRecord(ev[1], e->stream));
         tf_before_list<T>(e, par);
-        if (a.n_cells) {
-            if (list_threads(e)) {
-                k_e_list<T><<<(list_threads(e) + 255) / 256, 256, 0, e->stream>>>(a);
-                g_launches++;
-            }
-            if (e->n_t3_cells) {
-                k_t3_cells<T><<<(e->n_t3_cells + 255) / 256, 256, 0, e->stream>>>(a, e->t3_cells, e->n_t3_cells);
-                g_launches++;
-            }
-            if (e->n_ade_cells) {
-                k_ade_cells<T><<<(e->n_ade_cells + 255) / 256, 256, 0, e->stream>>>(a, e->ade_cells, e->n_ade_cells);
-                g_launches++;
-            }
-        }
+        launch_list<T>(e, a);
+        g_launches += list_launches(e);
         ProbeArgs<T> p;
         p.n = e->n_probes;
         p.cell = e->probe_cell;

@@ -72,8 +72,8 @@ struct Args {
     long long skip[MAX_SKIP];
     // interface list
     int n_cells;
-    // NULL, or the n_work entries k_e_list updates (the others belong to
-    // cells k_t3_cells updates whole)
+    // NULL, or the n_work entries the per-entry update takes (the others
+    // belong to cells k_list_cells updates whole)
     const int *l_work;
     int n_work;
     const int *lc_ijk;
@@ -392,12 +392,6 @@ __device__ __forceinline__ void t3_cell(const Args<T> &a, int cell) {
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_t3_cells(Args<T> a, const int *cells, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) t3_cell(a, cells[t]);
-}
-
 // Cells whose three samples are dispersive (ADE) samples outside every CPML
 // slab, with no source and no TF/SF term: one thread per cell takes its
 // three components -- the nine H values they read loaded once, the 15 state
@@ -405,10 +399,7 @@ __global__ void __launch_bounds__(256) k_t3_cells(Args<T> a, const int *cells, i
 // operations of e_ade per sample (ade_core), so the results are
 // bit-identical to the per-entry form.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ade_cells(Args<T> a, const int *cells, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int cell = cells[t];
+__device__ __forceinline__ void ade_cell(const Args<T> &a, int cell) {
     const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
     const long long c = cidx(a, i, j, k);
     const int im = i == 0 ? a.nx - 1 : i - 1;
@@ -444,7 +435,7 @@ __device__ __forceinline__ void e_list_entry(const Args<T> &a, int e) {
     const int i = a.lc_ijk[3 * cell], j = a.lc_ijk[3 * cell + 1], k = a.lc_ijk[3 * cell + 2];
     const long long c = cidx(a, i, j, k);
     const int kind = a.l_kind[e];
-    if (kind == 5 || kind == 6) return;  // a 3x3 / ADE cell: k_t3_cells / k_ade_cells updates it
+    if (kind == 5 || kind == 6) return;  // a 3x3 / ADE cell: k_list_cells updates it per cell
     T v = a.E[comp][c];
     const int s = a.l_src[e];
     if (s >= 0) {
@@ -549,6 +540,29 @@ __global__ void __launch_bounds__(256) k_e_list(Args<T> a) {
     }
     if (t >= 3 * a.n_cells) return;
     e_list_entry(a, t);
+}
+
+// The whole interface list of a step in one launch when some cells have
+// per-cell updates: blocks [0, nb_t3) take the whole 3x3 cells (t3_cell),
+// the next nb_ade blocks the dispersive cells (ade_cell), the rest the list
+// entries left to the per-entry update (a.l_work).  The three parts touch
+// disjoint samples and read only the step's advanced H and the previous E,
+// so running them side by side changes no result, and their dependent
+// gathers overlap instead of ending one launch before the next begins.
+template <typename T>
+__global__ void __launch_bounds__(256) k_list_cells(Args<T> a, const int *t3, int n_t3, int nb_t3, const int *ade,
+                                                    int n_ade, int nb_ade) {
+    const int b = blockIdx.x;
+    if (b < nb_t3) {
+        const int t = b * blockDim.x + threadIdx.x;
+        if (t < n_t3) t3_cell(a, t3[t]);
+    } else if (b < nb_t3 + nb_ade) {
+        const int t = (b - nb_t3) * blockDim.x + threadIdx.x;
+        if (t < n_ade) ade_cell(a, ade[t]);
+    } else {
+        const int t = (b - nb_t3 - nb_ade) * blockDim.x + threadIdx.x;
+        if (t < a.n_work) e_list_entry(a, a.l_work[t]);
+    }
 }
 
 // ---- probes ---------------------------------------------------------------
