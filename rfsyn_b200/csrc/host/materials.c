@@ -71,7 +71,7 @@ static void omap_free(omap_t *m) {
 }
 
 static long omap_find(const omap_t *m, uint64_t key) {
-    if (!m->cap) return -1;
+    if (!m->count) return -1; /* an empty map: no probe (deletes and lookups in maps a scene never filled) */
     size_t mask = m->cap - 1, h = omap_home(key, mask);
     for (;;) {
         if (m->keys[h] == OMAP_EMPTY) return -1;
@@ -835,6 +835,27 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                                     size_t n_spheres, int smoothing) {
     if (!materials_matches(mat, g) || (!spheres && n_spheres)) return -1;
     const size_t n[3] = {g->nx, g->ny, g->nz};
+    {
+        /* room in the maps for every sphere's samples at once (a surface
+         * shell about 1.3 cells thick, three samples a cell; a dispersive
+         * sphere's whole volume), so the maps are not rehashed sphere after
+         * sphere as they grow */
+        double shell = 0.0, vol = 0.0;
+        for (size_t q = 0; q < n_spheres; q++) {
+            const double r = spheres[q].radius;
+            if (!isfinite(r) || r <= 0.0) continue;
+            if (spheres[q].model)
+                vol += 3.0 * (4.0 / 3.0) * M_PI * (r + 1.0) * (r + 1.0) * (r + 1.0);
+            else
+                shell += 3.0 * 4.0 * M_PI * (r + 1.0) * (r + 1.0) * 1.3;
+        }
+        const double cap = 3.0 * (double)mat->total;
+        omap_t *dst = smoothing == 2 ? &mat->tensor3 : &mat->scalar;
+        if (omap_reserve(dst, (size_t)fmin(shell, cap)) != 0 || omap_reserve(&mat->disp, (size_t)fmin(vol, cap)) != 0) {
+            rfb_set_error("out of host memory rasterising spheres");
+            return -1;
+        }
+    }
     for (size_t q = 0; q < n_spheres; q++) {
         const fdtd_b200_sphere_t *sp = &spheres[q];
         if (!isfinite(sp->cx) || !isfinite(sp->cy) || !isfinite(sp->cz) || !isfinite(sp->radius) || sp->radius <= 0.0)
@@ -883,12 +904,24 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
             free(n2);
             return -1;
         }
+        {
+            /* room for this sphere's surface samples in the map they go to,
+             * reserved once instead of grown through every power of two */
+            size_t cut = 0;
+            if (sp->model)
+                for (size_t q3 = 0; q3 < 3 * ncell; q3++) cut += f[q3] >= 0.5;
+            else
+                for (size_t q3 = 0; q3 < 3 * ncell; q3++) cut += f[q3] > 0.0 && f[q3] < 1.0;
+            omap_t *dst = sp->model ? &mat->disp : (full ? &mat->tensor3 : &mat->scalar);
+            if (omap_reserve(dst, cut) != 0) goto oom;
+        }
         for (int di = 0; di < ni; di++)
             for (int dj = 0; dj < nj; dj++)
                 for (int dk = 0; dk < nk; dk++) {
                     const size_t i = (size_t)(lo[0] + di), j = (size_t)(lo[1] + dj), k = (size_t)(lo[2] + dk);
                     const size_t cell = ((size_t)di * nj + (size_t)dj) * nk + (size_t)dk;
                     const double *fc = f + 3 * cell, *nc = n2 + (full ? 9 : 3) * cell;
+                    if (fc[0] <= 0.0 && fc[1] <= 0.0 && fc[2] <= 0.0) continue; /* outside the sphere */
                     int valid[3];
                     for (int c = 0; c < 3; c++) valid[c] = sample_valid(g, c, i, j, k);
                     const size_t w = fdtd_index(g, i, j, k);
