@@ -325,6 +325,13 @@ int fdtd_b200_mlp_train(fdtd_b200_mlp_t *mlp, size_t steps, int batch, double lr
 /* Outputs of n inputs (n x n_out). */
 int fdtd_b200_mlp_predict(fdtd_b200_mlp_t *mlp, const float *X, size_t n, float *Y);
 unsigned long long fdtd_b200_mlp_launch_count(const fdtd_b200_mlp_t *mlp);
+/* How many of those launches were products on the tcgen05 tensor cores
+ * (accumulators in tensor memory).  The products run on mma.sync tiles of
+ * 64 x 64, faster on this network's small products; with the environment
+ * variable RFSYN_FDTD_MLP_GEMM=tcgen05 set when the network is created,
+ * every product whose rows are a multiple of 128, columns of 32 and depth
+ * of 64 runs on tcgen05 tiles of 128 x 32 instead. */
+unsigned long long fdtd_b200_mlp_tensor_core_launches(const fdtd_b200_mlp_t *mlp);
 
 /* ---- dispersive media (auxiliary differential equations) ----------------------
  * rfsyn models only static eps_r and sigma (engine/fdtd/materials.c:92-125);

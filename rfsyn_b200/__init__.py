@@ -325,6 +325,7 @@ def load() -> C.CDLL:
         "fdtd_b200_mlp_train": (I, [P, S, I, D, D, D, D, C.c_uint64, C.POINTER(D)]),
         "fdtd_b200_mlp_predict": (I, [P, C.POINTER(C.c_float), S, C.POINTER(C.c_float)]),
         "fdtd_b200_mlp_launch_count": (C.c_ulonglong, [P]),
+        "fdtd_b200_mlp_tensor_core_launches": (C.c_ulonglong, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -664,6 +665,10 @@ class Mlp:
     def _ok(self, rc):
         if rc != 0:
             raise RuntimeError(last_error())
+
+    def tensor_core_launches(self) -> int:
+        """Products run so far on the tcgen05 tensor cores."""
+        return int(self.lib.fdtd_b200_mlp_tensor_core_launches(self.h))
 
     @property
     def n_params(self) -> int:

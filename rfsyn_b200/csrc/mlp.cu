@@ -10,6 +10,8 @@
 //               GELU (hidden layers, pre-activation kept in FP32), bias (output
 //               layer), GELU' (backward through a hidden layer, dZ in FP32,
 //               BF16 and transposed BF16), plain FP32 (weight gradients);
+//   k_gemm_tc   the same products and epilogues on tcgen05 (accumulators in
+//               tensor memory), selectable; slower on this network's products;
 //   k_mse       loss gradient 2 (out - y) / (M N), FP32 / BF16 / transposed,
 //               per-block loss partials (deterministic);
 //   k_colsum    bias gradients as deterministic column sums of dZ;
@@ -169,6 +171,211 @@ __global__ void __launch_bounds__(128) k_gemm_nt(const bf16 *__restrict__ A, int
             }
 }
 
+// ---- the same contraction on the 5th-generation tensor cores ----------------
+// k_gemm_tc: C = A . B^T with one tcgen05.mma (M 128, N 32, K 16, BF16 in,
+// FP32 accumulation in tensor memory) stream per CTA tile of 128 x 32.
+// K is staged 64 at a time (one 128-byte row per tile row) by cp.async into
+// a four-stage ring in the 128-byte-swizzled K-major layout the MMA's shared
+// memory descriptors describe (16-byte chunk c of row r at chunk c ^ (r % 8)
+// of the row, 8-row groups 1024 bytes apart).  One thread issues the four
+// MMAs of a stage and commits them to the stage's mbarrier, which frees the
+// stage for a later load; the last commit releases the accumulator, which
+// eight warps read back (tcgen05.ld, warp w lanes 32 (w % 4) .. +31 = tile
+// rows, columns 16 (w / 4) .. +15) into the same fused epilogues as
+// k_gemm_nt.  Every wait is bounded: on a timeout the CTA records it,
+// waits (bounded) for its MMAs in flight, frees its tensor memory and
+// returns.  Measured on the surrogate's network (54-512x4-512, one B200):
+// a training step takes 0.226-0.233 ms at batch 256 against 0.189-0.191
+// ms on k_gemm_nt, and 0.51 against 0.42 ms at batch 2048 -- products of
+// at most 512 x 2048 x 512 are latency-bound on staging their tiles, which
+// this cp.async-fed form does no faster than the mma.sync tiles -- so it
+// runs only when asked for (RFSYN_FDTD_MLP_GEMM=tcgen05).
+namespace tc {
+// Tiles of 128 rows x BN columns (BN 32: more CTAs on these small products
+// -- 128 x 128 tiles, fewer CTAs and fewer re-reads of A, measured slower
+// even on 2048-row batches), K staged 64 at a time in a 4-stage ring filled
+// three steps ahead (a refill waits for the MMAs of the step before, which
+// take far less than a load)
+constexpr int BM = 128, BK = 64, STAGES = 4, DIST = 3, THREADS = 256;
+template <int BN>
+struct Shape {
+    static constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+    static_assert(STAGE_BYTES % 1024 == 0 && A_BYTES % 1024 == 0, "swizzle atoms stay 1024-byte aligned");
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 64;  // tiles 1024-aligned, then barriers, TMEM address
+    static constexpr uint32_t TMEM_COLS = BN;                     // FP32 accumulator: a column per output column
+    // instruction descriptor: F32 accumulator, BF16 A and B, both K-major,
+    // N >> 3 at bit 17, M >> 4 at bit 24
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+};
+constexpr long long WAIT = 2000000000LL;  // SM cycles, about a second
+}  // namespace tc
+
+__device__ __forceinline__ unsigned sm_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Shared-memory descriptor of a K-major, 128-byte-swizzled operand tile at
+// shared address `a`: start address >> 4, leading offset 16 bytes (unused
+// with swizzling), stride offset 1024 bytes (one 8-row group), descriptor
+// version 1, layout 2 (128-byte swizzle).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t a) {
+    return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) |
+           ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void tc_mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(sm_addr(bar)));
+}
+
+__device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, unsigned parity) {
+    const long long t0 = clock64();
+    for (;;) {
+        unsigned ok;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(sm_addr(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > tc::WAIT) return false;
+    }
+}
+
+template <int EPI>
+__device__ __forceinline__ void epi_store(const Epi &epi, int M, int N, int r, int c, float v) {
+    const size_t o = (size_t)r * N + c;
+    if (EPI == EPI_HIDDEN || EPI == EPI_OUT) {
+        v += epi.bias[c];
+        epi.f32[o] = v;
+        if (EPI == EPI_HIDDEN) epi.b16[o] = __float2bfloat16_rn(gelu(v));
+    } else if (EPI == EPI_BWD_GELU) {
+        v *= gelu_grad(epi.pre[o]);
+        epi.f32[o] = v;
+        const bf16 b = __float2bfloat16_rn(v);
+        epi.b16[o] = b;
+        epi.b16t[(size_t)c * M + r] = b;
+    } else {
+        epi.f32[o] = v;
+    }
+}
+
+// C = A . B^T.  A: [M][lda], B: [N][ldb], BF16 row-major (K-major); M a
+// multiple of 128, N of 32, K of 64, lda / ldb multiples of 8.
+template <int EPI, int BN>
+__global__ void __launch_bounds__(tc::THREADS) k_gemm_tc(const bf16 *__restrict__ A, int lda, const bf16 *__restrict__ B,
+                                                 int ldb, int M, int N, int K, Epi epi, int *err) {
+    using S = tc::Shape<BN>;
+    extern __shared__ unsigned char tc_smem[];
+    const unsigned pad = (1024u - (sm_addr(tc_smem) & 1023u)) & 1023u;
+    unsigned char *tiles = tc_smem + pad;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(tiles + tc::STAGES * S::STAGE_BYTES);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + tc::STAGES);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * tc::BM, n0 = blockIdx.x * BN;
+    if (tid == 0) {
+        for (int s = 0; s < tc::STAGES; s++) tc_mbar_init(&bar[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sm_addr(tmem_slot)),
+                     "r"(S::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    auto load = [&](int s, int k0) {
+        unsigned char *as = tiles + s * S::STAGE_BYTES, *bs = as + S::A_BYTES;
+        for (int q = tid; q < tc::BM * 8; q += tc::THREADS) {
+            const int r = q >> 3, c = q & 7;
+            cp16(as + r * 128 + ((c ^ (r & 7)) << 4), A + (size_t)(m0 + r) * lda + k0 + c * 8);
+        }
+        for (int q = tid; q < BN * 8; q += tc::THREADS) {
+            const int r = q >> 3, c = q & 7;
+            cp16(bs + r * 128 + ((c ^ (r & 7)) << 4), B + (size_t)(n0 + r) * ldb + k0 + c * 8);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    const int nk = K / tc::BK;
+    bool failed = false;
+    int committed = -1;  // the last K step whose MMAs were committed
+    for (int p = 0; p < tc::DIST && p < nk; p++) load(p % tc::STAGES, p * tc::BK);
+    for (int kt = 0; kt < nk; kt++) {
+        const int s = kt % tc::STAGES, nxt = kt + tc::DIST;
+        if (nxt < nk) {
+            // stage nxt % STAGES was last read by the MMAs of step nxt - STAGES
+            const int ns = nxt % tc::STAGES, prev = nxt - tc::STAGES;
+            if (prev >= 0 && !tc_mbar_wait(&bar[ns], (prev / tc::STAGES) & 1)) failed = true;
+            if (__syncthreads_or(failed)) break;
+            load(ns, nxt * tc::BK);
+        }
+        // step kt's copies are complete once at most the copies of the steps
+        // loaded after it are pending
+        const int after = nk - 1 - kt < tc::DIST ? nk - 1 - kt : tc::DIST;
+        static_assert(tc::DIST <= 3, "the waits below cover up to three later groups");
+        if (after >= 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+        else if (after == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+        else if (after == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        // make them visible to the tensor core's (async-proxy) reads, then to
+        // the issuing thread
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t as = sm_addr(tiles + s * S::STAGE_BYTES), bs = as + S::A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < tc::BK / 16; kk++) {
+                const uint64_t da = sw128_desc(as + 32 * kk), db = sw128_desc(bs + 32 * kk);
+                const uint32_t acc = (kt | kk) ? 1u : 0u;
+                asm volatile(
+                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(S::IDESC), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             sm_addr(&bar[s]))
+                         : "memory");
+        }
+        committed = kt;
+    }
+    // the last commit covers every MMA this CTA issued; copies still in
+    // flight (after an early exit) land before the shared memory is released
+    if (committed >= 0 && !tc_mbar_wait(&bar[committed % tc::STAGES], (committed / tc::STAGES) & 1)) failed = true;
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (__syncthreads_or(failed)) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        // warp w reads TMEM lanes 32 (w % 4) .. (the tile rows it may
+        // access) and the BN / 2 columns of half w / 4, 16 at a time
+        static_assert(tc::THREADS == 256 && BN % 32 == 0, "eight warps: four lane groups x two column halves");
+        const int r = m0 + 32 * (warp & 3) + lane;  // TMEM lane = tile row
+#pragma unroll
+        for (int cc = (BN / 2) * (warp >> 2); cc < (BN / 2) * ((warp >> 2) + 1); cc += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)cc));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 16; q++) epi_store<EPI>(epi, M, N, r, n0 + cc + q, __uint_as_float(v[q]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(S::TMEM_COLS)
+                     : "memory");
+}
+
 // Loss gradient of the mean squared error over M x N outputs; per-block
 // partial sums of the squared error (fixed order: deterministic).
 __global__ void k_mse(const float *out, const float *y, int M, int N, float *d32, bf16 *d16, bf16 *d16t,
@@ -196,12 +403,22 @@ __global__ void k_mse(const float *out, const float *y, int M, int N, float *d32
 }
 
 // Column sums of d [M][N] (bias gradients), one thread per column.
-__global__ void k_colsum(const float *d, int M, int N, float *out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= N) return;
+// Block of 32 columns x 8 warps: warp w sums rows w, w + 8, ... of its
+// lane's column, then the eight partial sums are added in warp order (a
+// fixed order: deterministic).
+__global__ void __launch_bounds__(256) k_colsum(const float *d, int M, int N, float *out) {
+    __shared__ float part[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, c = blockIdx.x * 32 + lane;
     float s = 0.f;
-    for (int r = 0; r < M; r++) s += d[(size_t)r * N + c];
-    out[c] = s;
+    if (c < N)
+        for (int r = w; r < M; r += 8) s += d[(size_t)r * N + c];
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && c < N) {
+        float t = part[0][lane];
+        for (int q = 1; q < 8; q++) t += part[q][lane];
+        out[c] = t;
+    }
 }
 
 struct AdamArgs {
@@ -303,6 +520,11 @@ struct fdtd_b200_mlp {
     int graph_b = 0;
     AdamArgs adam_cfg{};
     unsigned long long launches = 0;
+    // tensor-core products: enabled (the shared memory attribute was set),
+    // their launches, and the device flag a timed-out wait sets
+    int tc = 0;
+    unsigned long long tc_launches = 0;
+    int *d_err = nullptr;
 };
 
 typedef struct fdtd_b200_mlp fdtd_b200_mlp_t;
@@ -360,11 +582,51 @@ static int mlp_batch_buffers(fdtd_b200_mlp *m, int B) {
     return 0;
 }
 
+// The network's products: k_gemm_nt (64 x 64 tiles, mma.sync), or with
+// RFSYN_FDTD_MLP_GEMM=tcgen05 k_gemm_tc where the shapes fit its tiles (M a
+// multiple of 128, N of 32, K of 64 -- every training-step product of the
+// surrogate does).
 template <int EPI>
 static void gemm(fdtd_b200_mlp *m, const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, Epi epi) {
-    dim3 grid(N / GT, M / GT);
-    k_gemm_nt<EPI><<<grid, 128, 0, m->st>>>(A, lda, B, ldb, M, N, K, epi);
+    if (m->tc && M % tc::BM == 0 && N % 32 == 0 && K % tc::BK == 0 && lda % 8 == 0 && ldb % 8 == 0) {
+        dim3 grid(N / 32, M / tc::BM);
+        k_gemm_tc<EPI, 32><<<grid, tc::THREADS, tc::Shape<32>::SMEM, m->st>>>(A, lda, B, ldb, M, N, K, epi,
+                                                                            m->d_err);
+        m->tc_launches++;
+    } else {
+        dim3 grid(N / GT, M / GT);
+        k_gemm_nt<EPI><<<grid, 128, 0, m->st>>>(A, lda, B, ldb, M, N, K, epi);
+    }
     m->launches++;
+}
+
+// The tensor-core products need more than 48 KB of shared memory.
+template <int BN>
+static bool tc_attrs() {
+    const int sm = tc::Shape<BN>::SMEM;
+    return cudaFuncSetAttribute(k_gemm_tc<EPI_HIDDEN, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_gemm_tc<EPI_OUT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_gemm_tc<EPI_BWD_GELU, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_gemm_tc<EPI_F32, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+               cudaSuccess;
+}
+
+// A timed-out wait in a tensor-core product, reported once per call.
+static int mlp_check_err(fdtd_b200_mlp *m) {
+    int e = 0;
+    if (cudaMemcpy(&e, m->d_err, sizeof e, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        rfb_set_error("surrogate: reading the error flag failed");
+        return -1;
+    }
+    if (e) {
+        cudaMemset(m->d_err, 0, sizeof(int));
+        rfb_set_error("surrogate: a tensor-core product's wait timed out");
+        return -1;
+    }
+    return 0;
 }
 
 // Forward pass of B rows whose input is already in act[0].
@@ -417,7 +679,7 @@ static void mlp_backward(fdtd_b200_mlp *m, int B) {
         Epi e{};
         e.f32 = ly.gw;
         gemm<EPI_F32>(m, g16t[cur], B, m->actt[l], B, ly.out, ly.in, B, e);
-        k_colsum<<<(ly.out + 127) / 128, 128, 0, m->st>>>(g32[cur], B, ly.out, ly.gb);
+        k_colsum<<<(ly.out + 31) / 32, 256, 0, m->st>>>(g32[cur], B, ly.out, ly.gb);
         m->launches++;
         if (l > 0) {
             // dX = dZ . W = dZ [B][out] . (W^T [in][out])^T, times GELU' of the
@@ -478,7 +740,7 @@ extern "C" void fdtd_b200_mlp_destroy(fdtd_b200_mlp_t *m) {
         cudaFree(ly.w); cudaFree(ly.b); cudaFree(ly.mw); cudaFree(ly.vw); cudaFree(ly.mb); cudaFree(ly.vb);
         cudaFree(ly.gw); cudaFree(ly.gb); cudaFree(ly.w16); cudaFree(ly.w16t);
     }
-    cudaFree(m->X); cudaFree(m->Y); cudaFree(m->perm); cudaFree(m->step);
+    cudaFree(m->X); cudaFree(m->Y); cudaFree(m->perm); cudaFree(m->step); cudaFree(m->d_err);
     if (m->st) cudaStreamDestroy(m->st);
     delete m;
 }
@@ -544,6 +806,21 @@ extern "C" fdtd_b200_mlp_t *fdtd_b200_mlp_create(int n_in, int width, int depth,
     }
     if (cudaMalloc(&m->step, sizeof(long long)) != cudaSuccess) return fail();
     if (cudaMemset(m->step, 0, sizeof(long long)) != cudaSuccess) return fail();
+    if (cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess) return fail();
+    if (cudaMemset(m->d_err, 0, sizeof(int)) != cudaSuccess) return fail();
+    {
+        // RFSYN_FDTD_MLP_GEMM=tcgen05 puts the products whose shapes fit on
+        // k_gemm_tc; by default every product runs on k_gemm_nt, which is
+        // faster on this network's products at every batch measured (see
+        // k_gemm_tc)
+        const char *v = getenv("RFSYN_FDTD_MLP_GEMM");
+        const bool want = v && !strcmp(v, "tcgen05");
+        m->tc = want && tc_attrs<32>();
+        if (want && !m->tc) {
+            rfb_set_error("mlp: cannot configure the tensor-core products' shared memory");
+            return fail();
+        }
+    }
     if (mlp_sync_bf16(m) != 0) return fail();
     if (cudaStreamSynchronize(m->st) != cudaSuccess) return fail();
     return m;
@@ -636,6 +913,7 @@ extern "C" int fdtd_b200_mlp_grad(fdtd_b200_mlp_t *m, const float *X, const floa
     const int nb = (B * m->n_out + 255) / 256;
     MCK(cudaMemcpyAsync(part.data(), m->partial, nb * 4, cudaMemcpyDeviceToHost, m->st));
     if (mlp_read_grads(m, grads) != 0) return -1;
+    if (mlp_check_err(m) != 0) return -1;
     double se = 0;
     for (int q = 0; q < nb; q++) se += part[q];
     if (loss) *loss = se / ((double)B * m->n_out);
@@ -748,7 +1026,7 @@ extern "C" int fdtd_b200_mlp_train(fdtd_b200_mlp_t *m, size_t steps, int B, doub
         for (float v : part) se += v;
         *final_loss = se / ((double)B * m->n_out);
     }
-    return 0;
+    return mlp_check_err(m);
 }
 
 // Network outputs of n inputs (any n; evaluated in batches of up to 1024).
@@ -760,7 +1038,8 @@ extern "C" int fdtd_b200_mlp_predict(fdtd_b200_mlp_t *m, const float *X, size_t 
         const size_t rows = std::min<size_t>(B, n - r0);
         std::fill(xb.begin(), xb.end(), 0.f);
         memcpy(xb.data(), X + r0 * m->n_in, rows * m->n_in * sizeof(float));
-        const int Bp = (int)((rows + 63) / 64 * 64);
+        // rows padded to the tensor-core tile height (zero rows)
+        const int Bp = (int)((rows + tc::BM - 1) / tc::BM * tc::BM);
         if (mlp_upload_x(m, xb.data(), Bp, m->act[0]) != 0) return -1;
         mlp_forward(m, Bp);
         MCK(cudaGetLastError());
@@ -768,7 +1047,9 @@ extern "C" int fdtd_b200_mlp_predict(fdtd_b200_mlp_t *m, const float *X, size_t 
                             m->st));
         MCK(cudaStreamSynchronize(m->st));
     }
-    return 0;
+    return mlp_check_err(m);
 }
 
 extern "C" unsigned long long fdtd_b200_mlp_launch_count(const fdtd_b200_mlp_t *m) { return m->launches; }
+
+extern "C" unsigned long long fdtd_b200_mlp_tensor_core_launches(const fdtd_b200_mlp_t *m) { return m->tc_launches; }

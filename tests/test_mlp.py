@@ -1,6 +1,11 @@
 """The surrogate network's GPU kernels (BF16 tensor-core GEMMs with FP32
 accumulation, GELU epilogues, MSE gradient, Adam) against the CPU oracle
 (oracle/mlp_oracle.py, FP64 with the pipeline's bfloat16 rounding points).
+The products run on mma.sync tiles; with RFSYN_FDTD_MLP_GEMM=tcgen05,
+those whose rows are a multiple of 128 run on the tcgen05 tensor cores
+(accumulators in tensor memory): batches of 128 and 256 put every product
+there, checked against the oracle and against the mma.sync products of the
+same network.
 
 Tolerances: the GPU and the oracle round the same operands to bfloat16, so
 they differ by FP32 accumulation order and by an occasional operand that
@@ -97,3 +102,48 @@ def test_training_reduces_loss():
     err = np.mean((net.predict(X[:512]) - Y[:512]) ** 2)
     assert err < 0.1 * loss0
     net.close()
+
+
+@pytest.fixture(scope="module")
+def data256():
+    rng = np.random.default_rng(15)
+    X = rng.uniform(-1, 1, (256, SHAPE["n_in"]))
+    Y = rng.normal(0, 1, (256, SHAPE["n_out"]))
+    return X, Y
+
+
+@pytest.mark.parametrize("batch", [128, 256])
+def test_tensor_core_gradient_matches_oracle(data256, batch, monkeypatch):
+    X, Y = data256
+    monkeypatch.setenv("RFSYN_FDTD_MLP_GEMM", "tcgen05")
+    net = rb.Mlp(**SHAPE, seed=11)
+    orc = MlpOracle(**SHAPE)
+    p = net.params().astype(np.float64)
+    n0 = net.tensor_core_launches()
+    loss, g = net.grad(X[:batch], Y[:batch])
+    # every product of the pass (forward, dW, dX) ran on the tcgen05 path
+    assert net.tensor_core_launches() - n0 == 3 * (SHAPE["depth"] + 1) - 1
+    loss_o, g_o = orc.loss_grad(p, X[:batch], Y[:batch], bf16=True)
+    assert abs(loss - loss_o) <= 1e-4 * abs(loss_o)
+    assert _rel(g.astype(np.float64), g_o) < 2e-3
+    out = net.predict(X[:batch])
+    assert _rel(out.astype(np.float64), orc.predict(p, X[:batch], bf16=True)) < 2e-3
+    net.close()
+
+
+def test_tensor_core_products_agree_with_mma_sync(data256, monkeypatch):
+    """The same network, batch and data through both product kernels: they
+    differ only by the FP32 accumulation order."""
+    X, Y = data256
+    monkeypatch.setenv("RFSYN_FDTD_MLP_GEMM", "tcgen05")
+    a = rb.Mlp(**SHAPE, seed=12)
+    monkeypatch.delenv("RFSYN_FDTD_MLP_GEMM")
+    b = rb.Mlp(**SHAPE, seed=12)
+    la, ga = a.grad(X, Y)
+    lb, gb = b.grad(X, Y)
+    assert a.tensor_core_launches() > 0 and b.tensor_core_launches() == 0
+    assert abs(la - lb) <= 1e-5 * abs(lb)
+    assert _rel(ga.astype(np.float64), gb.astype(np.float64)) < 1e-3
+    a.close()
+    b.close()
+
