@@ -2,9 +2,13 @@
 counterpart.  The CPU oracle restates them (oracle/fdtd_oracle.c) and is
 pinned by physics: the static limit (delta_eps -> 0 reproduces a plain
 eps_inf medium), the reflection of a plane wave from Debye / Lorentz
-half-spaces against Fresnel with eps(omega), and the sphere fill
-fractions' volume partition.  The GPU
-paths are held bit-for-bit to the oracle in FP64."""
+half-spaces against Fresnel with eps(omega), the field energy of passive
+dispersive media in a closed box (never growing, decaying), and the sphere
+fill fractions' volume partition, their known answers (half, quarter and
+three-eighths cubes, 0 / 1 beyond the half diagonal, the squared normal)
+and their z-invariant limit against rfsyn's 2-D square share
+(subpixel_te_rectangle_fraction).  The GPU paths are held bit-for-bit to
+the oracle in FP64."""
 from __future__ import annotations
 
 import math
@@ -180,3 +184,127 @@ def test_sphere_fractions_partition_volume():
     for c in range(3):
         assert abs(fr[c::3].sum() - vol) / vol < 2e-3
     assert fr.min() >= 0.0 and fr.max() <= 1.0
+
+
+# ---- known answers of the fill fractions and a passivity pin ------------------------
+# A sphere of radius 1e4 is a plane at the scale of one cell (its surface
+# leaves the tangent plane by at most (sqrt(3)/2)^2 / 2e4 < 4e-5 cells over a
+# cube), so with the centre placed at p + (d - R) n the sphere holds the
+# points x near the sample p with n . (x - p) <= d.
+_R = 1.0e4
+
+
+def _fractions():
+    import ctypes as C
+
+    lib = rb.load()
+    f = lib.rfb_sphere_fractions
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(C.c_double), C.c_double] + [C.c_int] * 6 + [C.POINTER(C.c_double)] * 2
+
+    def plane(cell, comp, n, d):
+        p = np.array(cell, dtype=float)
+        p[comp] += 0.5
+        cen = (C.c_double * 3)(*(p + (d - _R) * np.asarray(n, dtype=float)))
+        fr, n2 = np.zeros(3), np.zeros(3)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        assert f(cen, _R, cell[0], cell[1], cell[2], 1, 1, 1, dp(fr), dp(n2)) == 0
+        return fr[comp], n2[comp]
+
+    return plane
+
+
+_LAT = (np.arange(8) + 0.5) / 8 - 0.5  # lattice offsets of the 8^3 points
+
+
+@pytest.mark.gpu
+def test_sphere_fraction_known_answers():
+    """Axis-aligned surfaces through and near the sample: half, quarter and
+    three-eighths cubes exactly (lattice layers at odd sixteenths), 0 and 1
+    beyond the half diagonal, and the squared normal of the sample's
+    component exactly 1 or 0."""
+    plane = _fractions()
+    want = {0.0: 0.5, 0.25: 0.75, -0.25: 0.25, 0.375: 0.875, -0.375: 0.125, 0.9: 1.0, -0.9: 0.0}
+    for comp in range(3):
+        for axis in range(3):
+            for sign in (1.0, -1.0):
+                n = np.zeros(3)
+                n[axis] = sign
+                for d, fw in want.items():
+                    fr, n2 = plane((7, 6, 5), comp, n, d)
+                    assert fr == fw, (comp, axis, sign, d, fr)
+                    assert n2 == (1.0 if axis == comp else 0.0)
+
+
+@pytest.mark.gpu
+def test_sphere_fraction_two_d_limit_against_subpixel_te():
+    """A surface invariant along z: the cube's share is the 8 x 8 lattice
+    count of the square cut by the line, exactly, and within the lattice's
+    resolution of rfsyn's exact square share (subpixel_te_rectangle_fraction
+    of a rectangle whose edge is that line)."""
+    import ctypes as C
+
+    from tests.test_subpixel import Rect, _bind
+
+    plane = _fractions()
+    lib = _bind(rb.load())
+    rng = np.random.default_rng(21)
+    diffs = []
+    checked = 0
+    while checked < 300:
+        th, d = rng.uniform(-np.pi, np.pi), rng.uniform(-0.7, 0.7)
+        n = np.array([np.cos(th), np.sin(th), 0.0])
+        s = n[0] * _LAT[:, None] + n[1] * _LAT[None, :] - d
+        if np.abs(s).min() < 1e-3:  # a lattice point on the line: the curvature decides it
+            continue
+        fr, n2 = plane((9, 9, 4), 2, n, d)
+        assert fr == np.count_nonzero(s <= 0) / 64.0, (th, d, fr)
+        assert n2 <= 1e-20  # Ez sample, normal in the (x, y) plane
+        p2 = np.array([9.0, 9.0])
+        cen = p2 + (d - 0.5 * _R) * n[:2]
+        area = C.c_double()
+        assert lib.subpixel_te_rectangle_fraction(C.byref(Rect(cen[0], cen[1], _R, _R, th)), p2[0], p2[1], 1.0, 1.0,
+                                                  C.byref(area)) == 0
+        diffs.append(abs(fr - area.value))
+        checked += 1
+    # an 8 x 8 lattice of a unit square cut by a straight line: at most one
+    # point per lattice column or row misjudged, |error| <= 8 / 64
+    assert max(diffs) <= 0.125 and np.mean(diffs) < 0.03, (max(diffs), np.mean(diffs))
+
+
+@pytest.mark.gpu
+def test_passive_dispersive_media_do_not_gain_energy():
+    """A PEC box holding lossy Debye and damped Lorentz media (passive:
+    delta_eps > 0, tau > 0, gamma > 0, sigma >= 0), excited by a short pulse
+    and then left alone: the field energy never grows window over window
+    (rfsyn's windowed-peak test, validate_long_term_stability.c:226-253,
+    with a 5 % margin for beating) and decays as the media absorb it."""
+    lorentz = ("lorentz", 3.0, 2 * math.pi * 12e9, 2 * math.pi * 2e9)
+    debye = ("debye", 5.0, 3e-11)
+    n_steps = 3000
+    s = Scene(nx=20, ny=20, nz=20, n_steps=n_steps, npml=0,
+              sources=[(10, 10, 10, 2, 0, 1.0, 0, 20 * DT, 5 * DT, 0)], probes=[(12, 10, 10, 2)],
+              disp=[disp_entry(c, i, j, k, 2.0, 0.005, [lorentz, debye] if (i + j) % 2 else [debye])
+                    for c in range(3) for i in range(4, 16) for j in range(4, 16) for k in range(4, 16)])
+    for precision in (rb.FP64, rb.FP32):
+        from tests.cases import scene_run_config
+
+        import ctypes as C
+
+        rc = scene_run_config(s, precision, rb.FUSED)
+        cs = s.to_c()
+        sim = rb.Sim(rc, oracle.device_setup(), C.cast(C.pointer(cs), C.c_void_p))
+        energy = []
+        try:
+            for _ in range(n_steps // 10):
+                sim.advance(10)
+                e = sim.energy()
+                energy.append(e["electric_j"] + e["magnetic_j"])
+        finally:
+            sim.close()
+        energy = np.array(energy)
+        assert np.all(np.isfinite(energy)) and energy.max() > 0
+        tail = energy[10:]  # the pulse ends by step 50
+        peaks = tail[: len(tail) // 29 * 29].reshape(-1, 29).max(axis=1)  # windows of 290 steps
+        assert np.all(peaks[1:] <= 1.05 * peaks[:-1]), (precision, peaks)
+        assert peaks[-1] <= 0.5 * peaks[0], (precision, peaks)
