@@ -618,8 +618,8 @@ struct rfb_engine {
     double dft_t_off = 0.0;
     double *d_run_omega = nullptr;
     void *d_acc = nullptr;
-    cudaStream_t stream = nullptr, stream2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
     int own_stream = 0;
     int parity = 0;
     static constexpr int CHUNK = 16;
@@ -772,25 +772,42 @@ static void launch_int(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st
     } else if (e->plan.tma) launch_interior_tma<T>(a, e->plan, m, e->d_err, st);
     else launch_interior<T>(a, e->plan, st);
 }
-// Everything else of the sweep: the slab / boundary queue (mode 2) and the
-// cp.async-fed edge sweep (the items whose halo wraps, in mode 2).
+// Work-queue plans that also hold cp.async-fed edge items (the tiles whose
+// halo wraps around a periodic y / z axis) run those on a third stream:
+// both edge launches are bound by the march of one item, so one after the
+// other they would take twice as long as side by side.
+static bool edge_on_third_stream(const rfb_engine *e) {
+    return e->plan.tma >= 2 && e->plan.n_edge > 0 && e->stream3 != nullptr;
+}
+
+// Everything else of the sweep: the slab / boundary queue (modes 2-4) and
+// the cp.async-fed edge sweep (mode 0 and 1 edge tiles; in modes 2-4 the
+// items whose halo wraps, unless they have the third stream).
 template <typename T>
 static void launch_rest(rfb_engine *e, const Args<T> &a, int par, cudaStream_t st) {
     if (e->plan.tma >= 2) launch_q_t<T>(a, e->plan, 2, e->tmaps[e->nbuf == 2 ? par : 0], e->d_err, st);
-    launch_edge<T>(a, e->plan, st);
+    if (!edge_on_third_stream(e)) launch_edge<T>(a, e->plan, st);
 }
 
 // One fused sweep: the interior kinds on the engine stream, the slab /
 // boundary kinds on the second stream, side by side (they touch disjoint
-// cells).  A third stream for the x-slab kind measured slower on C2.
+// cells); a work-queue plan's cp.async-fed edge items on a third.  A third
+// stream for the x-slab kind measured slower on C2.
 template <typename T>
 static void launch_sweep(rfb_engine *e, const Args<T> &a, int par) {
+    const bool third = edge_on_third_stream(e);
     cudaEventRecord(e->ev_fork, e->stream);
     cudaStreamWaitEvent(e->stream2, e->ev_fork, 0);
+    if (third) cudaStreamWaitEvent(e->stream3, e->ev_fork, 0);
     launch_int<T>(e, a, par, e->stream);
     launch_rest<T>(e, a, par, e->stream2);
+    if (third) {
+        launch_edge<T>(a, e->plan, e->stream3);
+        cudaEventRecord(e->ev_join3, e->stream3);
+    }
     cudaEventRecord(e->ev_join, e->stream2);
     cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+    if (third) cudaStreamWaitEvent(e->stream, e->ev_join3, 0);
 }
 
 // Threads of the interface-list launch: the entries left to it when some
@@ -1395,7 +1412,9 @@ extern "C" void rfb_engine_destroy(rfb_engine_t *e) {
     t_phase = rfb_now();
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
+    if (e->ev_join3) cudaEventDestroy(e->ev_join3);
     if (e->stream2) cudaStreamDestroy(e->stream2);
+    if (e->stream3) cudaStreamDestroy(e->stream3);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
     rfb_trace("destroy: streams and host state", t_phase);
@@ -1567,8 +1586,10 @@ static rfb_engine_t *engine_create(const rfb_geom_t *geom, int precision, int sc
             goto created;
         }
         CK(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&e->stream3, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_join3, cudaEventDisableTiming));
         if (tma_prepare() != 0 || q_prepare() != 0 || qi2_prepare() != 0) {
             rfb_set_error("cannot configure the TMA sweep kernels' shared memory");
             goto fail_noset;
