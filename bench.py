@@ -12,6 +12,12 @@ Mcell-updates/s = nx*ny*nz*n_steps*K / seconds, whole job.
 --impl reference times rfsyn's own CPU loop (compiled from its sources into
 oracle/_ref, or the CPU oracle port when that build is absent) on all host
 cores, on a bounded sample of the same scene.
+
+On one GPU the default run also runs the other workloads after its own
+measurements -- the C3 periodic cell, the C4 batch of 512 scenes and the C5
+surrogate path, each `python bench.py --workload cN ...` in its own process
+-- and carries their figures under "other_workloads" (--no-other-workloads
+skips them; about three minutes).
 """
 from __future__ import annotations
 
@@ -423,6 +429,9 @@ def run_b200(args) -> None:
     ranks.finish(rk)
     if rank != 0:
         return
+    # a default single-GPU run also records the other workloads (after this
+    # workload's measurements, so they do not disturb them)
+    others = other_workloads() if (world == 1 and args.workload == "c2" and not args.no_other_workloads) else None
     field_mb = (w.nx + 1) * (w.ny + 1) * (w.nz + 1) * esz / 1e6
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -457,7 +466,62 @@ def run_b200(args) -> None:
         "fp64": {"value": w.cells * w.n_steps / (fp64["ms"] / 1e3) / 1e6, "unit": METRIC, "ms_per_step": fp64["ms"],
                  "note": "the same scene and step loop in FP64 on the device, one run after a warm-up run"},
     }
+    if others is not None:
+        line["other_workloads"] = others
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# The other workloads, summarised in the default run's line
+# ---------------------------------------------------------------------------
+OTHER_RUNS = {
+    "c3": ["--workload", "c3", "--steps", "2", "--warmup", "3", "--no-cpu-baseline"],
+    "c4": ["--workload", "c4", "--steps", "2", "--warmup", "3"],
+    "c5": ["--workload", "c5"],
+}
+
+
+def _summary(name: str, d: dict) -> dict:
+    """The figures of another workload's line that the default line carries."""
+    r, e = d.get("roofline") or {}, d.get("e2e") or {}
+    out = {"metric": d.get("metric"), "value": d.get("value"), "unit": d.get("unit"),
+           "ms_per_step": d.get("ms_per_step"), "frac": r.get("frac"), "e2e": e.get("value"),
+           "clocks": d.get("clocks")}
+    if name == "c3":
+        out.update({"workload": (d.get("config") or {}).get("workload"), "plan": (d.get("config") or {}).get("plan"),
+                    "parity_spec_l2_max": (d.get("parity") or {}).get("spec_l2_max"),
+                    "fp64": (d.get("fp64") or {}).get("value")})
+    elif name == "c4":
+        out.update({"scenes_per_s": d.get("scenes_per_s"), "plain_one_at_a_time": d.get("plain_one_at_a_time")})
+    elif name == "c5":
+        out.update({"speedup_vs_plain": d.get("speedup_vs_plain"), "accepted_scene_frac": d.get("accepted_scene_frac"),
+                    "plain_one_at_a_time_scenes_s": d.get("plain_one_at_a_time_scenes_s"),
+                    "batched_fdtd_scenes_s": d.get("batched_fdtd_scenes_s"),
+                    "transfer_rel_err": d.get("transfer_rel_err"), "timings_s": d.get("timings_s")})
+    return out
+
+
+def other_workloads() -> dict:
+    """Runs the C3, C4 and C5 benches (each its own process, one after the
+    other on this GPU) and returns their figures, so a default single-GPU
+    run records every workload; a workload that fails is reported, never
+    fatal."""
+    res = {}
+    for name, argv in OTHER_RUNS.items():
+        t0 = time.perf_counter()
+        try:
+            p = subprocess.run([sys.executable, str(ROOT / "bench.py"), *argv], capture_output=True, text=True,
+                               timeout=1200)
+            lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
+            if p.returncode != 0 or not lines:
+                res[name] = {"error": f"exit {p.returncode}: {(p.stderr or p.stdout)[-300:]}"}
+            else:
+                res[name] = _summary(name, json.loads(lines[-1]))
+        except Exception as exc:  # reported, never fatal
+            res[name] = {"error": str(exc)[:300]}
+        res[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+        res[name]["command"] = "python bench.py " + " ".join(argv)
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -732,6 +796,8 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=3, help="end-to-end calls averaged for e2e")
     ap.add_argument("--ref-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="c2 on one GPU: skip the C3, C4 and C5 runs summarised in the line")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--train-scenes", type=int, default=5000, help="c5: training scenes (4 samples each)")
     ap.add_argument("--test-scenes", type=int, default=500, help="c5: held-out scenes")
