@@ -588,7 +588,8 @@ static int mlp_batch_buffers(fdtd_b200_mlp *m, int B) {
 // surrogate does).
 template <int EPI>
 static void gemm(fdtd_b200_mlp *m, const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, Epi epi) {
-    if (m->tc && M % tc::BM == 0 && N % 32 == 0 && K % tc::BK == 0 && lda % 8 == 0 && ldb % 8 == 0) {
+    if (m->tc && M > 0 && N > 0 && K > 0 && M % tc::BM == 0 && N % 32 == 0 && K % tc::BK == 0 && lda % 8 == 0 &&
+        ldb % 8 == 0) {
         dim3 grid(N / 32, M / tc::BM);
         k_gemm_tc<EPI, 32><<<grid, tc::THREADS, tc::Shape<32>::SMEM, m->st>>>(A, lda, B, ldb, M, N, K, epi,
                                                                             m->d_err);
