@@ -842,12 +842,21 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
          * sphere as they grow */
         double shell = 0.0, vol = 0.0;
         for (size_t q = 0; q < n_spheres; q++) {
-            const double r = spheres[q].radius;
-            if (!isfinite(r) || r <= 0.0) continue;
-            if (spheres[q].model)
-                vol += 3.0 * (4.0 / 3.0) * M_PI * (r + 1.0) * (r + 1.0) * (r + 1.0);
+            const fdtd_b200_sphere_t *sp = &spheres[q];
+            const double r = sp->radius, cen[3] = {sp->cx, sp->cy, sp->cz};
+            if (!isfinite(r) || r <= 0.0 || !isfinite(cen[0]) || !isfinite(cen[1]) || !isfinite(cen[2])) continue;
+            /* the part of its box inside the grid bounds both: its volume
+             * the dispersive samples, its surface area the sphere's surface
+             * inside it (the part of a convex surface inside a box has no
+             * more area than the box) */
+            double e[3];
+            for (int a = 0; a < 3; a++)
+                e[a] = fmax(0.0, fmin(cen[a] + r + 2.0, (double)n[a]) - fmax(cen[a] - r - 2.0, 0.0) + 1.0);
+            const double box_vol = e[0] * e[1] * e[2], box_area = 2.0 * (e[0] * e[1] + e[1] * e[2] + e[2] * e[0]);
+            if (sp->model)
+                vol += 3.0 * fmin((4.0 / 3.0) * M_PI * (r + 1.0) * (r + 1.0) * (r + 1.0), box_vol);
             else
-                shell += 3.0 * 4.0 * M_PI * (r + 1.0) * (r + 1.0) * 1.3;
+                shell += 3.0 * 1.3 * fmin(4.0 * M_PI * (r + 1.0) * (r + 1.0), box_area);
         }
         const double cap = 3.0 * (double)mat->total;
         omap_t *dst = smoothing == 2 ? &mat->tensor3 : &mat->scalar;
