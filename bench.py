@@ -506,12 +506,16 @@ def other_workloads() -> dict:
     other on this GPU) and returns their figures, so a default single-GPU
     run records every workload; a workload that fails is reported, never
     fatal."""
+    # each run is a standalone single-GPU process (no rendezvous variables)
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE", "GROUP_RANK", "MASTER_ADDR",
+                        "MASTER_PORT") and not k.startswith("TORCHELASTIC_")}
     res = {}
     for name, argv in OTHER_RUNS.items():
         t0 = time.perf_counter()
         try:
             p = subprocess.run([sys.executable, str(ROOT / "bench.py"), *argv], capture_output=True, text=True,
-                               timeout=1200)
+                               timeout=1200, env=env)
             lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
             if p.returncode != 0 or not lines:
                 res[name] = {"error": f"exit {p.returncode}: {(p.stderr or p.stdout)[-300:]}"}

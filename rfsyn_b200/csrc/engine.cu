@@ -1745,6 +1745,9 @@ extern "C" int rfb_engine_reset(rfb_engine_t *e) {
     }
     if (e->d_acc)
         CK(cudaMemsetAsync(e->d_acc, 0, (size_t)(e->n_probes + e->n_planes) * e->n_freqs * 4 * e->esz, e->stream));
+    // the plane gather's counters are zero between launches; a launch cut
+    // short by an error would leave them counting
+    if (e->d_plane_count) CK(cudaMemsetAsync(e->d_plane_count, 0, (size_t)e->n_planes * sizeof(int), e->stream));
     CK(cudaMemsetAsync(e->d_step, 0, sizeof(int), e->stream));
     e->steps_done = 0;
     e->parity = 0;
