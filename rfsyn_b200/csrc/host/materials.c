@@ -8,6 +8,8 @@
  * clear / lookup instead of sorted arrays with memmove), and are sorted only
  * once, when the device image is built. */
 #include <math.h>
+#include <pthread.h>
+#include <unistd.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1215,6 +1217,88 @@ static int32_t t3_record_index(t3_dedupe_t *d, double *recs, size_t *n) {
     }
 }
 
+/* Pass 1 of the image's list entries over list cells [q0, q1): cell
+ * coordinates, the scalar (Ca, Cb) of every entry and its kind -- COPY for
+ * components the sweep does not update, TENSOR3 (map slot in tix), TENSOR,
+ * ADE (map slot in aix) or SCALAR, in that precedence.  It only reads the
+ * maps, so ranges run on several threads. */
+typedef struct {
+    const materials_t *mat;
+    const fdtd_grid_t *g;
+    const uint64_t *cells;
+    rfb_scene_build_t *out;
+    size_t q0, q1;
+} image_range_t;
+
+static void *image_pass1_range(void *arg) {
+    const image_range_t *p = arg;
+    const materials_t *mat = p->mat;
+    const fdtd_grid_t *g = p->g;
+    rfb_scene_build_t *out = p->out;
+    const size_t nz1 = g->nz + 1;
+    for (size_t q = p->q0; q < p->q1; q++) {
+        const size_t idx = (size_t)p->cells[q];
+        const size_t k = idx % nz1, row = idx / nz1, j = row % (g->ny + 1), i = row / (g->ny + 1);
+        out->cell_ijk[3 * q] = (int32_t)i;
+        out->cell_ijk[3 * q + 1] = (int32_t)j;
+        out->cell_ijk[3 * q + 2] = (int32_t)k;
+        for (int c = 0; c < 3; c++) {
+            const size_t e = 3 * q + (size_t)c;
+            out->tix[e] = -1;
+            out->src[e] = -1;
+            out->aix[e] = -1;
+            const material_coeff_t co = lookup(mat, idx, c);
+            out->ca[e] = co.Ca;
+            out->cb[e] = co.Cb;
+            if (!rfb_e_swept(g, c, i, j, k)) {
+                out->kind[e] = RFB_LK_COPY;
+                continue;
+            }
+            const long t3 = omap_find(&mat->tensor3, (uint64_t)idx * 3 + (uint64_t)c);
+            if (t3 >= 0) {
+                out->kind[e] = RFB_LK_TENSOR3;
+                out->tix[e] = (int32_t)t3;
+                continue;
+            }
+            if (c < 2 && tensor_at(mat, idx, c)) {
+                out->kind[e] = RFB_LK_TENSOR;
+                continue;
+            }
+            const long dm = omap_find(&mat->disp, (uint64_t)idx * 3 + (uint64_t)c);
+            if (dm < 0) {
+                out->kind[e] = RFB_LK_SCALAR;
+            } else {
+                out->kind[e] = RFB_LK_ADE;
+                out->aix[e] = (int32_t)dm;
+            }
+        }
+    }
+    return NULL;
+}
+
+/* Pass 1 over all nc list cells on up to 16 threads (the online cores;
+ * one for short lists); a thread that cannot start leaves its range to
+ * the calling thread. */
+static void image_pass1(const materials_t *mat, const fdtd_grid_t *g, const uint64_t *cells, size_t nc,
+                        rfb_scene_build_t *out) {
+    enum { MAX_T = 16 };
+    long nt = sysconf(_SC_NPROCESSORS_ONLN);
+    if (nt > MAX_T) nt = MAX_T;
+    if (nt > (long)(nc / 16384) + 1) nt = (long)(nc / 16384) + 1;
+    if (nt < 1) nt = 1;
+    image_range_t job[MAX_T];
+    pthread_t th[MAX_T];
+    int started[MAX_T] = {0};
+    for (long t = 0; t < nt; t++)
+        job[t] = (image_range_t){mat, g, cells, out, nc * (size_t)t / (size_t)nt, nc * (size_t)(t + 1) / (size_t)nt};
+    for (long t = 1; t < nt; t++) started[t] = pthread_create(&th[t], NULL, image_pass1_range, &job[t]) == 0;
+    image_pass1_range(&job[0]);
+    for (long t = 1; t < nt; t++) {
+        if (started[t]) pthread_join(th[t], NULL);
+        else image_pass1_range(&job[t]);
+    }
+}
+
 int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n_extra, const rfb_extra_cell_t *extra,
                           rfb_scene_build_t *out) {
     memset(out, 0, sizeof(*out));
@@ -1328,26 +1412,28 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
         free(models);
         goto oom;
     }
+    /* pass 1, in parallel over ranges of list cells: coordinates, scalar
+     * coefficients and each entry's kind; a 3x3 or dispersive sample keeps
+     * its map slot in tix / aix for pass 2 */
+    if (mat->tensor3.cap >= (size_t)INT32_MAX || mat->disp.cap >= (size_t)INT32_MAX) {
+        free(models);
+        goto oom;
+    }
+    image_pass1(mat, g, cells, nc, out);
+    /* pass 2, in entry order: the records, numbered as the entries meet
+     * them (3x3 records deduplicated, ADE models, 2x2 tensor records); the
+     * last 3x3 record of each component and the last model are tried
+     * first (neighbouring cells of a uniform region share them) */
+    int32_t last3[3] = {-1, -1, -1};
+    size_t last_model = 0;
     for (size_t q = 0; q < nc; q++) {
-        size_t idx = (size_t)cells[q];
-        size_t k = idx % nz1, row = idx / nz1, j = row % (g->ny + 1), i = row / (g->ny + 1);
-        out->cell_ijk[3 * q] = (int32_t)i;
-        out->cell_ijk[3 * q + 1] = (int32_t)j;
-        out->cell_ijk[3 * q + 2] = (int32_t)k;
+        const size_t idx = (size_t)cells[q];
+        const size_t i = (size_t)out->cell_ijk[3 * q], j = (size_t)out->cell_ijk[3 * q + 1],
+                     k = (size_t)out->cell_ijk[3 * q + 2];
         for (int c = 0; c < 3; c++) {
-            size_t e = 3 * q + (size_t)c;
-            out->tix[e] = -1;
-            out->src[e] = -1;
-            out->aix[e] = -1;
-            material_coeff_t co = lookup(mat, idx, c);
-            out->ca[e] = co.Ca;
-            out->cb[e] = co.Cb;
-            if (!rfb_e_swept(g, c, i, j, k)) {
-                out->kind[e] = RFB_LK_COPY;
-                continue;
-            }
-            long long t3 = omap_find(&mat->tensor3, (uint64_t)idx * 3 + (uint64_t)c);
-            if (t3 >= 0) {
+            const size_t e = 3 * q + (size_t)c;
+            const uint8_t kind = out->kind[e];
+            if (kind == RFB_LK_TENSOR3) {
                 /* full 3x3 sample: its row of eps_r^-1, then the update's
                  * coefficients E+ = ca E + s value with the loss of sigma
                  * taken at the component's own permittivity 1/m_cc, as
@@ -1355,7 +1441,7 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
                  * s = dt/(eps0 dx) / (1 + loss), ca = (1 - loss)/(1 + loss),
                  * loss = sigma dt / (2 eps0 / m_cc); lossless: s = dt/(eps0
                  * dx), ca = 1 */
-                const double *row = mat->tensor3.vals + (size_t)t3 * 4;
+                const double *row = mat->tensor3.vals + (size_t)out->tix[e] * 4;
                 double *rec = out->t3 + 5 * nt3;
                 rec[0] = row[0];
                 rec[1] = row[1];
@@ -1363,23 +1449,23 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
                 const double loss = (row[3] * mat->dt) / (2.0 * (EPS0 / row[c]));
                 rec[3] = (mat->dt / (EPS0 * mat->dx)) / (1.0 + loss);
                 rec[4] = (1.0 - loss) / (1.0 + loss);
-                out->kind[e] = RFB_LK_TENSOR3;
                 /* samples with the same record share it (a uniform anisotropic
                  * region is one record per component): fewer record bytes
                  * for the list kernels to read */
-                out->tix[e] = t3_record_index(&t3d, out->t3, &nt3);
+                if (last3[c] >= 0 && !memcmp(out->t3 + 5 * (size_t)last3[c], rec, 5 * sizeof(double)))
+                    out->tix[e] = last3[c];
+                else
+                    out->tix[e] = last3[c] = t3_record_index(&t3d, out->t3, &nt3);
                 continue;
             }
-            const double *t = (c < 2) ? tensor_at(mat, idx, c) : NULL;
-            if (!t) {
-                long long dm = omap_find(&mat->disp, (uint64_t)idx * 3 + (uint64_t)c);
-                if (dm < 0) {
-                    out->kind[e] = RFB_LK_SCALAR;
-                    continue;
-                }
-                const double *mv = mat->disp.vals + (size_t)dm * DISP_W;
+            if (kind == RFB_LK_ADE) {
+                const double *mv = mat->disp.vals + (size_t)out->aix[e] * DISP_W;
                 size_t r = 0;
-                while (r < n_models && memcmp(models + r * DISP_W, mv, DISP_W * sizeof(double)) != 0) r++;
+                if (last_model < n_models && !memcmp(models + last_model * DISP_W, mv, DISP_W * sizeof(double)))
+                    r = last_model;
+                else
+                    while (r < n_models && memcmp(models + r * DISP_W, mv, DISP_W * sizeof(double)) != 0) r++;
+                last_model = r;
                 if (r == n_models) {
                     if (n_models == model_cap) {
                         model_cap *= 2;
@@ -1396,10 +1482,11 @@ int materials_build_image(const materials_t *mat, const fdtd_grid_t *g, size_t n
                     rfb_ade_record(mv, mat->dt, mat->dx, records + r * RFB_ADE_NC);
                     n_models++;
                 }
-                out->kind[e] = RFB_LK_ADE;
                 out->aix[e] = (int32_t)r;
                 continue;
             }
+            if (kind != RFB_LK_TENSOR) continue;
+            const double *t = tensor_at(mat, idx, c);
             /* tensor edge record (materials.c:847-903) */
             out->kind[e] = RFB_LK_TENSOR;
             out->tix[e] = (int32_t)nt;
