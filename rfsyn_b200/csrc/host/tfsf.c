@@ -235,7 +235,12 @@ int rfb_tfsf_build(const fdtd_grid_t *g, const materials_t *mat, const fdtd_b200
                 int near = 0;
                 for (int a = 0; a < 3; a++)
                     if (!(t.per & (1u << a)) && (p[a] <= (long)bl[a] + 2 || p[a] >= (long)bh[a] - 2)) near = 1;
-                if (!near) continue;
+                if (!near) {
+                    /* a column that is near no x / y face meets the shell
+                     * again only at the high z face: skip to it */
+                    if (!(t.per & 4u) && k < (long)bh[2] - 2) k = (long)bh[2] - 3;
+                    continue;
+                }
                 for (int c = 0; c < 3; c++) {
                     /* ---- H_c at p: H -= cbh (dA - dB), dA = E_fa(p+e_axa) - E_fa(p), dB likewise */
                     {
