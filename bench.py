@@ -394,22 +394,30 @@ def run_b200(args) -> None:
 
     # end to end through the C ABI with host buffers: setup on the host,
     # scene upload, the full loop, DFT, download of series and spectra
-    e2e_ms = []
+    # every call with the library's phase trace on (a few lines to a file):
+    # where each call spends its time
+    calls = []
     h2d = d2h = 0
+
+    def one_call():
+        t0 = time.perf_counter()
+        out = rb.run(rc, setup.ptr if setup else None, None)
+        return out, (time.perf_counter() - t0) * 1e3
+
     for _ in range(max(1, args.e2e_steps)):
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = rb.run(rc, setup.ptr if setup else None, None)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        (r, call_ms), call_phases = traced_call(one_call)
+        calls.append((call_ms, call_phases))
         d2h = r["td"].nbytes + r["dft"].nbytes
     h2d = info.h2d_bytes
-    e2e_calls = [round(x, 1) for x in e2e_ms]
-    e2e_mean = sum(e2e_ms) / len(e2e_ms)
+    e2e_calls = [round(c[0], 1) for c in calls]
+    e2e_mean = sum(c[0] for c in calls) / len(calls)
     # the median call: the host set-up of one call now and then takes far
-    # longer than the others on a shared host (every call is listed beside)
-    e2e_ms = ranks.max_over(rk, statistics.median(e2e_ms))
-    # where one end-to-end call spends its time (host phase trace of one more call)
-    _, phases = traced_call(lambda: rb.run(rc, setup.ptr if setup else None, None))
+    # longer than the others on a shared host (every call is listed beside,
+    # with the phases of the median and of the slowest call)
+    by_time = sorted(calls, key=lambda c: c[0])
+    phases, slowest_phases = by_time[len(by_time) // 2][1], by_time[-1][1]
+    e2e_ms = ranks.max_over(rk, statistics.median(c[0] for c in calls))
     e2e_value = ranks.weak_rate(w.cells * w.n_steps, e2e_ms, rk) / 1e6
 
     cpu = None
@@ -463,6 +471,7 @@ def run_b200(args) -> None:
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms, "statistic": "median of the calls", "calls": len(e2e_calls),
                 "calls_ms": e2e_calls, "mean_ms": e2e_mean,
+                "slowest_call_phases_ms": {k: round(v, 3) for k, v in slowest_phases.items()},
                 "phases_ms": {k: round(v, 3) for k, v in phases.items()}},
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -524,8 +524,9 @@ const char *fdtd_b200_last_error(void);
 unsigned long long fdtd_b200_launch_count(void);
 /* Library version string. */
 const char *fdtd_b200_version(void);
-/* Device memory blocks of 1 MB and more that destroyed simulations, stages
- * and batches freed are kept by the library for the next creation (up to a
+/* Device memory blocks that destroyed simulations, stages and batches freed
+ * (1 MB and more rounded to 2 MB, smaller ones to a power of two) are kept
+ * by the library for the next creation (up to a
  * quarter of each device's memory; an allocation that fails empties the
  * cache first).  fdtd_b200_cached_bytes reports what is held;
  * fdtd_b200_release_cached_memory returns all of it to the driver. */

@@ -56,9 +56,11 @@ extern "C" void rfb_count_launch(void) { g_launches++; }
 // a few milliseconds each on B200 (measured), and one scene holds dozens of
 // them, so a process that creates and destroys simulations again and again
 // (end-to-end runs, batches, sweeps of scenes) spent most of its set-up time
-// in the driver.  Blocks of 1 MB and more are rounded up to 2 MB and, when
-// freed, kept per device for the next allocation of a size within a quarter
-// of theirs.  A freed block enters the cache after a device synchronisation,
+// in the driver.  Blocks of 1 MB and more are rounded up to 2 MB, smaller
+// ones to a power of two (at least 256 bytes; the driver calls for small
+// blocks were seen to stall a session's set-up or destroy by tens of
+// milliseconds now and then), and, when freed, kept per device for the next
+// allocation of a size within a quarter of theirs.  A freed block enters the cache after a device synchronisation,
 // the same implicit synchronisation cudaFree performs, so no pending work
 // can still touch it when it is handed out again.  The cache holds at most a
 // quarter of the device's memory; an allocation that fails empties the
@@ -104,12 +106,20 @@ static void arm_alloc_failure(bool on) {
 static cudaError_t dmalloc_raw(void **p, size_t n) {
     *p = nullptr;
     if (g_fail_countdown > 0 && --g_fail_countdown == 0) return cudaErrorMemoryAllocation;
-    if (n < MC_MIN) return cudaMalloc(p, n);
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return ce;
     if (dev < 0 || dev >= 64) return cudaMalloc(p, n);
-    const size_t want = (n + MC_GRAIN - 1) / MC_GRAIN * MC_GRAIN;
+    // size classes: powers of two from 256 bytes below MC_MIN, multiples
+    // of MC_GRAIN above, so a block freed by one session fits the same
+    // request of the next and steady-state sessions make no driver calls
+    size_t want;
+    if (n < MC_MIN) {
+        want = 256;
+        while (want < n) want *= 2;
+    } else {
+        want = (n + MC_GRAIN - 1) / MC_GRAIN * MC_GRAIN;
+    }
     MemCache &c = mem_cache();
     std::lock_guard<std::mutex> lk(c.mu);
     auto &fb = c.free_blocks[dev];

@@ -1,5 +1,6 @@
-"""The library's device memory cache: blocks of 1 MB and more that a
-destroyed simulation freed are handed to the next creation, still holding
+"""The library's device memory cache: blocks that a destroyed simulation
+freed (1 MB and more rounded to 2 MB, smaller ones to a power of two) are
+handed to the next creation, still holding
 the previous simulation's fields, PML state and scene arrays.  A simulation
 built on reused blocks must give the same probe series and spectra, bit for
 bit, as the same simulation built on fresh memory, and releasing the cache
