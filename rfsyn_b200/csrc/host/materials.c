@@ -933,8 +933,9 @@ int fdtd_b200_materials_add_spheres(materials_t *mat, const fdtd_grid_t *g, cons
                     const size_t cell = ((size_t)di * nj + (size_t)dj) * nk + (size_t)dk;
                     const double *fc = f + 3 * cell, *nc = n2 + (full ? 9 : 3) * cell;
                     if (fc[0] <= 0.0 && fc[1] <= 0.0 && fc[2] <= 0.0) continue; /* outside the sphere */
-                    int valid[3];
-                    for (int c = 0; c < 3; c++) valid[c] = sample_valid(g, c, i, j, k);
+                    int valid[3] = {1, 1, 1};  /* every sample of a cell below the last planes */
+                    if (i + 1 >= n[0] || j + 1 >= n[1] || k + 1 >= n[2])
+                        for (int c = 0; c < 3; c++) valid[c] = sample_valid(g, c, i, j, k);
                     const size_t w = fdtd_index(g, i, j, k);
                     if (fc[0] == 1.0 && fc[1] == 1.0 && fc[2] == 1.0 && valid[0] && valid[1] && valid[2]) {
                         if (mat->touched[w]) {
