@@ -499,8 +499,10 @@ int fdtd_b200_materials_apply_heightmap(materials_t *mat, const fdtd_grid_t *g, 
  * every GPU that loads it until the process exits; a box of more than 2^20
  * samples is rejected with -1.  The first call on a device sets that device
  * up (once): it looks the staging array up, which may load the part of the
- * library that holds it and so commit its 16 MiB at that moment, and it
- * creates the non-blocking stream the calls run on.  Make that first call at
+ * library that holds it and so commit its 16 MiB at that moment (CUDA loads
+ * a library's device code lazily by default; with CUDA_MODULE_LOADING=EAGER
+ * in the environment the array is committed with the device's context
+ * instead), and it creates the non-blocking stream the calls run on.  Make that first call at
  * start-up: before any stream capture, and before another framework's pool
  * takes the device's memory.  Later calls launch on that stream and copy back
  * with asynchronous copies on it, so they never wait on the legacy default
