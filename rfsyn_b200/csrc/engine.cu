@@ -153,16 +153,24 @@ static cudaError_t dmalloc(X **p, size_t n) {
 static cudaError_t dfree(void *p) {
     if (!p) return cudaSuccess;
     MemCache &c = mem_cache();
-    std::lock_guard<std::mutex> lk(c.mu);
+    std::unique_lock<std::mutex> lk(c.mu);
     auto it = c.live.find(p);
-    if (it == c.live.end()) return cudaFree(p);
+    if (it == c.live.end()) {
+        lk.unlock();
+        return cudaFree(p);
+    }
     const int dev = it->second.first;
     const size_t size = it->second.second;
     c.live.erase(it);
+    // the block is cached only once no work queued before this call can
+    // still touch it; the wait runs without the lock, so other threads'
+    // allocations and frees are not held up behind this device's work
+    lk.unlock();
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != dev) cudaSetDevice(dev);
     cudaError_t ce = cudaDeviceSynchronize();
+    lk.lock();
     if (!c.cap[dev]) {
         size_t fr = 0, tot = 0;
         c.cap[dev] = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? tot / 4 : 0;
