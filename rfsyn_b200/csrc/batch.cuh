@@ -134,9 +134,12 @@ __global__ void k_probe_gather_b(const ProbeRefB<T> *p, int n, int out_buf, long
 // CTAs per SM of the batched sweeps: the interior as in the single-scene
 // plan; the FP32 x-slab and edge kinds, which keep the scene's parameters in
 // registers loaded from shared memory, at 3 (8-row tiles) or 1 (16-row);
-// FP64 as in the single-scene plan.
+// the FP32 single-queue kind with 8-row tiles at 4 (64 registers, 176 bytes
+// of spills, against 80 registers at 3: stalled on waits, barriers and
+// instruction fetch, it gains from the extra warps -- C4's step 4.681 ->
+// 4.616 ms); FP64 as in the single-scene plan.
 #define RFB_QB_MINB(TT, TJ_, MBI_, MBE_, KIND_) \
-    ((KIND_) == 0 ? (MBI_) : sizeof(TT) == 8 ? (MBE_) : ((TJ_) == 16 ? 1 : 3))
+    ((KIND_) == 0 ? (MBI_) : sizeof(TT) == 8 ? (MBE_) : ((TJ_) == 16 ? 1 : (KIND_) == 5 ? 4 : 3))
 #define RFB_LAUNCH_QB(TT, TJ_, NS_, MBI_, MBE_)                                                            \
     if (tj == TJ_ && ns == NS_) {                                                                          \
         constexpr int MB_ = RFB_QB_MINB(TT, TJ_, MBI_, MBE_, KIND);                                                  \
