@@ -32,6 +32,7 @@ batch engine (fdtd_b200_batch_*).
 """
 from __future__ import annotations
 
+import functools
 import math
 import time
 from dataclasses import dataclass
@@ -105,14 +106,24 @@ def features(w: sc.Workload, rx: int) -> np.ndarray:
 
 def source_spectrum(w: sc.Workload) -> np.ndarray:
     """DFT of the transmitted waveform samples (engine convention: sample n
-    at t = n dt for the source, weight dt)."""
+    at t = n dt for the source, weight dt).  Scenes that share the waveform,
+    dt, step count and bins share one (read-only) array: the transform
+    costs ~10-20 ms of host time and every surrogate scene has the same."""
     s = w.sources[0]
-    dt = w.dt
-    t = np.arange(w.n_steps) * dt
-    u = (t - s["p1"]) / s["p2"]
-    v = s["amplitude"] * np.exp(-u * u) * np.sin(2.0 * math.pi * s["p0"] * (t - s["p1"]))
-    f = np.asarray(w.freqs)
-    return (v[None, :] * np.exp(-2j * math.pi * f[:, None] * t[None, :])).sum(axis=1) * dt
+    return _source_spectrum(float(s["amplitude"]), float(s["p0"]), float(s["p1"]), float(s["p2"]), float(w.dt),
+                            int(w.n_steps), tuple(float(f) for f in w.freqs))
+
+
+@functools.lru_cache(maxsize=16)
+def _source_spectrum(amplitude: float, p0: float, p1: float, p2: float, dt: float, n_steps: int,
+                     freqs: tuple) -> np.ndarray:
+    t = np.arange(n_steps) * dt
+    u = (t - p1) / p2
+    v = amplitude * np.exp(-u * u) * np.sin(2.0 * math.pi * p0 * (t - p1))
+    f = np.asarray(freqs)
+    S = (v[None, :] * np.exp(-2j * math.pi * f[:, None] * t[None, :])).sum(axis=1) * dt
+    S.setflags(write=False)
+    return S
 
 
 def ez_free(w: sc.Workload, rx: int) -> np.ndarray:
